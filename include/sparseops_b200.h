@@ -1,0 +1,153 @@
+/* sparseops_b200.h -- C ABI of the B200 (sm_100a) SparseOps hot path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, status codes.  No C++,
+ * torch or CUDA types appear in the signatures (streams are passed as void*,
+ * i.e. a cudaStream_t).  Every entry point names the reference interface it
+ * replaces (lsl036/SparseOps, file:line).  The reference is a C++ template
+ * library with no FFI of its own; these are the functions a cgo / ctypes /
+ * JNI binding of its hot path binds (INTEGRATION.md shows the stubs), and the
+ * header-compatible C++ shim in include/spops_b200/SpOps.h is built on them.
+ *
+ * Conventions
+ *  - Every function returns spops_status_t; SPOPS_OK is 0.  On failure the
+ *    library never exits the process (the reference calls exit()/assert:
+ *    include/sparse_conversion.h:365-369, 728-743); spops_last_error() returns
+ *    a message for the calling thread.
+ *  - "device pointer" = memory of the context's device; "host pointer" =
+ *    ordinary (pageable or pinned) host memory.
+ *  - A matrix handle holds one storage format on the device plus whatever
+ *    analysis its kernels need (row blocks, transposes), built once and reused.
+ *  - Work is enqueued on the context's stream; functions that return host
+ *    data synchronise that stream.
+ */
+#ifndef SPARSEOPS_B200_H
+#define SPARSEOPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPOPS_ABI_VERSION 1
+
+typedef enum {
+  SPOPS_OK = 0,
+  SPOPS_ERR_INVALID = 1,     /* bad argument, shape or pointer */
+  SPOPS_ERR_UNSUPPORTED = 2, /* type/format combination not provided */
+  SPOPS_ERR_ALLOC = 3,       /* device or host allocation failed */
+  SPOPS_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+  SPOPS_ERR_TOO_LARGE = 5,   /* result would exceed a stated limit (e.g. DIA diagonals, ELL bytes) */
+  SPOPS_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up (work queue) */
+} spops_status_t;
+
+typedef enum { SPOPS_INDEX_I32 = 0, SPOPS_INDEX_I64 = 1 } spops_index_t;
+typedef enum { SPOPS_VALUE_F32 = 0, SPOPS_VALUE_F64 = 1 } spops_value_t;
+typedef enum { SPOPS_MEM_DEVICE = 0, SPOPS_MEM_HOST = 1 } spops_mem_t;
+
+/* Storage formats: the nine SpMV formats of include/sparse_format.h:49-295. */
+typedef enum {
+  SPOPS_FMT_CSR = 0,
+  SPOPS_FMT_COO = 1,
+  SPOPS_FMT_ELL = 2,
+  SPOPS_FMT_SELL = 3,         /* S-ELL: sliced ELL, chunks of C consecutive rows */
+  SPOPS_FMT_SELL_C_SIGMA = 4,
+  SPOPS_FMT_SELL_C_R = 5,     /* SELL-C-sigma with one global sort */
+  SPOPS_FMT_DIA = 6,
+  SPOPS_FMT_BSR = 7,
+  SPOPS_FMT_CSR5 = 8
+} spops_format_t;
+
+/* Element layout inside an ELL matrix or a SELL chunk.  ROW_MAJOR is the
+ * reference layout (include/sparse_conversion.h:237-249, 470-481); COL_MAJOR
+ * is the device-native one (lane i of a warp reads row i: coalesced). */
+typedef enum { SPOPS_ROW_MAJOR = 0, SPOPS_COL_MAJOR = 1 } spops_layout_t;
+
+typedef struct spops_context_s* spops_context_t;
+typedef struct spops_matrix_s* spops_matrix_t;
+
+/* Parameters of a format conversion; zero means "reference default". */
+typedef struct {
+  int64_t sigma;      /* SELL-C-sigma slice height (reference SELL_SIGMA = 16384) */
+  int64_t chunk;      /* C: rows per chunk (reference CHUNK_SIZE = 4) */
+  int64_t alignment;  /* chunk width multiple (reference SIMD_WIDTH/8/sizeof(V)) */
+  int64_t max_diags;  /* DIA limit (reference MAX_DIAG_NUM = 10240) */
+  int64_t block_rows; /* BSR (reference BSR_BlockDimRow = 16) */
+  int64_t block_cols; /* BSR (reference SIMD_WIDTH/8/sizeof(V)) */
+  int32_t layout;     /* spops_layout_t for ELL / SELL variants */
+  int32_t reserved;
+} spops_format_params_t;
+
+/* Scalar description of a matrix handle.  `extra` is format specific:
+ *   SELL_C_SIGMA: [sliceNum, chunkNum, validchunkNum, chunk_num_per_slice, stored_elems]
+ *   SELL_C_R / SELL: [chunks, stored_elems]
+ *   ELL:  [max_row_width, min_row_width]
+ *   DIA:  [complete_ndiags, stride]
+ *   BSR:  [mb, nb, nnzb, blockDim_r, blockDim_c]
+ *   CSR5: [tiles, omega, sigma] */
+typedef struct {
+  int64_t rows, cols, nnz;
+  int32_t format, index_type, value_type, layout;
+  int64_t sigma, chunk, alignment;
+  int64_t extra[8];
+} spops_matrix_info_t;
+
+/* ------------------------------------------------------------ context */
+/* One context per (device, stream).  stream may be NULL (legacy default). */
+spops_status_t spops_create(spops_context_t* ctx, int device, void* stream);
+spops_status_t spops_destroy(spops_context_t ctx);
+spops_status_t spops_set_stream(spops_context_t ctx, void* stream);
+spops_status_t spops_synchronize(spops_context_t ctx);
+const char* spops_status_string(spops_status_t s);
+const char* spops_last_error(void);
+int spops_abi_version(void);
+
+/* ------------------------------------------------------------- matrices */
+/* CSR matrix from row_offset[rows+1], col_index[nnz], values[nnz].
+ * SPOPS_MEM_DEVICE: the arrays are BORROWED (not copied); they must outlive
+ *   the handle and must not change while analysis results are in use
+ *   (call spops_matrix_touch after changing values in place).
+ * SPOPS_MEM_HOST: the arrays are uploaded into device memory the handle owns.
+ * Replaces the reference's host-side CSR_Matrix<I,V> (include/sparse_format.h:95-104)
+ * as consumed by SpOps_csr (src/spmv_csr.cpp:165). */
+spops_status_t spops_csr_create(spops_context_t ctx, spops_matrix_t* A, int64_t rows, int64_t cols, int64_t nnz,
+                                const void* row_offset, const void* col_index, const void* values,
+                                spops_index_t itype, spops_value_t vtype, spops_mem_t mem);
+/* COO triplets; rows need not be sorted (include/sparse_format.h:72-81). */
+spops_status_t spops_coo_create(spops_context_t ctx, spops_matrix_t* A, int64_t rows, int64_t cols, int64_t nnz,
+                                const void* row_index, const void* col_index, const void* values,
+                                spops_index_t itype, spops_value_t vtype, spops_mem_t mem);
+spops_status_t spops_matrix_destroy(spops_matrix_t A);
+spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info);
+/* Values changed in place (same pattern): drop value-derived caches. */
+spops_status_t spops_matrix_touch(spops_matrix_t A);
+/* Build the analysis a format's SpMV uses (lazily done by the first SpMV). */
+spops_status_t spops_matrix_analyse(spops_context_t ctx, spops_matrix_t A);
+/* Bytes of device memory the handle owns (arrays + analysis). */
+spops_status_t spops_matrix_device_bytes(spops_matrix_t A, int64_t* bytes);
+
+/* ---------------------------------------------------------------- SpMV */
+/* y = alpha*A*x + beta*y on the device; x[cols], y[rows] device pointers of
+ * A's value type.  beta == 0 overwrites y without reading it.
+ * Replaces SpOps_<fmt>(alpha, A, x, beta, y) for every format:
+ *   csr src/spmv_csr.cpp:165, coo src/spmv_coo.cpp:160, ell src/spmv_ell.cpp:225,
+ *   sell src/spmv_s_ell.cpp:202, sell_c_sigma src/spmv_sell_c_sigma.cpp:189,
+ *   sell_c_R src/spmv_sell_c_R.cpp:190, dia src/spmv_dia.cpp:177,
+ *   bsr src/spmv_bsr.cpp:214, csr5 src/spmv_csr5.cpp:439. */
+spops_status_t spops_spmv(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x, double beta,
+                          void* y);
+/* Same with HOST x and y: uploads x (and y when beta != 0), downloads y.
+ * The drop-in path of the header shim (host pointers in, host pointers out). */
+spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x_host,
+                               double beta, void* y_host);
+/* Multi-RHS: Y = alpha*A*X + beta*Y with X [cols x k], Y [rows x k],
+ * row-major with leading dimensions ldx, ldy (>= k).  No reference
+ * counterpart (the reference has no SpMM); equals k SpOps_csr calls. */
+spops_status_t spops_spmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* X, int64_t ldx,
+                          int64_t k, double beta, void* Y, int64_t ldy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPARSEOPS_B200_H */

@@ -1,0 +1,295 @@
+"""The oracle: CPU restatement of the SparseOps hot path, plus the reference
+library itself compiled from its sources (oracle/_ref).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()`` and
+bench.py's CPU-baseline / reference legs may import this package, and only as
+the checker or as the timed CPU baseline.  The product package
+(``sparseops_b200``) never imports it.
+
+``Oracle`` wraps liboracle.so (oracle/spops_oracle.cpp, this repository's own
+restatement).  ``Reference`` wraps oracle/_ref/libspops_ref_v{3,4}.so, the
+reference's own OpenMP kernels behind oracle/ref_harness.cpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_i64 = C.c_int64
+_vp = C.c_void_p
+_dbl = C.c_double
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference sources exist)."""
+    target = "all" if ref else "oracle"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+def _cpu_has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+        return all(x in flags for x in ("avx512f", "avx512dq", "avx512bw", "avx512vl"))
+    except OSError:
+        return False
+
+
+class Oracle:
+    """ctypes view of liboracle.so; numpy in, numpy out."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        self.L = L = C.CDLL(path)
+        for name in ("orc_lsh_pairs", "orc_spgemm"):
+            getattr(L, name).restype = _vp
+        for name in ("orc_pairs_count", "orc_hc", "orc_dia_offsets", "orc_bsr_structure",
+                     "orc_spgemm_flop"):
+            getattr(L, name).restype = _i64
+
+    # ---- SpMV
+    def spmv_csr(self, rp, ci, v, x, alpha=1.0, beta=0.0, y=None):
+        n = len(rp) - 1
+        out = np.zeros(n) if y is None else np.array(y, dtype=np.float64, copy=True)
+        if v.dtype == np.float32:
+            self.L.orc_spmv_csr_f32_i32(_i64(n), _p(rp), _p(ci), _p(v), _dbl(alpha), _p(x), _dbl(beta),
+                                        _p(None if y is None else np.ascontiguousarray(y, np.float32)),
+                                        _p(out))
+        elif rp.dtype == np.int64:
+            self.L.orc_spmv_csr_f64_i64(_i64(n), _p(rp), _p(ci), _p(v), _dbl(alpha), _p(x), _dbl(beta), _p(out))
+        else:
+            self.L.orc_spmv_csr_f64_i32(_i64(n), _p(rp), _p(ci), _p(v), _dbl(alpha), _p(x), _dbl(beta), _p(out))
+        return out
+
+    def absdot(self, rp, ci, v, x):
+        n = len(rp) - 1
+        out = np.zeros(n)
+        self.L.orc_absdot_csr_f64_i32(_i64(n), _p(rp), _p(ci), _p(np.ascontiguousarray(v, np.float64)),
+                                      _p(np.ascontiguousarray(x, np.float64)), _p(out))
+        return out
+
+    def spmm_csr(self, rp, ci, v, X, alpha=1.0, beta=0.0, Y=None):
+        n, k = len(rp) - 1, X.shape[1]
+        out = np.zeros((n, k)) if Y is None else np.array(Y, dtype=np.float64, copy=True)
+        self.L.orc_spmm_csr_f64_i32(_i64(n), _p(rp), _p(ci), _p(v), _i64(k), _dbl(alpha),
+                                    _p(np.ascontiguousarray(X)), _dbl(beta), _p(out))
+        return out
+
+    # ---- layouts
+    def sell_c_sigma_layout(self, rp, sigma, C_, align):
+        n = len(rp) - 1
+        reorder = np.zeros(n, np.int32)
+        chunk_len = np.zeros((n + C_ - 1) // C_, np.int32)
+        self.L.orc_sell_c_sigma_layout(_i64(n), _p(rp), _i64(sigma), _i64(C_), _i64(align), _p(reorder),
+                                       _p(chunk_len))
+        return reorder, chunk_len
+
+    def sell_row_width(self, rp, C_, align):
+        n = len(rp) - 1
+        w = np.zeros((n + C_ - 1) // C_, np.int32)
+        self.L.orc_sell_row_width(_i64(n), _p(rp), _i64(C_), _i64(align), _p(w))
+        return w
+
+    def dia_offsets(self, rp, ci, ncols, max_out=1 << 20):
+        n = len(rp) - 1
+        off = np.zeros(max_out, np.int64)
+        nd = self.L.orc_dia_offsets(_i64(n), _i64(ncols), _p(rp), _p(ci), _i64(max_out), _p(off))
+        return off[:min(nd, max_out)], nd
+
+    def bsr_structure(self, rp, ci, ncols, br, bc):
+        n = len(rp) - 1
+        mb = (n + br - 1) // br
+        row_ptr = np.zeros(mb + 1, np.int32)
+        nnzb = self.L.orc_bsr_structure(_i64(n), _i64(ncols), _p(rp), _p(ci), _i64(br), _i64(bc), _p(row_ptr),
+                                        None)
+        bcol = np.zeros(max(nnzb, 1), np.int32)
+        self.L.orc_bsr_structure(_i64(n), _i64(ncols), _p(rp), _p(ci), _i64(br), _i64(bc), _p(row_ptr), _p(bcol))
+        return row_ptr, bcol[:nnzb]
+
+    # ---- LeSpGEMM preprocessing
+    def minhash(self, rp, ci, k, seed):
+        n = len(rp) - 1
+        sig = np.zeros((n, k), np.uint64)
+        self.L.orc_minhash(_p(rp), _p(ci), _i64(n), C.c_int32(k), C.c_uint64(seed), _p(sig))
+        return sig
+
+    def lsh_pairs(self, sig, bands, constrain=True):
+        n, k = sig.shape
+        h = self.L.orc_lsh_pairs(_p(np.ascontiguousarray(sig)), _i64(n), C.c_int32(k), C.c_int32(bands),
+                                 C.c_int32(1 if constrain else 0))
+        m = self.L.orc_pairs_count(_vp(h))
+        i, j, s = np.zeros(m, np.int64), np.zeros(m, np.int64), np.zeros(m)
+        self.L.orc_pairs_copy(_vp(h), _p(i), _p(j), _p(s))
+        self.L.orc_pairs_free(_vp(h))
+        return i, j, s
+
+    def hc(self, rp, ci, pi, pj, ps, cluster_size):
+        n = len(rp) - 1
+        perm, offs = np.zeros(n, np.int64), np.zeros(n + 1, np.int64)
+        nc = self.L.orc_hc(_p(rp), _p(ci), _i64(n), _p(pi), _p(pj), _p(ps), _i64(len(pi)), _i64(cluster_size),
+                           _p(perm), _p(offs))
+        return perm, offs[:nc + 1]
+
+    def spgemm(self, A, B, perm, offsets, sort_output=False, l2_budget=67108864 * 0.75):
+        arp, aci, av = A
+        brp, bci, bv = B[:3]
+        n = len(arp) - 1
+        h = self.L.orc_spgemm(_i64(n), _p(arp), _p(aci), _p(av), _i64(len(brp) - 1), _i64(0), _p(brp), _p(bci),
+                              _p(bv), _p(perm), _p(offsets), _i64(len(offsets) - 1), C.c_int32(int(sort_output)),
+                              _dbl(l2_budget))
+        info = np.zeros(4, np.int64)
+        self.L.orc_csr_info(_vp(h), _p(info))
+        rp = np.zeros(n + 1, np.int64)
+        ci, v, a = np.zeros(info[1], np.int64), np.zeros(info[1]), np.zeros(info[1])
+        self.L.orc_csr_copy(_vp(h), _p(rp), _p(ci), _p(v), _p(a))
+        self.L.orc_csr_free(_vp(h))
+        return dict(rp=rp, ci=ci, v=v, absv=a, dense_clusters=int(info[2]), flops=int(info[3]))
+
+    def spgemm_flop(self, A, B):
+        arp, aci = A[0], A[1]
+        brp = B[0]
+        return int(self.L.orc_spgemm_flop(_i64(len(arp) - 1), _p(arp), _p(aci), _i64(len(brp) - 1), _p(brp)))
+
+    # ---- adjoints
+    def spmv_t(self, rp, ci, v, g, ncols):
+        y = np.zeros(ncols)
+        self.L.orc_spmv_t_csr_f64_i32(_i64(len(rp) - 1), _i64(ncols), _p(rp), _p(ci),
+                                      _p(np.ascontiguousarray(v, np.float64)), _p(g), _p(y))
+        return y
+
+    def sddmm(self, rp, ci, g, x):
+        out = np.zeros(int(rp[-1]))
+        self.L.orc_sddmm_csr_f64_i32(_i64(len(rp) - 1), _p(rp), _p(ci), _p(g), _p(x), _p(out))
+        return out
+
+
+class Reference:
+    """ctypes view of the reference library compiled from its own sources.
+
+    Picks the AVX-512 build when the host supports it, else the AVX2 build.
+    ``threads`` sets the reference's global thread count (Le_set_thread_num).
+    """
+
+    KINDS = dict(csr=1, sell_c_sigma=2, sell_c_R=3, sell=4, ell=5, dia=6, bsr=7, coo=8)
+
+    def __init__(self, threads: int | None = None):
+        v = "v4" if _cpu_has_avx512() else "v3"
+        path = os.path.join(HERE, "_ref", f"libspops_ref_{v}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference library not built: {path}")
+        self.path = path
+        self.L = L = C.CDLL(path)
+        for name in ("ref_fmt_build", "ref_lsh_pairs", "ref_spgemm_kernel3", "ref_csr_transpose"):
+            getattr(L, name).restype = _vp
+        L.ref_pairs_count.restype = _i64
+        L.ref_hc.restype = _i64
+        L.ref_spgemm_kernel3_time.restype = _dbl
+        self.set_threads(threads or os.cpu_count() or 1)
+
+    def set_threads(self, n: int) -> None:
+        self.L.ref_set_threads(C.c_int(int(n)))
+        self.threads = int(n)
+
+    def spmv_csr(self, rp, ci, v, x, alpha=1.0, beta=0.0, y=None, flag=2, out=None):
+        """Reference SpOps_csr.  `out` (contiguous, v.dtype) is written in place
+        when given; otherwise a new array (initialised from y) is returned."""
+        n = len(rp) - 1
+        if out is None:
+            out = np.zeros(n, v.dtype) if y is None else np.array(y, dtype=v.dtype, copy=True)
+        ncols = len(x)
+        if v.dtype == np.float32:
+            self.L.ref_spmv_csr_f32(C.c_int(n), C.c_int(ncols), C.c_int(len(ci)), _p(rp), _p(ci), _p(v),
+                                    C.c_float(alpha), _p(x), C.c_float(beta), _p(out), C.c_int(flag))
+        elif rp.dtype == np.int64:
+            self.L.ref_spmv_csr_f64_i64(_i64(n), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _p(v), _dbl(alpha),
+                                        _p(x), _dbl(beta), _p(out), C.c_int(flag))
+        else:
+            self.L.ref_spmv_csr_f64(C.c_int(n), C.c_int(ncols), C.c_int(len(ci)), _p(rp), _p(ci), _p(v),
+                                    _dbl(alpha), _p(x), _dbl(beta), _p(out), C.c_int(flag))
+        return out
+
+    # format handle: build, inspect, run, free
+    def fmt_build(self, kind, rp, ci, v, ncols, p0=0, p1=0, p2=0, flag=1):
+        n = len(rp) - 1
+        return self.L.ref_fmt_build(C.c_int(self.KINDS[kind]), C.c_int(n), C.c_int(ncols), C.c_int(len(ci)),
+                                    _p(rp), _p(ci), _p(v), _i64(p0), _i64(p1), _i64(p2), C.c_int(flag))
+
+    def fmt_info(self, h):
+        out = np.zeros(8, np.int64)
+        self.L.ref_fmt_info(_vp(h), _p(out))
+        return out
+
+    def fmt_copy(self, h, a=None, b=None, c=None, d=None):
+        self.L.ref_fmt_copy(_vp(h), _p(a), _p(b), _p(c), _p(d))
+
+    def fmt_spmv(self, h, x, alpha=1.0, beta=0.0, y=None, n=None):
+        out = np.zeros(n) if y is None else np.array(y, dtype=np.float64, copy=True)
+        self.L.ref_fmt_spmv(_vp(h), _dbl(alpha), _p(x), _dbl(beta), _p(out))
+        return out
+
+    def fmt_free(self, h):
+        self.L.ref_fmt_free(_vp(h))
+
+    def minhash(self, rp, ci, k, seed):
+        n = len(rp) - 1
+        sig = np.zeros((n, k), np.uint64)
+        self.L.ref_minhash_flat(_p(rp), _p(ci), _i64(n), C.c_int(k), C.c_uint64(seed), _p(sig))
+        return sig
+
+    def lsh_pairs(self, rp, ci, k, bands, seed, constrain=True):
+        h = self.L.ref_lsh_pairs(_p(rp), _p(ci), _i64(len(rp) - 1), C.c_int(k), C.c_int(bands),
+                                 C.c_uint64(seed), C.c_int(1 if constrain else 0))
+        m = self.L.ref_pairs_count(_vp(h))
+        i, j, s = np.zeros(m, np.int64), np.zeros(m, np.int64), np.zeros(m)
+        self.L.ref_pairs_copy(_vp(h), _p(i), _p(j), _p(s))
+        self.L.ref_pairs_free(_vp(h))
+        return i, j, s
+
+    def hc(self, rp, ci, pi, pj, ps, cluster_size):
+        n = len(rp) - 1
+        perm, offs = np.zeros(n, np.int64), np.zeros(n + 1, np.int64)
+        nc = self.L.ref_hc(_p(rp), _p(ci), _i64(n), _p(pi), _p(pj), _p(ps), _i64(len(pi)), _i64(cluster_size),
+                           _p(perm), _p(offs))
+        return perm, offs[:nc + 1]
+
+    def spgemm_kernel3(self, A, B, perm, offsets, sort_output=False, l2_fraction=-1.0):
+        arp, aci, av = A
+        brp, bci, bv = B[:3]
+        n = len(arp) - 1
+        bcols = int(B[3]) if len(B) > 3 else n
+        h = self.L.ref_spgemm_kernel3(_i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av),
+                                      _i64(len(brp) - 1), _i64(bcols), _i64(len(bci)), _p(brp), _p(bci),
+                                      _p(bv), _p(perm), _p(offsets), _i64(len(offsets) - 1),
+                                      C.c_int(int(sort_output)), _dbl(l2_fraction))
+        info = np.zeros(6, np.int64)
+        self.L.ref_csr_info(_vp(h), _p(info))
+        rp = np.zeros(info[0] + 1, np.int64)
+        ci, v = np.zeros(max(info[2], 1), np.int64), np.zeros(max(info[2], 1))
+        self.L.ref_csr_copy(_vp(h), _p(rp), _p(ci), _p(v))
+        self.L.ref_csr_free(_vp(h))
+        return dict(rp=rp, ci=ci[:info[2]], v=v[:info[2]], dense_clusters=int(info[3]), clusters=int(info[4]))
+
+    def csr_transpose(self, rp, ci, v, ncols):
+        h = self.L.ref_csr_transpose(_i64(len(rp) - 1), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _p(v))
+        info = np.zeros(6, np.int64)
+        self.L.ref_csr_info(_vp(h), _p(info))
+        trp = np.zeros(info[0] + 1, np.int64)
+        tci, tv = np.zeros(max(info[2], 1), np.int64), np.zeros(max(info[2], 1))
+        self.L.ref_csr_copy(_vp(h), _p(trp), _p(tci), _p(tv))
+        self.L.ref_csr_free(_vp(h))
+        return trp, tci[:info[2]], tv[:info[2]]
+
+
+def reference_available() -> bool:
+    v = "v4" if _cpu_has_avx512() else "v3"
+    return os.path.exists(os.path.join(HERE, "_ref", f"libspops_ref_{v}.so"))

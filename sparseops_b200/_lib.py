@@ -1,0 +1,95 @@
+"""ctypes binding of libsparseops_b200.so (the C ABI in include/sparseops_b200.h).
+
+The product path has no fallback: if the shared library is missing or does
+not load, every entry point raises.  Build it with
+``python -m sparseops_b200.build`` (``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsparseops_b200.so")
+
+i64, i32, u64, dbl, vp = C.c_int64, C.c_int32, C.c_uint64, C.c_double, C.c_void_p
+
+
+class SpOpsError(RuntimeError):
+    """A C ABI call returned a status other than SPOPS_OK."""
+
+    def __init__(self, status: int, func: str, msg: str):
+        self.status = status
+        super().__init__(f"{func} -> {STATUS_NAMES.get(status, status)}: {msg}")
+
+
+STATUS_NAMES = {0: "SPOPS_OK", 1: "SPOPS_ERR_INVALID", 2: "SPOPS_ERR_UNSUPPORTED", 3: "SPOPS_ERR_ALLOC",
+                4: "SPOPS_ERR_CUDA", 5: "SPOPS_ERR_TOO_LARGE", 6: "SPOPS_ERR_TIMEOUT"}
+
+INDEX = {"i32": 0, "i64": 1}
+VALUE = {"f32": 0, "f64": 1}
+FORMATS = {"csr": 0, "coo": 1, "ell": 2, "sell": 3, "sell_c_sigma": 4, "sell_c_R": 5, "dia": 6, "bsr": 7,
+           "csr5": 8}
+
+
+class MatrixInfo(C.Structure):
+    _fields_ = [("rows", i64), ("cols", i64), ("nnz", i64), ("format", i32), ("index_type", i32),
+                ("value_type", i32), ("layout", i32), ("sigma", i64), ("chunk", i64), ("alignment", i64),
+                ("extra", i64 * 8)]
+
+
+class FormatParams(C.Structure):
+    _fields_ = [("sigma", i64), ("chunk", i64), ("alignment", i64), ("max_diags", i64), ("block_rows", i64),
+                ("block_cols", i64), ("layout", i32), ("reserved", i32)]
+
+
+# name -> argtypes (restype is spops_status_t unless listed in _RESTYPE)
+_SIGS = {
+    "spops_create": [vp, C.c_int, vp],
+    "spops_destroy": [vp],
+    "spops_set_stream": [vp, vp],
+    "spops_synchronize": [vp],
+    "spops_csr_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
+    "spops_matrix_destroy": [vp],
+    "spops_matrix_info": [vp, vp],
+    "spops_matrix_touch": [vp],
+    "spops_matrix_analyse": [vp, vp],
+    "spops_matrix_device_bytes": [vp, vp],
+    "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
+    "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
+}
+_RESTYPE = {"spops_last_error": C.c_char_p, "spops_status_string": C.c_char_p, "spops_abi_version": C.c_int}
+
+_L = None
+
+
+def lib() -> C.CDLL:
+    """Load the library once; raise if it is missing (no fallback path)."""
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m sparseops_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, argt in _SIGS.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.argtypes = argt
+            f.restype = C.c_int
+        for name, rt in _RESTYPE.items():
+            getattr(L, name).restype = rt
+        _L = L
+    return _L
+
+
+def call(name: str, *args) -> None:
+    """Call a C ABI function and raise SpOpsError on a non-OK status."""
+    L = lib()
+    st = getattr(L, name)(*args)
+    if st != 0:
+        msg = L.spops_last_error()
+        raise SpOpsError(st, name, msg.decode() if msg else "")
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS) + list(_RESTYPE)

@@ -1,0 +1,130 @@
+// Context, error reporting and device buffers behind the C ABI.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "spops_internal.h"
+
+namespace spops {
+
+namespace {
+thread_local char g_err[1024] = "";
+}
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+spops_status_t fail(spops_status_t s, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return s;
+}
+
+spops_status_t cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  const char* base = strrchr(file, '/');
+  set_error("%s failed: %s (%s:%d)", what, cudaGetErrorString(e), base ? base + 1 : file, line);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();  // clear the sticky-free allocation error
+    return SPOPS_ERR_ALLOC;
+  }
+  return SPOPS_ERR_CUDA;
+}
+
+spops_status_t DevBuf::alloc(size_t n) {
+  release();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+  }
+  bytes = n;
+  own = true;
+  return SPOPS_OK;
+}
+
+void DevBuf::release() {
+  if (own && p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  own = false;
+}
+
+spops_status_t Context::scratch_reserve(size_t n) {
+  if (scratch.bytes >= n && scratch.p) return SPOPS_OK;
+  // work queued on the stream may still read the old scratch
+  SPOPS_CUDA(cudaStreamSynchronize(stream));
+  size_t want = n + n / 4 + 4096;
+  return scratch.alloc(want);
+}
+
+}  // namespace spops
+
+using namespace spops;
+
+extern "C" {
+
+const char* spops_last_error(void) { return g_err; }
+
+int spops_abi_version(void) { return SPOPS_ABI_VERSION; }
+
+const char* spops_status_string(spops_status_t s) {
+  switch (s) {
+    case SPOPS_OK: return "SPOPS_OK";
+    case SPOPS_ERR_INVALID: return "SPOPS_ERR_INVALID";
+    case SPOPS_ERR_UNSUPPORTED: return "SPOPS_ERR_UNSUPPORTED";
+    case SPOPS_ERR_ALLOC: return "SPOPS_ERR_ALLOC";
+    case SPOPS_ERR_CUDA: return "SPOPS_ERR_CUDA";
+    case SPOPS_ERR_TOO_LARGE: return "SPOPS_ERR_TOO_LARGE";
+    case SPOPS_ERR_TIMEOUT: return "SPOPS_ERR_TIMEOUT";
+  }
+  return "SPOPS_ERR_UNKNOWN";
+}
+
+spops_status_t spops_create(spops_context_t* out, int device, void* stream) {
+  if (!out) return fail(SPOPS_ERR_INVALID, "spops_create: null output");
+  int ndev = 0;
+  SPOPS_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(SPOPS_ERR_INVALID, "spops_create: device %d of %d", device, ndev);
+  DeviceGuard g(device);
+  spops_context_s* c = new spops_context_s();
+  c->device = device;
+  c->stream = static_cast<cudaStream_t>(stream);
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  *out = c;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_destroy(spops_context_t c) {
+  if (!c) return SPOPS_OK;
+  DeviceGuard g(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->scratch.release();
+  c->xbuf.release();
+  c->ybuf.release();
+  if (c->pinned) cudaFreeHost(c->pinned);
+  delete c;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_set_stream(spops_context_t c, void* stream) {
+  if (!c) return fail(SPOPS_ERR_INVALID, "spops_set_stream: null context");
+  c->stream = static_cast<cudaStream_t>(stream);
+  return SPOPS_OK;
+}
+
+spops_status_t spops_synchronize(spops_context_t c) {
+  if (!c) return fail(SPOPS_ERR_INVALID, "spops_synchronize: null context");
+  DeviceGuard g(c->device);
+  SPOPS_CUDA(cudaStreamSynchronize(c->stream));
+  return SPOPS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+// Internal C++ view of the library state behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/sparseops_b200.h"
+
+namespace spops {
+
+// ----------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+spops_status_t fail(spops_status_t s, const char* fmt, ...);
+spops_status_t cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define SPOPS_CUDA(call)                                                     \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return ::spops::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define SPOPS_TRY(call)                        \
+  do {                                         \
+    spops_status_t s_ = (call);                \
+    if (s_ != SPOPS_OK) return s_;             \
+  } while (0)
+
+// Kernel launch check: launch-configuration errors only (no synchronisation).
+#define SPOPS_LAUNCH_CHECK() SPOPS_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------- buffers
+// Device allocation owned by a handle (or borrowed when own == false).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool own = false;
+  spops_status_t alloc(size_t n);
+  void release();
+  void borrow(const void* q, size_t n) { release(); p = const_cast<void*>(q); bytes = n; own = false; }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------- context
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  // grow-only scratch for temporary device storage (CUB temp, staging)
+  DevBuf scratch;
+  spops_status_t scratch_reserve(size_t bytes);
+  // pinned staging for host x / y in spops_spmv_host
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  DevBuf xbuf, ybuf;
+};
+
+// RAII guard: make ctx->device current for the duration of an API call.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// --------------------------------------------------- CSR stream analysis
+// Row-block partition of a CSR matrix for the streaming SpMV kernel
+// (spmv_csr.cu).  Block b covers rows [blk_row[b], next block's row) when
+// blk_chunk[b] < 0 (a segment of short rows whose entries fit in shared
+// memory), or chunk blk_chunk[b] of the single long row blk_row[b].
+struct CsrPlan {
+  bool ready = false;
+  int64_t nblocks = 0;
+  int64_t nlong = 0;       // long rows (more than one chunk)
+  int cap = 0;             // entries per chunk
+  DevBuf blk_row;          // int64 [nblocks + 1]
+  DevBuf blk_chunk;        // int32 [nblocks]
+  DevBuf partial;          // V [nblocks] long-row chunk sums
+  DevBuf counter;          // int32 [nblocks] arrival counters (zero between calls)
+  void release() { blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); ready = false; }
+};
+
+// ---------------------------------------------------------------- matrix
+struct Matrix {
+  Context* ctx = nullptr;
+  spops_format_t format = SPOPS_FMT_CSR;
+  spops_index_t itype = SPOPS_INDEX_I32;
+  spops_value_t vtype = SPOPS_VALUE_F64;
+  spops_layout_t layout = SPOPS_ROW_MAJOR;
+  int64_t rows = 0, cols = 0, nnz = 0;
+  // CSR / COO arrays (COO: row = row index array)
+  DevBuf row, col, val;
+  CsrPlan plan;
+  size_t isize() const { return itype == SPOPS_INDEX_I32 ? 4 : 8; }
+  size_t vsize() const { return vtype == SPOPS_VALUE_F32 ? 4 : 8; }
+  void release_all() { row.release(); col.release(); val.release(); plan.release(); }
+};
+
+// ------------------------------------------------------------ kernels API
+spops_status_t csr_analyse(Context* ctx, Matrix* A);
+spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+
+}  // namespace spops
+
+struct spops_context_s : spops::Context {};
+struct spops_matrix_s : spops::Matrix {};

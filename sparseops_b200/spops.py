@@ -1,0 +1,197 @@
+"""Host-side mirror of the reference's SpOps API over the C ABI.
+
+Names, argument order and meaning follow the reference's include/SpOps.h
+templates: ``SpOps_csr(alpha, A, x, beta, y)`` computes y = alpha*A*x + beta*y
+(src/spmv_csr.cpp:165).  Matrices are the reference's structs
+(include/sparse_format.h) with their arrays held either in host numpy arrays
+(uploaded once, like the C++ shim's device cache) or in CUDA tensors
+(borrowed, zero copy).  Vectors may be CUDA tensors (device path) or numpy
+arrays (host path: x is uploaded, y downloaded, per call).
+
+torch is used only for device memory and the current stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, dbl, i64, vp
+
+try:  # torch is plumbing: device memory, streams
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+
+def _is_cuda_tensor(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if _is_cuda_tensor(a):
+        return vp(a.data_ptr())
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(vp)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _itype(a) -> int:
+    dt = a.dtype
+    if dt in (np.int32, getattr(torch, "int32", None)):
+        return 0
+    if dt in (np.int64, getattr(torch, "int64", None)):
+        return 1
+    raise TypeError(f"index arrays must be int32 or int64, got {dt}")
+
+
+def _vtype(a) -> int:
+    dt = a.dtype
+    if dt in (np.float32, getattr(torch, "float32", None)):
+        return 0
+    if dt in (np.float64, getattr(torch, "float64", None)):
+        return 1
+    raise TypeError(f"value arrays must be float32 or float64, got {dt}")
+
+
+class Context:
+    """A library context bound to one device and one stream (spops_create)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        h = vp()
+        call("spops_create", C.byref(h), int(device), vp(stream) if stream else None)
+        self.handle = h
+        self.device = int(device)
+        self._stream = stream
+
+    def set_stream(self, stream: int | None) -> None:
+        if stream != self._stream:
+            call("spops_set_stream", self.handle, vp(stream) if stream else None)
+            self._stream = stream
+
+    def follow_torch(self) -> "Context":
+        """Enqueue on torch's current stream for this device."""
+        if torch is not None and torch.cuda.is_available():
+            self.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+        return self
+
+    def synchronize(self) -> None:
+        call("spops_synchronize", self.handle)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            _lib.lib().spops_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_CTX: dict[int, Context] = {}
+
+
+def default_context(device: int | None = None) -> Context:
+    if device is None:
+        device = torch.cuda.current_device() if (torch is not None and torch.cuda.is_available()) else 0
+    ctx = _CTX.get(device)
+    if ctx is None:
+        ctx = _CTX[device] = Context(device)
+    return ctx.follow_torch()
+
+
+class _Handle:
+    """Owns one spops_matrix_t and keeps its borrowed arrays alive."""
+
+    def __init__(self, ctx: Context, handle, keep=()):
+        self.ctx, self.handle, self._keep = ctx, handle, keep
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                _lib.lib().spops_matrix_destroy(self.handle)
+        except Exception:
+            pass
+
+    def info(self) -> _lib.MatrixInfo:
+        out = _lib.MatrixInfo()
+        call("spops_matrix_info", self.handle, C.byref(out))
+        return out
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        call("spops_matrix_device_bytes", self.handle, C.byref(b))
+        return b.value
+
+
+class Matrix_Features:
+    """Common fields of every reference format (include/sparse_format.h:49-69)."""
+
+    num_rows: int
+    num_cols: int
+    num_nnzs: int
+    kernel_flag: int = 1
+
+    def __init__(self):
+        self._h: _Handle | None = None
+        self.kernel_flag = 1
+
+
+class CSR_Matrix(Matrix_Features):
+    """Compressed sparse row matrix (include/sparse_format.h:95-104).
+
+    Arrays may be numpy (host, uploaded on first use) or CUDA tensors
+    (device, borrowed).  ``kernel_flag`` is accepted for API compatibility;
+    every value selects the same device kernel.
+    """
+
+    def __init__(self, num_rows, num_cols, row_offset, col_index, values, kernel_flag: int = 1):
+        super().__init__()
+        self.num_rows, self.num_cols = int(num_rows), int(num_cols)
+        self.row_offset, self.col_index, self.values = row_offset, col_index, values
+        self.num_nnzs = int(len(col_index))
+        self.kernel_flag = kernel_flag
+
+    def device(self, ctx: Context | None = None) -> _Handle:
+        """The device-resident handle (created, and analysed, on first use)."""
+        if self._h is None:
+            ctx = ctx or default_context()
+            on_dev = _is_cuda_tensor(self.values)
+            h = vp()
+            call("spops_csr_create", ctx.handle, C.byref(h), i64(self.num_rows), i64(self.num_cols),
+                 i64(self.num_nnzs), _ptr(self.row_offset), _ptr(self.col_index), _ptr(self.values),
+                 _itype(self.col_index), _vtype(self.values), 0 if on_dev else 1)
+            self._h = _Handle(ctx, h, (self.row_offset, self.col_index, self.values) if on_dev else ())
+            call("spops_matrix_analyse", ctx.handle, h)
+        return self._h
+
+    def touch(self) -> None:
+        """Values were changed in place (same pattern)."""
+        if self._h is not None:
+            call("spops_matrix_touch", self._h.handle)
+
+
+def _spmv(alpha, A: Matrix_Features, x, beta, y):
+    h = A.device()
+    ctx = h.ctx
+    if _is_cuda_tensor(x):
+        if not _is_cuda_tensor(y):
+            raise TypeError("x is a CUDA tensor but y is not")
+        ctx.follow_torch()
+        call("spops_spmv", ctx.handle, dbl(alpha), h.handle, _ptr(x), dbl(beta), _ptr(y))
+    else:
+        if not (isinstance(x, np.ndarray) and isinstance(y, np.ndarray)):
+            raise TypeError("x and y must both be CUDA tensors or both numpy arrays")
+        call("spops_spmv_host", ctx.handle, dbl(alpha), h.handle, _ptr(np.ascontiguousarray(x)), dbl(beta),
+             _ptr(y))
+    return y
+
+
+def SpOps_csr(alpha, csr: CSR_Matrix, x, beta, y):
+    """y = alpha*A*x + beta*y for a CSR matrix (reference src/spmv_csr.cpp:165)."""
+    return _spmv(alpha, csr, x, beta, y)

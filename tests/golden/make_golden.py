@@ -1,0 +1,136 @@
+"""Write the golden fixtures in this directory from the REFERENCE itself.
+
+    python tests/golden/make_golden.py      (needs oracle/_ref, i.e. `make -C oracle ref`)
+
+Every array in golden.npz is an output of the reference SparseOps library,
+compiled from its own sources (oracle/Makefile) and called through
+oracle/ref_harness.cpp, on small seeded synthetic inputs (sparseops_b200.synth).
+The reference ships no golden vectors or known-answer tests of its own
+(its SpGEMM goldens and SuiteSparse inputs are not part of the repository), so
+these fixtures pin the oracle's restatement (tests/test_oracle_golden.py) and,
+through the oracle, the device kernels.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import Reference  # noqa: E402
+from sparseops_b200 import synth  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.npz")
+
+
+def sort_rows(rp, ci, v):
+    ci, v = ci.copy(), v.copy()
+    for r in range(len(rp) - 1):
+        a, b = rp[r], rp[r + 1]
+        o = np.argsort(ci[a:b], kind="stable")
+        ci[a:b], v[a:b] = ci[a:b][o], v[a:b][o]
+    return ci, v
+
+
+def main():
+    R = Reference(threads=4)
+    g = {}
+
+    # ---- CSR SpMV: y = 0.8*A*x + 0.7*y0 (the reference's own test alpha/beta,
+    # include/sparse_operation.h:123-124), kernel_flag 2
+    for name, (rp, ci, v) in {
+        "lap": synth.laplacian_2d(32),
+        "pl": synth.powerlaw(2000, hi=300, seed=11),
+    }.items():
+        n = len(rp) - 1
+        x = synth.uniform(n, 0)
+        y0 = synth.uniform(n, 1)
+        g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"], g[f"{name}_x"], g[f"{name}_y0"] = rp, ci, v, x, y0
+        g[f"{name}_y"] = R.spmv_csr(rp, ci, v, x, 0.8, 0.7, y0, flag=2)
+
+    # ---- layouts on the power-law matrix
+    rp, ci, v = g["pl_rp"], g["pl_ci"], g["pl_v"]
+    n = len(rp) - 1
+    for tag, (sig, C_, al) in {"a": (512, 32, 8), "b": (64, 4, 4), "c": (16384, 4, 4)}.items():
+        h = R.fmt_build("sell_c_sigma", rp, ci, v, n, sig, C_, al)
+        info = R.fmt_info(h)
+        ro, cl = np.zeros(n, np.int32), np.zeros(info[2], np.int32)
+        col, val = np.zeros(info[5], np.int32), np.zeros(info[5])
+        R.fmt_copy(h, ro, cl, col, val)
+        g[f"scs_{tag}_reorder"], g[f"scs_{tag}_chunk_len"] = ro, cl
+        R.fmt_free(h)
+    h = R.fmt_build("sell_c_R", rp, ci, v, n, 0, 32, 8)
+    info = R.fmt_info(h)
+    ro, cl = np.zeros(n, np.int32), np.zeros(info[0], np.int32)
+    R.fmt_copy(h, ro, cl)
+    g["scr_reorder"], g["scr_chunk_len"] = ro, cl
+    R.fmt_free(h)
+    h = R.fmt_build("sell", rp, ci, v, n, 0, 4, 4)
+    info = R.fmt_info(h)
+    w = np.zeros(info[0], np.int32)
+    R.fmt_copy(h, w)
+    g["sell_row_width"] = w
+    R.fmt_free(h)
+
+    # ---- DIA on the Laplacian and on a banded matrix
+    for name, (brp, bci, bv) in {"lap": (g["lap_rp"], g["lap_ci"], g["lap_v"]),
+                                 "band": synth.banded_random(1500, mean=6, band=8, seed=12)}.items():
+        nn = len(brp) - 1
+        h = R.fmt_build("dia", brp, bci, bv, nn, 10240, 0, 4)
+        info = R.fmt_info(h)
+        off = np.zeros(info[0], np.int64)
+        data = np.zeros(info[0] * info[1])
+        R.fmt_copy(h, off, None, None, data)
+        g[f"dia_{name}_offsets"], g[f"dia_{name}_stride"] = off, np.int64(info[1])
+        if name == "band":
+            g["band_rp"], g["band_ci"], g["band_v"] = brp, bci, bv
+        R.fmt_free(h)
+
+    # ---- BSR structure
+    for name, (brp, bci, bv, br, bc) in {"lap": (g["lap_rp"], g["lap_ci"], g["lap_v"], 16, 4),
+                                         "pl": (rp, ci, v, 16, 8)}.items():
+        nn = len(brp) - 1
+        h = R.fmt_build("bsr", brp, bci, bv, nn, br, bc)
+        info = R.fmt_info(h)
+        brow, bcol = np.zeros(info[0] + 1, np.int32), np.zeros(info[2], np.int32)
+        bdata = np.zeros(info[2] * br * bc)
+        R.fmt_copy(h, brow, bcol, None, bdata)
+        g[f"bsr_{name}_row_ptr"], g[f"bsr_{name}_col"] = brow, bcol
+        R.fmt_free(h)
+
+    # ---- LeSpGEMM preprocessing and kernel 3 on a planted-community matrix
+    arp, aci, av = synth.planted_communities(1024, ncomm=32, mean=12.0, seed=13)
+    brp, bci, bv = synth.transpose(arp, aci, av, 1024)
+    g["sp_arp"], g["sp_aci"], g["sp_av"] = arp, aci, av
+    sig = R.minhash(arp, aci, 64, 7)
+    g["sp_sig"] = sig
+    pi, pj, ps = R.lsh_pairs(arp, aci, 64, 16, 7, True)
+    g["sp_pi"], g["sp_pj"], g["sp_ps"] = pi, pj, ps
+    perm, offs = R.hc(arp, aci, pi, pj, ps, 8)
+    g["sp_perm"], g["sp_offsets"] = perm, offs
+    for so in (0, 1):
+        c = R.spgemm_kernel3((arp, aci, av), (brp, bci, bv, 1024), perm, offs, sort_output=bool(so))
+        cci, cv = sort_rows(c["rp"], c["ci"], c["v"])
+        g[f"sp_c{so}_rp"], g[f"sp_c{so}_ci"], g[f"sp_c{so}_v"] = c["rp"], cci, cv
+        g[f"sp_c{so}_dense"] = np.int64(c["dense_clusters"])
+    # a bucket larger than 256 rows (window rule): 400 identical rows
+    rp2 = np.arange(0, 401 * 3, 3, dtype=np.int64)
+    ci2 = np.tile(np.array([5, 17, 99], np.int64), 400)
+    pi2, pj2, ps2 = R.lsh_pairs(rp2, ci2, 64, 16, 7, True)
+    g["big_pi"], g["big_pj"], g["big_ps"] = pi2, pj2, ps2
+
+    # ---- transpose (csr_transpose: duplicates summed, exact zeros dropped)
+    brp, bci, bv = g["band_rp"], g["band_ci"], g["band_v"]
+    trp, tci, tv = R.csr_transpose(brp.astype(np.int64), bci.astype(np.int64), bv, len(brp) - 1)
+    tci, tv = sort_rows(trp, tci, tv)
+    g["tr_rp"], g["tr_ci"], g["tr_v"] = trp, tci, tv
+
+    np.savez_compressed(OUT, **g)
+    print(OUT, os.path.getsize(OUT), "bytes,", len(g), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+"""Pin the oracle (oracle/spops_oracle.cpp) against the reference's own outputs.
+
+The golden fixtures were written by tests/golden/make_golden.py from the
+reference library compiled from its sources.  Integer outputs must match bit
+for bit; FP64 values to 1e-13 relative (the reference sums in OpenMP-SIMD lane
+order, the oracle sequentially).  These tests need no GPU.
+"""
+import numpy as np
+import pytest
+
+from sparseops_b200 import synth
+
+
+def test_golden_inputs_regenerate(golden):
+    """The seeded generators still produce the fixture inputs bit for bit."""
+    rp, ci, v = synth.laplacian_2d(32)
+    assert np.array_equal(rp, golden["lap_rp"]) and np.array_equal(ci, golden["lap_ci"])
+    assert np.array_equal(v, golden["lap_v"])
+    rp, ci, v = synth.powerlaw(2000, hi=300, seed=11)
+    assert np.array_equal(rp, golden["pl_rp"]) and np.array_equal(ci, golden["pl_ci"])
+    assert np.array_equal(v, golden["pl_v"])
+    assert np.array_equal(synth.uniform(len(rp) - 1, 0), golden["pl_x"])
+
+
+@pytest.mark.parametrize("name", ["lap", "pl"])
+def test_spmv_csr(golden, orc, name):
+    g = golden
+    y = orc.spmv_csr(g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"], g[f"{name}_x"], 0.8, 0.7, g[f"{name}_y0"])
+    den = orc.absdot(g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"], g[f"{name}_x"]) + np.abs(g[f"{name}_y0"])
+    err = np.abs(y - g[f"{name}_y"]) / np.maximum(den, 1e-300)
+    assert err.max() <= 1e-13
+
+
+@pytest.mark.parametrize("tag,sigma,C,align", [("a", 512, 32, 8), ("b", 64, 4, 4), ("c", 16384, 4, 4)])
+def test_sell_c_sigma_layout(golden, orc, tag, sigma, C, align):
+    ro, cl = orc.sell_c_sigma_layout(golden["pl_rp"], sigma, C, align)
+    assert np.array_equal(ro, golden[f"scs_{tag}_reorder"])
+    assert np.array_equal(cl, golden[f"scs_{tag}_chunk_len"])
+
+
+def test_sell_c_R_layout(golden, orc):
+    n = len(golden["pl_rp"]) - 1
+    ro, cl = orc.sell_c_sigma_layout(golden["pl_rp"], n, 32, 8)
+    assert np.array_equal(ro, golden["scr_reorder"]) and np.array_equal(cl, golden["scr_chunk_len"])
+
+
+def test_sell_row_width(golden, orc):
+    assert np.array_equal(orc.sell_row_width(golden["pl_rp"], 4, 4), golden["sell_row_width"])
+
+
+@pytest.mark.parametrize("name", ["lap", "band"])
+def test_dia_offsets(golden, orc, name):
+    rp, ci = golden[f"{name}_rp"], golden[f"{name}_ci"]
+    off, nd = orc.dia_offsets(rp, ci, len(rp) - 1)
+    assert nd == len(golden[f"dia_{name}_offsets"])
+    assert np.array_equal(off, golden[f"dia_{name}_offsets"])
+
+
+@pytest.mark.parametrize("name,br,bc", [("lap", 16, 4), ("pl", 16, 8)])
+def test_bsr_structure(golden, orc, name, br, bc):
+    rp, ci = golden[f"{name}_rp"], golden[f"{name}_ci"]
+    row_ptr, bcol = orc.bsr_structure(rp, ci, len(rp) - 1, br, bc)
+    assert np.array_equal(row_ptr, golden[f"bsr_{name}_row_ptr"]) and np.array_equal(bcol, golden[f"bsr_{name}_col"])
+
+
+def test_minhash(golden, orc):
+    sig = orc.minhash(golden["sp_arp"], golden["sp_aci"], 64, 7)
+    assert np.array_equal(sig, golden["sp_sig"])
+
+
+def test_lsh_pairs(golden, orc):
+    i, j, s = orc.lsh_pairs(golden["sp_sig"], 16, True)
+    assert np.array_equal(i, golden["sp_pi"]) and np.array_equal(j, golden["sp_pj"])
+    assert np.array_equal(s, golden["sp_ps"])
+
+
+def test_lsh_window_rule(orc, golden):
+    """A bucket of 400 rows (> 256) pairs each row with its next 16 rows only."""
+    rp = np.arange(0, 401 * 3, 3, dtype=np.int64)
+    ci = np.tile(np.array([5, 17, 99], np.int64), 400)
+    sig = orc.minhash(rp, ci, 64, 7)
+    i, j, s = orc.lsh_pairs(sig, 16, True)
+    assert np.array_equal(i, golden["big_pi"]) and np.array_equal(j, golden["big_pj"])
+    assert np.array_equal(s, golden["big_ps"])
+
+
+def test_hc(golden, orc):
+    perm, offs = orc.hc(golden["sp_arp"], golden["sp_aci"], golden["sp_pi"], golden["sp_pj"], golden["sp_ps"], 8)
+    assert np.array_equal(perm, golden["sp_perm"]) and np.array_equal(offs, golden["sp_offsets"])
+
+
+@pytest.mark.parametrize("so", [0, 1])
+def test_spgemm_kernel3(golden, orc, so):
+    g = golden
+    A = (g["sp_arp"], g["sp_aci"], g["sp_av"])
+    B = synth.transpose(*A, 1024)
+    c = orc.spgemm(A, B, g["sp_perm"], g["sp_offsets"], sort_output=bool(so))
+    assert c["dense_clusters"] == int(g[f"sp_c{so}_dense"])
+    assert np.array_equal(c["rp"], g[f"sp_c{so}_rp"]) and np.array_equal(c["ci"], g[f"sp_c{so}_ci"])
+    err = np.abs(c["v"] - g[f"sp_c{so}_v"]) / c["absv"]
+    assert err.max() <= 1e-13
+
+
+def test_transpose_spmv(golden, orc):
+    """A^T g from the oracle equals SpMV with the reference's csr_transpose."""
+    g = golden
+    rp, ci, v = g["band_rp"], g["band_ci"], g["band_v"]
+    n = len(rp) - 1
+    gv = synth.normal(n, 3)
+    y = orc.spmv_t(rp, ci, v, gv, n)
+    yt = orc.spmv_csr(g["tr_rp"], g["tr_ci"], g["tr_v"], gv)
+    assert np.abs(y - yt).max() <= 1e-13 * (1 + np.abs(y).max())

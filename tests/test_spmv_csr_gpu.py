@@ -1,0 +1,147 @@
+"""CSR SpMV on the device vs the oracle (and the reference's golden outputs).
+
+Error metric (FP64): componentwise |y - y_ref| / (sum_j |a_ij x_j| + |beta*y0_i|),
+bound 1e-12.  FP32 values/accumulation: bound 1e-5 on the same metric.
+"""
+import numpy as np
+import pytest
+
+from sparseops_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def _run(rp, ci, v, x, alpha=1.0, beta=0.0, y0=None, ncols=None, dev="cuda"):
+    import torch
+    from sparseops_b200 import CSR_Matrix, SpOps_csr
+    n = len(rp) - 1
+    ncols = len(x) if ncols is None else ncols
+    A = CSR_Matrix(n, ncols, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev), torch.from_numpy(v).to(dev))
+    xd = torch.from_numpy(x).to(dev)
+    yd = torch.from_numpy(y0.copy()).to(dev) if y0 is not None else torch.full((n,), float("nan"), dtype=xd.dtype,
+                                                                                device=dev)
+    SpOps_csr(alpha, A, xd, beta, yd)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy(), A
+
+
+def _err(orc, rp, ci, v, x, y, yref, beta=0.0, y0=None, alpha=1.0):
+    den = abs(alpha) * orc.absdot(rp, ci, v, x)
+    if y0 is not None:
+        den = den + np.abs(beta * y0)
+    return (np.abs(y - yref) / np.maximum(den, 1e-300)).max() if len(y) else 0.0
+
+
+@pytest.mark.parametrize("name", ["lap", "pl"])
+def test_golden_reference_outputs(cuda, golden, orc, name):
+    g = golden
+    rp, ci, v, x, y0 = g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"], g[f"{name}_x"], g[f"{name}_y0"]
+    y, _ = _run(rp, ci, v, x, 0.8, 0.7, y0)
+    assert _err(orc, rp, ci, v, x, y, g[f"{name}_y"], 0.7, y0) <= TOL64
+
+
+def test_laplacian_512_full_config(cuda, orc):
+    rp, ci, v = synth.laplacian_2d(512)
+    x = synth.uniform(len(rp) - 1, 0)
+    y, _ = _run(rp, ci, v, x)
+    assert _err(orc, rp, ci, v, x, y, orc.spmv_csr(rp, ci, v, x)) <= TOL64
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (0.8, 0.7), (-2.0, 1.0), (0.0, 0.5), (1.0, -1.0)])
+def test_alpha_beta(cuda, orc, alpha, beta):
+    rp, ci, v = synth.powerlaw(20000, hi=5000, seed=21)
+    n = len(rp) - 1
+    x, y0 = synth.uniform(n, 1), synth.uniform(n, 2)
+    y, _ = _run(rp, ci, v, x, alpha, beta, y0)
+    yref = orc.spmv_csr(rp, ci, v, x, alpha, beta, y0)
+    assert _err(orc, rp, ci, v, x, y, yref, beta, y0, alpha) <= TOL64
+
+
+def test_beta_zero_ignores_nan_y(cuda, orc):
+    rp, ci, v = synth.powerlaw(5000, seed=22)
+    x = synth.uniform(5000, 3)
+    y, _ = _run(rp, ci, v, x, 1.5, 0.0, None)  # y starts as NaN
+    assert np.isfinite(y).all()
+    assert _err(orc, rp, ci, v, x, y, orc.spmv_csr(rp, ci, v, x, 1.5, 0.0), alpha=1.5) <= TOL64
+
+
+def test_long_rows_and_empty_rows(cuda, orc):
+    """Rows longer than one chunk (multi-block path), runs of > 1024 empty rows,
+    and a row exactly at the chunk boundary."""
+    rng = np.random.default_rng(5)
+    n, ncols = 9000, 300000
+    lens = rng.integers(0, 40, n)
+    lens[100] = 100000      # many chunks
+    lens[101] = 2048        # exactly one chunk
+    lens[102] = 2049        # just over
+    lens[2000:4500] = 0     # long empty run
+    lens[n - 1] = 70000     # long last row
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    x = rng.uniform(-1, 1, ncols)
+    rp = rp.astype(np.int32)
+    y, _ = _run(rp, ci, v, x, 0.8, 0.7, np.ones(n))
+    yref = orc.spmv_csr(rp, ci, v, x, 0.8, 0.7, np.ones(n))
+    assert _err(orc, rp, ci, v, x, y, yref, 0.7, np.ones(n), 0.8) <= TOL64
+
+
+def test_deterministic(cuda):
+    rp, ci, v = synth.powerlaw(100000, seed=23)
+    x = synth.uniform(100000, 4)
+    y1, A = _run(rp, ci, v, x)
+    y2, _ = _run(rp, ci, v, x)
+    assert np.array_equal(y1, y2)
+
+
+def test_int64_indices(cuda, orc):
+    rp, ci, v = synth.powerlaw(30000, seed=24)
+    x = synth.uniform(30000, 5)
+    y, _ = _run(rp.astype(np.int64), ci.astype(np.int64), v, x, 0.8, 0.7, np.ones(30000))
+    yref = orc.spmv_csr(rp, ci, v, x, 0.8, 0.7, np.ones(30000))
+    assert _err(orc, rp, ci, v, x, y, yref, 0.7, np.ones(30000)) <= TOL64
+
+
+def test_float32(cuda, orc):
+    rp, ci, v = synth.powerlaw(30000, seed=25)
+    x = synth.uniform(30000, 6)
+    v32, x32 = v.astype(np.float32), x.astype(np.float32)
+    y, _ = _run(rp, ci, v32, x32)
+    yref = orc.spmv_csr(rp, ci, v32, x32)
+    assert _err(orc, rp, ci, v32.astype(np.float64), x32.astype(np.float64), y.astype(np.float64), yref) <= TOL32
+
+
+def test_empty_matrices(cuda):
+    # no rows
+    y, _ = _run(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0), np.zeros(5))
+    assert y.shape == (0,)
+    # rows but no entries: y = beta*y0
+    n = 3000
+    y, _ = _run(np.zeros(n + 1, np.int32), np.zeros(0, np.int32), np.zeros(0), np.zeros(7), 1.0, 0.5, np.ones(n))
+    assert np.array_equal(y, np.full(n, 0.5))
+
+
+def test_host_vectors(cuda, orc):
+    """numpy x / y: the host path (spops_spmv_host) uploads x and downloads y."""
+    from sparseops_b200 import CSR_Matrix, SpOps_csr
+    rp, ci, v = synth.powerlaw(40000, seed=26)
+    x, y0 = synth.uniform(40000, 7), synth.uniform(40000, 8)
+    A = CSR_Matrix(40000, 40000, rp, ci, v)
+    y = y0.copy()
+    SpOps_csr(0.8, A, x, 0.7, y)
+    yref = orc.spmv_csr(rp, ci, v, x, 0.8, 0.7, y0)
+    assert _err(orc, rp, ci, v, x, y, yref, 0.7, y0) <= TOL64
+
+
+def test_powerlaw_full_config(cuda, orc):
+    """Power-law config at full size: n = 4,194,304, lognormal(ln 12, 1.2) rows."""
+    import math
+    n = 4194304
+    rp, ci, v = synth.powerlaw(n, mu=math.log(12.0), sigma=1.2, lo=1, hi=20000, seed=1)
+    x = synth.uniform(n, 1)
+    y, _ = _run(rp, ci, v, x)
+    assert _err(orc, rp, ci, v, x, y, orc.spmv_csr(rp, ci, v, x)) <= TOL64
