@@ -99,6 +99,13 @@ spops_status_t spops_create(spops_context_t* ctx, int device, void* stream);
 spops_status_t spops_destroy(spops_context_t ctx);
 spops_status_t spops_set_stream(spops_context_t ctx, void* stream);
 spops_status_t spops_synchronize(spops_context_t ctx);
+/* Synchronise and read (then clear) the context's device error word: bounded
+ * device-side waits that ran out set bits there.  Returns SPOPS_ERR_TIMEOUT
+ * when any bit was set; *flags (may be NULL) receives the bits. */
+spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
+/* Tuning / diagnostic switches.  Keys: "csr_plain_kernel" (0/1): run CSR
+ * SpMV with the plain kernel instead of the bulk-copy pipelined one. */
+spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);
 int spops_abi_version(void);

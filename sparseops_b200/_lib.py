@@ -49,6 +49,8 @@ _SIGS = {
     "spops_destroy": [vp],
     "spops_set_stream": [vp, vp],
     "spops_synchronize": [vp],
+    "spops_check_device": [vp, vp],
+    "spops_set_option": [vp, C.c_char_p, i64],
     "spops_csr_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
     "spops_matrix_destroy": [vp],
     "spops_matrix_info": [vp, vp],

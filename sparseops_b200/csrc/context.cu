@@ -65,6 +65,13 @@ spops_status_t Context::scratch_reserve(size_t n) {
   return scratch.alloc(want);
 }
 
+spops_status_t Context::ensure_errword() {
+  if (errword.p) return SPOPS_OK;
+  SPOPS_TRY(errword.alloc(16));
+  SPOPS_CUDA(cudaMemsetAsync(errword.p, 0, 16, stream));
+  return SPOPS_OK;
+}
+
 }  // namespace spops
 
 using namespace spops;
@@ -107,6 +114,7 @@ spops_status_t spops_destroy(spops_context_t c) {
   DeviceGuard g(c->device);
   cudaStreamSynchronize(c->stream);
   c->scratch.release();
+  c->errword.release();
   c->xbuf.release();
   c->ybuf.release();
   if (c->pinned) cudaFreeHost(c->pinned);
@@ -118,6 +126,26 @@ spops_status_t spops_set_stream(spops_context_t c, void* stream) {
   if (!c) return fail(SPOPS_ERR_INVALID, "spops_set_stream: null context");
   c->stream = static_cast<cudaStream_t>(stream);
   return SPOPS_OK;
+}
+
+spops_status_t spops_check_device(spops_context_t c, int32_t* flags) {
+  if (!c) return fail(SPOPS_ERR_INVALID, "spops_check_device: null context");
+  DeviceGuard g(c->device);
+  int32_t f = 0;
+  if (c->errword.p) {
+    SPOPS_CUDA(cudaMemcpyAsync(&f, c->errword.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    SPOPS_CUDA(cudaStreamSynchronize(c->stream));
+    if (f) SPOPS_CUDA(cudaMemsetAsync(c->errword.p, 0, sizeof(int32_t), c->stream));
+  }
+  if (flags) *flags = f;
+  if (f) return fail(SPOPS_ERR_TIMEOUT, "a device-side wait gave up (flags 0x%x)", (unsigned)f);
+  return SPOPS_OK;
+}
+
+spops_status_t spops_set_option(spops_context_t c, const char* key, int64_t value) {
+  if (!c || !key) return fail(SPOPS_ERR_INVALID, "spops_set_option: null argument");
+  if (!strcmp(key, "csr_plain_kernel")) { c->force_plain = value != 0; return SPOPS_OK; }
+  return fail(SPOPS_ERR_INVALID, "spops_set_option: unknown key '%s'", key);
 }
 
 spops_status_t spops_synchronize(spops_context_t c) {

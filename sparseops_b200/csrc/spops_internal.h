@@ -52,6 +52,11 @@ struct Context {
   // grow-only scratch for temporary device storage (CUB temp, staging)
   DevBuf scratch;
   spops_status_t scratch_reserve(size_t bytes);
+  // device error word: bounded waits that ran out set bits here
+  DevBuf errword;
+  spops_status_t ensure_errword();
+  // use the plain (non-bulk-copy) CSR kernel even when arrays are aligned
+  bool force_plain = false;
   // pinned staging for host x / y in spops_spmv_host
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -73,6 +78,14 @@ struct DeviceGuard {
 };
 
 // --------------------------------------------------- CSR stream analysis
+// One unit of CSR SpMV work: entries [p0, p1) of rows r0 .. r0+nr-1
+// (chunk < 0), or chunk `chunk` of the long row r0 which has nr chunks.
+struct CsrSeg {
+  int64_t p0, p1, r0;
+  int32_t nr;
+  int32_t chunk;
+};
+
 // Row-block partition of a CSR matrix for the streaming SpMV kernel
 // (spmv_csr.cu).  Block b covers rows [blk_row[b], next block's row) when
 // blk_chunk[b] < 0 (a segment of short rows whose entries fit in shared
@@ -86,7 +99,12 @@ struct CsrPlan {
   DevBuf blk_chunk;        // int32 [nblocks]
   DevBuf partial;          // V [nblocks] long-row chunk sums
   DevBuf counter;          // int32 [nblocks] arrival counters (zero between calls)
-  void release() { blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); ready = false; }
+  DevBuf seg;              // CsrSeg [nblocks]
+  bool pipelined = false;  // arrays 16-byte aligned: bulk-copy kernel usable
+  void release() {
+    blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); seg.release();
+    ready = false;
+  }
 };
 
 // ---------------------------------------------------------------- matrix

@@ -81,6 +81,15 @@ class Context:
     def synchronize(self) -> None:
         call("spops_synchronize", self.handle)
 
+    def check_device(self) -> int:
+        """Raise SpOpsError(SPOPS_ERR_TIMEOUT) if a bounded device wait gave up."""
+        f = C.c_int32()
+        call("spops_check_device", self.handle, C.byref(f))
+        return f.value
+
+    def set_option(self, key: str, value: int) -> None:
+        call("spops_set_option", self.handle, key.encode(), i64(int(value)))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             _lib.lib().spops_destroy(self.handle)
