@@ -245,6 +245,8 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     ctx = default_context(local)
+    if args.csr_variant:
+        ctx.set_option("csr_variant", args.csr_variant)
     A = CSR_Matrix(n, n, rp, ci, v)
     h = A.device(ctx)
     xd = torch.from_numpy(x).to(dev)
@@ -330,7 +332,7 @@ def run_ours(args):
         "pct_of_peak": round(100 * value / world / peak, 2),
         "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
-                     "peak_source": peak_kind, "kernel": "csr_stream_kernel<int,double>",
+                     "peak_source": peak_kind, "kernel": "csr_warp_kernel<int,double>",
                      "traffic": traffic},
         "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                 "steps": e2e_steps, "matches_device_result": ok,
@@ -351,6 +353,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--csr-variant", type=int, default=0, help="CSR kernel shape (spops_set_option)")
     ap.add_argument("--rows", type=int, default=N_ROWS,
                     help="matrix rows (default: the benchmark size; smaller only for profiling captures)")
     args = ap.parse_args()

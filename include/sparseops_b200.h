@@ -103,8 +103,9 @@ spops_status_t spops_synchronize(spops_context_t ctx);
  * device-side waits that ran out set bits there.  Returns SPOPS_ERR_TIMEOUT
  * when any bit was set; *flags (may be NULL) receives the bits. */
 spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
-/* Tuning / diagnostic switches.  Keys: "csr_plain_kernel" (0/1): run CSR
- * SpMV with the plain kernel instead of the bulk-copy pipelined one. */
+/* Tuning switches by name; unknown keys are rejected with SPOPS_ERR_INVALID.
+ *   "csr_variant" 0..2: CSR SpMV kernel shape (entries per lane per load
+ *   round / resident blocks per SM: 0 = 8/4 (default), 1 = 4/6, 2 = 16/2). */
 spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);

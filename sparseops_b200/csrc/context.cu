@@ -144,7 +144,11 @@ spops_status_t spops_check_device(spops_context_t c, int32_t* flags) {
 
 spops_status_t spops_set_option(spops_context_t c, const char* key, int64_t value) {
   if (!c || !key) return fail(SPOPS_ERR_INVALID, "spops_set_option: null argument");
-  if (!strcmp(key, "csr_plain_kernel")) { c->force_plain = value != 0; return SPOPS_OK; }
+  if (!strcmp(key, "csr_variant")) {
+    if (value < 0 || value > 2) return fail(SPOPS_ERR_INVALID, "csr_variant must be 0..2");
+    c->csr_variant = (int)value;
+    return SPOPS_OK;
+  }
   return fail(SPOPS_ERR_INVALID, "spops_set_option: unknown key '%s'", key);
 }
 

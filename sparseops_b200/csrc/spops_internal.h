@@ -55,8 +55,8 @@ struct Context {
   // device error word: bounded waits that ran out set bits here
   DevBuf errword;
   spops_status_t ensure_errword();
-  // use the plain (non-bulk-copy) CSR kernel even when arrays are aligned
-  bool force_plain = false;
+  // CSR SpMV kernel variant (spmv_csr.cu)
+  int csr_variant = 0;
   // pinned staging for host x / y in spops_spmv_host
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -100,7 +100,6 @@ struct CsrPlan {
   DevBuf partial;          // V [nblocks] long-row chunk sums
   DevBuf counter;          // int32 [nblocks] arrival counters (zero between calls)
   DevBuf seg;              // CsrSeg [nblocks]
-  bool pipelined = false;  // arrays 16-byte aligned: bulk-copy kernel usable
   void release() {
     blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); seg.release();
     ready = false;

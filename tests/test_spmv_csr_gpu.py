@@ -147,33 +147,9 @@ def test_powerlaw_full_config(cuda, orc):
     assert _err(orc, rp, ci, v, x, y, orc.spmv_csr(rp, ci, v, x)) <= TOL64
 
 
-def test_plain_kernel_bit_identical(cuda):
-    """The plain kernel (no bulk copies) and the pipelined kernel reduce in the
-    same order, so their results are bit-identical."""
-    import torch
-    from sparseops_b200 import CSR_Matrix, Context, SpOps_csr
-    rp, ci, v = synth.powerlaw(60000, hi=8000, seed=27)
-    x = synth.uniform(60000, 9)
-    d = torch.device("cuda")
-    ys = []
-    for plain in (0, 1):
-        ctx = Context(0)
-        ctx.set_option("csr_plain_kernel", plain)
-        A = CSR_Matrix(60000, 60000, torch.from_numpy(rp).to(d), torch.from_numpy(ci).to(d), torch.from_numpy(v).to(d))
-        A.device(ctx)
-        xd, yd = torch.from_numpy(x).to(d), torch.zeros(60000, dtype=torch.float64, device=d)
-        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-        from sparseops_b200._lib import call, dbl, vp
-        call("spops_spmv", ctx.handle, dbl(1.0), A.device().handle, vp(xd.data_ptr()), dbl(0.0), vp(yd.data_ptr()))
-        torch.cuda.synchronize()
-        assert ctx.check_device() == 0
-        ys.append(yd.cpu().numpy())
-    assert np.array_equal(ys[0], ys[1])
-
-
 def test_unaligned_borrowed_arrays(cuda, orc):
     """Arrays that start 4/8 bytes past a 16-byte boundary (views into larger
-    buffers) take the plain kernel and still give the right answer."""
+    buffers) give the right answer."""
     import torch
     from sparseops_b200 import CSR_Matrix, SpOps_csr
     rp, ci, v = synth.powerlaw(20000, seed=28)
