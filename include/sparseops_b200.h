@@ -135,6 +135,67 @@ spops_status_t spops_matrix_analyse(spops_context_t ctx, spops_matrix_t A);
 /* Bytes of device memory the handle owns (arrays + analysis). */
 spops_status_t spops_matrix_device_bytes(spops_matrix_t A, int64_t* bytes);
 
+/* ------------------------------------------------------ format handles */
+/* Device conversion of a CSR handle into another format (all work on the
+ * device; integer layout arrays are bit-identical to the reference's):
+ *   SELL_C_SIGMA  csr_to_sell_c_sigma  include/sparse_conversion.h:344
+ *   SELL_C_R      csr_to_sell_c_R      include/sparse_conversion.h:490
+ *   SELL (S-ELL)  csr_to_sell          include/sparse_conversion.h:265
+ *   ELL           csr_to_ell           include/sparse_conversion.h:194
+ *   DIA           csr_to_dia           include/sparse_conversion.h:619
+ *   BSR           csr_to_bsr           include/sparse_conversion.h:776
+ *   COO           csr_to_coo           include/sparse_conversion.h:152
+ * params may be NULL (reference defaults).  Errors the reference reports by
+ * exit() come back as status codes: sigma not a multiple of C ->
+ * SPOPS_ERR_INVALID; more than max_diags diagonals, or padded storage that
+ * cannot fit in device memory -> SPOPS_ERR_TOO_LARGE. */
+spops_status_t spops_convert(spops_context_t ctx, spops_matrix_t csr, spops_format_t format,
+                             const spops_format_params_t* params, spops_matrix_t* out);
+
+/* Padded-row matrix (SELL_C_SIGMA, SELL_C_R, SELL or ELL) from the arrays of
+ * a reference struct, chunks concatenated in chunk order: chunk_len[nchunks]
+ * (ELL: one chunk of width max_row_width), col[stored] (-1 = padding),
+ * val[stored], reorder[rows] (SELL_C_SIGMA / SELL_C_R only, else NULL).
+ * layout: SPOPS_ROW_MAJOR (reference) or SPOPS_COL_MAJOR.
+ * Replaces the host structs of include/sparse_format.h:190-295 as consumed by
+ * SpOps_sell_c_sigma / SpOps_sell_c_R / SpOps_sell / SpOps_ell. */
+spops_status_t spops_padded_create(spops_context_t ctx, spops_matrix_t* A, spops_format_t format, int64_t rows,
+                                   int64_t cols, int64_t nnz, int64_t chunk, int64_t sigma, int64_t alignment,
+                                   spops_layout_t layout, const void* reorder, const void* chunk_len,
+                                   int64_t nchunks, const void* col, const void* val, int64_t stored,
+                                   spops_index_t itype, spops_value_t vtype, spops_mem_t mem);
+/* DIA from diag_offsets[ndiag] (int64) and diag_data[ndiag * stride]
+ * (include/sparse_format.h:172-184, consumed by SpOps_dia src/spmv_dia.cpp:177). */
+spops_status_t spops_dia_create(spops_context_t ctx, spops_matrix_t* A, int64_t rows, int64_t cols, int64_t nnz,
+                                int64_t ndiag, int64_t stride, const int64_t* diag_offsets, const void* diag_data,
+                                spops_value_t vtype, spops_mem_t mem);
+/* BSR from row_ptr[mb+1], block_colindex[nnzb], block_data[nnzb*br*bc]
+ * (include/sparse_format.h:110-127, consumed by SpOps_bsr src/spmv_bsr.cpp:214). */
+spops_status_t spops_bsr_create(spops_context_t ctx, spops_matrix_t* A, int64_t rows, int64_t cols, int64_t nnz,
+                                int64_t block_rows, int64_t block_cols, int64_t nnzb, const void* row_ptr,
+                                const void* block_col, const void* block_data, spops_index_t itype,
+                                spops_value_t vtype, spops_mem_t mem);
+
+/* Arrays of a handle, for export into the reference structs. */
+typedef enum {
+  SPOPS_ARR_ROW = 0,           /* CSR row_offset / COO row_index */
+  SPOPS_ARR_COL = 1,           /* column indices (padded formats: slots, -1 = padding) */
+  SPOPS_ARR_VAL = 2,           /* values; padded slots; DIA diag_data; BSR block_data */
+  SPOPS_ARR_REORDER = 3,       /* SELL-C-sigma / SELL-C-R: stored row -> original row */
+  SPOPS_ARR_CHUNK_LEN = 4,     /* chunk_len / S-ELL row_width / ELL max_row_width */
+  SPOPS_ARR_CHUNK_OFF = 5,     /* int64 first slot of every chunk (nchunks + 1) */
+  SPOPS_ARR_ROW_LEN = 6,       /* int32 slots up to each stored row's last entry */
+  SPOPS_ARR_DIAG_OFFSETS = 7,  /* int64 DIA diag_offsets */
+  SPOPS_ARR_BLOCK_ROW_PTR = 8, /* BSR row_ptr */
+  SPOPS_ARR_BLOCK_COL = 9      /* BSR block_colindex */
+} spops_array_t;
+/* Device pointer, element count and element size of one array (no copy). */
+spops_status_t spops_matrix_array(spops_matrix_t A, spops_array_t which, const void** dev_ptr, int64_t* count,
+                                  int32_t* elem_bytes);
+/* Copy one array into host memory (count elements; synchronises). */
+spops_status_t spops_matrix_download(spops_context_t ctx, spops_matrix_t A, spops_array_t which, void* host_dst,
+                                     int64_t count);
+
 /* ---------------------------------------------------------------- SpMV */
 /* y = alpha*A*x + beta*y on the device; x[cols], y[rows] device pointers of
  * A's value type.  beta == 0 overwrites y without reading it.

@@ -57,6 +57,14 @@ _SIGS = {
     "spops_matrix_touch": [vp],
     "spops_matrix_analyse": [vp, vp],
     "spops_matrix_device_bytes": [vp, vp],
+    "spops_coo_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
+    "spops_convert": [vp, vp, C.c_int, vp, vp],
+    "spops_padded_create": [vp, vp, C.c_int, i64, i64, i64, i64, i64, i64, C.c_int, vp, vp, i64, vp, vp, i64,
+                            C.c_int, C.c_int, C.c_int],
+    "spops_dia_create": [vp, vp, i64, i64, i64, i64, i64, vp, vp, C.c_int, C.c_int],
+    "spops_bsr_create": [vp, vp, i64, i64, i64, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
+    "spops_matrix_array": [vp, C.c_int, vp, vp, vp],
+    "spops_matrix_download": [vp, vp, C.c_int, vp, i64],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
     "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
 }

@@ -106,6 +106,59 @@ struct CsrPlan {
   }
 };
 
+// --------------------------------------------------- padded-row formats
+// SELL-C-sigma, SELL-C-R, S-ELL and ELL share one device representation:
+// stored rows i = 0..rows-1 (sorted order for SELL-C-sigma / SELL-C-R),
+// chunk c = i / C holding C stored rows of chunk_len[c] slots each, starting
+// at chunk_off[c]; slot k of stored row i is at
+//   row-major: chunk_off[c] + (i - c*C) * chunk_len[c] + k   (reference layout)
+//   col-major: chunk_off[c] + (i - c*C) + k * C              (device-native)
+// Padding slots hold column -1 and value 0.  row_len[i] is the number of
+// slots of stored row i up to its last real entry; y[reorder[i]] (or y[i]
+// when unsorted) receives its sum.  Rows longer than kPadLong slots are
+// summed by whole thread blocks over pieces of kPadPiece slots.
+struct PadPiece {
+  int64_t row;      // stored row
+  int32_t piece;    // piece index within the row
+  int32_t npieces;  // pieces of this row
+};
+
+struct PaddedData {
+  int64_t C = 0, sigma = 0, align = 1, nchunks = 0, stored = 0;
+  bool sorted = false;
+  int64_t max_row = 0, min_row = 0;
+  DevBuf reorder;    // I [rows]
+  DevBuf chunk_len;  // I [nchunks]
+  DevBuf chunk_off;  // int64 [nchunks + 1]
+  DevBuf row_len;    // int32 [rows]
+  int64_t npieces = 0;
+  DevBuf piece;      // PadPiece [npieces]
+  DevBuf partial;    // double [npieces]
+  DevBuf counter;    // int32 [npieces]
+  void release() {
+    reorder.release(); chunk_len.release(); chunk_off.release(); row_len.release();
+    piece.release(); partial.release(); counter.release();
+  }
+};
+
+// DIA: diag_offsets (int64, ndiag) in first-appearance order; diag_data
+// [ndiag x stride] indexed by row (include/sparse_format.h:172-184).
+struct DiaData {
+  int64_t ndiag = 0, stride = 0;
+  DevBuf offsets;  // int64 [ndiag]
+  DevBuf data;     // V [ndiag * stride]
+  void release() { offsets.release(); data.release(); }
+};
+
+// BSR: block rows of br x bc blocks stored row-major (include/sparse_format.h:110-127).
+struct BsrData {
+  int64_t br = 0, bc = 0, mb = 0, nb = 0, nnzb = 0;
+  DevBuf row_ptr;  // I [mb + 1]
+  DevBuf bcol;     // I [nnzb]
+  DevBuf data;     // V [nnzb * br * bc]
+  void release() { row_ptr.release(); bcol.release(); data.release(); }
+};
+
 // ---------------------------------------------------------------- matrix
 struct Matrix {
   Context* ctx = nullptr;
@@ -117,14 +170,30 @@ struct Matrix {
   // CSR / COO arrays (COO: row = row index array)
   DevBuf row, col, val;
   CsrPlan plan;
+  PaddedData pad;
+  DiaData dia;
+  BsrData bsr;
+  // COO: the same entries as a CSR matrix sorted by row (owned)
+  Matrix* csr_view = nullptr;
   size_t isize() const { return itype == SPOPS_INDEX_I32 ? 4 : 8; }
   size_t vsize() const { return vtype == SPOPS_VALUE_F32 ? 4 : 8; }
-  void release_all() { row.release(); col.release(); val.release(); plan.release(); }
+  void release_all();
 };
 
 // ------------------------------------------------------------ kernels API
 spops_status_t csr_analyse(Context* ctx, Matrix* A);
 spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+
+// formats.cu
+spops_status_t convert_from_csr(Context* ctx, Matrix* A, spops_format_t fmt, const spops_format_params_t& p,
+                                Matrix** out);
+spops_status_t padded_finish(Context* ctx, Matrix* M);  // row lengths, long pieces (after arrays are set)
+spops_status_t padded_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+spops_status_t dia_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+spops_status_t bsr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+spops_status_t coo_analyse(Context* ctx, Matrix* A);
+spops_status_t validate_columns(Context* ctx, const void* col, int64_t count, spops_index_t it, int64_t ncols,
+                                bool allow_pad);
 
 }  // namespace spops
 

@@ -1,0 +1,216 @@
+"""Device format conversions and per-format SpMV.
+
+Layout arrays (SELL reorder / chunk_len, S-ELL row_width, DIA diag_offsets,
+BSR row_ptr / block_colindex) must equal the reference's bit for bit (golden
+fixtures written by the reference itself); padded col/val arrays must equal
+the reference layout built from them; SpMV results must match the oracle to
+1e-12 on the componentwise metric.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from sparseops_b200 import synth
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def _csr(rp, ci, v, ncols=None, on_device=True):
+    from sparseops_b200 import CSR_Matrix
+    n = len(rp) - 1
+    ncols = n if ncols is None else ncols
+    if on_device:
+        return CSR_Matrix(n, ncols, _dev(rp), _dev(ci), _dev(v))
+    return CSR_Matrix(n, ncols, rp, ci, v)
+
+
+def _spmv(fn, A, x, alpha=0.8, beta=0.7, y0=None):
+    import torch
+    n = A.num_rows
+    y0 = np.ones(n) if y0 is None else y0
+    xd, yd = _dev(x), _dev(y0.copy())
+    fn(alpha, A, xd, beta, yd)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
+def _check(orc, rp, ci, v, x, y, alpha=0.8, beta=0.7, y0=None):
+    n = len(rp) - 1
+    y0 = np.ones(n) if y0 is None else y0
+    yref = orc.spmv_csr(rp, ci, v, x, alpha, beta, y0)
+    den = abs(alpha) * orc.absdot(rp, ci, v, x) + np.abs(beta * y0)
+    err = (np.abs(y - yref) / np.maximum(den, 1e-300)).max() if n else 0.0
+    assert err <= TOL, err
+
+
+def _ref_layout(rp, ci, v, reorder, chunk_len, C):
+    """Reference row-major padded arrays (include/sparse_conversion.h:460-484)."""
+    n = len(rp) - 1
+    off = np.concatenate([[0], np.cumsum(chunk_len.astype(np.int64) * C)])
+    col = np.full(off[-1], -1, np.int32)
+    val = np.zeros(off[-1])
+    for i in range(n):
+        r = reorder[i] if reorder is not None else i
+        c = i // C
+        base = off[c] + (i - c * C) * chunk_len[c]
+        L = rp[r + 1] - rp[r]
+        col[base:base + L] = ci[rp[r]:rp[r + 1]]
+        val[base:base + L] = v[rp[r]:rp[r + 1]]
+    return col, val
+
+
+@pytest.mark.parametrize("tag,sigma,C,align", [("a", 512, 32, 8), ("b", 64, 4, 4), ("c", 16384, 4, 4)])
+def test_sell_c_sigma(cuda, golden, orc, tag, sigma, C, align):
+    from sparseops_b200 import SpOps_sell_c_sigma, csr_to_sell_c_sigma
+    g = golden
+    rp, ci, v, x = g["pl_rp"], g["pl_ci"], g["pl_v"], g["pl_x"]
+    S = csr_to_sell_c_sigma(_csr(rp, ci, v), None, sigma, C, align)
+    assert np.array_equal(S.reorder, g[f"scs_{tag}_reorder"])
+    assert np.array_equal(S.chunk_len, g[f"scs_{tag}_chunk_len"])
+    col, val = _ref_layout(rp, ci, v, S.reorder, S.chunk_len, C)
+    assert np.array_equal(np.concatenate(S.col_index), col) and np.array_equal(np.concatenate(S.values), val)
+    assert S.validchunkNum == len(S.chunk_len)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x))
+
+
+def test_sell_c_sigma_col_major_and_uploaded(cuda, golden, orc):
+    """Device-native column-major chunks, and a struct uploaded from host
+    arrays in the reference layout, give the same SpMV."""
+    from sparseops_b200 import SELL_C_Sigma_Matrix, SpOps_sell_c_sigma, csr_to_sell_c_sigma
+    g = golden
+    rp, ci, v, x = g["pl_rp"], g["pl_ci"], g["pl_v"], g["pl_x"]
+    S = csr_to_sell_c_sigma(_csr(rp, ci, v), None, 512, 32, 8, layout=1)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x))
+    col, val = _ref_layout(rp, ci, v, g["scs_a_reorder"], g["scs_a_chunk_len"], 32)
+    U = SELL_C_Sigma_Matrix.from_arrays(len(rp) - 1, len(rp) - 1, len(ci), 512, 32, 8, g["scs_a_reorder"],
+                                        g["scs_a_chunk_len"], col, val)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, U, x))
+
+
+def test_sell_c_R(cuda, golden, orc):
+    from sparseops_b200 import SpOps_sell_c_R, csr_to_sell_c_R
+    g = golden
+    rp, ci, v, x = g["pl_rp"], g["pl_ci"], g["pl_v"], g["pl_x"]
+    S = csr_to_sell_c_R(_csr(rp, ci, v), None, 32, 8)
+    assert np.array_equal(S.reorder, g["scr_reorder"]) and np.array_equal(S.chunk_len, g["scr_chunk_len"])
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_R, S, x))
+
+
+def test_s_ell(cuda, golden, orc):
+    from sparseops_b200 import SpOps_sell, csr_to_sell
+    g = golden
+    rp, ci, v, x = g["pl_rp"], g["pl_ci"], g["pl_v"], g["pl_x"]
+    S = csr_to_sell(_csr(rp, ci, v), None, 4, 4)
+    assert np.array_equal(S.row_width, g["sell_row_width"])
+    col, val = _ref_layout(rp, ci, v, None, S.row_width, 4)
+    assert np.array_equal(np.concatenate(S.col_index), col)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell, S, x))
+
+
+@pytest.mark.parametrize("ld", [0, 1])
+def test_ell(cuda, golden, orc, ld):
+    from sparseops_b200 import SpOps_ell, csr_to_ell
+    g = golden
+    rp, ci, v, x = g["lap_rp"], g["lap_ci"], g["lap_v"], g["lap_x"]
+    E = csr_to_ell(_csr(rp, ci, v), ld)
+    assert E.max_row_width == int(np.diff(rp).max())
+    n, w = len(rp) - 1, E.max_row_width
+    col = np.asarray(E.col_index).reshape((n, w) if ld == 0 else (w, n))
+    if ld == 1:
+        col = col.T
+    for r in (0, 1, n // 2, n - 1):  # row r holds its entries first, then -1
+        L = rp[r + 1] - rp[r]
+        assert np.array_equal(col[r, :L], ci[rp[r]:rp[r + 1]]) and (col[r, L:] == -1).all()
+    _check(orc, rp, ci, v, x, _spmv(SpOps_ell, E, x))
+
+
+@pytest.mark.parametrize("name", ["lap", "band"])
+def test_dia(cuda, golden, orc, name):
+    from sparseops_b200 import SpOps_dia, csr_to_dia
+    g = golden
+    rp, ci, v = g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"]
+    x = synth.uniform(len(rp) - 1, 17)
+    D = csr_to_dia(_csr(rp, ci, v), 10240, None, 4)
+    assert np.array_equal(D.diag_offsets, g[f"dia_{name}_offsets"])
+    assert D.stride == int(g[f"dia_{name}_stride"])
+    _check(orc, rp, ci, v, x, _spmv(SpOps_dia, D, x))
+
+
+def test_dia_too_many_diagonals(cuda):
+    from sparseops_b200 import SpOpsError, csr_to_dia
+    rp, ci, v = synth.powerlaw(3000, seed=30)
+    with pytest.raises(SpOpsError) as e:
+        csr_to_dia(_csr(rp, ci, v), 100)
+    assert e.value.status == 5
+
+
+@pytest.mark.parametrize("name,br,bc", [("lap", 16, 4), ("pl", 16, 8)])
+def test_bsr(cuda, golden, orc, name, br, bc):
+    from sparseops_b200 import SpOps_bsr, csr_to_bsr
+    g = golden
+    rp, ci, v = g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"]
+    x = synth.uniform(len(rp) - 1, 18)
+    B = csr_to_bsr(_csr(rp, ci, v), br, bc)
+    assert np.array_equal(B.row_ptr, g[f"bsr_{name}_row_ptr"]) and np.array_equal(B.block_colindex,
+                                                                                  g[f"bsr_{name}_col"])
+    _check(orc, rp, ci, v, x, _spmv(SpOps_bsr, B, x))
+
+
+def test_coo(cuda, golden, orc):
+    from sparseops_b200 import COO_Matrix, SpOps_coo, csr_to_coo
+    g = golden
+    rp, ci, v, x = g["pl_rp"], g["pl_ci"], g["pl_v"], g["pl_x"]
+    K = csr_to_coo(_csr(rp, ci, v))
+    rows = np.repeat(np.arange(len(rp) - 1, dtype=np.int32), np.diff(rp))
+    assert np.array_equal(K.row_index, rows) and np.array_equal(K.col_index, ci)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_coo, K, x))
+    # unsorted triplets from the host
+    perm = np.random.default_rng(3).permutation(len(ci))
+    U = COO_Matrix(len(rp) - 1, len(rp) - 1, rows[perm], ci[perm], v[perm])
+    _check(orc, rp, ci, v, x, _spmv(SpOps_coo, U, x))
+
+
+def test_sell_long_rows_and_empty_rows(cuda, orc):
+    """Stored rows longer than one piece (2048 slots) and empty rows, both layouts."""
+    from sparseops_b200 import SpOps_sell_c_sigma, csr_to_sell_c_sigma
+    rng = np.random.default_rng(9)
+    n, ncols = 5000, 100000
+    lens = rng.integers(0, 30, n)
+    lens[7], lens[1500], lens[4999] = 9000, 2049, 30000
+    lens[100:700] = 0
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    x = rng.uniform(-1, 1, ncols)
+    rp = rp.astype(np.int32)
+    for layout in (0, 1):
+        S = csr_to_sell_c_sigma(_csr(rp, ci, v, ncols), None, 512, 32, 8, layout=layout)
+        _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x))
+
+
+def test_powerlaw_full_sell_and_ell(cuda, orc):
+    """Power-law config at full size: SELL-C-sigma (C=32, sigma=512) and
+    SELL-C-R match the oracle; ELL is refused (it would need ~1 TB)."""
+    from sparseops_b200 import (SpOps_sell_c_R, SpOps_sell_c_sigma, SpOpsError, csr_to_ell, csr_to_sell_c_R,
+                                csr_to_sell_c_sigma)
+    n = 4194304
+    rp, ci, v = synth.powerlaw(n, mu=math.log(12.0), sigma=1.2, lo=1, hi=20000, seed=1)
+    x = synth.uniform(n, 1)
+    A = _csr(rp, ci, v)
+    S = csr_to_sell_c_sigma(A, None, 512, 32, 8)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x, 1.0, 0.0), 1.0, 0.0)
+    del S
+    R = csr_to_sell_c_R(A, None, 32, 8)
+    _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_R, R, x, 1.0, 0.0), 1.0, 0.0)
+    del R
+    with pytest.raises(SpOpsError) as e:
+        csr_to_ell(A)
+    assert e.value.status == 5
