@@ -135,6 +135,10 @@ spops_status_t spops_matrix_analyse(spops_context_t ctx, spops_matrix_t A);
 /* Bytes of device memory the handle owns (arrays + analysis). */
 spops_status_t spops_matrix_device_bytes(spops_matrix_t A, int64_t* bytes);
 
+/* Point a CSR handle at new values (same pattern, same length, device
+ * pointer, borrowed).  Keeps the analysis; marks derived values stale. */
+spops_status_t spops_csr_set_values(spops_matrix_t A, const void* values);
+
 /* ------------------------------------------------------ format handles */
 /* Device conversion of a CSR handle into another format (all work on the
  * device; integer layout arrays are bit-identical to the reference's):
@@ -215,6 +219,20 @@ spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t
  * counterpart (the reference has no SpMM); equals k SpOps_csr calls. */
 spops_status_t spops_spmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* X, int64_t ldx,
                           int64_t k, double beta, void* Y, int64_t ldy);
+
+/* ------------------------------------------------------------ adjoints */
+/* y = alpha * A^T x + beta * y for a CSR handle: x[rows], y[cols] (device).
+ * Replaces csr_transpose (include/sparse_conversion.h:2066) followed by
+ * SpOps_csr on the transpose; the transpose pattern is built once on the
+ * device (no atomics) and its values follow A's (spops_matrix_touch). */
+spops_status_t spops_spmv_t(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x, double beta,
+                            void* y);
+/* out[k] = alpha * g[row(k)] * x[col(k)] for every stored entry k of a CSR
+ * handle (sampled dense-dense product on A's pattern): the gradient of
+ * sum_i g_i * (alpha*A*x)_i with respect to A's values.  No reference
+ * counterpart (the reference has no differentiation). */
+spops_status_t spops_sddmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* g, const void* x,
+                           void* out);
 
 #ifdef __cplusplus
 }

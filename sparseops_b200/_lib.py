@@ -65,6 +65,9 @@ _SIGS = {
     "spops_bsr_create": [vp, vp, i64, i64, i64, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
     "spops_matrix_array": [vp, C.c_int, vp, vp, vp],
     "spops_matrix_download": [vp, vp, C.c_int, vp, i64],
+    "spops_csr_set_values": [vp, vp],
+    "spops_spmv_t": [vp, dbl, vp, vp, dbl, vp],
+    "spops_sddmm": [vp, dbl, vp, vp, vp, vp],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
     "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
 }

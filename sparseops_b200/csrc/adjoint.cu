@@ -1,0 +1,232 @@
+// Adjoint kernels of y = alpha*A*x + beta*y for a CSR matrix A:
+//   dL/dx      = alpha * A^T g      (transpose SpMV)
+//   dL/dA_ij   = alpha * g_i * x_j  on A's pattern (SDDMM)
+// The reference has no differentiation; the transpose it offers is
+// csr_transpose (include/sparse_conversion.h:2066-2108: CSR -> COO -> swap ->
+// counting sort, then SpOps_csr), which the oracle restates for grad_x.
+//
+// Transpose, atomic-free: once per pattern a stable radix sort of the column
+// indices gives perm (entry of A at each position of A^T) together with the
+// row indices, and a histogram + scan gives A^T's row offsets; A^T's values
+// are gathered through perm whenever A's values change (spops_matrix_touch /
+// spops_csr_set_values).  A^T g then runs the ordinary CSR kernel on that
+// matrix, so it needs no atomics and is deterministic.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "device_util.cuh"
+#include "spops_internal.h"
+
+namespace spops {
+namespace {
+
+inline unsigned grid_for(int64_t work, int threads = 256) {
+  int64_t g = (work + threads - 1) / threads;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+template <typename I>
+__global__ void expand_rows_kernel(const I* __restrict__ rp, int64_t n, I* __restrict__ row) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  for (int64_t k = (int64_t)rp[r] + lane; k < (int64_t)rp[r + 1]; k += 32) row[k] = (I)r;
+}
+
+template <typename I>
+__global__ void count_cols_kernel(const I* __restrict__ ci, int64_t nnz, unsigned long long* __restrict__ cnt) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += stride)
+    atomicAdd(cnt + ci[k], 1ULL);
+}
+
+template <typename I>
+__global__ void cast_kernel(const unsigned long long* __restrict__ in, int64_t m, I* __restrict__ out) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) out[k] = (I)in[k];
+}
+
+__global__ void iota64_kernel(int64_t* __restrict__ a, int64_t m) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) a[k] = k;
+}
+
+template <typename I>
+__global__ void gather_index_kernel(const int64_t* __restrict__ perm, const I* __restrict__ src, int64_t m,
+                                    I* __restrict__ dst) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) dst[k] = src[perm[k]];
+}
+
+template <typename V>
+__global__ void gather_values_kernel(const int64_t* __restrict__ perm, const V* __restrict__ src, int64_t m,
+                                     V* __restrict__ dst) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) dst[k] = src[perm[k]];
+}
+
+// out[k] = alpha * g[row(k)] * x[col(k)], over the CSR plan's segments.
+template <typename I, typename V>
+__global__ void __launch_bounds__(256) sddmm_kernel(const I* __restrict__ rp, const I* __restrict__ ci,
+                                                    const V* __restrict__ g, const V* __restrict__ x,
+                                                    V* __restrict__ out, V alpha, const CsrSeg* __restrict__ segs,
+                                                    int64_t nseg) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < nseg; j += nwarps) {
+    const CsrSeg d = segs[j];
+    if (d.chunk >= 0) {
+      const V gi = alpha * g[d.r0];
+      for (int64_t k = d.p0 + lane; k < d.p1; k += 32) out[k] = gi * ld_gather(x + ld_stream(ci + k));
+    } else {
+      const int nr = d.nr;
+      int t = 32 / (nr > 0 ? nr : 1);
+      t = t >= 32 ? 32 : t >= 16 ? 16 : t >= 8 ? 8 : t >= 4 ? 4 : t >= 2 ? 2 : 1;
+      const int groups = 32 / t, grp = lane / t, sub = lane % t;
+      for (int rb = 0; rb < nr; rb += groups) {
+        const int rr = rb + grp;
+        if (rr < nr) {
+          const int64_t r = d.r0 + rr;
+          const V gi = alpha * g[r];
+          for (int64_t k = (int64_t)rp[r] + sub; k < (int64_t)rp[r + 1]; k += t)
+            out[k] = gi * ld_gather(x + ld_stream(ci + k));
+        }
+      }
+    }
+  }
+}
+
+template <typename I, typename V>
+spops_status_t build_transpose_t(Context* ctx, Matrix* A) {
+  TransposeData& T = A->tr;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = A->rows, nc = A->cols, nnz = A->nnz;
+  size_t cub_sort = 0, cub_scan = 0;
+  {
+    I* k = nullptr;
+    int64_t* v = nullptr;
+    unsigned long long* u = nullptr;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort, k, k, v, v, (int64_t)(nnz > 0 ? nnz : 1), 0,
+                                               8 * (int)sizeof(I), st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, u, u, (int64_t)(nc + 1), st));
+  }
+  const size_t nz = (size_t)(nnz > 0 ? nnz : 1), nc1 = (size_t)nc + 1;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t need = al(nz * sizeof(I)) * 2 + al(nz * 8) + al(nc1 * 8) * 2 + std::max(cub_sort, cub_scan);
+  SPOPS_TRY(ctx->scratch_reserve(need));
+  char* base = ctx->scratch.as<char>();
+  size_t off = 0;
+  auto take = [&](size_t b) { char* p = base + off; off += al(b); return p; };
+  I* keys_out = reinterpret_cast<I*>(take(nz * sizeof(I)));
+  I* rows = reinterpret_cast<I*>(take(nz * sizeof(I)));
+  int64_t* idx = reinterpret_cast<int64_t*>(take(nz * 8));
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(take(nc1 * 8));
+  unsigned long long* scan = reinterpret_cast<unsigned long long*>(take(nc1 * 8));
+  void* cub_tmp = take(std::max(cub_sort, cub_scan));
+
+  T.release();
+  SPOPS_TRY(T.rp.alloc(nc1 * sizeof(I)));
+  SPOPS_TRY(T.ri.alloc(nz * sizeof(I)));
+  SPOPS_TRY(T.perm.alloc(nz * 8));
+  SPOPS_TRY(T.val.alloc(nz * sizeof(V)));
+  SPOPS_CUDA(cudaMemsetAsync(cnt, 0, nc1 * 8, st));
+  if (nnz > 0) {
+    count_cols_kernel<I><<<std::min<unsigned>(grid_for(nnz), 8192u), 256, 0, st>>>(A->col.as<I>(), nnz, cnt);
+    iota64_kernel<<<grid_for(nnz), 256, 0, st>>>(idx, nnz);
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_sort, A->col.as<I>(), keys_out, idx, T.perm.as<int64_t>(),
+                                               nnz, 0, 8 * (int)sizeof(I), st));
+    expand_rows_kernel<I><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), n, rows);
+    gather_index_kernel<I><<<grid_for(nnz), 256, 0, st>>>(T.perm.as<int64_t>(), rows, nnz, T.ri.as<I>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, cnt, scan, (int64_t)nc1, st));
+  cast_kernel<I><<<grid_for((int64_t)nc1), 256, 0, st>>>(scan, (int64_t)nc1, T.rp.as<I>());
+  SPOPS_LAUNCH_CHECK();
+  // the CSR handle of A^T borrows the arrays above
+  Matrix* V_ = new Matrix();
+  V_->ctx = ctx;
+  V_->format = SPOPS_FMT_CSR;
+  V_->itype = A->itype;
+  V_->vtype = A->vtype;
+  V_->rows = nc;
+  V_->cols = n;
+  V_->nnz = nnz;
+  V_->row.borrow(T.rp.p, T.rp.bytes);
+  V_->col.borrow(T.ri.p, T.ri.bytes);
+  V_->val.borrow(T.val.p, T.val.bytes);
+  T.view = V_;
+  spops_status_t s = csr_analyse(ctx, V_);
+  if (s != SPOPS_OK) {
+    T.release();
+    return s;
+  }
+  T.ready = true;
+  T.values_fresh = false;
+  return SPOPS_OK;
+}
+
+template <typename I, typename V>
+spops_status_t refresh_values_t(Context* ctx, Matrix* A) {
+  TransposeData& T = A->tr;
+  if (A->nnz > 0) {
+    gather_values_kernel<V><<<grid_for(A->nnz), 256, 0, ctx->stream>>>(T.perm.as<int64_t>(), A->val.as<V>(), A->nnz,
+                                                                       T.val.as<V>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  T.values_fresh = true;
+  return SPOPS_OK;
+}
+
+template <typename I, typename V>
+spops_status_t sddmm_t(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out) {
+  const CsrPlan& P = A->plan;
+  if (P.nblocks == 0) return SPOPS_OK;
+  int64_t grid = (int64_t)ctx->num_sms * 8;
+  const int64_t need = (P.nblocks + 7) / 8;
+  if (grid > need) grid = need;
+  sddmm_kernel<I, V><<<(unsigned)grid, 256, 0, ctx->stream>>>(A->row.as<I>(), A->col.as<I>(),
+                                                              static_cast<const V*>(g), static_cast<const V*>(x),
+                                                              static_cast<V*>(out), (V)alpha, P.seg.as<CsrSeg>(),
+                                                              P.nblocks);
+  SPOPS_LAUNCH_CHECK();
+  return SPOPS_OK;
+}
+
+#define SPOPS_DISPATCH2(A, FN, ...)                                                             \
+  (((A)->itype == SPOPS_INDEX_I32)                                                              \
+       ? (((A)->vtype == SPOPS_VALUE_F64) ? FN<int32_t, double>(__VA_ARGS__) : FN<int32_t, float>(__VA_ARGS__)) \
+       : (((A)->vtype == SPOPS_VALUE_F64) ? FN<int64_t, double>(__VA_ARGS__) : FN<int64_t, float>(__VA_ARGS__)))
+
+}  // namespace
+
+void TransposeData::release() {
+  rp.release();
+  ri.release();
+  perm.release();
+  val.release();
+  if (view) {
+    view->release_all();
+    delete view;
+    view = nullptr;
+  }
+  ready = false;
+  values_fresh = false;
+}
+
+spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "transpose SpMV needs a CSR matrix");
+  if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+  if (!A->tr.ready) SPOPS_TRY(SPOPS_DISPATCH2(A, build_transpose_t, ctx, A));
+  if (!A->tr.values_fresh) SPOPS_TRY(SPOPS_DISPATCH2(A, refresh_values_t, ctx, A));
+  return csr_spmv(ctx, A->tr.view, alpha, x, beta, y);
+}
+
+spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out) {
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "SDDMM needs a CSR matrix");
+  if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+  return SPOPS_DISPATCH2(A, sddmm_t, ctx, A, alpha, g, x, out);
+}
+
+}  // namespace spops

@@ -359,7 +359,33 @@ spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info) {
 
 spops_status_t spops_matrix_touch(spops_matrix_t A) {
   if (!A) return fail(SPOPS_ERR_INVALID, "spops_matrix_touch: null matrix");
-  return SPOPS_OK;  // the CSR plan depends on the pattern only
+  A->tr.values_fresh = false;  // the CSR plan depends on the pattern only
+  return SPOPS_OK;
+}
+
+spops_status_t spops_csr_set_values(spops_matrix_t A, const void* values) {
+  if (!A) return fail(SPOPS_ERR_INVALID, "spops_csr_set_values: null matrix");
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "spops_csr_set_values: not a CSR matrix");
+  if (!values && A->nnz > 0) return fail(SPOPS_ERR_INVALID, "spops_csr_set_values: null values");
+  A->val.borrow(values, (size_t)A->nnz * A->vsize());
+  A->tr.values_fresh = false;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_spmv_t(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x, double beta,
+                            void* y) {
+  if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_spmv_t: null context/matrix");
+  if ((!x && A->rows > 0) || (!y && A->cols > 0)) return fail(SPOPS_ERR_INVALID, "spops_spmv_t: null vector");
+  DeviceGuard g(ctx->device);
+  return csr_spmv_transpose(ctx, A, alpha, x, beta, y);
+}
+
+spops_status_t spops_sddmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* g, const void* x,
+                           void* out) {
+  if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_sddmm: null context/matrix");
+  if (A->nnz > 0 && (!g || !x || !out)) return fail(SPOPS_ERR_INVALID, "spops_sddmm: null vector");
+  DeviceGuard gd(ctx->device);
+  return csr_sddmm(ctx, A, alpha, g, x, out);
 }
 
 spops_status_t spops_matrix_analyse(spops_context_t ctx, spops_matrix_t A) {
@@ -382,6 +408,11 @@ spops_status_t spops_matrix_device_bytes(spops_matrix_t A, int64_t* bytes) {
   b += own(D.reorder) + own(D.chunk_len) + own(D.chunk_off) + own(D.row_len) + own(D.piece) + own(D.partial) +
        own(D.counter);
   b += own(A->dia.offsets) + own(A->dia.data) + own(A->bsr.row_ptr) + own(A->bsr.bcol) + own(A->bsr.data);
+  b += own(A->tr.rp) + own(A->tr.ri) + own(A->tr.perm) + own(A->tr.val);
+  if (A->tr.view) {
+    const CsrPlan& Q = A->tr.view->plan;
+    b += own(Q.blk_row) + own(Q.blk_chunk) + own(Q.partial) + own(Q.counter) + own(Q.seg);
+  }
   if (A->csr_view) {
     int64_t c = 0;
     spops_matrix_device_bytes(static_cast<spops_matrix_s*>(A->csr_view), &c);

@@ -962,6 +962,7 @@ void Matrix::release_all() {
   pad.release();
   dia.release();
   bsr.release();
+  tr.release();
   if (csr_view) {
     csr_view->release_all();
     delete csr_view;

@@ -159,6 +159,19 @@ struct BsrData {
   void release() { row_ptr.release(); bcol.release(); data.release(); }
 };
 
+// Transpose of a CSR pattern (A^T as CSR), built once per pattern; values
+// refreshed through perm after A's values change (adjoint.cu).
+struct Matrix;
+struct TransposeData {
+  bool ready = false, values_fresh = false;
+  DevBuf rp;    // I [cols + 1]
+  DevBuf ri;    // I [nnz]
+  DevBuf perm;  // int64 [nnz]: entry of A at each position of A^T
+  DevBuf val;   // V [nnz]
+  Matrix* view = nullptr;  // CSR handle of A^T over the arrays above
+  void release();
+};
+
 // ---------------------------------------------------------------- matrix
 struct Matrix {
   Context* ctx = nullptr;
@@ -173,6 +186,7 @@ struct Matrix {
   PaddedData pad;
   DiaData dia;
   BsrData bsr;
+  TransposeData tr;
   // COO: the same entries as a CSR matrix sorted by row (owned)
   Matrix* csr_view = nullptr;
   size_t isize() const { return itype == SPOPS_INDEX_I32 ? 4 : 8; }
@@ -192,6 +206,9 @@ spops_status_t padded_spmv(Context* ctx, Matrix* A, double alpha, const void* x,
 spops_status_t dia_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t bsr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t coo_analyse(Context* ctx, Matrix* A);
+// adjoint.cu
+spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out);
 spops_status_t validate_columns(Context* ctx, const void* col, int64_t count, spops_index_t it, int64_t ncols,
                                 bool allow_pad);
 
