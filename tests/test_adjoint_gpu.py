@@ -129,7 +129,7 @@ def test_values_update_refreshes_transpose(cuda, orc):
     n = 30000
     rp, ci, v = _graph(n, seed=8)
     m = SparseLinear(n, n, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda())
-    opt = torch.optim.SGD(m.parameters(), lr=0.1)
+    opt = torch.optim.SGD(m.parameters(), lr=1e-4)
     x = torch.from_numpy(synth.uniform(n, 48)).cuda().requires_grad_(True)
     for _ in range(3):
         opt.zero_grad()
