@@ -66,6 +66,7 @@ typedef enum { SPOPS_ROW_MAJOR = 0, SPOPS_COL_MAJOR = 1 } spops_layout_t;
 
 typedef struct spops_context_s* spops_context_t;
 typedef struct spops_matrix_s* spops_matrix_t;
+typedef struct spops_batch_s* spops_batch_t;
 
 /* Parameters of a format conversion; zero means "reference default". */
 typedef struct {
@@ -219,6 +220,36 @@ spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t
  * counterpart (the reference has no SpMM); equals k SpOps_csr calls. */
 spops_status_t spops_spmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* X, int64_t ldx,
                           int64_t k, double beta, void* Y, int64_t ldy);
+
+/* ------------------------------------------------------------- batches */
+/* Many CSR matrices (uneven sizes, same index/value types) run as ONE
+ * persistent kernel launch: y_m = alpha * A_m x_m + beta * y_m for every m,
+ * or with k > 1 right-hand sides Y_m = alpha * A_m X_m + beta * Y_m
+ * (row-major X_m [cols_m x ldx_m], Y_m [rows_m x ldy_m]).
+ * No reference counterpart: the reference calls SpOps_csr once per matrix
+ * and column (the baseline these are compared with).
+ * The handles must outlive the batch.  Work runs on the batch's own stream,
+ * ordered after and before the context's stream with events. */
+spops_status_t spops_batch_create(spops_context_t ctx, spops_batch_t* batch, int64_t count,
+                                  const spops_matrix_t* mats, int64_t k);
+spops_status_t spops_batch_destroy(spops_batch_t batch);
+/* Device pointers of x/X and y/Y per matrix (host arrays of `count`
+ * pointers); ldx / ldy may be NULL (= k). */
+spops_status_t spops_batch_set_vectors(spops_batch_t batch, const void* const* X, const int64_t* ldx,
+                                       void* const* Y, const int64_t* ldy);
+/* Autotune: per matrix (k = 1) time CSR against SELL-C-sigma with C = 32,
+ * sigma in {256, 4096}, row- and column-major chunks, on the device, and keep
+ * the fastest; for k > 1 pick the right-hand-side tile (8 or 32 lanes).
+ * flags bit 0: CSR only.  Needs the vectors set (it runs the products). */
+spops_status_t spops_batch_tune(spops_context_t ctx, spops_batch_t batch, int32_t flags);
+/* One persistent launch over all matrices (a captured graph is replayed
+ * when alpha/beta match the captured ones). */
+spops_status_t spops_batch_run(spops_context_t ctx, spops_batch_t batch, double alpha, double beta);
+/* Capture the launch into a CUDA graph for later spops_batch_run calls. */
+spops_status_t spops_batch_capture(spops_context_t ctx, spops_batch_t batch, double alpha, double beta);
+/* items: work items of the launch; choice[count]: 0 = CSR, 1..4 = SELL-C-sigma
+ * candidate (sigma 256/4096 x row/col-major); rhs_tile: lanes per RHS tile. */
+spops_status_t spops_batch_info(spops_batch_t batch, int64_t* items, int32_t* choice, int32_t* rhs_tile);
 
 /* ------------------------------------------------------------ adjoints */
 /* y = alpha * A^T x + beta * y for a CSR handle: x[rows], y[cols] (device).

@@ -68,6 +68,14 @@ _SIGS = {
     "spops_csr_set_values": [vp, vp],
     "spops_spmv_t": [vp, dbl, vp, vp, dbl, vp],
     "spops_sddmm": [vp, dbl, vp, vp, vp, vp],
+    "spops_spmm": [vp, dbl, vp, vp, i64, i64, dbl, vp, i64],
+    "spops_batch_create": [vp, vp, i64, vp, i64],
+    "spops_batch_destroy": [vp],
+    "spops_batch_set_vectors": [vp, vp, vp, vp, vp],
+    "spops_batch_tune": [vp, vp, i32],
+    "spops_batch_run": [vp, vp, dbl, dbl],
+    "spops_batch_capture": [vp, vp, dbl, dbl],
+    "spops_batch_info": [vp, vp, vp, vp],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
     "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
 }

@@ -1,0 +1,561 @@
+// Batched SpMV / SpMM: many matrices of uneven sizes in ONE persistent launch.
+//
+// No reference counterpart (the reference runs one SpOps_<fmt> call per
+// matrix and has no multi-RHS product); its per-matrix loop is the baseline.
+//
+// A batch lists work items (matrix, kind, index) over all its matrices, in
+// matrix order so each matrix's x stays in L2 while its items run:
+//   kind 0  CSR segment of the matrix's CSR plan (csr_segment_spmv / _spmm)
+//   kind 1  32 stored rows of the matrix's padded (SELL) form (padded_rows32)
+//   kind 2  one piece of a long padded row (padded_piece)
+// A persistent grid (SMs x resident blocks) of warps walks the item list.
+// Per-matrix pointers live in a device table; the launch itself (on the
+// batch's own stream, ordered against the caller's stream with events) can
+// be captured once into a CUDA graph and replayed.
+//
+// Autotuner (spops_batch_tune): per matrix, times the candidate forms with
+// CUDA events on the device -- CSR (segments of kCsrCap entries), and
+// SELL-C-sigma with C = 32 and sigma in {256, 4096}, row-major and
+// column-major chunks -- and keeps the fastest for the batched launch.  For
+// k > 1 the CSR form is used and the tuner picks the RHS tile (8 or 32 lanes).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "device_util.cuh"
+#include "spops_internal.h"
+#include "warp_work.cuh"
+
+namespace spops {
+
+struct BatchItem {
+  int32_t mat;
+  int32_t kind;
+  int64_t idx;
+};
+
+struct BatchMat {
+  // CSR form
+  const void* rp;
+  const void* ci;
+  const void* val;
+  const CsrSeg* seg;
+  void* partial;  // CSR long-row chunk sums (k per chunk for SpMM)
+  int* counter;
+  // padded form
+  const void* pcol;
+  const void* pval;
+  const void* chunk_len;
+  const int64_t* chunk_off;
+  const int* row_len;
+  const void* reorder;
+  const PadPiece* pieces;
+  void* ppartial;
+  int* pcounter;
+  int64_t C;
+  int32_t colmajor;
+  int32_t pad0;
+  int64_t rows;
+  // vectors
+  const void* x;
+  void* y;
+  int64_t ldx, ldy;
+};
+
+namespace {
+
+constexpr int kBatchBlock = 256;
+
+template <typename I, typename V, int KT>
+__global__ void __launch_bounds__(kBatchBlock, 4) batch_kernel(const BatchItem* __restrict__ items, int64_t nitems,
+                                                               const BatchMat* __restrict__ mats, int64_t k, V alpha,
+                                                               V beta, bool bz) {
+  __shared__ V prod_all[kBatchBlock / 32][2 * kCsrCap];
+  const int lane = threadIdx.x & 31;
+  V* prod = prod_all[threadIdx.x >> 5];
+  const int64_t nwarps = (int64_t)gridDim.x * (kBatchBlock / 32);
+  for (int64_t j = (blockIdx.x * (int64_t)kBatchBlock + threadIdx.x) >> 5; j < nitems; j += nwarps) {
+    const BatchItem it = items[j];
+    const BatchMat& M = mats[it.mat];
+    if (KT == 1) {
+      if (it.kind == 0) {
+        csr_segment_spmv<I, V, 8>(M.seg[it.idx], it.idx, static_cast<const I*>(M.ci), static_cast<const V*>(M.val),
+                                  static_cast<const I*>(M.rp), static_cast<const V*>(M.x), static_cast<V*>(M.y),
+                                  alpha, beta, bz, prod, static_cast<V*>(M.partial), M.counter, lane);
+      } else if (it.kind == 1) {
+        if (M.colmajor)
+          padded_rows32<I, V, true>(it.idx * 32, static_cast<const I*>(M.pcol), static_cast<const V*>(M.pval),
+                                    static_cast<const I*>(M.chunk_len), M.chunk_off, M.row_len,
+                                    static_cast<const I*>(M.reorder), M.rows, M.C, static_cast<const V*>(M.x),
+                                    static_cast<V*>(M.y), alpha, beta, bz, lane);
+        else
+          padded_rows32<I, V, false>(it.idx * 32, static_cast<const I*>(M.pcol), static_cast<const V*>(M.pval),
+                                     static_cast<const I*>(M.chunk_len), M.chunk_off, M.row_len,
+                                     static_cast<const I*>(M.reorder), M.rows, M.C, static_cast<const V*>(M.x),
+                                     static_cast<V*>(M.y), alpha, beta, bz, lane);
+      } else {
+        if (M.colmajor)
+          padded_piece<I, V, true>(it.idx, M.pieces[it.idx], static_cast<const I*>(M.pcol),
+                                   static_cast<const V*>(M.pval), static_cast<const I*>(M.chunk_len), M.chunk_off,
+                                   M.row_len, static_cast<const I*>(M.reorder), M.C, static_cast<const V*>(M.x),
+                                   static_cast<V*>(M.y), alpha, beta, bz, static_cast<V*>(M.ppartial), M.pcounter,
+                                   lane);
+        else
+          padded_piece<I, V, false>(it.idx, M.pieces[it.idx], static_cast<const I*>(M.pcol),
+                                    static_cast<const V*>(M.pval), static_cast<const I*>(M.chunk_len), M.chunk_off,
+                                    M.row_len, static_cast<const I*>(M.reorder), M.C, static_cast<const V*>(M.x),
+                                    static_cast<V*>(M.y), alpha, beta, bz, static_cast<V*>(M.ppartial), M.pcounter,
+                                    lane);
+      }
+    } else {
+      csr_segment_spmm<I, V, KT>(M.seg[it.idx], it.idx, static_cast<const I*>(M.ci), static_cast<const V*>(M.val),
+                                 static_cast<const I*>(M.rp), static_cast<const V*>(M.x), M.ldx,
+                                 static_cast<V*>(M.y), M.ldy, k, alpha, beta, bz, static_cast<V*>(M.partial),
+                                 M.counter, lane);
+    }
+  }
+}
+
+// Single-matrix SpMM over the CSR plan (the per-matrix path of spops_spmm).
+template <typename I, typename V, int KT>
+__global__ void __launch_bounds__(256, 4) spmm_kernel(const CsrSeg* __restrict__ segs, int64_t nseg,
+                                                      const I* __restrict__ ci, const V* __restrict__ val,
+                                                      const I* __restrict__ rp, const V* __restrict__ X, int64_t ldx,
+                                                      V* __restrict__ Y, int64_t ldy, int64_t k, V alpha, V beta,
+                                                      bool bz, V* __restrict__ partial, int* __restrict__ counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < nseg; j += nwarps)
+    csr_segment_spmm<I, V, KT>(segs[j], j, ci, val, rp, X, ldx, Y, ldy, k, alpha, beta, bz, partial, counter, lane);
+}
+
+template <typename K>
+int occupancy(K kernel, int threads) {
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, 0) != cudaSuccess || bps < 1) return 1;
+  return bps;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- SpMM (single)
+template <typename I, typename V>
+static spops_status_t spmm_t(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k,
+                             double beta, void* Y, int64_t ldy) {
+  CsrPlan& P = A->plan;
+  if (P.nblocks == 0 || k == 0) return SPOPS_OK;
+  if (P.nlong > 0 && A->spmm_partial.bytes < (size_t)P.nblocks * k * sizeof(V))
+    SPOPS_TRY(A->spmm_partial.alloc((size_t)P.nblocks * k * sizeof(V)));
+  const int kt = k >= 32 ? 32 : (k >= 8 ? 8 : 8);
+  const bool bz = beta == 0.0;
+  auto launch = [&](auto kern) -> spops_status_t {
+    static int bps = -1;
+    if (bps < 0) bps = occupancy(kern, 256);
+    int64_t grid = (int64_t)ctx->num_sms * bps;
+    const int64_t need = (P.nblocks + 7) / 8;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, 256, 0, ctx->stream>>>(P.seg.as<CsrSeg>(), P.nblocks, A->col.as<I>(), A->val.as<V>(),
+                                                  A->row.as<I>(), static_cast<const V*>(X), ldx, static_cast<V*>(Y),
+                                                  ldy, k, (V)alpha, (V)beta, bz, A->spmm_partial.as<V>(),
+                                                  P.counter.as<int>());
+    SPOPS_LAUNCH_CHECK();
+    return SPOPS_OK;
+  };
+  if (kt == 32) return launch(spmm_kernel<I, V, 32>);
+  return launch(spmm_kernel<I, V, 8>);
+}
+
+spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k, double beta,
+                        void* Y, int64_t ldy) {
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "SpMM needs a CSR matrix");
+  if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+  const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return spmm_t<int32_t, double>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+  if (i32) return spmm_t<int32_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+  if (f64) return spmm_t<int64_t, double>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+  return spmm_t<int64_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+}
+
+// ------------------------------------------------------------------ batch
+struct Batch {
+  Context* ctx = nullptr;
+  int64_t count = 0, k = 1;
+  spops_index_t itype = SPOPS_INDEX_I32;
+  spops_value_t vtype = SPOPS_VALUE_F64;
+  std::vector<Matrix*> src;
+  std::vector<Matrix*> form;  // padded form chosen by the tuner (owned), or null for CSR
+  std::vector<int> choice;    // 0 CSR, 1.. padded candidate index
+  std::vector<BatchMat> host;
+  std::vector<DevBuf> spmm_partial;
+  DevBuf items, table;
+  int64_t nitems = 0;
+  int kt = 8;  // RHS tile for k > 1
+  bool dirty = true;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double cap_alpha = 0, cap_beta = 0;
+  ~Batch() {
+    for (Matrix* m : form)
+      if (m) {
+        m->release_all();
+        delete static_cast<spops_matrix_s*>(m);
+      }
+    for (auto& b : spmm_partial) b.release();
+    items.release();
+    table.release();
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// the padded candidates the tuner tries: (sigma, layout)
+const int64_t kCandSigma[4] = {256, 4096, 256, 4096};
+const spops_layout_t kCandLayout[4] = {SPOPS_ROW_MAJOR, SPOPS_ROW_MAJOR, SPOPS_COL_MAJOR, SPOPS_COL_MAJOR};
+
+spops_status_t build_items(Batch* B) {
+  std::vector<BatchItem> it;
+  for (int64_t m = 0; m < B->count; ++m) {
+    Matrix* A = B->src[m];
+    Matrix* F = B->form[m];
+    if (!F || B->k > 1) {
+      for (int64_t s = 0; s < A->plan.nblocks; ++s) it.push_back(BatchItem{(int32_t)m, 0, s});
+    } else {
+      const int64_t groups = (F->rows + 31) / 32;
+      for (int64_t g = 0; g < groups; ++g) it.push_back(BatchItem{(int32_t)m, 1, g});
+      for (int64_t q = 0; q < F->pad.npieces; ++q) it.push_back(BatchItem{(int32_t)m, 2, q});
+    }
+  }
+  B->nitems = (int64_t)it.size();
+  SPOPS_TRY(B->items.alloc(std::max<size_t>(it.size(), 1) * sizeof(BatchItem)));
+  if (!it.empty())
+    SPOPS_CUDA(cudaMemcpy(B->items.p, it.data(), it.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
+  return SPOPS_OK;
+}
+
+spops_status_t build_table(Batch* B) {
+  for (int64_t m = 0; m < B->count; ++m) {
+    Matrix* A = B->src[m];
+    Matrix* F = B->form[m];
+    BatchMat& t = B->host[m];
+    t.rp = A->row.p;
+    t.ci = A->col.p;
+    t.val = A->val.p;
+    t.seg = A->plan.seg.as<CsrSeg>();
+    t.partial = B->k > 1 ? B->spmm_partial[m].p : A->plan.partial.p;
+    t.counter = A->plan.counter.as<int>();
+    t.rows = A->rows;
+    if (F) {
+      t.pcol = F->col.p;
+      t.pval = F->val.p;
+      t.chunk_len = F->pad.chunk_len.p;
+      t.chunk_off = F->pad.chunk_off.as<int64_t>();
+      t.row_len = F->pad.row_len.as<int>();
+      t.reorder = F->pad.sorted ? F->pad.reorder.p : nullptr;
+      t.pieces = F->pad.piece.as<PadPiece>();
+      t.ppartial = F->pad.partial.p;
+      t.pcounter = F->pad.counter.as<int>();
+      t.C = F->pad.C;
+      t.colmajor = F->layout == SPOPS_COL_MAJOR;
+    }
+  }
+  SPOPS_TRY(B->table.alloc(std::max<size_t>(B->host.size(), 1) * sizeof(BatchMat)));
+  SPOPS_CUDA(cudaMemcpy(B->table.p, B->host.data(), B->host.size() * sizeof(BatchMat), cudaMemcpyHostToDevice));
+  return SPOPS_OK;
+}
+
+template <typename I, typename V>
+spops_status_t launch_batch(Batch* B, double alpha, double beta, cudaStream_t st) {
+  if (B->nitems == 0) return SPOPS_OK;
+  const bool bz = beta == 0.0;
+  auto go = [&](auto kern) -> spops_status_t {
+    static int bps = -1;
+    if (bps < 0) bps = occupancy(kern, kBatchBlock);
+    int64_t grid = (int64_t)B->ctx->num_sms * bps;
+    const int64_t need = (B->nitems + 7) / 8;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, kBatchBlock, 0, st>>>(B->items.as<BatchItem>(), B->nitems, B->table.as<BatchMat>(), B->k,
+                                                 (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+    return SPOPS_OK;
+  };
+  if (B->k == 1) return go(batch_kernel<I, V, 1>);
+  if (B->kt == 32) return go(batch_kernel<I, V, 32>);
+  return go(batch_kernel<I, V, 8>);
+}
+
+spops_status_t launch_any(Batch* B, double alpha, double beta, cudaStream_t st) {
+  const bool i32 = B->itype == SPOPS_INDEX_I32, f64 = B->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return launch_batch<int32_t, double>(B, alpha, beta, st);
+  if (i32) return launch_batch<int32_t, float>(B, alpha, beta, st);
+  if (f64) return launch_batch<int64_t, double>(B, alpha, beta, st);
+  return launch_batch<int64_t, float>(B, alpha, beta, st);
+}
+
+spops_status_t prepare(Batch* B) {
+  if (!B->dirty) return SPOPS_OK;
+  for (int64_t m = 0; m < B->count; ++m) {
+    Matrix* A = B->src[m];
+    if (!A->plan.ready) SPOPS_TRY(csr_analyse(B->ctx, A));
+    if (B->k > 1 && A->plan.nlong > 0) {
+      const size_t bytes = (size_t)A->plan.nblocks * B->k * A->vsize();
+      if (B->spmm_partial[m].bytes < bytes) SPOPS_TRY(B->spmm_partial[m].alloc(bytes));
+    }
+  }
+  SPOPS_TRY(build_items(B));
+  SPOPS_TRY(build_table(B));
+  if (B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  if (B->graph) {
+    cudaGraphDestroy(B->graph);
+    B->graph = nullptr;
+  }
+  B->dirty = false;
+  return SPOPS_OK;
+}
+
+// time fn() on stream st: min over reps of CUDA-event durations (ms)
+template <typename F>
+spops_status_t time_ms(cudaStream_t st, F fn, int reps, float* out) {
+  cudaEvent_t a, b;
+  SPOPS_CUDA(cudaEventCreate(&a));
+  SPOPS_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  spops_status_t s = fn();  // warm-up
+  for (int r = 0; r < reps && s == SPOPS_OK; ++r) {
+    cudaEventRecord(a, st);
+    s = fn();
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *out = best;
+  return s;
+}
+
+}  // namespace
+
+spops_status_t batch_tune(Batch* B, int flags) {
+  Context* ctx = B->ctx;
+  cudaStream_t st = ctx->stream;
+  const bool try_padded = !(flags & 1);
+  for (int64_t m = 0; m < B->count; ++m) {
+    Matrix* A = B->src[m];
+    if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+    if (B->form[m]) {
+      B->form[m]->release_all();
+      delete static_cast<spops_matrix_s*>(B->form[m]);
+      B->form[m] = nullptr;
+    }
+    B->choice[m] = 0;
+    if (B->k > 1 || !try_padded) continue;
+    const BatchMat& t = B->host[m];
+    if (!t.x || !t.y) return fail(SPOPS_ERR_INVALID, "spops_batch_tune: vectors not set");
+    float best = 0;
+    SPOPS_TRY(time_ms(st, [&] { return csr_spmv(ctx, A, 1.0, t.x, 0.0, t.y); }, 3, &best));
+    for (int c = 0; c < 4; ++c) {
+      spops_format_params_t p;
+      std::memset(&p, 0, sizeof(p));
+      p.sigma = kCandSigma[c];
+      p.chunk = 32;
+      p.alignment = 1;
+      p.layout = kCandLayout[c];
+      Matrix* F = nullptr;
+      spops_status_t s = convert_from_csr(ctx, A, SPOPS_FMT_SELL_C_SIGMA, p, &F);
+      if (s == SPOPS_ERR_TOO_LARGE) continue;
+      SPOPS_TRY(s);
+      float ms = 0;
+      s = time_ms(st, [&] { return padded_spmv(ctx, F, 1.0, t.x, 0.0, t.y); }, 3, &ms);
+      if (s != SPOPS_OK || ms >= 0.97f * best) {  // keep CSR unless clearly faster
+        F->release_all();
+        delete static_cast<spops_matrix_s*>(F);
+        SPOPS_TRY(s);
+        continue;
+      }
+      if (B->form[m]) {
+        B->form[m]->release_all();
+        delete static_cast<spops_matrix_s*>(B->form[m]);
+      }
+      B->form[m] = F;
+      B->choice[m] = 1 + c;
+      best = ms;
+    }
+  }
+  if (B->k > 1) {  // RHS tile: time both on the whole batch
+    float t8 = 0, t32 = 0;
+    B->kt = 8;
+    B->dirty = true;
+    SPOPS_TRY(prepare(B));
+    SPOPS_TRY(time_ms(st, [&] { return launch_any(B, 1.0, 0.0, st); }, 3, &t8));
+    if (B->k >= 32) {
+      B->kt = 32;
+      SPOPS_TRY(time_ms(st, [&] { return launch_any(B, 1.0, 0.0, st); }, 3, &t32));
+      B->kt = t32 < t8 ? 32 : 8;
+    }
+  }
+  B->dirty = true;
+  return prepare(B);
+}
+
+spops_status_t batch_run(Batch* B, double alpha, double beta) {
+  Context* ctx = B->ctx;
+  SPOPS_TRY(prepare(B));
+  // order the batch's stream after the caller's, and the caller's after it
+  SPOPS_CUDA(cudaEventRecord(B->ev_in, ctx->stream));
+  SPOPS_CUDA(cudaStreamWaitEvent(B->stream, B->ev_in, 0));
+  if (B->exec && alpha == B->cap_alpha && beta == B->cap_beta) {
+    SPOPS_CUDA(cudaGraphLaunch(B->exec, B->stream));
+  } else {
+    SPOPS_TRY(launch_any(B, alpha, beta, B->stream));
+  }
+  SPOPS_CUDA(cudaEventRecord(B->ev_out, B->stream));
+  SPOPS_CUDA(cudaStreamWaitEvent(ctx->stream, B->ev_out, 0));
+  return SPOPS_OK;
+}
+
+spops_status_t batch_capture(Batch* B, double alpha, double beta) {
+  SPOPS_TRY(prepare(B));
+  if (B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  if (B->graph) {
+    cudaGraphDestroy(B->graph);
+    B->graph = nullptr;
+  }
+  // warm the occupancy queries outside the capture
+  SPOPS_TRY(launch_any(B, alpha, beta, B->stream));
+  SPOPS_CUDA(cudaStreamSynchronize(B->stream));
+  SPOPS_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+  spops_status_t s = launch_any(B, alpha, beta, B->stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+  if (s != SPOPS_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  B->graph = g;
+  SPOPS_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+  B->cap_alpha = alpha;
+  B->cap_beta = beta;
+  return SPOPS_OK;
+}
+
+}  // namespace spops
+
+using namespace spops;
+
+struct spops_batch_s : spops::Batch {};
+
+extern "C" {
+
+spops_status_t spops_spmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* X, int64_t ldx, int64_t k,
+                          double beta, void* Y, int64_t ldy) {
+  if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_spmm: null context/matrix");
+  if (k < 0 || ldx < k || ldy < k) return fail(SPOPS_ERR_INVALID, "spops_spmm: k / leading dimensions");
+  DeviceGuard g(ctx->device);
+  return csr_spmm(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+}
+
+spops_status_t spops_batch_create(spops_context_t ctx, spops_batch_t* out, int64_t count, const spops_matrix_t* mats,
+                                  int64_t k) {
+  if (!ctx || !out || (count > 0 && !mats)) return fail(SPOPS_ERR_INVALID, "spops_batch_create: null argument");
+  if (count < 0 || count > INT32_MAX || k < 1) return fail(SPOPS_ERR_INVALID, "spops_batch_create: count/k");
+  for (int64_t m = 0; m < count; ++m) {
+    if (!mats[m] || mats[m]->format != SPOPS_FMT_CSR)
+      return fail(SPOPS_ERR_INVALID, "spops_batch_create: matrix %lld is not a CSR handle", (long long)m);
+    if (mats[m]->itype != mats[0]->itype || mats[m]->vtype != mats[0]->vtype)
+      return fail(SPOPS_ERR_INVALID, "spops_batch_create: mixed index/value types");
+  }
+  DeviceGuard g(ctx->device);
+  spops_batch_s* B = new spops_batch_s();
+  B->ctx = ctx;
+  B->count = count;
+  B->k = k;
+  if (count > 0) {
+    B->itype = mats[0]->itype;
+    B->vtype = mats[0]->vtype;
+  }
+  B->src.assign(mats, mats + count);
+  B->form.assign((size_t)count, nullptr);
+  B->choice.assign((size_t)count, 0);
+  B->host.assign((size_t)count, BatchMat{});
+  B->spmm_partial.resize((size_t)count);
+  cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    delete B;
+    return cuda_fail(e, "batch stream/events", __FILE__, __LINE__);
+  }
+  *out = B;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_batch_destroy(spops_batch_t B) {
+  if (!B) return SPOPS_OK;
+  DeviceGuard g(B->ctx->device);
+  cudaStreamSynchronize(B->stream);
+  delete B;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_batch_set_vectors(spops_batch_t B, const void* const* X, const int64_t* ldx, void* const* Y,
+                                       const int64_t* ldy) {
+  if (!B || (B->count > 0 && (!X || !Y))) return fail(SPOPS_ERR_INVALID, "spops_batch_set_vectors: null argument");
+  for (int64_t m = 0; m < B->count; ++m) {
+    const int64_t lx = ldx ? ldx[m] : B->k, ly = ldy ? ldy[m] : B->k;
+    if (lx < B->k || ly < B->k) return fail(SPOPS_ERR_INVALID, "spops_batch_set_vectors: leading dimension < k");
+    B->host[m].x = X[m];
+    B->host[m].y = Y[m];
+    B->host[m].ldx = lx;
+    B->host[m].ldy = ly;
+  }
+  B->dirty = true;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_batch_tune(spops_context_t ctx, spops_batch_t B, int32_t flags) {
+  if (!ctx || !B) return fail(SPOPS_ERR_INVALID, "spops_batch_tune: null argument");
+  DeviceGuard g(ctx->device);
+  B->ctx = ctx;
+  return batch_tune(B, flags);
+}
+
+spops_status_t spops_batch_run(spops_context_t ctx, spops_batch_t B, double alpha, double beta) {
+  if (!ctx || !B) return fail(SPOPS_ERR_INVALID, "spops_batch_run: null argument");
+  DeviceGuard g(ctx->device);
+  B->ctx = ctx;
+  return batch_run(B, alpha, beta);
+}
+
+spops_status_t spops_batch_capture(spops_context_t ctx, spops_batch_t B, double alpha, double beta) {
+  if (!ctx || !B) return fail(SPOPS_ERR_INVALID, "spops_batch_capture: null argument");
+  DeviceGuard g(ctx->device);
+  B->ctx = ctx;
+  return batch_capture(B, alpha, beta);
+}
+
+spops_status_t spops_batch_info(spops_batch_t B, int64_t* items, int32_t* choice, int32_t* rhs_tile) {
+  if (!B) return fail(SPOPS_ERR_INVALID, "spops_batch_info: null batch");
+  if (items) *items = B->nitems;
+  if (choice)
+    for (int64_t m = 0; m < B->count; ++m) choice[m] = B->choice[m];
+  if (rhs_tile) *rhs_tile = B->k > 1 ? B->kt : 1;
+  return SPOPS_OK;
+}
+
+}  // extern "C"

@@ -33,13 +33,12 @@
 
 #include "device_util.cuh"
 #include "spops_internal.h"
+#include "warp_work.cuh"
 
 namespace spops {
 
 namespace {
 
-constexpr int kPadLong = 2048;   // slots; longer stored rows are summed by pieces
-constexpr int kPadPiece = 2048;  // slots per piece
 
 template <typename I>
 __device__ __forceinline__ int64_t row_length(const I* rp, int64_t r) {
@@ -164,92 +163,16 @@ __global__ void __launch_bounds__(256) padded_kernel(
     const I* __restrict__ col, const V* __restrict__ val, const I* __restrict__ chunk_len,
     const int64_t* __restrict__ chunk_off, const int* __restrict__ row_len, const I* __restrict__ reorder,
     int64_t n, int64_t C, const V* __restrict__ x, V* __restrict__ y, V alpha, V beta, bool bz,
-    int64_t main_blocks, const PadPiece* __restrict__ pieces, V* __restrict__ partial, int* __restrict__ counter) {
-  __shared__ V red[8];
-  if ((int64_t)blockIdx.x < main_blocks) {
-    const int lane = threadIdx.x & 31;
-    const int64_t i0 = ((int64_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * 32;
-    if (i0 >= n) return;  // whole warp leaves together; no block barrier below
-    const int64_t i = i0 + lane;
-    int len = 0;
-    int64_t base = 0;
-    if (i < n) {
-      len = row_len[i];
-      if (len > kPadLong) len = -1;  // long row: summed by pieces
-      const int64_t c = i / C;
-      base = chunk_off[c] + (kColMajor ? (i - c * C) : (i - c * C) * (int64_t)chunk_len[c]);
-    }
-    if (kColMajor) {
-      V s0 = V(0), s1 = V(0);
-      int k = 0;
-      for (; k + 1 < len; k += 2) {
-        const int64_t a = base + (int64_t)k * C, b = a + C;
-        const I ca = ld_stream(col + a), cb = ld_stream(col + b);
-        if (ca >= 0) s0 += ld_stream(val + a) * ld_gather(x + ca);
-        if (cb >= 0) s1 += ld_stream(val + b) * ld_gather(x + cb);
-      }
-      if (k < len) {
-        const int64_t a = base + (int64_t)k * C;
-        const I ca = ld_stream(col + a);
-        if (ca >= 0) s0 += ld_stream(val + a) * ld_gather(x + ca);
-      }
-      if (i < n && len >= 0) axpby_store(y + (reorder ? (int64_t)reorder[i] : i), s0 + s1, alpha, beta, bz);
-    } else {
-      const unsigned ml = __reduce_max_sync(0xffffffffu, (unsigned)(len > 0 ? len : 0));
-      int t = 1;
-      while (t < 32 && (unsigned)(t * 4) < ml) t <<= 1;
-      const int per = 32 / t, sub = lane % t;
-      for (int p = 0; p < t; ++p) {
-        const int j = p * per + lane / t;
-        const int L = __shfl_sync(0xffffffffu, len, j);
-        const int64_t b = __shfl_sync(0xffffffffu, base, j);
-        V s0 = V(0), s1 = V(0);
-        int k = sub;
-        for (; k + t < L; k += 2 * t) {
-          const I ca = ld_stream(col + b + k), cb = ld_stream(col + b + k + t);
-          if (ca >= 0) s0 += ld_stream(val + b + k) * ld_gather(x + ca);
-          if (cb >= 0) s1 += ld_stream(val + b + k + t) * ld_gather(x + cb);
-        }
-        if (k < L) {
-          const I ca = ld_stream(col + b + k);
-          if (ca >= 0) s0 += ld_stream(val + b + k) * ld_gather(x + ca);
-        }
-        const V sum = warp_sum(s0 + s1, t);
-        const int64_t row = i0 + j;
-        if (sub == 0 && row < n && L >= 0)
-          axpby_store(y + (reorder ? (int64_t)reorder[row] : row), sum, alpha, beta, bz);
-      }
-    }
-  } else {
-    const int64_t q = (int64_t)blockIdx.x - main_blocks;
-    const PadPiece pc = pieces[q];
-    const int64_t i = pc.row;
-    const int len = row_len[i];
-    const int64_t c = i / C;
-    const int64_t base = chunk_off[c] + (kColMajor ? (i - c * C) : (i - c * C) * (int64_t)chunk_len[c]);
-    const int64_t stride = kColMajor ? C : 1;
-    const int64_t k0 = (int64_t)pc.piece * kPadPiece;
-    const int64_t k1 = (k0 + kPadPiece < len) ? k0 + kPadPiece : len;
-    V sum = V(0);
-    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-      const int64_t a = base + k * stride;
-      const I ca = ld_stream(col + a);
-      if (ca >= 0) sum += ld_stream(val + a) * ld_gather(x + ca);
-    }
-    sum = block_sum(sum, red);
-    if (threadIdx.x == 0) {
-      const int64_t first = q - pc.piece;
-      partial[q] = sum;
-      __threadfence();
-      if (atomicAdd(counter + first, 1) == pc.npieces - 1) {
-        __threadfence();
-        V tot = V(0);
-        for (int t = 0; t < pc.npieces; ++t) tot += ld_cg(partial + first + t);
-        axpby_store(y + (reorder ? (int64_t)reorder[i] : i), tot, alpha, beta, bz);
-        counter[first] = 0;
-      }
-    }
-  }
+    int64_t main_warps, int64_t npieces, const PadPiece* __restrict__ pieces, V* __restrict__ partial,
+    int* __restrict__ counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (w < main_warps)
+    padded_rows32<I, V, kColMajor>(w * 32, col, val, chunk_len, chunk_off, row_len, reorder, n, C, x, y, alpha,
+                                   beta, bz, lane);
+  else if (w - main_warps < npieces)
+    padded_piece<I, V, kColMajor>(w - main_warps, pieces[w - main_warps], col, val, chunk_len, chunk_off, row_len,
+                                  reorder, C, x, y, alpha, beta, bz, partial, counter, lane);
 }
 
 // ------------------------------------------------------------------ DIA
@@ -681,19 +604,19 @@ spops_status_t padded_spmv_t(Context* ctx, Matrix* A, double alpha, const void* 
   const PaddedData& P = A->pad;
   const int64_t n = A->rows;
   if (n == 0) return SPOPS_OK;
-  const int64_t main_blocks = (n + 255) / 256;
-  const int64_t grid = main_blocks + P.npieces;
+  const int64_t main_warps = (n + 31) / 32;
+  const int64_t grid = (main_warps + P.npieces + 7) / 8;
   if (grid > INT32_MAX) return fail(SPOPS_ERR_TOO_LARGE, "padded SpMV grid");
   const I* ro = P.sorted ? P.reorder.as<I>() : nullptr;
   if (A->layout == SPOPS_COL_MAJOR)
     padded_kernel<I, V, true><<<(unsigned)grid, 256, 0, ctx->stream>>>(
         A->col.as<I>(), A->val.as<V>(), P.chunk_len.as<I>(), P.chunk_off.as<int64_t>(), P.row_len.as<int>(), ro, n,
-        P.C, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, main_blocks,
+        P.C, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, main_warps, P.npieces,
         P.piece.as<PadPiece>(), P.partial.as<V>(), P.counter.as<int>());
   else
     padded_kernel<I, V, false><<<(unsigned)grid, 256, 0, ctx->stream>>>(
         A->col.as<I>(), A->val.as<V>(), P.chunk_len.as<I>(), P.chunk_off.as<int64_t>(), P.row_len.as<int>(), ro, n,
-        P.C, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, main_blocks,
+        P.C, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, main_warps, P.npieces,
         P.piece.as<PadPiece>(), P.partial.as<V>(), P.counter.as<int>());
   SPOPS_LAUNCH_CHECK();
   return SPOPS_OK;
@@ -963,6 +886,7 @@ void Matrix::release_all() {
   dia.release();
   bsr.release();
   tr.release();
+  spmm_partial.release();
   if (csr_view) {
     csr_view->release_all();
     delete csr_view;

@@ -21,13 +21,14 @@
 
 #include "device_util.cuh"
 #include "spops_internal.h"
+#include "warp_work.cuh"
 
 namespace spops {
 namespace {
 
 constexpr int kBlock = 256;                 // 8 warps, each on its own segments
-constexpr int kCap = 256;                   // entries per long-row chunk; short segments < 2*kCap
-constexpr int kRowCap = 32;                 // rows per short segment at most
+constexpr int kCap = kCsrCap;               // entries per long-row chunk; short segments < 2*kCap
+constexpr int kRowCap = kCsrRowCap;         // rows per short segment at most
 // Kernel variants (entries per lane per load round, resident blocks per SM):
 // more items keep more bytes in flight per warp, fewer leave room for more
 // warps.  Variant 0 is the default; spops_set_option("csr_variant", v).
@@ -82,6 +83,12 @@ __global__ void plan_fill_kernel(const I* __restrict__ rp, int64_t n, const int6
   }
 }
 
+__global__ void count_long_kernel(const int* __restrict__ blk_chunk, int64_t nblocks,
+                                  unsigned long long* __restrict__ nlong) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (b < nblocks && blk_chunk[b] == 0) atomicAdd(nlong, 1ULL);
+}
+
 template <typename I>
 __global__ void plan_seg_kernel(const I* __restrict__ rp, const int64_t* __restrict__ blk_row,
                                 const int* __restrict__ blk_chunk, int64_t nblocks, CsrSeg* __restrict__ seg) {
@@ -123,78 +130,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) csr_warp_kernel(
   const int lane = threadIdx.x & 31;
   V* prod = prod_all[threadIdx.x >> 5];
   const int64_t nwarps = (int64_t)gridDim.x * (kBlock / 32);
-  for (int64_t j = blockIdx.x * (int64_t)(kBlock / 32) + (threadIdx.x >> 5); j < nseg; j += nwarps) {
-    const CsrSeg d = segs[j];
-    const int m = (int)(d.p1 - d.p0);
-    const bool is_long = d.chunk >= 0;
-    const I* cseg = ci + d.p0;
-    const V* vseg = val + d.p0;
-    V lsum = V(0);
-    for (int base = 0; base < m; base += 32 * kItems) {
-      I c[kItems];
-      V a[kItems];
-#pragma unroll
-      for (int it = 0; it < kItems; ++it) {
-        const int k = base + lane + 32 * it;
-        if (k < m) {
-          c[it] = ld_stream(cseg + k);
-          a[it] = ld_stream(vseg + k);
-        }
-      }
-#pragma unroll
-      for (int it = 0; it < kItems; ++it) {
-        const int k = base + lane + 32 * it;
-        if (k < m) {
-          const V p = a[it] * ld_gather(x + c[it]);
-          if (is_long) lsum += p; else prod[k] = p;
-        }
-      }
-    }
-    if (!is_long) {
-      __syncwarp();
-      const int nr = d.nr;
-      int t = 32 / (nr > 0 ? nr : 1);
-      t = t >= 32 ? 32 : t >= 16 ? 16 : t >= 8 ? 8 : t >= 4 ? 4 : t >= 2 ? 2 : 1;
-      const int groups = 32 / t, g = lane / t, sub = lane % t;
-      for (int rb = 0; rb < nr; rb += groups) {
-        const int rr = rb + g;
-        V s0 = V(0), s1 = V(0);
-        if (rr < nr) {
-          const int s = (int)((int64_t)rp[d.r0 + rr] - d.p0), e = (int)((int64_t)rp[d.r0 + rr + 1] - d.p0);
-          int k = s + sub;
-          for (; k + t < e; k += 2 * t) {
-            s0 += prod[k];
-            s1 += prod[k + t];
-          }
-          if (k < e) s0 += prod[k];
-        }
-        const V sum = warp_sum(s0 + s1, t);
-        if (rr < nr && sub == 0) axpby_store(y + d.r0 + rr, sum, alpha, beta, beta_zero);
-      }
-      __syncwarp();
-    } else {
-      // chunk sums of one long row, combined by the last chunk to finish
-      lsum = warp_sum(lsum);
-      const int64_t first = j - d.chunk;
-      int last = 0;
-      if (lane == 0) {
-        partial[j] = lsum;
-        __threadfence();
-        last = (atomicAdd(counter + first, 1) == d.nr - 1);
-      }
-      last = __shfl_sync(0xffffffffu, last, 0);
-      if (last) {
-        __threadfence();
-        V tot = V(0);
-        for (int q = lane; q < d.nr; q += 32) tot += ld_cg(partial + first + q);
-        tot = warp_sum(tot);
-        if (lane == 0) {
-          axpby_store(y + d.r0, tot, alpha, beta, beta_zero);
-          counter[first] = 0;
-        }
-      }
-    }
-  }
+  for (int64_t j = blockIdx.x * (int64_t)(kBlock / 32) + (threadIdx.x >> 5); j < nseg; j += nwarps)
+    csr_segment_spmv<I, V, kItems>(segs[j], j, ci, val, rp, x, y, alpha, beta, beta_zero, prod, partial, counter,
+                                   lane);
 }
 
 template <typename I>
@@ -265,7 +203,14 @@ spops_status_t analyse_t(Context* ctx, Matrix* A) {
     if (nblocks > 0) {
       plan_seg_kernel<I><<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(
           rp, P.blk_row.as<int64_t>(), P.blk_chunk.as<int>(), nblocks, P.seg.as<CsrSeg>());
+      unsigned long long* nl = reinterpret_cast<unsigned long long*>(nblk);  // scratch reuse
+      SPOPS_CUDA(cudaMemsetAsync(nl, 0, 8, st));
+      count_long_kernel<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(P.blk_chunk.as<int>(), nblocks, nl);
       SPOPS_LAUNCH_CHECK();
+      unsigned long long hl = 0;
+      SPOPS_CUDA(cudaMemcpyAsync(&hl, nl, 8, cudaMemcpyDeviceToHost, st));
+      SPOPS_CUDA(cudaStreamSynchronize(st));
+      P.nlong = (int64_t)hl;
     }
   } else {
     SPOPS_CUDA(cudaMemsetAsync(P.blk_row.p, 0, sizeof(int64_t), st));

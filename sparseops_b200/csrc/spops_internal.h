@@ -187,6 +187,7 @@ struct Matrix {
   DiaData dia;
   BsrData bsr;
   TransposeData tr;
+  DevBuf spmm_partial;  // SpMM long-row chunk sums (k per chunk)
   // COO: the same entries as a CSR matrix sorted by row (owned)
   Matrix* csr_view = nullptr;
   size_t isize() const { return itype == SPOPS_INDEX_I32 ? 4 : 8; }
@@ -209,6 +210,9 @@ spops_status_t coo_analyse(Context* ctx, Matrix* A);
 // adjoint.cu
 spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out);
+// batched.cu
+spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k, double beta,
+                        void* Y, int64_t ldy);
 spops_status_t validate_columns(Context* ctx, const void* col, int64_t count, spops_index_t it, int64_t ncols,
                                 bool allow_pad);
 

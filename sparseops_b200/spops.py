@@ -204,3 +204,69 @@ def _spmv(alpha, A: Matrix_Features, x, beta, y):
 def SpOps_csr(alpha, csr: CSR_Matrix, x, beta, y):
     """y = alpha*A*x + beta*y for a CSR matrix (reference src/spmv_csr.cpp:165)."""
     return _spmv(alpha, csr, x, beta, y)
+
+
+def SpMM_csr(alpha, csr: CSR_Matrix, X, beta, Y):
+    """Y = alpha*A*X + beta*Y for row-major X [cols x k], Y [rows x k] (CUDA
+    tensors).  No reference counterpart; equals k SpOps_csr calls."""
+    h = csr.device()
+    ctx = h.ctx.follow_torch()
+    k = X.shape[1]
+    call("spops_spmm", ctx.handle, dbl(alpha), h.handle, _ptr(X), i64(X.stride(0)), i64(k), dbl(beta), _ptr(Y),
+         i64(Y.stride(0)))
+    return Y
+
+
+class Batch:
+    """Many CSR matrices in one persistent launch (spops_batch_*).
+
+    ``X`` / ``Y`` are lists of CUDA tensors: vectors for k = 1, row-major
+    [n x k] matrices otherwise.  ``tune()`` picks the form per matrix on the
+    device; ``capture()`` records the launch in a CUDA graph that ``run()``
+    replays."""
+
+    def __init__(self, matrices, k: int = 1, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.matrices = list(matrices)
+        self.handles = [m.device(self.ctx) for m in self.matrices]
+        arr = (vp * len(self.handles))(*[h.handle for h in self.handles])
+        self.k = int(k)
+        h = vp()
+        call("spops_batch_create", self.ctx.handle, C.byref(h), i64(len(self.handles)), arr, i64(self.k))
+        self.handle = h
+        self._vecs = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                _lib.lib().spops_batch_destroy(self.handle)
+        except Exception:
+            pass
+
+    def set_vectors(self, X, Y):
+        n = len(self.handles)
+        xs = (vp * n)(*[vp(x.data_ptr()) for x in X])
+        ys = (vp * n)(*[vp(y.data_ptr()) for y in Y])
+        ldx = (C.c_int64 * n)(*[(x.stride(0) if x.dim() == 2 else 1) for x in X])
+        ldy = (C.c_int64 * n)(*[(y.stride(0) if y.dim() == 2 else 1) for y in Y])
+        call("spops_batch_set_vectors", self.handle, xs, ldx, ys, ldy)
+        self._vecs = (list(X), list(Y))
+
+    def tune(self, csr_only: bool = False):
+        self.ctx.follow_torch()
+        call("spops_batch_tune", self.ctx.handle, self.handle, C.c_int32(1 if csr_only else 0))
+
+    def run(self, alpha: float = 1.0, beta: float = 0.0):
+        self.ctx.follow_torch()
+        call("spops_batch_run", self.ctx.handle, self.handle, dbl(alpha), dbl(beta))
+
+    def capture(self, alpha: float = 1.0, beta: float = 0.0):
+        self.ctx.follow_torch()
+        call("spops_batch_capture", self.ctx.handle, self.handle, dbl(alpha), dbl(beta))
+
+    def info(self):
+        items = C.c_int64()
+        ch = (C.c_int32 * len(self.handles))()
+        kt = C.c_int32()
+        call("spops_batch_info", self.handle, C.byref(items), ch, C.byref(kt))
+        return items.value, list(ch), kt.value
