@@ -67,6 +67,7 @@ typedef enum { SPOPS_ROW_MAJOR = 0, SPOPS_COL_MAJOR = 1 } spops_layout_t;
 typedef struct spops_context_s* spops_context_t;
 typedef struct spops_matrix_s* spops_matrix_t;
 typedef struct spops_batch_s* spops_batch_t;
+typedef struct spops_pairs_s* spops_pairs_t;
 
 /* Parameters of a format conversion; zero means "reference default". */
 typedef struct {
@@ -250,6 +251,63 @@ spops_status_t spops_batch_capture(spops_context_t ctx, spops_batch_t batch, dou
 /* items: work items of the launch; choice[count]: 0 = CSR, 1..4 = SELL-C-sigma
  * candidate (sigma 256/4096 x row/col-major); rhs_tile: lanes per RHS tile. */
 spops_status_t spops_batch_info(spops_batch_t batch, int64_t* items, int32_t* choice, int32_t* rhs_tile);
+
+/* ------------------------------------------------------------ LeSpGEMM */
+/* MinHash signatures of A's rows: sig[rows x k] (device, uint64), row-major.
+ * Replaces minhash_signatures_flat (include/spgemm_MinHashLSH.h:119);
+ * bit-identical (same LCG coefficients from seed). */
+spops_status_t spops_minhash(spops_context_t ctx, spops_matrix_t A, int32_t k, uint64_t seed, void* sig);
+/* LSH candidate pairs (i < j, sorted, unique) with MinHash-estimated scores
+ * (matches / k), on the device.  Replaces lsh_candidate_pairs_vector
+ * (include/spgemm_MinHashLSH.h:777); constrain != 0: a bucket of more than
+ * 256 rows pairs each row with its next 16 only. */
+spops_status_t spops_lsh_pairs(spops_context_t ctx, spops_matrix_t A, int32_t k, int32_t bands, uint64_t seed,
+                               int32_t constrain, spops_pairs_t* pairs);
+/* Same from precomputed device signatures (lsh_candidate_pairs_from_flat_vector, :427). */
+spops_status_t spops_lsh_pairs_from_signatures(spops_context_t ctx, const void* sig, int64_t rows, int32_t k,
+                                               int32_t bands, int32_t constrain, spops_pairs_t* pairs);
+spops_status_t spops_pairs_count(spops_pairs_t pairs, int64_t* count);
+/* Device arrays of the pairs: i, j (int64) and score (double). */
+spops_status_t spops_pairs_arrays(spops_pairs_t pairs, const int64_t** i, const int64_t** j, const double** score);
+/* Copy the pairs to host arrays of spops_pairs_count elements (any may be NULL). */
+spops_status_t spops_pairs_download(spops_pairs_t pairs, int64_t* i, int64_t* j, double* score);
+spops_status_t spops_pairs_destroy(spops_pairs_t pairs);
+/* Hierarchical clustering of rows from sorted candidate pairs, on HOST arrays
+ * (sequential merge order).  Replaces hierarchical_clustering_v0_fast
+ * (include/spgemm_utility.h:742); bit-identical permutation[rows] (new row ->
+ * original row) and offsets[nclusters + 1] (caller sizes it rows + 1). */
+spops_status_t spops_hierarchical_clustering(const int64_t* row_ptr, const int64_t* col_index, int64_t rows,
+                                             const int64_t* pi, const int64_t* pj, const double* score,
+                                             int64_t npairs, int64_t cluster_size, int64_t* permutation,
+                                             int64_t* offsets, int64_t* nclusters);
+
+typedef struct {
+  int64_t flops;             /* 2 x intermediate products (get_spgemm_flop, src/spgemm.cpp:24) */
+  int64_t clusters, dense_clusters, pairs;
+  int64_t cluster_columns;   /* nnzc of the clustered A */
+  int64_t c_cluster_columns; /* nnzc of the clustered C (before dropping zeros) */
+  double minhash_ms, lsh_ms, hc_ms, cluster_ms, symbolic_ms, numeric_ms, to_csr_ms;
+} spops_spgemm_stats_t;
+
+/* C = A * B with the rows of A grouped into clusters (permutation / offsets
+ * from the clustering), cluster-wise symbolic and numeric phases on the
+ * device (hash / dense hybrid accumulator rules of kernel 3).  C is a new CSR
+ * handle in A's original row order with ascending columns; entries whose
+ * value is exactly zero are dropped as vlength_cluster2csr does.  Replaces
+ * csr_reorder_rows + csr_to_vlength_cluster + LeSpGEMM_VLength(kernel 3) +
+ * vlength_cluster2csr + inverse reorder (test/test_spgemm_hc_lsh.cpp:230-300,
+ * src/spgemm.cpp:661).  l2_budget_bytes: the dense/hash classification
+ * budget (the reference: CPU_L2CACHE_SIZE * 0.75); it only decides which
+ * clusters drop all-below-1e-12 columns.  stats may be NULL. */
+spops_status_t spops_spgemm_clustered(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B,
+                                      const int64_t* permutation, const int64_t* offsets, int64_t nclusters,
+                                      int32_t sort_output, double l2_budget_bytes, spops_matrix_t* C,
+                                      spops_spgemm_stats_t* stats);
+/* The whole LeSpGEMM pipeline: MinHash + LSH (device), clustering (host),
+ * cluster-wise SpGEMM (device). */
+spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B, int32_t k, int32_t bands,
+                                uint64_t seed, int64_t cluster_size, int32_t sort_output, double l2_budget_bytes,
+                                spops_matrix_t* C, spops_spgemm_stats_t* stats);
 
 /* ------------------------------------------------------------ adjoints */
 /* y = alpha * A^T x + beta * y for a CSR handle: x[rows], y[cols] (device).

@@ -38,6 +38,15 @@ class MatrixInfo(C.Structure):
                 ("extra", i64 * 8)]
 
 
+class SpgemmStats(C.Structure):
+    _fields_ = [("flops", i64), ("clusters", i64), ("dense_clusters", i64), ("pairs", i64),
+                ("cluster_columns", i64), ("c_cluster_columns", i64), ("minhash_ms", dbl), ("lsh_ms", dbl),
+                ("hc_ms", dbl), ("cluster_ms", dbl), ("symbolic_ms", dbl), ("numeric_ms", dbl), ("to_csr_ms", dbl)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class FormatParams(C.Structure):
     _fields_ = [("sigma", i64), ("chunk", i64), ("alignment", i64), ("max_diags", i64), ("block_rows", i64),
                 ("block_cols", i64), ("layout", i32), ("reserved", i32)]
@@ -76,6 +85,16 @@ _SIGS = {
     "spops_batch_run": [vp, vp, dbl, dbl],
     "spops_batch_capture": [vp, vp, dbl, dbl],
     "spops_batch_info": [vp, vp, vp, vp],
+    "spops_minhash": [vp, vp, i32, u64, vp],
+    "spops_lsh_pairs": [vp, vp, i32, i32, u64, i32, vp],
+    "spops_lsh_pairs_from_signatures": [vp, vp, i64, i32, i32, i32, vp],
+    "spops_pairs_count": [vp, vp],
+    "spops_pairs_arrays": [vp, vp, vp, vp],
+    "spops_pairs_download": [vp, vp, vp, vp],
+    "spops_pairs_destroy": [vp],
+    "spops_hierarchical_clustering": [vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp],
+    "spops_spgemm_clustered": [vp, vp, vp, vp, vp, i64, i32, dbl, vp, vp],
+    "spops_spgemm_lsh": [vp, vp, vp, i32, i32, u64, i64, i32, dbl, vp, vp],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
     "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
 }

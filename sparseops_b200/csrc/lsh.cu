@@ -1,0 +1,264 @@
+// MinHash signatures and LSH candidate pairs on the device.
+//
+// Replaces minhash_signatures_flat (reference include/spgemm_MinHashLSH.h:119-180)
+// and lsh_candidate_pairs_from_flat_vector (427-605), which
+// lsh_candidate_pairs_vector (777-791) chains.  Outputs are bit-identical:
+//   signatures  sig[r][d] = min over the row's columns c of a_d*c + b_d
+//               (mod 2^64), a_d, b_d from the reference's LCG (40-43,
+//               134-141); empty rows keep UINT64_MAX.  One warp per row, the
+//               row's columns broadcast, each lane owning k/32 hash functions.
+//   records     bucket = band hash of the band's r = k/bands values
+//               (h = h*0x9e3779b97f4a7c15 + v, 277-283), per band a stable
+//               radix sort of (bucket -> row) over rows given in ascending
+//               order, i.e. the reference's (band, bucket, row) order.
+//   pairs       each run of equal buckets (size >= 2) pairs every row with
+//               every later row, or -- when constrained and the run is longer
+//               than 256 -- with its next 16 rows (481-516); pairs (i < j)
+//               from all bands are sorted and deduplicated (544-545).
+//   scores      matches / k over the two signatures (183-204), one warp per
+//               pair.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "spops_internal.h"
+
+namespace spops {
+namespace {
+
+inline unsigned grid_for(int64_t work, int threads = 256) {
+  int64_t g = (work + threads - 1) / threads;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+template <typename I>
+__global__ void minhash_kernel(const I* __restrict__ rp, const I* __restrict__ ci, int64_t n, int k,
+                               const uint64_t* __restrict__ a, const uint64_t* __restrict__ b,
+                               uint64_t* __restrict__ sig) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t s = rp[r], e = rp[r + 1];
+  for (int d0 = 0; d0 < k; d0 += 64) {  // two hash functions per lane per pass
+    const int d1 = d0 + lane, d2 = d0 + 32 + lane;
+    const uint64_t a1 = d1 < k ? a[d1] : 0, b1 = d1 < k ? b[d1] : 0;
+    const uint64_t a2 = d2 < k ? a[d2] : 0, b2 = d2 < k ? b[d2] : 0;
+    uint64_t m1 = ~0ULL, m2 = ~0ULL;
+    for (int64_t t = s; t < e; ++t) {
+      const uint64_t x = (uint64_t)(int64_t)ci[t];
+      const uint64_t h1 = a1 * x + b1, h2 = a2 * x + b2;
+      m1 = h1 < m1 ? h1 : m1;
+      m2 = h2 < m2 ? h2 : m2;
+    }
+    if (d1 < k) sig[r * k + d1] = m1;
+    if (d2 < k) sig[r * k + d2] = m2;
+  }
+}
+
+__global__ void band_hash_kernel(const uint64_t* __restrict__ sig, int64_t n, int k, int band, int r,
+                                 uint64_t* __restrict__ bucket, int32_t* __restrict__ rows) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t* s = sig + i * k + band * r;
+  uint64_t h = 0;
+  for (int t = 0; t < r; ++t) h = h * 0x9e3779b97f4a7c15ULL + s[t];
+  bucket[i] = h;
+  rows[i] = (int32_t)i;
+}
+
+__global__ void run_flag_kernel(const uint64_t* __restrict__ key, int64_t n, int64_t* __restrict__ flag) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = (i == 0 || key[i] != key[i - 1]) ? 1 : 0;
+}
+
+// Per sorted record: pairs it starts (with later rows of its run).
+__global__ void pair_count_kernel(const int64_t* __restrict__ gid, const int64_t* __restrict__ run_off,
+                                  const int64_t* __restrict__ run_len, int64_t n, bool constrain,
+                                  int64_t* __restrict__ cnt) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t g = gid[i] - 1;
+  const int64_t size = run_len[g];
+  int64_t c = run_off[g] + size - 1 - i;  // later rows in the run
+  if (constrain && size > 256 && c > 16) c = 16;
+  cnt[i] = size >= 2 ? c : 0;
+}
+
+__global__ void pair_emit_kernel(const int32_t* __restrict__ rows, int64_t n, const int64_t* __restrict__ cnt,
+                                 const int64_t* __restrict__ off, uint64_t* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t c = cnt[i], o = off[i];
+  const uint64_t ri = (uint64_t)(uint32_t)rows[i];
+  for (int64_t t = 0; t < c; ++t) out[o + t] = (ri << 32) | (uint64_t)(uint32_t)rows[i + 1 + t];
+}
+
+__global__ void score_kernel(const uint64_t* __restrict__ sig, int k, const uint64_t* __restrict__ pairs,
+                             int64_t np, int64_t* __restrict__ pi, int64_t* __restrict__ pj,
+                             double* __restrict__ score) {
+  const int64_t p = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (p >= np) return;
+  const uint64_t key = pairs[p];
+  const int64_t i = (int64_t)(key >> 32), j = (int64_t)(key & 0xffffffffULL);
+  int m = 0;
+  for (int d = lane; d < k; d += 32) m += (sig[i * k + d] == sig[j * k + d]) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) m += __shfl_down_sync(0xffffffffu, m, o);
+  if (lane == 0) {
+    pi[p] = i;
+    pj[p] = j;
+    score[p] = (double)m / (double)k;
+  }
+}
+
+template <typename I>
+spops_status_t minhash_t(Context* ctx, Matrix* A, int k, uint64_t seed, uint64_t* sig) {
+  std::vector<uint64_t> ha((size_t)k), hb((size_t)k);
+  uint64_t s = seed;
+  for (int d = 0; d < k; ++d) {  // the reference's LCG (spgemm_MinHashLSH.h:40-43, 134-141)
+    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+    ha[d] = (s >> 1) * 2 + 1;
+    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+    hb[d] = s;
+  }
+  SPOPS_TRY(ctx->scratch_reserve(2 * (size_t)k * 8 + 512));
+  uint64_t* da = ctx->scratch.as<uint64_t>();
+  uint64_t* db = da + k;
+  SPOPS_CUDA(cudaMemcpyAsync(da, ha.data(), (size_t)k * 8, cudaMemcpyHostToDevice, ctx->stream));
+  SPOPS_CUDA(cudaMemcpyAsync(db, hb.data(), (size_t)k * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (A->rows > 0)
+    minhash_kernel<I><<<grid_for(A->rows * 32), 256, 0, ctx->stream>>>(A->row.as<I>(), A->col.as<I>(), A->rows, k, da,
+                                                                       db, sig);
+  SPOPS_LAUNCH_CHECK();
+  SPOPS_CUDA(cudaStreamSynchronize(ctx->stream));  // da/db live in scratch
+  return SPOPS_OK;
+}
+
+}  // namespace
+
+spops_status_t minhash_signatures(Context* ctx, Matrix* A, int k, uint64_t seed, uint64_t* sig) {
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "MinHash needs a CSR matrix");
+  if (k <= 0) return fail(SPOPS_ERR_INVALID, "MinHash: k must be positive");
+  if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));  // validates the pattern
+  return A->itype == SPOPS_INDEX_I32 ? minhash_t<int32_t>(ctx, A, k, seed, sig)
+                                     : minhash_t<int64_t>(ctx, A, k, seed, sig);
+}
+
+spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, int bands, bool constrain,
+                         PairSet* out) {
+  out->release();
+  if (n <= 0 || bands <= 0 || k <= 0 || k % bands) return SPOPS_OK;  // the reference returns no pairs
+  if (n > INT32_MAX) return fail(SPOPS_ERR_UNSUPPORTED, "LSH: more than 2^31 rows");
+  const int r = k / bands;
+  cudaStream_t st = ctx->stream;
+  const size_t nn = (size_t)n;
+  size_t cub_sort = 0, cub_scan = 0, cub_rle = 0;
+  {
+    uint64_t* kk = nullptr;
+    int32_t* vv = nullptr;
+    int64_t* cc = nullptr;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort, kk, kk, vv, vv, (int64_t)n, 0, 64, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, cc, cc, (int64_t)n, st));
+    SPOPS_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, cub_rle, kk, kk, cc, cc, (int64_t)n, st));
+    size_t inc = 0;
+    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, inc, cc, cc, (int64_t)n, st));
+    cub_scan = std::max(cub_scan, inc);
+  }
+  const size_t cub_max = std::max({cub_sort, cub_scan, cub_rle});
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t need = al(nn * 8) * 2 + al(nn * 4) * 2 + al(nn * 8) * 7 + cub_max + 512;
+  SPOPS_TRY(ctx->scratch_reserve(need));
+  char* base = ctx->scratch.as<char>();
+  size_t o = 0;
+  auto take = [&](size_t b) { char* p = base + o; o += al(b); return p; };
+  uint64_t* key_in = reinterpret_cast<uint64_t*>(take(nn * 8));
+  uint64_t* key_out = reinterpret_cast<uint64_t*>(take(nn * 8));
+  int32_t* row_in = reinterpret_cast<int32_t*>(take(nn * 4));
+  int32_t* row_out = reinterpret_cast<int32_t*>(take(nn * 4));
+  int64_t* flag = reinterpret_cast<int64_t*>(take(nn * 8));
+  int64_t* gid = reinterpret_cast<int64_t*>(take(nn * 8));
+  uint64_t* ukeys = reinterpret_cast<uint64_t*>(take(nn * 8));
+  int64_t* run_len = reinterpret_cast<int64_t*>(take(nn * 8));
+  int64_t* run_off = reinterpret_cast<int64_t*>(take(nn * 8));
+  int64_t* cnt = reinterpret_cast<int64_t*>(take(nn * 8));
+  int64_t* off = reinterpret_cast<int64_t*>(take(nn * 8));
+  int64_t* nruns = reinterpret_cast<int64_t*>(take(8));
+  void* cub_tmp = take(cub_max);
+
+  // pairs of every band, appended
+  DevBuf all;
+  int64_t total = 0, cap = 0;
+  for (int band = 0; band < bands; ++band) {
+    band_hash_kernel<<<grid_for(n), 256, 0, st>>>(sig, n, k, band, r, key_in, row_in);
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_sort, key_in, key_out, row_in, row_out, n, 0, 64, st));
+    run_flag_kernel<<<grid_for(n), 256, 0, st>>>(key_out, n, flag);
+    SPOPS_LAUNCH_CHECK();
+    size_t inc_bytes = cub_max;
+    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, inc_bytes, flag, gid, n, st));
+    SPOPS_CUDA(cub::DeviceRunLengthEncode::Encode(cub_tmp, cub_rle, key_out, ukeys, run_len, nruns, n, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, run_len, run_off, n, st));
+    pair_count_kernel<<<grid_for(n), 256, 0, st>>>(gid, run_off, run_len, n, constrain, cnt);
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, cnt, off, n, st));
+    int64_t h[2];
+    SPOPS_CUDA(cudaMemcpyAsync(&h[0], off + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&h[1], cnt + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    const int64_t np = h[0] + h[1];
+    if (np == 0) continue;
+    if (total + np > cap) {  // grow the pair buffer
+      DevBuf bigger;
+      const int64_t ncap = std::max<int64_t>(2 * cap, total + np);
+      SPOPS_TRY(bigger.alloc((size_t)ncap * 8));
+      if (total) SPOPS_CUDA(cudaMemcpyAsync(bigger.p, all.p, (size_t)total * 8, cudaMemcpyDeviceToDevice, st));
+      SPOPS_CUDA(cudaStreamSynchronize(st));
+      all.release();
+      all = bigger;
+      bigger.p = nullptr;
+      bigger.own = false;
+      cap = ncap;
+    }
+    pair_emit_kernel<<<grid_for(n), 256, 0, st>>>(row_out, n, cnt, off, all.as<uint64_t>() + total);
+    SPOPS_LAUNCH_CHECK();
+    total += np;
+  }
+  if (total == 0) {
+    all.release();
+    return SPOPS_OK;
+  }
+  // sort + unique all pairs
+  size_t cub2 = 0, cub3 = 0;
+  int64_t* nsel = nullptr;
+  {
+    uint64_t* kk = nullptr;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, cub2, kk, kk, total, 0, 64, st));
+    SPOPS_CUDA(cub::DeviceSelect::Unique(nullptr, cub3, kk, kk, nsel, total, st));
+  }
+  DevBuf sorted, uniq, tmp;
+  SPOPS_TRY(sorted.alloc((size_t)total * 8));
+  SPOPS_TRY(uniq.alloc((size_t)total * 8));
+  SPOPS_TRY(tmp.alloc(std::max(cub2, cub3) + 256));
+  nsel = reinterpret_cast<int64_t*>(tmp.as<char>() + std::max(cub2, cub3));
+  SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, cub2, all.as<uint64_t>(), sorted.as<uint64_t>(), total, 0, 64, st));
+  SPOPS_CUDA(cub::DeviceSelect::Unique(tmp.p, cub3, sorted.as<uint64_t>(), uniq.as<uint64_t>(), nsel, total, st));
+  int64_t nu = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  all.release();
+  sorted.release();
+  tmp.release();
+  SPOPS_TRY(out->pi.alloc((size_t)nu * 8));
+  SPOPS_TRY(out->pj.alloc((size_t)nu * 8));
+  SPOPS_TRY(out->score.alloc((size_t)nu * 8));
+  score_kernel<<<grid_for(nu * 32), 256, 0, st>>>(sig, k, uniq.as<uint64_t>(), nu, out->pi.as<int64_t>(),
+                                                  out->pj.as<int64_t>(), out->score.as<double>());
+  SPOPS_LAUNCH_CHECK();
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  uniq.release();
+  out->count = nu;
+  return SPOPS_OK;
+}
+
+}  // namespace spops

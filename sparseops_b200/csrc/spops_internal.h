@@ -195,6 +195,18 @@ struct Matrix {
   void release_all();
 };
 
+// LSH candidate pairs (device arrays, sorted by (i, j), unique)
+struct PairSet {
+  int64_t count = 0;
+  DevBuf pi, pj, score;  // int64, int64, double
+  void release() { pi.release(); pj.release(); score.release(); count = 0; }
+};
+
+struct SpgemmStats {
+  int64_t flops = 0, clusters = 0, dense_clusters = 0, pairs = 0, cluster_columns = 0, c_cluster_columns = 0;
+  double minhash_ms = 0, lsh_ms = 0, hc_ms = 0, cluster_ms = 0, symbolic_ms = 0, numeric_ms = 0, to_csr_ms = 0;
+};
+
 // ------------------------------------------------------------ kernels API
 spops_status_t csr_analyse(Context* ctx, Matrix* A);
 spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
@@ -210,6 +222,15 @@ spops_status_t coo_analyse(Context* ctx, Matrix* A);
 // adjoint.cu
 spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out);
+// lsh.cu, hc.cpp, spgemm.cu
+spops_status_t minhash_signatures(Context* ctx, Matrix* A, int k, uint64_t seed, uint64_t* sig);
+spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, int bands, bool constrain,
+                         PairSet* out);
+spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int64_t n, const int64_t* pi,
+                                       const int64_t* pj, const double* ps, int64_t np, int64_t cluster_size,
+                                       std::vector<int64_t>& perm, std::vector<int64_t>& offsets);
+spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
+                              int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st);
 // batched.cu
 spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k, double beta,
                         void* Y, int64_t ldy);

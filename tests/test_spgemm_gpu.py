@@ -1,0 +1,140 @@
+"""LeSpGEMM on the device: MinHash, LSH pairs, clustering, cluster-wise C = A*A^T.
+
+Integer outputs (signatures, pairs, permutation, offsets, C row_ptr / col_idx)
+bit-exact against the reference's golden outputs or the pinned oracle; C
+values within 1e-12 of sum_k |a_ik b_kj| (componentwise).
+"""
+import numpy as np
+import pytest
+
+from sparseops_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _csr(rp, ci, v, ncols=None):
+    import torch
+    from sparseops_b200 import CSR_Matrix
+    n = len(rp) - 1
+    d = torch.device("cuda")
+    return CSR_Matrix(n, n if ncols is None else ncols, torch.from_numpy(rp).to(d), torch.from_numpy(ci).to(d),
+                      torch.from_numpy(v).to(d))
+
+
+def _check_c(C, ref):
+    rp, ci, v = C.host()
+    assert np.array_equal(rp.astype(np.int64), ref["rp"])
+    assert np.array_equal(ci.astype(np.int64), ref["ci"])
+    err = np.abs(v - ref["v"]) / np.maximum(ref["absv"], 1e-300)
+    assert (err.max() if len(err) else 0.0) <= 1e-12
+
+
+def test_minhash_and_pairs_golden(cuda, golden):
+    from sparseops_b200.spgemm import lsh_candidate_pairs_vector, minhash_signatures_flat
+    g = golden
+    A = _csr(g["sp_arp"], g["sp_aci"], g["sp_av"])
+    assert np.array_equal(minhash_signatures_flat(A, 64, 7), g["sp_sig"])
+    i, j, s = lsh_candidate_pairs_vector(A, 64, 16, 7).host()
+    assert np.array_equal(i, g["sp_pi"]) and np.array_equal(j, g["sp_pj"]) and np.array_equal(s, g["sp_ps"])
+
+
+def test_lsh_window_rule_golden(cuda, golden):
+    from sparseops_b200.spgemm import lsh_candidate_pairs_vector
+    rp = np.arange(0, 401 * 3, 3, dtype=np.int64)
+    ci = np.tile(np.array([5, 17, 99], np.int64), 400)
+    A = _csr(rp, ci, np.ones(len(ci)), ncols=100)
+    i, j, s = lsh_candidate_pairs_vector(A, 64, 16, 7).host()
+    assert np.array_equal(i, golden["big_pi"]) and np.array_equal(j, golden["big_pj"])
+    assert np.array_equal(s, golden["big_ps"])
+
+
+@pytest.mark.parametrize("so", [0, 1])
+def test_spgemm_clustered_golden(cuda, golden, orc, so):
+    from sparseops_b200.spgemm import LeSpGEMM_clustered
+    g = golden
+    arp, aci, av = g["sp_arp"], g["sp_aci"], g["sp_av"]
+    brp, bci, bv = synth.transpose(arp, aci, av, 1024)
+    C = LeSpGEMM_clustered(_csr(arp, aci, av), _csr(brp, bci, bv), g["sp_perm"], g["sp_offsets"], sort_output=bool(so))
+    ref = orc.spgemm((arp, aci, av), (brp, bci, bv), g["sp_perm"], g["sp_offsets"], sort_output=bool(so))
+    assert np.array_equal(C.host()[0].astype(np.int64), g[f"sp_c{so}_rp"])
+    assert np.array_equal(C.host()[1].astype(np.int64), g[f"sp_c{so}_ci"])
+    _check_c(C, ref)
+    assert C.stats["dense_clusters"] == int(g[f"sp_c{so}_dense"])
+
+
+@pytest.mark.parametrize("n,ncomm", [(16384, 64), (131072, 512)])
+def test_pipeline_vs_oracle(cuda, orc, n, ncomm):
+    """MinHash -> LSH -> clustering -> SpGEMM, every stage against the oracle."""
+    from sparseops_b200.spgemm import (LeSpGEMM_clustered, LeSpGEMM_lsh, hierarchical_clustering_v0_fast,
+                                       lsh_candidate_pairs_vector, minhash_signatures_flat)
+    arp, aci, av = synth.planted_communities(n, ncomm=ncomm, mean=20.0, seed=17)
+    brp, bci, bv = synth.transpose(arp, aci, av, n)
+    A, B = _csr(arp, aci, av), _csr(brp, bci, bv)
+    sig = minhash_signatures_flat(A, 64, 7)
+    assert np.array_equal(sig, orc.minhash(arp, aci, 64, 7))
+    pairs = lsh_candidate_pairs_vector(A, 64, 16, 7).host()
+    opi, opj, ops = orc.lsh_pairs(sig, 16, True)
+    assert np.array_equal(pairs[0], opi) and np.array_equal(pairs[1], opj) and np.array_equal(pairs[2], ops)
+    perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
+    operm, ooffs = orc.hc(arp, aci, opi, opj, ops, 8)
+    assert np.array_equal(perm, operm) and np.array_equal(offs, ooffs)
+    ref = orc.spgemm((arp, aci, av), (brp, bci, bv), perm, offs)
+    _check_c(LeSpGEMM_clustered(A, B, perm, offs), ref)
+    C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
+    _check_c(C, ref)
+    assert C.stats["flops"] == orc.spgemm_flop((arp, aci), (brp,))
+
+
+def test_int32_and_float32(cuda, orc):
+    from sparseops_b200.spgemm import LeSpGEMM_lsh
+    arp, aci, av = synth.planted_communities(8192, ncomm=32, mean=12.0, seed=19)
+    brp, bci, bv = synth.transpose(arp, aci, av, 8192)
+    C = LeSpGEMM_lsh(_csr(arp.astype(np.int32), aci.astype(np.int32), av),
+                     _csr(brp.astype(np.int32), bci.astype(np.int32), bv), 64, 16, 7, 8)
+    C64 = LeSpGEMM_lsh(_csr(arp, aci, av), _csr(brp, bci, bv), 64, 16, 7, 8)
+    assert np.array_equal(C.host()[0], C64.host()[0]) and np.array_equal(C.host()[1], C64.host()[1])
+    assert np.array_equal(C.host()[2], C64.host()[2])
+    C32 = LeSpGEMM_lsh(_csr(arp, aci, av.astype(np.float32)), _csr(brp, bci, bv.astype(np.float32)), 64, 16, 7, 8)
+    assert np.array_equal(C32.host()[0], C64.host()[0])
+    rel = np.abs(C32.host()[2] - C64.host()[2]) / (np.abs(C64.host()[2]) + 1e-3)
+    assert rel.max() < 1e-3
+
+
+def test_full_config_properties(cuda):
+    """Config size (524,288 rows, 2,048 communities): C = A*A^T must be
+    symmetric, and C*1 = A*(A^T*1) (linearity), checked with the SpMV kernels."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, SpOps_csr
+    from sparseops_b200.spgemm import LeSpGEMM_lsh
+    n = 524288
+    arp, aci, av = synth.planted_communities(n, ncomm=2048, mean=20.0, seed=5)
+    brp, bci, bv = synth.transpose(arp, aci, av, n)
+    A, B = _csr(arp, aci, av), _csr(brp, bci, bv)
+    C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
+    rp, ci, v = C.host()
+    assert C.stats["flops"] > 0 and rp[-1] == len(ci)
+    # symmetry on 2,000 random rows: every (i, j, v) has its (j, i, v)
+    rng = np.random.default_rng(1)
+    for i in rng.integers(0, n, 2000):
+        for t in range(rp[i], rp[i + 1]):
+            j = ci[t]
+            q = rp[j] + np.searchsorted(ci[rp[j]:rp[j + 1]], i)
+            assert q < rp[j + 1] and ci[q] == i
+            assert abs(v[q] - v[t]) <= 1e-12 * (1 + abs(v[t]) + np.abs(v[rp[i]:rp[i + 1]]).max())
+    # linearity: C*1 vs A*(B*1)
+    d = torch.device("cuda")
+    ones = torch.ones(n, dtype=torch.float64, device=d)
+    t, y1, y2 = (torch.zeros(n, dtype=torch.float64, device=d) for _ in range(3))
+    SpOps_csr(1.0, B, ones, 0.0, t)
+    SpOps_csr(1.0, A, t, 0.0, y1)
+    Cd = CSR_Matrix(n, n, torch.from_numpy(rp).to(d), torch.from_numpy(ci).to(d), torch.from_numpy(v).to(d))
+    SpOps_csr(1.0, Cd, ones, 0.0, y2)
+    torch.cuda.synchronize()
+    scale = torch.zeros(n, dtype=torch.float64, device=d)
+    Ad = CSR_Matrix(n, n, torch.from_numpy(arp).to(d), torch.from_numpy(aci).to(d), torch.from_numpy(np.abs(av)).to(d))
+    Bd = CSR_Matrix(n, n, torch.from_numpy(brp).to(d), torch.from_numpy(bci).to(d), torch.from_numpy(np.abs(bv)).to(d))
+    tt = torch.zeros(n, dtype=torch.float64, device=d)
+    SpOps_csr(1.0, Bd, ones, 0.0, tt)
+    SpOps_csr(1.0, Ad, tt, 0.0, scale)
+    torch.cuda.synchronize()
+    assert float(((y1 - y2).abs() / (scale + 1e-300)).max()) <= 1e-12
