@@ -151,6 +151,9 @@ spops_status_t spops_csr_set_values(spops_matrix_t A, const void* values);
  *   DIA           csr_to_dia           include/sparse_conversion.h:619
  *   BSR           csr_to_bsr           include/sparse_conversion.h:776
  *   COO           csr_to_coo           include/sparse_conversion.h:152
+ *   CSR5          csr_to_csr5          include/sparse_conversion.h:946 (device
+ *                 tiles of 32 lanes x 16 entries; tile arrays differ from the
+ *                 reference's CPU-SIMD tiles, SpMV results agree)
  * params may be NULL (reference defaults).  Errors the reference reports by
  * exit() come back as status codes: sigma not a multiple of C ->
  * SPOPS_ERR_INVALID; more than max_diags diagonals, or padded storage that
@@ -193,7 +196,9 @@ typedef enum {
   SPOPS_ARR_ROW_LEN = 6,       /* int32 slots up to each stored row's last entry */
   SPOPS_ARR_DIAG_OFFSETS = 7,  /* int64 DIA diag_offsets */
   SPOPS_ARR_BLOCK_ROW_PTR = 8, /* BSR row_ptr */
-  SPOPS_ARR_BLOCK_COL = 9      /* BSR block_colindex */
+  SPOPS_ARR_BLOCK_COL = 9,     /* BSR block_colindex */
+  SPOPS_ARR_TILE_PTR = 10,     /* CSR5 tile_ptr (uint32, bit 31: tile spans an empty row) */
+  SPOPS_ARR_TILE_DESC = 11     /* CSR5 per-lane row-start flags (uint32, tiles x 32) */
 } spops_array_t;
 /* Device pointer, element count and element size of one array (no copy). */
 spops_status_t spops_matrix_array(spops_matrix_t A, spops_array_t which, const void** dev_ptr, int64_t* count,

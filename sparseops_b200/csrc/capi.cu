@@ -286,6 +286,8 @@ spops_status_t spops_matrix_array(spops_matrix_t A, spops_array_t which, const v
     case SPOPS_ARR_DIAG_OFFSETS: p = A->dia.offsets.p; eb = 8; n = A->dia.ndiag; break;
     case SPOPS_ARR_BLOCK_ROW_PTR: p = A->bsr.row_ptr.p; eb = is; n = A->bsr.row_ptr.p ? A->bsr.mb + 1 : 0; break;
     case SPOPS_ARR_BLOCK_COL: p = A->bsr.bcol.p; eb = is; n = A->bsr.nnzb; break;
+    case SPOPS_ARR_TILE_PTR: p = A->csr5.tile_ptr.p; eb = 4; n = A->csr5.tile_ptr.p ? A->csr5.tiles + 1 : 0; break;
+    case SPOPS_ARR_TILE_DESC: p = A->csr5.desc.p; eb = 4; n = A->csr5.tiles * 32; break;
     default: return fail(SPOPS_ERR_INVALID, "spops_matrix_array: unknown array %d", (int)which);
   }
   if (n > 0 && !p) return fail(SPOPS_ERR_INVALID, "spops_matrix_array: array %d not present", (int)which);
@@ -352,6 +354,9 @@ spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info) {
       info->extra[0] = A->bsr.mb; info->extra[1] = A->bsr.nb; info->extra[2] = A->bsr.nnzb;
       info->extra[3] = A->bsr.br; info->extra[4] = A->bsr.bc;
       break;
+    case SPOPS_FMT_CSR5:
+      info->extra[0] = A->csr5.tiles; info->extra[1] = 32; info->extra[2] = 16; info->extra[3] = A->csr5.nempty;
+      break;
     default: break;
   }
   return SPOPS_OK;
@@ -409,6 +414,9 @@ spops_status_t spops_matrix_device_bytes(spops_matrix_t A, int64_t* bytes) {
        own(D.counter);
   b += own(A->dia.offsets) + own(A->dia.data) + own(A->bsr.row_ptr) + own(A->bsr.bcol) + own(A->bsr.data);
   b += own(A->tr.rp) + own(A->tr.ri) + own(A->tr.perm) + own(A->tr.val);
+  const Csr5Data& F = A->csr5;
+  b += own(F.tcol) + own(F.tval) + own(F.desc) + own(F.lane_row) + own(F.tile_ptr) + own(F.carry_in) +
+       own(F.open_sum) + own(F.open_row) + own(F.empty);
   if (A->tr.view) {
     const CsrPlan& Q = A->tr.view->plan;
     b += own(Q.blk_row) + own(Q.blk_chunk) + own(Q.partial) + own(Q.counter) + own(Q.seg);
@@ -437,6 +445,7 @@ spops_status_t spops_spmv(spops_context_t ctx, double alpha, spops_matrix_t A, c
     case SPOPS_FMT_ELL: return padded_spmv(ctx, A, alpha, x, beta, y);
     case SPOPS_FMT_DIA: return dia_spmv(ctx, A, alpha, x, beta, y);
     case SPOPS_FMT_BSR: return bsr_spmv(ctx, A, alpha, x, beta, y);
+    case SPOPS_FMT_CSR5: return csr5_spmv(ctx, A, alpha, x, beta, y);
     default: return fail(SPOPS_ERR_UNSUPPORTED, "SpMV for format %d", (int)A->format);
   }
 }

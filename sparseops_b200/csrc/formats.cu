@@ -866,6 +866,7 @@ spops_status_t convert_t(Context* ctx, Matrix* A, spops_format_t fmt, const spop
     case SPOPS_FMT_DIA: return to_dia<I, V>(ctx, A, p, M);
     case SPOPS_FMT_BSR: return to_bsr<I, V>(ctx, A, p, M);
     case SPOPS_FMT_COO: return to_coo<I, V>(ctx, A, M);
+    case SPOPS_FMT_CSR5: return csr5_build(ctx, A, M);
     default: return fail(SPOPS_ERR_UNSUPPORTED, "conversion CSR -> format %d", (int)fmt);
   }
 }
@@ -886,6 +887,7 @@ void Matrix::release_all() {
   dia.release();
   bsr.release();
   tr.release();
+  csr5.release();
   spmm_partial.release();
   if (csr_view) {
     csr_view->release_all();

@@ -239,8 +239,9 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   DevBuf sorted, uniq, tmp;
   SPOPS_TRY(sorted.alloc((size_t)total * 8));
   SPOPS_TRY(uniq.alloc((size_t)total * 8));
-  SPOPS_TRY(tmp.alloc(std::max(cub2, cub3) + 256));
-  nsel = reinterpret_cast<int64_t*>(tmp.as<char>() + std::max(cub2, cub3));
+  const size_t nsel_off = (std::max(cub2, cub3) + 255) & ~(size_t)255;  // 8-byte aligned count slot
+  SPOPS_TRY(tmp.alloc(nsel_off + 256));
+  nsel = reinterpret_cast<int64_t*>(tmp.as<char>() + nsel_off);
   SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, cub2, all.as<uint64_t>(), sorted.as<uint64_t>(), total, 0, 64, st));
   SPOPS_CUDA(cub::DeviceSelect::Unique(tmp.p, cub3, sorted.as<uint64_t>(), uniq.as<uint64_t>(), nsel, total, st));
   int64_t nu = 0;

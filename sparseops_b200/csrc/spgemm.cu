@@ -169,6 +169,20 @@ __global__ void cluster_flops_kernel(const int64_t* __restrict__ cptr, const int
   if (lane == 0) flops[c] = f;
 }
 
+// get_spgemm_flop (src/spgemm.cpp:24-42): 2 x sum over A's entries of nnz(B row)
+template <typename I>
+__global__ void product_count_kernel(const I* __restrict__ aci, int64_t nnz, const I* __restrict__ brp, int64_t brows,
+                                     unsigned long long* __restrict__ out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long s = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    const int64_t c = aci[k];
+    if (c < brows) s += (unsigned long long)((int64_t)brp[c + 1] - (int64_t)brp[c]);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
 // ------------------------------------------------------------ symbolic
 // Block per cluster; table of tsize slots in shared memory, or at
 // gtab + goff[b] in global memory when gtab != nullptr.
@@ -508,7 +522,19 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   std::vector<int64_t> hflops;
   SPOPS_TRY(d2h(st, hflops, flops.p, (size_t)ncl));
   int64_t total_products = 0;
-  for (int64_t f : hflops) total_products += f;
+  {
+    DevBuf pc;
+    SPOPS_TRY(pc.alloc(8));
+    SPOPS_CUDA(cudaMemsetAsync(pc.p, 0, 8, st));
+    if (nnz > 0) {
+      product_count_kernel<I><<<std::min<unsigned>(grid_for(nnz), 4096u), 256, 0, st>>>(
+          A->col.as<I>(), nnz, B->row.as<I>(), B->rows, reinterpret_cast<unsigned long long*>(pc.p));
+      SPOPS_LAUNCH_CHECK();
+    }
+    SPOPS_CUDA(cudaMemcpyAsync(&total_products, pc.p, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    pc.release();
+  }
   const int64_t bcols = B->cols;
   // symbolic: table >= 2 * min(flops, cols) slots
   struct Bin {

@@ -159,6 +159,18 @@ struct BsrData {
   void release() { row_ptr.release(); bcol.release(); data.release(); }
 };
 
+// CSR5 tiles of 32 lanes x 16 entries (csr5.cu).
+struct Csr5Data {
+  int64_t tiles = 0, nempty = 0;
+  DevBuf tcol, tval;   // I, V [tiles * 512], transposed within tiles
+  DevBuf desc;         // uint32 [tiles * 32] row-start flags per lane
+  DevBuf lane_row;     // int64 [tiles * 32] row of each lane's first entry
+  DevBuf tile_ptr;     // uint32 [tiles + 1]
+  DevBuf carry_in, open_sum, open_row;  // calibrator: V, V, int64 [tiles]
+  DevBuf empty;        // int64 [nempty] empty rows
+  void release();
+};
+
 // Transpose of a CSR pattern (A^T as CSR), built once per pattern; values
 // refreshed through perm after A's values change (adjoint.cu).
 struct Matrix;
@@ -187,6 +199,7 @@ struct Matrix {
   DiaData dia;
   BsrData bsr;
   TransposeData tr;
+  Csr5Data csr5;
   DevBuf spmm_partial;  // SpMM long-row chunk sums (k per chunk)
   // COO: the same entries as a CSR matrix sorted by row (owned)
   Matrix* csr_view = nullptr;
@@ -219,6 +232,9 @@ spops_status_t padded_spmv(Context* ctx, Matrix* A, double alpha, const void* x,
 spops_status_t dia_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t bsr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t coo_analyse(Context* ctx, Matrix* A);
+// csr5.cu
+spops_status_t csr5_build(Context* ctx, Matrix* A, Matrix* M);
+spops_status_t csr5_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 // adjoint.cu
 spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out);

@@ -37,7 +37,7 @@ SIMD_WIDTH = 256
 RowMajor, ColMajor = 0, 1
 
 _ARR = dict(row=0, col=1, val=2, reorder=3, chunk_len=4, chunk_off=5, row_len=6, diag_offsets=7,
-            block_row_ptr=8, block_col=9)
+            block_row_ptr=8, block_col=9, tile_ptr=10, tile_desc=11)
 _NP = {(4, "i"): np.int32, (8, "i"): np.int64, (4, "f"): np.float32, (8, "f"): np.float64}
 
 
@@ -296,6 +296,27 @@ class COO_Matrix(_Converted):
         return self._download("val", "f")
 
 
+class CSR5_Matrix(_Converted):
+    """CSR5 (include/sparse_format.h:137-166) with device tiles of omega = 32
+    lanes x sigma = 16 entries; tile_ptr / tile_desc follow that tiling."""
+
+    _fmt = "csr5"
+    sigma = 16
+    omega = 32
+
+    @property
+    def _p(self):
+        return int(self._info().extra[0])
+
+    @property
+    def tile_ptr(self):
+        return self._download("tile_ptr", "i").view(np.uint32)
+
+    @property
+    def tile_desc(self):
+        return self._download("tile_desc", "i").view(np.uint32)
+
+
 def _wrap(cls, csr: CSR_Matrix, h: _Handle, **fields):
     m = cls()
     m.num_rows, m.num_cols, m.num_nnzs = csr.num_rows, csr.num_cols, csr.num_nnzs
@@ -353,6 +374,12 @@ def csr_to_bsr(csr: CSR_Matrix, blockDimRow: int = BSR_BlockDimRow, blockDimCol:
                  blockNNZ=blockDimRow * blockDimCol)
 
 
+def csr_to_csr5(csr: CSR_Matrix, fp_feature=None):
+    """include/sparse_conversion.h:946 (device tiles; see CSR5_Matrix)."""
+    h = _convert(csr, "csr5")
+    return _wrap(CSR5_Matrix, csr, h, row_offset=csr.row_offset, col_index=csr.col_index, values=csr.values)
+
+
 def csr_to_coo(csr: CSR_Matrix):
     """include/sparse_conversion.h:152."""
     h = _convert(csr, "coo")
@@ -389,6 +416,11 @@ def SpOps_dia(alpha, A: DIA_Matrix, x, beta, y):
 
 def SpOps_bsr(alpha, A: BSR_Matrix, x, beta, y):
     """src/spmv_bsr.cpp:214."""
+    return _spmv(alpha, A, x, beta, y)
+
+
+def SpOps_csr5(alpha, A: CSR5_Matrix, x, beta, y):
+    """src/spmv_csr5.cpp:439."""
     return _spmv(alpha, A, x, beta, y)
 
 

@@ -214,3 +214,51 @@ def test_powerlaw_full_sell_and_ell(cuda, orc):
     with pytest.raises(SpOpsError) as e:
         csr_to_ell(A)
     assert e.value.status == 5
+
+
+@pytest.mark.parametrize("name", ["lap", "pl"])
+def test_csr5_golden(cuda, golden, orc, name):
+    from sparseops_b200 import SpOps_csr5, csr_to_csr5
+    g = golden
+    rp, ci, v, x = g[f"{name}_rp"], g[f"{name}_ci"], g[f"{name}_v"], g[f"{name}_x"]
+    T = csr_to_csr5(_csr(rp, ci, v))
+    assert T._p == (len(ci) + 511) // 512 and len(T.tile_ptr) == T._p + 1
+    _check(orc, rp, ci, v, x, _spmv(SpOps_csr5, T, x))
+
+
+@pytest.mark.parametrize("itype,vtype", [(np.int32, np.float64), (np.int64, np.float64), (np.int32, np.float32)])
+def test_csr5_edges(cuda, orc, itype, vtype):
+    """Rows spanning many tiles, rows ending exactly on lane/tile boundaries,
+    runs of empty rows (also at the start and end), a partial last tile."""
+    from sparseops_b200 import SpOps_csr5, csr_to_csr5
+    rng = np.random.default_rng(11)
+    n, ncols = 7000, 50000
+    lens = rng.integers(0, 20, n)
+    lens[:5] = 0
+    lens[10], lens[11], lens[12] = 16, 512, 5000
+    lens[3000:3100] = 0
+    lens[-7:] = 0
+    lens[-8] = 1001
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens])
+    v = rng.standard_normal(len(ci))
+    x = rng.uniform(-1, 1, ncols)
+    T = csr_to_csr5(_csr(rp.astype(itype), ci.astype(itype), v.astype(vtype), ncols))
+    y = _spmv(SpOps_csr5, T, x.astype(vtype), 0.8, 0.7, np.ones(n, vtype))
+    if vtype == np.float64:
+        _check(orc, rp, ci, v, x, y)
+    else:
+        v32, x32 = v.astype(np.float32).astype(np.float64), x.astype(np.float32).astype(np.float64)
+        yref = orc.spmv_csr(rp, ci, v32, x32, 0.8, 0.7, np.ones(n))
+        den = 0.8 * orc.absdot(rp, ci, v32, x32) + 0.7
+        assert (np.abs(y - yref) / den).max() <= 1e-5
+
+
+def test_csr5_powerlaw_full(cuda, orc):
+    from sparseops_b200 import SpOps_csr5, csr_to_csr5
+    n = 4194304
+    rp, ci, v = synth.powerlaw(n, mu=math.log(12.0), sigma=1.2, lo=1, hi=20000, seed=1)
+    x = synth.uniform(n, 1)
+    T = csr_to_csr5(_csr(rp, ci, v))
+    _check(orc, rp, ci, v, x, _spmv(SpOps_csr5, T, x, 1.0, 0.0), 1.0, 0.0)
