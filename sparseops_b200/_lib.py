@@ -6,6 +6,7 @@ not load, every entry point raises.  Build it with
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
 
@@ -101,6 +102,29 @@ _SIGS = {
 _RESTYPE = {"spops_last_error": C.c_char_p, "spops_status_string": C.c_char_p, "spops_abi_version": C.c_int}
 
 _L = None
+_SHUTDOWN = False
+
+
+def _mark_shutdown() -> None:
+    global _SHUTDOWN
+    _SHUTDOWN = True
+
+
+# Handles still alive when the interpreter exits are not destroyed one by one:
+# the process exit releases their device memory, and the CUDA runtime may be
+# torn down before the last finalisers run.
+atexit.register(_mark_shutdown)
+
+
+def release(name: str, handle, owner_ctx=None) -> None:
+    """Destroy a handle with `name` (spops_*_destroy) unless the interpreter is
+    exiting or its owning context was closed first (its stream and device
+    binding are gone with it)."""
+    if _SHUTDOWN or _L is None or not handle:
+        return
+    if owner_ctx is not None and not getattr(owner_ctx, "handle", None):
+        return
+    getattr(_L, name)(handle)
 
 
 def lib() -> C.CDLL:

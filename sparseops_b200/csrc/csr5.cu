@@ -150,25 +150,33 @@ __global__ void __launch_bounds__(256) csr5_kernel(const I* __restrict__ rp, int
   const bool has_flag = flags != 0;
   V tail = V(0);
   if (in_head) head = acc; else tail = acc;
-  // inclusive prefix of heads over the lanes
-  V P = head;
+  // Heads of lanes f+1 .. m (m = next flagged lane, or 31) belong to the row
+  // of flagged lane f; heads of lanes 0 .. m0 (first flagged lane) to the row
+  // open at the tile's start.  Segmented inclusive scan of the heads with a
+  // segment starting after every flagged lane (no prefix differences, so no
+  // cancellation): S(m) = sum of its group.
+  const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
+  V S = head;
+  bool seg = lane == 0 || ((fmask >> (lane - 1)) & 1u);
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const V u = __shfl_up_sync(0xffffffffu, P, o);
-    if (lane >= o) P += u;
+    const V su = __shfl_up_sync(0xffffffffu, S, o);
+    const bool gu = __shfl_up_sync(0xffffffffu, seg, o);
+    if (lane >= o) {
+      if (!seg) S += su;
+      seg = seg || gu;
+    }
   }
-  const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
-  const V P31 = __shfl_sync(0xffffffffu, P, 31);
   const unsigned later = fmask & ~((2u << lane) - 1u);  // flagged lanes after this one (lane 31: none)
   const int m = later ? __ffs(later) - 1 : 31;
-  const V Pm = __shfl_sync(0xffffffffu, P, m);
+  const V Sm = __shfl_sync(0xffffffffu, S, m);
   const int m0 = fmask ? __ffs(fmask) - 1 : 31;
-  const V cin = __shfl_sync(0xffffffffu, P, m0);  // heads up to the first flagged lane
+  const V cin = __shfl_sync(0xffffffffu, S, m0);  // heads of lanes 0 .. m0
   if (has_flag) {
     if (later) {
-      axpby_store(y + row, tail + Pm - P, alpha, beta, bz);
+      axpby_store(y + row, tail + Sm, alpha, beta, bz);
     } else {  // the tile's last row: may continue into the next tile
-      open_sum[t] = tail + P31 - P;
+      open_sum[t] = tail + (lane < 31 ? Sm : V(0));
       open_row[t] = row;
     }
   }

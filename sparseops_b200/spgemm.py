@@ -52,7 +52,7 @@ class CandidatePairs:
 
     def __del__(self):  # pragma: no cover
         try:
-            _lib.lib().spops_pairs_destroy(self.handle)
+            _lib.release("spops_pairs_destroy", self.handle, self.ctx)
         except Exception:
             pass
 

@@ -92,8 +92,8 @@ class Context:
 
     def close(self) -> None:
         if getattr(self, "handle", None):
-            _lib.lib().spops_destroy(self.handle)
-            self.handle = None
+            h, self.handle = self.handle, None
+            _lib.release("spops_destroy", h)
 
     def __del__(self):  # pragma: no cover - interpreter shutdown order
         try:
@@ -122,8 +122,7 @@ class _Handle:
 
     def __del__(self):  # pragma: no cover
         try:
-            if self.handle:
-                _lib.lib().spops_matrix_destroy(self.handle)
+            _lib.release("spops_matrix_destroy", self.handle, self.ctx)
         except Exception:
             pass
 
@@ -238,8 +237,7 @@ class Batch:
 
     def __del__(self):  # pragma: no cover
         try:
-            if self.handle:
-                _lib.lib().spops_batch_destroy(self.handle)
+            _lib.release("spops_batch_destroy", getattr(self, "handle", None), self.ctx)
         except Exception:
             pass
 
