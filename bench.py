@@ -71,7 +71,7 @@ def spmv_bytes(n_rows, n_cols, nnz, isz=4, vsz=8):
     return isz * (n_rows + 1) + (isz + vsz) * nnz + vsz * n_cols + vsz * n_rows
 
 
-def profile_traffic(name="csr_stream_kernel_powerlaw.txt"):
+def profile_traffic(name="csr_warp_kernel_powerlaw.txt"):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", name)
     try:
