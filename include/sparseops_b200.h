@@ -328,6 +328,24 @@ spops_status_t spops_spmv_t(spops_context_t ctx, double alpha, spops_matrix_t A,
 spops_status_t spops_sddmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* g, const void* x,
                            void* out);
 
+/* ------------------------------------------------------ no allocation */
+/* y = alpha*A*x + beta*y for a CSR matrix given by device pointers, without
+ * allocating any device memory.  No counterpart in the reference: it is for
+ * callers that cannot call cudaMalloc at this point (a process whose device
+ * memory is reserved up front by a pool, a plug-in or callback that must not
+ * touch the allocator, a latency-bound loop that cannot take an allocation's
+ * synchronisation).  Scratch lives in one fixed 4 MiB device array of the
+ * library (held by every GPU that loads it until exit), which limits nnz to
+ * 134,217,728 (larger: SPOPS_ERR_TOO_LARGE, nothing launched).  The first call
+ * on a device looks that array up (make it before any stream capture).  Calls
+ * whose work overlaps on the GPU race on the array.  Out-of-range column
+ * indices are skipped and reported (SPOPS_ERR_INVALID).  Synchronises
+ * `stream` (a cudaStream_t, may be NULL) before returning. */
+spops_status_t spops_csr_spmv_noalloc(int64_t rows, int64_t cols, int64_t nnz, const void* row_offset,
+                                      const void* col_index, const void* values, spops_index_t itype,
+                                      spops_value_t vtype, double alpha, const void* x, double beta, void* y,
+                                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

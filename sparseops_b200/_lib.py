@@ -96,6 +96,7 @@ _SIGS = {
     "spops_hierarchical_clustering": [vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp],
     "spops_spgemm_clustered": [vp, vp, vp, vp, vp, i64, i32, dbl, vp, vp],
     "spops_spgemm_lsh": [vp, vp, vp, i32, i32, u64, i64, i32, dbl, vp, vp],
+    "spops_csr_spmv_noalloc": [i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, dbl, vp, dbl, vp, vp],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
     "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
 }
