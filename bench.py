@@ -129,6 +129,21 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """Max of a per-rank time over all ranks (identity without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(world: int, nbytes: int, ms: float) -> float:
+    """Replicas: every rank processes `nbytes`; the job takes the slowest rank's time."""
+    return world * nbytes / (ms * 1e-3) / 1e9
+
+
 def cpu_reference_sample(rp, ci, v, x, budget_s=10.0, threads=None):
     """Time the reference's CSR kernel (flag 2) on host cores on a row slab of
     the workload sized to about `budget_s` of CPU work.  Returns (GB/s, info)."""
@@ -273,12 +288,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
     ck = clocks.stop()
+    ms = max_over_ranks(ms, dist, dev)
     if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * nbytes / (ms * 1e-3) / 1e9
+    value = whole_job_gbs(world, nbytes, ms)
 
     # ---- e2e: the host path through the C ABI (pinned x in, y out, per step)
     xh = torch.from_numpy(x).pin_memory()
@@ -298,12 +311,8 @@ def run_ours(args):
         step_host()
     e1.record(stream)
     torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1) / e2e_steps
-    if dist:
-        t = torch.tensor([ems], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e = world * nbytes / (ems * 1e-3) / 1e9
+    ems = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, dev)
+    e2e = whole_job_gbs(world, nbytes, ems)
     # correctness spot check of the e2e result against the device result
     ok = bool(torch.equal(yh.to(dev), yd))
 
