@@ -106,8 +106,11 @@ spops_status_t spops_synchronize(spops_context_t ctx);
  * when any bit was set; *flags (may be NULL) receives the bits. */
 spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
 /* Tuning switches by name; unknown keys are rejected with SPOPS_ERR_INVALID.
- *   "csr_variant" 0..2: CSR SpMV kernel shape (entries per lane per load
- *   round / resident blocks per SM: 0 = 8/4 (default), 1 = 4/6, 2 = 16/2). */
+ *   "csr_variant" 0..4: CSR SpMV kernel.  0 (default) and 1: tiles of 32*K
+ *   entries summed in registers, K = 8 or 4 entries per lane (needs column
+ *   and value arrays aligned to min(32, K * element size) bytes, otherwise
+ *   variant 2 runs); 2, 3, 4: nnz-balanced row segments through shared memory
+ *   with 8/4, 4/6, 16/2 entries per lane per round / blocks per SM. */
 spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);

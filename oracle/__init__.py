@@ -74,6 +74,10 @@ class Oracle:
     def absdot(self, rp, ci, v, x):
         n = len(rp) - 1
         out = np.zeros(n)
+        if rp.dtype != np.int32 or ci.dtype != np.int32:
+            if len(ci) >= 2**31 or len(x) >= 2**31:
+                raise ValueError("absdot: indices beyond int32")
+            rp, ci = np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32)
         self.L.orc_absdot_csr_f64_i32(_i64(n), _p(rp), _p(ci), _p(np.ascontiguousarray(v, np.float64)),
                                       _p(np.ascontiguousarray(x, np.float64)), _p(out))
         return out

@@ -15,8 +15,11 @@
 //   its own segment.  The column indices are checked once against [0, cols)
 //   and the row offsets for monotonicity, so the kernel never gathers outside x.
 //
-// SpMV (csr_warp_kernel): see the kernel.  The summation order depends only
-// on the matrix, so results are bit-reproducible run to run.
+// SpMV: by default the tile kernel of spmv_csr_tile.cu, which keeps products
+// in registers; this file's segment kernel (csr_warp_kernel) stages them in
+// shared memory and serves unaligned arrays, the batched persistent kernel and
+// multi-RHS.  Either way the summation order depends only on the matrix, so
+// results are bit-reproducible run to run.
 #include <cub/cub.cuh>
 
 #include "device_util.cuh"
@@ -29,10 +32,10 @@ namespace {
 constexpr int kBlock = 256;                 // 8 warps, each on its own segments
 constexpr int kCap = kCsrCap;               // entries per long-row chunk; short segments < 2*kCap
 constexpr int kRowCap = kCsrRowCap;         // rows per short segment at most
-// Kernel variants (entries per lane per load round, resident blocks per SM):
-// more items keep more bytes in flight per warp, fewer leave room for more
-// warps.  Variant 0 is the default; spops_set_option("csr_variant", v).
-constexpr int kVariants = 3;
+// Kernel choice (spops_set_option "csr_variant"): 0 / 1 the tile kernel of
+// spmv_csr_tile.cu with 8 / 4 entries per lane (the default, when the arrays
+// are aligned for its vector loads); 2 / 3 / 4 the segment kernel below with
+// (entries per lane per load round, resident blocks per SM) = 8/4, 4/6, 16/2.
 
 // ------------------------------------------------------------ analysis
 template <typename I>
@@ -241,11 +244,16 @@ spops_status_t launch_warp(Context* ctx, Matrix* A, double alpha, const void* x,
 
 template <typename I, typename V>
 spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
-  if (A->plan.nblocks == 0) return SPOPS_OK;
+  if (A->rows == 0) return SPOPS_OK;
   switch (ctx->csr_variant) {
-    case 1: return launch_warp<I, V, 4, 6>(ctx, A, alpha, x, beta, y);
-    case 2: return launch_warp<I, V, 16, 2>(ctx, A, alpha, x, beta, y);
-    default: return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);
+    case 2: return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);
+    case 3: return launch_warp<I, V, 4, 6>(ctx, A, alpha, x, beta, y);
+    case 4: return launch_warp<I, V, 16, 2>(ctx, A, alpha, x, beta, y);
+    default: {
+      const int k = ctx->csr_variant == 1 ? 4 : 8;
+      if (csr_tile_usable(A, k)) return csr_tile_spmv(ctx, A, k, alpha, x, beta, y);
+      return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);  // arrays not aligned for vector loads
+    }
   }
 }
 

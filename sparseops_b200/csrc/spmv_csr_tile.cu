@@ -1,0 +1,359 @@
+// CSR SpMV by fixed tiles of entries, summed in registers (the default CSR
+// kernel).
+//
+// The matrix stays in the caller's CSR arrays.  Entries are cut into tiles of
+// 32*K consecutive entries; lane l of the warp that owns tile t sums entries
+// [t*32K + l*K, +K) -- one 128- or 256-bit load for its columns and values,
+// K gathers of x, and a running sum that is cut at every row start inside the
+// run.  That is the tile-segmented sum of CSR5 (Liu & Vinter, ICS'15; the
+// reference's SpOps_csr5, src/spmv_csr5.cpp:113-457) applied to the plain
+// CSR layout: with vector loads each lane's run is already one contiguous
+// load, so no transposed copy of the matrix is made, and the products never
+// pass through shared memory (the round trip that bounds the segment kernel
+// in spmv_csr.cu).
+//
+// Analysis (once per matrix, csr_tile_analyse):
+//   flags[t*32 + l]  bit b set when entry t*32K + l*K + b starts a non-empty row
+//   tile_row[t]      row holding the tile's first entry; negative (~row) when
+//                    an empty row lies inside the tile ("slow" tile: lanes then
+//                    find their rows from the row offsets instead of counting
+//                    flags)
+//   empty            list of empty rows (y = beta*y for them)
+// SpMV (csr_tile_kernel + csr_tile_calibrate_kernel):
+//   lane row   = tile_row + number of flags before the lane's first entry
+//                (bit-sliced ballots, no shared memory)
+//   in-lane    complete rows go straight to y
+//   cross-lane heads (before a lane's first flag) are summed by a segmented
+//              warp scan into the row of the previous flagged lane
+//   cross-tile the row open at a tile's end (open_row, open_sum) receives the
+//              heads (carry_in) of the following tiles up to the next tile
+//              that starts a row -- a second small kernel, in tile order.
+// Summation order depends only on the matrix: results are bit-reproducible.
+#include <cub/cub.cuh>
+
+#include "device_util.cuh"
+#include "spops_internal.h"
+
+namespace spops {
+namespace {
+
+constexpr int kTileBlock = 256;
+
+inline unsigned grid_of(int64_t work, int threads = 256) {
+  int64_t g = (work + threads - 1) / threads;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+// last r in [0, n-1] with rp[r] <= e (the non-empty row holding entry e)
+template <typename I>
+__device__ __forceinline__ int64_t row_holding(const I* rp, int64_t n, int64_t e) {
+  int64_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if ((int64_t)rp[mid] <= e) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// One thread per tile: walk the tile's entries with a row cursor.
+template <typename I, int K>
+__global__ void tile_build_kernel(const I* __restrict__ rp, int64_t n, int64_t nnz, int64_t tiles,
+                                  int64_t* __restrict__ tile_row, uint8_t* __restrict__ flags) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= tiles) return;
+  constexpr int T = 32 * K;
+  const int64_t e0 = t * T, e1 = (e0 + T < nnz) ? e0 + T : nnz;
+  int64_t r = row_holding(rp, n, e0);
+  const int64_t r0 = r;
+  bool slow = false;
+  uint32_t word = 0;  // flags of 4 lanes, written as one 32-bit word
+  for (int64_t e = e0; e < e0 + T; ++e) {
+    const int q = (int)(e - e0);
+    if (e < e1) {
+      int steps = 0;
+      while ((int64_t)rp[r + 1] <= e) {
+        ++r;
+        ++steps;
+      }
+      if (steps > 1) slow = true;  // passed over an empty row inside the tile
+      if ((int64_t)rp[r] == e) word |= 1u << (((q / K) & 3) * 8 + (q % K));
+    }
+    if ((q + 1) % (4 * K) == 0) {
+      reinterpret_cast<uint32_t*>(flags)[t * 8 + q / (4 * K)] = word;
+      word = 0;
+    }
+  }
+  tile_row[t] = slow ? ~r0 : r0;
+}
+
+template <typename I>
+__global__ void tile_empty_kernel(const I* __restrict__ rp, int64_t n, int64_t* __restrict__ list,
+                                  unsigned long long* __restrict__ count) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n && rp[r] == rp[r + 1]) list[atomicAdd(count, 1ULL)] = r;
+}
+
+// ---- vector loads of one lane's run (32-byte aligned for 32-byte runs)
+template <int BYTES>
+struct RunLoad;
+template <>
+struct RunLoad<16> {
+  static __device__ __forceinline__ void ld(const void* p, uint32_t (&w)[4]) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+                 : "l"(p));
+  }
+};
+template <>
+struct RunLoad<32> {
+  static __device__ __forceinline__ void ld(const void* p, uint32_t (&w)[8]) {
+    asm volatile("ld.global.nc.L1::no_allocate.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+                 : "l"(p));
+  }
+};
+
+// K elements of T from p (aligned to min(32, K*sizeof(T)) bytes) into out.
+template <typename T, int K>
+__device__ __forceinline__ void load_run(const T* __restrict__ p, T (&out)[K]) {
+  constexpr int BYTES = K * (int)sizeof(T);
+  static_assert(BYTES == 16 || BYTES % 32 == 0, "run must be 16 bytes or a multiple of 32");
+  if constexpr (BYTES == 16) {
+    uint32_t w[4];
+    RunLoad<16>::ld(p, w);
+    memcpy(out, w, 16);
+  } else {
+#pragma unroll
+    for (int q = 0; q < BYTES / 32; ++q) {
+      uint32_t w[8];
+      RunLoad<32>::ld(reinterpret_cast<const char*>(p) + 32 * q, w);
+      memcpy(reinterpret_cast<char*>(out) + 32 * q, w, 32);
+    }
+  }
+}
+
+template <typename I, typename V, int K, int kMinBlocks>
+__global__ void __launch_bounds__(kTileBlock, kMinBlocks) csr_tile_kernel(
+    const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
+    const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t tiles,
+    const V* __restrict__ x, V* __restrict__ y, V alpha, V beta, bool bz, V* __restrict__ carry_in,
+    V* __restrict__ open_sum, int64_t* __restrict__ open_row) {
+  constexpr int T = 32 * K;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;  // lanes below this one
+  const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
+  for (int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5); t < tiles; t += nw) {
+    const int64_t el = t * T + (int64_t)lane * K;
+    const uint32_t flags = flags_all[t * 32 + lane];
+    const int64_t tr = tile_row[t];
+    // ---- products of the lane's run
+    V p[K];
+    if (el + K <= nnz) {
+      I c[K];
+      V a[K];
+      load_run<I, K>(ci + el, c);
+      load_run<V, K>(val + el, a);
+#pragma unroll
+      for (int b = 0; b < K; ++b) p[b] = a[b] * ld_gather(x + c[b]);
+    } else {
+#pragma unroll
+      for (int b = 0; b < K; ++b) p[b] = (el + b < nnz) ? ld_stream(val + el + b) * ld_gather(x + ci[el + b]) : V(0);
+    }
+    // ---- row of the lane's first entry
+    int64_t row;
+    if (tr >= 0) {
+      const int cnt = __popc(flags);
+      int excl = 0;
+#pragma unroll
+      for (int bit = 0; bit < 4; ++bit) excl += __popc(__ballot_sync(0xffffffffu, (cnt >> bit) & 1) & lt) << bit;
+      const int first0 = (int)(__ballot_sync(0xffffffffu, flags & 1u) & 1u);
+      row = tr + excl + (int)(flags & 1u) - first0;
+    } else {
+      row = row_holding(rp, n, el < nnz ? el : nnz - 1);
+    }
+    // ---- in-lane segments
+    V head = V(0), acc = V(0);
+    bool in_head = (flags & 1u) == 0;
+#pragma unroll
+    for (int b = 0; b < K; ++b) {
+      if (b > 0 && ((flags >> b) & 1u)) {
+        if (in_head) {
+          head = acc;
+          in_head = false;
+        } else {
+          axpby_store(y + row, acc, alpha, beta, bz);
+        }
+        acc = V(0);
+        ++row;
+        if (tr < 0)
+          while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
+      }
+      acc += p[b];
+    }
+    V tail = V(0);
+    if (in_head) head = acc; else tail = acc;
+    // ---- cross-lane: segmented inclusive scan of the heads, a segment
+    // starting right after every flagged lane
+    const bool has_flag = flags != 0;
+    const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
+    const unsigned starts = (fmask << 1) | 1u;  // lane l starts a segment if lane l-1 is flagged (or l == 0)
+    V S = head;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const V su = __shfl_up_sync(0xffffffffu, S, o);
+      // add lane (l - o)'s sum unless a segment starts in lanes l-o+1 .. l
+      const unsigned span = (lane >= o) ? ((2u << lane) - 1u) & ~((2u << (lane - o)) - 1u) : 0u;
+      if (lane >= o && !(starts & span)) S += su;
+    }
+    const unsigned later = fmask & ~((2u << lane) - 1u);  // flagged lanes after this one
+    const int m = later ? __ffs(later) - 1 : 31;
+    const V Sm = __shfl_sync(0xffffffffu, S, m);
+    const int m0 = fmask ? __ffs(fmask) - 1 : 31;
+    const V cin = __shfl_sync(0xffffffffu, S, m0);
+    if (has_flag) {
+      if (later) {
+        axpby_store(y + row, tail + Sm, alpha, beta, bz);
+      } else {  // the tile's last row: may continue into the next tile
+        open_sum[t] = tail + (lane < 31 ? Sm : V(0));
+        open_row[t] = row;
+      }
+    }
+    if (lane == 0) {
+      carry_in[t] = cin;
+      if (!fmask) open_row[t] = -1;
+    }
+  }
+}
+
+// Rows open at a tile's end receive the heads of the following tiles up to the
+// first one that starts a row; empty rows get y = beta*y.
+template <typename V>
+__global__ void csr_tile_calibrate_kernel(int64_t tiles, const V* __restrict__ carry_in, const V* __restrict__ open_sum,
+                                          const int64_t* __restrict__ open_row, const int64_t* __restrict__ empty,
+                                          int64_t nempty, V* __restrict__ y, V alpha, V beta, bool bz) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < tiles) {
+    const int64_t r = open_row[t];
+    if (r < 0) return;
+    V tot = open_sum[t];
+    for (int64_t u = t + 1; u < tiles; ++u) {
+      tot += carry_in[u];
+      if (open_row[u] >= 0) break;
+    }
+    axpby_store(y + r, tot, alpha, beta, bz);
+  } else if (t - tiles < nempty) {
+    axpby_store(y + empty[t - tiles], V(0), alpha, beta, bz);
+  }
+}
+
+template <int K>
+int64_t tiles_of(int64_t nnz) {
+  return (nnz + 32 * K - 1) / (32 * K);
+}
+
+template <typename I, int K>
+spops_status_t analyse_t(Context* ctx, Matrix* A) {
+  CsrTiles& D = A->plan.tiles;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = A->rows, nnz = A->nnz;
+  D.release();
+  D.k = K;
+  D.tiles = tiles_of<K>(nnz);
+  const size_t nt1 = (size_t)(D.tiles > 0 ? D.tiles : 1);
+  SPOPS_TRY(D.tile_row.alloc(nt1 * 8));
+  SPOPS_TRY(D.flags.alloc(nt1 * 32));
+  SPOPS_TRY(D.carry_in.alloc(nt1 * 8));
+  SPOPS_TRY(D.open_sum.alloc(nt1 * 8));
+  SPOPS_TRY(D.open_row.alloc(nt1 * 8));
+  SPOPS_TRY(D.empty.alloc((size_t)(n > 0 ? n : 1) * 8));
+  if (D.tiles > 0 && n > 0) {
+    tile_build_kernel<I, K><<<grid_of(D.tiles), 256, 0, st>>>(A->row.as<I>(), n, nnz, D.tiles,
+                                                                D.tile_row.as<int64_t>(), D.flags.as<uint8_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  SPOPS_TRY(ctx->scratch_reserve(256));
+  unsigned long long* cnt = ctx->scratch.as<unsigned long long>();
+  SPOPS_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
+  if (n > 0) {
+    tile_empty_kernel<I><<<grid_of(n), 256, 0, st>>>(A->row.as<I>(), n, D.empty.as<int64_t>(), cnt);
+    SPOPS_LAUNCH_CHECK();
+  }
+  unsigned long long h = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  D.nempty = (int64_t)h;
+  D.ready = true;
+  return SPOPS_OK;
+}
+
+template <typename I, typename V, int K, int kMinBlocks>
+spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
+  const CsrTiles& D = A->plan.tiles;
+  const bool bz = beta == 0.0;
+  if (D.tiles > 0) {
+    static int blocks_per_sm = -1;  // per instantiation
+    if (blocks_per_sm < 0) {
+      int bps = 0;
+      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_kernel<I, V, K, kMinBlocks>,
+                                                               kTileBlock, 0));
+      blocks_per_sm = bps > 0 ? bps : 1;
+    }
+    int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
+    const int64_t need = (D.tiles + kTileBlock / 32 - 1) / (kTileBlock / 32);
+    if (grid > need) grid = need;
+    csr_tile_kernel<I, V, K, kMinBlocks><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
+        A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), A->val.as<V>(), D.tile_row.as<int64_t>(),
+        D.flags.as<uint8_t>(), D.tiles, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, bz,
+        D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  if (D.tiles + D.nempty > 0) {
+    csr_tile_calibrate_kernel<V><<<grid_of(D.tiles + D.nempty), 256, 0, ctx->stream>>>(
+        D.tiles, D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), D.nempty,
+        static_cast<V*>(y), (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
+}
+
+// K for a (value type, variant): 4 entries per lane (one 256-bit value load
+// for FP64) or 8.
+template <typename I, typename V>
+spops_status_t dispatch(Context* ctx, Matrix* A, int k, double alpha, const void* x, double beta, void* y) {
+  if (k == 8) return spmv_t<I, V, 8, 4>(ctx, A, alpha, x, beta, y);
+  return spmv_t<I, V, 4, 4>(ctx, A, alpha, x, beta, y);
+}
+
+}  // namespace
+
+void CsrTiles::release() {
+  tile_row.release(); flags.release(); carry_in.release(); open_sum.release(); open_row.release(); empty.release();
+  tiles = 0;
+  nempty = 0;
+  k = 0;
+  ready = false;
+}
+
+bool csr_tile_usable(const Matrix* A, int k) {
+  // vector loads need each lane's run aligned: run bytes (capped at 32)
+  const size_t ca = (size_t)k * A->isize() >= 32 ? 32 : (size_t)k * A->isize();
+  const size_t va = (size_t)k * A->vsize() >= 32 ? 32 : (size_t)k * A->vsize();
+  return ((uintptr_t)A->col.p % ca) == 0 && ((uintptr_t)A->val.p % va) == 0;
+}
+
+spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k) {
+  const bool i32 = A->itype == SPOPS_INDEX_I32;
+  if (k == 8) return i32 ? analyse_t<int32_t, 8>(ctx, A) : analyse_t<int64_t, 8>(ctx, A);
+  return i32 ? analyse_t<int32_t, 4>(ctx, A) : analyse_t<int64_t, 4>(ctx, A);
+}
+
+spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int k, double alpha, const void* x, double beta, void* y) {
+  if (!A->plan.tiles.ready || A->plan.tiles.k != k) SPOPS_TRY(csr_tile_analyse(ctx, A, k));
+  const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return dispatch<int32_t, double>(ctx, A, k, alpha, x, beta, y);
+  if (i32) return dispatch<int32_t, float>(ctx, A, k, alpha, x, beta, y);
+  if (f64) return dispatch<int64_t, double>(ctx, A, k, alpha, x, beta, y);
+  return dispatch<int64_t, float>(ctx, A, k, alpha, x, beta, y);
+}
+
+}  // namespace spops

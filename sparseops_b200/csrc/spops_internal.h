@@ -86,6 +86,22 @@ struct CsrSeg {
   int32_t chunk;
 };
 
+// Tile analysis of a CSR matrix for the register-sum kernel
+// (spmv_csr_tile.cu): tiles of 32*k consecutive entries, one warp each.
+struct CsrTiles {
+  bool ready = false;
+  int k = 0;               // entries per lane
+  int64_t tiles = 0;
+  int64_t nempty = 0;
+  DevBuf tile_row;         // int64 [tiles]: row of the tile's first entry (~row: tile spans an empty row)
+  DevBuf flags;            // uint8 [tiles*32]: row starts within each lane's run
+  DevBuf carry_in;         // V [tiles]: sum of the tile's entries before its first row start
+  DevBuf open_sum;         // V [tiles]: partial sum of the row open at the tile's end
+  DevBuf open_row;         // int64 [tiles]: that row, or -1 (no row starts in the tile)
+  DevBuf empty;            // int64 [rows]: empty rows
+  void release();
+};
+
 // Row-block partition of a CSR matrix for the streaming SpMV kernel
 // (spmv_csr.cu).  Block b covers rows [blk_row[b], next block's row) when
 // blk_chunk[b] < 0 (a segment of short rows whose entries fit in shared
@@ -100,8 +116,10 @@ struct CsrPlan {
   DevBuf partial;          // V [nblocks] long-row chunk sums
   DevBuf counter;          // int32 [nblocks] arrival counters (zero between calls)
   DevBuf seg;              // CsrSeg [nblocks]
+  CsrTiles tiles;          // built on first use by the tile kernel
   void release() {
     blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); seg.release();
+    tiles.release();
     ready = false;
   }
 };
@@ -223,6 +241,11 @@ struct SpgemmStats {
 // ------------------------------------------------------------ kernels API
 spops_status_t csr_analyse(Context* ctx, Matrix* A);
 spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
+// tile kernel (spmv_csr_tile.cu); usable when the column and value arrays are
+// aligned for the lane's vector loads
+bool csr_tile_usable(const Matrix* A, int k);
+spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k);
+spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int k, double alpha, const void* x, double beta, void* y);
 
 // formats.cu
 spops_status_t convert_from_csr(Context* ctx, Matrix* A, spops_format_t fmt, const spops_format_params_t& p,

@@ -178,3 +178,40 @@ def test_invalid_pattern_rejected(cuda):
     with pytest.raises(SpOpsError) as e:
         A.device()
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("dtype,itype", [(np.float64, np.int32), (np.float32, np.int32), (np.float64, np.int64)])
+def test_kernel_variants_identical(cuda, orc, dtype, itype):
+    """Every CSR kernel (spops_set_option "csr_variant") agrees with the oracle,
+    including long rows (chunk and tile combines) and empty-row runs; the
+    segment-kernel shapes (2, 3, 4) give the same y bit for bit."""
+    from sparseops_b200 import default_context
+    rng = np.random.default_rng(11)
+    n, ncols = 20000, 120000
+    lens = rng.poisson(20, n)
+    lens[7], lens[8], lens[9] = 30000, 256, 257
+    lens[500:900] = 0
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(itype)
+    v = rng.standard_normal(len(ci)).astype(dtype)
+    x = rng.uniform(-1, 1, ncols).astype(dtype)
+    y0 = rng.uniform(-1, 1, n).astype(dtype)
+    rp = rp.astype(itype)
+    ctx = default_context()
+    ys = []
+    try:
+        for var in range(5):
+            ctx.set_option("csr_variant", var)
+            y, _ = _run(rp, ci, v, x, 0.8, 0.7, y0)
+            ys.append(y)
+    finally:
+        ctx.set_option("csr_variant", 0)
+    yref = orc.spmv_csr(rp.astype(np.int64), ci.astype(np.int64), v.astype(np.float64), x.astype(np.float64),
+                        0.8, 0.7, y0.astype(np.float64))
+    tol = TOL64 if dtype == np.float64 else TOL32
+    for var, y in enumerate(ys):
+        assert _err(orc, rp.astype(np.int64), ci.astype(np.int64), v.astype(np.float64), x.astype(np.float64),
+                    y.astype(np.float64), yref, 0.7, y0.astype(np.float64), 0.8) <= tol, var
+        if var > 2:
+            assert np.array_equal(y, ys[2]), var
