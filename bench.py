@@ -71,7 +71,7 @@ def spmv_bytes(n_rows, n_cols, nnz, isz=4, vsz=8):
     return isz * (n_rows + 1) + (isz + vsz) * nnz + vsz * n_cols + vsz * n_rows
 
 
-def profile_traffic(name="csr_warp_kernel_powerlaw.txt"):
+def profile_traffic(name="csr_tile_kernel_powerlaw.txt"):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", name)
     try:
@@ -341,12 +341,14 @@ def run_ours(args):
         "pct_of_peak": round(100 * value / world / peak, 2),
         "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
-                     "peak_source": peak_kind, "kernel": "csr_warp_kernel<int,double>",
+                     "peak_source": peak_kind,
+                     "kernel": "csr_tile_kernel<int,double,8,3,1> + csr_tile_calibrate_kernel<double>",
                      "traffic": traffic},
         "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                 "steps": e2e_steps, "matches_device_result": ok,
                 "path": "spops_spmv_host (matrix resident after first upload)"},
-        "gpu_launches": args.steps,
+        # tile kernel + its calibrator per SpMV; one launch for the segment kernel
+        "gpu_launches": args.steps * (1 if args.csr_variant in (2, 3, 4) else 2),
         "clocks": ck,
         "cpu_baseline": cpu,
     }

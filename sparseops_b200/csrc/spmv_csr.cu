@@ -1,3 +1,8 @@
+// Kernel choice (spops_set_option "csr_variant"): the tile kernel of
+// spmv_csr_tile.cu (entries per lane / resident blocks per SM / next tile
+// prefetched) 0 = 8/3/yes (default), 1 = 8/4/no, 5 = 4/4/no, 6 = 8/5/no, used
+// when the arrays are aligned for its vector loads; the segment kernel below
+// (entries per lane per load round / blocks per SM) 2 = 8/4, 3 = 4/6, 4 = 16/2.
 // CSR SpMV y = alpha*A*x + beta*y for sm_100a.
 //
 // Replaces SpOps_csr (reference src/spmv_csr.cpp:165-185), whose variants are
@@ -250,8 +255,7 @@ spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, doub
     case 3: return launch_warp<I, V, 4, 6>(ctx, A, alpha, x, beta, y);
     case 4: return launch_warp<I, V, 16, 2>(ctx, A, alpha, x, beta, y);
     default: {
-      const int k = ctx->csr_variant == 1 ? 4 : 8;
-      if (csr_tile_usable(A, k)) return csr_tile_spmv(ctx, A, k, alpha, x, beta, y);
+      if (csr_tile_usable(A, ctx->csr_variant)) return csr_tile_spmv(ctx, A, ctx->csr_variant, alpha, x, beta, y);
       return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);  // arrays not aligned for vector loads
     }
   }

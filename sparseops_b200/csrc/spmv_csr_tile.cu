@@ -132,96 +132,139 @@ __device__ __forceinline__ void load_run(const T* __restrict__ p, T (&out)[K]) {
   }
 }
 
-template <typename I, typename V, int K, int kMinBlocks>
+// Columns and values of lane `lane`'s run of tile t; entries past nnz read as
+// column 0 with value 0.
+template <typename I, typename V, int K>
+__device__ __forceinline__ void tile_load(const I* __restrict__ ci, const V* __restrict__ val, int64_t nnz, int64_t t,
+                                          int lane, I (&c)[K], V (&a)[K]) {
+  const int64_t el = t * (32 * K) + (int64_t)lane * K;
+  if (el + K <= nnz) {
+    load_run<I, K>(ci + el, c);
+    load_run<V, K>(val + el, a);
+  } else {
+#pragma unroll
+    for (int b = 0; b < K; ++b) {
+      const bool in = el + b < nnz;
+      c[b] = in ? ci[el + b] : I(0);
+      a[b] = in ? ld_stream(val + el + b) : V(0);
+    }
+  }
+}
+
+// Given the products p of the lane's run: rows complete inside the lane go to
+// y, the heads combine across lanes, the tile's open row and carry go to the
+// calibrator arrays.
+template <typename I, typename V, int K>
+__device__ __forceinline__ void tile_finish(const I* __restrict__ rp, int64_t n, int64_t nnz, int64_t t, int lane,
+                                            uint32_t flags, int64_t tr, const V (&p)[K], V* __restrict__ y, V alpha,
+                                            V beta, bool bz, V* __restrict__ carry_in, V* __restrict__ open_sum,
+                                            int64_t* __restrict__ open_row) {
+  const unsigned lt = (1u << lane) - 1u;  // lanes below this one
+  const int64_t el = t * (32 * K) + (int64_t)lane * K;
+  // ---- row of the lane's first entry
+  int64_t row;
+  if (tr >= 0) {
+    const int cnt = __popc(flags);
+    int excl = 0;
+#pragma unroll
+    for (int bit = 0; bit < 4; ++bit) excl += __popc(__ballot_sync(0xffffffffu, (cnt >> bit) & 1) & lt) << bit;
+    const int first0 = (int)(__ballot_sync(0xffffffffu, flags & 1u) & 1u);
+    row = tr + excl + (int)(flags & 1u) - first0;
+  } else {
+    row = row_holding(rp, n, el < nnz ? el : nnz - 1);
+  }
+  // ---- in-lane segments
+  V head = V(0), acc = V(0);
+  bool in_head = (flags & 1u) == 0;
+#pragma unroll
+  for (int b = 0; b < K; ++b) {
+    if (b > 0 && ((flags >> b) & 1u)) {
+      if (in_head) {
+        head = acc;
+        in_head = false;
+      } else {
+        axpby_store(y + row, acc, alpha, beta, bz);
+      }
+      acc = V(0);
+      ++row;
+      if (tr < 0)
+        while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
+    }
+    acc += p[b];
+  }
+  V tail = V(0);
+  if (in_head) head = acc; else tail = acc;
+  // ---- cross-lane: segmented inclusive scan of the heads, a segment
+  // starting right after every flagged lane
+  const bool has_flag = flags != 0;
+  const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
+  const unsigned starts = (fmask << 1) | 1u;  // lane l starts a segment if lane l-1 is flagged (or l == 0)
+  V S = head;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const V su = __shfl_up_sync(0xffffffffu, S, o);
+    // add lane (l - o)'s sum unless a segment starts in lanes l-o+1 .. l
+    const unsigned span = (lane >= o) ? ((2u << lane) - 1u) & ~((2u << (lane - o)) - 1u) : 0u;
+    if (lane >= o && !(starts & span)) S += su;
+  }
+  const unsigned later = fmask & ~((2u << lane) - 1u);  // flagged lanes after this one
+  const int m = later ? __ffs(later) - 1 : 31;
+  const V Sm = __shfl_sync(0xffffffffu, S, m);
+  const int m0 = fmask ? __ffs(fmask) - 1 : 31;
+  const V cin = __shfl_sync(0xffffffffu, S, m0);
+  if (has_flag) {
+    if (later) {
+      axpby_store(y + row, tail + Sm, alpha, beta, bz);
+    } else {  // the tile's last row: may continue into the next tile
+      open_sum[t] = tail + (lane < 31 ? Sm : V(0));
+      open_row[t] = row;
+    }
+  }
+  if (lane == 0) {
+    carry_in[t] = cin;
+    if (!fmask) open_row[t] = -1;
+  }
+}
+
+// One warp per tile, grid-stride over tiles.  kPipe: the next tile's columns,
+// values and flags are loaded before this tile's gathers are used, so the
+// streaming loads of one tile overlap the gathers of the previous one.
+template <typename I, typename V, int K, int kMinBlocks, bool kPipe>
 __global__ void __launch_bounds__(kTileBlock, kMinBlocks) csr_tile_kernel(
     const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
     const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t tiles,
     const V* __restrict__ x, V* __restrict__ y, V alpha, V beta, bool bz, V* __restrict__ carry_in,
     V* __restrict__ open_sum, int64_t* __restrict__ open_row) {
-  constexpr int T = 32 * K;
   const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;  // lanes below this one
   const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
-  for (int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5); t < tiles; t += nw) {
-    const int64_t el = t * T + (int64_t)lane * K;
-    const uint32_t flags = flags_all[t * 32 + lane];
-    const int64_t tr = tile_row[t];
-    // ---- products of the lane's run
+  int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5);
+  if (t >= tiles) return;
+  I c[K];
+  V a[K];
+  uint32_t flags = 0;
+  int64_t tr = 0;
+  if (kPipe) {
+    tile_load<I, V, K>(ci, val, nnz, t, lane, c, a);
+    flags = flags_all[t * 32 + lane];
+    tr = tile_row[t];
+  }
+  for (; t < tiles; t += nw) {
+    if (!kPipe) {
+      tile_load<I, V, K>(ci, val, nnz, t, lane, c, a);
+      flags = flags_all[t * 32 + lane];
+      tr = tile_row[t];
+    }
     V p[K];
-    if (el + K <= nnz) {
-      I c[K];
-      V a[K];
-      load_run<I, K>(ci + el, c);
-      load_run<V, K>(val + el, a);
 #pragma unroll
-      for (int b = 0; b < K; ++b) p[b] = a[b] * ld_gather(x + c[b]);
-    } else {
-#pragma unroll
-      for (int b = 0; b < K; ++b) p[b] = (el + b < nnz) ? ld_stream(val + el + b) * ld_gather(x + ci[el + b]) : V(0);
+    for (int b = 0; b < K; ++b) p[b] = a[b] * ld_gather(x + c[b]);
+    const uint32_t f = flags;
+    const int64_t r0 = tr;
+    if (kPipe && t + nw < tiles) {
+      tile_load<I, V, K>(ci, val, nnz, t + nw, lane, c, a);
+      flags = flags_all[(t + nw) * 32 + lane];
+      tr = tile_row[t + nw];
     }
-    // ---- row of the lane's first entry
-    int64_t row;
-    if (tr >= 0) {
-      const int cnt = __popc(flags);
-      int excl = 0;
-#pragma unroll
-      for (int bit = 0; bit < 4; ++bit) excl += __popc(__ballot_sync(0xffffffffu, (cnt >> bit) & 1) & lt) << bit;
-      const int first0 = (int)(__ballot_sync(0xffffffffu, flags & 1u) & 1u);
-      row = tr + excl + (int)(flags & 1u) - first0;
-    } else {
-      row = row_holding(rp, n, el < nnz ? el : nnz - 1);
-    }
-    // ---- in-lane segments
-    V head = V(0), acc = V(0);
-    bool in_head = (flags & 1u) == 0;
-#pragma unroll
-    for (int b = 0; b < K; ++b) {
-      if (b > 0 && ((flags >> b) & 1u)) {
-        if (in_head) {
-          head = acc;
-          in_head = false;
-        } else {
-          axpby_store(y + row, acc, alpha, beta, bz);
-        }
-        acc = V(0);
-        ++row;
-        if (tr < 0)
-          while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
-      }
-      acc += p[b];
-    }
-    V tail = V(0);
-    if (in_head) head = acc; else tail = acc;
-    // ---- cross-lane: segmented inclusive scan of the heads, a segment
-    // starting right after every flagged lane
-    const bool has_flag = flags != 0;
-    const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
-    const unsigned starts = (fmask << 1) | 1u;  // lane l starts a segment if lane l-1 is flagged (or l == 0)
-    V S = head;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const V su = __shfl_up_sync(0xffffffffu, S, o);
-      // add lane (l - o)'s sum unless a segment starts in lanes l-o+1 .. l
-      const unsigned span = (lane >= o) ? ((2u << lane) - 1u) & ~((2u << (lane - o)) - 1u) : 0u;
-      if (lane >= o && !(starts & span)) S += su;
-    }
-    const unsigned later = fmask & ~((2u << lane) - 1u);  // flagged lanes after this one
-    const int m = later ? __ffs(later) - 1 : 31;
-    const V Sm = __shfl_sync(0xffffffffu, S, m);
-    const int m0 = fmask ? __ffs(fmask) - 1 : 31;
-    const V cin = __shfl_sync(0xffffffffu, S, m0);
-    if (has_flag) {
-      if (later) {
-        axpby_store(y + row, tail + Sm, alpha, beta, bz);
-      } else {  // the tile's last row: may continue into the next tile
-        open_sum[t] = tail + (lane < 31 ? Sm : V(0));
-        open_row[t] = row;
-      }
-    }
-    if (lane == 0) {
-      carry_in[t] = cin;
-      if (!fmask) open_row[t] = -1;
-    }
+    tile_finish<I, V, K>(rp, n, nnz, t, lane, f, r0, p, y, alpha, beta, bz, carry_in, open_sum, open_row);
   }
 }
 
@@ -286,7 +329,7 @@ spops_status_t analyse_t(Context* ctx, Matrix* A) {
   return SPOPS_OK;
 }
 
-template <typename I, typename V, int K, int kMinBlocks>
+template <typename I, typename V, int K, int kMinBlocks, bool kPipe>
 spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
   const CsrTiles& D = A->plan.tiles;
   const bool bz = beta == 0.0;
@@ -294,14 +337,14 @@ spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, doub
     static int blocks_per_sm = -1;  // per instantiation
     if (blocks_per_sm < 0) {
       int bps = 0;
-      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_kernel<I, V, K, kMinBlocks>,
+      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_kernel<I, V, K, kMinBlocks, kPipe>,
                                                                kTileBlock, 0));
       blocks_per_sm = bps > 0 ? bps : 1;
     }
     int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
     const int64_t need = (D.tiles + kTileBlock / 32 - 1) / (kTileBlock / 32);
     if (grid > need) grid = need;
-    csr_tile_kernel<I, V, K, kMinBlocks><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
+    csr_tile_kernel<I, V, K, kMinBlocks, kPipe><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
         A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), A->val.as<V>(), D.tile_row.as<int64_t>(),
         D.flags.as<uint8_t>(), D.tiles, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, bz,
         D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>());
@@ -316,12 +359,15 @@ spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, doub
   return SPOPS_OK;
 }
 
-// K for a (value type, variant): 4 entries per lane (one 256-bit value load
-// for FP64) or 8.
+// Kernel shape by variant: (entries per lane, resident blocks, pipelined).
 template <typename I, typename V>
-spops_status_t dispatch(Context* ctx, Matrix* A, int k, double alpha, const void* x, double beta, void* y) {
-  if (k == 8) return spmv_t<I, V, 8, 4>(ctx, A, alpha, x, beta, y);
-  return spmv_t<I, V, 4, 4>(ctx, A, alpha, x, beta, y);
+spops_status_t dispatch(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y) {
+  switch (variant) {
+    case 1: return spmv_t<I, V, 8, 4, false>(ctx, A, alpha, x, beta, y);
+    case 5: return spmv_t<I, V, 4, 4, false>(ctx, A, alpha, x, beta, y);
+    case 6: return spmv_t<I, V, 8, 5, false>(ctx, A, alpha, x, beta, y);
+    default: return spmv_t<I, V, 8, 3, true>(ctx, A, alpha, x, beta, y);
+  }
 }
 
 }  // namespace
@@ -334,10 +380,13 @@ void CsrTiles::release() {
   ready = false;
 }
 
-bool csr_tile_usable(const Matrix* A, int k) {
+int csr_tile_k(int variant) { return variant == 5 ? 4 : 8; }
+
+bool csr_tile_usable(const Matrix* A, int variant) {
   // vector loads need each lane's run aligned: run bytes (capped at 32)
-  const size_t ca = (size_t)k * A->isize() >= 32 ? 32 : (size_t)k * A->isize();
-  const size_t va = (size_t)k * A->vsize() >= 32 ? 32 : (size_t)k * A->vsize();
+  const size_t k = (size_t)csr_tile_k(variant);
+  const size_t ca = k * A->isize() >= 32 ? 32 : k * A->isize();
+  const size_t va = k * A->vsize() >= 32 ? 32 : k * A->vsize();
   return ((uintptr_t)A->col.p % ca) == 0 && ((uintptr_t)A->val.p % va) == 0;
 }
 
@@ -347,13 +396,15 @@ spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k) {
   return i32 ? analyse_t<int32_t, 4>(ctx, A) : analyse_t<int64_t, 4>(ctx, A);
 }
 
-spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int k, double alpha, const void* x, double beta, void* y) {
+spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta,
+                             void* y) {
+  const int k = csr_tile_k(variant);
   if (!A->plan.tiles.ready || A->plan.tiles.k != k) SPOPS_TRY(csr_tile_analyse(ctx, A, k));
   const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
-  if (i32 && f64) return dispatch<int32_t, double>(ctx, A, k, alpha, x, beta, y);
-  if (i32) return dispatch<int32_t, float>(ctx, A, k, alpha, x, beta, y);
-  if (f64) return dispatch<int64_t, double>(ctx, A, k, alpha, x, beta, y);
-  return dispatch<int64_t, float>(ctx, A, k, alpha, x, beta, y);
+  if (i32 && f64) return dispatch<int32_t, double>(ctx, A, variant, alpha, x, beta, y);
+  if (i32) return dispatch<int32_t, float>(ctx, A, variant, alpha, x, beta, y);
+  if (f64) return dispatch<int64_t, double>(ctx, A, variant, alpha, x, beta, y);
+  return dispatch<int64_t, float>(ctx, A, variant, alpha, x, beta, y);
 }
 
 }  // namespace spops
