@@ -243,9 +243,9 @@ spops_status_t csr_analyse(Context* ctx, Matrix* A);
 spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y);
 // tile kernel (spmv_csr_tile.cu); usable when the column and value arrays are
 // aligned for the lane's vector loads
-bool csr_tile_usable(const Matrix* A, int k);
+bool csr_tile_usable(const Matrix* A, int variant);
 spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k);
-spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int k, double alpha, const void* x, double beta, void* y);
+spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y);
 
 // formats.cu
 spops_status_t convert_from_csr(Context* ctx, Matrix* A, spops_format_t fmt, const spops_format_params_t& p,
