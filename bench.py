@@ -185,6 +185,288 @@ def cpu_reference_sample(rp, ci, v, x, budget_s=10.0, threads=None):
                                    sample=f"rows [0,{m}) of {n} ({int(rps[-1])} nnz), {iters} SpMV")
 
 
+# ---------------------------------------------------------------- extras
+# The other parts of the headline metric, each measured on the device with
+# CUDA events against a "plain" path through the same library: per-format
+# SpMV on the power-law matrix, batched SpMV/SpMM against per-matrix
+# launches, fwd+bwd SpMV against a path that rebuilds the transpose, and the
+# LeSpGEMM pipeline on the planted-community matrix.
+
+def _ev_ms(fn, reps, warm=3):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _graph_ms(fn, reps, ctx):
+    """Device time of `fn` (a sequence of library launches) replayed from a
+    CUDA graph, i.e. without host issue overhead.  None if capture fails."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    try:
+        with torch.cuda.stream(s):
+            ctx.follow_torch()
+            g.capture_begin()
+            try:
+                fn()
+            finally:
+                g.capture_end()
+        ctx.follow_torch()
+        return _ev_ms(g.replay, reps, warm=2)
+    except Exception as e:  # report eager timing instead
+        log(f"graph capture failed: {e}")
+        torch.cuda.synchronize()
+        ctx.follow_torch()
+        return None
+
+
+def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
+    """SpMV of the power-law matrix in each format (GB/s on the CSR algorithmic
+    bytes; error componentwise against the CSR result over |A||x|)."""
+    import torch
+    from sparseops_b200 import CSR_Matrix
+    from sparseops_b200 import formats as F
+    from sparseops_b200._lib import call, dbl, vp
+    out = {}
+    absA = CSR_Matrix(n, n, A.row_offset, A.col_index, np.abs(A.values))
+    den = torch.zeros(n, dtype=torch.float64, device=dev)
+    xa = xd.abs()
+    call("spops_spmv", ctx.handle, dbl(1.0), absA.device(ctx).handle, vp(xa.data_ptr()), dbl(0.0),
+         vp(den.data_ptr()))
+    torch.cuda.synchronize()
+    del absA
+    cands = [
+        ("csr5", lambda: F.csr_to_csr5(A), F.SpOps_csr5),
+        ("sell_c_sigma C=32 sigma=512 col-major", lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.ColMajor),
+         F.SpOps_sell_c_sigma),
+        ("sell_c_sigma C=32 sigma=512 row-major", lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.RowMajor),
+         F.SpOps_sell_c_sigma),
+        ("sell_c_R C=32 col-major", lambda: F.csr_to_sell_c_R(A, None, 32, 1, F.ColMajor), F.SpOps_sell_c_R),
+        ("ell", lambda: F.csr_to_ell(A, F.ColMajor), F.SpOps_ell),
+    ]
+    for name, conv, op in cands:
+        try:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            M = conv()
+            torch.cuda.synchronize()
+            tconv = (time.perf_counter() - t0) * 1e3
+            y = torch.zeros(n, dtype=torch.float64, device=dev)
+            op(1.0, M, xd, 0.0, y)
+            torch.cuda.synchronize()
+            err = float(((y - yref).abs() / den.clamp_min(1e-300)).max())
+            ms = _ev_ms(lambda: op(1.0, M, xd, 0.0, y), 200)
+            out[name] = {"ms": round(ms, 4), "GB/s": round(nbytes / ms / 1e6, 1),
+                         "frac": round(nbytes / ms / 1e6 / peak, 4), "rel_err": err,
+                         "convert_ms": round(tconv, 2)}
+            del M, y
+        except Exception as e:
+            out[name] = {"unavailable": str(e)[:160]}
+    return out
+
+
+def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024):
+    """256 banded-plus-random matrices, n log-uniform in [1e3, 2e5], Poisson(16)
+    per row; one persistent graph-captured launch against per-matrix launches."""
+    import torch
+    from sparseops_b200 import Batch, CSR_Matrix, synth
+    from sparseops_b200._lib import call, dbl, i64, vp
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(2e5), count)).astype(np.int64)
+    mats, hs = [], []
+    tot_rows = tot_nnz = 0
+    for m, n in enumerate(ns):
+        rp, ci, v = synth.banded_random(int(n), 16.0, 64, seed=5000 + m)
+        M = CSR_Matrix(int(n), int(n), torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
+                       torch.from_numpy(v).to(dev))
+        mats.append(M)
+        hs.append(M.device(ctx))
+        tot_rows += int(n)
+        tot_nnz += len(ci)
+    res = {"matrices": count, "rows": tot_rows, "nnz": tot_nnz}
+    for k in ks:
+        X = [torch.rand(int(n), k, dtype=torch.float64, device=dev) * 2 - 1 for n in ns]
+        Yb = [torch.zeros(int(n), k, dtype=torch.float64, device=dev) for n in ns]
+        Xc = [x.t().contiguous() for x in X]  # column j of X contiguous (the per-column loop)
+        Yc = [torch.zeros(k, int(n), dtype=torch.float64, device=dev) for n in ns]
+        Ym = [torch.zeros(int(n), k, dtype=torch.float64, device=dev) for n in ns]
+        if k == 1:
+            X = [x.reshape(-1) for x in X]
+            Yb = [y.reshape(-1) for y in Yb]
+
+        def plain_cols():
+            for h, xc, yc in zip(hs, Xc, Yc):
+                for j in range(k):
+                    call("spops_spmv", ctx.handle, dbl(1.0), h.handle, vp(xc[j].data_ptr()), dbl(0.0),
+                         vp(yc[j].data_ptr()))
+
+        def plain_spmm():
+            for h, x, y in zip(hs, X, Ym):
+                call("spops_spmm", ctx.handle, dbl(1.0), h.handle, vp(x.data_ptr()), i64(k), i64(k), dbl(0.0),
+                     vp(y.data_ptr()), i64(k))
+
+        ctx.follow_torch()
+        eager_cols = _ev_ms(plain_cols, 3, warm=1)
+        graph_cols = _graph_ms(plain_cols, 5, ctx)
+        r = {"plain_per_column_eager_ms": round(eager_cols, 3),
+             "plain_per_column_graph_ms": None if graph_cols is None else round(graph_cols, 3)}
+        if k > 1:
+            r["plain_per_matrix_spmm_ms"] = round(_ev_ms(plain_spmm, 5, warm=2), 3)
+        B = Batch(mats, k=k, ctx=ctx)
+        B.set_vectors(X, Yb)
+        B.tune()
+        B.capture(1.0, 0.0)
+        bms = _ev_ms(B.run, 20)
+        torch.cuda.synchronize()
+        plain_cols()
+        torch.cuda.synchronize()
+        num = max(float((yb.reshape(-1, k) - yc.t()).abs().max()) for yb, yc in zip(Yb, Yc))
+        dnm = max(float(yc.abs().max()) for yc in Yc)
+        nbytes = sum(4 * (int(n) + 1) for n in ns) + 12 * tot_nnz + 16 * k * tot_rows
+        best_plain = min(v for v in (graph_cols, eager_cols) if v is not None)
+        r.update({"batched_ms": round(bms, 3), "batched_GB/s": round(nbytes / bms / 1e6, 1),
+                  "speedup_vs_per_column": round(best_plain / bms, 2),
+                  "normwise_rel_err_vs_plain": num / max(dnm, 1e-300)})
+        if k > 1:
+            r["speedup_vs_per_matrix_spmm"] = round(r["plain_per_matrix_spmm_ms"] / bms, 2)
+        items, choice, kt = B.info()
+        r["tuned"] = {"work_items": int(items), "rhs_tile": int(kt),
+                      "formats": {str(c): int(np.sum(np.asarray(choice) == c)) for c in sorted(set(choice))}}
+        res[f"k={k}"] = r
+        del B, X, Yb, Xc, Yc, Ym
+        torch.cuda.empty_cache()
+    return res
+
+
+def bench_fwd_bwd(ctx, dev, n=1 << 20):
+    """y = A(v) x, then grad_x = A^T g and grad_v = g_i x_j: the adjoint kernels
+    (cached device transpose, fused SDDMM) against a plain path that builds the
+    transpose as a new CSR matrix every step (the reference's csr_transpose
+    route) and forms grad_v elementwise."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, synth
+    from sparseops_b200._lib import call, dbl, vp
+    from sparseops_b200.autograd import SparsePattern, spmv
+    rp, ci, v = synth.symmetric_graph(n, 32.0, seed=4)
+    nnz = len(ci)
+    rpt, cit = torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev)
+    rows = torch.repeat_interleave(torch.arange(n, device=dev, dtype=torch.int32), torch.diff(rpt.long()))
+    out = {"rows": n, "nnz": nnz}
+    for dt, name in ((torch.float64, "f64"), (torch.float32, "f32")):
+        vt = torch.from_numpy(v).to(dev).to(dt)
+        x = (torch.rand(n, device=dev, dtype=torch.float64) * 2 - 1).to(dt)
+        g = torch.randn(n, device=dev, dtype=torch.float64).to(dt)
+        pat = SparsePattern(n, n, rpt, cit, vt)
+        h = pat.handle
+        y, gx, gv = (torch.empty(n, dtype=dt, device=dev), torch.empty(n, dtype=dt, device=dev),
+                     torch.empty(nnz, dtype=dt, device=dev))
+
+        def ours():
+            call("spops_matrix_touch", h.handle)  # values changed (an optimizer step)
+            call("spops_spmv", ctx.handle, dbl(1.0), h.handle, vp(x.data_ptr()), dbl(0.0), vp(y.data_ptr()))
+            call("spops_sddmm", ctx.handle, dbl(1.0), h.handle, vp(g.data_ptr()), vp(x.data_ptr()),
+                 vp(gv.data_ptr()))
+            call("spops_spmv_t", ctx.handle, dbl(1.0), h.handle, vp(g.data_ptr()), dbl(0.0), vp(gx.data_ptr()))
+
+        py, pgx = torch.empty(n, dtype=dt, device=dev), torch.empty(n, dtype=dt, device=dev)
+        keep = {}
+
+        def plain():
+            call("spops_spmv", ctx.handle, dbl(1.0), h.handle, vp(x.data_ptr()), dbl(0.0), vp(py.data_ptr()))
+            key, perm = torch.sort(cit, stable=True)
+            trp = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+            trp[1:] = torch.cumsum(torch.bincount(key, minlength=n), 0)
+            AT = CSR_Matrix(n, n, trp, rows[perm].contiguous(), vt[perm].contiguous())
+            call("spops_spmv", ctx.handle, dbl(1.0), AT.device(ctx).handle, vp(g.data_ptr()), dbl(0.0),
+                 vp(pgx.data_ptr()))
+            keep["gv"] = g[rows.long()] * x[cit.long()]
+            keep["AT"] = AT
+
+        ctx.follow_torch()
+        t_ours = _ev_ms(ours, 20)
+        t_plain = _ev_ms(plain, 5)
+        torch.cuda.synchronize()
+        # the user-facing torch.autograd.Function, forward + backward
+        vp_ = vt.clone().requires_grad_(True)
+        xp_ = x.clone().requires_grad_(True)
+
+        def autograd_step():
+            vp_.grad = None
+            xp_.grad = None
+            yy = spmv(vp_, xp_, pat)
+            yy.backward(g)
+
+        t_auto = _ev_ms(autograd_step, 10)
+        ours()
+        plain()
+        torch.cuda.synchronize()
+
+        def rel(a, b):
+            return float((a.double() - b.double()).abs().max() / b.double().abs().max().clamp_min(1e-300))
+        out[name] = {"ours_ms": round(t_ours, 4), "plain_ms": round(t_plain, 4),
+                     "speedup_vs_plain": round(t_plain / t_ours, 2), "autograd_ms": round(t_auto, 4),
+                     "normwise_rel_err": {"y": rel(y, py), "grad_x": rel(gx, pgx), "grad_v": rel(gv, keep["gv"])}}
+        del pat, keep
+        torch.cuda.empty_cache()
+    return out
+
+
+def bench_spgemm(dev, cpu_ref: bool, n=524288):
+    """LeSpGEMM C = A A^T on the planted-community matrix (2,048 communities,
+    85 % in-community, row nnz lognormal mean 20): MinHash (64), LSH (16
+    bands), clustering (8), cluster-wise kernel-3 SpGEMM."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, synth
+    from sparseops_b200.spgemm import LeSpGEMM_clustered, LeSpGEMM_lsh
+    arp, aci, av = synth.planted_communities(n, ncomm=2048, mean=20.0, seed=5)
+    brp, bci, bv = synth.transpose(arp, aci, av, n)
+    A = CSR_Matrix(n, n, torch.from_numpy(arp).to(dev), torch.from_numpy(aci).to(dev), torch.from_numpy(av).to(dev))
+    B = CSR_Matrix(n, n, torch.from_numpy(brp).to(dev), torch.from_numpy(bci).to(dev), torch.from_numpy(bv).to(dev))
+    C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)  # warm-up
+    torch.cuda.synchronize()
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
+    torch.cuda.synchronize()
+    total = (time.perf_counter() - t0) * 1e3 / reps
+    st = C.stats
+    flops = st["flops"]
+    out = {"rows": n, "nnz_A": int(len(aci)), "nnz_C": int(C.num_nnzs), "flops": int(flops),
+           "pipeline_ms": round(total, 3), "pipeline_GFLOP/s": round(flops / total / 1e6, 2),
+           "stages_ms": {k: round(st[k], 3) for k in st if k.endswith("_ms")},
+           "clusters": st.get("clusters"), "dense_clusters": st.get("dense_clusters")}
+    # the SpGEMM proper (symbolic + numeric + to CSR) for a fixed clustering
+    from sparseops_b200.spgemm import hierarchical_clustering_v0_fast, lsh_candidate_pairs_vector
+    pairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
+    perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
+    kms = _ev_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 3, warm=1)
+    out["spgemm_clustered_ms"] = round(kms, 3)
+    out["spgemm_clustered_GFLOP/s"] = round(flops / kms / 1e6, 2)
+    if cpu_ref:
+        try:
+            from oracle import Reference, reference_available
+            if reference_available():
+                R = Reference(threads=os.cpu_count())
+                ms = R.spgemm_kernel3_time((arp, aci, av), (brp, bci, bv), perm, offs, iters=2)
+                out["cpu_reference_kernel3"] = {"ms": round(ms, 2), "GFLOP/s": round(flops / ms / 1e6, 2),
+                                                "cores": os.cpu_count(), "kind": "reference"}
+        except Exception as e:
+            out["cpu_reference_kernel3"] = {"error": str(e)[:160]}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -325,6 +607,19 @@ def run_ours(args):
             cpu = dict(value=round(gbs, 3), unit="GB/s", **info)
         except Exception as e:  # keep the line even if the baseline cannot run
             cpu = {"value": None, "unit": "GB/s", "error": str(e)[:200]}
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        for key, fn in (("formats", lambda: bench_formats(A, ctx, xd, yd, n, nnz, nbytes, peak, dev)),
+                        ("batched", lambda: bench_batched(ctx, dev)),
+                        ("fwd_bwd", lambda: bench_fwd_bwd(ctx, dev)),
+                        ("spgemm", lambda: bench_spgemm(dev, not args.no_cpu_baseline))):
+            t0 = time.time()
+            try:
+                extra[key] = fn()
+            except Exception as e:
+                extra[key] = {"error": str(e)[:200]}
+            log(f"{key}: {time.time() - t0:.1f}s")
+            torch.cuda.empty_cache()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -352,6 +647,7 @@ def run_ours(args):
         "clocks": ck,
         "cpu_baseline": cpu,
     }
+    out.update(extra)
     print(json.dumps(out))
     return 0
 
@@ -364,6 +660,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the per-format, batched, fwd+bwd and SpGEMM sections")
     ap.add_argument("--csr-variant", type=int, default=0, help="CSR kernel shape (spops_set_option)")
     ap.add_argument("--rows", type=int, default=N_ROWS,
                     help="matrix rows (default: the benchmark size; smaller only for profiling captures)")

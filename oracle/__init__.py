@@ -283,6 +283,19 @@ class Reference:
         self.L.ref_csr_free(_vp(h))
         return dict(rp=rp, ci=ci[:info[2]], v=v[:info[2]], dense_clusters=int(info[3]), clusters=int(info[4]))
 
+    def spgemm_kernel3_time(self, A, B, perm, offsets, iters=3, l2_fraction=-1.0):
+        """Mean ms of the reference's LeSpGEMM_VLength kernel 3 (numeric and
+        symbolic phases on the clustered A) over `iters` runs."""
+        arp, aci, av = A
+        brp, bci, bv = B[:3]
+        n = len(arp) - 1
+        bcols = int(B[3]) if len(B) > 3 else n
+        self.L.ref_spgemm_kernel3_time.restype = C.c_double
+        return float(self.L.ref_spgemm_kernel3_time(
+            _i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av), _i64(len(brp) - 1),
+            _i64(bcols), _i64(len(bci)), _p(brp), _p(bci), _p(bv), _p(perm), _p(offsets), _i64(len(offsets) - 1),
+            C.c_int(int(iters)), _dbl(l2_fraction)))
+
     def csr_transpose(self, rp, ci, v, ncols):
         h = self.L.ref_csr_transpose(_i64(len(rp) - 1), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _p(v))
         info = np.zeros(6, np.int64)
