@@ -520,6 +520,25 @@ def run_reference(args):
     return 0
 
 
+def run_section(args):
+    """One extra section alone (for profiling captures); prints its JSON."""
+    import torch
+    from sparseops_b200 import default_context
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    ctx = default_context(0)
+    if args.section == "batched":
+        res = bench_batched(ctx, dev)
+    elif args.section == "fwd_bwd":
+        res = bench_fwd_bwd(ctx, dev)
+    elif args.section == "spgemm":
+        res = bench_spgemm(dev, not args.no_cpu_baseline)
+    else:
+        raise SystemExit(f"unknown section {args.section}")
+    print(json.dumps({"section": args.section, args.section: res}))
+    return 0
+
+
 def run_ours(args):
     import torch
     import ctypes as C
@@ -660,6 +679,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--section", default="all", choices=["all", "batched", "fwd_bwd", "spgemm"],
+                    help="run one extra section alone (profiling); the headline line needs 'all'")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-format, batched, fwd+bwd and SpGEMM sections")
     ap.add_argument("--csr-variant", type=int, default=0, help="CSR kernel shape (spops_set_option)")
@@ -670,6 +691,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.section != "all":
+        return run_section(args)
     return run_ours(args)
 
 

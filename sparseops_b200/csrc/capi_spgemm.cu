@@ -2,6 +2,8 @@
 // hierarchical clustering and the cluster-wise SpGEMM.
 #include <chrono>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "spops_internal.h"
@@ -186,19 +188,26 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   s.lsh_ms = ms_since(t0);
   s.pairs = P.count;
   t0 = std::chrono::steady_clock::now();
+  const bool trace = std::getenv("SPOPS_TRACE") && std::getenv("SPOPS_TRACE")[0] == '1';
+  auto lap = [&](const char* what) {
+    if (trace) std::fprintf(stderr, "[spgemm_lsh] %-24s %9.3f ms\n", what, ms_since(t0));
+  };
   std::vector<int64_t> rp, ci, pi((size_t)P.count), pj((size_t)P.count), perm, offs;
   std::vector<double> ps((size_t)P.count);
   st = host_pattern(ctx, A, rp, ci);
+  lap("pattern to host");
   if (st == SPOPS_OK && P.count) {
     cudaMemcpy(pi.data(), P.pi.p, pi.size() * 8, cudaMemcpyDeviceToHost);
     cudaMemcpy(pj.data(), P.pj.p, pj.size() * 8, cudaMemcpyDeviceToHost);
     cudaMemcpy(ps.data(), P.score.p, ps.size() * 8, cudaMemcpyDeviceToHost);
   }
   P.release();
+  lap("pairs to host");
   if (st == SPOPS_OK)
     st = hierarchical_clustering(rp.data(), ci.data(), A->rows, pi.data(), pj.data(), ps.data(), (int64_t)pi.size(),
                                  cluster_size, perm, offs);
   if (st != SPOPS_OK) return st;
+  lap("clustering");
   s.hc_ms = ms_since(t0);
   Matrix* out = nullptr;
   SpgemmStats s2;

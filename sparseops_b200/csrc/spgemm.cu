@@ -38,6 +38,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -238,6 +240,217 @@ struct NumSlot {   // per-cluster arena layout (elements)
   int64_t lsize;   // sort list length (power of two >= nz)
 };
 
+// ------------------------------------------------- warp-per-cluster phases
+// Clusters with at most 32 distinct A columns and small tables run one warp
+// each, several per block, with the table in the warp's slice of shared
+// memory.  All (column j, B entry k) products of the cluster are visited in
+// one flat, lane-parallel sweep: lane j holds B row j's start and the
+// exclusive prefix of the row lengths, and product t finds its j by a 5-step
+// shuffle search -- so every B entry load of the cluster is issued at once
+// instead of one B row at a time.
+struct WarpRows {
+  int64_t start;  // B row start of this lane's column (lane < nj)
+  int64_t off;    // products before it
+  int64_t total;  // products of the cluster
+};
+
+template <typename I>
+__device__ __forceinline__ WarpRows warp_rows(const int64_t* __restrict__ cptr, const int32_t* __restrict__ colids,
+                                              int64_t c, const I* __restrict__ brp, int lane) {
+  const int64_t j0 = cptr[c], nj = cptr[c + 1] - j0;
+  int64_t st = 0, len = 0;
+  if (lane < nj) {
+    const int64_t r = colids[j0 + lane];
+    st = brp[r];
+    len = (int64_t)brp[r + 1] - st;
+  }
+  int64_t inc = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  return WarpRows{st, inc - len, __shfl_sync(0xffffffffu, inc, 31)};
+}
+
+// the column j (0..nj-1) holding flat product t: the largest j with off_j <= t
+__device__ __forceinline__ int warp_find_row(const WarpRows& w, int64_t nj, int64_t t) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    const int cand = lo + step;
+    const int64_t oc = __shfl_sync(0xffffffffu, w.off, cand & 31);
+    if (cand < nj && oc <= t) lo = cand;
+  }
+  return lo;
+}
+
+template <typename I>
+__global__ void symbolic_warp_kernel(const int64_t* __restrict__ list, int64_t nlist, const int64_t* __restrict__ tsizes,
+                                     int64_t warp_tab, const int64_t* __restrict__ cptr,
+                                     const int32_t* __restrict__ colids, const I* __restrict__ brp,
+                                     const I* __restrict__ bci, int64_t* __restrict__ nz, int64_t* __restrict__ cmin,
+                                     int64_t* __restrict__ cmax) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t b = blockIdx.x * (int64_t)(blockDim.x >> 5) + w;
+  if (b >= nlist) return;
+  const int64_t c = list[b];
+  const int64_t tsize = tsizes[b];
+  int32_t* tab = reinterpret_cast<int32_t*>(sm) + (int64_t)w * warp_tab;
+  const uint32_t mask = (uint32_t)(tsize - 1);
+  for (int64_t t = lane; t < tsize; t += 32) tab[t] = -1;
+  __syncwarp();
+  const WarpRows wr = warp_rows(cptr, colids, c, brp, lane);
+  const int64_t nj = cptr[c + 1] - cptr[c];
+  unsigned long long cnt = 0;
+  int mn = INT32_MAX, mx = -1;
+  for (int64_t base = 0; base < wr.total; base += 32) {
+    const int64_t t = base + lane;
+    const int j = warp_find_row(wr, nj, t);
+    const int64_t st = __shfl_sync(0xffffffffu, wr.start, j), of = __shfl_sync(0xffffffffu, wr.off, j);
+    if (t < wr.total) {
+      const int32_t key = (int32_t)bci[st + (t - of)];
+      if (hash_insert(tab, mask, key)) {
+        ++cnt;
+        mn = key < mn ? key : mn;
+        mx = key > mx ? key : mx;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  if (lane == 0) {
+    nz[c] = (int64_t)cnt;
+    cmin[c] = cnt ? mn : 0;
+    cmax[c] = cnt ? mx : 0;
+  }
+}
+
+// Numeric phase, one warp per cluster.  Warp arena (bytes at w * warp_bytes):
+// tab (int32, tsize) | pos (int32, tsize) | keys (int32, nz) | acc (V, nz*csz).
+// Columns are ranked by counting (rank = number of smaller columns), which
+// gives the ascending output order and each column's accumulator row.  The
+// products are accumulated in flat (j, k) order, 32 at a time; products of one
+// sweep that hit the same column are first summed in lane order (= ascending
+// j) and added by the lowest lane, so the per-column summation order depends
+// only on the matrices.
+template <typename I, typename V>
+__global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nlist, const NumSlot* __restrict__ slots,
+                                    int64_t warp_bytes, const int64_t* __restrict__ cptr,
+                                    const int64_t* __restrict__ cptr_val, const int32_t* __restrict__ colids,
+                                    const V* __restrict__ avals, const int64_t* __restrict__ offsets,
+                                    const I* __restrict__ brp, const I* __restrict__ bci, const V* __restrict__ bv,
+                                    const int64_t* __restrict__ nz, const int64_t* __restrict__ ccptr,
+                                    const int64_t* __restrict__ ccptr_val, const unsigned char* __restrict__ drop_small,
+                                    int32_t* __restrict__ ccol, V* __restrict__ cval) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  constexpr int kMaxPerLane = 16;  // nz <= 512
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t b = blockIdx.x * (int64_t)(blockDim.x >> 5) + w;
+  if (b >= nlist) return;
+  const int64_t c = list[b];
+  const NumSlot S = slots[b];
+  const int64_t nzc = nz[c];
+  const int64_t csz = offsets[c + 1] - offsets[c];
+  unsigned char* base = sm + (int64_t)w * warp_bytes;
+  int32_t* tab = reinterpret_cast<int32_t*>(base);
+  int32_t* pos = tab + S.tsize;
+  int32_t* keys = pos + S.tsize;
+  V* acc = reinterpret_cast<V*>(base + ((4 * (2 * S.tsize + nzc) + 15) & ~15LL));
+  const uint32_t mask = (uint32_t)(S.tsize - 1);
+  for (int64_t t = lane; t < S.tsize; t += 32) tab[t] = -1;
+  for (int64_t t = lane; t < nzc * csz; t += 32) acc[t] = V(0);
+  __syncwarp();
+  const WarpRows wr = warp_rows(cptr, colids, c, brp, lane);
+  const int64_t j0 = cptr[c], nj = cptr[c + 1] - j0;
+  // 1. distinct columns
+  for (int64_t b0 = 0; b0 < wr.total; b0 += 32) {
+    const int64_t t = b0 + lane;
+    const int j = warp_find_row(wr, nj, t);
+    const int64_t st = __shfl_sync(0xffffffffu, wr.start, j), of = __shfl_sync(0xffffffffu, wr.off, j);
+    if (t < wr.total) hash_insert(tab, mask, (int32_t)bci[st + (t - of)]);
+  }
+  __syncwarp();
+  // 2. compact (slot order)
+  int64_t n = 0;
+  for (int64_t t0 = 0; t0 < S.tsize; t0 += 32) {
+    const int32_t v = t0 + lane < S.tsize ? tab[t0 + lane] : -1;
+    const unsigned m = __ballot_sync(0xffffffffu, v != -1);
+    if (v != -1) keys[n + __popc(m & ((1u << lane) - 1u))] = v;
+    n += __popc(m);
+  }
+  __syncwarp();
+  // 3. rank by counting; the output column list is written in rank order
+  int32_t mine[kMaxPerLane];
+  int rank[kMaxPerLane];
+#pragma unroll
+  for (int q = 0; q < kMaxPerLane; ++q) {
+    const int64_t p = lane + 32 * q;
+    mine[q] = p < nzc ? keys[p] : INT32_MAX;
+    rank[q] = 0;
+  }
+  for (int64_t p = 0; p < nzc; ++p) {
+    const int32_t kq = keys[p];
+#pragma unroll
+    for (int q = 0; q < kMaxPerLane; ++q) rank[q] += kq < mine[q] ? 1 : 0;
+  }
+  const int64_t co = ccptr[c], cvo = ccptr_val[c];
+#pragma unroll
+  for (int q = 0; q < kMaxPerLane; ++q) {
+    const int64_t p = lane + 32 * q;
+    if (p < nzc) {
+      pos[hash_find(tab, mask, mine[q])] = rank[q];
+      ccol[co + rank[q]] = mine[q];
+    }
+  }
+  __syncwarp();
+  // 4. accumulate in flat (j, k) order
+  const int64_t vbase = cptr_val[c];
+  for (int64_t b0 = 0; b0 < wr.total; b0 += 32) {
+    const int64_t t = b0 + lane;
+    const int j = warp_find_row(wr, nj, t);
+    const int64_t st = __shfl_sync(0xffffffffu, wr.start, j), of = __shfl_sync(0xffffffffu, wr.off, j);
+    const bool valid = t < wr.total;
+    int32_t p = -1 - lane;  // distinct for idle lanes
+    V bval = V(0);
+    if (valid) {
+      const int64_t k = st + (t - of);
+      p = pos[hash_find(tab, mask, (int32_t)bci[k])];
+      bval = bv[k];
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, p);
+    const int leader = __ffs(grp) - 1;
+    for (int64_t l = 0; l < csz; ++l) {
+      const V v = valid ? avals[vbase + (int64_t)j * csz + l] * bval : V(0);
+      V sum = v;
+      if (grp != (1u << lane)) {  // several products of this sweep hit the column: sum in lane order
+        sum = V(0);
+        for (unsigned m = grp; m; m &= m - 1) sum += __shfl_sync(grp, v, __ffs(m) - 1);
+      }
+      if (valid && lane == leader) acc[p * csz + l] += sum;
+    }
+    __syncwarp();
+  }
+  // 5. drop rule and output (values in rank order, rows of the cluster interleaved)
+  const bool drop = drop_small[c] != 0;
+  for (int64_t p = lane; p < nzc; p += 32) {
+    bool small = drop;
+    if (drop)
+      for (int64_t l = 0; l < csz; ++l)
+        if (fabs((double)acc[p * csz + l]) >= 1e-12) {
+          small = false;
+          break;
+        }
+    for (int64_t l = 0; l < csz; ++l) cval[cvo + p * csz + l] = small ? V(0) : acc[p * csz + l];
+  }
+}
+
+
 template <typename I, typename V>
 __global__ void numeric_kernel(const int64_t* __restrict__ list, int64_t nlist, const NumSlot* __restrict__ slots,
                                const int64_t* __restrict__ cptr, const int64_t* __restrict__ cptr_val,
@@ -409,6 +622,24 @@ spops_status_t h2d(cudaStream_t st, DevBuf& d, const std::vector<T>& h) {
   return SPOPS_OK;
 }
 
+// SPOPS_TRACE=1 in the environment: wall time of each step of the SpGEMM
+// driver on stderr (the stream is synchronised at every mark).
+struct Trace {
+  bool on = false;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  Trace() {
+    const char* e = std::getenv("SPOPS_TRACE");
+    on = e && e[0] == '1';
+  }
+  void mark(cudaStream_t st, const char* what) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    const auto n = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[spgemm] %-28s %9.3f ms\n", what, std::chrono::duration<double, std::milli>(n - t).count());
+    t = n;
+  }
+};
+
 struct Timer {
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
   double lap(cudaStream_t st) {
@@ -426,6 +657,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   cudaStream_t st = ctx->stream;
   const int64_t n = A->rows, nnz = A->nnz;
   Timer tm;
+  Trace tr;
   // --- permutation, offsets, per-row cluster
   DevBuf perm, offs, rowcl, rlen, rpr, keys, skeys, src, ssrc, flag, uidx, colids, ncols_u, cptr, cptr_val, avals,
       row_of_entry, tmp;
@@ -444,6 +676,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cb, rlen.as<int64_t>(), rpr.as<int64_t>(), (int64_t)nn, st));
   SPOPS_TRY(tmp.alloc(cb + 256));
   SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cb, rlen.as<int64_t>(), rpr.as<int64_t>(), (int64_t)n, st));
+  tr.mark(st, "setup + reordered row scan");
   // --- cluster keys, sort, unique
   SPOPS_TRY(keys.alloc(nz1 * 8));
   SPOPS_TRY(skeys.alloc(nz1 * 8));
@@ -452,6 +685,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(flag.alloc(nz1 * 8));
   SPOPS_TRY(uidx.alloc(nz1 * 8));
   SPOPS_TRY(row_of_entry.alloc(nz1 * 8));
+  tr.mark(st, "alloc key arrays");
   if (n > 0) {
     cluster_keys_kernel<I, V><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), perm.as<int64_t>(),
                                                                 rowcl.as<int64_t>(), n, rpr.as<int64_t>(),
@@ -477,6 +711,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_CUDA(cudaMemcpyAsync(&nnzc, uidx.as<int64_t>() + nnz - 1, 8, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
   }
+  tr.mark(st, "keys + sort + unique");
   SPOPS_TRY(colids.alloc((size_t)std::max<int64_t>(nnzc, 1) * 4));
   if (nnz > 0) {
     cluster_cols_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), flag.as<int64_t>(), uidx.as<int64_t>(),
@@ -494,6 +729,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   }
   SPOPS_TRY(h2d(st, cptr, hcptr));
   SPOPS_TRY(h2d(st, cptr_val, hcptr_val));
+  tr.mark(st, "cluster pointers (host)");
   const int64_t nnzv = hcptr_val[ncl];
   SPOPS_TRY(avals.alloc((size_t)std::max<int64_t>(nnzv, 1) * sizeof(V)));
   SPOPS_CUDA(cudaMemsetAsync(avals.p, 0, avals.bytes, st));
@@ -507,6 +743,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   keys.release(); skeys.release(); src.release(); ssrc.release(); flag.release(); uidx.release();
   row_of_entry.release(); rlen.release(); rpr.release(); rowcl.release();
   if (stats) stats->cluster_ms = tm.lap(st);
+  tr.mark(st, "cluster values + frees");
 
   // --- flops per cluster and symbolic bins
   DevBuf flops, nzd, cmin, cmax;
@@ -521,6 +758,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   }
   std::vector<int64_t> hflops;
   SPOPS_TRY(d2h(st, hflops, flops.p, (size_t)ncl));
+  tr.mark(st, "flops per cluster");
   int64_t total_products = 0;
   {
     DevBuf pc;
@@ -548,9 +786,18 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   sb[0].threads = 32; sb[0].smem = 16 << 10;
   sb[1].threads = 256; sb[1].smem = 128 << 10;
   sb[2].threads = 256; sb[2].global = true;
+  // warp-per-cluster bin: at most 32 distinct A columns, table of <= kSymWarpTab slots
+  constexpr int kSymWarps = 8;
+  constexpr int64_t kSymWarpTab = 2048;
+  std::vector<int64_t> wlist, wtsize;
   int64_t gsym = 0;
   for (int64_t c = 0; c < ncl; ++c) {
     const int64_t ts = sym_tsize(c);
+    if (hcnt[c] <= 32 && ts <= kSymWarpTab) {
+      wlist.push_back(c);
+      wtsize.push_back(ts);
+      continue;
+    }
     const int which = ts * 4 <= (int64_t)sb[0].smem ? 0 : (ts * 4 <= (int64_t)sb[1].smem ? 1 : 2);
     sb[which].list.push_back(c);
     sb[which].tsize.push_back(ts);
@@ -559,8 +806,23 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
       gsym += ts;
     }
   }
+  if (!wlist.empty()) {
+    DevBuf dl, dt;
+    SPOPS_TRY(h2d(st, dl, wlist));
+    SPOPS_TRY(h2d(st, dt, wtsize));
+    const size_t smem = (size_t)kSymWarps * kSymWarpTab * 4;
+    SPOPS_CUDA(cudaFuncSetAttribute(symbolic_warp_kernel<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t blocks = ((int64_t)wlist.size() + kSymWarps - 1) / kSymWarps;
+    symbolic_warp_kernel<I><<<(unsigned)blocks, 32 * kSymWarps, smem, st>>>(
+        dl.as<int64_t>(), (int64_t)wlist.size(), dt.as<int64_t>(), kSymWarpTab, cptr.as<int64_t>(),
+        colids.as<int32_t>(), B->row.as<I>(), B->col.as<I>(), nzd.as<int64_t>(), cmin.as<int64_t>(),
+        cmax.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+  }
   DevBuf gtab;
   if (gsym) SPOPS_TRY(gtab.alloc((size_t)gsym * 4));
+  tr.mark(st, "symbolic bins + warp kernel");
   for (int w = 0; w < 3; ++w) {
     Bin& bn = sb[w];
     if (bn.list.empty()) continue;
@@ -589,6 +851,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     hccptr_val[c + 1] = hccptr_val[c] + hnz[c] * csz;
   }
   if (stats) stats->symbolic_ms = tm.lap(st);
+  tr.mark(st, "symbolic block kernels + nz");
 
   // --- classify (drop rule)
   DevBuf drop, ndense;
@@ -612,6 +875,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(h2d(st, ccptr_val, hccptr_val));
   SPOPS_TRY(ccol.alloc((size_t)std::max<int64_t>(hccptr[ncl], 1) * 4));
   SPOPS_TRY(cval.alloc((size_t)std::max<int64_t>(hccptr_val[ncl], 1) * sizeof(V)));
+  tr.mark(st, "classify + cluster output alloc");
   struct NBin {
     std::vector<int64_t> list, goff;
     std::vector<NumSlot> slots;
@@ -623,6 +887,14 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
                 {{}, {}, {}, 128, 96 << 10, false},
                 {{}, {}, {}, 256, 200 << 10, false},
                 {{}, {}, {}, 256, 0, true}};
+  // warp-per-cluster bins (at most 32 distinct A columns, nz <= 512): arena bytes per warp, warps per block
+  struct WBin {
+    std::vector<int64_t> list;
+    std::vector<NumSlot> slots;
+    int64_t bytes;
+    int warps;
+  };
+  WBin wb[2] = {{{}, {}, 8 << 10, 8}, {{}, {}, 16 << 10, 4}};
   int64_t garena = 0;
   for (int64_t c = 0; c < ncl; ++c) {
     if (hnz[c] == 0) continue;
@@ -630,6 +902,17 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     NumSlot S;
     S.tsize = pow2_at_least(std::max<int64_t>(2 * hnz[c], 2));
     S.lsize = pow2_at_least(std::max<int64_t>(hnz[c], 1));
+    if (hcnt[c] <= 32 && hnz[c] <= 512) {
+      const int64_t wbytes = ((4 * (2 * S.tsize + hnz[c]) + 15) & ~15LL) + hnz[c] * csz * (int64_t)sizeof(V);
+      int w = -1;
+      for (int t = 0; t < 2 && w < 0; ++t)
+        if (wbytes <= wb[t].bytes) w = t;
+      if (w >= 0) {
+        wb[w].list.push_back(c);
+        wb[w].slots.push_back(S);
+        continue;
+      }
+    }
     const int64_t bytes = ((hnz[c] * csz * (int64_t)sizeof(V) + 15) & ~15LL) + 4 * (2 * S.tsize + S.lsize);
     int w = 3;
     for (int t = 0; t < 3; ++t)
@@ -641,8 +924,26 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
       garena += (bytes + 255) & ~255LL;
     }
   }
+  for (int w = 0; w < 2; ++w) {
+    WBin& bn = wb[w];
+    if (bn.list.empty()) continue;
+    DevBuf dl, ds;
+    SPOPS_TRY(h2d(st, dl, bn.list));
+    SPOPS_TRY(h2d(st, ds, bn.slots));
+    const size_t smem = (size_t)bn.warps * (size_t)bn.bytes;
+    SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t blocks = ((int64_t)bn.list.size() + bn.warps - 1) / bn.warps;
+    numeric_warp_kernel<I, V><<<(unsigned)blocks, 32 * bn.warps, smem, st>>>(
+        dl.as<int64_t>(), (int64_t)bn.list.size(), ds.as<NumSlot>(), bn.bytes, cptr.as<int64_t>(),
+        cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
+        B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+        drop.as<unsigned char>(), ccol.as<int32_t>(), cval.as<V>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+  }
   DevBuf arena;
   if (garena) SPOPS_TRY(arena.alloc((size_t)garena));
+  tr.mark(st, "numeric bins + warp kernels");
   for (int w = 0; w < 4; ++w) {
     NBin& bn = nb[w];
     if (bn.list.empty()) continue;
@@ -664,6 +965,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   }
   arena.release();
   if (stats) stats->numeric_ms = tm.lap(st);
+  tr.mark(st, "numeric block kernels");
 
   // --- back to CSR, original row order
   DevBuf rowcnt, crp;
@@ -682,6 +984,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   int64_t cnnz = 0;
   SPOPS_CUDA(cudaMemcpyAsync(&cnnz, crp.as<int64_t>() + n, 8, cudaMemcpyDeviceToHost, st));
   SPOPS_CUDA(cudaStreamSynchronize(st));
+  tr.mark(st, "row counts + scan");
   if (sizeof(I) == 4 && cnnz > INT32_MAX)
     return fail(SPOPS_ERR_TOO_LARGE, "SpGEMM: %lld output entries exceed int32 indices", (long long)cnnz);
   Matrix* C = new spops_matrix_s();
@@ -701,6 +1004,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     return s;
   }
   // row offsets in the index type
+  tr.mark(st, "C alloc");
   std::vector<int64_t> hcrp;
   SPOPS_TRY(d2h(st, hcrp, crp.p, (size_t)n + 1));
   if (sizeof(I) == 8) {
@@ -718,6 +1022,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_LAUNCH_CHECK();
   }
   SPOPS_CUDA(cudaStreamSynchronize(st));
+  tr.mark(st, "row offsets + row write");
   if (stats) {
     stats->to_csr_ms = tm.lap(st);
     stats->flops = 2 * total_products;
