@@ -168,11 +168,86 @@ __global__ void __launch_bounds__(256) padded_kernel(
   const int lane = threadIdx.x & 31;
   const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   if (w < main_warps)
-    padded_rows32<I, V, kColMajor>(w * 32, col, val, chunk_len, chunk_off, row_len, reorder, n, C, x, y, alpha,
-                                   beta, bz, lane);
+    padded_rows32<I, V, kColMajor>(w * 32, col, val, chunk_len, chunk_off, row_len, reorder, n, C, x, y, alpha, beta,
+                                   bz, lane);
   else if (w - main_warps < npieces)
     padded_piece<I, V, kColMajor>(w - main_warps, pieces[w - main_warps], col, val, chunk_len, chunk_off, row_len,
                                   reorder, C, x, y, alpha, beta, bz, partial, counter, lane);
+}
+
+// Column-major SELL with C = 32: one warp per step window of a chunk
+// (padded_window32); windows of one chunk combine their per-row partial sums
+// in window order on the last one to finish.  Long rows go to pieces.
+template <typename I, typename V>
+__global__ void __launch_bounds__(256) padded_win_kernel(
+    const I* __restrict__ col, const V* __restrict__ val, const int64_t* __restrict__ chunk_off,
+    const int* __restrict__ row_len, const I* __restrict__ reorder, int64_t n, const V* __restrict__ x,
+    V* __restrict__ y, V alpha, V beta, bool bz, const PadWin* __restrict__ wins, int64_t nwin,
+    V* __restrict__ wpartial, int* __restrict__ wcounter, int64_t npieces, const PadPiece* __restrict__ pieces,
+    V* __restrict__ partial, int* __restrict__ counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (w >= nwin) {
+    if (w - nwin < npieces)
+      padded_piece<I, V, true>(w - nwin, pieces[w - nwin], col, val, nullptr, chunk_off, row_len, reorder, 32, x, y,
+                               alpha, beta, bz, partial, counter, lane);
+    return;
+  }
+  const PadWin W = wins[w];
+  const int64_t i0 = W.chunk * 32, i = i0 + lane;
+  int len = 0;
+  if (i < n) {
+    len = row_len[i];
+    if (len > kPadLong || len < 0) len = 0;  // long rows: pieces
+  }
+  auto store = [&](int r, V s) {
+    const int64_t row = i0 + r;
+    if (row < n && row_len[row] <= kPadLong)
+      axpby_store(y + (reorder ? (int64_t)reorder[row] : row), s, alpha, beta, bz);
+  };
+  if (W.nw == 1) {
+    padded_window32<I, V>(chunk_off[W.chunk], len, 0, col, val, x, lane, store);
+    return;
+  }
+  V* part = wpartial + (W.first + W.widx) * 32;
+  padded_window32<I, V>(chunk_off[W.chunk], len, W.widx * kPadWindow, col, val, x, lane,
+                        [&](int r, V s) { part[r] = s; });
+  __syncwarp();
+  int last = 0;
+  if (lane == 0) {
+    __threadfence();
+    last = atomicAdd(wcounter + W.chunk, 1) == W.nw - 1;
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (last) {
+    __threadfence();
+    V tot = V(0);
+    for (int q = 0; q < W.nw; ++q) tot += ld_cg(wpartial + (W.first + q) * 32 + lane);
+    store(lane, tot);
+    __syncwarp();
+    if (lane == 0) wcounter[W.chunk] = 0;
+  }
+}
+
+// windows per 32-row chunk: ceil(longest row that is not long / kPadWindow)
+__global__ void pad_win_count_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks,
+                                     int64_t* __restrict__ nw) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t c = t >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= nchunks) return;
+  const int64_t i = c * 32 + lane;
+  int len = i < n ? row_len[i] : 0;
+  if (len > kPadLong || len < 0) len = 0;
+  const unsigned m = __reduce_max_sync(0xffffffffu, (unsigned)len);
+  if (lane == 0) nw[c] = m > (unsigned)kPadWindow ? ((int64_t)m + kPadWindow - 1) / kPadWindow : 1;
+}
+
+__global__ void pad_win_fill_kernel(const int64_t* __restrict__ nw, const int64_t* __restrict__ off, int64_t nchunks,
+                                    PadWin* __restrict__ wins) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= nchunks) return;
+  for (int64_t q = 0; q < nw[c]; ++q) wins[off[c] + q] = PadWin{c, off[c], (int32_t)q, (int32_t)nw[c]};
 }
 
 // ------------------------------------------------------------------ DIA
@@ -596,6 +671,24 @@ spops_status_t padded_finish_t(Context* ctx, Matrix* M) {
     SPOPS_LAUNCH_CHECK();
   }
   SPOPS_CUDA(cudaStreamSynchronize(st));
+  if (P.C == 32 && M->layout == SPOPS_COL_MAJOR && n > 0) {
+    // step windows of the 32-row chunks (np / off reused: one entry per chunk)
+    const int64_t nch = (n + 31) / 32;
+    pad_win_count_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, np);
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, np, off, nch, st));
+    int64_t h[2];
+    SPOPS_TRY(download(ctx, &h[0], off + nch - 1, 1));
+    SPOPS_TRY(download(ctx, &h[1], np + nch - 1, 1));
+    P.nwin = h[0] + h[1];
+    SPOPS_TRY(P.win.alloc((size_t)P.nwin * sizeof(PadWin)));
+    SPOPS_TRY(P.win_partial.alloc((size_t)P.nwin * 32 * sizeof(double)));
+    SPOPS_TRY(P.win_counter.alloc((size_t)nch * sizeof(int)));
+    SPOPS_CUDA(cudaMemsetAsync(P.win_counter.p, 0, P.win_counter.bytes, st));
+    pad_win_fill_kernel<<<grid_for(nch), 256, 0, st>>>(np, off, nch, P.win.as<PadWin>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+  }
   return SPOPS_OK;
 }
 
@@ -608,6 +701,17 @@ spops_status_t padded_spmv_t(Context* ctx, Matrix* A, double alpha, const void* 
   const int64_t grid = (main_warps + P.npieces + 7) / 8;
   if (grid > INT32_MAX) return fail(SPOPS_ERR_TOO_LARGE, "padded SpMV grid");
   const I* ro = P.sorted ? P.reorder.as<I>() : nullptr;
+  if (P.nwin > 0) {
+    const int64_t g = (P.nwin + P.npieces + 7) / 8;
+    if (g > INT32_MAX) return fail(SPOPS_ERR_TOO_LARGE, "padded SpMV grid");
+    padded_win_kernel<I, V><<<(unsigned)g, 256, 0, ctx->stream>>>(
+        A->col.as<I>(), A->val.as<V>(), P.chunk_off.as<int64_t>(), P.row_len.as<int>(), ro, n,
+        static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, P.win.as<PadWin>(), P.nwin,
+        P.win_partial.as<V>(), P.win_counter.as<int>(), P.npieces, P.piece.as<PadPiece>(), P.partial.as<V>(),
+        P.counter.as<int>());
+    SPOPS_LAUNCH_CHECK();
+    return SPOPS_OK;
+  }
   if (A->layout == SPOPS_COL_MAJOR)
     padded_kernel<I, V, true><<<(unsigned)grid, 256, 0, ctx->stream>>>(
         A->col.as<I>(), A->val.as<V>(), P.chunk_len.as<I>(), P.chunk_off.as<int64_t>(), P.row_len.as<int>(), ro, n,

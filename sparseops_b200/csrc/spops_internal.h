@@ -141,6 +141,14 @@ struct PadPiece {
   int32_t npieces;  // pieces of this row
 };
 
+// Step window of a 32-row column-major chunk (see padded_window32).
+struct PadWin {
+  int64_t chunk;   // chunk index
+  int64_t first;   // index of the chunk's first window
+  int32_t widx;    // this window: steps [widx * kPadWindow, +kPadWindow)
+  int32_t nw;      // windows of the chunk
+};
+
 struct PaddedData {
   int64_t C = 0, sigma = 0, align = 1, nchunks = 0, stored = 0;
   bool sorted = false;
@@ -153,9 +161,16 @@ struct PaddedData {
   DevBuf piece;      // PadPiece [npieces]
   DevBuf partial;    // double [npieces]
   DevBuf counter;    // int32 [npieces]
+  // windows of 32-row column-major chunks (C == 32 only)
+  int64_t nwin = 0;
+  DevBuf win;        // PadWin [nwin]
+  DevBuf win_partial;  // double [nwin * 32]
+  DevBuf win_counter;  // int32 [nchunks]
   void release() {
     reorder.release(); chunk_len.release(); chunk_off.release(); row_len.release();
     piece.release(); partial.release(); counter.release();
+    win.release(); win_partial.release(); win_counter.release();
+    nwin = 0;
   }
 };
 

@@ -235,6 +235,103 @@ __device__ __forceinline__ void padded_rows32(int64_t i0, const I* __restrict__ 
   }
 }
 
+// Steps (slots per row) of a 32-row column-major chunk that one warp takes:
+// chunks with longer rows are cut into windows of kPadWindow steps, each its
+// own warp, whose per-row partial sums the last window to finish adds up.
+constexpr int kPadWindow = 128;
+
+// Window [k0, k0 + kPadWindow) of a column-major chunk of exactly 32 rows,
+// with one warp; emit(r, sum) receives the sum of row i0 + r over the window,
+// exactly once per row.  The window's rows are ranked by length (longest
+// first, one bitonic sort across the warp); in phase p = 0..5 the 32 >> p
+// longest unfinished rows get 1 << p lanes each, which take every (1 << p)-th
+// slot, until the row of rank (32 >> p) / 2 runs out; rows that finish in a
+// phase are reduced over their lanes and emitted.  So a window whose rows
+// differ in length (SELL-C-sigma with a small sigma) keeps its lanes busy
+// instead of idling on padding; balanced windows keep one lane per row, as
+// every phase costs a memory round trip.  `len` is the row's slot count
+// (0 for rows handled elsewhere).
+template <typename I, typename V, typename Emit>
+__device__ __forceinline__ void padded_window32(int64_t base, int len, int k0, const I* __restrict__ col,
+                                                const V* __restrict__ val, const V* __restrict__ x, int lane,
+                                                Emit&& emit) {
+  len = len - k0;
+  len = len < 0 ? 0 : (len > kPadWindow ? kPadWindow : len);
+  base += 32 * (int64_t)k0;
+  const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned)len);
+  const unsigned longest = __reduce_max_sync(0xffffffffu, (unsigned)len);
+  if (32u * longest <= total + total / 4 + 32u * 8u) {
+    V s0 = V(0), s1 = V(0);
+    const int64_t rb = base + lane;
+    int k = 0;
+    for (; k + 1 < len; k += 2) {
+      const int64_t a = rb + 32 * (int64_t)k, b = a + 32;
+      const I ca = ld_stream(col + a), cb = ld_stream(col + b);
+      const V va = ld_stream(val + a), vb = ld_stream(val + b);
+      if (ca >= 0) s0 += va * ld_gather(x + ca);
+      if (cb >= 0) s1 += vb * ld_gather(x + cb);
+    }
+    if (k < len) {
+      const int64_t a = rb + 32 * (int64_t)k;
+      const I ca = ld_stream(col + a);
+      const V va = ld_stream(val + a);
+      if (ca >= 0) s0 += va * ld_gather(x + ca);
+    }
+    emit(lane, s0 + s1);
+    return;
+  }
+  // rank rows by length, descending (ties: lower row first)
+  uint32_t key = ((uint32_t)len << 5) | (uint32_t)(31 - lane);
+#pragma unroll
+  for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+    for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+      const uint32_t other = __shfl_xor_sync(0xffffffffu, key, jj);
+      const bool first_half = (lane & kk) == 0, lower = (lane & jj) == 0;
+      key = (lower == first_half) ? (key > other ? key : other) : (key < other ? key : other);
+    }
+  }
+  const int rank_len = (int)(key >> 5), rank_row = 31 - (int)(key & 31u);
+  V sum = V(0);
+  int kbeg = 0;
+#pragma unroll 1
+  for (int p = 0; p < 6; ++p) {
+    const int R = 32 >> p, g = 1 << p;
+    const int q = lane & (R - 1), sub = lane >> (5 - p);
+    const int L = __shfl_sync(0xffffffffu, rank_len, q);
+    const int r = __shfl_sync(0xffffffffu, rank_row, q);
+    const int kend = __shfl_sync(0xffffffffu, rank_len, R > 1 ? R / 2 : 0);
+    const int lim = L < kend ? L : kend;
+    const int64_t rb = base + r;
+    V s0 = V(0), s1 = V(0);
+    int k = kbeg + sub;
+    for (; k + g < lim; k += 2 * g) {
+      const int64_t a = rb + 32 * (int64_t)k, b = a + 32 * (int64_t)g;
+      const I ca = ld_stream(col + a), cb = ld_stream(col + b);
+      const V va = ld_stream(val + a), vb = ld_stream(val + b);
+      if (ca >= 0) s0 += va * ld_gather(x + ca);
+      if (cb >= 0) s1 += vb * ld_gather(x + cb);
+    }
+    if (k < lim) {
+      const int64_t a = rb + 32 * (int64_t)k;
+      const I ca = ld_stream(col + a);
+      const V va = ld_stream(val + a);
+      if (ca >= 0) s0 += va * ld_gather(x + ca);
+    }
+    sum += s0 + s1;
+    // rows of rank [R/2, R) end in this phase (rank 0 in the last one)
+    V tot = sum;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      if (o >= R) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (q >= (R > 1 ? R / 2 : 0)) {
+      if (sub == 0) emit(r, tot);
+      sum = V(0);
+    }
+    kbeg = kend;
+  }
+}
+
 // One piece q of a long padded row, with one warp.
 template <typename I, typename V, bool kColMajor>
 __device__ __forceinline__ void padded_piece(int64_t q, const PadPiece& pc, const I* __restrict__ col,

@@ -196,6 +196,38 @@ def test_sell_long_rows_and_empty_rows(cuda, orc):
         _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x))
 
 
+@pytest.mark.parametrize("sigma", [32, 512, 1 << 20])
+def test_sell_col_major_windows_and_packing(cuda, orc, sigma):
+    """C = 32 column-major: chunks cut into step windows (rows longer than 128
+    slots, one with more than 2048), rows of very different lengths in one
+    chunk (the lane re-dealing path), empty rows, rows past the last full
+    chunk, unsorted (sigma = C) and sorted slices; FP64 and FP32 values."""
+    from sparseops_b200 import SpOps_sell_c_sigma, csr_to_sell_c_sigma
+    rng = np.random.default_rng(21)
+    n, ncols = 3000 + 17, 50000
+    lens = rng.integers(0, 12, n)
+    lens[rng.choice(n, 40, replace=False)] = rng.integers(130, 900, 40)
+    lens[5], lens[33], lens[2999] = 2500, 129, 4097
+    lens[64:96] = 0
+    lens[200:232] = np.arange(1, 33) * 7
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    x = rng.uniform(-1, 1, ncols)
+    y0 = rng.uniform(-1, 1, n)
+    rp = rp.astype(np.int32)
+    S = csr_to_sell_c_sigma(_csr(rp, ci, v, ncols), None, sigma, 32, 1, layout=1)
+    for _ in range(2):  # the window counters must be back at zero for the next call
+        _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x, 0.8, 0.7, y0), 0.8, 0.7, y0)
+    v32, x32 = v.astype(np.float32), x.astype(np.float32)
+    S32 = csr_to_sell_c_sigma(_csr(rp, ci, v32, ncols), None, sigma, 32, 1, layout=1)
+    y = _spmv(SpOps_sell_c_sigma, S32, x32, 1.0, 0.0, np.zeros(n, np.float32))
+    yref = orc.spmv_csr(rp, ci, v32.astype(np.float64), x32.astype(np.float64))
+    den = orc.absdot(rp, ci, v32, x32)
+    assert (np.abs(y - yref) / np.maximum(den, 1e-300)).max() <= 1e-5
+
+
 def test_powerlaw_full_sell_and_ell(cuda, orc):
     """Power-law config at full size: SELL-C-sigma (C=32, sigma=512) and
     SELL-C-R match the oracle; ELL is refused (it would need ~1 TB)."""
