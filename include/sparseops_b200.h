@@ -133,6 +133,13 @@ spops_status_t spops_csr_create(spops_context_t ctx, spops_matrix_t* A, int64_t 
 spops_status_t spops_coo_create(spops_context_t ctx, spops_matrix_t* A, int64_t rows, int64_t cols, int64_t nnz,
                                 const void* row_index, const void* col_index, const void* values,
                                 spops_index_t itype, spops_value_t vtype, spops_mem_t mem);
+/* CSR handle (owned arrays) from a COO handle, on the device.  Replaces
+ * coo_to_csr (include/sparse_conversion.h:37-99): rows in order, file order
+ * kept within a row.  compact != 0 adds the reference's sum_csr_duplicates
+ * (include/sparse_operation.h:21-69): equal columns of a row summed in file
+ * order, distinct columns listed in reverse order of first appearance,
+ * exact-zero sums dropped -- bit-identical to the reference. */
+spops_status_t spops_coo_to_csr(spops_context_t ctx, spops_matrix_t coo, int32_t compact, spops_matrix_t* csr);
 spops_status_t spops_matrix_destroy(spops_matrix_t A);
 spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info);
 /* Values changed in place (same pattern): drop value-derived caches. */

@@ -54,7 +54,7 @@ class Oracle:
         for name in ("orc_lsh_pairs", "orc_spgemm"):
             getattr(L, name).restype = _vp
         for name in ("orc_pairs_count", "orc_hc", "orc_dia_offsets", "orc_bsr_structure",
-                     "orc_spgemm_flop"):
+                     "orc_spgemm_flop", "orc_coo_to_csr_f64", "orc_coo_to_csr_f32"):
             getattr(L, name).restype = _i64
 
     # ---- SpMV
@@ -164,6 +164,19 @@ class Oracle:
         brp = B[0]
         return int(self.L.orc_spgemm_flop(_i64(len(arp) - 1), _p(arp), _p(aci), _i64(len(brp) - 1), _p(brp)))
 
+    # ---- COO -> CSR
+    def coo_to_csr(self, n, ri, ci, v, compact=False):
+        """(rp, ci, v) of coo_to_csr; v's dtype (float32 / float64) is kept."""
+        ri = np.ascontiguousarray(ri, np.int64)
+        ci = np.ascontiguousarray(ci, np.int64)
+        f32 = np.asarray(v).dtype == np.float32
+        v = np.ascontiguousarray(v, np.float32 if f32 else np.float64)
+        m = len(ci)
+        rp, oc, ov = np.zeros(n + 1, np.int64), np.zeros(max(m, 1), np.int64), np.zeros(max(m, 1), v.dtype)
+        fn = self.L.orc_coo_to_csr_f32 if f32 else self.L.orc_coo_to_csr_f64
+        k = fn(_i64(n), _i64(m), _p(ri), _p(ci), _p(v), C.c_int32(1 if compact else 0), _p(rp), _p(oc), _p(ov))
+        return rp, oc[:k], ov[:k]
+
     # ---- adjoints
     def spmv_t(self, rp, ci, v, g, ncols):
         y = np.zeros(ncols)
@@ -193,7 +206,7 @@ class Reference:
             raise FileNotFoundError(f"reference library not built: {path}")
         self.path = path
         self.L = L = C.CDLL(path)
-        for name in ("ref_fmt_build", "ref_lsh_pairs", "ref_spgemm_kernel3", "ref_csr_transpose"):
+        for name in ("ref_fmt_build", "ref_lsh_pairs", "ref_spgemm_kernel3", "ref_csr_transpose", "ref_coo_to_csr"):
             getattr(L, name).restype = _vp
         L.ref_pairs_count.restype = _i64
         L.ref_hc.restype = _i64
@@ -295,6 +308,21 @@ class Reference:
             _i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av), _i64(len(brp) - 1),
             _i64(bcols), _i64(len(bci)), _p(brp), _p(bci), _p(bv), _p(perm), _p(offsets), _i64(len(offsets) - 1),
             C.c_int(int(iters)), _dbl(l2_fraction)))
+
+    def coo_to_csr(self, n, ncols, ri, ci, v, compact=False):
+        """The reference's coo_to_csr<int64_t, double> (include/sparse_conversion.h:37)."""
+        ri = np.ascontiguousarray(ri, np.int64)
+        ci = np.ascontiguousarray(ci, np.int64)
+        v = np.ascontiguousarray(v, np.float64)
+        h = self.L.ref_coo_to_csr(_i64(n), _i64(ncols), _i64(len(ci)), _p(ri), _p(ci), _p(v),
+                                  C.c_int(1 if compact else 0))
+        info = np.zeros(6, np.int64)
+        self.L.ref_csr_info(_vp(h), _p(info))
+        rp = np.zeros(info[0] + 1, np.int64)
+        oc, ov = np.zeros(max(info[2], 1), np.int64), np.zeros(max(info[2], 1))
+        self.L.ref_csr_copy(_vp(h), _p(rp), _p(oc), _p(ov))
+        self.L.ref_csr_free(_vp(h))
+        return rp, oc[:info[2]], ov[:info[2]]
 
     def csr_transpose(self, rp, ci, v, ncols):
         h = self.L.ref_csr_transpose(_i64(len(rp) - 1), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _p(v))

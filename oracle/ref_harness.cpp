@@ -414,6 +414,23 @@ void ref_csr_free(void* vh) {
   delete h;
 }
 
+// ------------------------------------------------------------ COO -> CSR
+// The reference's coo_to_csr<int64_t, double> (include/sparse_conversion.h:37)
+// on caller arrays; the result is read back through ref_csr_info / copy / free.
+void* ref_coo_to_csr(ll nr, ll nc, ll nnz, const ll* ri, const ll* ci, const double* v, int compact) {
+  COO_Matrix<int64_t, double> coo;
+  std::memset(static_cast<void*>(&coo), 0, sizeof(coo));
+  coo.num_rows = nr;
+  coo.num_cols = nc;
+  coo.num_nnzs = nnz;
+  coo.row_index = const_cast<int64_t*>((const int64_t*)ri);
+  coo.col_index = const_cast<int64_t*>((const int64_t*)ci);
+  coo.values = const_cast<double*>(v);
+  CsrHandle* h = new CsrHandle();
+  h->C = coo_to_csr<int64_t, double>(coo, compact != 0);
+  return h;
+}
+
 // --------------------------------------------------------------- transpose
 void* ref_csr_transpose(ll nr, ll nc, ll nnz, const ll* rp, const ll* ci, const double* v) {
   CSR_Matrix<int64_t, double> A = wrap_csr<int64_t, double>(nr, nc, nnz, (const int64_t*)rp,

@@ -464,6 +464,74 @@ int64_t orc_spgemm_flop(int64_t a_rows, const int64_t* arp, const int64_t* aci, 
   return 2 * f;
 }
 
+// ------------------------------------------------------------ COO -> CSR
+// coo_to_csr (include/sparse_conversion.h:37-99): rows by a stable counting
+// sort (file order kept within a row); with compact, sum_csr_duplicates
+// (include/sparse_operation.h:21-69): per row, the values of a column are
+// added in file order from zero; the distinct columns come out in reverse
+// order of first appearance; exact-zero sums are dropped.  Returns the
+// output entry count (arrays sized for nnz entries, rp for n + 1).
+}  // extern "C"
+
+template <typename V>
+static int64_t coo_to_csr_impl(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const V* v,
+                               int32_t compact, int64_t* rp, int64_t* oc, V* ov) {
+  std::vector<int64_t> cnt((size_t)n + 1, 0);
+  for (int64_t e = 0; e < nnz; ++e) ++cnt[(size_t)ri[e] + 1];
+  for (int64_t r = 0; r < n; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
+  std::vector<int64_t> at(cnt.begin(), cnt.end() - 1);
+  std::vector<int64_t> col((size_t)nnz);
+  std::vector<V> val((size_t)nnz);
+  for (int64_t e = 0; e < nnz; ++e) {
+    const int64_t d = at[(size_t)ri[e]]++;
+    col[(size_t)d] = ci[e];
+    val[(size_t)d] = v[e];
+  }
+  if (!compact) {
+    std::copy(cnt.begin(), cnt.end(), rp);
+    std::copy(col.begin(), col.end(), oc);
+    std::copy(val.begin(), val.end(), ov);
+    return nnz;
+  }
+  int64_t out = 0;
+  rp[0] = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    std::vector<int64_t> order;        // distinct columns, first appearance order
+    std::map<int64_t, V> sum;
+    for (int64_t e = cnt[(size_t)r]; e < cnt[(size_t)r + 1]; ++e) {
+      auto it = sum.find(col[(size_t)e]);
+      if (it == sum.end()) {
+        order.push_back(col[(size_t)e]);
+        sum.emplace(col[(size_t)e], V(0) + val[(size_t)e]);
+      } else {
+        it->second += val[(size_t)e];
+      }
+    }
+    for (auto k = order.rbegin(); k != order.rend(); ++k) {
+      const V s = sum[*k];
+      if (s != V(0)) {
+        oc[out] = *k;
+        ov[out] = s;
+        ++out;
+      }
+    }
+    rp[r + 1] = out;
+  }
+  return out;
+}
+
+extern "C" {
+
+int64_t orc_coo_to_csr_f64(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const double* v,
+                           int32_t compact, int64_t* rp, int64_t* oc, double* ov) {
+  return coo_to_csr_impl<double>(n, nnz, ri, ci, v, compact, rp, oc, ov);
+}
+
+int64_t orc_coo_to_csr_f32(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const float* v,
+                           int32_t compact, int64_t* rp, int64_t* oc, float* ov) {
+  return coo_to_csr_impl<float>(n, nnz, ri, ci, v, compact, rp, oc, ov);
+}
+
 // ------------------------------------------------------------ adjoints
 void orc_spmv_t_csr_f64_i32(int64_t nr, int64_t nc, const int32_t* rp, const int32_t* ci, const double* v,
                             const double* g, double* y) {

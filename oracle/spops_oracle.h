@@ -73,6 +73,14 @@ void orc_csr_free(void* h);
 int64_t orc_spgemm_flop(int64_t a_rows, const int64_t* arp, const int64_t* aci, int64_t b_rows,
                         const int64_t* brp);
 
+/* COO -> CSR (include/sparse_conversion.h:37-99), with compact != 0 the
+ * duplicate summation of include/sparse_operation.h:21-69.  Output arrays
+ * sized nnz (rp: n + 1); returns the output entry count. */
+int64_t orc_coo_to_csr_f64(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const double* v,
+                           int32_t compact, int64_t* rp, int64_t* oc, double* ov);
+int64_t orc_coo_to_csr_f32(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const float* v,
+                           int32_t compact, int64_t* rp, int64_t* oc, float* ov);
+
 /* y = A^T g by scatter (the value the reference's csr_transpose + SpOps_csr
  * gives, include/sparse_conversion.h:2066-2108), FP64. */
 void orc_spmv_t_csr_f64_i32(int64_t nr, int64_t nc, const int32_t* rp, const int32_t* ci, const double* v,

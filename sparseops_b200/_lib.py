@@ -62,6 +62,7 @@ _SIGS = {
     "spops_check_device": [vp, vp],
     "spops_set_option": [vp, C.c_char_p, i64],
     "spops_csr_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
+    "spops_coo_to_csr": [vp, vp, C.c_int32, C.POINTER(vp)],
     "spops_matrix_destroy": [vp],
     "spops_matrix_info": [vp, vp],
     "spops_matrix_touch": [vp],

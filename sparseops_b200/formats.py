@@ -380,6 +380,19 @@ def csr_to_csr5(csr: CSR_Matrix, fp_feature=None):
     return _wrap(CSR5_Matrix, csr, h, row_offset=csr.row_offset, col_index=csr.col_index, values=csr.values)
 
 
+def coo_to_csr(coo: COO_Matrix, compact: bool = False):
+    """include/sparse_conversion.h:37 on the device: CSR with rows in order and
+    file order kept within a row; compact=True also sums duplicates like
+    sum_csr_duplicates (include/sparse_operation.h:21): distinct columns in
+    reverse order of first appearance, exact-zero sums dropped."""
+    from .spops import DeviceCSR
+    h = coo.device()
+    ctx = h.ctx.follow_torch()
+    out = vp()
+    call("spops_coo_to_csr", ctx.handle, h.handle, C.c_int32(1 if compact else 0), C.byref(out))
+    return DeviceCSR(_Handle(ctx, out), coo.num_rows, coo.num_cols)
+
+
 def csr_to_coo(csr: CSR_Matrix):
     """include/sparse_conversion.h:152."""
     h = _convert(csr, "coo")

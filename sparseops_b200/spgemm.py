@@ -21,7 +21,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import SpgemmStats, call, dbl, i32, i64, u64, vp
-from .spops import CSR_Matrix, _Handle, default_context
+from .spops import CSR_Matrix, DeviceCSR, _Handle, default_context
 
 L2_BUDGET_DEFAULT = 67108864 * 0.75  # reference CPU_L2CACHE_SIZE (as shipped) x MIXED_L2_FRACTION
 
@@ -91,38 +91,12 @@ def hierarchical_clustering_v0_fast(rowptr, colids, num_rows: int, pairs, cluste
     return perm, offs[:nc.value + 1]
 
 
-class SpGEMMResult(CSR_Matrix):
+class SpGEMMResult(DeviceCSR):
     """C = A*B as a device CSR handle; arrays downloaded on first access."""
 
     def __init__(self, handle: _Handle, rows: int, cols: int, itype, vtype, stats: dict):
-        info = handle.info()
-        super().__init__(rows, cols, None, np.zeros(0, np.int64), None)
-        self.num_nnzs = int(info.nnz)
-        self._h = handle
-        self._it, self._vt = itype, vtype
+        super().__init__(handle, rows, cols)
         self.stats = stats
-        self._host = None
-
-    def host(self):
-        if self._host is None:
-            h = self._h
-            idx = np.int32 if self._it == 0 else np.int64
-            val = np.float32 if self._vt == 0 else np.float64
-            rp = np.empty(self.num_rows + 1, idx)
-            ci = np.empty(self.num_nnzs, idx)
-            v = np.empty(self.num_nnzs, val)
-            for arr, which in ((rp, 0), (ci, 1), (v, 2)):
-                if len(arr):
-                    call("spops_matrix_download", h.ctx.handle, h.handle, which, _p(arr), i64(len(arr)))
-            self._host = (rp, ci, v)
-        return self._host
-
-    row_offset = property(lambda self: self.host()[0], lambda self, v: None)
-    col_index = property(lambda self: self.host()[1] if self._h is not None else np.zeros(0), lambda self, v: None)
-    values = property(lambda self: self.host()[2] if self._h is not None else None, lambda self, v: None)
-
-    def device(self, ctx=None):
-        return self._h
 
 
 def _types(A: CSR_Matrix):

@@ -200,6 +200,39 @@ def _spmv(alpha, A: Matrix_Features, x, beta, y):
     return y
 
 
+class DeviceCSR(CSR_Matrix):
+    """A CSR matrix produced on the device (conversion or product result),
+    held by its handle; host copies of the arrays are made on first access."""
+
+    def __init__(self, handle: _Handle, rows: int, cols: int):
+        info = handle.info()
+        super().__init__(rows, cols, None, np.zeros(0, np.int64), None)
+        self.num_nnzs = int(info.nnz)
+        self._h = handle
+        self._it, self._vt = int(info.index_type), int(info.value_type)
+        self._host = None
+
+    def host(self):
+        """(row_offset, col_index, values) as numpy arrays."""
+        if self._host is None:
+            h = self._h
+            idx = np.int32 if self._it == 0 else np.int64
+            val = np.float32 if self._vt == 0 else np.float64
+            arrs = (np.empty(self.num_rows + 1, idx), np.empty(self.num_nnzs, idx), np.empty(self.num_nnzs, val))
+            for arr, which in zip(arrs, (0, 1, 2)):
+                if len(arr):
+                    call("spops_matrix_download", h.ctx.handle, h.handle, which, vp(arr.ctypes.data), i64(len(arr)))
+            self._host = arrs
+        return self._host
+
+    row_offset = property(lambda self: self.host()[0], lambda self, v: None)
+    col_index = property(lambda self: self.host()[1] if self._h is not None else np.zeros(0), lambda self, v: None)
+    values = property(lambda self: self.host()[2] if self._h is not None else None, lambda self, v: None)
+
+    def device(self, ctx=None):
+        return self._h
+
+
 def SpOps_csr(alpha, csr: CSR_Matrix, x, beta, y):
     """y = alpha*A*x + beta*y for a CSR matrix (reference src/spmv_csr.cpp:165)."""
     return _spmv(alpha, csr, x, beta, y)

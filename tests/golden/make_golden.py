@@ -128,6 +128,18 @@ def main():
     tci, tv = sort_rows(trp, tci, tv)
     g["tr_rp"], g["tr_ci"], g["tr_v"] = trp, tci, tv
 
+    # ---- COO -> CSR (coo_to_csr, plain and with sum_csr_duplicates):
+    # duplicates in random file order, values that cancel exactly
+    rng = np.random.default_rng(77)
+    n, nc, m = 300, 60, 4000
+    ri = rng.integers(0, n, m).astype(np.int64)
+    ci = rng.integers(0, nc, m).astype(np.int64)
+    cv = rng.integers(-3, 4, m).astype(np.float64) * 0.25
+    g["coo_ri"], g["coo_ci"], g["coo_v"], g["coo_shape"] = ri, ci, cv, np.array([n, nc], np.int64)
+    for compact in (0, 1):
+        crp, cci, ccv = R.coo_to_csr(n, nc, ri, ci, cv, bool(compact))
+        g[f"coo_rp{compact}"], g[f"coo_csr_ci{compact}"], g[f"coo_csr_v{compact}"] = crp, cci, ccv
+
     np.savez_compressed(OUT, **g)
     print(OUT, os.path.getsize(OUT), "bytes,", len(g), "arrays")
 

@@ -294,3 +294,56 @@ def test_csr5_powerlaw_full(cuda, orc):
     x = synth.uniform(n, 1)
     T = csr_to_csr5(_csr(rp, ci, v))
     _check(orc, rp, ci, v, x, _spmv(SpOps_csr5, T, x, 1.0, 0.0), 1.0, 0.0)
+
+
+@pytest.mark.parametrize("compact", [0, 1])
+def test_coo_to_csr_golden_device(cuda, golden, compact):
+    """Device coo_to_csr against the reference's own output, bit for bit."""
+    import torch
+    from sparseops_b200 import COO_Matrix, coo_to_csr
+    n, nc = (int(t) for t in golden["coo_shape"])
+    coo = COO_Matrix(n, nc, _dev(golden["coo_ri"]), _dev(golden["coo_ci"]), _dev(golden["coo_v"]))
+    C = coo_to_csr(coo, bool(compact))
+    torch.cuda.synchronize()
+    rp, ci, v = C.host()
+    assert np.array_equal(rp, golden[f"coo_rp{compact}"])
+    assert np.array_equal(ci, golden[f"coo_csr_ci{compact}"])
+    assert np.array_equal(v, golden[f"coo_csr_v{compact}"])
+
+
+@pytest.mark.parametrize("itype,vtype", [(np.int32, np.float64), (np.int64, np.float32), (np.int32, np.float32)])
+@pytest.mark.parametrize("compact", [False, True])
+def test_coo_to_csr_vs_oracle(cuda, orc, itype, vtype, compact):
+    """Random file order with duplicates, exact cancellations, empty rows, a
+    long row; also an already row-sorted COO (its arrays are borrowed by the
+    view, the result must still own copies) and an empty matrix."""
+    import torch
+    from sparseops_b200 import COO_Matrix, SpOps_csr, coo_to_csr
+    rng = np.random.default_rng(5)
+    n, nc, m = 5000, 3000, 120000
+    ri = rng.integers(0, n, m)
+    ri[:20000] = 17  # a long row with many duplicates
+    ri[(ri >= 100) & (ri < 400)] = 99  # rows 100..399 empty
+    ci = rng.integers(0, nc, m)
+    v = (rng.integers(-4, 5, m) * 0.5).astype(vtype)
+    for order in ("file", "sorted"):
+        if order == "sorted":
+            p = np.argsort(ri, kind="stable")
+            ri, ci, v = ri[p], ci[p], v[p]
+        coo = COO_Matrix(n, nc, _dev(ri.astype(itype)), _dev(ci.astype(itype)), _dev(v))
+        C = coo_to_csr(coo, compact)
+        rp, oc, ov = C.host()
+        erp, eci, ev = orc.coo_to_csr(n, ri, ci, v, compact)
+        assert np.array_equal(rp.astype(np.int64), erp) and np.array_equal(oc.astype(np.int64), eci)
+        assert ov.dtype == vtype and np.array_equal(ov, ev)
+        del coo  # the result owns its arrays
+        x = torch.ones(nc, dtype=torch.float64 if vtype == np.float64 else torch.float32, device="cuda")
+        y = torch.zeros(n, dtype=x.dtype, device="cuda")
+        SpOps_csr(1.0, C, x, 0.0, y)
+        torch.cuda.synchronize()
+        ref = np.add.reduceat(np.concatenate([ev, [0]]).astype(np.float64), erp[:-1]) * (np.diff(erp) > 0)
+        assert np.allclose(y.cpu().numpy(), ref, rtol=1e-5, atol=1e-5)
+    empty = coo_to_csr(COO_Matrix(7, 3, _dev(np.zeros(0, itype)), _dev(np.zeros(0, itype)), _dev(np.zeros(0, vtype))),
+                       compact)
+    rp, oc, ov = empty.host()
+    assert np.array_equal(rp, np.zeros(8)) and len(oc) == 0

@@ -110,3 +110,14 @@ def test_transpose_spmv(golden, orc):
     y = orc.spmv_t(rp, ci, v, gv, n)
     yt = orc.spmv_csr(g["tr_rp"], g["tr_ci"], g["tr_v"], gv)
     assert np.abs(y - yt).max() <= 1e-13 * (1 + np.abs(y).max())
+
+
+@pytest.mark.parametrize("compact", [0, 1])
+def test_coo_to_csr_golden(golden, orc, compact):
+    """coo_to_csr and its duplicate summation (compact) against the reference's
+    own output: row offsets, column order and values bit for bit."""
+    n = int(golden["coo_shape"][0])
+    rp, ci, v = orc.coo_to_csr(n, golden["coo_ri"], golden["coo_ci"], golden["coo_v"], bool(compact))
+    assert np.array_equal(rp, golden[f"coo_rp{compact}"])
+    assert np.array_equal(ci, golden[f"coo_csr_ci{compact}"])
+    assert np.array_equal(v, golden[f"coo_csr_v{compact}"])
