@@ -274,6 +274,8 @@ spops_status_t spops_batch_info(spops_batch_t batch, int64_t* items, int32_t* ch
  * Replaces minhash_signatures_flat (include/spgemm_MinHashLSH.h:119);
  * bit-identical (same LCG coefficients from seed). */
 spops_status_t spops_minhash(spops_context_t ctx, spops_matrix_t A, int32_t k, uint64_t seed, void* sig);
+/* Same with a HOST output array sig_host[rows * k] (device scratch inside). */
+spops_status_t spops_minhash_host(spops_context_t ctx, spops_matrix_t A, int32_t k, uint64_t seed, void* sig_host);
 /* LSH candidate pairs (i < j, sorted, unique) with MinHash-estimated scores
  * (matches / k), on the device.  Replaces lsh_candidate_pairs_vector
  * (include/spgemm_MinHashLSH.h:777); constrain != 0: a bucket of more than

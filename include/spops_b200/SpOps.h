@@ -1,0 +1,1002 @@
+/* C++ drop-in for the SparseOps operator API (the reference's include/SpOps.h),
+ * running on one B200 through the C ABI of ../sparseops_b200.h.
+ *
+ * A caller of the reference switches its include path to this directory and
+ * links libsparseops_b200.so; the structs (include/sparse_format.h:49-295 of
+ * the reference), their field names and the call signatures stay the same:
+ *
+ *   SpOps_csr / _coo / _ell / _sell / _sell_c_sigma / _sell_c_R / _dia / _bsr / _csr5
+ *       (alpha, const FMT_Matrix<I,V>& A, const V* x, beta, V* y)    host x, y
+ *   coo_to_csr, csr_to_coo, csr_to_ell, csr_to_sell, csr_to_sell_c_sigma,
+ *   csr_to_sell_c_R, csr_to_dia, csr_to_bsr, csr_to_csr5             host structs out
+ *   delete_host_matrix(...)
+ *   minhash_signatures_flat, lsh_candidate_pairs_vector,
+ *   hierarchical_clustering_v0_fast                                   LeSpGEMM preprocessing
+ *
+ * What differs, and why:
+ *   - Work runs on the GPU.  The first SpOps call on a matrix uploads it and
+ *     keeps the device copy (with its analysis) keyed by the struct's first
+ *     array pointer; later calls only move x and y.  Host arrays are therefore
+ *     read once: after changing them in place, call spops_b200::invalidate(ptr)
+ *     (delete_host_matrix does it for you), or switch the cache off with
+ *     spops_b200::set_cache(false) to upload on every call as the reference
+ *     reads on every call.
+ *   - Conversions run on the device; the returned host structs hold the
+ *     reference's layouts (row-major chunks, reorder, chunk_len, ...) and the
+ *     device copy used by SpOps_<fmt> keeps the device-native layout.
+ *   - Errors throw std::runtime_error with the library's message where the
+ *     reference calls exit() or asserts.
+ *   - CSR5 tiles are the device's (32 lanes x 16 entries): tile_ptr/tile_desc
+ *     are filled from them; y agrees with the reference, tile arrays do not.
+ *   - Host arrays come from posix_memalign and are released with free(), as
+ *     the reference's delete_array does; pointer-per-chunk tables use new[].
+ */
+#ifndef SPOPS_B200_CXX_SPOPS_H
+#define SPOPS_B200_CXX_SPOPS_H
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <unordered_map>
+#include <vector>
+
+#include "../sparseops_b200.h"
+
+/* Defaults as the reference ships them (include/general_config.h,
+ * include/plat_config.h); a caller's own definitions win. */
+#ifndef CHUNK_SIZE
+#define CHUNK_SIZE 4
+#endif
+#ifndef SELL_SIGMA
+#define SELL_SIGMA 16384
+#endif
+#ifndef MAX_DIAG_NUM
+#define MAX_DIAG_NUM 10240
+#endif
+#ifndef BSR_BlockDimRow
+#define BSR_BlockDimRow 16
+#endif
+#ifndef SIMD_WIDTH
+#define SIMD_WIDTH 256
+#endif
+
+typedef enum { RowMajor = 0, ColMajor = 1 } LeadingDimension;
+
+/* ------------------------------------------------------------- structs */
+template <typename IndexType>
+struct Matrix_Features {
+  typedef IndexType index_type;
+  IndexType num_rows;
+  IndexType num_cols;
+  IndexType num_nnzs;
+  double sparsity;
+  IndexType* partition = nullptr;
+  double time, gflops, gbytes;
+  int tag;
+  int kernel_flag;
+};
+
+template <typename IndexType, typename ValueType>
+struct COO_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType* row_index;
+  IndexType* col_index;
+  ValueType* values;
+};
+
+template <typename IndexType, typename ValueType>
+struct CSR_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType* row_offset;
+  IndexType* col_index;
+  ValueType* values;
+};
+
+template <typename IndexType, typename ValueType>
+struct BSR_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType blockDim_r;
+  IndexType blockDim_c;
+  IndexType blockNNZ;
+  IndexType mb;
+  IndexType nb;
+  IndexType nnzb;
+  IndexType* row_ptr;
+  IndexType* block_colindex;
+  ValueType* block_data;  // blocks row-major inside
+};
+
+template <typename IndexType, typename UIndexType, typename ValueType>
+struct CSR5_Matrix : public CSR_Matrix<IndexType, ValueType> {
+  IndexType sigma;
+  IndexType omega;
+  IndexType bit_y_offset;
+  IndexType bit_scansum_offset;
+  IndexType num_packets;
+  IndexType num_offsets;
+  IndexType _p;  // tiles
+  IndexType tail_partition_start;
+  UIndexType* tile_ptr;   // [_p + 1]
+  UIndexType* tile_desc;  // [_p * omega]
+  IndexType* tile_desc_offset_ptr;
+  IndexType* tile_desc_offset;
+  ValueType* calibrator;
+};
+
+template <typename IndexType, typename ValueType>
+struct DIA_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType stride;
+  IndexType complete_ndiags;
+  long int* diag_offsets;
+  ValueType* diag_data;  // [complete_ndiags * stride]
+};
+
+template <typename IndexType, typename ValueType>
+struct ELL_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  LeadingDimension ld;
+  IndexType max_row_width;
+  IndexType min_row_width;
+  IndexType* col_index;  // [num_rows * max_row_width], -1 = padding
+  ValueType* values;
+};
+
+template <typename IndexType, typename ValueType>
+struct S_ELL_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType sliceWidth;
+  IndexType chunk_num;
+  IndexType alignment;
+  IndexType* row_width;    // [chunk_num]
+  IndexType** col_index;   // [chunk_num][sliceWidth * row_width[c]], row-major
+  ValueType** values;
+};
+
+template <typename IndexType, typename ValueType>
+struct SELL_C_Sigma_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType sliceWidth_Sigma;
+  IndexType chunkWidth_C;
+  IndexType sliceNum;
+  IndexType chunkNum;
+  IndexType validchunkNum;
+  IndexType chunk_num_per_slice;
+  IndexType alignment;
+  IndexType* reorder;      // [num_rows]: stored row -> original row
+  IndexType* chunk_len;    // [validchunkNum]
+  IndexType** col_index;   // [validchunkNum][chunkWidth_C * chunk_len[c]], row-major
+  ValueType** values;
+};
+
+template <typename IndexType, typename ValueType>
+struct SELL_C_R_Matrix : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType chunkWidth_C;
+  IndexType validchunkNum;
+  IndexType alignment;
+  IndexType* reorder;
+  IndexType* chunk_len;
+  IndexType** col_index;
+  ValueType** values;
+};
+
+template <typename IndexType, typename ValueType>
+struct CandidatePair {
+  IndexType i;
+  IndexType j;
+  ValueType score;
+};
+
+/* --------------------------------------------------------------- state */
+namespace spops_b200 {
+namespace detail {
+
+struct Entry {
+  spops_matrix_t h = nullptr;
+  int64_t rows = 0, cols = 0, nnz = 0;
+};
+
+struct State {
+  std::mutex mu;
+  int device = 0;
+  bool cache = true;
+  spops_context_t ctx = nullptr;
+  std::unordered_map<const void*, Entry> handles;
+};
+
+// never destroyed: at process exit the CUDA runtime may already be gone
+inline State& state() {
+  static State* s = new State();
+  return *s;
+}
+
+inline void check(spops_status_t s, const char* what) {
+  if (s != SPOPS_OK) {
+    const char* m = spops_last_error();
+    throw std::runtime_error(std::string(what) + ": " + spops_status_string(s) + (m ? std::string(": ") + m : ""));
+  }
+}
+
+inline spops_context_t ctx() {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  if (!s.ctx) check(spops_create(&s.ctx, s.device, nullptr), "spops_create");
+  return s.ctx;
+}
+
+// the argument's own type, kept out of template argument deduction (so that
+// size arguments given as int literals work with 64-bit index types)
+template <typename T>
+struct same {
+  typedef T type;
+};
+template <typename T>
+using same_t = typename same<T>::type;
+
+template <typename I>
+constexpr spops_index_t itype() {
+  static_assert(std::is_integral<I>::value && (sizeof(I) == 4 || sizeof(I) == 8), "index type: 32- or 64-bit integer");
+  return sizeof(I) == 4 ? SPOPS_INDEX_I32 : SPOPS_INDEX_I64;
+}
+
+template <typename V>
+constexpr spops_value_t vtype() {
+  static_assert(std::is_same<V, float>::value || std::is_same<V, double>::value, "value type: float or double");
+  return std::is_same<V, float>::value ? SPOPS_VALUE_F32 : SPOPS_VALUE_F64;
+}
+
+template <typename T>
+inline T* host_alloc(int64_t n) {
+  void* p = nullptr;
+  const size_t bytes = (size_t)(n > 0 ? n : 1) * sizeof(T);
+  if (posix_memalign(&p, 64, bytes) != 0) throw std::bad_alloc();
+  return static_cast<T*>(p);
+}
+
+inline void release(const void* key) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  auto it = s.handles.find(key);
+  if (it != s.handles.end()) {
+    spops_matrix_destroy(it->second.h);
+    s.handles.erase(it);
+  }
+}
+
+// cached device handle for `key`, or nullptr (sizes must match)
+inline spops_matrix_t find(const void* key, int64_t rows, int64_t cols, int64_t nnz) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  auto it = s.handles.find(key);
+  if (it == s.handles.end()) return nullptr;
+  if (it->second.rows == rows && it->second.cols == cols && it->second.nnz == nnz) return it->second.h;
+  spops_matrix_destroy(it->second.h);
+  s.handles.erase(it);
+  return nullptr;
+}
+
+inline void put(const void* key, spops_matrix_t h, int64_t rows, int64_t cols, int64_t nnz) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  auto it = s.handles.find(key);
+  if (it != s.handles.end() && it->second.h != h) spops_matrix_destroy(it->second.h);
+  s.handles[key] = Entry{h, rows, cols, nnz};
+}
+
+inline bool caching() { return state().cache; }
+
+// run y = alpha*A*x + beta*y with host vectors on handle h.  A handle this
+// call created (fresh) is cached under `key`, or destroyed when the cache is
+// off; a handle found in the cache stays there.
+inline void spmv_host(spops_matrix_t h, bool fresh, const void* key, double alpha, const void* x, double beta,
+                      void* y, const char* what, int64_t rows, int64_t cols, int64_t nnz) {
+  spops_status_t s = spops_spmv_host(ctx(), alpha, h, x, beta, y);
+  if (fresh) {
+    if (caching()) put(key, h, rows, cols, nnz); else spops_matrix_destroy(h);
+  }
+  check(s, what);
+}
+
+template <typename T>
+inline T* fetch(spops_matrix_t h, spops_array_t which, int64_t* count) {
+  const void* dp = nullptr;
+  int64_t n = 0;
+  int32_t eb = 0;
+  check(spops_matrix_array(h, which, &dp, &n, &eb), "spops_matrix_array");
+  if (n > 0 && eb != (int32_t)sizeof(T)) throw std::runtime_error("spops_b200: array element size mismatch");
+  T* out = host_alloc<T>(n);
+  if (n > 0) check(spops_matrix_download(ctx(), h, which, out, n), "spops_matrix_download");
+  if (count) *count = n;
+  return out;
+}
+
+inline spops_matrix_info_t info(spops_matrix_t h) {
+  spops_matrix_info_t i;
+  check(spops_matrix_info(h, &i), "spops_matrix_info");
+  return i;
+}
+
+template <typename I, typename V>
+inline spops_matrix_t upload_csr(const CSR_Matrix<I, V>& A) {
+  spops_matrix_t h = nullptr;
+  check(spops_csr_create(ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.row_offset, A.col_index, A.values,
+                         itype<I>(), vtype<V>(), SPOPS_MEM_HOST),
+        "spops_csr_create");
+  return h;
+}
+
+// pattern-only handle: the value slot borrows the column array (never read)
+template <typename I>
+inline spops_matrix_t upload_pattern(const I* rowptr, const I* col, I n) {
+  spops_matrix_t h = nullptr;
+  const int64_t nnz = n > 0 ? (int64_t)rowptr[n] : 0;
+  const int64_t cols = sizeof(I) == 4 ? (int64_t)INT32_MAX : ((int64_t)1 << 40);  // no column bound is needed
+  check(spops_csr_create(ctx(), &h, n, cols, nnz, rowptr, col, col, itype<I>(),
+                         sizeof(I) == 4 ? SPOPS_VALUE_F32 : SPOPS_VALUE_F64, SPOPS_MEM_HOST),
+        "spops_csr_create");
+  return h;
+}
+
+inline spops_matrix_t convert(spops_matrix_t csr, spops_format_t f, const spops_format_params_t& p) {
+  spops_matrix_t out = nullptr;
+  check(spops_convert(ctx(), csr, f, &p, &out), "spops_convert");
+  return out;
+}
+
+template <typename I, typename V, typename M>
+inline void set_features(M& m, int64_t rows, int64_t cols, int64_t nnz) {
+  std::memset(static_cast<void*>(&m), 0, sizeof(M));
+  m.num_rows = (I)rows;
+  m.num_cols = (I)cols;
+  m.num_nnzs = (I)nnz;
+  m.sparsity = (rows > 0 && cols > 0) ? (double)nnz / ((double)rows * (double)cols) : 0.0;
+}
+
+// split concatenated row-major chunks into one host array per chunk
+template <typename T, typename I>
+inline T** split_chunks(const T* all, int64_t total, const I* len, int64_t nchunks, int64_t C) {
+  int64_t need = 0;
+  for (int64_t c = 0; c < nchunks; ++c) need += C * (int64_t)len[c];
+  if (need != total) throw std::runtime_error("spops_b200: padded arrays do not match the chunk widths");
+  T** out = new T*[(size_t)(nchunks > 0 ? nchunks : 1)];
+  int64_t at = 0;
+  for (int64_t c = 0; c < nchunks; ++c) {
+    const int64_t m = C * (int64_t)len[c];
+    out[c] = host_alloc<T>(m);
+    if (m) std::memcpy(out[c], all + at, (size_t)m * sizeof(T));
+    at += m;
+  }
+  return out;
+}
+
+template <typename T, typename I>
+inline std::vector<T> join_chunks(T* const* parts, const I* len, int64_t nchunks, int64_t C) {
+  std::vector<T> all;
+  for (int64_t c = 0; c < nchunks; ++c) all.insert(all.end(), parts[c], parts[c] + C * (int64_t)len[c]);
+  return all;
+}
+
+}  // namespace detail
+
+/* Device used by the calls below (before the first call). */
+inline void set_device(int device) { detail::state().device = device; }
+/* Keep device copies of matrices between calls (default) or upload on every call. */
+inline void set_cache(bool on) { detail::state().cache = on; }
+/* Drop the device copy of the matrix whose first array is `key` (e.g.
+ * A.row_offset, coo.row_index, sell.reorder) after changing it in place. */
+inline void invalidate(const void* key) { detail::release(key); }
+
+}  // namespace spops_b200
+
+/* ---------------------------------------------------------------- SpMV */
+template <typename IndexType, typename ValueType>
+void SpOps_csr(const ValueType alpha, const CSR_Matrix<IndexType, ValueType>& A, const ValueType* x,
+               const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.row_offset, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h) h = d::upload_csr(A);
+  d::spmv_host(h, fresh, A.row_offset, alpha, x, beta, y, "SpOps_csr", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_coo(const ValueType alpha, const COO_Matrix<IndexType, ValueType>& A, const ValueType* x,
+               const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.row_index, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h)
+    d::check(spops_coo_create(d::ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.row_index, A.col_index, A.values,
+                              d::itype<IndexType>(), d::vtype<ValueType>(), SPOPS_MEM_HOST),
+             "spops_coo_create");
+  d::spmv_host(h, fresh, A.row_index, alpha, x, beta, y, "SpOps_coo", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_ell(const ValueType alpha, const ELL_Matrix<IndexType, ValueType>& A, const ValueType* x,
+               const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.col_index, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h) {
+    const IndexType w = A.max_row_width;
+    d::check(spops_padded_create(d::ctx(), &h, SPOPS_FMT_ELL, A.num_rows, A.num_cols, A.num_nnzs,
+                                 A.num_rows > 0 ? A.num_rows : 1, 0, 1,
+                                 A.ld == ColMajor ? SPOPS_COL_MAJOR : SPOPS_ROW_MAJOR, nullptr, &w, 1, A.col_index,
+                                 A.values, (int64_t)A.num_rows * w, d::itype<IndexType>(), d::vtype<ValueType>(),
+                                 SPOPS_MEM_HOST),
+             "spops_padded_create");
+  }
+  d::spmv_host(h, fresh, A.col_index, alpha, x, beta, y, "SpOps_ell", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_sell(const ValueType alpha, const S_ELL_Matrix<IndexType, ValueType>& A, const ValueType* x,
+                const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.row_width, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h) {
+    const std::vector<IndexType> col = d::join_chunks(A.col_index, A.row_width, A.chunk_num, A.sliceWidth);
+    const std::vector<ValueType> val = d::join_chunks(A.values, A.row_width, A.chunk_num, A.sliceWidth);
+    d::check(spops_padded_create(d::ctx(), &h, SPOPS_FMT_SELL, A.num_rows, A.num_cols, A.num_nnzs, A.sliceWidth, 0,
+                                 A.alignment, SPOPS_ROW_MAJOR, nullptr, A.row_width, A.chunk_num, col.data(),
+                                 val.data(), (int64_t)col.size(), d::itype<IndexType>(), d::vtype<ValueType>(),
+                                 SPOPS_MEM_HOST),
+             "spops_padded_create");
+  }
+  d::spmv_host(h, fresh, A.row_width, alpha, x, beta, y, "SpOps_sell", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_sell_c_sigma(const ValueType alpha, const SELL_C_Sigma_Matrix<IndexType, ValueType>& A, const ValueType* x,
+                        const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.reorder, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h) {
+    const std::vector<IndexType> col = d::join_chunks(A.col_index, A.chunk_len, A.validchunkNum, A.chunkWidth_C);
+    const std::vector<ValueType> val = d::join_chunks(A.values, A.chunk_len, A.validchunkNum, A.chunkWidth_C);
+    d::check(spops_padded_create(d::ctx(), &h, SPOPS_FMT_SELL_C_SIGMA, A.num_rows, A.num_cols, A.num_nnzs,
+                                 A.chunkWidth_C, A.sliceWidth_Sigma, A.alignment, SPOPS_ROW_MAJOR, A.reorder,
+                                 A.chunk_len, A.validchunkNum, col.data(), val.data(), (int64_t)col.size(),
+                                 d::itype<IndexType>(), d::vtype<ValueType>(), SPOPS_MEM_HOST),
+             "spops_padded_create");
+  }
+  d::spmv_host(h, fresh, A.reorder, alpha, x, beta, y, "SpOps_sell_c_sigma", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_sell_c_R(const ValueType alpha, const SELL_C_R_Matrix<IndexType, ValueType>& A, const ValueType* x,
+                    const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.reorder, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h) {
+    const std::vector<IndexType> col = d::join_chunks(A.col_index, A.chunk_len, A.validchunkNum, A.chunkWidth_C);
+    const std::vector<ValueType> val = d::join_chunks(A.values, A.chunk_len, A.validchunkNum, A.chunkWidth_C);
+    d::check(spops_padded_create(d::ctx(), &h, SPOPS_FMT_SELL_C_R, A.num_rows, A.num_cols, A.num_nnzs,
+                                 A.chunkWidth_C, A.num_rows, A.alignment, SPOPS_ROW_MAJOR, A.reorder, A.chunk_len,
+                                 A.validchunkNum, col.data(), val.data(), (int64_t)col.size(), d::itype<IndexType>(),
+                                 d::vtype<ValueType>(), SPOPS_MEM_HOST),
+             "spops_padded_create");
+  }
+  d::spmv_host(h, fresh, A.reorder, alpha, x, beta, y, "SpOps_sell_c_R", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_dia(const ValueType alpha, const DIA_Matrix<IndexType, ValueType>& A, const ValueType* x,
+               const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  static_assert(sizeof(long int) == 8, "diag_offsets must be 64-bit");
+  spops_matrix_t h = d::find(A.diag_offsets, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h)
+    d::check(spops_dia_create(d::ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.complete_ndiags, A.stride,
+                              reinterpret_cast<const int64_t*>(A.diag_offsets), A.diag_data, d::vtype<ValueType>(),
+                              SPOPS_MEM_HOST),
+             "spops_dia_create");
+  d::spmv_host(h, fresh, A.diag_offsets, alpha, x, beta, y, "SpOps_dia", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename ValueType>
+void SpOps_bsr(const ValueType alpha, const BSR_Matrix<IndexType, ValueType>& A, const ValueType* x,
+               const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.row_ptr, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h)
+    d::check(spops_bsr_create(d::ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.blockDim_r, A.blockDim_c, A.nnzb,
+                              A.row_ptr, A.block_colindex, A.block_data, d::itype<IndexType>(), d::vtype<ValueType>(),
+                              SPOPS_MEM_HOST),
+             "spops_bsr_create");
+  d::spmv_host(h, fresh, A.row_ptr, alpha, x, beta, y, "SpOps_bsr", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+template <typename IndexType, typename UIndexType, typename ValueType>
+void SpOps_csr5(const ValueType alpha, const CSR5_Matrix<IndexType, UIndexType, ValueType>& A, const ValueType* x,
+                const ValueType beta, ValueType* y) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = d::find(A.tile_ptr, A.num_rows, A.num_cols, A.num_nnzs);
+  const bool fresh = h == nullptr;
+  if (!h) {  // rebuild the device tiles from the CSR arrays the struct carries
+    spops_matrix_t c = d::upload_csr(static_cast<const CSR_Matrix<IndexType, ValueType>&>(A));
+    spops_format_params_t p;
+    std::memset(&p, 0, sizeof(p));
+    spops_status_t s = spops_convert(d::ctx(), c, SPOPS_FMT_CSR5, &p, &h);
+    spops_matrix_destroy(c);
+    d::check(s, "spops_convert");
+  }
+  d::spmv_host(h, fresh, A.tile_ptr, alpha, x, beta, y, "SpOps_csr5", A.num_rows, A.num_cols, A.num_nnzs);
+}
+
+/* ---------------------------------------------------------- conversions */
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> coo_to_csr(const COO_Matrix<IndexType, ValueType>& coo, bool compact = false) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t hc = nullptr, h = nullptr;
+  d::check(spops_coo_create(d::ctx(), &hc, coo.num_rows, coo.num_cols, coo.num_nnzs, coo.row_index, coo.col_index,
+                            coo.values, d::itype<IndexType>(), d::vtype<ValueType>(), SPOPS_MEM_HOST),
+           "spops_coo_create");
+  spops_status_t s = spops_coo_to_csr(d::ctx(), hc, compact ? 1 : 0, &h);
+  spops_matrix_destroy(hc);
+  d::check(s, "spops_coo_to_csr");
+  const spops_matrix_info_t i = d::info(h);
+  CSR_Matrix<IndexType, ValueType> csr;
+  d::set_features<IndexType, ValueType>(csr, i.rows, i.cols, i.nnz);
+  csr.row_offset = d::fetch<IndexType>(h, SPOPS_ARR_ROW, nullptr);
+  csr.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
+  csr.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  if (d::caching()) d::put(csr.row_offset, h, i.rows, i.cols, i.nnz); else spops_matrix_destroy(h);
+  return csr;
+}
+
+template <class IndexType, class ValueType>
+COO_Matrix<IndexType, ValueType> csr_to_coo(const CSR_Matrix<IndexType, ValueType>& csr) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t c = d::upload_csr(csr);
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  spops_matrix_t h = nullptr;
+  spops_status_t s = spops_convert(d::ctx(), c, SPOPS_FMT_COO, &p, &h);
+  spops_matrix_destroy(c);
+  d::check(s, "spops_convert");
+  COO_Matrix<IndexType, ValueType> coo;
+  d::set_features<IndexType, ValueType>(coo, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  coo.row_index = d::fetch<IndexType>(h, SPOPS_ARR_ROW, nullptr);
+  coo.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
+  coo.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  if (d::caching()) d::put(coo.row_index, h, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(h);
+  return coo;
+}
+
+template <class IndexType, class ValueType>
+ELL_Matrix<IndexType, ValueType> csr_to_ell(const CSR_Matrix<IndexType, ValueType>& csr,
+                                            const LeadingDimension ld = RowMajor) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t c = d::upload_csr(csr);
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  p.layout = ld == ColMajor ? SPOPS_COL_MAJOR : SPOPS_ROW_MAJOR;
+  spops_matrix_t h = nullptr;
+  spops_status_t s = spops_convert(d::ctx(), c, SPOPS_FMT_ELL, &p, &h);
+  spops_matrix_destroy(c);
+  d::check(s, "spops_convert");
+  const spops_matrix_info_t i = d::info(h);
+  ELL_Matrix<IndexType, ValueType> ell;
+  d::set_features<IndexType, ValueType>(ell, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  ell.ld = ld;
+  ell.max_row_width = (IndexType)i.extra[0];
+  ell.min_row_width = (IndexType)i.extra[1];
+  ell.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
+  ell.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  if (d::caching()) d::put(ell.col_index, h, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(h);
+  return ell;
+}
+
+namespace spops_b200 {
+namespace detail {
+// padded SELL-type conversion: host arrays in the reference (row-major)
+// layout from one conversion, the cached device copy column-major
+inline void sell_pair(spops_matrix_t c, spops_format_t f, spops_format_params_t p, spops_matrix_t* host_side,
+                      spops_matrix_t* dev_side) {
+  p.layout = SPOPS_ROW_MAJOR;
+  *host_side = convert(c, f, p);
+  p.layout = SPOPS_COL_MAJOR;
+  spops_status_t s = spops_convert(ctx(), c, f, &p, dev_side);
+  if (s != SPOPS_OK) {
+    spops_matrix_destroy(*host_side);
+    check(s, "spops_convert");
+  }
+}
+}  // namespace detail
+}  // namespace spops_b200
+
+template <class IndexType, class ValueType>
+S_ELL_Matrix<IndexType, ValueType> csr_to_sell(const CSR_Matrix<IndexType, ValueType>& csr, FILE* fp_feature,
+                                               const int chunkwidth = CHUNK_SIZE,
+                                               const spops_b200::detail::same_t<IndexType> alignment =
+                                                   (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  namespace d = spops_b200::detail;
+  (void)fp_feature;
+  spops_matrix_t c = d::upload_csr(csr), hh = nullptr, hd = nullptr;
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  p.chunk = chunkwidth;
+  p.alignment = alignment;
+  try {
+    d::sell_pair(c, SPOPS_FMT_SELL, p, &hh, &hd);
+  } catch (...) {
+    spops_matrix_destroy(c);
+    throw;
+  }
+  spops_matrix_destroy(c);
+  const spops_matrix_info_t i = d::info(hh);
+  S_ELL_Matrix<IndexType, ValueType> s;
+  d::set_features<IndexType, ValueType>(s, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  s.sliceWidth = (IndexType)chunkwidth;
+  s.chunk_num = (IndexType)i.extra[0];
+  s.alignment = alignment;
+  s.row_width = d::fetch<IndexType>(hh, SPOPS_ARR_CHUNK_LEN, nullptr);
+  int64_t ncol = 0, nval = 0;
+  IndexType* col = d::fetch<IndexType>(hh, SPOPS_ARR_COL, &ncol);
+  ValueType* val = d::fetch<ValueType>(hh, SPOPS_ARR_VAL, &nval);
+  s.col_index = d::split_chunks(col, ncol, s.row_width, s.chunk_num, chunkwidth);
+  s.values = d::split_chunks(val, nval, s.row_width, s.chunk_num, chunkwidth);
+  std::free(col);
+  std::free(val);
+  spops_matrix_destroy(hh);
+  if (d::caching()) d::put(s.row_width, hd, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(hd);
+  return s;
+}
+
+template <class IndexType, class ValueType>
+SELL_C_Sigma_Matrix<IndexType, ValueType> csr_to_sell_c_sigma(
+    const CSR_Matrix<IndexType, ValueType>& csr, FILE* fp_feature, const int slicewidth = SELL_SIGMA,
+    const int chunkwidth = CHUNK_SIZE,
+    const spops_b200::detail::same_t<IndexType> alignment = (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  namespace d = spops_b200::detail;
+  (void)fp_feature;
+  spops_matrix_t c = d::upload_csr(csr), hh = nullptr, hd = nullptr;
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  p.sigma = slicewidth;
+  p.chunk = chunkwidth;
+  p.alignment = alignment;
+  try {
+    d::sell_pair(c, SPOPS_FMT_SELL_C_SIGMA, p, &hh, &hd);
+  } catch (...) {
+    spops_matrix_destroy(c);
+    throw;
+  }
+  spops_matrix_destroy(c);
+  const spops_matrix_info_t i = d::info(hh);
+  SELL_C_Sigma_Matrix<IndexType, ValueType> s;
+  d::set_features<IndexType, ValueType>(s, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  s.sliceWidth_Sigma = (IndexType)slicewidth;
+  s.chunkWidth_C = (IndexType)chunkwidth;
+  s.sliceNum = (IndexType)i.extra[0];
+  s.chunkNum = (IndexType)i.extra[1];
+  s.validchunkNum = (IndexType)i.extra[2];
+  s.chunk_num_per_slice = (IndexType)i.extra[3];
+  s.alignment = alignment;
+  s.reorder = d::fetch<IndexType>(hh, SPOPS_ARR_REORDER, nullptr);
+  s.chunk_len = d::fetch<IndexType>(hh, SPOPS_ARR_CHUNK_LEN, nullptr);
+  int64_t ncol = 0, nval = 0;
+  IndexType* col = d::fetch<IndexType>(hh, SPOPS_ARR_COL, &ncol);
+  ValueType* val = d::fetch<ValueType>(hh, SPOPS_ARR_VAL, &nval);
+  s.col_index = d::split_chunks(col, ncol, s.chunk_len, s.validchunkNum, chunkwidth);
+  s.values = d::split_chunks(val, nval, s.chunk_len, s.validchunkNum, chunkwidth);
+  std::free(col);
+  std::free(val);
+  spops_matrix_destroy(hh);
+  if (d::caching()) d::put(s.reorder, hd, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(hd);
+  return s;
+}
+
+template <class IndexType, class ValueType>
+SELL_C_R_Matrix<IndexType, ValueType> csr_to_sell_c_R(const CSR_Matrix<IndexType, ValueType>& csr, FILE* fp_feature,
+                                                      const int chunkwidth = CHUNK_SIZE,
+                                                      const spops_b200::detail::same_t<IndexType> alignment =
+                                                          (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  namespace d = spops_b200::detail;
+  (void)fp_feature;
+  spops_matrix_t c = d::upload_csr(csr), hh = nullptr, hd = nullptr;
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  p.chunk = chunkwidth;
+  p.alignment = alignment;
+  try {
+    d::sell_pair(c, SPOPS_FMT_SELL_C_R, p, &hh, &hd);
+  } catch (...) {
+    spops_matrix_destroy(c);
+    throw;
+  }
+  spops_matrix_destroy(c);
+  const spops_matrix_info_t i = d::info(hh);
+  SELL_C_R_Matrix<IndexType, ValueType> s;
+  d::set_features<IndexType, ValueType>(s, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  s.chunkWidth_C = (IndexType)chunkwidth;
+  s.validchunkNum = (IndexType)i.extra[0];
+  s.alignment = alignment;
+  s.reorder = d::fetch<IndexType>(hh, SPOPS_ARR_REORDER, nullptr);
+  s.chunk_len = d::fetch<IndexType>(hh, SPOPS_ARR_CHUNK_LEN, nullptr);
+  int64_t ncol = 0, nval = 0;
+  IndexType* col = d::fetch<IndexType>(hh, SPOPS_ARR_COL, &ncol);
+  ValueType* val = d::fetch<ValueType>(hh, SPOPS_ARR_VAL, &nval);
+  s.col_index = d::split_chunks(col, ncol, s.chunk_len, s.validchunkNum, chunkwidth);
+  s.values = d::split_chunks(val, nval, s.chunk_len, s.validchunkNum, chunkwidth);
+  std::free(col);
+  std::free(val);
+  spops_matrix_destroy(hh);
+  if (d::caching()) d::put(s.reorder, hd, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(hd);
+  return s;
+}
+
+template <class IndexType, class ValueType>
+DIA_Matrix<IndexType, ValueType> csr_to_dia(const CSR_Matrix<IndexType, ValueType>& csr,
+                                            const spops_b200::detail::same_t<IndexType> max_diags, FILE* fp_feature,
+                                            const spops_b200::detail::same_t<IndexType> alignment =
+                                                (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  namespace d = spops_b200::detail;
+  (void)fp_feature;
+  spops_matrix_t c = d::upload_csr(csr), h = nullptr;
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  p.max_diags = max_diags;
+  p.alignment = alignment;
+  spops_status_t s = spops_convert(d::ctx(), c, SPOPS_FMT_DIA, &p, &h);
+  spops_matrix_destroy(c);
+  d::check(s, "spops_convert");
+  const spops_matrix_info_t i = d::info(h);
+  DIA_Matrix<IndexType, ValueType> dia;
+  d::set_features<IndexType, ValueType>(dia, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  dia.complete_ndiags = (IndexType)i.extra[0];
+  dia.stride = (IndexType)i.extra[1];
+  dia.diag_offsets = reinterpret_cast<long int*>(d::fetch<int64_t>(h, SPOPS_ARR_DIAG_OFFSETS, nullptr));
+  dia.diag_data = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  if (d::caching()) d::put(dia.diag_offsets, h, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(h);
+  return dia;
+}
+
+template <class IndexType, class ValueType>
+BSR_Matrix<IndexType, ValueType> csr_to_bsr(const CSR_Matrix<IndexType, ValueType>& csr,
+                                            const spops_b200::detail::same_t<IndexType> blockDimRow = BSR_BlockDimRow,
+                                            spops_b200::detail::same_t<IndexType> blockDimCol =
+                                                (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t c = d::upload_csr(csr), h = nullptr;
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  p.block_rows = blockDimRow;
+  p.block_cols = blockDimCol;
+  spops_status_t s = spops_convert(d::ctx(), c, SPOPS_FMT_BSR, &p, &h);
+  spops_matrix_destroy(c);
+  d::check(s, "spops_convert");
+  const spops_matrix_info_t i = d::info(h);
+  BSR_Matrix<IndexType, ValueType> bsr;
+  d::set_features<IndexType, ValueType>(bsr, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  bsr.mb = (IndexType)i.extra[0];
+  bsr.nb = (IndexType)i.extra[1];
+  bsr.nnzb = (IndexType)i.extra[2];
+  bsr.blockDim_r = (IndexType)i.extra[3];
+  bsr.blockDim_c = (IndexType)i.extra[4];
+  bsr.blockNNZ = bsr.blockDim_r * bsr.blockDim_c;
+  bsr.row_ptr = d::fetch<IndexType>(h, SPOPS_ARR_BLOCK_ROW_PTR, nullptr);
+  bsr.block_colindex = d::fetch<IndexType>(h, SPOPS_ARR_BLOCK_COL, nullptr);
+  bsr.block_data = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  if (d::caching()) d::put(bsr.row_ptr, h, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(h);
+  return bsr;
+}
+
+template <class IndexType, class UIndexType, class ValueType>
+CSR5_Matrix<IndexType, UIndexType, ValueType> csr_to_csr5(const CSR_Matrix<IndexType, ValueType>& csr,
+                                                          FILE* fp_feature) {
+  namespace d = spops_b200::detail;
+  static_assert(sizeof(UIndexType) == 4, "CSR5 tile words are 32-bit");
+  (void)fp_feature;
+  spops_matrix_t c = d::upload_csr(csr), h = nullptr;
+  spops_format_params_t p;
+  std::memset(&p, 0, sizeof(p));
+  spops_status_t s = spops_convert(d::ctx(), c, SPOPS_FMT_CSR5, &p, &h);
+  spops_matrix_destroy(c);
+  d::check(s, "spops_convert");
+  const spops_matrix_info_t i = d::info(h);
+  CSR5_Matrix<IndexType, UIndexType, ValueType> m;
+  std::memset(static_cast<void*>(&m), 0, sizeof(m));
+  m.num_rows = csr.num_rows;
+  m.num_cols = csr.num_cols;
+  m.num_nnzs = csr.num_nnzs;
+  m.sparsity = (csr.num_rows > 0 && csr.num_cols > 0)
+                   ? (double)csr.num_nnzs / ((double)csr.num_rows * (double)csr.num_cols)
+                   : 0.0;
+  m.row_offset = d::host_alloc<IndexType>((int64_t)csr.num_rows + 1);
+  m.col_index = d::host_alloc<IndexType>(csr.num_nnzs);
+  m.values = d::host_alloc<ValueType>(csr.num_nnzs);
+  std::memcpy(m.row_offset, csr.row_offset, ((size_t)csr.num_rows + 1) * sizeof(IndexType));
+  std::memcpy(m.col_index, csr.col_index, (size_t)csr.num_nnzs * sizeof(IndexType));
+  std::memcpy(m.values, csr.values, (size_t)csr.num_nnzs * sizeof(ValueType));
+  m._p = (IndexType)i.extra[0];
+  m.omega = (IndexType)i.extra[1];
+  m.sigma = (IndexType)i.extra[2];
+  m.tile_ptr = d::fetch<UIndexType>(h, SPOPS_ARR_TILE_PTR, nullptr);
+  m.tile_desc = d::fetch<UIndexType>(h, SPOPS_ARR_TILE_DESC, nullptr);
+  if (d::caching()) d::put(m.tile_ptr, h, csr.num_rows, csr.num_cols, csr.num_nnzs); else spops_matrix_destroy(h);
+  return m;
+}
+
+/* ------------------------------------------------------------- delete */
+namespace spops_b200 {
+namespace detail {
+template <typename T>
+inline void free_array(T*& p) {
+  std::free(p);
+  p = nullptr;
+}
+template <typename T, typename I>
+inline void free_chunks(T**& parts, I n) {
+  if (parts) {
+    for (I c = 0; c < n; ++c) std::free(parts[c]);
+    delete[] parts;
+  }
+  parts = nullptr;
+}
+}  // namespace detail
+}  // namespace spops_b200
+
+template <typename I, typename V>
+void delete_host_matrix(COO_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.row_index);
+  spops_b200::detail::free_array(m.row_index);
+  spops_b200::detail::free_array(m.col_index);
+  spops_b200::detail::free_array(m.values);
+}
+template <typename I, typename V>
+void delete_host_matrix(CSR_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.row_offset);
+  spops_b200::detail::free_array(m.row_offset);
+  spops_b200::detail::free_array(m.col_index);
+  spops_b200::detail::free_array(m.values);
+}
+template <typename I, typename V>
+void delete_host_matrix(ELL_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.col_index);
+  spops_b200::detail::free_array(m.col_index);
+  spops_b200::detail::free_array(m.values);
+  m.max_row_width = m.min_row_width = 0;
+}
+template <typename I, typename V>
+void delete_host_matrix(S_ELL_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.row_width);
+  spops_b200::detail::free_chunks(m.col_index, m.chunk_num);
+  spops_b200::detail::free_chunks(m.values, m.chunk_num);
+  spops_b200::detail::free_array(m.row_width);
+  m.chunk_num = 0;
+}
+template <typename I, typename V>
+void delete_host_matrix(SELL_C_Sigma_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.reorder);
+  spops_b200::detail::free_chunks(m.col_index, m.validchunkNum);
+  spops_b200::detail::free_chunks(m.values, m.validchunkNum);
+  spops_b200::detail::free_array(m.reorder);
+  spops_b200::detail::free_array(m.chunk_len);
+  m.validchunkNum = m.chunkNum = m.sliceNum = 0;
+}
+template <typename I, typename V>
+void delete_host_matrix(SELL_C_R_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.reorder);
+  spops_b200::detail::free_chunks(m.col_index, m.validchunkNum);
+  spops_b200::detail::free_chunks(m.values, m.validchunkNum);
+  spops_b200::detail::free_array(m.reorder);
+  spops_b200::detail::free_array(m.chunk_len);
+  m.validchunkNum = 0;
+}
+template <typename I, typename V>
+void delete_host_matrix(DIA_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.diag_offsets);
+  spops_b200::detail::free_array(m.diag_offsets);
+  spops_b200::detail::free_array(m.diag_data);
+}
+template <typename I, typename V>
+void delete_host_matrix(BSR_Matrix<I, V>& m) {
+  spops_b200::invalidate(m.row_ptr);
+  spops_b200::detail::free_array(m.row_ptr);
+  spops_b200::detail::free_array(m.block_colindex);
+  spops_b200::detail::free_array(m.block_data);
+}
+template <typename I, typename U, typename V>
+void delete_host_matrix(CSR5_Matrix<I, U, V>& m) {
+  spops_b200::invalidate(m.tile_ptr);
+  spops_b200::detail::free_array(m.row_offset);
+  spops_b200::detail::free_array(m.col_index);
+  spops_b200::detail::free_array(m.values);
+  spops_b200::detail::free_array(m.tile_ptr);
+  spops_b200::detail::free_array(m.tile_desc);
+  spops_b200::detail::free_array(m.tile_desc_offset_ptr);
+  spops_b200::detail::free_array(m.tile_desc_offset);
+  spops_b200::detail::free_array(m.calibrator);
+}
+
+/* ------------------------------------------------- LeSpGEMM preprocessing */
+template <typename IndexType>
+std::vector<uint64_t> minhash_signatures_flat(const IndexType* rowptr, const IndexType* col_index, IndexType num_rows,
+                                              int k, uint64_t seed = 12345) {
+  namespace d = spops_b200::detail;
+  std::vector<uint64_t> sig((size_t)(num_rows > 0 ? num_rows : 0) * (size_t)(k > 0 ? k : 0));
+  if (num_rows <= 0 || k <= 0) return sig;
+  spops_matrix_t h = d::upload_pattern(rowptr, col_index, num_rows);
+  spops_status_t s = spops_minhash_host(d::ctx(), h, k, seed, sig.data());
+  spops_matrix_destroy(h);
+  d::check(s, "spops_minhash_host");
+  return sig;
+}
+
+template <typename IndexType, typename ValueType>
+std::vector<CandidatePair<IndexType, ValueType>> lsh_candidate_pairs_vector(const IndexType* rowptr,
+                                                                            const IndexType* col_index,
+                                                                            IndexType num_rows, int k, int num_bands,
+                                                                            uint64_t seed = 12345,
+                                                                            bool constrain_large_buckets = true) {
+  namespace d = spops_b200::detail;
+  std::vector<CandidatePair<IndexType, ValueType>> out;
+  if (num_rows <= 0) return out;
+  spops_matrix_t h = d::upload_pattern(rowptr, col_index, num_rows);
+  spops_pairs_t P = nullptr;
+  spops_status_t s = spops_lsh_pairs(d::ctx(), h, k, num_bands, seed, constrain_large_buckets ? 1 : 0, &P);
+  spops_matrix_destroy(h);
+  d::check(s, "spops_lsh_pairs");
+  int64_t n = 0;
+  spops_pairs_count(P, &n);
+  std::vector<int64_t> pi((size_t)n), pj((size_t)n);
+  std::vector<double> ps((size_t)n);
+  s = n ? spops_pairs_download(P, pi.data(), pj.data(), ps.data()) : SPOPS_OK;
+  spops_pairs_destroy(P);
+  d::check(s, "spops_pairs_download");
+  out.resize((size_t)n);
+  for (int64_t t = 0; t < n; ++t)
+    out[(size_t)t] = CandidatePair<IndexType, ValueType>{(IndexType)pi[(size_t)t], (IndexType)pj[(size_t)t],
+                                                         (ValueType)ps[(size_t)t]};
+  return out;
+}
+
+template <typename IndexType, typename ValueType, typename PairLike>
+inline void hierarchical_clustering_v0_fast(const IndexType* rowptr, const IndexType* colids, IndexType num_rows,
+                                            const std::vector<PairLike>& pairs, IndexType cluster_size,
+                                            std::vector<IndexType>& permutation_out,
+                                            std::vector<IndexType>& offsets_out) {
+  namespace d = spops_b200::detail;
+  const int64_t n = num_rows > 0 ? num_rows : 0, nnz = n ? (int64_t)rowptr[n] : 0;
+  std::vector<int64_t> rp((size_t)n + 1), ci((size_t)nnz), pi(pairs.size()), pj(pairs.size());
+  std::vector<double> ps(pairs.size());
+  for (int64_t r = 0; r <= n && n; ++r) rp[(size_t)r] = (int64_t)rowptr[r];
+  for (int64_t e = 0; e < nnz; ++e) ci[(size_t)e] = (int64_t)colids[e];
+  for (size_t t = 0; t < pairs.size(); ++t) {
+    pi[t] = (int64_t)pairs[t].i;
+    pj[t] = (int64_t)pairs[t].j;
+    ps[t] = (double)pairs[t].score;
+  }
+  std::vector<int64_t> perm((size_t)n), offs((size_t)n + 1);
+  int64_t ncl = 0;
+  d::check(spops_hierarchical_clustering(rp.data(), ci.data(), n, pi.data(), pj.data(), ps.data(),
+                                         (int64_t)pairs.size(), cluster_size, perm.data(), offs.data(), &ncl),
+           "spops_hierarchical_clustering");
+  permutation_out.assign(perm.begin(), perm.end());
+  offsets_out.assign(offs.begin(), offs.begin() + ncl + 1);
+}
+
+#endif /* SPOPS_B200_CXX_SPOPS_H */

@@ -88,6 +88,7 @@ _SIGS = {
     "spops_batch_capture": [vp, vp, dbl, dbl],
     "spops_batch_info": [vp, vp, vp, vp],
     "spops_minhash": [vp, vp, i32, u64, vp],
+    "spops_minhash_host": [vp, vp, i32, u64, vp],
     "spops_lsh_pairs": [vp, vp, i32, i32, u64, i32, vp],
     "spops_lsh_pairs_from_signatures": [vp, vp, i64, i32, i32, i32, vp],
     "spops_pairs_count": [vp, vp],

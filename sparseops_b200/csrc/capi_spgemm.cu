@@ -67,6 +67,25 @@ spops_status_t spops_minhash(spops_context_t ctx, spops_matrix_t A, int32_t k, u
   return minhash_signatures(ctx, A, k, seed, static_cast<uint64_t*>(sig));
 }
 
+spops_status_t spops_minhash_host(spops_context_t ctx, spops_matrix_t A, int32_t k, uint64_t seed, void* sig_host) {
+  if (!ctx || !A || (!sig_host && A->rows > 0)) return fail(SPOPS_ERR_INVALID, "spops_minhash_host: null argument");
+  if (k <= 0) return fail(SPOPS_ERR_INVALID, "spops_minhash_host: k must be positive");
+  DeviceGuard g(ctx->device);
+  const size_t bytes = (size_t)std::max<int64_t>(A->rows, 1) * (size_t)k * 8;
+  DevBuf sig;
+  SPOPS_TRY(sig.alloc(bytes));
+  spops_status_t s = minhash_signatures(ctx, A, k, seed, sig.as<uint64_t>());
+  if (s == SPOPS_OK && A->rows > 0) {
+    const cudaError_t e = cudaMemcpyAsync(sig_host, sig.p, (size_t)A->rows * (size_t)k * 8, cudaMemcpyDeviceToHost,
+                                          ctx->stream);
+    const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess || e2 != cudaSuccess)
+      s = fail(SPOPS_ERR_CUDA, "spops_minhash_host: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  sig.release();
+  return s;
+}
+
 spops_status_t spops_lsh_pairs_from_signatures(spops_context_t ctx, const void* sig, int64_t rows, int32_t k,
                                                int32_t bands, int32_t constrain, spops_pairs_t* out) {
   if (!ctx || !out || (!sig && rows > 0)) return fail(SPOPS_ERR_INVALID, "spops_lsh_pairs_from_signatures: null");

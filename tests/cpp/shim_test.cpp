@@ -1,0 +1,261 @@
+// Exercises include/spops_b200/SpOps.h the way a caller of the reference's
+// SpOps.h would: host structs and vectors in, host results out.  Every SpMV
+// is checked against a plain CPU loop (componentwise error over |A||x|,
+// 1e-12 for double, 1e-5 for float); conversions against properties of the
+// reference layouts.  Prints "shim OK" and exits 0 on success.
+#include "SpOps.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+static int failures = 0;
+#define EXPECT(cond, msg)                                          \
+  do {                                                             \
+    if (!(cond)) {                                                 \
+      std::printf("FAIL %s:%d %s\n", __FILE__, __LINE__, msg);     \
+      ++failures;                                                  \
+    }                                                              \
+  } while (0)
+
+template <typename I, typename V>
+CSR_Matrix<I, V> random_csr(I n, I ncols, unsigned seed, bool banded) {
+  std::mt19937_64 rng(seed);
+  std::vector<I> rp(1, 0), ci;
+  std::vector<V> v;
+  for (I r = 0; r < n; ++r) {
+    int len = (int)(rng() % 40);
+    if (r % 97 == 5) len = 0;     // empty rows
+    if (r == 11) len = 900;       // a long row
+    std::vector<I> cols;
+    for (int k = 0; k < len; ++k) {
+      I c = banded ? (I)((int64_t)r + (int64_t)(rng() % 9) - 4) : (I)(rng() % (uint64_t)ncols);
+      if (c >= 0 && c < ncols) cols.push_back(c);
+    }
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+    for (I c : cols) {
+      ci.push_back(c);
+      v.push_back((V)((double)(rng() % 2001) / 1000.0 - 1.0));
+    }
+    rp.push_back((I)ci.size());
+  }
+  CSR_Matrix<I, V> A;
+  std::memset(static_cast<void*>(&A), 0, sizeof(A));
+  A.num_rows = n;
+  A.num_cols = ncols;
+  A.num_nnzs = (I)ci.size();
+  A.row_offset = spops_b200::detail::host_alloc<I>((int64_t)rp.size());
+  A.col_index = spops_b200::detail::host_alloc<I>((int64_t)ci.size());
+  A.values = spops_b200::detail::host_alloc<V>((int64_t)v.size());
+  std::copy(rp.begin(), rp.end(), A.row_offset);
+  std::copy(ci.begin(), ci.end(), A.col_index);
+  std::copy(v.begin(), v.end(), A.values);
+  return A;
+}
+
+template <typename I, typename V>
+void check_y(const char* what, const CSR_Matrix<I, V>& A, const std::vector<V>& x, const std::vector<V>& y0,
+             double alpha, double beta, const std::vector<V>& y) {
+  const double tol = sizeof(V) == 8 ? 1e-12 : 1e-5;
+  double worst = 0;
+  for (I r = 0; r < A.num_rows; ++r) {
+    double s = 0, a = 0;
+    for (I k = A.row_offset[r]; k < A.row_offset[r + 1]; ++k) {
+      s += (double)A.values[k] * (double)x[A.col_index[k]];
+      a += std::fabs((double)A.values[k] * (double)x[A.col_index[k]]);
+    }
+    const double ref = alpha * s + beta * (double)y0[r];
+    const double den = std::fabs(alpha) * a + std::fabs(beta * (double)y0[r]);
+    worst = std::max(worst, std::fabs((double)y[r] - ref) / std::max(den, 1e-300));
+  }
+  if (worst > tol) std::printf("  %s: error %.3e\n", what, worst);
+  EXPECT(worst <= tol, what);
+}
+
+template <typename I, typename V>
+void run_all() {
+  const I n = 3001, nc = 2500;
+  CSR_Matrix<I, V> A = random_csr<I, V>(n, nc, 7, false);
+  std::vector<V> x(nc), y0(n);
+  std::mt19937_64 rng(3);
+  for (auto& t : x) t = (V)((double)(rng() % 2001) / 1000.0 - 1.0);
+  for (auto& t : y0) t = (V)((double)(rng() % 2001) / 1000.0 - 1.0);
+  const double alpha = 0.8, beta = 0.7;
+  auto run = [&](const char* what, auto&& op) {
+    std::printf("  %s (index %zu bytes, value %zu bytes)\n", what, sizeof(I), sizeof(V));
+    std::vector<V> y = y0;
+    op((V)alpha, x.data(), (V)beta, y.data());
+    check_y(what, A, x, y0, alpha, beta, y);
+  };
+  run("SpOps_csr", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+  run("SpOps_csr again (cached)", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+
+  // COO both ways
+  COO_Matrix<I, V> coo = csr_to_coo(A);
+  EXPECT(coo.num_nnzs == A.num_nnzs, "csr_to_coo nnz");
+  bool rows_ok = true;
+  for (I r = 0; r < n; ++r)
+    for (I k = A.row_offset[r]; k < A.row_offset[r + 1]; ++k)
+      rows_ok = rows_ok && coo.row_index[k] == r && coo.col_index[k] == A.col_index[k] && coo.values[k] == A.values[k];
+  EXPECT(rows_ok, "csr_to_coo arrays");
+  run("SpOps_coo", [&](V a, const V* xx, V b, V* yy) { SpOps_coo(a, coo, xx, b, yy); });
+  CSR_Matrix<I, V> back = coo_to_csr(coo);
+  bool same = back.num_nnzs == A.num_nnzs;
+  for (I r = 0; same && r <= n; ++r) same = back.row_offset[r] == A.row_offset[r];
+  for (I k = 0; same && k < A.num_nnzs; ++k) same = back.col_index[k] == A.col_index[k] && back.values[k] == A.values[k];
+  EXPECT(same, "coo_to_csr round trip");
+  // compact: a row with duplicates in file order 5, 3, 5, 7 (7 cancels) -> 3, 5
+  {
+    COO_Matrix<I, V> d;
+    std::memset(static_cast<void*>(&d), 0, sizeof(d));
+    d.num_rows = 2;
+    d.num_cols = 8;
+    d.num_nnzs = 5;
+    I ri[5] = {1, 1, 1, 1, 1}, cj[5] = {5, 3, 5, 7, 7};
+    V vv[5] = {(V)1, (V)2, (V)4, (V)1.5, (V)-1.5};
+    d.row_index = ri;
+    d.col_index = cj;
+    d.values = vv;
+    CSR_Matrix<I, V> c = coo_to_csr(d, true);
+    EXPECT(c.num_nnzs == 2 && c.row_offset[1] == 0 && c.row_offset[2] == 2, "compact sizes");
+    EXPECT(c.col_index[0] == 3 && c.col_index[1] == 5 && c.values[0] == (V)2 && c.values[1] == (V)5,
+           "compact order: reverse first appearance, zeros dropped");
+    delete_host_matrix(c);
+  }
+
+  ELL_Matrix<I, V> ell = csr_to_ell(A, RowMajor);
+  I widest = 0;
+  for (I r = 0; r < n; ++r) widest = std::max(widest, (I)(A.row_offset[r + 1] - A.row_offset[r]));
+  bool ell_ok = ell.max_row_width == widest;
+  for (I r = 0; ell_ok && r < n; ++r) {
+    const I len = A.row_offset[r + 1] - A.row_offset[r];
+    for (I k = 0; ell_ok && k < ell.max_row_width; ++k) {
+      const I c = ell.col_index[(int64_t)r * ell.max_row_width + k];
+      ell_ok = k < len ? c == A.col_index[A.row_offset[r] + k] : c == (I)-1;
+    }
+  }
+  EXPECT(ell_ok, "csr_to_ell row-major layout");
+  run("SpOps_ell", [&](V a, const V* xx, V b, V* yy) { SpOps_ell(a, ell, xx, b, yy); });
+
+  S_ELL_Matrix<I, V> sell = csr_to_sell(A, nullptr, 4, 4);
+  EXPECT(sell.chunk_num == (n + 3) / 4, "csr_to_sell chunk_num");
+  run("SpOps_sell", [&](V a, const V* xx, V b, V* yy) { SpOps_sell(a, sell, xx, b, yy); });
+
+  SELL_C_Sigma_Matrix<I, V> scs = csr_to_sell_c_sigma(A, nullptr, 512, 32, 1);
+  std::vector<int> seen(n, 0);
+  for (I r = 0; r < n; ++r) seen[scs.reorder[r]]++;
+  EXPECT(std::count(seen.begin(), seen.end(), 1) == n, "sell_c_sigma reorder is a permutation");
+  bool desc = true;  // within each slice of 512 stored rows, lengths do not increase
+  for (I r = 1; r < n; ++r)
+    if (r % 512) {
+      const I a0 = scs.reorder[r - 1], a1 = scs.reorder[r];
+      desc = desc && (A.row_offset[a0 + 1] - A.row_offset[a0]) >= (A.row_offset[a1 + 1] - A.row_offset[a1]);
+    }
+  EXPECT(desc, "sell_c_sigma slices sorted by length");
+  run("SpOps_sell_c_sigma", [&](V a, const V* xx, V b, V* yy) { SpOps_sell_c_sigma(a, scs, xx, b, yy); });
+  // the same struct uploaded from its host arrays (as a struct a caller built)
+  spops_b200::invalidate(scs.reorder);
+  run("SpOps_sell_c_sigma from host arrays", [&](V a, const V* xx, V b, V* yy) { SpOps_sell_c_sigma(a, scs, xx, b, yy); });
+
+  SELL_C_R_Matrix<I, V> scr = csr_to_sell_c_R(A, nullptr, 32, 1);
+  run("SpOps_sell_c_R", [&](V a, const V* xx, V b, V* yy) { SpOps_sell_c_R(a, scr, xx, b, yy); });
+  spops_b200::invalidate(scr.reorder);
+  run("SpOps_sell_c_R from host arrays", [&](V a, const V* xx, V b, V* yy) { SpOps_sell_c_R(a, scr, xx, b, yy); });
+
+  BSR_Matrix<I, V> bsr = csr_to_bsr(A, (I)4, (I)4);
+  EXPECT(bsr.blockDim_r == 4 && bsr.blockDim_c == 4 && bsr.row_ptr[bsr.mb] == bsr.nnzb, "csr_to_bsr shape");
+  run("SpOps_bsr", [&](V a, const V* xx, V b, V* yy) { SpOps_bsr(a, bsr, xx, b, yy); });
+  spops_b200::invalidate(bsr.row_ptr);
+  run("SpOps_bsr from host arrays", [&](V a, const V* xx, V b, V* yy) { SpOps_bsr(a, bsr, xx, b, yy); });
+
+  CSR5_Matrix<I, uint32_t, V> c5 = csr_to_csr5<I, uint32_t, V>(A, nullptr);
+  EXPECT(c5.omega == 32 && c5.sigma == 16, "csr5 tile shape");
+  run("SpOps_csr5", [&](V a, const V* xx, V b, V* yy) { SpOps_csr5(a, c5, xx, b, yy); });
+
+  // DIA on a banded matrix
+  CSR_Matrix<I, V> B = random_csr<I, V>(n, n, 9, true);
+  DIA_Matrix<I, V> dia = csr_to_dia(B, (I)MAX_DIAG_NUM, nullptr, (I)4);
+  EXPECT(dia.complete_ndiags >= 1 && dia.complete_ndiags <= 9, "csr_to_dia diagonals");
+  {
+    std::vector<V> xb(n), yb0(n), yb;
+    for (I r = 0; r < n; ++r) {
+      xb[r] = (V)((double)((r * 37) % 101) / 50.0 - 1.0);
+      yb0[r] = (V)((double)((r * 11) % 13) / 6.0 - 1.0);
+    }
+    yb = yb0;
+    SpOps_dia((V)alpha, dia, xb.data(), (V)beta, yb.data());
+    check_y("SpOps_dia", B, xb, yb0, alpha, beta, yb);
+    spops_b200::invalidate(dia.diag_offsets);
+    yb = yb0;
+    SpOps_dia((V)alpha, dia, xb.data(), (V)beta, yb.data());
+    check_y("SpOps_dia from host arrays", B, xb, yb0, alpha, beta, yb);
+  }
+
+  // upload on every call
+  spops_b200::set_cache(false);
+  run("SpOps_csr without cache", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+  spops_b200::set_cache(true);
+
+  delete_host_matrix(back);
+  delete_host_matrix(coo);
+  delete_host_matrix(ell);
+  delete_host_matrix(sell);
+  delete_host_matrix(scs);
+  delete_host_matrix(scr);
+  delete_host_matrix(bsr);
+  delete_host_matrix(c5);
+  delete_host_matrix(dia);
+  delete_host_matrix(B);
+  delete_host_matrix(A);
+}
+
+void lsh_checks() {
+  // 64 rows in 4 groups of identical patterns: every group must end up together
+  std::vector<long long> rp(1, 0), ci;
+  for (int r = 0; r < 64; ++r) {
+    const int g = r % 4;
+    for (int k = 0; k < 12; ++k) ci.push_back(g * 100 + k * 3);
+    rp.push_back((long long)ci.size());
+  }
+  std::vector<uint64_t> sig = minhash_signatures_flat<long long>(rp.data(), ci.data(), 64, 64, 7);
+  EXPECT(sig.size() == 64 * 64, "minhash size");
+  bool same = true;
+  for (int k = 0; k < 64; ++k) same = same && sig[(size_t)0 * 64 + k] == sig[(size_t)4 * 64 + k];
+  EXPECT(same, "identical rows share signatures");
+  auto pairs = lsh_candidate_pairs_vector<long long, double>(rp.data(), ci.data(), 64, 64, 16, 7, true);
+  EXPECT(!pairs.empty(), "lsh pairs found");
+  bool within = true;
+  for (auto& p : pairs) within = within && (p.i % 4) == (p.j % 4) && p.i < p.j && p.score == 1.0;
+  EXPECT(within, "pairs only inside groups, score 1");
+  std::vector<long long> perm, offs;
+  hierarchical_clustering_v0_fast<long long, double>(rp.data(), ci.data(), 64, pairs, 8LL, perm, offs);
+  EXPECT(perm.size() == 64 && offs.front() == 0 && offs.back() == 64, "clustering shape");
+  bool grouped = true;
+  for (size_t c = 0; c + 1 < offs.size(); ++c) {
+    EXPECT(offs[c + 1] - offs[c] <= 8, "cluster size cap");
+    for (long long t = offs[c]; t < offs[c + 1]; ++t) grouped = grouped && perm[t] % 4 == perm[offs[c]] % 4;
+  }
+  EXPECT(grouped, "clusters inside groups");
+}
+
+int main() {
+  std::setvbuf(stdout, nullptr, _IONBF, 0);
+  try {
+    run_all<int, double>();
+    run_all<int, float>();
+    run_all<long long, double>();
+    lsh_checks();
+  } catch (const std::exception& e) {
+    std::printf("exception: %s\n", e.what());
+    return 2;
+  }
+  if (failures) {
+    std::printf("%d failure(s)\n", failures);
+    return 1;
+  }
+  std::printf("shim OK\n");
+  return 0;
+}
