@@ -342,6 +342,48 @@ spops_status_t spops_spmv_t(spops_context_t ctx, double alpha, spops_matrix_t A,
 spops_status_t spops_sddmm(spops_context_t ctx, double alpha, spops_matrix_t A, const void* g, const void* x,
                            void* out);
 
+/* ------------------------------------------- features and format choice */
+/* Structure features of a CSR matrix, computed on the device.  Replaces the
+ * non-tile part of MTX::CalculateFeatures (src/sparse_features.cpp:643-775,
+ * with the per-entry counts MTX::MtxLoad gathers, :336-478) for a general
+ * (non-symmetric storage) matrix without duplicate entries:
+ *   ndiags / diag_close_ratio: distinct diagonals; share of entries with
+ *     |col - row| <= (rows + cols - 1) / 20
+ *   p_ratio_*: smallest fraction p of rows (columns) holding at least 1 - p
+ *     of the entries; gini_*: Gini coefficient of the per-row (per-column)
+ *     counts by the trapezoid rule
+ *   diagonal_dominant_ratio: rows whose |a_ii| exceeds the sum of their
+ *     off-diagonal |a_ij|, over min(rows, cols)
+ *   row_ / col_variability: largest log10 range of |a| over rows (columns)
+ *     that hold a value below 1, with the reference's clamping at 0 (-1 if none)
+ *   pattern_symm / value_symm (square only): share of off-diagonal entries
+ *     whose mirror exists / exists with the same value printed to 6 decimals */
+typedef struct {
+  int64_t rows, cols, nnz;
+  int64_t nnz_lower, nnz_upper, nnz_diagonal, ndiags;
+  int64_t min_nnz_row, max_nnz_row, min_nnz_col, max_nnz_col;
+  double nnz_ratio, diag_close_ratio, pattern_symm, value_symm;
+  double nz_row_ratio, ave_nnz_row, var_nnz_row, std_nnz_row, p_ratio_row, gini_row;
+  double nz_col_ratio, ave_nnz_col, var_nnz_col, std_nnz_col, p_ratio_col, gini_col;
+  double diagonal_dominant_ratio, max_value_offdiag, max_value_diagonal, row_variability, col_variability;
+} spops_features_t;
+spops_status_t spops_matrix_features(spops_context_t ctx, spops_matrix_t csr, spops_features_t* features);
+
+/* Storage format for y = A*x on this GPU.  No counterpart in the reference,
+ * which computes features but leaves the choice to the caller.
+ *   mode 0: rules on the features -- DIA when at most 64 diagonals hold at
+ *     least half of the diagonal slots, otherwise CSR (the default CSR kernel
+ *     needs no conversion and is within a few percent of the best padded
+ *     format on irregular rows);
+ *   mode 1: timed -- converts to each candidate (CSR, SELL-C-R and
+ *     SELL-C-sigma with C = 32, CSR5, and DIA / BSR where the features allow
+ *     them), runs a few SpMVs of each on the context stream, and returns the
+ *     fastest.
+ * *params receives the conversion parameters for spops_convert; ms (may be
+ * NULL) the measured time per SpMV of the choice (mode 1; 0 in mode 0). */
+spops_status_t spops_select_format(spops_context_t ctx, spops_matrix_t csr, int32_t mode, spops_format_t* format,
+                                   spops_format_params_t* params, double* ms);
+
 /* ------------------------------------------------------ no allocation */
 /* y = alpha*A*x + beta*y for a CSR matrix given by device pointers, without
  * allocating any device memory.  No counterpart in the reference: it is for

@@ -164,6 +164,15 @@ class Oracle:
         brp = B[0]
         return int(self.L.orc_spgemm_flop(_i64(len(arp) - 1), _p(arp), _p(aci), _i64(len(brp) - 1), _p(brp)))
 
+    # ---- features
+    def features(self, rp, ci, v, ncols):
+        """The 32 feature values (spops_features_t order) of a CSR matrix."""
+        out = np.zeros(32)
+        self.L.orc_features(_i64(len(rp) - 1), _i64(ncols), _p(np.ascontiguousarray(rp, np.int64)),
+                            _p(np.ascontiguousarray(ci, np.int64)), _p(np.ascontiguousarray(v, np.float64)),
+                            _p(out))
+        return out
+
     # ---- COO -> CSR
     def coo_to_csr(self, n, ri, ci, v, compact=False):
         """(rp, ci, v) of coo_to_csr; v's dtype (float32 / float64) is kept."""
@@ -323,6 +332,28 @@ class Reference:
         self.L.ref_csr_copy(_vp(h), _p(rp), _p(oc), _p(ov))
         self.L.ref_csr_free(_vp(h))
         return rp, oc[:info[2]], ov[:info[2]]
+
+    def features(self, rp, ci, v, ncols):
+        """The reference's MtxLoad + CalculateFeatures on the matrix written as
+        a general real Matrix Market file (entries in CSR order)."""
+        import tempfile
+        fd, path = tempfile.mkstemp(suffix=".mtx")
+        try:
+            with os.fdopen(fd, "w") as f:
+                n = len(rp) - 1
+                f.write("%%MatrixMarket matrix coordinate real general\n")
+                f.write(f"{n} {ncols} {len(ci)}\n")
+                rows = np.repeat(np.arange(n), np.diff(np.asarray(rp, np.int64)))
+                for r, c, x in zip(rows, ci, v):
+                    f.write(f"{r + 1} {c + 1} {float(x)!r}\n")
+            out = np.zeros(32)
+            self.L.ref_features.restype = C.c_int
+            rc = self.L.ref_features(path.encode(), _p(out))
+            if rc != 0:
+                raise RuntimeError(f"ref_features failed ({rc})")
+            return out
+        finally:
+            os.remove(path)
 
     def csr_transpose(self, rp, ci, v, ncols):
         h = self.L.ref_csr_transpose(_i64(len(rp) - 1), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _p(v))

@@ -6,6 +6,10 @@
 #include "spops_oracle.h"
 
 #include <algorithm>
+#include <cfloat>
+#include <cstdio>
+#include <numeric>
+#include <string>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -530,6 +534,123 @@ int64_t orc_coo_to_csr_f64(int64_t n, int64_t nnz, const int64_t* ri, const int6
 int64_t orc_coo_to_csr_f32(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const float* v,
                            int32_t compact, int64_t* rp, int64_t* oc, float* ov) {
   return coo_to_csr_impl<float>(n, nnz, ri, ci, v, compact, rp, oc, ov);
+}
+
+// ------------------------------------------------------------ features
+// MTX::CalculateFeatures (src/sparse_features.cpp:643-775) with the counts
+// MtxLoad gathers for a general real matrix (:336-478), read in CSR order.
+// out: the 32 values of spops_features_t, in its order.
+static void count_stats(const std::vector<int64_t>& cnt, int64_t nnz, double* nzr, int64_t* mn, int64_t* mx,
+                        double* ave, double* var, double* sd, double* p, double* gini) {
+  const int64_t len = (int64_t)cnt.size();
+  int64_t nzc = 0, lo = 100000000, hi = 0;
+  *ave = (double)nnz / (double)len;
+  double v = 0.0;
+  for (int64_t c : cnt) {
+    lo = std::min(lo, c);
+    hi = std::max(hi, c);
+    if (c) ++nzc;
+    const double d = (double)c - *ave;
+    v += d * d;
+  }
+  *nzr = (double)nzc / (double)len;
+  *mn = lo;
+  *mx = hi;
+  *var = v / (double)len;
+  *sd = std::sqrt(*var);
+  std::vector<int64_t> o(cnt);
+  std::sort(o.begin(), o.end());
+  int64_t quit = len, count = 0, step = 0;
+  double pt = 0.0, q = 0.0;
+  do {
+    --quit;
+    ++count;
+    step += o[(size_t)quit];
+    pt = (double)count / (double)len;
+    q = (double)step / (double)nnz;
+  } while (pt + q < 1.0 && quit > 0);
+  *p = pt;
+  std::vector<int64_t> cum(o.size());
+  std::partial_sum(o.begin(), o.end(), cum.begin());
+  double area = (double)(cum[0] + 0) / 2.0;
+  for (size_t i = 0; i + 1 < cum.size(); ++i) area += (double)(cum[i] + cum[i + 1]) / 2.0;
+  const double total = (double)nnz * (double)len / 2.0;
+  *gini = (total - area) / total;
+}
+
+void orc_features(int64_t n, int64_t nc, const int64_t* rp, const int64_t* ci, const double* v, double* out) {
+  std::vector<int64_t> rcnt((size_t)n, 0), ccnt((size_t)nc, 0);
+  std::vector<double> dom((size_t)n, 0.0), rmax((size_t)n, 0.0), rmin((size_t)n, 0.0), cmax((size_t)nc, 0.0),
+      cmin((size_t)nc, 0.0);
+  std::map<int64_t, int64_t> diag;
+  int64_t lower = 0, upper = 0, dg = 0;
+  double maxd = -DBL_MAX, maxo = -DBL_MAX;
+  const int64_t nnz = n ? rp[n] : 0;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) {
+      const int64_t c = ci[k], d = c - r;
+      const double a = std::fabs(v[k]);
+      ++rcnt[(size_t)r];
+      ++ccnt[(size_t)c];
+      ++diag[d];
+      if (d == 0) {
+        ++dg;
+        maxd = std::max(maxd, a);
+        dom[(size_t)r] += a;
+      } else {
+        if (d < 0) ++lower; else ++upper;
+        maxo = std::max(maxo, a);
+        dom[(size_t)r] -= a;
+      }
+      const double l = std::log10(a);
+      if (rmax[(size_t)r] < l) rmax[(size_t)r] = l;
+      if (a > 0.0 && rmin[(size_t)r] > l) rmin[(size_t)r] = l;
+      if (cmax[(size_t)c] < l) cmax[(size_t)c] = l;
+      if (a > 0.0 && cmin[(size_t)c] > l) cmin[(size_t)c] = l;
+    }
+  const int64_t thr = (n + nc - 1) / 20;
+  int64_t close = 0;
+  for (const auto& kv : diag)
+    if (std::llabs(kv.first) <= thr) close += kv.second;
+  double rvar = -1.0, cvar = -1.0;
+  int64_t dominant = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    if (rmin[(size_t)r] != 0.0) rvar = std::max(rvar, rmax[(size_t)r] - rmin[(size_t)r]);
+    if (dom[(size_t)r] > 0) ++dominant;
+  }
+  for (int64_t c = 0; c < nc; ++c)
+    if (cmin[(size_t)c] != 0.0) cvar = std::max(cvar, cmax[(size_t)c] - cmin[(size_t)c]);
+  double ps = 0.0, vs = 0.0;
+  if (n == nc) {
+    std::map<std::pair<int64_t, int64_t>, std::string> text;
+    char buf[64];
+    for (int64_t r = 0; r < n; ++r)
+      for (int64_t k = rp[r]; k < rp[r + 1]; ++k) {
+        std::snprintf(buf, sizeof(buf), "%lf", v[k]);
+        text.emplace(std::make_pair(r, ci[k]), buf);
+      }
+    int64_t sp = 0, sv = 0;
+    for (const auto& kv : text) {
+      if (kv.first.first == kv.first.second) continue;
+      auto it = text.find(std::make_pair(kv.first.second, kv.first.first));
+      if (it != text.end()) {
+        ++sp;
+        if (it->second == kv.second) ++sv;
+      }
+    }
+    ps = (double)sp / (double)(nnz - dg);
+    vs = (double)sv / (double)(nnz - dg);
+  }
+  double rnz, rave, rv, rsd, rp_, rg, cnz, cave, cv, csd, cp_, cg;
+  int64_t rmn, rmx, cmn, cmx;
+  count_stats(rcnt, nnz, &rnz, &rmn, &rmx, &rave, &rv, &rsd, &rp_, &rg);
+  count_stats(ccnt, nnz, &cnz, &cmn, &cmx, &cave, &cv, &csd, &cp_, &cg);
+  const double vals[32] = {(double)n, (double)nc, (double)nnz, (double)lower, (double)upper, (double)dg,
+                           (double)diag.size(), (double)rmn, (double)rmx, (double)cmn, (double)cmx,
+                           (double)nnz / ((double)n * (double)nc), (double)close / (double)nnz, ps, vs, rnz, rave, rv,
+                           rsd, rp_, rg, cnz, cave, cv, csd, cp_, cg, (double)dominant / (double)std::min(n, nc),
+                           maxo, maxd, rvar, cvar};
+  std::memcpy(out, vals, sizeof(vals));
 }
 
 // ------------------------------------------------------------ adjoints

@@ -81,6 +81,10 @@ int64_t orc_coo_to_csr_f64(int64_t n, int64_t nnz, const int64_t* ri, const int6
 int64_t orc_coo_to_csr_f32(int64_t n, int64_t nnz, const int64_t* ri, const int64_t* ci, const float* v,
                            int32_t compact, int64_t* rp, int64_t* oc, float* ov);
 
+/* Structure features (src/sparse_features.cpp:643-775 with MtxLoad's counts,
+ * :336-478) of a general CSR matrix, in spops_features_t order (32 values). */
+void orc_features(int64_t n, int64_t nc, const int64_t* rp, const int64_t* ci, const double* v, double* out);
+
 /* y = A^T g by scatter (the value the reference's csr_transpose + SpOps_csr
  * gives, include/sparse_conversion.h:2066-2108), FP64. */
 void orc_spmv_t_csr_f64_i32(int64_t nr, int64_t nc, const int32_t* rp, const int32_t* ci, const double* v,

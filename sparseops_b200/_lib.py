@@ -53,6 +53,21 @@ class FormatParams(C.Structure):
                 ("block_cols", i64), ("layout", i32), ("reserved", i32)]
 
 
+FEATURE_NAMES = ("rows", "cols", "nnz", "nnz_lower", "nnz_upper", "nnz_diagonal", "ndiags", "min_nnz_row",
+                 "max_nnz_row", "min_nnz_col", "max_nnz_col", "nnz_ratio", "diag_close_ratio", "pattern_symm",
+                 "value_symm", "nz_row_ratio", "ave_nnz_row", "var_nnz_row", "std_nnz_row", "p_ratio_row",
+                 "gini_row", "nz_col_ratio", "ave_nnz_col", "var_nnz_col", "std_nnz_col", "p_ratio_col",
+                 "gini_col", "diagonal_dominant_ratio", "max_value_offdiag", "max_value_diagonal",
+                 "row_variability", "col_variability")
+
+
+class Features(C.Structure):
+    _fields_ = [(n, i64) for n in FEATURE_NAMES[:11]] + [(n, C.c_double) for n in FEATURE_NAMES[11:]]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n in FEATURE_NAMES}
+
+
 # name -> argtypes (restype is spops_status_t unless listed in _RESTYPE)
 _SIGS = {
     "spops_create": [vp, C.c_int, vp],
@@ -63,6 +78,8 @@ _SIGS = {
     "spops_set_option": [vp, C.c_char_p, i64],
     "spops_csr_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
     "spops_coo_to_csr": [vp, vp, C.c_int32, C.POINTER(vp)],
+    "spops_matrix_features": [vp, vp, vp],
+    "spops_select_format": [vp, vp, i32, C.POINTER(C.c_int), vp, C.POINTER(C.c_double)],
     "spops_matrix_destroy": [vp],
     "spops_matrix_info": [vp, vp],
     "spops_matrix_touch": [vp],

@@ -380,6 +380,60 @@ def csr_to_csr5(csr: CSR_Matrix, fp_feature=None):
     return _wrap(CSR5_Matrix, csr, h, row_offset=csr.row_offset, col_index=csr.col_index, values=csr.values)
 
 
+def matrix_features(csr: CSR_Matrix) -> dict:
+    """Structure features of the matrix, on the device: the non-tile part of
+    the reference's MTX::CalculateFeatures (src/sparse_features.cpp:643) as
+    a dict (names of spops_features_t)."""
+    h = csr.device()
+    f = _lib.Features()
+    call("spops_matrix_features", h.ctx.follow_torch().handle, h.handle, C.byref(f))
+    return f.as_dict()
+
+
+_FORMAT_NAMES = {v: k for k, v in _lib.FORMATS.items()}
+
+
+def select_format(csr: CSR_Matrix, timed: bool = False) -> dict:
+    """Storage format for SpMV with this matrix on this GPU: rules on the
+    features (timed=False) or the fastest of the candidate formats measured
+    on the device (timed=True).  Returns {"format", "params", "ms"}; the
+    params are the spops_convert parameters (see convert_to)."""
+    h = csr.device()
+    fmt = C.c_int()
+    p = FormatParams()
+    ms = C.c_double()
+    call("spops_select_format", h.ctx.follow_torch().handle, h.handle, C.c_int32(1 if timed else 0), C.byref(fmt),
+         C.byref(p), C.byref(ms))
+    params = {k: int(getattr(p, k)) for k, _ in FormatParams._fields_ if k != "reserved" and getattr(p, k)}
+    return {"format": _FORMAT_NAMES[fmt.value], "params": params, "ms": ms.value}
+
+
+_CONVERTED = {"sell_c_sigma": SELL_C_Sigma_Matrix, "sell_c_R": SELL_C_R_Matrix, "sell": S_ELL_Matrix,
+              "ell": ELL_Matrix, "dia": DIA_Matrix, "bsr": BSR_Matrix, "csr5": CSR5_Matrix}
+
+
+def convert_to(csr: CSR_Matrix, fmt: str, **params):
+    """The matrix in format `fmt` with spops_convert parameters (e.g. the
+    result of select_format); "csr" returns the matrix itself."""
+    if fmt == "csr":
+        return csr
+    if fmt == "coo":
+        return csr_to_coo(csr)
+    return _wrap(_CONVERTED[fmt], csr, _convert(csr, fmt, **params))
+
+
+def SpOps_auto(alpha, csr: CSR_Matrix, x, beta, y, timed: bool = False):
+    """y = alpha*A*x + beta*y in the format select_format picks for A; the
+    choice and the converted matrix are kept on the CSR object."""
+    key = "timed" if timed else "rules"
+    cache = getattr(csr, "_auto", None)
+    if cache is None or cache[0] != key:
+        choice = select_format(csr, timed)
+        cache = (key, choice, convert_to(csr, choice["format"], **choice["params"]))
+        csr._auto = cache
+    return _spmv(alpha, cache[2], x, beta, y)
+
+
 def coo_to_csr(coo: COO_Matrix, compact: bool = False):
     """include/sparse_conversion.h:37 on the device: CSR with rows in order and
     file order kept within a row; compact=True also sums duplicates like

@@ -140,6 +140,45 @@ def main():
         crp, cci, ccv = R.coo_to_csr(n, nc, ri, ci, cv, bool(compact))
         g[f"coo_rp{compact}"], g[f"coo_csr_ci{compact}"], g[f"coo_csr_v{compact}"] = crp, cci, ccv
 
+    # ---- structure features (MTX::MtxLoad + CalculateFeatures on the matrix
+    # written as a general real Matrix Market file): rectangular random,
+    # square with partly mirrored entries, banded with mixed magnitudes
+    rng = np.random.default_rng(91)
+    cases = []
+    rp, ci, cv = [0], [], []
+    for r in range(180):
+        cols = np.sort(rng.choice(150, int(rng.integers(0, 9)), replace=False))
+        ci += list(cols)
+        cv += list(rng.choice([-4.0, -0.5, 0.125, 1.0, 3.0, 250.0, 0.0], len(cols)))
+        rp.append(len(ci))
+    cases.append((np.array(rp), np.array(ci), np.array(cv), 150))
+    ent = {}
+    for _ in range(900):
+        r, c = int(rng.integers(0, 120)), int(rng.integers(0, 120))
+        x = float(rng.choice([-3.0, -0.5, 0.25, 1.0, 7.0]))
+        ent[(r, c)] = x
+        if rng.random() < 0.6:
+            ent[(c, r)] = x if rng.random() < 0.75 else x + 0.5
+    for i in range(0, 120, 2):
+        ent[(i, i)] = 40.0
+    keys = sorted(ent)
+    rp = np.zeros(121, np.int64)
+    for r, _ in keys:
+        rp[r + 1] += 1
+    cases.append((np.cumsum(rp), np.array([c for _, c in keys]), np.array([ent[k] for k in keys]), 120))
+    rp, ci, cv = [0], [], []
+    for r in range(400):
+        for d in (-3, -1, 0, 1, 7):
+            if 0 <= r + d < 400 and rng.random() < 0.9:
+                ci.append(r + d)
+                cv.append(float(rng.choice([0.001, 0.5, 2.0, 1000.0])) * (1 if d else 5))
+        rp.append(len(ci))
+    cases.append((np.array(rp), np.array(ci), np.array(cv), 400))
+    for k, (frp, fci, fv, fnc) in enumerate(cases):
+        g[f"feat{k}_rp"], g[f"feat{k}_ci"], g[f"feat{k}_v"] = frp.astype(np.int64), fci.astype(np.int64), fv
+        g[f"feat{k}_nc"] = np.int64(fnc)
+        g[f"feat{k}_out"] = R.features(frp, fci, fv, fnc)
+
     np.savez_compressed(OUT, **g)
     print(OUT, os.path.getsize(OUT), "bytes,", len(g), "arrays")
 

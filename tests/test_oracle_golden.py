@@ -121,3 +121,15 @@ def test_coo_to_csr_golden(golden, orc, compact):
     assert np.array_equal(rp, golden[f"coo_rp{compact}"])
     assert np.array_equal(ci, golden[f"coo_csr_ci{compact}"])
     assert np.array_equal(v, golden[f"coo_csr_v{compact}"])
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_features_golden(golden, orc, k):
+    """The restated feature extraction against the reference's own
+    MtxLoad + CalculateFeatures: integer features exact, the rest to 1e-12."""
+    got = orc.features(golden[f"feat{k}_rp"], golden[f"feat{k}_ci"], golden[f"feat{k}_v"], int(golden[f"feat{k}_nc"]))
+    ref = golden[f"feat{k}_out"]
+    assert np.array_equal(got[:11], ref[:11])
+    both_nan = np.isnan(got) & np.isnan(ref)
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
+    assert np.all(both_nan | (rel <= 1e-12) | (got == ref))
