@@ -16,10 +16,15 @@ struct spops_pairs_s : spops::PairSet {
 
 namespace {
 
-// CSR pattern of a handle as host int64 arrays (for the host clustering).
-spops_status_t host_pattern(Context* ctx, Matrix* A, std::vector<int64_t>& rp, std::vector<int64_t>& ci) {
-  rp.resize((size_t)A->rows + 1);
-  ci.resize((size_t)A->nnz);
+// The CSR pattern of A as int64 host arrays (for the host clustering), copied
+// once per handle and kept on it: a handle's pattern never changes
+// (spops_csr_set_values replaces values only).
+spops_status_t host_pattern(Context* ctx, Matrix* A, const std::vector<int64_t>** rp_out,
+                            const std::vector<int64_t>** ci_out) {
+  *rp_out = &A->host_rp;
+  *ci_out = &A->host_ci;
+  if (A->host_rp.size() == (size_t)A->rows + 1) return SPOPS_OK;
+  std::vector<int64_t> rp((size_t)A->rows + 1), ci((size_t)A->nnz);
   cudaStream_t st = ctx->stream;
   if (A->itype == SPOPS_INDEX_I64) {
     SPOPS_CUDA(cudaMemcpyAsync(rp.data(), A->row.p, rp.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -33,6 +38,8 @@ spops_status_t host_pattern(Context* ctx, Matrix* A, std::vector<int64_t>& rp, s
     std::copy(r32.begin(), r32.end(), rp.begin());
     std::copy(c32.begin(), c32.end(), ci.begin());
   }
+  A->host_rp.swap(rp);
+  A->host_ci.swap(ci);
   return SPOPS_OK;
 }
 
@@ -189,7 +196,7 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   DeviceGuard g(ctx->device);
   SpgemmStats s;
   auto t0 = std::chrono::steady_clock::now();
-  DevBuf sig;
+  PoolBuf sig(ctx);
   SPOPS_TRY(sig.alloc((size_t)std::max<int64_t>(A->rows, 1) * (size_t)std::max(k, 1) * 8));
   spops_status_t st = minhash_signatures(ctx, A, k, seed, sig.as<uint64_t>());
   if (st != SPOPS_OK) {
@@ -211,9 +218,11 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   auto lap = [&](const char* what) {
     if (trace) std::fprintf(stderr, "[spgemm_lsh] %-24s %9.3f ms\n", what, ms_since(t0));
   };
-  std::vector<int64_t> rp, ci, pi((size_t)P.count), pj((size_t)P.count), perm, offs;
+  std::vector<int64_t> pi((size_t)P.count), pj((size_t)P.count), perm, offs;
   std::vector<double> ps((size_t)P.count);
-  st = host_pattern(ctx, A, rp, ci);
+  const std::vector<int64_t>* rp = nullptr;
+  const std::vector<int64_t>* ci = nullptr;
+  st = host_pattern(ctx, A, &rp, &ci);
   lap("pattern to host");
   if (st == SPOPS_OK && P.count) {
     cudaMemcpy(pi.data(), P.pi.p, pi.size() * 8, cudaMemcpyDeviceToHost);
@@ -223,7 +232,7 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   P.release();
   lap("pairs to host");
   if (st == SPOPS_OK)
-    st = hierarchical_clustering(rp.data(), ci.data(), A->rows, pi.data(), pj.data(), ps.data(), (int64_t)pi.size(),
+    st = hierarchical_clustering(rp->data(), ci->data(), A->rows, pi.data(), pj.data(), ps.data(), (int64_t)pi.size(),
                                  cluster_size, perm, offs);
   if (st != SPOPS_OK) return st;
   lap("clustering");

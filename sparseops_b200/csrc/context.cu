@@ -57,6 +57,25 @@ void DevBuf::release() {
   own = false;
 }
 
+spops_status_t Context::pool_alloc(void** out, size_t bytes) {
+  if (!pool) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    SPOPS_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~0ULL;  // never trim on synchronisation: the next call reuses the memory
+    SPOPS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  SPOPS_CUDA(cudaMallocFromPoolAsync(out, bytes, pool, stream));
+  return SPOPS_OK;
+}
+
+void Context::pool_free(void* q) {
+  if (q) cudaFreeAsync(q, stream);
+}
+
 spops_status_t Context::scratch_reserve(size_t n) {
   if (scratch.bytes >= n && scratch.p) return SPOPS_OK;
   // work queued on the stream may still read the old scratch
@@ -118,6 +137,10 @@ spops_status_t spops_destroy(spops_context_t c) {
   c->xbuf.release();
   c->ybuf.release();
   if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->pool) {
+    cudaStreamSynchronize(c->stream);
+    cudaMemPoolDestroy(c->pool);
+  }
   delete c;
   return SPOPS_OK;
 }

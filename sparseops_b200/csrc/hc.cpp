@@ -51,10 +51,19 @@ struct KeyHash {
   }
 };
 
-double jaccard_rows(const int64_t* rp, const int64_t* ci, int64_t a, int64_t b, bool sorted_unique) {
+bool row_sorted_unique(const int64_t* rp, const int64_t* ci, int64_t r) {
+  for (int64_t e = rp[r] + 1; e < rp[r + 1]; ++e)
+    if (ci[e - 1] >= ci[e]) return false;
+  return true;
+}
+
+// |row a ∩ row b| / |row a ∪ row b| over entry counts.  Rows with strictly
+// increasing columns take a merge; any other pair counts row b's entries found
+// in the set of row a's columns, which gives the same number on unique rows.
+double jaccard_rows(const int64_t* rp, const int64_t* ci, int64_t a, int64_t b) {
   const int64_t la = rp[a + 1] - rp[a], lb = rp[b + 1] - rp[b];
   int64_t common = 0;
-  if (sorted_unique) {
+  if (row_sorted_unique(rp, ci, a) && row_sorted_unique(rp, ci, b)) {
     int64_t x = rp[a], y = rp[b];
     while (x < rp[a + 1] && y < rp[b + 1]) {
       if (ci[x] == ci[y]) { ++common; ++x; ++y; }
@@ -95,10 +104,6 @@ spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int
     }
     return lo < np && pi[lo] == a && pj[lo] == b;
   };
-  bool sorted_unique = true;
-  for (int64_t r = 0; r < n && sorted_unique; ++r)
-    for (int64_t e = rp[r] + 1; e < rp[r + 1]; ++e)
-      if (ci[e - 1] >= ci[e]) { sorted_unique = false; break; }
 
   std::vector<int64_t> parent((size_t)n), size((size_t)n, 1);
   std::vector<unsigned char> open((size_t)n, 1);
@@ -144,7 +149,7 @@ spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int
       if (!open[ri] || !open[rj] || ri == rj) continue;
       const int64_t a = std::min(ri, rj), b = std::max(ri, rj);
       if (given(a, b)) continue;
-      if (seen.insert(key_of(a, b)).second) found.push(Cand{jaccard_rows(rp, ci, a, b, sorted_unique), a, b});
+      if (seen.insert(key_of(a, b)).second) found.push(Cand{jaccard_rows(rp, ci, a, b), a, b});
     }
   }
   // clusters by root, rows ascending

@@ -616,7 +616,7 @@ spops_status_t d2h(cudaStream_t st, std::vector<T>& h, const void* d, size_t n) 
 }
 
 template <typename T>
-spops_status_t h2d(cudaStream_t st, DevBuf& d, const std::vector<T>& h) {
+spops_status_t h2d(cudaStream_t st, PoolBuf& d, const std::vector<T>& h) {
   SPOPS_TRY(d.alloc(std::max<size_t>(h.size(), 1) * sizeof(T)));
   if (!h.empty()) SPOPS_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   return SPOPS_OK;
@@ -659,8 +659,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   Timer tm;
   Trace tr;
   // --- permutation, offsets, per-row cluster
-  DevBuf perm, offs, rowcl, rlen, rpr, keys, skeys, src, ssrc, flag, uidx, colids, ncols_u, cptr, cptr_val, avals,
-      row_of_entry, tmp;
+  PoolBuf perm(ctx), offs(ctx), rowcl(ctx), rlen(ctx), rpr(ctx), keys(ctx), skeys(ctx), src(ctx), ssrc(ctx), flag(ctx), uidx(ctx), colids(ctx), ncols_u(ctx), cptr(ctx), cptr_val(ctx), avals(ctx), row_of_entry(ctx), tmp(ctx);
   SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(n, 1) * 8));
   SPOPS_TRY(offs.alloc((size_t)(ncl + 1) * 8));
   SPOPS_CUDA(cudaMemcpyAsync(perm.p, perm_h, (size_t)n * 8, cudaMemcpyHostToDevice, st));
@@ -746,7 +745,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   tr.mark(st, "cluster values + frees");
 
   // --- flops per cluster and symbolic bins
-  DevBuf flops, nzd, cmin, cmax;
+  PoolBuf flops(ctx), nzd(ctx), cmin(ctx), cmax(ctx);
   SPOPS_TRY(flops.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
   SPOPS_TRY(nzd.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
   SPOPS_TRY(cmin.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
@@ -761,7 +760,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   tr.mark(st, "flops per cluster");
   int64_t total_products = 0;
   {
-    DevBuf pc;
+    PoolBuf pc(ctx);
     SPOPS_TRY(pc.alloc(8));
     SPOPS_CUDA(cudaMemsetAsync(pc.p, 0, 8, st));
     if (nnz > 0) {
@@ -807,7 +806,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     }
   }
   if (!wlist.empty()) {
-    DevBuf dl, dt;
+    PoolBuf dl(ctx), dt(ctx);
     SPOPS_TRY(h2d(st, dl, wlist));
     SPOPS_TRY(h2d(st, dt, wtsize));
     const size_t smem = (size_t)kSymWarps * kSymWarpTab * 4;
@@ -820,13 +819,13 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_LAUNCH_CHECK();
     SPOPS_CUDA(cudaStreamSynchronize(st));
   }
-  DevBuf gtab;
+  PoolBuf gtab(ctx);
   if (gsym) SPOPS_TRY(gtab.alloc((size_t)gsym * 4));
   tr.mark(st, "symbolic bins + warp kernel");
   for (int w = 0; w < 3; ++w) {
     Bin& bn = sb[w];
     if (bn.list.empty()) continue;
-    DevBuf dl, dt, dg;
+    PoolBuf dl(ctx), dt(ctx), dg(ctx);
     SPOPS_TRY(h2d(st, dl, bn.list));
     SPOPS_TRY(h2d(st, dt, bn.tsize));
     if (bn.global) SPOPS_TRY(h2d(st, dg, bn.goff));
@@ -854,7 +853,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   tr.mark(st, "symbolic block kernels + nz");
 
   // --- classify (drop rule)
-  DevBuf drop, ndense;
+  PoolBuf drop(ctx), ndense(ctx);
   SPOPS_TRY(drop.alloc((size_t)std::max<int64_t>(ncl, 1)));
   SPOPS_TRY(ndense.alloc(8));
   SPOPS_CUDA(cudaMemsetAsync(ndense.p, 0, 8, st));
@@ -870,7 +869,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_CUDA(cudaMemcpyAsync(&hdense, ndense.p, 8, cudaMemcpyDeviceToHost, st));
 
   // --- numeric bins by arena size
-  DevBuf ccptr, ccptr_val, ccol, cval;
+  PoolBuf ccptr(ctx), ccptr_val(ctx), ccol(ctx), cval(ctx);
   SPOPS_TRY(h2d(st, ccptr, hccptr));
   SPOPS_TRY(h2d(st, ccptr_val, hccptr_val));
   SPOPS_TRY(ccol.alloc((size_t)std::max<int64_t>(hccptr[ncl], 1) * 4));
@@ -927,7 +926,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   for (int w = 0; w < 2; ++w) {
     WBin& bn = wb[w];
     if (bn.list.empty()) continue;
-    DevBuf dl, ds;
+    PoolBuf dl(ctx), ds(ctx);
     SPOPS_TRY(h2d(st, dl, bn.list));
     SPOPS_TRY(h2d(st, ds, bn.slots));
     const size_t smem = (size_t)bn.warps * (size_t)bn.bytes;
@@ -941,13 +940,13 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_LAUNCH_CHECK();
     SPOPS_CUDA(cudaStreamSynchronize(st));
   }
-  DevBuf arena;
+  PoolBuf arena(ctx);
   if (garena) SPOPS_TRY(arena.alloc((size_t)garena));
   tr.mark(st, "numeric bins + warp kernels");
   for (int w = 0; w < 4; ++w) {
     NBin& bn = nb[w];
     if (bn.list.empty()) continue;
-    DevBuf dl, ds, dg;
+    PoolBuf dl(ctx), ds(ctx), dg(ctx);
     SPOPS_TRY(h2d(st, dl, bn.list));
     SPOPS_TRY(h2d(st, ds, bn.slots));
     if (bn.global) SPOPS_TRY(h2d(st, dg, bn.goff));
@@ -968,7 +967,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   tr.mark(st, "numeric block kernels");
 
   // --- back to CSR, original row order
-  DevBuf rowcnt, crp;
+  PoolBuf rowcnt(ctx), crp(ctx);
   SPOPS_TRY(rowcnt.alloc((nn + 1) * 8));
   SPOPS_TRY(crp.alloc((nn + 1) * 8));
   SPOPS_CUDA(cudaMemsetAsync(rowcnt.p, 0, (nn + 1) * 8, st));

@@ -61,6 +61,41 @@ struct Context {
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
   DevBuf xbuf, ybuf;
+  // stream-ordered pool for per-call temporaries (PoolBuf): memory freed by
+  // one call is handed to the next without returning it to the driver
+  cudaMemPool_t pool = nullptr;
+  spops_status_t pool_alloc(void** p, size_t bytes);
+  void pool_free(void* p);
+};
+
+// Temporary device buffer of one API call, from the context's pool and
+// ordered on its stream (alloc and free both enqueue on ctx->stream, so the
+// memory is reused only by work queued after this call's last use of it).
+struct PoolBuf {
+  Context* ctx;
+  void* p = nullptr;
+  size_t bytes = 0;
+  explicit PoolBuf(Context* c) : ctx(c) {}
+  PoolBuf(const PoolBuf&) = delete;
+  PoolBuf& operator=(const PoolBuf&) = delete;
+  ~PoolBuf() { release(); }
+  spops_status_t alloc(size_t n) {
+    release();
+    if (n == 0) n = 16;
+    spops_status_t s = ctx->pool_alloc(&p, n);
+    if (s != SPOPS_OK) {
+      p = nullptr;
+      return s;
+    }
+    bytes = n;
+    return SPOPS_OK;
+  }
+  void release() {
+    if (p) ctx->pool_free(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
 // RAII guard: make ctx->device current for the duration of an API call.
@@ -236,6 +271,8 @@ struct Matrix {
   DevBuf spmm_partial;  // SpMM long-row chunk sums (k per chunk)
   // COO: the same entries as a CSR matrix sorted by row (owned)
   Matrix* csr_view = nullptr;
+  // host copy of the pattern (int64), made once for the host clustering
+  std::vector<int64_t> host_rp, host_ci;
   size_t isize() const { return itype == SPOPS_INDEX_I32 ? 4 : 8; }
   size_t vsize() const { return vtype == SPOPS_VALUE_F32 ? 4 : 8; }
   void release_all();
