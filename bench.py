@@ -539,6 +539,15 @@ def run_section(args):
     return 0
 
 
+def csr_kernel_name(variant):
+    if variant in (7, 8, 9):
+        per_sm = {7: 1, 8: 2, 9: 4}[variant]
+        return f"csr_win_kernel<double,{1024 // per_sm},{per_sm}>"
+    if variant in (2, 3, 4):
+        return "csr_warp_kernel<int,double,%d,%d>" % {2: (8, 4), 3: (4, 6), 4: (16, 2)}[variant]
+    return "csr_tile_kernel<int,double,8,3,1> + csr_tile_calibrate_kernel<double>"
+
+
 def run_ours(args):
     import torch
     import ctypes as C
@@ -614,8 +623,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     ems = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, dev)
     e2e = whole_job_gbs(world, nbytes, ems)
-    # correctness spot check of the e2e result against the device result
-    ok = bool(torch.equal(yh.to(dev), yd))
+    # correctness spot check of the e2e result against the device result (the
+    # window variants may differ at rounding level between runs)
+    e2e_diff = float(((yh.to(dev) - yd).norm() / yd.norm().clamp_min(1e-300)).item())
+    ok = e2e_diff <= 1e-12
 
     peak, peak_kind = peaks()
     traffic = profile_traffic()
@@ -656,13 +667,13 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
                      "peak_source": peak_kind,
-                     "kernel": "csr_tile_kernel<int,double,8,3,1> + csr_tile_calibrate_kernel<double>",
+                     "kernel": csr_kernel_name(args.csr_variant),
                      "traffic": traffic},
         "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
-                "steps": e2e_steps, "matches_device_result": ok,
+                "steps": e2e_steps, "matches_device_result": ok, "normwise_diff_vs_device": e2e_diff,
                 "path": "spops_spmv_host (matrix resident after first upload)"},
-        # tile kernel + its calibrator per SpMV; one launch for the segment kernel
-        "gpu_launches": args.steps * (1 if args.csr_variant in (2, 3, 4) else 2),
+        # tile kernel + its calibrator per SpMV; one launch for the segment and window kernels
+        "gpu_launches": args.steps * (1 if args.csr_variant in (2, 3, 4, 7, 8, 9) else 2),
         "clocks": ck,
         "cpu_baseline": cpu,
     }

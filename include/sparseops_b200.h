@@ -106,13 +106,18 @@ spops_status_t spops_synchronize(spops_context_t ctx);
  * when any bit was set; *flags (may be NULL) receives the bits. */
 spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
 /* Tuning switches by name; unknown keys are rejected with SPOPS_ERR_INVALID.
- *   "csr_variant" 0..6: CSR SpMV kernel.  Tiles of 32*K entries summed in
+ *   "csr_variant" 0..9: CSR SpMV kernel.  Tiles of 32*K entries summed in
  *   registers (K entries per lane / resident blocks per SM / next tile's
  *   loads issued early): 0 = 8/3/yes (default), 1 = 8/4/no, 5 = 4/4/no,
  *   6 = 8/5/no; they need the column and value arrays aligned to
  *   min(32, K * element size) bytes, otherwise variant 2 runs.  Row segments
  *   through shared memory (entries per lane per round / blocks per SM):
- *   2 = 8/4, 3 = 4/6, 4 = 16/2. */
+ *   2 = 8/4, 3 = 4/6, 4 = 16/2.  Column-sorted row windows whose partial y
+ *   stays in shared memory (windows resident per SM): 7 = 1, 8 = 2, 9 = 4;
+ *   they keep a copy of the values (refreshed after spops_csr_set_values or
+ *   spops_matrix_touch), need cols and nnz below 2^31 (otherwise variant 2
+ *   runs), and add a row's products in an order that can change from run to
+ *   run at rounding level; variants 0-6 are bit-reproducible. */
 spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);

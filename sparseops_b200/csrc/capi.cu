@@ -364,7 +364,8 @@ spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info) {
 
 spops_status_t spops_matrix_touch(spops_matrix_t A) {
   if (!A) return fail(SPOPS_ERR_INVALID, "spops_matrix_touch: null matrix");
-  A->tr.values_fresh = false;  // the CSR plan depends on the pattern only
+  A->tr.values_fresh = false;  // the row-ordered CSR plans depend on the pattern only
+  A->plan.win.values_fresh = false;  // the window plan keeps a copy of the values
   return SPOPS_OK;
 }
 
@@ -374,6 +375,7 @@ spops_status_t spops_csr_set_values(spops_matrix_t A, const void* values) {
   if (!values && A->nnz > 0) return fail(SPOPS_ERR_INVALID, "spops_csr_set_values: null values");
   A->val.borrow(values, (size_t)A->nnz * A->vsize());
   A->tr.values_fresh = false;
+  A->plan.win.values_fresh = false;
   return SPOPS_OK;
 }
 

@@ -254,6 +254,11 @@ spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, doub
     case 2: return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);
     case 3: return launch_warp<I, V, 4, 6>(ctx, A, alpha, x, beta, y);
     case 4: return launch_warp<I, V, 16, 2>(ctx, A, alpha, x, beta, y);
+    case 7:
+    case 8:
+    case 9:
+      if (csr_win_usable(A)) return csr_win_spmv(ctx, A, ctx->csr_variant, alpha, x, beta, y);
+      return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);
     default: {
       if (csr_tile_usable(A, ctx->csr_variant)) return csr_tile_spmv(ctx, A, ctx->csr_variant, alpha, x, beta, y);
       return launch_warp<I, V, 8, 4>(ctx, A, alpha, x, beta, y);  // arrays not aligned for vector loads

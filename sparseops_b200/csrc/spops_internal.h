@@ -137,6 +137,23 @@ struct CsrTiles {
   void release();
 };
 
+// Column-sorted row windows of a CSR matrix (spmv_csr_win.cu).
+struct CsrWin {
+  bool ready = false;
+  int per_sm = 0;          // windows resident per SM (variant 7 / 8 / 9: 1 / 2 / 4)
+  int64_t nwin = 0, ntiles = 0, nesc = 0;
+  int64_t max_rows = 0;    // rows of the largest window (shared memory per CTA)
+  DevBuf win_row0;         // int64 [nwin + 1]
+  DevBuf win_tile0;        // int64 [nwin + 1]
+  DevBuf tbase;            // int32 [ntiles]: first column, or -1 - escape index
+  DevBuf tidx;             // uint32 [ntiles * 32]: (local row << 16) | column offset
+  DevBuf tval;             // V [ntiles * 32]: copy of the values
+  DevBuf tperm;            // int32 [ntiles * 32]: CSR entry of each slot (-1: padding)
+  bool values_fresh = false;
+  DevBuf tesc;             // int32 [nesc * 32]: full columns of wide tiles
+  void release();
+};
+
 // Row-block partition of a CSR matrix for the streaming SpMV kernel
 // (spmv_csr.cu).  Block b covers rows [blk_row[b], next block's row) when
 // blk_chunk[b] < 0 (a segment of short rows whose entries fit in shared
@@ -152,9 +169,11 @@ struct CsrPlan {
   DevBuf counter;          // int32 [nblocks] arrival counters (zero between calls)
   DevBuf seg;              // CsrSeg [nblocks]
   CsrTiles tiles;          // built on first use by the tile kernel
+  CsrWin win;              // built on first use by the window kernel
   void release() {
     blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); seg.release();
     tiles.release();
+    win.release();
     ready = false;
   }
 };
@@ -298,6 +317,10 @@ spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, do
 bool csr_tile_usable(const Matrix* A, int variant);
 spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k);
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y);
+
+// spmv_csr_win.cu
+bool csr_win_usable(const Matrix* A);
+spops_status_t csr_win_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y);
 
 // formats.cu
 spops_status_t convert_from_csr(Context* ctx, Matrix* A, spops_format_t fmt, const spops_format_params_t& p,

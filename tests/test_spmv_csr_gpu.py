@@ -201,7 +201,7 @@ def test_kernel_variants_identical(cuda, orc, dtype, itype):
     ctx = default_context()
     ys = []
     try:
-        for var in range(7):
+        for var in range(10):
             ctx.set_option("csr_variant", var)
             y, _ = _run(rp, ci, v, x, 0.8, 0.7, y0)
             ys.append(y)
@@ -215,3 +215,79 @@ def test_kernel_variants_identical(cuda, orc, dtype, itype):
                     y.astype(np.float64), yref, 0.7, y0.astype(np.float64), 0.8) <= tol, var
         if var in (3, 4):
             assert np.array_equal(y, ys[2]), var
+
+
+def _with_variant(var, fn):
+    from sparseops_b200 import default_context
+    ctx = default_context()
+    ctx.set_option("csr_variant", var)
+    try:
+        return fn()
+    finally:
+        ctx.set_option("csr_variant", 0)
+
+
+@pytest.mark.parametrize("var", [7, 8, 9])
+def test_windows_wide_tiles_and_empty(cuda, orc, var):
+    """Column-sorted windows: tiles whose columns span more than 65535 (full
+    columns stored aside), empty rows and windows, FP64 and FP32."""
+    rng = np.random.default_rng(5)
+    n, ncols = 3000, 5_000_000
+    lens = rng.integers(0, 4, n)
+    lens[100:400] = 0
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(np.int64)
+    for dtype, tol in [(np.float64, TOL64), (np.float32, TOL32)]:
+        v = rng.standard_normal(len(ci)).astype(dtype)
+        x = rng.uniform(-1, 1, ncols).astype(dtype)
+        y0 = rng.uniform(-1, 1, n).astype(dtype)
+        y, _ = _with_variant(var, lambda: _run(rp, ci, v, x, 0.8, 0.7, y0))
+        f = lambda a: a.astype(np.float64)
+        yref = orc.spmv_csr(rp, ci, f(v), f(x), 0.8, 0.7, f(y0))
+        assert _err(orc, rp, ci, f(v), f(x), f(y), yref, 0.7, f(y0), 0.8) <= tol
+
+
+@pytest.mark.parametrize("var", [7, 8])
+def test_windows_no_entries(cuda, var):
+    rp = np.zeros(1001, np.int64)
+    ci = np.zeros(0, np.int64)
+    v = np.zeros(0)
+    x = np.ones(50)
+    y0 = np.arange(1000, dtype=np.float64)
+    y, _ = _with_variant(var, lambda: _run(rp, ci, v, x, 1.0, 0.5, y0))
+    assert np.array_equal(y, 0.5 * y0)
+    y, _ = _with_variant(var, lambda: _run(rp, ci, v, x, 1.0, 0.0, y0))
+    assert np.array_equal(y, np.zeros(1000))
+
+
+def test_windows_powerlaw_and_value_updates(cuda, orc):
+    """Windows on a power-law matrix large enough for many rows per window;
+    new values through spops_csr_set_values and in place with touch()."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, SpOps_csr, default_context
+    from sparseops_b200._lib import call, vp
+    rp, ci, v = synth.powerlaw(300000, hi=20000, seed=3)
+    n = len(rp) - 1
+    x = synth.uniform(n, 4)
+    dev = "cuda"
+    A = CSR_Matrix(n, n, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev), torch.from_numpy(v).to(dev))
+    xd = torch.from_numpy(x).to(dev)
+    yd = torch.zeros(n, dtype=torch.float64, device=dev)
+    ctx = default_context()
+    ctx.set_option("csr_variant", 7)
+    try:
+        SpOps_csr(1.0, A, xd, 0.0, yd)
+        assert _err(orc, rp, ci, v, x, yd.cpu().numpy(), orc.spmv_csr(rp, ci, v, x)) <= TOL64
+        v2 = -2.0 * v + 1.0
+        vd2 = torch.from_numpy(v2).to(dev)
+        call("spops_csr_set_values", A.device().handle, vp(vd2.data_ptr()))
+        SpOps_csr(1.0, A, xd, 0.0, yd)
+        assert _err(orc, rp, ci, v2, x, yd.cpu().numpy(), orc.spmv_csr(rp, ci, v2, x)) <= TOL64
+        vd2.mul_(0.5)
+        A.touch()
+        SpOps_csr(1.0, A, xd, 0.0, yd)
+        v3 = 0.5 * v2
+        assert _err(orc, rp, ci, v3, x, yd.cpu().numpy(), orc.spmv_csr(rp, ci, v3, x)) <= TOL64
+    finally:
+        ctx.set_option("csr_variant", 0)
