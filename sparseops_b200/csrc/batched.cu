@@ -66,15 +66,33 @@ namespace {
 
 constexpr int kBatchBlock = 256;
 
+// Items are taken from a queue (next_item, zeroed before the launch) kGrab at
+// a time, the next grab requested while the current one runs: the items in
+// flight stay a contiguous window of the list, so the matrices whose vectors
+// must be in L2 at once are the one or two that window covers.  (A fixed
+// stride per warp lets warps drift apart across many matrices.)
+constexpr int kGrab = 2;
+
 template <typename I, typename V, int KT>
-__global__ void __launch_bounds__(kBatchBlock, 4) batch_kernel(const BatchItem* __restrict__ items, int64_t nitems,
+__global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(const BatchItem* __restrict__ items, int64_t nitems,
                                                                const BatchMat* __restrict__ mats, int64_t k, V alpha,
-                                                               V beta, bool bz) {
-  __shared__ V prod_all[kBatchBlock / 32][2 * kCsrCap];
+                                                               V beta, bool bz,
+                                                               unsigned long long* __restrict__ next_item) {
+  __shared__ V prod_all[KT == 1 ? kBatchBlock / 32 : 1][KT == 1 ? 2 * kCsrCap : 1];
+  extern __shared__ __align__(16) unsigned char batch_dyn_smem[];  // SpMM: one SpmmStage per warp
   const int lane = threadIdx.x & 31;
-  V* prod = prod_all[threadIdx.x >> 5];
-  const int64_t nwarps = (int64_t)gridDim.x * (kBatchBlock / 32);
-  for (int64_t j = (blockIdx.x * (int64_t)kBatchBlock + threadIdx.x) >> 5; j < nitems; j += nwarps) {
+  V* prod = prod_all[KT == 1 ? threadIdx.x >> 5 : 0];
+  SpmmStage<I, V>& stage = reinterpret_cast<SpmmStage<I, V>*>(batch_dyn_smem)[KT == 1 ? 0 : threadIdx.x >> 5];
+  unsigned long long grab = 0, ahead = 0;
+  if (lane == 0) {
+    grab = atomicAdd(next_item, (unsigned long long)kGrab);
+    ahead = atomicAdd(next_item, (unsigned long long)kGrab);
+  }
+  grab = __shfl_sync(0xffffffffu, grab, 0);
+  for (;;) {
+    if ((int64_t)grab >= nitems) break;
+    const int64_t jend = (int64_t)grab + kGrab < nitems ? (int64_t)grab + kGrab : nitems;
+    for (int64_t j = (int64_t)grab; j < jend; ++j) {
     const BatchItem it = items[j];
     const BatchMat& M = mats[it.mat];
     if (KT == 1) {
@@ -111,29 +129,70 @@ __global__ void __launch_bounds__(kBatchBlock, 4) batch_kernel(const BatchItem* 
       csr_segment_spmm<I, V, KT>(M.seg[it.idx], it.idx, static_cast<const I*>(M.ci), static_cast<const V*>(M.val),
                                  static_cast<const I*>(M.rp), static_cast<const V*>(M.x), M.ldx,
                                  static_cast<V*>(M.y), M.ldy, k, alpha, beta, bz, static_cast<V*>(M.partial),
-                                 M.counter, lane);
+                                 M.counter, stage, lane);
     }
+    }
+    grab = __shfl_sync(0xffffffffu, ahead, 0);
+    if (lane == 0 && (int64_t)grab < nitems) ahead = atomicAdd(next_item, (unsigned long long)kGrab);
   }
 }
 
 // Single-matrix SpMM over the CSR plan (the per-matrix path of spops_spmm).
 template <typename I, typename V, int KT>
-__global__ void __launch_bounds__(256, 4) spmm_kernel(const CsrSeg* __restrict__ segs, int64_t nseg,
+__global__ void __launch_bounds__(256, 3) spmm_kernel(const CsrSeg* __restrict__ segs, int64_t nseg,
                                                       const I* __restrict__ ci, const V* __restrict__ val,
                                                       const I* __restrict__ rp, const V* __restrict__ X, int64_t ldx,
                                                       V* __restrict__ Y, int64_t ldy, int64_t k, V alpha, V beta,
                                                       bool bz, V* __restrict__ partial, int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char spmm_dyn_smem[];  // one SpmmStage per warp
+  SpmmStage<I, V>& stage = reinterpret_cast<SpmmStage<I, V>*>(spmm_dyn_smem)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < nseg; j += nwarps)
-    csr_segment_spmm<I, V, KT>(segs[j], j, ci, val, rp, X, ldx, Y, ldy, k, alpha, beta, bz, partial, counter, lane);
+    csr_segment_spmm<I, V, KT>(segs[j], j, ci, val, rp, X, ldx, Y, ldy, k, alpha, beta, bz, partial, counter, stage,
+                               lane);
+}
+
+// dynamic shared memory of the SpMM kernels: one stage per warp
+template <typename I, typename V>
+constexpr size_t spmm_smem(int threads) {
+  return (size_t)(threads / 32) * sizeof(SpmmStage<I, V>);
 }
 
 template <typename K>
-int occupancy(K kernel, int threads) {
+int occupancy(K kernel, int threads, size_t smem = 0) {
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, 0) != cudaSuccess || bps < 1) return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, smem) != cudaSuccess || bps < 1) return 1;
   return bps;
+}
+
+// Resident blocks per SM of a kernel with `smem` bytes of dynamic shared
+// memory, the attribute set once per instantiation and device; 0 when it
+// cannot be set.
+constexpr int kMaxDevices = 64;
+
+template <typename K>
+int blocks_per_sm(K kern, int threads, size_t smem, int* cache) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = 0;
+  if (cache[dev] == 0) {
+    if (smem && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return 0;
+    cache[dev] = occupancy(kern, threads, smem);
+  }
+  return cache[dev];
+}
+
+template <typename I, typename V, int KT>
+int spmm_blocks_per_sm() {
+  static int cache[kMaxDevices];
+  return blocks_per_sm(spmm_kernel<I, V, KT>, 256, spmm_smem<I, V>(256), cache);
+}
+
+template <typename I, typename V, int KT>
+int batch_blocks_per_sm() {
+  static int cache[kMaxDevices];
+  return blocks_per_sm(batch_kernel<I, V, KT>, kBatchBlock, KT == 1 ? 0 : spmm_smem<I, V>(kBatchBlock), cache);
 }
 
 }  // namespace
@@ -148,21 +207,21 @@ static spops_status_t spmm_t(Context* ctx, Matrix* A, double alpha, const void* 
     SPOPS_TRY(A->spmm_partial.alloc((size_t)P.nblocks * k * sizeof(V)));
   const int kt = k >= 32 ? 32 : (k >= 8 ? 8 : 8);
   const bool bz = beta == 0.0;
-  auto launch = [&](auto kern) -> spops_status_t {
-    static int bps = -1;
-    if (bps < 0) bps = occupancy(kern, 256);
+  auto launch = [&](auto kern, int bps) -> spops_status_t {
+    const size_t smem = spmm_smem<I, V>(256);
+    if (bps < 1) return fail(SPOPS_ERR_CUDA, "spmm: kernel attributes could not be set");
     int64_t grid = (int64_t)ctx->num_sms * bps;
     const int64_t need = (P.nblocks + 7) / 8;
     if (grid > need) grid = need;
-    kern<<<(unsigned)grid, 256, 0, ctx->stream>>>(P.seg.as<CsrSeg>(), P.nblocks, A->col.as<I>(), A->val.as<V>(),
+    kern<<<(unsigned)grid, 256, smem, ctx->stream>>>(P.seg.as<CsrSeg>(), P.nblocks, A->col.as<I>(), A->val.as<V>(),
                                                   A->row.as<I>(), static_cast<const V*>(X), ldx, static_cast<V*>(Y),
                                                   ldy, k, (V)alpha, (V)beta, bz, A->spmm_partial.as<V>(),
                                                   P.counter.as<int>());
     SPOPS_LAUNCH_CHECK();
     return SPOPS_OK;
   };
-  if (kt == 32) return launch(spmm_kernel<I, V, 32>);
-  return launch(spmm_kernel<I, V, 8>);
+  if (kt == 32) return launch(spmm_kernel<I, V, 32>, spmm_blocks_per_sm<I, V, 32>());
+  return launch(spmm_kernel<I, V, 8>, spmm_blocks_per_sm<I, V, 8>());
 }
 
 spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k, double beta,
@@ -188,6 +247,7 @@ struct Batch {
   std::vector<BatchMat> host;
   std::vector<DevBuf> spmm_partial;
   DevBuf items, table;
+  DevBuf queue;  // next item of the running launch
   int64_t nitems = 0;
   int kt = 8;  // RHS tile for k > 1
   bool dirty = true;
@@ -205,6 +265,7 @@ struct Batch {
     for (auto& b : spmm_partial) b.release();
     items.release();
     table.release();
+    queue.release();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (ev_in) cudaEventDestroy(ev_in);
@@ -233,6 +294,7 @@ spops_status_t build_items(Batch* B) {
     }
   }
   B->nitems = (int64_t)it.size();
+  if (!B->queue.p) SPOPS_TRY(B->queue.alloc(8));
   SPOPS_TRY(B->items.alloc(std::max<size_t>(it.size(), 1) * sizeof(BatchItem)));
   if (!it.empty())
     SPOPS_CUDA(cudaMemcpy(B->items.p, it.data(), it.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
@@ -274,20 +336,21 @@ template <typename I, typename V>
 spops_status_t launch_batch(Batch* B, double alpha, double beta, cudaStream_t st) {
   if (B->nitems == 0) return SPOPS_OK;
   const bool bz = beta == 0.0;
-  auto go = [&](auto kern) -> spops_status_t {
-    static int bps = -1;
-    if (bps < 0) bps = occupancy(kern, kBatchBlock);
+  auto go = [&](auto kern, size_t smem, int bps) -> spops_status_t {
+    if (bps < 1) return fail(SPOPS_ERR_CUDA, "batch: kernel attributes could not be set");
     int64_t grid = (int64_t)B->ctx->num_sms * bps;
     const int64_t need = (B->nitems + 7) / 8;
     if (grid > need) grid = need;
-    kern<<<(unsigned)grid, kBatchBlock, 0, st>>>(B->items.as<BatchItem>(), B->nitems, B->table.as<BatchMat>(), B->k,
-                                                 (V)alpha, (V)beta, bz);
+    SPOPS_CUDA(cudaMemsetAsync(B->queue.p, 0, 8, st));
+    kern<<<(unsigned)grid, kBatchBlock, smem, st>>>(B->items.as<BatchItem>(), B->nitems, B->table.as<BatchMat>(), B->k,
+                                                 (V)alpha, (V)beta, bz, B->queue.as<unsigned long long>());
     SPOPS_LAUNCH_CHECK();
     return SPOPS_OK;
   };
-  if (B->k == 1) return go(batch_kernel<I, V, 1>);
-  if (B->kt == 32) return go(batch_kernel<I, V, 32>);
-  return go(batch_kernel<I, V, 8>);
+  if (B->k == 1) return go(batch_kernel<I, V, 1>, 0, batch_blocks_per_sm<I, V, 1>());
+  if (B->kt == 32)
+    return go(batch_kernel<I, V, 32>, spmm_smem<I, V>(kBatchBlock), batch_blocks_per_sm<I, V, 32>());
+  return go(batch_kernel<I, V, 8>, spmm_smem<I, V>(kBatchBlock), batch_blocks_per_sm<I, V, 8>());
 }
 
 spops_status_t launch_any(Batch* B, double alpha, double beta, cudaStream_t st) {

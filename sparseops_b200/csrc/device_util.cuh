@@ -55,4 +55,11 @@ __device__ __forceinline__ void axpby_store(V* y, V sum, V alpha, V beta, bool b
   *y = beta_zero ? alpha * sum : alpha * sum + beta * (*y);
 }
 
+// The same with streaming (evict-first) accesses to y, for outputs that
+// would otherwise push gathered operands out of L2.
+template <typename V>
+__device__ __forceinline__ void axpby_store_cs(V* y, V sum, V alpha, V beta, bool beta_zero) {
+  __stcs(y, beta_zero ? alpha * sum : alpha * sum + beta * __ldcs(y));
+}
+
 }  // namespace spops

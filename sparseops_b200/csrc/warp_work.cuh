@@ -112,50 +112,144 @@ __device__ __forceinline__ void csr_segment_spmv(const CsrSeg& d, int64_t j, con
 }
 
 // Multi-RHS CSR segment: Y[r, 0:k] = alpha * A[r,:] X[:, 0:k] + beta * Y[r, 0:k]
-// (row-major X [cols x ldx], Y [rows x ldy]).  Lanes = KT RHS columns x
-// 32/KT entry groups; rows of the segment one after another; the entry-group
-// partial sums combine with xor shuffles (fixed order).  Long chunks combine
-// through partial[slot * k + r].
+// (row-major X [cols x ldx], Y [rows x ldy]).  The segment's X row offsets
+// (column * ldx), values and row starts are first staged in the warp's
+// SpmmStage (one coalesced pass), so the gathers need no dependent global
+// loads.  The warp is 32/KT groups of KT lanes; lane rl of a group owns RHS
+// column t0 + rl.  A short segment gives each group a run of whole rows
+// holding about a 32/KT-th of its entries; the group streams that run in
+// batches of U entries (U gathers per lane in flight) that cross row
+// boundaries, storing each row as its last entry passes.  A long-row chunk is
+// split between the groups, whose sums combine with xor shuffles; chunk sums
+// then combine through partial[slot * k + r].  Every sum is taken in a fixed
+// order, so results are bit-reproducible.
+template <typename I, typename V>
+struct SpmmStage {
+  int64_t off[2 * kCsrCap];  // column * ldx
+  V a[2 * kCsrCap];
+  int rs[kCsrRowCap + 1];
+};
+
+// Entries [e0, e1) of the stage, rows [r, r_end) with starts rs (rs[r_end] >=
+// e1): Y[row] = alpha * sum + beta * Y[row] per row as the stream passes it.
+// With rs == nullptr the range is one row's chunk and its sum is returned.
+template <typename I, typename V, int U>
+__device__ __forceinline__ V spmm_stream(const SpmmStage<I, V>& S, const V* __restrict__ X, int e0, int e1,
+                                         const int* rs, int r, int r_end, int64_t col0, bool rok,
+                                         V* __restrict__ Yrow0, int64_t ldy, V alpha, V beta, bool bz) {
+  V acc = V(0);
+  int next = rs ? (r < r_end ? rs[r + 1] : e1) : e1;
+  if (rs)
+    while (r < r_end && next <= e0) {  // empty rows before the first entry
+      if (rok) axpby_store_cs(Yrow0 + (int64_t)r * ldy + col0, acc, alpha, beta, bz);
+      ++r;
+      next = r < r_end ? rs[r + 1] : e1;
+    }
+  for (int eb = e0; eb < e1; eb += U) {
+    V xv[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const int e = eb + q;
+      xv[q] = (e < e1 && rok) ? ld_gather(X + S.off[e] + col0) : V(0);
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const int e = eb + q;
+      if (e < e1) {
+        if (rs)
+          while (e >= next) {  // rows that end before entry e
+            if (rok) axpby_store_cs(Yrow0 + (int64_t)r * ldy + col0, acc, alpha, beta, bz);
+            acc = V(0);
+            ++r;
+            next = rs[r + 1];
+          }
+        acc += S.a[e] * xv[q];
+      }
+    }
+  }
+  if (rs)
+    while (r < r_end) {
+      if (rok) axpby_store_cs(Yrow0 + (int64_t)r * ldy + col0, acc, alpha, beta, bz);
+      acc = V(0);
+      ++r;
+    }
+  return acc;
+}
+
 template <typename I, typename V, int KT>
 __device__ __forceinline__ void csr_segment_spmm(const CsrSeg& d, int64_t j, const I* __restrict__ ci,
                                                  const V* __restrict__ val, const I* __restrict__ rp,
                                                  const V* __restrict__ X, int64_t ldx, V* __restrict__ Y,
                                                  int64_t ldy, int64_t k, V alpha, V beta, bool bz,
-                                                 V* __restrict__ partial, int* __restrict__ counter, int lane) {
+                                                 V* __restrict__ partial, int* __restrict__ counter,
+                                                 SpmmStage<I, V>& S, int lane) {
   constexpr int P = 32 / KT;
+  constexpr int U = KT == 32 ? 16 : 8;
   const int grp = lane / KT, rl = lane % KT;
-  auto row_dot = [&](int64_t e0, int64_t e1, int64_t t0) {
-    const bool rok = t0 + rl < k;
-    V s0 = V(0), s1 = V(0);
-    int64_t e = e0 + grp;
-    for (; e + P < e1; e += 2 * P) {
-      const V a0 = val[e], a1 = val[e + P];
-      const I c0 = ci[e], c1 = ci[e + P];
-      if (rok) {
-        s0 += a0 * ld_gather(X + (int64_t)c0 * ldx + t0 + rl);
-        s1 += a1 * ld_gather(X + (int64_t)c1 * ldx + t0 + rl);
-      }
-    }
-    if (e < e1 && rok) s0 += val[e] * ld_gather(X + (int64_t)ci[e] * ldx + t0 + rl);
-    V s = s0 + s1;
+  const int m = (int)(d.p1 - d.p0);
+  const bool is_long = d.chunk >= 0;
+  // stage: all loads of a round issued before any store (8 entries per lane
+  // in flight), the row starts in the first round
+  constexpr int kStageItems = 8;
+  __syncwarp();  // the previous segment's reads of the stage are done
+  for (int base = 0; base < m || base == 0; base += 32 * kStageItems) {
+    I c[kStageItems];
+    V a[kStageItems];
 #pragma unroll
-    for (int o = KT; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-  };
-  if (d.chunk < 0) {
-    for (int rr = 0; rr < d.nr; ++rr) {
-      const int64_t r = d.r0 + rr;
-      const int64_t e0 = rp[r], e1 = rp[r + 1];
-      for (int64_t t0 = 0; t0 < k; t0 += KT) {
-        const V s = row_dot(e0, e1, t0);
-        if (grp == 0 && t0 + rl < k) axpby_store(Y + r * ldy + t0 + rl, s, alpha, beta, bz);
+    for (int u = 0; u < kStageItems; ++u) {
+      const int e = base + lane + 32 * u;
+      if (e < m) {
+        c[u] = ld_stream(ci + d.p0 + e);
+        a[u] = ld_stream(val + d.p0 + e);
       }
     }
+    I r0v = 0, r1v = 0;
+    if (base == 0 && !is_long) {
+      if (lane <= d.nr) r0v = rp[d.r0 + lane];
+      if (lane + 32 <= d.nr) r1v = rp[d.r0 + lane + 32];
+    }
+#pragma unroll
+    for (int u = 0; u < kStageItems; ++u) {
+      const int e = base + lane + 32 * u;
+      if (e < m) {
+        S.off[e] = (int64_t)c[u] * ldx;
+        S.a[e] = a[u];
+      }
+    }
+    if (base == 0 && !is_long) {
+      if (lane <= d.nr) S.rs[lane] = (int)((int64_t)r0v - d.p0);
+      if (lane + 32 <= d.nr) S.rs[lane + 32] = (int)((int64_t)r1v - d.p0);
+    }
+  }
+  __syncwarp();
+  if (!is_long) {
+    // rows of this group: those starting in [m*grp/P, m*(grp+1)/P)
+    auto first_row = [&](int g) {
+      if (g >= P) return d.nr;
+      const int target = (int)((int64_t)m * g / P);
+      int lo = 0, hi = d.nr;  // first r in [0, nr] with rs[r] >= target
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (S.rs[mid] < target) lo = mid + 1; else hi = mid;
+      }
+      return g == 0 ? 0 : lo;
+    };
+    const int rb = first_row(grp), re = first_row(grp + 1);
+    if (rb < re)
+      for (int64_t t0 = 0; t0 < k; t0 += KT)
+        spmm_stream<I, V, U>(S, X, S.rs[rb], S.rs[re], S.rs, rb, re, t0 + rl, t0 + rl < k, Y + d.r0 * ldy, ldy,
+                             alpha, beta, bz);
+    __syncwarp();
   } else {
     // chunk sums per RHS column; the last chunk of the row adds them in order
+    const int e0 = (int)((int64_t)m * grp / P), e1 = (int)((int64_t)m * (grp + 1) / P);
     for (int64_t t0 = 0; t0 < k; t0 += KT) {
-      const V s = row_dot(d.p0, d.p1, t0);
-      if (grp == 0 && t0 + rl < k) partial[j * k + t0 + rl] = s;
+      const bool rok = t0 + rl < k;
+      V s = spmm_stream<I, V, U>(S, X, e0, e1, nullptr, 0, 0, t0 + rl, rok, nullptr, 0, alpha, beta, bz);
+      __syncwarp();
+#pragma unroll
+      for (int o = KT; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (grp == 0 && rok) partial[j * k + t0 + rl] = s;
     }
     __threadfence();
     __syncwarp();
