@@ -334,9 +334,12 @@ def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024):
         num = max(float((yb.reshape(-1, k) - yc.t()).abs().max()) for yb, yc in zip(Yb, Yc))
         dnm = max(float(yc.abs().max()) for yc in Yc)
         nbytes = sum(4 * (int(n) + 1) for n in ns) + 12 * tot_nnz + 16 * k * tot_rows
-        best_plain = min(v for v in (graph_cols, eager_cols) if v is not None)
+        # the plain path: one spops_spmv launch per matrix and RHS column, as a
+        # caller of the per-matrix API issues them; also replayed from a CUDA
+        # graph (launch gaps removed), the stricter comparison
         r.update({"batched_ms": round(bms, 3), "batched_GB/s": round(nbytes / bms / 1e6, 1),
-                  "speedup_vs_per_column": round(best_plain / bms, 2),
+                  "speedup_vs_plain_launches": round(eager_cols / bms, 2),
+                  "speedup_vs_plain_launches_graph": None if graph_cols is None else round(graph_cols / bms, 2),
                   "normwise_rel_err_vs_plain": num / max(dnm, 1e-300)})
         if k > 1:
             r["speedup_vs_per_matrix_spmm"] = round(r["plain_per_matrix_spmm_ms"] / bms, 2)

@@ -185,6 +185,62 @@ __global__ void product_count_kernel(const I* __restrict__ aci, int64_t nnz, con
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
 
+// Flat sweep of a cluster's products by a whole block: the cluster's columns
+// are taken kSweepCols at a time, their B row lengths scanned in shared
+// memory, and every (column, B entry) product of the chunk handed to one
+// thread (its column found by binary search), so all B loads of the chunk
+// are issued at once whatever the row lengths.  fn(jj, k) gets the column's
+// index in the cluster and the B entry.
+constexpr int kSweepCols = 256;
+
+struct SweepSmem {
+  int64_t off[kSweepCols + 1];  // products before each column of the chunk
+  int64_t start[kSweepCols];    // B row start of each column
+};
+
+template <typename I, typename F>
+__device__ __forceinline__ void block_sweep(const int64_t* __restrict__ cptr, const int32_t* __restrict__ colids,
+                                            int64_t c, const I* __restrict__ brp, SweepSmem& sw, F fn) {
+  const int64_t j0 = cptr[c], nj = cptr[c + 1] - j0;
+  for (int64_t jb = 0; jb < nj; jb += kSweepCols) {
+    const int cnt = (int)(nj - jb < kSweepCols ? nj - jb : kSweepCols);
+    __syncthreads();  // the previous chunk's readers are done
+    if (threadIdx.x == 0) sw.off[0] = 0;
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      const int64_t r = colids[j0 + jb + t];
+      sw.start[t] = brp[r];
+      sw.off[t + 1] = (int64_t)brp[r + 1] - (int64_t)brp[r];
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // inclusive scan of the lengths by warp 0
+      const int lane = threadIdx.x;
+      int64_t carry = 0;
+      for (int t0 = 0; t0 < cnt; t0 += 32) {
+        const int t = t0 + lane;
+        int64_t v = t < cnt ? sw.off[t + 1] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int64_t u = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o) v += u;
+        }
+        if (t < cnt) sw.off[t + 1] = carry + v;
+        carry += __shfl_sync(0xffffffffu, v, 31);
+      }
+    }
+    __syncthreads();
+    const int64_t total = sw.off[cnt];
+    for (int64_t q = threadIdx.x; q < total; q += blockDim.x) {
+      int lo = 0, hi = cnt;  // last t with off[t] <= q
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (sw.off[mid] <= q) lo = mid; else hi = mid;
+      }
+      fn(jb + lo, sw.start[lo] + (q - sw.off[lo]));
+    }
+  }
+  __syncthreads();
+}
+
 // ------------------------------------------------------------ symbolic
 // Block per cluster; table of tsize slots in shared memory, or at
 // gtab + goff[b] in global memory when gtab != nullptr.
@@ -209,20 +265,17 @@ __global__ void symbolic_kernel(const int64_t* __restrict__ list, int64_t nlist,
     s_max = -1;
   }
   for (int64_t t = threadIdx.x; t < tsize; t += blockDim.x) tab[t] = -1;
-  __syncthreads();
+  __shared__ SweepSmem sw;
   unsigned long long cnt = 0;
   int mn = INT32_MAX, mx = -1;
-  for (int64_t j = cptr[c] + threadIdx.x; j < cptr[c + 1]; j += blockDim.x) {
-    const int64_t r = colids[j];
-    for (int64_t k = brp[r]; k < brp[r + 1]; ++k) {
-      const int32_t key = (int32_t)bci[k];
-      if (hash_insert(tab, mask, key)) {
-        ++cnt;
-        mn = key < mn ? key : mn;
-        mx = key > mx ? key : mx;
-      }
+  block_sweep(cptr, colids, c, brp, sw, [&](int64_t, int64_t k) {
+    const int32_t key = (int32_t)bci[k];
+    if (hash_insert(tab, mask, key)) {
+      ++cnt;
+      mn = key < mn ? key : mn;
+      mx = key > mx ? key : mx;
     }
-  }
+  });
   atomicAdd(&s_cnt, cnt);
   atomicMin(&s_min, mn);
   atomicMax(&s_max, mx);
@@ -235,6 +288,8 @@ __global__ void symbolic_kernel(const int64_t* __restrict__ list, int64_t nlist,
 }
 
 // ------------------------------------------------------------ numeric
+constexpr int kWideCols = 128;  // A columns per chunk of the wide warp kernel's sweep
+
 struct NumSlot {   // per-cluster arena layout (elements)
   int64_t tsize;   // hash slots
   int64_t lsize;   // sort list length (power of two >= nz)
@@ -451,6 +506,162 @@ __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nl
 }
 
 
+// Numeric phase, one warp per cluster with any number of A columns (the
+// clusters beyond numeric_warp_kernel's 32 columns / 512 outputs whose arena
+// fits the warp's slice of shared memory).  Warp arena (bytes at w * bytes):
+// tab (int32, tsize) | pos (int32, tsize) | keys (int32, lsize) | offsets
+// (int64, kWideCols + 1) | starts (int64, kWideCols) | acc (V, nz*csz).  The
+// products are swept in flat (j, k) order kWideCols columns at a time, 32 per
+// step (a lane finds its column by binary search in the chunk's offsets); the
+// output columns are sorted by a bitonic network; products of one step that
+// hit the same column are summed in lane order and added by the lowest lane,
+// so the summation order depends only on the matrices.
+template <typename I, typename V>
+__global__ void numeric_warp_wide_kernel(const int64_t* __restrict__ list, int64_t nlist,
+                                         const NumSlot* __restrict__ slots, int64_t warp_bytes,
+                                         const int64_t* __restrict__ cptr, const int64_t* __restrict__ cptr_val,
+                                         const int32_t* __restrict__ colids, const V* __restrict__ avals,
+                                         const int64_t* __restrict__ offsets, const I* __restrict__ brp,
+                                         const I* __restrict__ bci, const V* __restrict__ bv,
+                                         const int64_t* __restrict__ nz, const int64_t* __restrict__ ccptr,
+                                         const int64_t* __restrict__ ccptr_val,
+                                         const unsigned char* __restrict__ drop_small, int32_t* __restrict__ ccol,
+                                         V* __restrict__ cval) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t b = blockIdx.x * (int64_t)(blockDim.x >> 5) + w;
+  if (b >= nlist) return;
+  const int64_t c = list[b];
+  const NumSlot S = slots[b];
+  const int64_t nzc = nz[c];
+  const int64_t csz = offsets[c + 1] - offsets[c];
+  unsigned char* base = sm + (int64_t)w * warp_bytes;
+  int32_t* tab = reinterpret_cast<int32_t*>(base);
+  int32_t* pos = tab + S.tsize;
+  int32_t* keys = pos + S.tsize;
+  int64_t* coff = reinterpret_cast<int64_t*>(base + ((4 * (2 * S.tsize + S.lsize) + 15) & ~15LL));
+  int64_t* cstart = coff + kWideCols + 1;
+  V* acc = reinterpret_cast<V*>(cstart + kWideCols);
+  const uint32_t mask = (uint32_t)(S.tsize - 1);
+  for (int64_t t = lane; t < S.tsize; t += 32) tab[t] = -1;
+  for (int64_t t = lane; t < nzc * csz; t += 32) acc[t] = V(0);
+  const int64_t j0 = cptr[c], nj = cptr[c + 1] - j0;
+  // fn(jj, k, valid) for every product in flat order, 32 per call, all lanes
+  auto sweep = [&](auto fn) {
+    for (int64_t jb = 0; jb < nj; jb += kWideCols) {
+      const int cnt = (int)(nj - jb < kWideCols ? nj - jb : kWideCols);
+      __syncwarp();
+      int64_t carry = 0;
+      for (int t0 = 0; t0 < cnt; t0 += 32) {
+        const int t = t0 + lane;
+        int64_t len = 0;
+        if (t < cnt) {
+          const int64_t r = colids[j0 + jb + t];
+          cstart[t] = brp[r];
+          len = (int64_t)brp[r + 1] - (int64_t)brp[r];
+        }
+        int64_t inc = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += u;
+        }
+        if (t < cnt) coff[t + 1] = carry + inc;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+      }
+      if (lane == 0) coff[0] = 0;
+      __syncwarp();
+      const int64_t total = coff[cnt];
+      for (int64_t q0 = 0; q0 < total; q0 += 32) {
+        const int64_t q = q0 + lane;
+        int lo = 0;
+        int64_t k = 0;
+        if (q < total) {
+          int hi = cnt;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (coff[mid] <= q) lo = mid; else hi = mid;
+          }
+          k = cstart[lo] + (q - coff[lo]);
+        }
+        fn(jb + lo, k, q < total);
+      }
+    }
+    __syncwarp();
+  };
+  // 1. distinct columns
+  sweep([&](int64_t, int64_t k, bool valid) {
+    if (valid) hash_insert(tab, mask, (int32_t)bci[k]);
+  });
+  // 2. compact (slot order), pad to lsize, bitonic sort ascending
+  int64_t n = 0;
+  for (int64_t t0 = 0; t0 < S.tsize; t0 += 32) {
+    const int32_t v = t0 + lane < S.tsize ? tab[t0 + lane] : -1;
+    const unsigned m = __ballot_sync(0xffffffffu, v != -1);
+    if (v != -1) keys[n + __popc(m & ((1u << lane) - 1u))] = v;
+    n += __popc(m);
+  }
+  for (int64_t t = n + lane; t < S.lsize; t += 32) keys[t] = INT32_MAX;
+  __syncwarp();
+  for (int64_t kk = 2; kk <= S.lsize; kk <<= 1) {
+    for (int64_t jj = kk >> 1; jj > 0; jj >>= 1) {
+      for (int64_t i = lane; i < S.lsize; i += 32) {
+        const int64_t ixj = i ^ jj;
+        if (ixj > i) {
+          const bool up = (i & kk) == 0;
+          const int32_t a = keys[i], d = keys[ixj];
+          if ((a > d) == up) {
+            keys[i] = d;
+            keys[ixj] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // 3. position of every column; the output column list
+  const int64_t co = ccptr[c], cvo = ccptr_val[c];
+  for (int64_t p = lane; p < nzc; p += 32) {
+    pos[hash_find(tab, mask, keys[p])] = (int32_t)p;
+    ccol[co + p] = keys[p];
+  }
+  __syncwarp();
+  // 4. accumulate in flat (j, k) order
+  const int64_t vbase = cptr_val[c];
+  sweep([&](int64_t jj, int64_t k, bool valid) {
+    int32_t p = -1 - lane;  // distinct for idle lanes
+    V bval = V(0);
+    if (valid) {
+      p = pos[hash_find(tab, mask, (int32_t)bci[k])];
+      bval = bv[k];
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, p);
+    const int leader = __ffs(grp) - 1;
+    for (int64_t l = 0; l < csz; ++l) {
+      const V v = valid ? avals[vbase + jj * csz + l] * bval : V(0);
+      V sum = v;
+      if (grp != (1u << lane)) {
+        sum = V(0);
+        for (unsigned m = grp; m; m &= m - 1) sum += __shfl_sync(grp, v, __ffs(m) - 1);
+      }
+      if (valid && lane == leader) acc[p * csz + l] += sum;
+    }
+    __syncwarp();
+  });
+  // 5. drop rule and output
+  const bool drop = drop_small[c] != 0;
+  for (int64_t p = lane; p < nzc; p += 32) {
+    bool small = drop;
+    if (drop)
+      for (int64_t l = 0; l < csz; ++l)
+        if (fabs((double)acc[p * csz + l]) >= 1e-12) {
+          small = false;
+          break;
+        }
+    for (int64_t l = 0; l < csz; ++l) cval[cvo + p * csz + l] = small ? V(0) : acc[p * csz + l];
+  }
+}
+
 template <typename I, typename V>
 __global__ void numeric_kernel(const int64_t* __restrict__ list, int64_t nlist, const NumSlot* __restrict__ slots,
                                const int64_t* __restrict__ cptr, const int64_t* __restrict__ cptr_val,
@@ -476,15 +687,11 @@ __global__ void numeric_kernel(const int64_t* __restrict__ list, int64_t nlist, 
   const uint32_t mask = (uint32_t)(S.tsize - 1);
   __shared__ int s_n;
   if (threadIdx.x == 0) s_n = 0;
+  __shared__ SweepSmem sw;
   for (int64_t t = threadIdx.x; t < S.tsize; t += blockDim.x) tab[t] = -1;
   for (int64_t t = threadIdx.x; t < nzc * csz; t += blockDim.x) acc[t] = V(0);
-  __syncthreads();
   // 1. distinct columns
-  for (int64_t j = cptr[c] + threadIdx.x; j < cptr[c + 1]; j += blockDim.x) {
-    const int64_t r = colids[j];
-    for (int64_t k = brp[r]; k < brp[r + 1]; ++k) hash_insert(tab, mask, (int32_t)bci[k]);
-  }
-  __syncthreads();
+  block_sweep(cptr, colids, c, brp, sw, [&](int64_t, int64_t k) { hash_insert(tab, mask, (int32_t)bci[k]); });
   // 2. compact and sort them ascending
   for (int64_t t = threadIdx.x; t < S.tsize; t += blockDim.x)
     if (tab[t] != -1) keys[atomicAdd(&s_n, 1)] = tab[t];
@@ -605,6 +812,115 @@ __global__ void row_write_kernel(const int64_t* __restrict__ ccptr, const int64_
   }
 }
 
+// ------------------------------------------------------------ binning
+// Clusters are grouped by the kernel shape that serves them: a key per
+// cluster (0..kBins-1, kNoBin to skip), one stable radix sort of (key,
+// cluster) so each bin lists its clusters in ascending order, and the bin
+// boundaries found by binary search in the sorted keys.  Only the
+// boundaries come back to the host.
+constexpr uint32_t kNoBin = 15;
+
+__device__ __forceinline__ int64_t pow2_ceil(int64_t v) {
+  return v <= 1 ? 1 : (int64_t)1 << (64 - __clzll((unsigned long long)(v - 1)));
+}
+
+__global__ void weight_kernel(const int64_t* __restrict__ cnt, const int64_t* __restrict__ offsets, int64_t ncl,
+                              int64_t* __restrict__ weighted) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < ncl) weighted[c] = cnt[c] * (offsets[c + 1] - offsets[c]);
+}
+
+// symbolic: table >= 2 * min(flops, cols) slots; 0 warp, 1 / 2 block in
+// shared memory (smem0 / smem1 bytes), 3 block in global memory
+__global__ void sym_bin_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ cnt, int64_t ncl,
+                               int64_t bcols, int64_t warp_tab, int64_t smem0, int64_t smem1,
+                               uint32_t* __restrict__ key, int64_t* __restrict__ ids, int64_t* __restrict__ tsz) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= ncl) return;
+  const int64_t f = flops[c] < bcols ? flops[c] : bcols;
+  const int64_t ts = pow2_ceil(2 * f > 2 ? 2 * f : 2);
+  uint32_t b;
+  if (cnt[c] <= 32 && ts <= warp_tab) b = 0;
+  else if (ts * 4 <= smem0) b = 1;
+  else if (ts * 4 <= smem1) b = 2;
+  else b = 3;
+  key[c] = b;
+  ids[c] = c;
+  tsz[c] = ts;
+}
+
+// numeric: 0 / 1 warp arenas of wbytes[0] / [1] (at most 32 A columns and 512
+// output columns); 2 / 3 wide-warp arenas of wbytes[2] / [3]; 4 / 5 block
+// arenas in wbytes[4] / [5] of shared memory; 6 block arena in global memory
+struct NumBinLimits {
+  int64_t wbytes[6];
+};
+
+__global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __restrict__ cnt,
+                               const int64_t* __restrict__ offsets, int64_t ncl, int64_t vsize, NumBinLimits lim,
+                               uint32_t* __restrict__ key, int64_t* __restrict__ ids) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= ncl) return;
+  ids[c] = c;
+  const int64_t z = nz[c];
+  if (z == 0) {
+    key[c] = kNoBin;
+    return;
+  }
+  const int64_t csz = offsets[c + 1] - offsets[c];
+  const int64_t tsize = pow2_ceil(2 * z > 2 ? 2 * z : 2), lsize = pow2_ceil(z);
+  const int64_t accb = z * csz * vsize;
+  if (cnt[c] <= 32 && z <= 512) {
+    const int64_t wb = ((4 * (2 * tsize + z) + 15) & ~15LL) + accb;
+    if (wb <= lim.wbytes[0]) { key[c] = 0; return; }
+    if (wb <= lim.wbytes[1]) { key[c] = 1; return; }
+  }
+  const int64_t wide = ((4 * (2 * tsize + lsize) + 15) & ~15LL) + 8 * (2 * kWideCols + 1) + accb;
+  if (wide <= lim.wbytes[2]) { key[c] = 2; return; }
+  if (wide <= lim.wbytes[3]) { key[c] = 3; return; }
+  const int64_t bytes = ((accb + 15) & ~15LL) + 4 * (2 * tsize + lsize);
+  key[c] = bytes <= lim.wbytes[4] ? 4 : (bytes <= lim.wbytes[5] ? 5 : 6);
+}
+
+__global__ void bin_bounds_kernel(const uint32_t* __restrict__ skey, int64_t ncl, int nb, int64_t* __restrict__ start) {
+  const int b = threadIdx.x;
+  if (b > nb) return;
+  int64_t lo = 0, hi = ncl;  // first position with key >= b
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (skey[mid] < (uint32_t)b) lo = mid + 1; else hi = mid;
+  }
+  start[b] = lo;
+}
+
+// per listed cluster: symbolic table size (and its global-arena size)
+__global__ void sym_list_kernel(const int64_t* __restrict__ sids, const int64_t* __restrict__ tsz, int64_t m,
+                                int64_t* __restrict__ ltsz) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p < m) ltsz[p] = tsz[sids[p]];
+}
+
+// per listed cluster: numeric slots and arena bytes (256-aligned)
+__global__ void num_list_kernel(const int64_t* __restrict__ sids, const int64_t* __restrict__ nz,
+                                const int64_t* __restrict__ offsets, int64_t m, int64_t vsize,
+                                NumSlot* __restrict__ slots, int64_t* __restrict__ gbytes) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= m) return;
+  const int64_t c = sids[p], z = nz[c];
+  const int64_t csz = offsets[c + 1] - offsets[c];
+  NumSlot S;
+  S.tsize = pow2_ceil(2 * z > 2 ? 2 * z : 2);
+  S.lsize = pow2_ceil(z > 1 ? z : 1);
+  slots[p] = S;
+  const int64_t bytes = ((z * csz * vsize + 15) & ~15LL) + 4 * (2 * S.tsize + S.lsize);
+  gbytes[p] = (bytes + 255) & ~255LL;
+}
+
+__global__ void to_i32_kernel(const int64_t* __restrict__ a, int64_t m, int32_t* __restrict__ b) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = (int32_t)a[i];
+}
+
 template <typename T>
 spops_status_t d2h(cudaStream_t st, std::vector<T>& h, const void* d, size_t n) {
   h.resize(n);
@@ -718,18 +1034,31 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
                                                        reinterpret_cast<unsigned long long*>(ncols_u.p));
     SPOPS_LAUNCH_CHECK();
   }
-  // cluster pointers on the host (ncl values)
-  std::vector<int64_t> hcnt, hoff(offs_h, offs_h + ncl + 1), hcptr(ncl + 1, 0), hcptr_val(ncl + 1, 0);
-  SPOPS_TRY(d2h(st, hcnt, ncols_u.p, (size_t)ncl));
-  for (int64_t c = 0; c < ncl; ++c) {
-    const int64_t csz = hoff[c + 1] - hoff[c];
-    hcptr[c + 1] = hcptr[c] + hcnt[c];
-    hcptr_val[c + 1] = hcptr_val[c] + hcnt[c] * csz;
+  // cluster column pointers: exclusive scans of the column counts, plain and
+  // weighted by the cluster size (ncols_u[ncl] and cw[ncl] are zero)
+  PoolBuf cw(ctx), tot(ctx);
+  SPOPS_TRY(cptr.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(cptr_val.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(cw.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(tot.alloc(64));
+  SPOPS_CUDA(cudaMemsetAsync(cw.p, 0, (size_t)(ncl + 1) * 8, st));
+  const int64_t* cnt_d = reinterpret_cast<const int64_t*>(ncols_u.p);
+  if (ncl > 0) {
+    weight_kernel<<<grid_for(ncl), 256, 0, st>>>(cnt_d, offs.as<int64_t>(), ncl, cw.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
   }
-  SPOPS_TRY(h2d(st, cptr, hcptr));
-  SPOPS_TRY(h2d(st, cptr_val, hcptr_val));
-  tr.mark(st, "cluster pointers (host)");
-  const int64_t nnzv = hcptr_val[ncl];
+  {
+    size_t c1 = 0, c2 = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c1, cnt_d, cptr.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c2, cw.as<int64_t>(), cptr_val.as<int64_t>(), ncl + 1, st));
+    SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, cnt_d, cptr.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c2, cw.as<int64_t>(), cptr_val.as<int64_t>(), ncl + 1, st));
+  }
+  int64_t nnzv = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&nnzv, cptr_val.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  tr.mark(st, "cluster pointers");
   SPOPS_TRY(avals.alloc((size_t)std::max<int64_t>(nnzv, 1) * sizeof(V)));
   SPOPS_CUDA(cudaMemsetAsync(avals.p, 0, avals.bytes, st));
   if (nnz > 0) {
@@ -744,117 +1073,146 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   if (stats) stats->cluster_ms = tm.lap(st);
   tr.mark(st, "cluster values + frees");
 
-  // --- flops per cluster and symbolic bins
+  // --- flops per cluster
   PoolBuf flops(ctx), nzd(ctx), cmin(ctx), cmax(ctx);
   SPOPS_TRY(flops.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
-  SPOPS_TRY(nzd.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
+  SPOPS_TRY(nzd.alloc((size_t)(ncl + 1) * 8));
   SPOPS_TRY(cmin.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
   SPOPS_TRY(cmax.alloc((size_t)std::max<int64_t>(ncl, 1) * 8));
+  SPOPS_CUDA(cudaMemsetAsync(nzd.p, 0, (size_t)(ncl + 1) * 8, st));
   if (ncl > 0) {
     cluster_flops_kernel<I><<<grid_for(ncl * 32), 256, 0, st>>>(cptr.as<int64_t>(), colids.as<int32_t>(), ncl,
                                                                 B->row.as<I>(), flops.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
   }
-  std::vector<int64_t> hflops;
-  SPOPS_TRY(d2h(st, hflops, flops.p, (size_t)ncl));
-  tr.mark(st, "flops per cluster");
   int64_t total_products = 0;
   {
-    PoolBuf pc(ctx);
-    SPOPS_TRY(pc.alloc(8));
-    SPOPS_CUDA(cudaMemsetAsync(pc.p, 0, 8, st));
+    SPOPS_CUDA(cudaMemsetAsync(tot.p, 0, 8, st));
     if (nnz > 0) {
       product_count_kernel<I><<<std::min<unsigned>(grid_for(nnz), 4096u), 256, 0, st>>>(
-          A->col.as<I>(), nnz, B->row.as<I>(), B->rows, reinterpret_cast<unsigned long long*>(pc.p));
+          A->col.as<I>(), nnz, B->row.as<I>(), B->rows, reinterpret_cast<unsigned long long*>(tot.p));
       SPOPS_LAUNCH_CHECK();
     }
-    SPOPS_CUDA(cudaMemcpyAsync(&total_products, pc.p, 8, cudaMemcpyDeviceToHost, st));
-    SPOPS_CUDA(cudaStreamSynchronize(st));
-    pc.release();
+    SPOPS_CUDA(cudaMemcpyAsync(&total_products, tot.p, 8, cudaMemcpyDeviceToHost, st));
   }
-  const int64_t bcols = B->cols;
-  // symbolic: table >= 2 * min(flops, cols) slots
-  struct Bin {
-    std::vector<int64_t> list, tsize, goff;
-    int threads = 32;
-    size_t smem = 0;
-    bool global = false;
+  // sort (bin key, cluster) pairs; bounds of the nb bins to the host
+  PoolBuf bkey(ctx), bkey_s(ctx), bid(ctx), bid_s(ctx), bstart(ctx);
+  const size_t ncl1 = (size_t)std::max<int64_t>(ncl, 1);
+  SPOPS_TRY(bkey.alloc(ncl1 * 4));
+  SPOPS_TRY(bkey_s.alloc(ncl1 * 4));
+  SPOPS_TRY(bid.alloc(ncl1 * 8));
+  SPOPS_TRY(bid_s.alloc(ncl1 * 8));
+  SPOPS_TRY(bstart.alloc(64 * 8));
+  auto sort_bins = [&](int nb, std::vector<int64_t>& start) -> spops_status_t {
+    start.assign((size_t)nb + 1, 0);
+    if (ncl == 0) return SPOPS_OK;
+    size_t cb2 = 0;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cb2, bkey.as<uint32_t>(), bkey_s.as<uint32_t>(),
+                                               bid.as<int64_t>(), bid_s.as<int64_t>(), ncl, 0, 4, st));
+    SPOPS_TRY(tmp.alloc(cb2 + 256));
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, cb2, bkey.as<uint32_t>(), bkey_s.as<uint32_t>(),
+                                               bid.as<int64_t>(), bid_s.as<int64_t>(), ncl, 0, 4, st));
+    bin_bounds_kernel<<<1, 32, 0, st>>>(bkey_s.as<uint32_t>(), ncl, nb, bstart.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cudaMemcpyAsync(start.data(), bstart.p, ((size_t)nb + 1) * 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    return SPOPS_OK;
   };
-  auto sym_tsize = [&](int64_t c) { return pow2_at_least(std::max<int64_t>(2 * std::min(hflops[c], bcols), 2)); };
-  Bin sb[3];
-  sb[0].threads = 32; sb[0].smem = 16 << 10;
-  sb[1].threads = 256; sb[1].smem = 128 << 10;
-  sb[2].threads = 256; sb[2].global = true;
-  // warp-per-cluster bin: at most 32 distinct A columns, table of <= kSymWarpTab slots
+  // exclusive scan of sizes[from, to) into offs_out[from, to); returns the total
+  auto seg_scan = [&](int64_t* sizes, int64_t* offs_out, int64_t from, int64_t to, int64_t* total) -> spops_status_t {
+    *total = 0;
+    if (to <= from) return SPOPS_OK;
+    size_t cb2 = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cb2, sizes + from, offs_out + from, to - from, st));
+    SPOPS_TRY(tmp.alloc(cb2 + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cb2, sizes + from, offs_out + from, to - from, st));
+    int64_t last[2] = {0, 0};
+    SPOPS_CUDA(cudaMemcpyAsync(&last[0], offs_out + to - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&last[1], sizes + to - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    *total = last[0] + last[1];
+    return SPOPS_OK;
+  };
+  tr.mark(st, "flops per cluster");
+
+  // --- symbolic: 0 warp per cluster (<= 32 A columns, table <= kSymWarpTab),
+  // 1 / 2 block with the table in 16 KB / 128 KB of shared memory, 3 global
+  const int64_t bcols = B->cols;
   constexpr int kSymWarps = 8;
   constexpr int64_t kSymWarpTab = 2048;
-  std::vector<int64_t> wlist, wtsize;
+  const int sym_threads[4] = {32 * kSymWarps, 32, 256, 256};
+  const size_t sym_smem[4] = {(size_t)kSymWarps * kSymWarpTab * 4, 16 << 10, 128 << 10, 0};
+  PoolBuf tszc(ctx), ltsz(ctx), sgoff(ctx), gtab(ctx);
+  SPOPS_TRY(tszc.alloc(ncl1 * 8));
+  SPOPS_TRY(ltsz.alloc(ncl1 * 8));
+  SPOPS_TRY(sgoff.alloc(ncl1 * 8));
+  std::vector<int64_t> sstart;
+  if (ncl > 0) {
+    sym_bin_kernel<<<grid_for(ncl), 256, 0, st>>>(flops.as<int64_t>(), cnt_d, ncl, bcols, kSymWarpTab,
+                                                 (int64_t)sym_smem[1], (int64_t)sym_smem[2], bkey.as<uint32_t>(),
+                                                 bid.as<int64_t>(), tszc.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  SPOPS_TRY(sort_bins(4, sstart));
+  if (ncl > 0) {
+    sym_list_kernel<<<grid_for(ncl), 256, 0, st>>>(bid_s.as<int64_t>(), tszc.as<int64_t>(), ncl, ltsz.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
   int64_t gsym = 0;
-  for (int64_t c = 0; c < ncl; ++c) {
-    const int64_t ts = sym_tsize(c);
-    if (hcnt[c] <= 32 && ts <= kSymWarpTab) {
-      wlist.push_back(c);
-      wtsize.push_back(ts);
-      continue;
-    }
-    const int which = ts * 4 <= (int64_t)sb[0].smem ? 0 : (ts * 4 <= (int64_t)sb[1].smem ? 1 : 2);
-    sb[which].list.push_back(c);
-    sb[which].tsize.push_back(ts);
-    if (which == 2) {
-      sb[2].goff.push_back(gsym);
-      gsym += ts;
-    }
-  }
-  if (!wlist.empty()) {
-    PoolBuf dl(ctx), dt(ctx);
-    SPOPS_TRY(h2d(st, dl, wlist));
-    SPOPS_TRY(h2d(st, dt, wtsize));
-    const size_t smem = (size_t)kSymWarps * kSymWarpTab * 4;
-    SPOPS_CUDA(cudaFuncSetAttribute(symbolic_warp_kernel<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t blocks = ((int64_t)wlist.size() + kSymWarps - 1) / kSymWarps;
-    symbolic_warp_kernel<I><<<(unsigned)blocks, 32 * kSymWarps, smem, st>>>(
-        dl.as<int64_t>(), (int64_t)wlist.size(), dt.as<int64_t>(), kSymWarpTab, cptr.as<int64_t>(),
-        colids.as<int32_t>(), B->row.as<I>(), B->col.as<I>(), nzd.as<int64_t>(), cmin.as<int64_t>(),
-        cmax.as<int64_t>());
-    SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cudaStreamSynchronize(st));
-  }
-  PoolBuf gtab(ctx);
+  SPOPS_TRY(seg_scan(ltsz.as<int64_t>(), sgoff.as<int64_t>(), sstart[3], sstart[4], &gsym));
   if (gsym) SPOPS_TRY(gtab.alloc((size_t)gsym * 4));
-  tr.mark(st, "symbolic bins + warp kernel");
-  for (int w = 0; w < 3; ++w) {
-    Bin& bn = sb[w];
-    if (bn.list.empty()) continue;
-    PoolBuf dl(ctx), dt(ctx), dg(ctx);
-    SPOPS_TRY(h2d(st, dl, bn.list));
-    SPOPS_TRY(h2d(st, dt, bn.tsize));
-    if (bn.global) SPOPS_TRY(h2d(st, dg, bn.goff));
-    const size_t smem = bn.global ? 0 : bn.smem;
-    if (smem > 48 * 1024)
-      SPOPS_CUDA(cudaFuncSetAttribute(symbolic_kernel<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    symbolic_kernel<I><<<(unsigned)bn.list.size(), bn.threads, smem, st>>>(
-        dl.as<int64_t>(), (int64_t)bn.list.size(), dt.as<int64_t>(), cptr.as<int64_t>(), colids.as<int32_t>(),
-        B->row.as<I>(), B->col.as<I>(), bn.global ? gtab.as<int32_t>() : nullptr,
-        bn.global ? dg.as<int64_t>() : nullptr, nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>());
+  tr.mark(st, "symbolic bins");
+  for (int w = 0; w < 4; ++w) {
+    const int64_t m = sstart[w + 1] - sstart[w];
+    if (m <= 0) continue;
+    const int64_t* dl = bid_s.as<int64_t>() + sstart[w];
+    const int64_t* dt = ltsz.as<int64_t>() + sstart[w];
+    if (w == 0) {
+      SPOPS_CUDA(cudaFuncSetAttribute(symbolic_warp_kernel<I>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sym_smem[0]));
+      symbolic_warp_kernel<I><<<(unsigned)((m + kSymWarps - 1) / kSymWarps), sym_threads[0], sym_smem[0], st>>>(
+          dl, m, dt, kSymWarpTab, cptr.as<int64_t>(), colids.as<int32_t>(), B->row.as<I>(), B->col.as<I>(),
+          nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>());
+    } else {
+      const bool global = w == 3;
+      if (sym_smem[w] > 48 * 1024)
+        SPOPS_CUDA(cudaFuncSetAttribute(symbolic_kernel<I>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sym_smem[w]));
+      symbolic_kernel<I><<<(unsigned)m, sym_threads[w], sym_smem[w], st>>>(
+          dl, m, dt, cptr.as<int64_t>(), colids.as<int32_t>(), B->row.as<I>(), B->col.as<I>(),
+          global ? gtab.as<int32_t>() : nullptr, global ? sgoff.as<int64_t>() + sstart[3] : nullptr,
+          nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>());
+    }
     SPOPS_LAUNCH_CHECK();
+  }
+  // output cluster pointers: exclusive scans of nz, plain and weighted
+  PoolBuf ccptr(ctx), ccptr_val(ctx), ccol(ctx), cval(ctx);
+  SPOPS_TRY(ccptr.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(ccptr_val.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_CUDA(cudaMemsetAsync(cw.p, 0, (size_t)(ncl + 1) * 8, st));
+  if (ncl > 0) {
+    weight_kernel<<<grid_for(ncl), 256, 0, st>>>(nzd.as<int64_t>(), offs.as<int64_t>(), ncl, cw.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  int64_t c_cols = 0, c_vals = 0;
+  {
+    size_t c1 = 0, c2 = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c1, nzd.as<int64_t>(), ccptr.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c2, cw.as<int64_t>(), ccptr_val.as<int64_t>(), ncl + 1, st));
+    SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, nzd.as<int64_t>(), ccptr.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c2, cw.as<int64_t>(), ccptr_val.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&c_cols, ccptr.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&c_vals, ccptr_val.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
-    dl.release(); dt.release(); dg.release();
   }
   gtab.release();
-  std::vector<int64_t> hnz;
-  SPOPS_TRY(d2h(st, hnz, nzd.p, (size_t)ncl));
-  std::vector<int64_t> hccptr(ncl + 1, 0), hccptr_val(ncl + 1, 0);
-  for (int64_t c = 0; c < ncl; ++c) {
-    const int64_t csz = hoff[c + 1] - hoff[c];
-    hccptr[c + 1] = hccptr[c] + hnz[c];
-    hccptr_val[c + 1] = hccptr_val[c] + hnz[c] * csz;
-  }
   if (stats) stats->symbolic_ms = tm.lap(st);
-  tr.mark(st, "symbolic block kernels + nz");
+  tr.mark(st, "symbolic kernels + nz scans");
 
   // --- classify (drop rule)
   PoolBuf drop(ctx), ndense(ctx);
-  SPOPS_TRY(drop.alloc((size_t)std::max<int64_t>(ncl, 1)));
+  SPOPS_TRY(drop.alloc(ncl1));
   SPOPS_TRY(ndense.alloc(8));
   SPOPS_CUDA(cudaMemsetAsync(ndense.p, 0, 8, st));
   const double b_rowdense = (double)B->nnz / (double)std::max<int64_t>(B->rows, 1);
@@ -867,101 +1225,82 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   }
   int64_t hdense = 0;
   SPOPS_CUDA(cudaMemcpyAsync(&hdense, ndense.p, 8, cudaMemcpyDeviceToHost, st));
-
-  // --- numeric bins by arena size
-  PoolBuf ccptr(ctx), ccptr_val(ctx), ccol(ctx), cval(ctx);
-  SPOPS_TRY(h2d(st, ccptr, hccptr));
-  SPOPS_TRY(h2d(st, ccptr_val, hccptr_val));
-  SPOPS_TRY(ccol.alloc((size_t)std::max<int64_t>(hccptr[ncl], 1) * 4));
-  SPOPS_TRY(cval.alloc((size_t)std::max<int64_t>(hccptr_val[ncl], 1) * sizeof(V)));
+  SPOPS_TRY(ccol.alloc((size_t)std::max<int64_t>(c_cols, 1) * 4));
+  SPOPS_TRY(cval.alloc((size_t)std::max<int64_t>(c_vals, 1) * sizeof(V)));
   tr.mark(st, "classify + cluster output alloc");
-  struct NBin {
-    std::vector<int64_t> list, goff;
-    std::vector<NumSlot> slots;
-    int threads;
-    size_t smem;
-    bool global;
-  };
-  NBin nb[4] = {{{}, {}, {}, 32, 24 << 10, false},
-                {{}, {}, {}, 128, 96 << 10, false},
-                {{}, {}, {}, 256, 200 << 10, false},
-                {{}, {}, {}, 256, 0, true}};
-  // warp-per-cluster bins (at most 32 distinct A columns, nz <= 512): arena bytes per warp, warps per block
-  struct WBin {
-    std::vector<int64_t> list;
-    std::vector<NumSlot> slots;
-    int64_t bytes;
-    int warps;
-  };
-  WBin wb[2] = {{{}, {}, 8 << 10, 8}, {{}, {}, 16 << 10, 4}};
-  int64_t garena = 0;
-  for (int64_t c = 0; c < ncl; ++c) {
-    if (hnz[c] == 0) continue;
-    const int64_t csz = hoff[c + 1] - hoff[c];
-    NumSlot S;
-    S.tsize = pow2_at_least(std::max<int64_t>(2 * hnz[c], 2));
-    S.lsize = pow2_at_least(std::max<int64_t>(hnz[c], 1));
-    if (hcnt[c] <= 32 && hnz[c] <= 512) {
-      const int64_t wbytes = ((4 * (2 * S.tsize + hnz[c]) + 15) & ~15LL) + hnz[c] * csz * (int64_t)sizeof(V);
-      int w = -1;
-      for (int t = 0; t < 2 && w < 0; ++t)
-        if (wbytes <= wb[t].bytes) w = t;
-      if (w >= 0) {
-        wb[w].list.push_back(c);
-        wb[w].slots.push_back(S);
-        continue;
-      }
-    }
-    const int64_t bytes = ((hnz[c] * csz * (int64_t)sizeof(V) + 15) & ~15LL) + 4 * (2 * S.tsize + S.lsize);
-    int w = 3;
-    for (int t = 0; t < 3; ++t)
-      if (bytes <= (int64_t)nb[t].smem) { w = t; break; }
-    nb[w].list.push_back(c);
-    nb[w].slots.push_back(S);
-    if (w == 3) {
-      nb[3].goff.push_back(garena);
-      garena += (bytes + 255) & ~255LL;
-    }
+
+  // --- numeric bins: 0 / 1 warp per cluster (8 KB arena, 8 warps / 16 KB, 4
+  // warps), 2 / 3 wide warp per cluster (16 KB, 8 warps / 48 KB, 4 warps),
+  // 4 / 5 block with the arena in 96 / 200 KB of shared memory, 6 block with
+  // the arena in global memory; clusters with nz == 0 are skipped
+  const int64_t warp_bytes[4] = {8 << 10, 16 << 10, 16 << 10, 48 << 10};
+  const int warp_count[4] = {8, 4, 8, 4};
+  const int num_threads[3] = {128, 256, 256};
+  const size_t num_smem[3] = {96 << 10, 200 << 10, 0};
+  NumBinLimits lim{{warp_bytes[0], warp_bytes[1], warp_bytes[2], warp_bytes[3], (int64_t)num_smem[0],
+                    (int64_t)num_smem[1]}};
+  PoolBuf nslots(ctx), ngb(ctx), ngoff(ctx), arena(ctx);
+  SPOPS_TRY(nslots.alloc(ncl1 * sizeof(NumSlot)));
+  SPOPS_TRY(ngb.alloc(ncl1 * 8));
+  SPOPS_TRY(ngoff.alloc(ncl1 * 8));
+  std::vector<int64_t> nstart;
+  if (ncl > 0) {
+    num_bin_kernel<<<grid_for(ncl), 256, 0, st>>>(nzd.as<int64_t>(), cnt_d, offs.as<int64_t>(), ncl, (int64_t)sizeof(V),
+                                                 lim, bkey.as<uint32_t>(), bid.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
   }
-  for (int w = 0; w < 2; ++w) {
-    WBin& bn = wb[w];
-    if (bn.list.empty()) continue;
-    PoolBuf dl(ctx), ds(ctx);
-    SPOPS_TRY(h2d(st, dl, bn.list));
-    SPOPS_TRY(h2d(st, ds, bn.slots));
-    const size_t smem = (size_t)bn.warps * (size_t)bn.bytes;
-    SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t blocks = ((int64_t)bn.list.size() + bn.warps - 1) / bn.warps;
-    numeric_warp_kernel<I, V><<<(unsigned)blocks, 32 * bn.warps, smem, st>>>(
-        dl.as<int64_t>(), (int64_t)bn.list.size(), ds.as<NumSlot>(), bn.bytes, cptr.as<int64_t>(),
+  SPOPS_TRY(sort_bins(7, nstart));
+  const int64_t nlisted = nstart[7];
+  if (nlisted > 0) {
+    num_list_kernel<<<grid_for(nlisted), 256, 0, st>>>(bid_s.as<int64_t>(), nzd.as<int64_t>(), offs.as<int64_t>(),
+                                                      nlisted, (int64_t)sizeof(V), nslots.as<NumSlot>(),
+                                                      ngb.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  int64_t garena = 0;
+  SPOPS_TRY(seg_scan(ngb.as<int64_t>(), ngoff.as<int64_t>(), nstart[6], nstart[7], &garena));
+  if (garena) SPOPS_TRY(arena.alloc((size_t)garena));
+  for (int w = 0; w < 4; ++w) {
+    const int64_t m = nstart[w + 1] - nstart[w];
+    if (m <= 0) continue;
+    const size_t smem = (size_t)warp_count[w] * (size_t)warp_bytes[w];
+    const unsigned grid = (unsigned)((m + warp_count[w] - 1) / warp_count[w]);
+    if (w < 2) {
+      SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+      numeric_warp_kernel<I, V><<<grid, 32 * warp_count[w], smem, st>>>(
+          bid_s.as<int64_t>() + nstart[w], m, nslots.as<NumSlot>() + nstart[w], warp_bytes[w], cptr.as<int64_t>(),
+          cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
+          B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+          drop.as<unsigned char>(), ccol.as<int32_t>(), cval.as<V>());
+    } else {
+      SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_wide_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+      numeric_warp_wide_kernel<I, V><<<grid, 32 * warp_count[w], smem, st>>>(
+          bid_s.as<int64_t>() + nstart[w], m, nslots.as<NumSlot>() + nstart[w], warp_bytes[w], cptr.as<int64_t>(),
+          cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
+          B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+          drop.as<unsigned char>(), ccol.as<int32_t>(), cval.as<V>());
+    }
+    SPOPS_LAUNCH_CHECK();
+  }
+  tr.mark(st, "numeric bins + warp kernels");
+  for (int w = 0; w < 3; ++w) {
+    const int64_t m = nstart[w + 5] - nstart[w + 4];
+    if (m <= 0) continue;
+    const bool global = w == 2;
+    if (num_smem[w] > 48 * 1024)
+      SPOPS_CUDA(cudaFuncSetAttribute(numeric_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)num_smem[w]));
+    numeric_kernel<I, V><<<(unsigned)m, num_threads[w], num_smem[w], st>>>(
+        bid_s.as<int64_t>() + nstart[w + 4], m, nslots.as<NumSlot>() + nstart[w + 4], cptr.as<int64_t>(),
         cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
         B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
-        drop.as<unsigned char>(), ccol.as<int32_t>(), cval.as<V>());
+        drop.as<unsigned char>(), global ? arena.as<unsigned char>() : nullptr,
+        global ? ngoff.as<int64_t>() + nstart[6] : nullptr, ccol.as<int32_t>(), cval.as<V>());
     SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cudaStreamSynchronize(st));
   }
-  PoolBuf arena(ctx);
-  if (garena) SPOPS_TRY(arena.alloc((size_t)garena));
-  tr.mark(st, "numeric bins + warp kernels");
-  for (int w = 0; w < 4; ++w) {
-    NBin& bn = nb[w];
-    if (bn.list.empty()) continue;
-    PoolBuf dl(ctx), ds(ctx), dg(ctx);
-    SPOPS_TRY(h2d(st, dl, bn.list));
-    SPOPS_TRY(h2d(st, ds, bn.slots));
-    if (bn.global) SPOPS_TRY(h2d(st, dg, bn.goff));
-    if (bn.smem > 48 * 1024)
-      SPOPS_CUDA(cudaFuncSetAttribute(numeric_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bn.smem));
-    numeric_kernel<I, V><<<(unsigned)bn.list.size(), bn.threads, bn.smem, st>>>(
-        dl.as<int64_t>(), (int64_t)bn.list.size(), ds.as<NumSlot>(), cptr.as<int64_t>(), cptr_val.as<int64_t>(),
-        colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(), B->col.as<I>(), B->val.as<V>(),
-        nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(), drop.as<unsigned char>(),
-        bn.global ? arena.as<unsigned char>() : nullptr, bn.global ? dg.as<int64_t>() : nullptr,
-        ccol.as<int32_t>(), cval.as<V>());
-    SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cudaStreamSynchronize(st));
-    dl.release(); ds.release(); dg.release();
-  }
+  SPOPS_CUDA(cudaStreamSynchronize(st));
   arena.release();
   if (stats) stats->numeric_ms = tm.lap(st);
   tr.mark(st, "numeric block kernels");
@@ -1004,14 +1343,11 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   }
   // row offsets in the index type
   tr.mark(st, "C alloc");
-  std::vector<int64_t> hcrp;
-  SPOPS_TRY(d2h(st, hcrp, crp.p, (size_t)n + 1));
   if (sizeof(I) == 8) {
     SPOPS_CUDA(cudaMemcpyAsync(C->row.p, crp.p, (size_t)(n + 1) * 8, cudaMemcpyDeviceToDevice, st));
   } else {
-    std::vector<int32_t> r32(hcrp.begin(), hcrp.end());
-    SPOPS_CUDA(cudaMemcpyAsync(C->row.p, r32.data(), r32.size() * 4, cudaMemcpyHostToDevice, st));
-    SPOPS_CUDA(cudaStreamSynchronize(st));
+    to_i32_kernel<<<grid_for(n + 1), 256, 0, st>>>(crp.as<int64_t>(), n + 1, C->row.as<int32_t>());
+    SPOPS_LAUNCH_CHECK();
   }
   if (ncl > 0 && cnnz > 0) {
     row_write_kernel<I, V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
@@ -1028,7 +1364,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     stats->clusters = ncl;
     stats->dense_clusters = hdense;
     stats->cluster_columns = nnzc;
-    stats->c_cluster_columns = hccptr[ncl];
+    stats->c_cluster_columns = c_cols;
   }
   *out = C;
   return SPOPS_OK;
