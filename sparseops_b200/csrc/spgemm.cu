@@ -394,6 +394,38 @@ __global__ void symbolic_warp_kernel(const int64_t* __restrict__ list, int64_t n
 // sweep that hit the same column are first summed in lane order (= ascending
 // j) and added by the lowest lane, so the per-column summation order depends
 // only on the matrices.
+// The keys of a hash table (slots != -1) compacted into keys[0..n), padded
+// with INT32_MAX to lsize (a power of two), and sorted ascending by one warp
+// with a bitonic network.
+__device__ __forceinline__ void warp_sort_keys(const int32_t* __restrict__ tab, int64_t tsize, int32_t* keys,
+                                               int64_t lsize, int lane) {
+  int64_t n = 0;
+  for (int64_t t0 = 0; t0 < tsize; t0 += 32) {
+    const int32_t v = t0 + lane < tsize ? tab[t0 + lane] : -1;
+    const unsigned m = __ballot_sync(0xffffffffu, v != -1);
+    if (v != -1) keys[n + __popc(m & ((1u << lane) - 1u))] = v;
+    n += __popc(m);
+  }
+  for (int64_t t = n + lane; t < lsize; t += 32) keys[t] = INT32_MAX;
+  __syncwarp();
+  for (int64_t kk = 2; kk <= lsize; kk <<= 1) {
+    for (int64_t jj = kk >> 1; jj > 0; jj >>= 1) {
+      for (int64_t i = lane; i < lsize; i += 32) {
+        const int64_t ixj = i ^ jj;
+        if (ixj > i) {
+          const bool up = (i & kk) == 0;
+          const int32_t a = keys[i], d = keys[ixj];
+          if ((a > d) == up) {
+            keys[i] = d;
+            keys[ixj] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 template <typename I, typename V>
 __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nlist, const NumSlot* __restrict__ slots,
                                     int64_t warp_bytes, const int64_t* __restrict__ cptr,
@@ -404,7 +436,6 @@ __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nl
                                     const int64_t* __restrict__ ccptr_val, const unsigned char* __restrict__ drop_small,
                                     int32_t* __restrict__ ccol, V* __restrict__ cval) {
   extern __shared__ __align__(16) unsigned char sm[];
-  constexpr int kMaxPerLane = 16;  // nz <= 512
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t b = blockIdx.x * (int64_t)(blockDim.x >> 5) + w;
   if (b >= nlist) return;
@@ -416,7 +447,7 @@ __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nl
   int32_t* tab = reinterpret_cast<int32_t*>(base);
   int32_t* pos = tab + S.tsize;
   int32_t* keys = pos + S.tsize;
-  V* acc = reinterpret_cast<V*>(base + ((4 * (2 * S.tsize + nzc) + 15) & ~15LL));
+  V* acc = reinterpret_cast<V*>(base + ((4 * (2 * S.tsize + S.lsize) + 15) & ~15LL));
   const uint32_t mask = (uint32_t)(S.tsize - 1);
   for (int64_t t = lane; t < S.tsize; t += 32) tab[t] = -1;
   for (int64_t t = lane; t < nzc * csz; t += 32) acc[t] = V(0);
@@ -431,37 +462,13 @@ __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nl
     if (t < wr.total) hash_insert(tab, mask, (int32_t)bci[st + (t - of)]);
   }
   __syncwarp();
-  // 2. compact (slot order)
-  int64_t n = 0;
-  for (int64_t t0 = 0; t0 < S.tsize; t0 += 32) {
-    const int32_t v = t0 + lane < S.tsize ? tab[t0 + lane] : -1;
-    const unsigned m = __ballot_sync(0xffffffffu, v != -1);
-    if (v != -1) keys[n + __popc(m & ((1u << lane) - 1u))] = v;
-    n += __popc(m);
-  }
-  __syncwarp();
-  // 3. rank by counting; the output column list is written in rank order
-  int32_t mine[kMaxPerLane];
-  int rank[kMaxPerLane];
-#pragma unroll
-  for (int q = 0; q < kMaxPerLane; ++q) {
-    const int64_t p = lane + 32 * q;
-    mine[q] = p < nzc ? keys[p] : INT32_MAX;
-    rank[q] = 0;
-  }
-  for (int64_t p = 0; p < nzc; ++p) {
-    const int32_t kq = keys[p];
-#pragma unroll
-    for (int q = 0; q < kMaxPerLane; ++q) rank[q] += kq < mine[q] ? 1 : 0;
-  }
+  // 2. compact (slot order), pad to lsize, 3. bitonic sort; positions and
+  //    the output column list in ascending order
+  warp_sort_keys(tab, S.tsize, keys, S.lsize, lane);
   const int64_t co = ccptr[c], cvo = ccptr_val[c];
-#pragma unroll
-  for (int q = 0; q < kMaxPerLane; ++q) {
-    const int64_t p = lane + 32 * q;
-    if (p < nzc) {
-      pos[hash_find(tab, mask, mine[q])] = rank[q];
-      ccol[co + rank[q]] = mine[q];
-    }
+  for (int64_t p = lane; p < nzc; p += 32) {
+    pos[hash_find(tab, mask, keys[p])] = (int32_t)p;
+    ccol[co + p] = keys[p];
   }
   __syncwarp();
   // 4. accumulate in flat (j, k) order
@@ -594,31 +601,7 @@ __global__ void numeric_warp_wide_kernel(const int64_t* __restrict__ list, int64
     if (valid) hash_insert(tab, mask, (int32_t)bci[k]);
   });
   // 2. compact (slot order), pad to lsize, bitonic sort ascending
-  int64_t n = 0;
-  for (int64_t t0 = 0; t0 < S.tsize; t0 += 32) {
-    const int32_t v = t0 + lane < S.tsize ? tab[t0 + lane] : -1;
-    const unsigned m = __ballot_sync(0xffffffffu, v != -1);
-    if (v != -1) keys[n + __popc(m & ((1u << lane) - 1u))] = v;
-    n += __popc(m);
-  }
-  for (int64_t t = n + lane; t < S.lsize; t += 32) keys[t] = INT32_MAX;
-  __syncwarp();
-  for (int64_t kk = 2; kk <= S.lsize; kk <<= 1) {
-    for (int64_t jj = kk >> 1; jj > 0; jj >>= 1) {
-      for (int64_t i = lane; i < S.lsize; i += 32) {
-        const int64_t ixj = i ^ jj;
-        if (ixj > i) {
-          const bool up = (i & kk) == 0;
-          const int32_t a = keys[i], d = keys[ixj];
-          if ((a > d) == up) {
-            keys[i] = d;
-            keys[ixj] = a;
-          }
-        }
-      }
-      __syncwarp();
-    }
-  }
+  warp_sort_keys(tab, S.tsize, keys, S.lsize, lane);
   // 3. position of every column; the output column list
   const int64_t co = ccptr[c], cvo = ccptr_val[c];
   for (int64_t p = lane; p < nzc; p += 32) {
@@ -850,10 +833,11 @@ __global__ void sym_bin_kernel(const int64_t* __restrict__ flops, const int64_t*
 }
 
 // numeric: 0 / 1 warp arenas of wbytes[0] / [1] (at most 32 A columns and 512
-// output columns); 2 / 3 wide-warp arenas of wbytes[2] / [3]; 4 / 5 block
-// arenas in wbytes[4] / [5] of shared memory; 6 block arena in global memory
+// output columns); 2 / 3 / 4 wide-warp arenas of wbytes[2] / [3] / [4]; 5 / 6
+// block arenas in wbytes[5] / [6] of shared memory; 7 block arena in global
+// memory
 struct NumBinLimits {
-  int64_t wbytes[6];
+  int64_t wbytes[7];
 };
 
 __global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __restrict__ cnt,
@@ -871,15 +855,15 @@ __global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __
   const int64_t tsize = pow2_ceil(2 * z > 2 ? 2 * z : 2), lsize = pow2_ceil(z);
   const int64_t accb = z * csz * vsize;
   if (cnt[c] <= 32 && z <= 512) {
-    const int64_t wb = ((4 * (2 * tsize + z) + 15) & ~15LL) + accb;
+    const int64_t wb = ((4 * (2 * tsize + lsize) + 15) & ~15LL) + accb;
     if (wb <= lim.wbytes[0]) { key[c] = 0; return; }
     if (wb <= lim.wbytes[1]) { key[c] = 1; return; }
   }
   const int64_t wide = ((4 * (2 * tsize + lsize) + 15) & ~15LL) + 8 * (2 * kWideCols + 1) + accb;
-  if (wide <= lim.wbytes[2]) { key[c] = 2; return; }
-  if (wide <= lim.wbytes[3]) { key[c] = 3; return; }
+  for (uint32_t b = 2; b <= 4; ++b)
+    if (wide <= lim.wbytes[b]) { key[c] = b; return; }
   const int64_t bytes = ((accb + 15) & ~15LL) + 4 * (2 * tsize + lsize);
-  key[c] = bytes <= lim.wbytes[4] ? 4 : (bytes <= lim.wbytes[5] ? 5 : 6);
+  key[c] = bytes <= lim.wbytes[5] ? 5 : (bytes <= lim.wbytes[6] ? 6 : 7);
 }
 
 __global__ void bin_bounds_kernel(const uint32_t* __restrict__ skey, int64_t ncl, int nb, int64_t* __restrict__ start) {
@@ -1095,6 +1079,12 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     }
     SPOPS_CUDA(cudaMemcpyAsync(&total_products, tot.p, 8, cudaMemcpyDeviceToHost, st));
   }
+  // the hash-table kernels want the largest shared-memory split of each SM
+  SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_kernel<I, V>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_wide_kernel<I, V>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  SPOPS_CUDA(cudaFuncSetAttribute(numeric_kernel<I, V>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  SPOPS_CUDA(cudaFuncSetAttribute(symbolic_warp_kernel<I>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  SPOPS_CUDA(cudaFuncSetAttribute(symbolic_kernel<I>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   // sort (bin key, cluster) pairs; bounds of the nb bins to the host
   PoolBuf bkey(ctx), bkey_s(ctx), bid(ctx), bid_s(ctx), bstart(ctx);
   const size_t ncl1 = (size_t)std::max<int64_t>(ncl, 1);
@@ -1230,14 +1220,16 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   tr.mark(st, "classify + cluster output alloc");
 
   // --- numeric bins: 0 / 1 warp per cluster (8 KB arena, 8 warps / 16 KB, 4
-  // warps), 2 / 3 wide warp per cluster (16 KB, 8 warps / 48 KB, 4 warps),
-  // 4 / 5 block with the arena in 96 / 200 KB of shared memory, 6 block with
-  // the arena in global memory; clusters with nz == 0 are skipped
-  const int64_t warp_bytes[4] = {8 << 10, 16 << 10, 16 << 10, 48 << 10};
-  const int warp_count[4] = {8, 4, 8, 4};
+  // warps), 2 / 3 / 4 wide warp per cluster (16 KB, 2 warps / 32 KB, 1 warp /
+  // 56 KB, 1 warp: small blocks so that the SM's shared memory fills), 5 / 6
+  // block with the arena in 96 / 200 KB of shared memory, 7 block with the
+  // arena in global memory; clusters with nz == 0 are skipped
+  constexpr int kWarpBins = 5;
+  const int64_t warp_bytes[kWarpBins] = {8 << 10, 16 << 10, 16 << 10, 32 << 10, 56 << 10};
+  const int warp_count[kWarpBins] = {8, 4, 2, 1, 1};
   const int num_threads[3] = {128, 256, 256};
   const size_t num_smem[3] = {96 << 10, 200 << 10, 0};
-  NumBinLimits lim{{warp_bytes[0], warp_bytes[1], warp_bytes[2], warp_bytes[3], (int64_t)num_smem[0],
+  NumBinLimits lim{{warp_bytes[0], warp_bytes[1], warp_bytes[2], warp_bytes[3], warp_bytes[4], (int64_t)num_smem[0],
                     (int64_t)num_smem[1]}};
   PoolBuf nslots(ctx), ngb(ctx), ngoff(ctx), arena(ctx);
   SPOPS_TRY(nslots.alloc(ncl1 * sizeof(NumSlot)));
@@ -1249,8 +1241,8 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
                                                  lim, bkey.as<uint32_t>(), bid.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
   }
-  SPOPS_TRY(sort_bins(7, nstart));
-  const int64_t nlisted = nstart[7];
+  SPOPS_TRY(sort_bins(8, nstart));
+  const int64_t nlisted = nstart[8];
   if (nlisted > 0) {
     num_list_kernel<<<grid_for(nlisted), 256, 0, st>>>(bid_s.as<int64_t>(), nzd.as<int64_t>(), offs.as<int64_t>(),
                                                       nlisted, (int64_t)sizeof(V), nslots.as<NumSlot>(),
@@ -1258,9 +1250,9 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_LAUNCH_CHECK();
   }
   int64_t garena = 0;
-  SPOPS_TRY(seg_scan(ngb.as<int64_t>(), ngoff.as<int64_t>(), nstart[6], nstart[7], &garena));
+  SPOPS_TRY(seg_scan(ngb.as<int64_t>(), ngoff.as<int64_t>(), nstart[7], nstart[8], &garena));
   if (garena) SPOPS_TRY(arena.alloc((size_t)garena));
-  for (int w = 0; w < 4; ++w) {
+  for (int w = 0; w < kWarpBins; ++w) {
     const int64_t m = nstart[w + 1] - nstart[w];
     if (m <= 0) continue;
     const size_t smem = (size_t)warp_count[w] * (size_t)warp_bytes[w];
@@ -1286,18 +1278,18 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   }
   tr.mark(st, "numeric bins + warp kernels");
   for (int w = 0; w < 3; ++w) {
-    const int64_t m = nstart[w + 5] - nstart[w + 4];
+    const int64_t m = nstart[w + kWarpBins + 1] - nstart[w + kWarpBins];
     if (m <= 0) continue;
     const bool global = w == 2;
     if (num_smem[w] > 48 * 1024)
       SPOPS_CUDA(cudaFuncSetAttribute(numeric_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)num_smem[w]));
     numeric_kernel<I, V><<<(unsigned)m, num_threads[w], num_smem[w], st>>>(
-        bid_s.as<int64_t>() + nstart[w + 4], m, nslots.as<NumSlot>() + nstart[w + 4], cptr.as<int64_t>(),
+        bid_s.as<int64_t>() + nstart[w + kWarpBins], m, nslots.as<NumSlot>() + nstart[w + kWarpBins], cptr.as<int64_t>(),
         cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
         B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
         drop.as<unsigned char>(), global ? arena.as<unsigned char>() : nullptr,
-        global ? ngoff.as<int64_t>() + nstart[6] : nullptr, ccol.as<int32_t>(), cval.as<V>());
+        global ? ngoff.as<int64_t>() + nstart[7] : nullptr, ccol.as<int32_t>(), cval.as<V>());
     SPOPS_LAUNCH_CHECK();
   }
   SPOPS_CUDA(cudaStreamSynchronize(st));
