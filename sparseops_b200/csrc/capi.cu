@@ -462,6 +462,44 @@ spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t
   cudaStream_t st = ctx->stream;
   if (xb) SPOPS_CUDA(cudaMemcpyAsync(ctx->xbuf.p, x_host, xb, cudaMemcpyHostToDevice, st));
   if (beta != 0.0 && yb) SPOPS_CUDA(cudaMemcpyAsync(ctx->ybuf.p, y_host, yb, cudaMemcpyHostToDevice, st));
+  // Large CSR matrices on the default kernel: the SpMV runs in kHostParts row
+  // ranges and each range's rows of y go back to the host on a second stream
+  // while the next range computes, so only the last range's copy is exposed.
+  constexpr int kHostParts = 8;
+  // (only into page-locked y: a copy to pageable memory blocks the host and
+  // would serialise the ranges)
+  cudaPointerAttributes ya{};
+  const bool y_pinned = y_host && cudaPointerGetAttributes(&ya, y_host) == cudaSuccess &&
+                        ya.type == cudaMemoryTypeHost;
+  cudaGetLastError();  // a pageable pointer may leave an error behind on some drivers
+  const bool piped = y_pinned && A->format == SPOPS_FMT_CSR && A->rows >= (int64_t)1 << 20 && A->nnz > 0 &&
+                     ctx->csr_variant == 0 && csr_tile_usable(A, 0);
+  if (piped) {
+    if (!ctx->copy_stream) SPOPS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    while ((int)ctx->part_events.size() < kHostParts) {
+      cudaEvent_t e;
+      SPOPS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ctx->part_events.push_back(e);
+    }
+    if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+    const size_t vs = A->vsize();
+    int used = 0;
+    spops_status_t s = csr_tile_spmv_parts(
+        ctx, A, kHostParts, alpha, ctx->xbuf.p, beta, ctx->ybuf.p, [&](int64_t r0, int64_t r1) -> spops_status_t {
+          cudaEvent_t e = ctx->part_events[(size_t)(used++ % kHostParts)];
+          SPOPS_CUDA(cudaEventRecord(e, st));
+          SPOPS_CUDA(cudaStreamWaitEvent(ctx->copy_stream, e, 0));
+          SPOPS_CUDA(cudaMemcpyAsync(static_cast<char*>(y_host) + r0 * vs, ctx->ybuf.as<char>() + r0 * vs,
+                                     (size_t)(r1 - r0) * vs, cudaMemcpyDeviceToHost, ctx->copy_stream));
+          return SPOPS_OK;
+        });
+    cudaError_t e1 = cudaStreamSynchronize(ctx->copy_stream);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    SPOPS_TRY(s);
+    SPOPS_CUDA(e1);
+    SPOPS_CUDA(e2);
+    return SPOPS_OK;
+  }
   SPOPS_TRY(spops_spmv(ctx, alpha, A, ctx->xbuf.p, beta, ctx->ybuf.p));
   if (yb) SPOPS_CUDA(cudaMemcpyAsync(y_host, ctx->ybuf.p, yb, cudaMemcpyDeviceToHost, st));
   SPOPS_CUDA(cudaStreamSynchronize(st));

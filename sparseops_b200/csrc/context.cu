@@ -136,6 +136,10 @@ spops_status_t spops_destroy(spops_context_t c) {
   c->errword.release();
   c->xbuf.release();
   c->ybuf.release();
+  for (cudaEvent_t e : c->part_events) cudaEventDestroy(e);
+  c->part_events.clear();
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  c->copy_stream = nullptr;
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->pool) {
     cudaStreamSynchronize(c->stream);

@@ -31,6 +31,9 @@
 // Summation order depends only on the matrix: results are bit-reproducible.
 #include <cub/cub.cuh>
 
+#include <functional>
+#include <vector>
+
 #include "device_util.cuh"
 #include "spops_internal.h"
 
@@ -232,12 +235,12 @@ __device__ __forceinline__ void tile_finish(const I* __restrict__ rp, int64_t n,
 template <typename I, typename V, int K, int kMinBlocks, bool kPipe>
 __global__ void __launch_bounds__(kTileBlock, kMinBlocks) csr_tile_kernel(
     const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
-    const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t tiles,
+    const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t t_begin, int64_t tiles,
     const V* __restrict__ x, V* __restrict__ y, V alpha, V beta, bool bz, V* __restrict__ carry_in,
     V* __restrict__ open_sum, int64_t* __restrict__ open_row) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
-  int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5);
+  int64_t t = t_begin + blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5);
   if (t >= tiles) return;
   I c[K];
   V a[K];
@@ -269,12 +272,14 @@ __global__ void __launch_bounds__(kTileBlock, kMinBlocks) csr_tile_kernel(
 }
 
 // Rows open at a tile's end receive the heads of the following tiles up to the
-// first one that starts a row; empty rows get y = beta*y.
+// first one that starts a row; empty rows get y = beta*y.  Tiles [t_begin,
+// tiles) only: a range ends where a row starts, so no chain crosses it.
 template <typename V>
-__global__ void csr_tile_calibrate_kernel(int64_t tiles, const V* __restrict__ carry_in, const V* __restrict__ open_sum,
-                                          const int64_t* __restrict__ open_row, const int64_t* __restrict__ empty,
-                                          int64_t nempty, V* __restrict__ y, V alpha, V beta, bool bz) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void csr_tile_calibrate_kernel(int64_t t_begin, int64_t tiles, const V* __restrict__ carry_in,
+                                          const V* __restrict__ open_sum, const int64_t* __restrict__ open_row,
+                                          const int64_t* __restrict__ empty, int64_t nempty, V* __restrict__ y,
+                                          V alpha, V beta, bool bz) {
+  const int64_t t = t_begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t < tiles) {
     const int64_t r = open_row[t];
     if (r < 0) return;
@@ -287,6 +292,25 @@ __global__ void csr_tile_calibrate_kernel(int64_t tiles, const V* __restrict__ c
   } else if (t - tiles < nempty) {
     axpby_store(y + empty[t - tiles], V(0), alpha, beta, bz);
   }
+}
+
+// Boundaries of `parts` tile ranges for the pipelined host SpMV: range p
+// starts at the first tile at or after p * tiles / parts whose first entry
+// starts a row (so every row lies in one range), and rb[p] is that row.
+template <typename I, int K>
+__global__ void part_bounds_kernel(const I* __restrict__ rp, int64_t n, const uint8_t* __restrict__ flags,
+                                   int64_t tiles, int parts, int64_t* __restrict__ tb, int64_t* __restrict__ rb) {
+  const int p = threadIdx.x;
+  if (p > parts) return;
+  if (p == 0 || p == parts) {
+    tb[p] = p == 0 ? 0 : tiles;
+    rb[p] = p == 0 ? 0 : n;
+    return;
+  }
+  int64_t t = tiles * p / parts;
+  while (t < tiles && !(flags[t * 32] & 1u)) ++t;
+  tb[p] = t;
+  rb[p] = t < tiles ? row_holding(rp, n, t * (32 * K)) : n;
 }
 
 template <int K>
@@ -329,11 +353,13 @@ spops_status_t analyse_t(Context* ctx, Matrix* A) {
   return SPOPS_OK;
 }
 
+// Tiles [t0, t1) and their calibration; the empty rows when `empty_rows`.
 template <typename I, typename V, int K, int kMinBlocks, bool kPipe>
-spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
+spops_status_t spmv_range(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y, int64_t t0,
+                          int64_t t1, bool empty_rows) {
   const CsrTiles& D = A->plan.tiles;
   const bool bz = beta == 0.0;
-  if (D.tiles > 0) {
+  if (t1 > t0) {
     static int blocks_per_sm = -1;  // per instantiation
     if (blocks_per_sm < 0) {
       int bps = 0;
@@ -342,19 +368,40 @@ spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, doub
       blocks_per_sm = bps > 0 ? bps : 1;
     }
     int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
-    const int64_t need = (D.tiles + kTileBlock / 32 - 1) / (kTileBlock / 32);
+    const int64_t need = (t1 - t0 + kTileBlock / 32 - 1) / (kTileBlock / 32);
     if (grid > need) grid = need;
     csr_tile_kernel<I, V, K, kMinBlocks, kPipe><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
         A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), A->val.as<V>(), D.tile_row.as<int64_t>(),
-        D.flags.as<uint8_t>(), D.tiles, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, bz,
+        D.flags.as<uint8_t>(), t0, t1, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, bz,
         D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
   }
-  if (D.tiles + D.nempty > 0) {
-    csr_tile_calibrate_kernel<V><<<grid_of(D.tiles + D.nempty), 256, 0, ctx->stream>>>(
-        D.tiles, D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), D.nempty,
+  const int64_t ne = empty_rows ? D.nempty : 0;
+  if (t1 - t0 + ne > 0) {
+    csr_tile_calibrate_kernel<V><<<grid_of(t1 - t0 + ne), 256, 0, ctx->stream>>>(
+        t0, t1, D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), ne,
         static_cast<V*>(y), (V)alpha, (V)beta, bz);
     SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
+}
+
+template <typename I, typename V, int K, int kMinBlocks, bool kPipe>
+spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
+  return spmv_range<I, V, K, kMinBlocks, kPipe>(ctx, A, alpha, x, beta, y, 0, A->plan.tiles.tiles, true);
+}
+
+// y in `parts` row ranges; after each range, done(r0, r1) with the stream
+// position at which rows [r0, r1) of y are final.
+template <typename I, typename V>
+spops_status_t spmv_parts_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y,
+                            const std::vector<int64_t>& tb, const std::vector<int64_t>& rb,
+                            const std::function<spops_status_t(int64_t, int64_t)>& done) {
+  const int parts = (int)tb.size() - 1;
+  for (int p = 0; p < parts; ++p) {
+    if (rb[p + 1] <= rb[p] && tb[p + 1] <= tb[p] && p > 0) continue;
+    SPOPS_TRY((spmv_range<I, V, 8, 3, true>(ctx, A, alpha, x, beta, y, tb[p], tb[p + 1], p == 0)));
+    if (rb[p + 1] > rb[p]) SPOPS_TRY(done(rb[p], rb[p + 1]));
   }
   return SPOPS_OK;
 }
@@ -374,6 +421,8 @@ spops_status_t dispatch(Context* ctx, Matrix* A, int variant, double alpha, cons
 
 void CsrTiles::release() {
   tile_row.release(); flags.release(); carry_in.release(); open_sum.release(); open_row.release(); empty.release();
+  part_tb.clear();
+  part_rb.clear();
   tiles = 0;
   nempty = 0;
   k = 0;
@@ -394,6 +443,34 @@ spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k) {
   const bool i32 = A->itype == SPOPS_INDEX_I32;
   if (k == 8) return i32 ? analyse_t<int32_t, 8>(ctx, A) : analyse_t<int64_t, 8>(ctx, A);
   return i32 ? analyse_t<int32_t, 4>(ctx, A) : analyse_t<int64_t, 4>(ctx, A);
+}
+
+spops_status_t csr_tile_spmv_parts(Context* ctx, Matrix* A, int parts, double alpha, const void* x, double beta,
+                                   void* y, const std::function<spops_status_t(int64_t, int64_t)>& done) {
+  if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(ctx, A, 8));
+  CsrTiles& D = A->plan.tiles;
+  const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
+  if ((int)D.part_tb.size() != parts + 1) {  // boundaries, once per matrix and part count
+    SPOPS_TRY(ctx->scratch_reserve((size_t)(2 * parts + 2) * 8));
+    int64_t* tb = ctx->scratch.as<int64_t>();
+    int64_t* rb = tb + parts + 1;
+    if (i32)
+      part_bounds_kernel<int32_t, 8><<<1, 64, 0, ctx->stream>>>(A->row.as<int32_t>(), A->rows, D.flags.as<uint8_t>(),
+                                                                D.tiles, parts, tb, rb);
+    else
+      part_bounds_kernel<int64_t, 8><<<1, 64, 0, ctx->stream>>>(A->row.as<int64_t>(), A->rows, D.flags.as<uint8_t>(),
+                                                                D.tiles, parts, tb, rb);
+    SPOPS_LAUNCH_CHECK();
+    std::vector<int64_t> h((size_t)(2 * parts + 2));
+    SPOPS_CUDA(cudaMemcpyAsync(h.data(), tb, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    SPOPS_CUDA(cudaStreamSynchronize(ctx->stream));
+    D.part_tb.assign(h.begin(), h.begin() + parts + 1);
+    D.part_rb.assign(h.begin() + parts + 1, h.end());
+  }
+  if (i32 && f64) return spmv_parts_t<int32_t, double>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
+  if (i32) return spmv_parts_t<int32_t, float>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
+  if (f64) return spmv_parts_t<int64_t, double>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
+  return spmv_parts_t<int64_t, float>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
 }
 
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta,

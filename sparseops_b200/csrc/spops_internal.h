@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "../../include/sparseops_b200.h"
@@ -61,6 +62,9 @@ struct Context {
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
   DevBuf xbuf, ybuf;
+  // second stream and per-range events of the pipelined spops_spmv_host
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> part_events;
   // stream-ordered pool for per-call temporaries (PoolBuf): memory freed by
   // one call is handed to the next without returning it to the driver
   cudaMemPool_t pool = nullptr;
@@ -134,6 +138,7 @@ struct CsrTiles {
   DevBuf open_sum;         // V [tiles]: partial sum of the row open at the tile's end
   DevBuf open_row;         // int64 [tiles]: that row, or -1 (no row starts in the tile)
   DevBuf empty;            // int64 [rows]: empty rows
+  std::vector<int64_t> part_tb, part_rb;  // tile / row bounds of the pipelined host SpMV's ranges
   void release();
 };
 
@@ -317,6 +322,10 @@ spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, do
 bool csr_tile_usable(const Matrix* A, int variant);
 spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k);
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y);
+// The default tile SpMV in `parts` row ranges; done(r0, r1) is called after
+// each range is enqueued, when rows [r0, r1) of y are final on the stream.
+spops_status_t csr_tile_spmv_parts(Context* ctx, Matrix* A, int parts, double alpha, const void* x, double beta,
+                                   void* y, const std::function<spops_status_t(int64_t, int64_t)>& done);
 
 // spmv_csr_win.cu
 bool csr_win_usable(const Matrix* A);

@@ -291,3 +291,33 @@ def test_windows_powerlaw_and_value_updates(cuda, orc):
         assert _err(orc, rp, ci, v3, x, yd.cpu().numpy(), orc.spmv_csr(rp, ci, v3, x)) <= TOL64
     finally:
         ctx.set_option("csr_variant", 0)
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_path_pipelined(cuda, orc, pinned):
+    """spops_spmv_host on a matrix large enough for the ranged path (rows >=
+    2^20): y comes back range by range while later ranges compute; the result
+    equals the device-resident SpMV bit for bit (same kernel and order)."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, default_context
+    from sparseops_b200._lib import call, dbl, vp
+    rp, ci, v = synth.powerlaw(1_300_000, mu=1.5, sigma=1.0, hi=3000, seed=9)
+    n = len(rp) - 1
+    x = synth.uniform(n, 3)
+    y0 = synth.uniform(n, 4)
+    ctx = default_context()
+    A = CSR_Matrix(n, n, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda())
+    h = A.device(ctx)
+    xd = torch.from_numpy(x).cuda()
+    for alpha, beta in [(1.0, 0.0), (0.5, 0.25)]:
+        yd = torch.from_numpy(y0.copy()).cuda()
+        call("spops_spmv", ctx.handle, dbl(alpha), h.handle, vp(xd.data_ptr()), dbl(beta), vp(yd.data_ptr()))
+        xh = torch.from_numpy(x.copy())
+        yh = torch.from_numpy(y0.copy())
+        if pinned:
+            xh, yh = xh.pin_memory(), yh.pin_memory()
+        call("spops_spmv_host", ctx.handle, dbl(alpha), h.handle, vp(xh.data_ptr()), dbl(beta), vp(yh.data_ptr()))
+        torch.cuda.synchronize()
+        assert torch.equal(yh, yd.cpu())
+        yref = orc.spmv_csr(rp.astype(np.int64), ci.astype(np.int64), v, x, alpha, beta, y0)
+        assert _err(orc, rp.astype(np.int64), ci.astype(np.int64), v, x, yh.numpy(), yref, beta, y0, alpha) <= TOL64
