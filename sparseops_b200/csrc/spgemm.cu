@@ -408,17 +408,19 @@ __device__ __forceinline__ void warp_sort_keys(const int32_t* __restrict__ tab, 
   }
   for (int64_t t = n + lane; t < lsize; t += 32) keys[t] = INT32_MAX;
   __syncwarp();
+  // one compare-exchange pair per lane and step: pair q of stage (kk, jj) is
+  // (i, i + jj) with i = q with a zero bit inserted at jj
+  const int64_t half = lsize >> 1;
   for (int64_t kk = 2; kk <= lsize; kk <<= 1) {
     for (int64_t jj = kk >> 1; jj > 0; jj >>= 1) {
-      for (int64_t i = lane; i < lsize; i += 32) {
-        const int64_t ixj = i ^ jj;
-        if (ixj > i) {
-          const bool up = (i & kk) == 0;
-          const int32_t a = keys[i], d = keys[ixj];
-          if ((a > d) == up) {
-            keys[i] = d;
-            keys[ixj] = a;
-          }
+      for (int64_t q = lane; q < half; q += 32) {
+        const int64_t i = ((q & ~(jj - 1)) << 1) | (q & (jj - 1));
+        const int64_t ixj = i + jj;
+        const bool up = (i & kk) == 0;
+        const int32_t a = keys[i], d = keys[ixj];
+        if ((a > d) == up) {
+          keys[i] = d;
+          keys[ixj] = a;
         }
       }
       __syncwarp();
