@@ -327,6 +327,20 @@ spops_status_t spops_spgemm_clustered(spops_context_t ctx, spops_matrix_t A, spo
                                       const int64_t* permutation, const int64_t* offsets, int64_t nclusters,
                                       int32_t sort_output, double l2_budget_bytes, spops_matrix_t* C,
                                       spops_spgemm_stats_t* stats);
+/* Row-wise C = A * B: every structural entry of the product kept (exact
+ * zeros included, no small-value drop), ascending columns in every row.
+ * Replaces LeSpGEMM<sortOutput,I,V>(A, B, C, kernel_flag) (src/spgemm.cpp:683)
+ * with its hash / array / sparse-accumulator row kernels (kernel_flag 1 / 2 /
+ * 3, src/spgemm.cpp:44-235); they produce the same entries and differ only in
+ * the unsorted column order of kernel 1, which ascending order satisfies. */
+spops_status_t spops_spgemm_rowwise(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B, int32_t kernel_flag,
+                                    int32_t sort_output, spops_matrix_t* C, spops_spgemm_stats_t* stats);
+/* Top-k Jaccard similarities of A's rows: for every row i, the top_k other
+ * rows j (j != i) sharing a column with it, by |A_i n A_j| / |A_i u A_j|
+ * (value type arithmetic, row lengths from A's offsets), ordered by
+ * similarity descending then column ascending.  Replaces HashSpGEMMTopK
+ * (src/spgemm.cpp:708-842, src/spgemm_hash.cpp:168-318). */
+spops_status_t spops_spgemm_topk(spops_context_t ctx, spops_matrix_t A, int64_t top_k, spops_matrix_t* C);
 /* The whole LeSpGEMM pipeline: MinHash + LSH (device), clustering (host),
  * cluster-wise SpGEMM (device). */
 spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B, int32_t k, int32_t bands,

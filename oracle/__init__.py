@@ -51,7 +51,7 @@ class Oracle:
         if not os.path.exists(path):
             build(ref=False)
         self.L = L = C.CDLL(path)
-        for name in ("orc_lsh_pairs", "orc_spgemm"):
+        for name in ("orc_lsh_pairs", "orc_spgemm", "orc_spgemm_rowwise", "orc_spgemm_topk"):
             getattr(L, name).restype = _vp
         for name in ("orc_pairs_count", "orc_hc", "orc_dia_offsets", "orc_bsr_structure",
                      "orc_spgemm_flop", "orc_coo_to_csr_f64", "orc_coo_to_csr_f32"):
@@ -159,6 +159,33 @@ class Oracle:
         self.L.orc_csr_free(_vp(h))
         return dict(rp=rp, ci=ci, v=v, absv=a, dense_clusters=int(info[2]), flops=int(info[3]))
 
+    def _orc_csr(self, h, n):
+        info = np.zeros(4, np.int64)
+        self.L.orc_csr_info(_vp(h), _p(info))
+        rp = np.zeros(n + 1, np.int64)
+        ci, v, a = np.zeros(info[1], np.int64), np.zeros(info[1]), np.zeros(info[1])
+        self.L.orc_csr_copy(_vp(h), _p(rp), _p(ci), _p(v), _p(a))
+        self.L.orc_csr_free(_vp(h))
+        return dict(rp=rp, ci=ci, v=v, absv=a, flops=int(info[3]))
+
+    def spgemm_rowwise(self, A, B):
+        """Row-wise C = A*B, every structural entry kept, columns ascending."""
+        arp, aci, av = (np.ascontiguousarray(np.asarray(a, t)) for a, t in zip(A[:3], (np.int64, np.int64, np.float64)))
+        brp, bci, bv = (np.ascontiguousarray(np.asarray(a, t)) for a, t in zip(B[:3], (np.int64, np.int64, np.float64)))
+        n = len(arp) - 1
+        h = self.L.orc_spgemm_rowwise(_i64(n), _p(arp), _p(aci), _p(av), _i64(len(brp) - 1), _p(brp), _p(bci),
+                                      _p(bv))
+        return self._orc_csr(h, n)
+
+    def spgemm_topk(self, rp, ci, ncols, top_k, f32=False):
+        """HashSpGEMMTopK's rows: (columns, Jaccard values) per row in the
+        reference's order."""
+        rp = np.ascontiguousarray(np.asarray(rp, np.int64))
+        ci = np.ascontiguousarray(np.asarray(ci, np.int64))
+        n = len(rp) - 1
+        h = self.L.orc_spgemm_topk(_i64(n), _p(rp), _p(ci), _i64(ncols), _i64(top_k), C.c_int32(1 if f32 else 0))
+        return self._orc_csr(h, n)
+
     def spgemm_flop(self, A, B):
         arp, aci = A[0], A[1]
         brp = B[0]
@@ -215,7 +242,8 @@ class Reference:
             raise FileNotFoundError(f"reference library not built: {path}")
         self.path = path
         self.L = L = C.CDLL(path)
-        for name in ("ref_fmt_build", "ref_lsh_pairs", "ref_spgemm_kernel3", "ref_csr_transpose", "ref_coo_to_csr"):
+        for name in ("ref_fmt_build", "ref_lsh_pairs", "ref_spgemm_kernel3", "ref_csr_transpose", "ref_coo_to_csr",
+                     "ref_spgemm_rowwise", "ref_spgemm_topk"):
             getattr(L, name).restype = _vp
         L.ref_pairs_count.restype = _i64
         L.ref_hc.restype = _i64
@@ -304,6 +332,33 @@ class Reference:
         self.L.ref_csr_copy(_vp(h), _p(rp), _p(ci), _p(v))
         self.L.ref_csr_free(_vp(h))
         return dict(rp=rp, ci=ci[:info[2]], v=v[:info[2]], dense_clusters=int(info[3]), clusters=int(info[4]))
+
+    def _ref_csr(self, h):
+        info = np.zeros(6, np.int64)
+        self.L.ref_csr_info(_vp(h), _p(info))
+        rp = np.zeros(info[0] + 1, np.int64)
+        ci, v = np.zeros(max(info[2], 1), np.int64), np.zeros(max(info[2], 1))
+        self.L.ref_csr_copy(_vp(h), _p(rp), _p(ci), _p(v))
+        self.L.ref_csr_free(_vp(h))
+        return dict(rp=rp, ci=ci[:info[2]], v=v[:info[2]])
+
+    def spgemm_rowwise(self, A, B, kernel_flag=1, sort_output=False):
+        """The reference's LeSpGEMM<sortOutput, int64_t, double>(A, B, C, kernel_flag)."""
+        arp, aci, av = A
+        brp, bci, bv = B[:3]
+        n = len(arp) - 1
+        bcols = int(B[3]) if len(B) > 3 else n
+        h = self.L.ref_spgemm_rowwise(_i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av),
+                                      _i64(len(brp) - 1), _i64(bcols), _i64(len(bci)), _p(brp), _p(bci), _p(bv),
+                                      C.c_int(int(kernel_flag)), C.c_int(int(sort_output)))
+        return self._ref_csr(h)
+
+    def spgemm_topk(self, rp, ci, ncols, top_k, f32=False):
+        """The reference's HashSpGEMMTopK<int64_t, V>(A, C, top_k)."""
+        n = len(rp) - 1
+        h = self.L.ref_spgemm_topk(_i64(n), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _i64(top_k),
+                                   C.c_int(1 if f32 else 0))
+        return self._ref_csr(h)
 
     def spgemm_kernel3_time(self, A, B, perm, offsets, iters=3, l2_fraction=-1.0):
         """Mean ms of the reference's LeSpGEMM_VLength kernel 3 (numeric and

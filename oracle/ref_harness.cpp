@@ -440,6 +440,54 @@ void* ref_csr_transpose(ll nr, ll nc, ll nnz, const ll* rp, const ll* ci, const 
   return h;
 }
 
+// ---------------------------------------------------- row-wise and top-k
+// LeSpGEMM<sortOutput, int64_t, double>(A, B, C, kernel_flag) (src/spgemm.cpp:683).
+void* ref_spgemm_rowwise(ll a_rows, ll a_cols, ll a_nnz, const ll* arp, const ll* aci, const double* av, ll b_rows,
+                         ll b_cols, ll b_nnz, const ll* brp, const ll* bci, const double* bv, int kernel_flag,
+                         int sort_output) {
+  CSR_Matrix<int64_t, double> A = wrap_csr<int64_t, double>(a_rows, a_cols, a_nnz, (const int64_t*)arp,
+                                                            (const int64_t*)aci, av, 0);
+  CSR_Matrix<int64_t, double> B = wrap_csr<int64_t, double>(b_rows, b_cols, b_nnz, (const int64_t*)brp,
+                                                            (const int64_t*)bci, bv, 0);
+  CsrHandle* h = new CsrHandle();
+  if (sort_output)
+    LeSpGEMM<true, int64_t, double>(A, B, h->C, kernel_flag);
+  else
+    LeSpGEMM<false, int64_t, double>(A, B, h->C, kernel_flag);
+  return h;
+}
+
+// HashSpGEMMTopK<int64_t, V>(A, C, top_k) (src/spgemm.cpp:708); float values
+// are widened to double in the handle.
+void* ref_spgemm_topk(ll nr, ll nc, ll nnz, const ll* rp, const ll* ci, ll top_k, int f32) {
+  CsrHandle* h = new CsrHandle();
+  if (f32) {
+    std::vector<float> ones((size_t)(nnz > 0 ? nnz : 1), 1.0f);
+    CSR_Matrix<int64_t, float> A = wrap_csr<int64_t, float>(nr, nc, nnz, (const int64_t*)rp, (const int64_t*)ci,
+                                                            ones.data(), 0);
+    CSR_Matrix<int64_t, float> C{};
+    HashSpGEMMTopK<int64_t, float>(A, C, (int64_t)top_k);
+    h->C.num_rows = C.num_rows;
+    h->C.num_cols = C.num_cols;
+    h->C.num_nnzs = C.num_nnzs;
+    h->C.row_offset = new_array<int64_t>(C.num_rows + 1);
+    std::memcpy(h->C.row_offset, C.row_offset, (size_t)(C.num_rows + 1) * sizeof(int64_t));
+    h->C.col_index = new_array<int64_t>(C.num_nnzs > 0 ? C.num_nnzs : 1);
+    h->C.values = new_array<double>(C.num_nnzs > 0 ? C.num_nnzs : 1);
+    for (ll t = 0; t < (ll)C.num_nnzs; ++t) {
+      h->C.col_index[t] = C.col_index[t];
+      h->C.values[t] = (double)C.values[t];
+    }
+    delete_host_matrix(C);
+  } else {
+    std::vector<double> ones((size_t)(nnz > 0 ? nnz : 1), 1.0);
+    CSR_Matrix<int64_t, double> A = wrap_csr<int64_t, double>(nr, nc, nnz, (const int64_t*)rp, (const int64_t*)ci,
+                                                              ones.data(), 0);
+    HashSpGEMMTopK<int64_t, double>(A, h->C, (int64_t)top_k);
+  }
+  return h;
+}
+
 }  // extern "C"
 
 extern "C" double ref_spgemm_kernel3_time(ll a_rows, ll a_cols, ll a_nnz, const ll* arp,

@@ -446,6 +446,96 @@ void* orc_spgemm(int64_t a_rows, const int64_t* arp, const int64_t* aci, const d
   return out;
 }
 
+// Row-wise C = A*B (src/spgemm.cpp:44-235; the hash kernel's per-row loop,
+// src/spgemm_hash.cpp:246-318): per row, products a_ij * b_jk added into an
+// accumulator per column in (j, k) order; every structural entry is kept,
+// exact zeros included; columns ascending.
+void* orc_spgemm_rowwise(int64_t a_rows, const int64_t* arp, const int64_t* aci, const double* av, int64_t b_rows,
+                         const int64_t* brp, const int64_t* bci, const double* bv) {
+  OrcCsr* out = new OrcCsr();
+  out->rows = a_rows;
+  out->rp.assign((size_t)a_rows + 1, 0);
+  std::map<int64_t, std::pair<double, double>> acc;
+  for (int64_t i = 0; i < a_rows; ++i) {
+    acc.clear();
+    for (int64_t e = arp[i]; e < arp[i + 1]; ++e) {
+      const int64_t j = aci[e];
+      for (int64_t f = brp[j]; f < brp[j + 1]; ++f) {
+        auto& a = acc[bci[f]];
+        a.first += av[e] * bv[f];
+        a.second += std::fabs(av[e] * bv[f]);
+        out->flops += 2;
+      }
+    }
+    for (const auto& kv : acc) {
+      out->ci.push_back(kv.first);
+      out->v.push_back(kv.second.first);
+      out->absv.push_back(kv.second.second);
+    }
+    out->rp[i + 1] = (int64_t)out->ci.size();
+  }
+  (void)b_rows;
+  return out;
+}
+
+// HashSpGEMMTopK (src/spgemm.cpp:708-842, src/spgemm_hash.cpp:168-318): the
+// binary pattern of A times its transpose gives |A_i n A_j| (sums of 1 in the
+// value type); per j != i, u = |A_i| + |A_j| - inter and jacc = u == 0 ? 0 :
+// 1 * inter / u (value type); per row, (jacc descending, column ascending),
+// the first top_k kept.  f32: the value type is float.
+}  // extern "C"
+
+template <typename V>
+static void* topk_impl(int64_t n, const int64_t* arp, const int64_t* aci, int64_t ncols, int64_t top_k) {
+  OrcCsr* out = new OrcCsr();
+  out->rows = n;
+  out->rp.assign((size_t)n + 1, 0);
+  // transpose of the pattern, rows of A^T in ascending original row
+  std::vector<int64_t> trp((size_t)ncols + 1, 0), tci((size_t)arp[n]);
+  for (int64_t e = 0; e < arp[n]; ++e) ++trp[(size_t)aci[e] + 1];
+  for (int64_t c = 0; c < ncols; ++c) trp[c + 1] += trp[c];
+  {
+    std::vector<int64_t> fill(trp.begin(), trp.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t e = arp[i]; e < arp[i + 1]; ++e) tci[(size_t)fill[aci[e]]++] = i;
+  }
+  std::map<int64_t, V> inter;
+  std::vector<std::pair<V, int64_t>> row;
+  for (int64_t i = 0; i < n; ++i) {
+    inter.clear();
+    for (int64_t e = arp[i]; e < arp[i + 1]; ++e) {
+      const int64_t c = aci[e];
+      for (int64_t f = trp[c]; f < trp[c + 1]; ++f) inter[tci[f]] += (V)1 * (V)1;
+    }
+    row.clear();
+    const int64_t li = arp[i + 1] - arp[i];
+    for (const auto& kv : inter) {
+      const int64_t j = kv.first;
+      if (j == i) continue;
+      const int64_t u = li + (arp[j + 1] - arp[j]) - (int64_t)kv.second;
+      const V jacc = u == 0 ? (V)0 : (V)1 * kv.second / (V)u;
+      row.push_back({jacc, j});
+    }
+    std::sort(row.begin(), row.end(), [](const std::pair<V, int64_t>& a, const std::pair<V, int64_t>& b) {
+      return a.first != b.first ? a.first > b.first : a.second < b.second;
+    });
+    const size_t keep = std::min<size_t>(row.size(), (size_t)std::max<int64_t>(top_k, 0));
+    for (size_t t = 0; t < keep; ++t) {
+      out->ci.push_back(row[t].second);
+      out->v.push_back((double)row[t].first);
+      out->absv.push_back((double)row[t].first);
+    }
+    out->rp[i + 1] = (int64_t)out->ci.size();
+  }
+  return out;
+}
+
+extern "C" {
+
+void* orc_spgemm_topk(int64_t n, const int64_t* arp, const int64_t* aci, int64_t ncols, int64_t top_k, int32_t f32) {
+  return f32 ? topk_impl<float>(n, arp, aci, ncols, top_k) : topk_impl<double>(n, arp, aci, ncols, top_k);
+}
+
 void orc_csr_info(void* h, int64_t* o) {
   OrcCsr* c = static_cast<OrcCsr*>(h);
   o[0] = c->rows; o[1] = c->rp.empty() ? 0 : c->rp.back(); o[2] = c->dense; o[3] = c->flops;

@@ -65,6 +65,13 @@ int64_t orc_hc(const int64_t* rp, const int64_t* ci, int64_t n, const int64_t* p
 void* orc_spgemm(int64_t a_rows, const int64_t* arp, const int64_t* aci, const double* av, int64_t b_rows,
                  int64_t b_cols, const int64_t* brp, const int64_t* bci, const double* bv, const int64_t* perm,
                  const int64_t* offsets, int64_t nclusters, int32_t sort_output, double l2_budget_bytes);
+/* Row-wise C = A*B (src/spgemm.cpp:44-235): every structural entry kept,
+ * columns ascending. */
+void* orc_spgemm_rowwise(int64_t a_rows, const int64_t* arp, const int64_t* aci, const double* av, int64_t b_rows,
+                         const int64_t* brp, const int64_t* bci, const double* bv);
+/* HashSpGEMMTopK (src/spgemm.cpp:708-842): top_k Jaccard-similar rows per
+ * row, (similarity descending, column ascending); f32: float arithmetic. */
+void* orc_spgemm_topk(int64_t n, const int64_t* arp, const int64_t* aci, int64_t ncols, int64_t top_k, int32_t f32);
 /* [rows, nnz, dense_clusters, flops] */
 void orc_csr_info(void* h, int64_t* out);
 void orc_csr_copy(void* h, int64_t* rp, int64_t* ci, double* v, double* absv);

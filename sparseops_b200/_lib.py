@@ -114,6 +114,8 @@ _SIGS = {
     "spops_pairs_destroy": [vp],
     "spops_hierarchical_clustering": [vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp],
     "spops_spgemm_clustered": [vp, vp, vp, vp, vp, i64, i32, dbl, vp, vp],
+    "spops_spgemm_rowwise": [vp, vp, vp, i32, i32, vp, vp],
+    "spops_spgemm_topk": [vp, vp, i64, vp],
     "spops_spgemm_lsh": [vp, vp, vp, i32, i32, u64, i64, i32, dbl, vp, vp],
     "spops_csr_spmv_noalloc": [i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, dbl, vp, dbl, vp, vp],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],

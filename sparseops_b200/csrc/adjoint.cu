@@ -223,6 +223,15 @@ spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const v
   return csr_spmv(ctx, A->tr.view, alpha, x, beta, y);
 }
 
+spops_status_t csr_transpose_view(Context* ctx, Matrix* A, Matrix** view) {
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "transpose needs a CSR matrix");
+  if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+  if (!A->tr.ready) SPOPS_TRY(SPOPS_DISPATCH2(A, build_transpose_t, ctx, A));
+  if (!A->tr.values_fresh) SPOPS_TRY(SPOPS_DISPATCH2(A, refresh_values_t, ctx, A));
+  *view = A->tr.view;
+  return SPOPS_OK;
+}
+
 spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out) {
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "SDDMM needs a CSR matrix");
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));

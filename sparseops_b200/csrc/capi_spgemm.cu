@@ -189,6 +189,28 @@ spops_status_t spops_spgemm_clustered(spops_context_t ctx, spops_matrix_t A, spo
   return SPOPS_OK;
 }
 
+spops_status_t spops_spgemm_rowwise(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B, int32_t kernel_flag,
+                                    int32_t sort_output, spops_matrix_t* C, spops_spgemm_stats_t* stats) {
+  if (!ctx || !A || !B || !C) return fail(SPOPS_ERR_INVALID, "spops_spgemm_rowwise: null argument");
+  (void)kernel_flag;  // kernels 1-3 give the same entries; columns always ascending here
+  DeviceGuard g(ctx->device);
+  SpgemmStats s;
+  Matrix* out = nullptr;
+  SPOPS_TRY(rowwise_spgemm(ctx, A, B, sort_output != 0, &out, &s));
+  *C = static_cast<spops_matrix_s*>(out);
+  put_stats(s, stats);
+  return SPOPS_OK;
+}
+
+spops_status_t spops_spgemm_topk(spops_context_t ctx, spops_matrix_t A, int64_t top_k, spops_matrix_t* C) {
+  if (!ctx || !A || !C) return fail(SPOPS_ERR_INVALID, "spops_spgemm_topk: null argument");
+  DeviceGuard g(ctx->device);
+  Matrix* out = nullptr;
+  SPOPS_TRY(topk_spgemm(ctx, A, top_k, &out));
+  *C = static_cast<spops_matrix_s*>(out);
+  return SPOPS_OK;
+}
+
 spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B, int32_t k, int32_t bands,
                                 uint64_t seed, int64_t cluster_size, int32_t sort_output, double l2_budget_bytes,
                                 spops_matrix_t* C, spops_spgemm_stats_t* stats) {

@@ -755,7 +755,7 @@ __global__ void classify_kernel(const int64_t* __restrict__ cptr, const int64_t*
 template <typename V>
 __global__ void row_count_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
                                  const int64_t* __restrict__ offsets, const int64_t* __restrict__ perm, int64_t ncl,
-                                 const V* __restrict__ cval, int64_t* __restrict__ rowcnt) {
+                                 const V* __restrict__ cval, bool keep_zeros, int64_t* __restrict__ rowcnt) {
   // warp per cluster, lanes over its rows (csz <= 32 common) and columns
   const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -764,7 +764,7 @@ __global__ void row_count_kernel(const int64_t* __restrict__ ccptr, const int64_
   const int64_t ncol = ccptr[c + 1] - ccptr[c];
   for (int64_t l = 0; l < csz; ++l) {
     int64_t cnt = 0;
-    for (int64_t p = lane; p < ncol; p += 32) cnt += cval[ccptr_val[c] + p * csz + l] != V(0) ? 1 : 0;
+    for (int64_t p = lane; p < ncol; p += 32) cnt += (keep_zeros || cval[ccptr_val[c] + p * csz + l] != V(0)) ? 1 : 0;
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
     if (lane == 0) rowcnt[perm[offsets[c] + l]] = cnt;
   }
@@ -773,7 +773,7 @@ __global__ void row_count_kernel(const int64_t* __restrict__ ccptr, const int64_
 template <typename I, typename V>
 __global__ void row_write_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
                                  const int64_t* __restrict__ offsets, const int64_t* __restrict__ perm, int64_t ncl,
-                                 const int32_t* __restrict__ ccol, const V* __restrict__ cval,
+                                 const int32_t* __restrict__ ccol, const V* __restrict__ cval, bool keep_zeros,
                                  const int64_t* __restrict__ crp, I* __restrict__ oci, V* __restrict__ ov) {
   const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -785,7 +785,7 @@ __global__ void row_write_kernel(const int64_t* __restrict__ ccptr, const int64_
     for (int64_t p0 = 0; p0 < ncol; p0 += 32) {
       const int64_t p = p0 + lane;
       const V v = p < ncol ? cval[ccptr_val[c] + p * csz + l] : V(0);
-      const bool keep = p < ncol && v != V(0);
+      const bool keep = p < ncol && (keep_zeros || v != V(0));
       const unsigned m = __ballot_sync(0xffffffffu, keep);
       if (keep) {
         const int64_t at = o + __popc(m & ((1u << lane) - 1));
@@ -953,9 +953,11 @@ struct Timer {
   }
 };
 
+// rowwise: the row-wise kernels' output rules (every structural entry kept,
+// exact zeros included; no small-value drop) instead of kernel 3's.
 template <typename I, typename V>
 spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_h, const int64_t* offs_h, int64_t ncl,
-                        bool sort_output, double l2_budget, Matrix** out, SpgemmStats* stats) {
+                        bool sort_output, double l2_budget, bool rowwise, Matrix** out, SpgemmStats* stats) {
   cudaStream_t st = ctx->stream;
   const int64_t n = A->rows, nnz = A->nnz;
   Timer tm;
@@ -1208,7 +1210,9 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(ndense.alloc(8));
   SPOPS_CUDA(cudaMemsetAsync(ndense.p, 0, 8, st));
   const double b_rowdense = (double)B->nnz / (double)std::max<int64_t>(B->rows, 1);
-  if (ncl > 0) {
+  if (rowwise) {
+    SPOPS_CUDA(cudaMemsetAsync(drop.p, 0, ncl1, st));
+  } else if (ncl > 0) {
     classify_kernel<<<grid_for(ncl), 256, 0, st>>>(cptr.as<int64_t>(), offs.as<int64_t>(), nzd.as<int64_t>(),
                                                    cmin.as<int64_t>(), cmax.as<int64_t>(), ncl, b_rowdense, l2_budget,
                                                    sort_output, sizeof(V), sizeof(int64_t), drop.as<unsigned char>(),
@@ -1307,7 +1311,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   if (ncl > 0) {
     row_count_kernel<V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
                                                             offs.as<int64_t>(), perm.as<int64_t>(), ncl, cval.as<V>(),
-                                                            rowcnt.as<int64_t>());
+                                                            rowwise, rowcnt.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
   }
   SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cb, rowcnt.as<int64_t>(), crp.as<int64_t>(), (int64_t)(n + 1), st));
@@ -1346,8 +1350,8 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   if (ncl > 0 && cnnz > 0) {
     row_write_kernel<I, V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
                                                                offs.as<int64_t>(), perm.as<int64_t>(), ncl,
-                                                               ccol.as<int32_t>(), cval.as<V>(), crp.as<int64_t>(),
-                                                               C->col.as<I>(), C->val.as<V>());
+                                                               ccol.as<int32_t>(), cval.as<V>(), rowwise,
+                                                               crp.as<int64_t>(), C->col.as<I>(), C->val.as<V>());
     SPOPS_LAUNCH_CHECK();
   }
   SPOPS_CUDA(cudaStreamSynchronize(st));
@@ -1367,7 +1371,8 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
 }  // namespace
 
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
-                              int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st) {
+                              int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st,
+                              bool rowwise) {
   if (A->format != SPOPS_FMT_CSR || B->format != SPOPS_FMT_CSR)
     return fail(SPOPS_ERR_INVALID, "SpGEMM needs CSR matrices");
   if (A->cols != B->rows) return fail(SPOPS_ERR_INVALID, "SpGEMM: A.cols (%lld) != B.rows (%lld)",
@@ -1389,10 +1394,10 @@ spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t*
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));  // validates patterns
   if (!B->plan.ready) SPOPS_TRY(csr_analyse(ctx, B));
   const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
-  if (i32 && f64) return spgemm_t<int32_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, C, st);
-  if (i32) return spgemm_t<int32_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, C, st);
-  if (f64) return spgemm_t<int64_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, C, st);
-  return spgemm_t<int64_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, C, st);
+  if (i32 && f64) return spgemm_t<int32_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
+  if (i32) return spgemm_t<int32_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
+  if (f64) return spgemm_t<int64_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
+  return spgemm_t<int64_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
 }
 
 }  // namespace spops

@@ -353,7 +353,13 @@ spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int
                                        const int64_t* pj, const double* ps, int64_t np, int64_t cluster_size,
                                        std::vector<int64_t>& perm, std::vector<int64_t>& offsets);
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
-                              int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st);
+                              int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st,
+                              bool rowwise = false);
+// spgemm_topk.cu
+spops_status_t rowwise_spgemm(Context* ctx, Matrix* A, Matrix* B, bool sort_output, Matrix** C, SpgemmStats* st);
+spops_status_t topk_spgemm(Context* ctx, Matrix* A, int64_t top_k, Matrix** C);
+// adjoint.cu: A^T as a CSR handle owned by A (built once, values refreshed)
+spops_status_t csr_transpose_view(Context* ctx, Matrix* A, Matrix** view);
 // batched.cu
 spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k, double beta,
                         void* Y, int64_t ldy);

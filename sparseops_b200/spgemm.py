@@ -8,6 +8,8 @@ src/spgemm.cpp):
     hierarchical_clustering_v0_fast(rp, ci, n, pairs, cs)    host, bit-identical
     LeSpGEMM_clustered(A, B, perm, offsets, ...)             device (kernel-3 rules)
     LeSpGEMM_lsh(A, B, k, bands, seed, cluster_size, ...)    the whole pipeline
+    LeSpGEMM(A, B, kernel_flag, sort_output)                 device, row-wise kernels 1-3
+    HashSpGEMMTopK(A, top_k)                                 device, top-k Jaccard rows
 
 Results of the SpGEMM are CSR matrices in A's original row order with
 ascending columns (``SpGEMMResult``), kept on the device; host copies are
@@ -132,3 +134,28 @@ def LeSpGEMM_lsh(A: CSR_Matrix, B: CSR_Matrix, k: int = 64, num_bands: int = 16,
          i32(1 if sort_output else 0), dbl(l2_budget), C.byref(out), C.byref(st))
     it, vt = _types(A)
     return SpGEMMResult(_Handle(ctx, out), A.num_rows, B.num_cols, it, vt, st.as_dict())
+
+
+def LeSpGEMM(A: CSR_Matrix, B: CSR_Matrix, kernel_flag: int = 1, sort_output: bool = False) -> SpGEMMResult:
+    """Row-wise C = A*B (src/spgemm.cpp:683): every structural entry kept,
+    exact zeros included; columns ascending in every row (kernels 1-3 give
+    the same entries; ascending order is valid for all of them)."""
+    ha, hb = A.device(), B.device()
+    ctx = ha.ctx.follow_torch()
+    out = vp()
+    st = SpgemmStats()
+    call("spops_spgemm_rowwise", ctx.handle, ha.handle, hb.handle, i32(kernel_flag), i32(1 if sort_output else 0),
+         C.byref(out), C.byref(st))
+    it, vt = _types(A)
+    return SpGEMMResult(_Handle(ctx, out), A.num_rows, B.num_cols, it, vt, st.as_dict())
+
+
+def HashSpGEMMTopK(A: CSR_Matrix, top_k: int) -> DeviceCSR:
+    """For every row, the top_k most Jaccard-similar other rows of A (by
+    similarity descending, then column ascending), as values
+    (src/spgemm.cpp:708)."""
+    ha = A.device()
+    ctx = ha.ctx.follow_torch()
+    out = vp()
+    call("spops_spgemm_topk", ctx.handle, ha.handle, i64(top_k), C.byref(out))
+    return DeviceCSR(_Handle(ctx, out), A.num_rows, A.num_rows)

@@ -116,6 +116,13 @@ def main():
         cci, cv = sort_rows(c["rp"], c["ci"], c["v"])
         g[f"sp_c{so}_rp"], g[f"sp_c{so}_ci"], g[f"sp_c{so}_v"] = c["rp"], cci, cv
         g[f"sp_c{so}_dense"] = np.int64(c["dense_clusters"])
+    # row-wise LeSpGEMM (kernels 1-3, sorted) and HashSpGEMMTopK on the same matrix
+    for kf in (1, 2, 3):
+        c = R.spgemm_rowwise((arp, aci, av), (brp, bci, bv, 1024), kf, True)
+        g[f"rw{kf}_rp"], g[f"rw{kf}_ci"], g[f"rw{kf}_v"] = c["rp"], c["ci"], c["v"]
+    for f32 in (0, 1):
+        c = R.spgemm_topk(arp, aci, 1024, 6, bool(f32))
+        g[f"topk{f32}_rp"], g[f"topk{f32}_ci"], g[f"topk{f32}_v"] = c["rp"], c["ci"], c["v"]
     # a bucket larger than 256 rows (window rule): 400 identical rows
     rp2 = np.arange(0, 401 * 3, 3, dtype=np.int64)
     ci2 = np.tile(np.array([5, 17, 99], np.int64), 400)

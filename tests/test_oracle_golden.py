@@ -133,3 +133,26 @@ def test_features_golden(golden, orc, k):
     both_nan = np.isnan(got) & np.isnan(ref)
     rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
     assert np.all(both_nan | (rel <= 1e-12) | (got == ref))
+
+
+@pytest.mark.parametrize("kf", [1, 2, 3])
+def test_spgemm_rowwise_golden(golden, orc, kf):
+    """Row-wise LeSpGEMM (src/spgemm.cpp:683): the restatement keeps every
+    structural entry; the reference's kernels 2/3 add in another order."""
+    g = golden
+    from sparseops_b200 import synth
+    arp, aci, av = g["sp_arp"], g["sp_aci"], g["sp_av"]
+    brp, bci, bv = synth.transpose(arp, aci, av, 1024)
+    c = orc.spgemm_rowwise((arp, aci, av), (brp, bci, bv))
+    assert np.array_equal(c["rp"], g[f"rw{kf}_rp"]) and np.array_equal(c["ci"], g[f"rw{kf}_ci"])
+    err = np.abs(c["v"] - g[f"rw{kf}_v"]) / np.maximum(c["absv"], 1e-300)
+    assert err.max() <= 1e-12
+
+
+@pytest.mark.parametrize("f32", [0, 1])
+def test_spgemm_topk_golden(golden, orc, f32):
+    """HashSpGEMMTopK (src/spgemm.cpp:708): columns, order and values exact."""
+    g = golden
+    c = orc.spgemm_topk(g["sp_arp"], g["sp_aci"], 1024, 6, bool(f32))
+    for key in ("rp", "ci", "v"):
+        assert np.array_equal(c[key], g[f"topk{f32}_{key}"]), key

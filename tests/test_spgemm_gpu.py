@@ -138,3 +138,64 @@ def test_full_config_properties(cuda):
     SpOps_csr(1.0, Ad, tt, 0.0, scale)
     torch.cuda.synchronize()
     assert float(((y1 - y2).abs() / (scale + 1e-300)).max()) <= 1e-12
+
+
+@pytest.mark.parametrize("itype", [np.int32, np.int64])
+def test_rowwise_golden(cuda, golden, orc, itype):
+    """Row-wise LeSpGEMM kernels 1-3 against the reference's sorted output."""
+    from sparseops_b200.spgemm import LeSpGEMM
+    g = golden
+    arp, aci, av = g["sp_arp"], g["sp_aci"], g["sp_av"]
+    brp, bci, bv = synth.transpose(arp, aci, av, 1024)
+    ref = orc.spgemm_rowwise((arp, aci, av), (brp, bci, bv))
+    A = _csr(arp.astype(itype), aci.astype(itype), av)
+    B = _csr(brp.astype(itype), bci.astype(itype), bv)
+    for kf in (1, 2, 3):
+        for so in (False, True):
+            C = LeSpGEMM(A, B, kf, so)
+            rp, ci, v = C.host()
+            assert np.array_equal(rp.astype(np.int64), g[f"rw{kf}_rp"])
+            assert np.array_equal(ci.astype(np.int64), g[f"rw{kf}_ci"])
+            err = np.abs(v - g[f"rw{kf}_v"]) / np.maximum(ref["absv"], 1e-300)
+            assert err.max() <= 1e-12
+
+
+def test_rowwise_keeps_exact_zeros(cuda, orc):
+    """Products that cancel exactly stay in C as zeros (the reference keeps
+    every structural entry of the symbolic phase)."""
+    from sparseops_b200.spgemm import LeSpGEMM
+    arp = np.array([0, 2, 3], np.int64)
+    aci = np.array([0, 1, 1], np.int64)
+    av = np.array([1.0, -1.0, 2.0])
+    brp = np.array([0, 1, 2], np.int64)
+    bci = np.array([0, 0], np.int64)
+    bv = np.array([3.0, 3.0])
+    rp, ci, v = LeSpGEMM(_csr(arp, aci, av), _csr(brp, bci, bv), 1, True).host()
+    assert list(rp) == [0, 1, 2] and list(ci) == [0, 0] and list(v) == [0.0, 6.0]
+    ref = orc.spgemm_rowwise((arp, aci, av), (brp, bci, bv))
+    assert np.array_equal(ref["rp"], rp) and np.array_equal(ref["v"], v)
+
+
+@pytest.mark.parametrize("f32", [0, 1])
+@pytest.mark.parametrize("itype", [np.int32, np.int64])
+def test_topk_golden(cuda, golden, f32, itype):
+    from sparseops_b200.spgemm import HashSpGEMMTopK
+    g = golden
+    vt = np.float32 if f32 else np.float64
+    A = _csr(g["sp_arp"].astype(itype), g["sp_aci"].astype(itype), g["sp_av"].astype(vt))
+    rp, ci, v = HashSpGEMMTopK(A, 6).host()
+    assert np.array_equal(rp.astype(np.int64), g[f"topk{f32}_rp"])
+    assert np.array_equal(ci.astype(np.int64), g[f"topk{f32}_ci"])
+    assert np.array_equal(v.astype(np.float64), g[f"topk{f32}_v"])
+
+
+@pytest.mark.parametrize("k", [0, 1, 40])
+def test_topk_vs_oracle(cuda, orc, k):
+    """A larger planted matrix; k = 0 keeps nothing, k = 40 exceeds many rows."""
+    from sparseops_b200.spgemm import HashSpGEMMTopK
+    arp, aci, av = synth.planted_communities(20000, ncomm=128, mean=14.0, seed=29)
+    ref = orc.spgemm_topk(arp, aci, 20000, k)
+    rp, ci, v = HashSpGEMMTopK(_csr(arp, aci, av), k).host()
+    assert np.array_equal(rp.astype(np.int64), ref["rp"])
+    assert np.array_equal(ci.astype(np.int64), ref["ci"])
+    assert np.array_equal(v, ref["v"])
