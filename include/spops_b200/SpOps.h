@@ -12,6 +12,8 @@
  *   delete_host_matrix(...)
  *   minhash_signatures_flat, lsh_candidate_pairs_vector,
  *   hierarchical_clustering_v0_fast                                   LeSpGEMM preprocessing
+ *   LeSpGEMM<sortOutput>(A, B, C, kernel_flag), HashSpGEMMTopK(A, C, top_k)
+ *                                                                     row-wise SpGEMM (include/spgemm.h)
  *
  * What differs, and why:
  *   - Work runs on the GPU.  The first SpOps call on a matrix uploads it and
@@ -997,6 +999,51 @@ inline void hierarchical_clustering_v0_fast(const IndexType* rowptr, const Index
            "spops_hierarchical_clustering");
   permutation_out.assign(perm.begin(), perm.end());
   offsets_out.assign(offs.begin(), offs.begin() + ncl + 1);
+}
+
+/* ---------------------------------------------------- row-wise SpGEMM */
+namespace spops_b200 {
+namespace detail {
+// a device result handle into a host CSR struct (arrays from posix_memalign)
+template <typename I, typename V>
+inline void take_csr(spops_matrix_t h, CSR_Matrix<I, V>& C) {
+  const spops_matrix_info_t i = info(h);
+  set_features<I, V>(C, i.rows, i.cols, i.nnz);
+  C.row_offset = fetch<I>(h, SPOPS_ARR_ROW, nullptr);
+  C.col_index = fetch<I>(h, SPOPS_ARR_COL, nullptr);
+  C.values = fetch<V>(h, SPOPS_ARR_VAL, nullptr);
+  spops_matrix_destroy(h);
+}
+}  // namespace detail
+}  // namespace spops_b200
+
+/* C = A * B row by row (include/spgemm.h:29, src/spgemm.cpp:683): every
+ * structural entry kept, columns ascending; kernel_flag is recorded in C. */
+template <bool sortOutput, typename IndexType, typename ValueType>
+void LeSpGEMM(const CSR_Matrix<IndexType, ValueType>& A, const CSR_Matrix<IndexType, ValueType>& B,
+              CSR_Matrix<IndexType, ValueType>& C, int kernel_flag) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t a = d::upload_csr(A), b = d::upload_csr(B), c = nullptr;
+  spops_status_t s = spops_spgemm_rowwise(d::ctx(), a, b, kernel_flag, sortOutput ? 1 : 0, &c, nullptr);
+  spops_matrix_destroy(a);
+  spops_matrix_destroy(b);
+  d::check(s, "spops_spgemm_rowwise");
+  d::take_csr<IndexType, ValueType>(c, C);
+  C.kernel_flag = kernel_flag;
+}
+
+/* Top-k Jaccard similarities of A's rows (src/spgemm.cpp:708): per row, the
+ * top_k other rows by similarity descending, then column ascending. */
+template <typename IndexType, typename ValueType>
+void HashSpGEMMTopK(const CSR_Matrix<IndexType, ValueType>& A, CSR_Matrix<IndexType, ValueType>& C,
+                    IndexType top_k) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t a = d::upload_csr(A), c = nullptr;
+  spops_status_t s = spops_spgemm_topk(d::ctx(), a, (int64_t)top_k, &c);
+  spops_matrix_destroy(a);
+  d::check(s, "spops_spgemm_topk");
+  d::take_csr<IndexType, ValueType>(c, C);
+  C.kernel_flag = 0;
 }
 
 #endif /* SPOPS_B200_CXX_SPOPS_H */

@@ -241,6 +241,66 @@ void lsh_checks() {
   EXPECT(grouped, "clusters inside groups");
 }
 
+// Row-wise SpGEMM and top-k against a direct host product on a small matrix.
+void spgemm_checks() {
+  // A: 6 x 5; B = A^T (5 x 6)
+  std::vector<long long> rp = {0, 2, 4, 5, 8, 8, 10}, ci = {0, 3, 1, 3, 2, 0, 1, 4, 3, 4};
+  std::vector<double> v = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
+  CSR_Matrix<long long, double> A{};
+  A.num_rows = 6;
+  A.num_cols = 5;
+  A.num_nnzs = 10;
+  A.row_offset = rp.data();
+  A.col_index = ci.data();
+  A.values = v.data();
+  std::vector<double> dense(30, 0.0);
+  for (long long r = 0; r < 6; ++r)
+    for (long long e = rp[r]; e < rp[r + 1]; ++e) dense[(size_t)(r * 5 + ci[e])] = v[e];
+  std::vector<long long> trp(6, 0), tci;
+  std::vector<double> tv;
+  for (long long c = 0; c < 5; ++c) {
+    for (long long r = 0; r < 6; ++r)
+      if (dense[(size_t)(r * 5 + c)] != 0.0) {
+        tci.push_back(r);
+        tv.push_back(dense[(size_t)(r * 5 + c)]);
+      }
+    trp[(size_t)c + 1] = (long long)tci.size();
+  }
+  CSR_Matrix<long long, double> B{};
+  B.num_rows = 5;
+  B.num_cols = 6;
+  B.num_nnzs = (long long)tci.size();
+  B.row_offset = trp.data();
+  B.col_index = tci.data();
+  B.values = tv.data();
+  CSR_Matrix<long long, double> C{};
+  LeSpGEMM<true, long long, double>(A, B, C, 2);
+  EXPECT(C.num_rows == 6 && C.num_cols == 6 && C.kernel_flag == 2, "LeSpGEMM shape");
+  bool ok = true;
+  for (long long i = 0; i < 6; ++i)
+    for (long long e = C.row_offset[i]; e < C.row_offset[i + 1]; ++e) {
+      double s = 0;
+      for (long long k = 0; k < 5; ++k) s += dense[(size_t)(i * 5 + k)] * dense[(size_t)(C.col_index[e] * 5 + k)];
+      ok = ok && std::fabs(s - C.values[e]) <= 1e-12 * std::fabs(s) && s != 0.0;
+      if (e > C.row_offset[i]) ok = ok && C.col_index[e] > C.col_index[e - 1];
+    }
+  EXPECT(ok, "LeSpGEMM values and ascending columns");
+  EXPECT(C.row_offset[5] == C.row_offset[4], "empty row stays empty");
+  delete_host_matrix(C);
+  CSR_Matrix<long long, double> T{};
+  HashSpGEMMTopK<long long, double>(A, T, 2LL);
+  bool topk = T.num_rows == 6;
+  for (long long i = 0; i < 6 && topk; ++i) {
+    topk = T.row_offset[i + 1] - T.row_offset[i] <= 2;
+    for (long long e = T.row_offset[i]; e < T.row_offset[i + 1]; ++e) {
+      topk = topk && T.col_index[e] != i && T.values[e] > 0.0 && T.values[e] <= 1.0;
+      if (e > T.row_offset[i]) topk = topk && T.values[e] <= T.values[e - 1];
+    }
+  }
+  EXPECT(topk, "HashSpGEMMTopK rows: at most k, no diagonal, similarity descending");
+  delete_host_matrix(T);
+}
+
 int main() {
   std::setvbuf(stdout, nullptr, _IONBF, 0);
   try {
@@ -248,6 +308,7 @@ int main() {
     run_all<int, float>();
     run_all<long long, double>();
     lsh_checks();
+    spgemm_checks();
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
     return 2;
