@@ -192,6 +192,24 @@ def cpu_reference_sample(rp, ci, v, x, budget_s=10.0, threads=None):
 # launches, fwd+bwd SpMV against a path that rebuilds the transpose, and the
 # LeSpGEMM pipeline on the planted-community matrix.
 
+def _host_ms(fn, reps, warm=1):
+    """Median wall ms of calls that return after their device work (the
+    SpGEMM entry points synchronise); the result of each call is released
+    before the next one."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        ts.append((time.perf_counter() - t0) * 1e3)
+        del r
+    return float(np.median(ts))
+
+
 def _ev_ms(fn, reps, warm=3):
     import torch
     for _ in range(warm):
@@ -436,14 +454,8 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
     brp, bci, bv = synth.transpose(arp, aci, av, n)
     A = CSR_Matrix(n, n, torch.from_numpy(arp).to(dev), torch.from_numpy(aci).to(dev), torch.from_numpy(av).to(dev))
     B = CSR_Matrix(n, n, torch.from_numpy(brp).to(dev), torch.from_numpy(bci).to(dev), torch.from_numpy(bv).to(dev))
-    C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)  # warm-up
-    torch.cuda.synchronize()
-    reps = 3
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
-    torch.cuda.synchronize()
-    total = (time.perf_counter() - t0) * 1e3 / reps
+    total = _host_ms(lambda: LeSpGEMM_lsh(A, B, 64, 16, 7, 8), 5, warm=2)
+    C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
     st = C.stats
     flops = st["flops"]
     out = {"rows": n, "nnz_A": int(len(aci)), "nnz_C": int(C.num_nnzs), "flops": int(flops),
@@ -454,9 +466,16 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
     from sparseops_b200.spgemm import hierarchical_clustering_v0_fast, lsh_candidate_pairs_vector
     pairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
     perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
-    kms = _ev_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 3, warm=1)
+    kms = _host_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 5, warm=2)
     out["spgemm_clustered_ms"] = round(kms, 3)
     out["spgemm_clustered_GFLOP/s"] = round(flops / kms / 1e6, 2)
+    # row-wise LeSpGEMM (kernel 1 entries) and the top-16 Jaccard rows of A
+    from sparseops_b200.spgemm import HashSpGEMMTopK, LeSpGEMM
+    rms = _host_ms(lambda: LeSpGEMM(A, B, 1, False), 3, warm=1)
+    out["rowwise_ms"] = round(rms, 3)
+    out["rowwise_GFLOP/s"] = round(flops / rms / 1e6, 2)
+    tms = _host_ms(lambda: HashSpGEMMTopK(A, 16), 3, warm=1)
+    out["topk16_ms"] = round(tms, 3)
     if cpu_ref:
         try:
             from oracle import Reference, reference_available
@@ -465,6 +484,13 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
                 ms = R.spgemm_kernel3_time((arp, aci, av), (brp, bci, bv), perm, offs, iters=2)
                 out["cpu_reference_kernel3"] = {"ms": round(ms, 2), "GFLOP/s": round(flops / ms / 1e6, 2),
                                                 "cores": os.cpu_count(), "kind": "reference"}
+                A64 = (arp.astype(np.int64), aci.astype(np.int64), av)
+                B64 = (brp.astype(np.int64), bci.astype(np.int64), bv)
+                ms = R.spgemm_rowwise_time(A64, B64, 1, -1, iters=1)
+                out["cpu_reference_rowwise_kernel1"] = {"ms": round(ms, 2), "cores": os.cpu_count(),
+                                                        "kind": "reference"}
+                ms = R.spgemm_rowwise_time(A64, B64, 1, 16, iters=1)
+                out["cpu_reference_topk16"] = {"ms": round(ms, 2), "cores": os.cpu_count(), "kind": "reference"}
         except Exception as e:
             out["cpu_reference_kernel3"] = {"error": str(e)[:160]}
     return out

@@ -360,6 +360,19 @@ class Reference:
                                    C.c_int(1 if f32 else 0))
         return self._ref_csr(h)
 
+    def spgemm_rowwise_time(self, A, B, kernel_flag=1, top_k=-1, iters=1):
+        """Mean ms of the reference's LeSpGEMM<false>(A, B, C, kernel_flag), or
+        of HashSpGEMMTopK(A, C, top_k) when top_k >= 0."""
+        arp, aci, av = A
+        brp, bci, bv = B[:3]
+        n = len(arp) - 1
+        bcols = int(B[3]) if len(B) > 3 else n
+        self.L.ref_spgemm_rowwise_time.restype = C.c_double
+        return float(self.L.ref_spgemm_rowwise_time(
+            _i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av), _i64(len(brp) - 1),
+            _i64(bcols), _i64(len(bci)), _p(brp), _p(bci), _p(bv), C.c_int(int(kernel_flag)), _i64(top_k),
+            C.c_int(int(iters))))
+
     def spgemm_kernel3_time(self, A, B, perm, offsets, iters=3, l2_fraction=-1.0):
         """Mean ms of the reference's LeSpGEMM_VLength kernel 3 (numeric and
         symbolic phases on the clustered A) over `iters` runs."""

@@ -22,6 +22,7 @@
 #include "spgemm_utility.h"
 
 #include <cstdint>
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -486,6 +487,30 @@ void* ref_spgemm_topk(ll nr, ll nc, ll nnz, const ll* rp, const ll* ci, ll top_k
     HashSpGEMMTopK<int64_t, double>(A, h->C, (int64_t)top_k);
   }
   return h;
+}
+
+// Mean ms over `iters` calls of LeSpGEMM<false, int64_t, double>(A, B, C,
+// kernel_flag), or of HashSpGEMMTopK<int64_t, double>(A, C, top_k) when
+// top_k >= 0 (B unused); the output is freed outside the timed region.
+double ref_spgemm_rowwise_time(ll a_rows, ll a_cols, ll a_nnz, const ll* arp, const ll* aci, const double* av,
+                               ll b_rows, ll b_cols, ll b_nnz, const ll* brp, const ll* bci, const double* bv,
+                               int kernel_flag, ll top_k, int iters) {
+  CSR_Matrix<int64_t, double> A = wrap_csr<int64_t, double>(a_rows, a_cols, a_nnz, (const int64_t*)arp,
+                                                            (const int64_t*)aci, av, 0);
+  CSR_Matrix<int64_t, double> B = wrap_csr<int64_t, double>(b_rows, b_cols, b_nnz, (const int64_t*)brp,
+                                                            (const int64_t*)bci, bv, 0);
+  double total = 0;
+  for (int it = 0; it < iters; ++it) {
+    CSR_Matrix<int64_t, double> C{};
+    auto t0 = std::chrono::steady_clock::now();
+    if (top_k >= 0)
+      HashSpGEMMTopK<int64_t, double>(A, C, (int64_t)top_k);
+    else
+      LeSpGEMM<false, int64_t, double>(A, B, C, kernel_flag);
+    total += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    delete_host_matrix(C);
+  }
+  return iters > 0 ? total / iters : 0.0;
 }
 
 }  // extern "C"
