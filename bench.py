@@ -496,6 +496,70 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
     return out
 
 
+def _mtx_parse_csr(text: bytes):
+    """spops_mtx_parse_csr on a file's bytes in host memory (int32, FP64)."""
+    import ctypes as C
+    from sparseops_b200._lib import call
+    from sparseops_b200.formats import _Handle, default_context
+    ctx = default_context()
+    out = C.c_void_p()
+    call("spops_mtx_parse_csr", ctx.handle, text, C.c_int64(len(text)), C.c_int(0), C.c_int(1), C.c_int32(0),
+         C.byref(out))
+    return _Handle(ctx, out)
+
+
+def bench_mtx(cpu_ref: bool):
+    """Matrix Market files read into CSR: the 512 x 512 Laplacian (diagonal 4,
+    off-diagonals -1, as the reference's benchmark writes it) and 2M entries of
+    17-digit random values; ours (host read, device parse, device coo_to_csr)
+    against the reference's read_csr_matrix on the host."""
+    import tempfile
+    from sparseops_b200 import read_csr_matrix, synth
+    out = {}
+    rng = np.random.default_rng(11)
+    rp, ci, v = synth.laplacian_2d(512)
+    rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp)) + 1
+    n2, m2 = 1 << 20, 2_000_000
+    cases = {
+        "laplacian_512": ("%%%%MatrixMarket matrix coordinate real general\n%d %d %d\n" % (len(rp) - 1, len(rp) - 1,
+                                                                                           len(ci)),
+                          rows, ci + 1, v, "%d %d %.17g"),
+        "random_2M_17digits": ("%%%%MatrixMarket matrix coordinate real general\n%d %d %d\n" % (n2, n2, m2),
+                               rng.integers(1, n2 + 1, m2), rng.integers(1, n2 + 1, m2),
+                               rng.standard_normal(m2) * 10.0 ** rng.integers(-20, 20, m2), "%d %d %.17g"),
+    }
+    with tempfile.TemporaryDirectory() as d:
+        for name, (head, r, c, x, fmt) in cases.items():
+            path = os.path.join(d, name + ".mtx")
+            with open(path, "w") as f:
+                f.write(head)
+                np.savetxt(f, np.column_stack([r, c, x]), fmt=fmt)
+            size = os.path.getsize(path)
+            ms = _host_ms(lambda: read_csr_matrix(path, False, np.int32, np.float64), 5, warm=1)
+            with open(path, "rb") as f:
+                text = f.read()
+            # the same file already in host memory: upload, parse and coo_to_csr only
+            pms = _host_ms(lambda: _mtx_parse_csr(text), 5, warm=1)
+            res = {"bytes": size, "entries": int(len(x)), "ms": round(ms, 2), "MB/s": round(size / ms / 1e3, 1),
+                   "from_memory_ms": round(pms, 2), "from_memory_MB/s": round(size / pms / 1e3, 1)}
+            if cpu_ref:
+                try:
+                    from oracle import Reference, reference_available
+                    if reference_available():
+                        R = Reference(threads=1)
+                        t0 = time.perf_counter()
+                        R.read_csr(path, compact=False)
+                        rms = (time.perf_counter() - t0) * 1e3
+                        res["cpu_reference_ms"] = round(rms, 1)
+                        res["cpu_reference_MB/s"] = round(size / rms / 1e3, 1)
+                        res["cpu_reference"] = {"kind": "reference", "cores": 1,
+                                                "note": "read_csr_matrix: fscanf per entry, then coo_to_csr"}
+                except Exception as e:
+                    res["cpu_reference_error"] = str(e)[:160]
+            out[name] = res
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -560,6 +624,8 @@ def run_section(args):
         res = bench_batched(ctx, dev)
     elif args.section == "fwd_bwd":
         res = bench_fwd_bwd(ctx, dev)
+    elif args.section == "mtx":
+        res = bench_mtx(not args.no_cpu_baseline)
     elif args.section == "spgemm":
         res = bench_spgemm(dev, not args.no_cpu_baseline)
     else:
@@ -671,7 +737,8 @@ def run_ours(args):
         for key, fn in (("formats", lambda: bench_formats(A, ctx, xd, yd, n, nnz, nbytes, peak, dev)),
                         ("batched", lambda: bench_batched(ctx, dev)),
                         ("fwd_bwd", lambda: bench_fwd_bwd(ctx, dev)),
-                        ("spgemm", lambda: bench_spgemm(dev, not args.no_cpu_baseline))):
+                        ("spgemm", lambda: bench_spgemm(dev, not args.no_cpu_baseline)),
+                        ("mtx", lambda: bench_mtx(not args.no_cpu_baseline))):
             t0 = time.time()
             try:
                 extra[key] = fn()
@@ -719,7 +786,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
-    ap.add_argument("--section", default="all", choices=["all", "batched", "fwd_bwd", "spgemm"],
+    ap.add_argument("--section", default="all", choices=["all", "batched", "fwd_bwd", "spgemm", "mtx"],
                     help="run one extra section alone (profiling); the headline line needs 'all'")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-format, batched, fwd+bwd and SpGEMM sections")

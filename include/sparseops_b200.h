@@ -138,6 +138,26 @@ spops_status_t spops_csr_create(spops_context_t ctx, spops_matrix_t* A, int64_t 
 spops_status_t spops_coo_create(spops_context_t ctx, spops_matrix_t* A, int64_t rows, int64_t cols, int64_t nnz,
                                 const void* row_index, const void* col_index, const void* values,
                                 spops_index_t itype, spops_value_t vtype, spops_mem_t mem);
+/* Matrix Market text parsed on the device.  Replaces read_coo_matrix and
+ * read_csr_matrix (utils/sparse_io.cpp:26-214; banner and size line as
+ * mm_read_banner / mm_read_mtx_crd_size, utils/mmio.cpp:144-283): sparse
+ * real, integer or pattern coordinate files; "symmetric" files expanded with
+ * each off-diagonal entry followed by its mirror; values converted as
+ * scanf("%lf") does (correctly rounded decimal to double) and then cast to
+ * vtype; indices 1-based in the file.  _read_ take a file path (read on the
+ * host, parsed on the device), _parse_ the file's bytes in host memory.  The
+ * COO handle keeps the file's entry order; the CSR handle is coo_to_csr's
+ * (compact: duplicates summed).  A file with zero rows gives a 0 x 0 matrix.
+ * Malformed numbers, indices outside the size line and fewer entries than it
+ * announces are refused with SPOPS_ERR_INVALID (the reference asserts). */
+spops_status_t spops_mtx_read_coo(spops_context_t ctx, const char* path, spops_index_t itype, spops_value_t vtype,
+                                  spops_matrix_t* coo);
+spops_status_t spops_mtx_parse_coo(spops_context_t ctx, const char* text, int64_t len, spops_index_t itype,
+                                   spops_value_t vtype, spops_matrix_t* coo);
+spops_status_t spops_mtx_read_csr(spops_context_t ctx, const char* path, spops_index_t itype, spops_value_t vtype,
+                                  int32_t compact, spops_matrix_t* csr);
+spops_status_t spops_mtx_parse_csr(spops_context_t ctx, const char* text, int64_t len, spops_index_t itype,
+                                   spops_value_t vtype, int32_t compact, spops_matrix_t* csr);
 /* CSR handle (owned arrays) from a COO handle, on the device.  Replaces
  * coo_to_csr (include/sparse_conversion.h:37-99): rows in order, file order
  * kept within a row.  compact != 0 adds the reference's sum_csr_duplicates

@@ -12,6 +12,7 @@
  *   delete_host_matrix(...)
  *   minhash_signatures_flat, lsh_candidate_pairs_vector,
  *   hierarchical_clustering_v0_fast                                   LeSpGEMM preprocessing
+ *   read_coo_matrix, read_csr_matrix                                  Matrix Market files
  *   LeSpGEMM<sortOutput>(A, B, C, kernel_flag), HashSpGEMMTopK(A, C, top_k)
  *                                                                     row-wise SpGEMM (include/spgemm.h)
  *
@@ -999,6 +1000,43 @@ inline void hierarchical_clustering_v0_fast(const IndexType* rowptr, const Index
            "spops_hierarchical_clustering");
   permutation_out.assign(perm.begin(), perm.end());
   offsets_out.assign(offs.begin(), offs.begin() + ncl + 1);
+}
+
+/* ------------------------------------------------- Matrix Market files */
+/* include/sparse_io.h:40 / :52: the file is read on the host and parsed on
+ * the device (values as scanf("%lf") converts them); host structs out.  A
+ * malformed file throws where the reference asserts or exits. */
+template <class IndexType, class ValueType>
+COO_Matrix<IndexType, ValueType> read_coo_matrix(const char* mm_filename) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = nullptr;
+  d::check(spops_mtx_read_coo(d::ctx(), mm_filename, d::itype<IndexType>(), d::vtype<ValueType>(), &h),
+           "spops_mtx_read_coo");
+  const spops_matrix_info_t i = d::info(h);
+  COO_Matrix<IndexType, ValueType> coo;
+  d::set_features<IndexType, ValueType>(coo, i.rows, i.cols, i.nnz);
+  coo.row_index = d::fetch<IndexType>(h, SPOPS_ARR_ROW, nullptr);
+  coo.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
+  coo.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  spops_matrix_destroy(h);
+  return coo;
+}
+
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> read_csr_matrix(const char* mm_filename, bool compact = false) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t h = nullptr;
+  d::check(spops_mtx_read_csr(d::ctx(), mm_filename, d::itype<IndexType>(), d::vtype<ValueType>(), compact ? 1 : 0,
+                              &h),
+           "spops_mtx_read_csr");
+  const spops_matrix_info_t i = d::info(h);
+  CSR_Matrix<IndexType, ValueType> csr;
+  d::set_features<IndexType, ValueType>(csr, i.rows, i.cols, i.nnz);
+  csr.row_offset = d::fetch<IndexType>(h, SPOPS_ARR_ROW, nullptr);
+  csr.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
+  csr.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
+  if (d::caching()) d::put(csr.row_offset, h, i.rows, i.cols, i.nnz); else spops_matrix_destroy(h);
+  return csr;
 }
 
 /* ---------------------------------------------------- row-wise SpGEMM */

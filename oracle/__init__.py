@@ -360,6 +360,12 @@ class Reference:
                                    C.c_int(1 if f32 else 0))
         return self._ref_csr(h)
 
+    def read_csr(self, path, compact=False, f32=False):
+        """The reference's read_csr_matrix<long long, V>(path, compact)."""
+        self.L.ref_read_csr.restype = _vp
+        h = self.L.ref_read_csr(str(path).encode(), C.c_int(int(compact)), C.c_int(int(f32)))
+        return self._ref_csr(h)
+
     def spgemm_rowwise_time(self, A, B, kernel_flag=1, top_k=-1, iters=1):
         """Mean ms of the reference's LeSpGEMM<false>(A, B, C, kernel_flag), or
         of HashSpGEMMTopK(A, C, top_k) when top_k >= 0."""

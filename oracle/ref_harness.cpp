@@ -441,6 +441,43 @@ void* ref_csr_transpose(ll nr, ll nc, ll nnz, const ll* rp, const ll* ci, const 
   return h;
 }
 
+// ------------------------------------------------------- Matrix Market
+// read_csr_matrix<long long, V>(path, compact) (utils/sparse_io.cpp:193), float
+// values widened to double in the handle.
+void* ref_read_csr(const char* path, int compact, int f32) {
+  CsrHandle* h = new CsrHandle();
+  if (f32) {
+    CSR_Matrix<long long, float> C = read_csr_matrix<long long, float>(path, compact != 0);
+    h->C.num_rows = C.num_rows;
+    h->C.num_cols = C.num_cols;
+    h->C.num_nnzs = C.num_nnzs;
+    h->C.row_offset = new_array<int64_t>(C.num_rows + 1);
+    h->C.col_index = new_array<int64_t>(C.num_nnzs > 0 ? C.num_nnzs : 1);
+    h->C.values = new_array<double>(C.num_nnzs > 0 ? C.num_nnzs : 1);
+    for (ll t = 0; t <= (ll)C.num_rows; ++t) h->C.row_offset[t] = C.row_offset ? C.row_offset[t] : 0;
+    for (ll t = 0; t < (ll)C.num_nnzs; ++t) {
+      h->C.col_index[t] = C.col_index[t];
+      h->C.values[t] = (double)C.values[t];
+    }
+    delete_host_matrix(C);
+  } else {
+    CSR_Matrix<long long, double> C = read_csr_matrix<long long, double>(path, compact != 0);
+    h->C.num_rows = C.num_rows;
+    h->C.num_cols = C.num_cols;
+    h->C.num_nnzs = C.num_nnzs;
+    h->C.row_offset = new_array<int64_t>(C.num_rows + 1);
+    h->C.col_index = new_array<int64_t>(C.num_nnzs > 0 ? C.num_nnzs : 1);
+    h->C.values = new_array<double>(C.num_nnzs > 0 ? C.num_nnzs : 1);
+    for (ll t = 0; t <= (ll)C.num_rows; ++t) h->C.row_offset[t] = C.row_offset ? C.row_offset[t] : 0;
+    for (ll t = 0; t < (ll)C.num_nnzs; ++t) {
+      h->C.col_index[t] = C.col_index[t];
+      h->C.values[t] = C.values[t];
+    }
+    delete_host_matrix(C);
+  }
+  return h;
+}
+
 // ---------------------------------------------------- row-wise and top-k
 // LeSpGEMM<sortOutput, int64_t, double>(A, B, C, kernel_flag) (src/spgemm.cpp:683).
 void* ref_spgemm_rowwise(ll a_rows, ll a_cols, ll a_nnz, const ll* arp, const ll* aci, const double* av, ll b_rows,

@@ -115,6 +115,10 @@ _SIGS = {
     "spops_hierarchical_clustering": [vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp],
     "spops_spgemm_clustered": [vp, vp, vp, vp, vp, i64, i32, dbl, vp, vp],
     "spops_spgemm_rowwise": [vp, vp, vp, i32, i32, vp, vp],
+    "spops_mtx_read_coo": [vp, C.c_char_p, C.c_int, C.c_int, vp],
+    "spops_mtx_parse_coo": [vp, C.c_char_p, i64, C.c_int, C.c_int, vp],
+    "spops_mtx_read_csr": [vp, C.c_char_p, C.c_int, C.c_int, i32, vp],
+    "spops_mtx_parse_csr": [vp, C.c_char_p, i64, C.c_int, C.c_int, i32, vp],
     "spops_spgemm_topk": [vp, vp, i64, vp],
     "spops_spgemm_lsh": [vp, vp, vp, i32, i32, u64, i64, i32, dbl, vp, vp],
     "spops_csr_spmv_noalloc": [i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, dbl, vp, dbl, vp, vp],

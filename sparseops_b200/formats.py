@@ -447,6 +447,42 @@ def coo_to_csr(coo: COO_Matrix, compact: bool = False):
     return DeviceCSR(_Handle(ctx, out), coo.num_rows, coo.num_cols)
 
 
+def _mtx_types(index_dtype, value_dtype):
+    it = 0 if np.dtype(index_dtype) == np.int32 else 1
+    vt = 0 if np.dtype(value_dtype) == np.float32 else 1
+    return C.c_int(it), C.c_int(vt)
+
+
+def read_coo_matrix(mm_filename, index_dtype=np.int32, value_dtype=np.float64, ctx=None) -> COO_Matrix:
+    """utils/sparse_io.cpp:26 with the text parsed on the device: the file's
+    entries in file order (symmetric files expanded), 0-based, held by a
+    device handle; host arrays on first access."""
+    ctx = ctx or default_context()
+    out = vp()
+    call("spops_mtx_read_coo", ctx.handle, str(mm_filename).encode(), *_mtx_types(index_dtype, value_dtype),
+         C.byref(out))
+    h = _Handle(ctx, out)
+    info = h.info()
+    m = COO_Matrix()
+    m.num_rows, m.num_cols, m.num_nnzs = int(info.rows), int(info.cols), int(info.nnz)
+    m._h = h
+    m._arrays = (None, None, None)
+    return m
+
+
+def read_csr_matrix(mm_filename, compact: bool = False, index_dtype=np.int32, value_dtype=np.float64, ctx=None):
+    """utils/sparse_io.cpp:193 on the device: read_coo_matrix then coo_to_csr
+    (compact: duplicates summed); a DeviceCSR."""
+    from .spops import DeviceCSR
+    ctx = ctx or default_context()
+    out = vp()
+    call("spops_mtx_read_csr", ctx.handle, str(mm_filename).encode(), *_mtx_types(index_dtype, value_dtype),
+         C.c_int32(1 if compact else 0), C.byref(out))
+    h = _Handle(ctx, out)
+    info = h.info()
+    return DeviceCSR(h, int(info.rows), int(info.cols))
+
+
 def csr_to_coo(csr: CSR_Matrix):
     """include/sparse_conversion.h:152."""
     h = _convert(csr, "coo")

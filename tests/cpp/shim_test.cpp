@@ -301,6 +301,30 @@ void spgemm_checks() {
   delete_host_matrix(T);
 }
 
+// A small symmetric Matrix Market file read into host structs.
+void mtx_checks() {
+  const char* path = "shim_test_matrix.mtx";
+  FILE* f = std::fopen(path, "w");
+  EXPECT(f != nullptr, "temporary file");
+  if (!f) return;
+  std::fprintf(f, "%%%%MatrixMarket matrix coordinate real symmetric\n%% comment\n3 3 4\n");
+  std::fprintf(f, "1 1 2.5\n2 1 -1e-3\n3 2 0.1\n3 3 4\n");
+  std::fclose(f);
+  COO_Matrix<int, double> coo = read_coo_matrix<int, double>(path);
+  EXPECT(coo.num_nnzs == 6 && coo.row_index[1] == 1 && coo.col_index[1] == 0 && coo.row_index[2] == 0 &&
+             coo.col_index[2] == 1 && coo.values[2] == -1e-3,
+         "read_coo_matrix expands the symmetric entries in file order");
+  CSR_Matrix<long long, float> csr = read_csr_matrix<long long, float>(path, true);
+  // compacting lists a row's columns in reverse order of first appearance
+  // (include/sparse_operation.h:22 threads them through a linked list)
+  EXPECT(csr.num_rows == 3 && csr.num_nnzs == 6 && csr.row_offset[3] == 6 && csr.col_index[0] == 1 &&
+             csr.values[0] == -1e-3f && csr.col_index[1] == 0 && csr.values[1] == 2.5f,
+         "read_csr_matrix shape and values");
+  delete_host_matrix(coo);
+  delete_host_matrix(csr);
+  std::remove(path);
+}
+
 int main() {
   std::setvbuf(stdout, nullptr, _IONBF, 0);
   try {
@@ -309,6 +333,7 @@ int main() {
     run_all<long long, double>();
     lsh_checks();
     spgemm_checks();
+    mtx_checks();
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
     return 2;

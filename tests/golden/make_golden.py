@@ -13,6 +13,7 @@ through the oracle, the device kernels.
 from __future__ import annotations
 
 import os
+import tempfile
 import sys
 
 import numpy as np
@@ -33,6 +34,52 @@ def sort_rows(rp, ci, v):
         o = np.argsort(ci[a:b], kind="stable")
         ci[a:b], v[a:b] = ci[a:b][o], v[a:b][o]
     return ci, v
+
+
+def mtx_cases():
+    """Matrix Market texts covering the reader's rules (banner case, comment
+    lines, a size line after a blank line, CRLF, symmetric / skew / pattern /
+    integer fields, duplicates, zero rows) and values that take every
+    conversion path (exact fast path, double-double, exact midpoints)."""
+    rng = np.random.default_rng(77)
+    cases = []
+    vals = ["1", "-2.5", "+3e2", "4.0E-3", "0.1", "1e-320", "2.4703282292062328e-324", "9007199254740993",
+            "1.7976931348623157e308", "123456789012345678901234567890e-10", "-0", "7.0000000000000000000001",
+            "1.00000000000000011102230246251565404236316680908203125", "6.02214076e23", ".5", "5."]
+    lines = ["%%MatrixMarket matrix coordinate real general", "% a comment", "%", "6 5 %d" % (len(vals) + 4)]
+    ents = [(1 + (i % 6), 1 + (i * 3 % 5), v) for i, v in enumerate(vals)]
+    ents += [(2, 2, "1.5"), (2, 2, "-1.5"), (6, 5, "%.17g" % rng.standard_normal()), (1, 1, "0.25")]
+    lines += ["%d %d %s" % e for e in ents]
+    cases.append("\n".join(lines) + "\n")
+    # symmetric, upper-case words, CRLF, a blank line before a split size line
+    n, ent = 40, []
+    for i in range(120):
+        r, c = int(rng.integers(1, n + 1)), int(rng.integers(1, n + 1))
+        r, c = max(r, c), min(r, c)
+        ent.append("%d %d %.17g" % (r, c, rng.standard_normal() * 10.0 ** rng.integers(-30, 30)))
+    cases.append("%%MatrixMarket MATRIX Coordinate REAL Symmetric\r\n%c\r\n\r\n  40 40\r\n120\r\n" +
+                 "\r\n".join(ent) + "\r\n")
+    # pattern general with duplicates and extra trailing tokens after the last entry
+    pat = ["%d %d" % (int(rng.integers(1, 30)), int(rng.integers(1, 25))) for _ in range(200)]
+    cases.append("%%MatrixMarket matrix coordinate pattern general\n29 24 200\n" + "\n".join(pat) + "\n7 7\n")
+    # integer symmetric, tabs
+    it = ["%d\t%d\t%d" % (max(a, b), min(a, b), v) for a, b, v in
+          zip(rng.integers(1, 20, 60), rng.integers(1, 20, 60), rng.integers(-50, 50, 60))]
+    cases.append("%%MatrixMarket matrix coordinate integer symmetric\n19 19 60\n" + "\n".join(it) + "\n")
+    # skew-symmetric (not expanded by the reference)
+    sk = ["%d %d %.6e" % (i + 2, i + 1, (i + 1) * 0.37) for i in range(10)]
+    cases.append("%%MatrixMarket matrix coordinate real skew-symmetric\n11 11 10\n" + "\n".join(sk) + "\n")
+    # no rows
+    cases.append("%%MatrixMarket matrix coordinate real general\n0 0 0\n")
+    # values around rounding midpoints and extremes, written with many digits
+    mid = []
+    for i in range(80):
+        x = float(rng.standard_normal()) * 10.0 ** int(rng.integers(-300, 300))
+        y = np.nextafter(x, np.inf)
+        m = (np.longdouble(x) + np.longdouble(y)) / 2
+        mid.append("%d %d %s" % (1 + i % 9, 1 + i % 7, np.format_float_scientific(m, unique=False, precision=60)))
+    cases.append("%%MatrixMarket matrix coordinate real general\n9 7 80\n" + "\n".join(mid) + "\n")
+    return cases
 
 
 def main():
@@ -185,6 +232,19 @@ def main():
         g[f"feat{k}_rp"], g[f"feat{k}_ci"], g[f"feat{k}_v"] = frp.astype(np.int64), fci.astype(np.int64), fv
         g[f"feat{k}_nc"] = np.int64(fnc)
         g[f"feat{k}_out"] = R.features(frp, fci, fv, fnc)
+
+    # ---- Matrix Market files through the reference's read_csr_matrix
+    for k, text in enumerate(mtx_cases()):
+        with tempfile.NamedTemporaryFile("wb", suffix=".mtx", delete=False) as f:
+            f.write(text.encode())
+            path = f.name
+        g[f"mtx{k}_text"] = np.frombuffer(text.encode(), np.uint8)
+        for compact in (0, 1):
+            for f32 in (0, 1):
+                c = R.read_csr(path, compact=bool(compact), f32=bool(f32))
+                for key in ("rp", "ci", "v"):
+                    g[f"mtx{k}_{compact}{f32}_{key}"] = c[key]
+        os.unlink(path)
 
     np.savez_compressed(OUT, **g)
     print(OUT, os.path.getsize(OUT), "bytes,", len(g), "arrays")
