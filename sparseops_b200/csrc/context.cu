@@ -141,6 +141,8 @@ spops_status_t spops_destroy(spops_context_t c) {
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->copy_stream = nullptr;
   if (c->pinned) cudaFreeHost(c->pinned);
+  for (cudaEvent_t e : c->file_events) cudaEventDestroy(e);
+  for (void* b : c->file_stage) cudaFreeHost(b);
   if (c->pool) {
     cudaStreamSynchronize(c->stream);
     cudaMemPoolDestroy(c->pool);

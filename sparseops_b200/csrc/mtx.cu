@@ -19,7 +19,11 @@
 // The CSR form is the device coo_to_csr (coo_csr.cu), with or without the
 // duplicate summation.
 //
-// Device steps: the data part of the file is uploaded once; one select over
+// From a path, the banner and size line are read from a prefix and the
+// entries part goes to the device in 4 MiB chunks: reader threads pread into
+// pinned buffers kept by the context, and each upload overlaps the next
+// chunk's read.  From bytes in host memory it is one copy.
+// Device steps: one select over
 // byte positions finds the token starts (a non-space after a space); one
 // thread per entry parses its row, column and value; tokens that the fast
 // conversions leave open (values within 2^-93 of a rounding midpoint, rare)
@@ -27,9 +31,17 @@
 // symmetric copies.
 #include <cub/cub.cuh>
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "decimal.cuh"
@@ -243,16 +255,15 @@ spops_status_t read_header(const char* s, size_t n, Header* h) {
   return SPOPS_OK;
 }
 
+// The entries part of the file (len bytes) is in dtext on the device,
+// written by work already queued on ctx->stream.
 template <typename I, typename V>
-spops_status_t read_t(Context* ctx, const char* text, size_t n, const Header& H, Matrix** out) {
+spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H, Matrix** out) {
   cudaStream_t st = ctx->stream;
   const int per = H.pattern ? 2 : 3;
-  const int64_t len = (int64_t)(n - H.data);
   const int64_t nnz = H.nnz;
-  PoolBuf dtext(ctx), starts(ctx), nsel(ctx), tmp(ctx), tab(ctx), r(ctx), c(ctx), v(ctx), cnt(ctx), pos(ctx),
-      misc(ctx), olist(ctx), ocand(ctx);
-  SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
-  if (len > 0) SPOPS_CUDA(cudaMemcpyAsync(dtext.p, text + H.data, (size_t)len, cudaMemcpyHostToDevice, st));
+  PoolBuf starts(ctx), nsel(ctx), tmp(ctx), tab(ctx), r(ctx), c(ctx), v(ctx), cnt(ctx), pos(ctx), misc(ctx),
+      olist(ctx), ocand(ctx);
   // token starts
   int64_t ntok = 0;
   SPOPS_TRY(nsel.alloc(8));
@@ -364,31 +375,161 @@ spops_status_t read_t(Context* ctx, const char* text, size_t n, const Header& H,
   return SPOPS_OK;
 }
 
-spops_status_t read_file(const char* path, std::vector<char>& buf) {
-  FILE* f = std::fopen(path, "rb");
-  if (!f) return fail(SPOPS_ERR_INVALID, "Matrix Market: unable to open file: %s", path);
-  std::fseek(f, 0, SEEK_END);
-  const long sz = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
-  buf.resize(sz > 0 ? (size_t)sz : 0);
-  const size_t got = sz > 0 ? std::fread(buf.data(), 1, (size_t)sz, f) : 0;
-  std::fclose(f);
-  if (sz < 0 || got != (size_t)sz) return fail(SPOPS_ERR_INVALID, "Matrix Market: read error: %s", path);
+spops_status_t check_header(const Header& H, spops_index_t itype) {
+  if (itype == SPOPS_INDEX_I32 && (H.rows > INT32_MAX || H.cols > INT32_MAX))
+    return fail(SPOPS_ERR_TOO_LARGE, "Matrix Market: %lld x %lld does not fit int32 indices", (long long)H.rows,
+                (long long)H.cols);
   return SPOPS_OK;
 }
 
+spops_status_t read_typed(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H, spops_index_t itype,
+                          spops_value_t vtype, Matrix** out) {
+  const bool i32 = itype == SPOPS_INDEX_I32, f64 = vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return read_t<int32_t, double>(ctx, dtext, len, H, out);
+  if (i32) return read_t<int32_t, float>(ctx, dtext, len, H, out);
+  if (f64) return read_t<int64_t, double>(ctx, dtext, len, H, out);
+  return read_t<int64_t, float>(ctx, dtext, len, H, out);
+}
+
+// the file's bytes in host memory
 spops_status_t parse_coo(Context* ctx, const char* text, size_t n, spops_index_t itype, spops_value_t vtype,
                          Matrix** out) {
   Header H;
   SPOPS_TRY(read_header(text, n, &H));
-  if (itype == SPOPS_INDEX_I32 && (H.rows > INT32_MAX || H.cols > INT32_MAX))
-    return fail(SPOPS_ERR_TOO_LARGE, "Matrix Market: %lld x %lld does not fit int32 indices", (long long)H.rows,
-                (long long)H.cols);
-  const bool i32 = itype == SPOPS_INDEX_I32, f64 = vtype == SPOPS_VALUE_F64;
-  if (i32 && f64) return read_t<int32_t, double>(ctx, text, n, H, out);
-  if (i32) return read_t<int32_t, float>(ctx, text, n, H, out);
-  if (f64) return read_t<int64_t, double>(ctx, text, n, H, out);
-  return read_t<int64_t, float>(ctx, text, n, H, out);
+  SPOPS_TRY(check_header(H, itype));
+  const int64_t len = (int64_t)(n - H.data);
+  PoolBuf dtext(ctx);
+  SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
+  if (len > 0) SPOPS_CUDA(cudaMemcpyAsync(dtext.p, text + H.data, (size_t)len, cudaMemcpyHostToDevice, ctx->stream));
+  return read_typed(ctx, dtext, len, H, itype, vtype, out);
+}
+
+// File chunks go to the device through pinned buffers: kReaders threads each
+// pread their chunks (every kReaders-th one) into their two buffers in turn
+// and queue the upload; a buffer is refilled once its previous upload ended.
+constexpr size_t kChunk = size_t(4) << 20;
+constexpr int kReaders = 4;
+
+spops_status_t ensure_file_stage(Context* ctx) {
+  if (!ctx->file_stage.empty()) return SPOPS_OK;
+  for (int i = 0; i < 2 * kReaders; ++i) {
+    void* b = nullptr;
+    cudaEvent_t e = nullptr;
+    if (cudaHostAlloc(&b, kChunk, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(b);
+      break;
+    }
+    ctx->file_stage.push_back(b);
+    ctx->file_events.push_back(e);
+  }
+  if ((int)ctx->file_stage.size() == 2 * kReaders) return SPOPS_OK;
+  for (cudaEvent_t e : ctx->file_events) cudaEventDestroy(e);
+  for (void* b : ctx->file_stage) cudaFreeHost(b);
+  ctx->file_events.clear();
+  ctx->file_stage.clear();
+  return fail(SPOPS_ERR_ALLOC, "Matrix Market: pinned staging buffers could not be allocated");
+}
+
+bool pread_all(int fd, char* dst, size_t n, int64_t off) {
+  size_t got = 0;
+  while (got < n) {
+    const ssize_t r = ::pread(fd, dst + got, n - got, (off_t)(off + (int64_t)got));
+    if (r < 0 && errno == EINTR) continue;
+    if (r <= 0) return false;
+    got += (size_t)r;
+  }
+  return true;
+}
+
+struct FileCloser {
+  int fd;
+  ~FileCloser() {
+    if (fd >= 0) ::close(fd);
+  }
+};
+
+spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, spops_value_t vtype, Matrix** out) {
+  const int fd = ::open(path, O_RDONLY | O_CLOEXEC);
+  if (fd < 0) return fail(SPOPS_ERR_INVALID, "Matrix Market: unable to open file: %s", path);
+  FileCloser closer{fd};
+  struct stat sb;
+  if (::fstat(fd, &sb) != 0 || sb.st_size < 0) return fail(SPOPS_ERR_INVALID, "Matrix Market: read error: %s", path);
+  const int64_t size = (int64_t)sb.st_size;
+  // the banner and size line from a prefix, grown until they end inside it
+  Header H;
+  std::string pre;
+  for (int64_t want = 65536;; want *= 4) {
+    const int64_t m = std::min(size, want);
+    pre.resize((size_t)m);
+    if (m > 0 && !pread_all(fd, &pre[0], (size_t)m, 0))
+      return fail(SPOPS_ERR_INVALID, "Matrix Market: read error: %s", path);
+    Header h;
+    const spops_status_t s = read_header(pre.data(), (size_t)m, &h);
+    if (m == size) {
+      SPOPS_TRY(s);
+      H = h;
+      break;
+    }
+    if (s == SPOPS_OK && (int64_t)h.data < m) {
+      H = h;
+      break;
+    }
+  }
+  SPOPS_TRY(check_header(H, itype));
+  const int64_t len = size - (int64_t)H.data;
+  PoolBuf dtext(ctx);
+  SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
+  if (len > 0) {
+    SPOPS_TRY(ensure_file_stage(ctx));
+    const int64_t nchunks = (len + (int64_t)kChunk - 1) / (int64_t)kChunk;
+    const int nt = (int)std::min<int64_t>(kReaders, nchunks);
+    std::atomic<int> bad{0};  // 1: read error, 2: CUDA error
+    char* dst = dtext.as<char>();
+    auto reader = [&](int w) {
+      if (nt > 1 && cudaSetDevice(ctx->device) != cudaSuccess) {
+        bad = 2;
+        return;
+      }
+      int turn = 0;
+      for (int64_t k = w; k < nchunks && !bad; k += nt, ++turn) {
+        const int b = 2 * w + (turn & 1);
+        char* buf = static_cast<char*>(ctx->file_stage[b]);
+        const int64_t off = k * (int64_t)kChunk;
+        const size_t n = (size_t)std::min<int64_t>((int64_t)kChunk, len - off);
+        if (cudaEventSynchronize(ctx->file_events[b]) != cudaSuccess) {
+          bad = 2;
+          return;
+        }
+        if (!pread_all(fd, buf, n, (int64_t)H.data + off)) {
+          bad = 1;
+          return;
+        }
+        if (cudaMemcpyAsync(dst + off, buf, n, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+            cudaEventRecord(ctx->file_events[b], ctx->stream) != cudaSuccess) {
+          bad = 2;
+          return;
+        }
+      }
+    };
+    if (nt == 1) {
+      reader(0);
+    } else {
+      std::vector<std::thread> th;
+      for (int w = 0; w < nt; ++w) th.emplace_back(reader, w);
+      for (auto& t : th) t.join();
+    }
+    if (bad == 1) return fail(SPOPS_ERR_INVALID, "Matrix Market: read error: %s", path);
+    if (bad == 2) {
+      cudaStreamSynchronize(ctx->stream);
+      return fail(SPOPS_ERR_CUDA, "Matrix Market: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+  }
+  return read_typed(ctx, dtext, len, H, itype, vtype, out);
 }
 
 spops_status_t check_types(spops_index_t itype, spops_value_t vtype) {
@@ -445,9 +586,12 @@ spops_status_t spops_mtx_parse_coo(spops_context_t ctx, const char* text, int64_
 spops_status_t spops_mtx_read_coo(spops_context_t ctx, const char* path, spops_index_t itype, spops_value_t vtype,
                                   spops_matrix_t* coo) {
   if (!ctx || !path || !coo) return fail(SPOPS_ERR_INVALID, "spops_mtx_read_coo: null argument");
-  std::vector<char> buf;
-  SPOPS_TRY(read_file(path, buf));
-  return spops_mtx_parse_coo(ctx, buf.data(), (int64_t)buf.size(), itype, vtype, coo);
+  SPOPS_TRY(check_types(itype, vtype));
+  DeviceGuard g(ctx->device);
+  Matrix* A = nullptr;
+  SPOPS_TRY(read_path(ctx, path, itype, vtype, &A));
+  *coo = static_cast<spops_matrix_s*>(A);
+  return SPOPS_OK;
 }
 
 spops_status_t spops_mtx_parse_csr(spops_context_t ctx, const char* text, int64_t len, spops_index_t itype,
@@ -463,9 +607,11 @@ spops_status_t spops_mtx_parse_csr(spops_context_t ctx, const char* text, int64_
 spops_status_t spops_mtx_read_csr(spops_context_t ctx, const char* path, spops_index_t itype, spops_value_t vtype,
                                   int32_t compact, spops_matrix_t* csr) {
   if (!ctx || !path || !csr) return fail(SPOPS_ERR_INVALID, "spops_mtx_read_csr: null argument");
-  std::vector<char> buf;
-  SPOPS_TRY(read_file(path, buf));
-  return spops_mtx_parse_csr(ctx, buf.data(), (int64_t)buf.size(), itype, vtype, compact, csr);
+  SPOPS_TRY(check_types(itype, vtype));
+  DeviceGuard g(ctx->device);
+  Matrix* A = nullptr;
+  SPOPS_TRY(read_path(ctx, path, itype, vtype, &A));
+  return coo_to_csr_out(ctx, A, compact, csr);
 }
 
 }  // extern "C"

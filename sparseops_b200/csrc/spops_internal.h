@@ -65,6 +65,10 @@ struct Context {
   // second stream and per-range events of the pipelined spops_spmv_host
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> part_events;
+  // pinned staging of the Matrix Market reader (file chunks on their way to
+  // the device) and the event that frees each buffer for its next chunk
+  std::vector<void*> file_stage;
+  std::vector<cudaEvent_t> file_events;
   // stream-ordered pool for per-call temporaries (PoolBuf): memory freed by
   // one call is handed to the next without returning it to the driver
   cudaMemPool_t pool = nullptr;

@@ -134,3 +134,56 @@ def test_missing_file(cuda, tmp_path):
     from sparseops_b200 import SpOpsError, read_csr_matrix
     with pytest.raises(SpOpsError):
         read_csr_matrix(str(tmp_path / "absent.mtx"))
+
+
+def _coo_from_memory(text):
+    import ctypes as C
+    from sparseops_b200._lib import call, i64, vp
+    from sparseops_b200.formats import _Handle, default_context
+    ctx = default_context()
+    out = vp()
+    call("spops_mtx_parse_coo", ctx.handle, text, i64(len(text)), C.c_int(1), C.c_int(1), C.byref(out))
+    h = _Handle(ctx, out)
+    n = int(h.info().nnz)
+    got = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n)]
+    for arr, which in zip(got, (0, 1, 2)):
+        if n:
+            call("spops_matrix_download", ctx.handle, h.handle, which, vp(arr.ctypes.data), i64(n))
+    return got
+
+
+@pytest.mark.parametrize("case", ["long_comments", "size_line_at_prefix_end", "many_chunks"])
+def test_path_read_matches_memory(cuda, tmp_path, case):
+    """Reading from a path (header from a growing prefix, entries streamed in
+    4 MiB chunks by several reader threads) gives the same COO as parsing the
+    same bytes from host memory: a header longer than the first 64 KiB
+    prefix, a size line cut by that prefix, and a 20 MB file of many chunks."""
+    from sparseops_b200 import read_coo_matrix
+    rng = np.random.default_rng(21)
+    head = "%%MatrixMarket matrix coordinate real general\n"
+    if case == "long_comments":
+        head += "".join("%% comment line %06d %s\n" % (i, "x" * 60) for i in range(1500))
+        nnz = 2000
+    elif case == "size_line_at_prefix_end":
+        pad = 65536 - len(head) - 4  # the size line starts 4 bytes before the prefix ends
+        head += "%" + "y" * (pad - 2) + "\n"
+        nnz = 2000
+    else:
+        nnz = 700_000
+    n = 100_000
+    r, c = rng.integers(1, n + 1, nnz), rng.integers(1, n + 1, nnz)
+    x = rng.standard_normal(nnz) * 10.0 ** rng.integers(-30, 30, nnz)
+    import io
+    buf = io.StringIO()
+    np.savetxt(buf, np.column_stack([r, c, x]), fmt="%d %d %.17g")
+    text = (head + "%d %d %d\n" % (n, n, nnz) + buf.getvalue()).encode()
+    if case == "size_line_at_prefix_end":
+        assert text.index(b"%d %d %d\n" % (n, n, nnz)) == 65532
+    path = _write(tmp_path, text)
+    m = read_coo_matrix(path, np.int64, np.float64)
+    er, ec, ev = _coo_from_memory(text)
+    assert m.num_nnzs == nnz
+    assert np.array_equal(m.row_index, er) and np.array_equal(m.col_index, ec)
+    assert np.array_equal(m.values.view(np.uint64), ev.view(np.uint64))
+    assert np.array_equal(er, r - 1) and np.array_equal(ec, c - 1)
+    assert np.array_equal(ev, x)
