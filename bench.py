@@ -613,6 +613,43 @@ def run_reference(args):
     return 0
 
 
+def bench_features(A, cpu_ref: bool, rp=None, ci=None):
+    """Structure features and tile features (256 x 256 grid) of the power-law
+    matrix on the device: median of 3 calls after a first call (which builds
+    the transpose that the column side of the tile features reads).  The CPU
+    leg runs the oracle's restatement of the reference's tile counting on the
+    first 1/16 of the rows, and the device on the same sample."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, matrix_features, matrix_tile_features
+    out = {}
+    t0 = time.perf_counter()
+    matrix_tile_features(A)
+    out["tile_first_call_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    out["tile_ms"] = round(_host_ms(lambda: matrix_tile_features(A), 3, warm=0), 2)
+    out["tile_with_maps_ms"] = round(_host_ms(lambda: matrix_tile_features(A, maps=True), 3, warm=1), 2)
+    out["structure_ms"] = round(_host_ms(lambda: matrix_features(A), 3, warm=1), 2)
+    if cpu_ref and rp is not None:
+        try:
+            from oracle import Oracle
+            m = (len(rp) - 1) // 16
+            srp, sci = rp[:m + 1].astype(np.int64), ci[:int(rp[m])].astype(np.int64)
+            nc = len(rp) - 1
+            t0 = time.perf_counter()
+            Oracle().tile_features(srp, sci, nc)
+            cms = (time.perf_counter() - t0) * 1e3
+            dev = torch.device("cuda", 0)
+            S = CSR_Matrix(m, nc, torch.from_numpy(srp.astype(np.int32)).to(dev),
+                           torch.from_numpy(sci.astype(np.int32)).to(dev),
+                           torch.ones(len(sci), dtype=torch.float64, device=dev))
+            matrix_tile_features(S)
+            out["sample"] = {"rows": int(m), "nnz": int(len(sci)), "cpu_port_ms": round(cms, 1),
+                             "device_ms": round(_host_ms(lambda: matrix_tile_features(S), 3, warm=0), 2),
+                             "cpu": {"kind": "port", "cores": 1}}
+        except Exception as e:
+            out["sample_error"] = str(e)[:160]
+    return out
+
+
 def run_section(args):
     """One extra section alone (for profiling captures); prints its JSON."""
     import torch
@@ -628,6 +665,12 @@ def run_section(args):
         res = bench_mtx(not args.no_cpu_baseline)
     elif args.section == "spgemm":
         res = bench_spgemm(dev, not args.no_cpu_baseline)
+    elif args.section == "features":
+        from sparseops_b200 import CSR_Matrix
+        rp, ci, v, _ = workload(args.rows)
+        A = CSR_Matrix(len(rp) - 1, len(rp) - 1, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
+                       torch.from_numpy(v).to(dev))
+        res = bench_features(A, not args.no_cpu_baseline, rp, ci)
     else:
         raise SystemExit(f"unknown section {args.section}")
     print(json.dumps({"section": args.section, args.section: res}))
@@ -738,7 +781,8 @@ def run_ours(args):
                         ("batched", lambda: bench_batched(ctx, dev)),
                         ("fwd_bwd", lambda: bench_fwd_bwd(ctx, dev)),
                         ("spgemm", lambda: bench_spgemm(dev, not args.no_cpu_baseline)),
-                        ("mtx", lambda: bench_mtx(not args.no_cpu_baseline))):
+                        ("mtx", lambda: bench_mtx(not args.no_cpu_baseline)),
+                        ("features", lambda: bench_features(A, not args.no_cpu_baseline, rp, ci))):
             t0 = time.time()
             try:
                 extra[key] = fn()
@@ -786,7 +830,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
-    ap.add_argument("--section", default="all", choices=["all", "batched", "fwd_bwd", "spgemm", "mtx"],
+    ap.add_argument("--section", default="all", choices=["all", "batched", "fwd_bwd", "spgemm", "mtx", "features"],
                     help="run one extra section alone (profiling); the headline line needs 'all'")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-format, batched, fwd+bwd and SpGEMM sections")

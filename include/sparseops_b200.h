@@ -408,6 +408,57 @@ typedef struct {
 } spops_features_t;
 spops_status_t spops_matrix_features(spops_context_t ctx, spops_matrix_t csr, spops_features_t* features);
 
+/* Tile features of a CSR matrix, computed on the device.  Replaces the tile
+ * part of MTX::MtxLoad (src/sparse_features.cpp:181-265 per entry, :484-625
+ * per tile and block), MTX::CalculateTilesFeatures (:783-846) and the
+ * distance_per_row_ of MTX::CalculateTilesExtraFeatures (:943-965).
+ * The matrix is cut into num_blocks x num_blocks tiles (MAT_TILE_SIZE = 256
+ * in the reference; num_blocks <= 0 means 256, at most 2048): rows into
+ * num_blocks row blocks (RB), of which the first rows % num_blocks hold
+ * rows / num_blocks + 1 rows and the rest rows / num_blocks; columns into
+ * column blocks (CB) alike.  The statistics over the tile, RB and CB entry
+ * counts follow CalculateTilesFeatures, including its starting values:
+ * nz_ratio_* = (non-empty count - 1) / length and var_* = (sum of squared
+ * deviations - 1) / length, std_* = sqrt(max(var_*, 0)); min_* is at most
+ * 100000000.  uniq_r / uniq_c: sum over tiles of the rows (columns) holding
+ * an entry in the tile, over nnz; pot_reuse_r / _c: the same sums over rows
+ * (columns).  distance_per_row: mean over rows of (last column - first
+ * column in storage order) / row length (0 for empty rows), as the
+ * reference's sum of neighbour distances telescopes to. */
+typedef struct {
+  int64_t num_blocks, rows_per_block, rows_mod, cols_per_block, cols_mod; /* t_num_blocks, t_num_RB, t_mod_RB, ... */
+  int64_t min_nnz_tile, max_nnz_tile, min_nnz_rb, max_nnz_rb, min_nnz_cb, max_nnz_cb;
+  double nz_ratio_tiles, ave_nnz_tile, var_nnz_tile, std_nnz_tile, p_ratio_tiles, gini_tiles;
+  double nz_ratio_rb, ave_nnz_rb, var_nnz_rb, std_nnz_rb, p_ratio_rb, gini_rb;
+  double nz_ratio_cb, ave_nnz_cb, var_nnz_cb, std_nnz_cb, p_ratio_cb, gini_cb;
+  double uniq_r, uniq_c, pot_reuse_r, pot_reuse_c, distance_per_row;
+} spops_tile_features_t;
+
+/* Per-tile and per-block maps (the files MTX::FeaturesWrite writes,
+ * src/sparse_features.cpp:1218-1330), host arrays filled when not NULL.
+ * tile_* hold num_blocks^2 values, tile (i, j) at i * num_blocks + j; the
+ * rb_* and cb_* arrays num_blocks values.  Row statistics of a tile run over
+ * all rows of its row block, empty ones included (std: population standard
+ * deviation); the RB / CB ones over the block's rows / columns. */
+typedef struct {
+  int64_t* tile_nnz;          /* nnz_by_Tiles_ */
+  int64_t* tile_rows;         /* uniq_RB: rows with an entry in the tile */
+  int64_t* tile_cols;         /* uniq_CB: columns with an entry in the tile */
+  int64_t* tile_max_row_nnz;  /* max_rownnz_per_tile_ */
+  double* tile_ave_row_nnz;   /* ave_rownnz_per_tile_ */
+  double* tile_std_row_nnz;   /* std_rownnz_per_tile_ */
+  int64_t* rb_nnz;            /* nnz_by_RB_ */
+  int64_t* rb_max_row_nnz;    /* max_rownnz_per_RB_ */
+  double* rb_ave_row_nnz;     /* ave_rownnz_per_RB_ */
+  double* rb_std_row_nnz;     /* std_rownnz_per_RB_ */
+  int64_t* cb_nnz;            /* nnz_by_CB_ */
+  int64_t* cb_max_col_nnz;    /* max_colnnz_per_CB_ */
+  double* cb_ave_col_nnz;     /* ave_colnnz_per_CB_ */
+  double* cb_std_col_nnz;     /* std_colnnz_per_CB_ */
+} spops_tile_maps_t;
+spops_status_t spops_matrix_tile_features(spops_context_t ctx, spops_matrix_t csr, int64_t num_blocks,
+                                          spops_tile_features_t* features, const spops_tile_maps_t* maps);
+
 /* Storage format for y = A*x on this GPU.  No counterpart in the reference,
  * which computes features but leaves the choice to the caller.
  *   mode 0: rules on the features -- DIA when at most 64 diagonals hold at

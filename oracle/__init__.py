@@ -200,6 +200,17 @@ class Oracle:
                             _p(out))
         return out
 
+    def tile_features(self, rp, ci, ncols, num_blocks=256):
+        """(scalars[34] in spops_tile_features_t order, tile_i[4, B*B],
+        tile_d[2, B*B], blk_i[4, B], blk_d[4, B]) of a CSR matrix."""
+        B = int(num_blocks)
+        sc, ti, td = np.zeros(34), np.zeros(4 * B * B, np.int64), np.zeros(2 * B * B)
+        bi, bd = np.zeros(4 * B, np.int64), np.zeros(4 * B)
+        self.L.orc_tile_features(_i64(len(rp) - 1), _i64(ncols), _p(np.ascontiguousarray(rp, np.int64)),
+                                 _p(np.ascontiguousarray(ci, np.int64)), _i64(B), _p(sc), _p(ti), _p(td), _p(bi),
+                                 _p(bd))
+        return sc, ti.reshape(4, -1), td.reshape(2, -1), bi.reshape(4, -1), bd.reshape(4, -1)
+
     # ---- COO -> CSR
     def coo_to_csr(self, n, ri, ci, v, compact=False):
         """(rp, ci, v) of coo_to_csr; v's dtype (float32 / float64) is kept."""
@@ -426,6 +437,31 @@ class Reference:
             if rc != 0:
                 raise RuntimeError(f"ref_features failed ({rc})")
             return out
+        finally:
+            os.remove(path)
+
+    def tile_features(self, rp, ci, v, ncols):
+        """The reference's MtxLoad + CalculateFeatures + CalculateTilesExtraFeatures
+        tile features (its 256 x 256 grid) on the matrix written as a general
+        real Matrix Market file; the same tuple as Oracle.tile_features."""
+        import tempfile
+        fd, path = tempfile.mkstemp(suffix=".mtx")
+        try:
+            with os.fdopen(fd, "w") as f:
+                n = len(rp) - 1
+                f.write("%%MatrixMarket matrix coordinate real general\n")
+                f.write(f"{n} {ncols} {len(ci)}\n")
+                rows = np.repeat(np.arange(n), np.diff(np.asarray(rp, np.int64)))
+                for r, c, x in zip(rows, ci, v):
+                    f.write(f"{r + 1} {c + 1} {float(x)!r}\n")
+            B = 256
+            sc, ti, td = np.zeros(34), np.zeros(4 * B * B, np.int64), np.zeros(2 * B * B)
+            bi, bd = np.zeros(4 * B, np.int64), np.zeros(4 * B)
+            self.L.ref_tile_features.restype = C.c_int
+            rc = self.L.ref_tile_features(path.encode(), _p(sc), _p(ti), _p(td), _p(bi), _p(bd))
+            if rc != 0:
+                raise RuntimeError(f"ref_tile_features failed ({rc})")
+            return sc, ti.reshape(4, -1), td.reshape(2, -1), bi.reshape(4, -1), bd.reshape(4, -1)
         finally:
             os.remove(path)
 

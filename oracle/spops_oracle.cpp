@@ -16,6 +16,7 @@
 #include <map>
 #include <queue>
 #include <set>
+#include <unordered_map>
 #include <unordered_set>
 #include <utility>
 #include <vector>
@@ -666,6 +667,163 @@ static void count_stats(const std::vector<int64_t>& cnt, int64_t nnz, double* nz
   for (size_t i = 0; i + 1 < cum.size(); ++i) area += (double)(cum[i] + cum[i + 1]) / 2.0;
   const double total = (double)nnz * (double)len / 2.0;
   *gini = (total - area) / total;
+}
+
+// Tile features: MtxLoad's tile counting (src/sparse_features.cpp:181-265
+// for the per-entry counts, :484-625 for the per-tile and per-block row
+// statistics), CalculateTilesFeatures (:783-846) and the distance of
+// CalculateTilesExtraFeatures (:943-965), for a general matrix read in CSR
+// order.  B x B tiles; the first n % B row blocks hold n / B + 1 rows.
+// As in the reference, the non-empty ratios and the variances of the tile,
+// row-block and column-block counts start from -1 before they are summed.
+// Output layout: sc[34] in the order of spops_tile_features_t; tile_i[4 B^2]
+// (nnz, rows, cols, max row nnz), tile_d[2 B^2] (ave, std row nnz), blk_i[4 B]
+// (RB nnz, RB max row nnz, CB nnz, CB max col nnz), blk_d[4 B] (RB ave, RB
+// std, CB ave, CB std).
+void orc_tile_features(int64_t n, int64_t nc, const int64_t* rp, const int64_t* ci, int64_t B, double* sc,
+                       int64_t* tile_i, double* tile_d, int64_t* blk_i, double* blk_d) {
+  const int64_t qr = n / B, mr = n % B, qc = nc / B, mc = nc % B;
+  const int64_t thr = mr * (qr + 1), thc = mc * (qc + 1);
+  auto rbk = [&](int64_t r) { return r < thr ? r / (qr + 1) : mr + (r - thr) / qr; };
+  auto cbk = [&](int64_t c) { return c < thc ? c / (qc + 1) : mc + (c - thc) / qc; };
+  auto rstart = [&](int64_t b) { return b < mr ? b * (qr + 1) : thr + (b - mr) * qr; };
+  auto cstart = [&](int64_t b) { return b < mc ? b * (qc + 1) : thc + (b - mc) * qc; };
+  const size_t T = (size_t)(B * B);
+  const int64_t nnz = n ? rp[n] : 0;
+  std::vector<int64_t> tnnz(T, 0), urows(T, 0), ucols(T, 0), tmax(T, 0), rbn(B, 0), cbn(B, 0), rbmax(B, 0),
+      cbmax(B, 0), ccnt((size_t)nc, 0);
+  std::vector<double> tave(T, 0.0), tstd(T, 0.0), rbave(B, 0.0), rbstd(B, 0.0), cbave(B, 0.0), cbstd(B, 0.0);
+  std::unordered_map<int64_t, int64_t> colblk;  // (col, row block) pairs seen: Cols_cnt > 0
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) {
+      const int64_t tr = rbk(r), tc = cbk(ci[k]);
+      ++tnnz[(size_t)(tr * B + tc)];
+      ++rbn[(size_t)tr];
+      ++cbn[(size_t)tc];
+      ++ccnt[(size_t)ci[k]];
+      if (colblk[ci[k] * B + tr]++ == 0) ++ucols[(size_t)(tr * B + tc)];
+    }
+  for (size_t i = 0; i < T; ++i) {
+    if ((int64_t)i < mr * B) tave[i] = (double)tnnz[i] / (double)(qr + 1);
+    else if (qr) tave[i] = (double)tnnz[i] / (double)qr;
+  }
+  for (int64_t b = 0; b < B; ++b) {
+    if (b < mr) rbave[(size_t)b] = (double)rbn[(size_t)b] / (double)(qr + 1);
+    else if (qr) rbave[(size_t)b] = (double)rbn[(size_t)b] / (double)qr;
+    if (b < mc) cbave[(size_t)b] = (double)cbn[(size_t)b] / (double)(qc + 1);
+    else if (qc) cbave[(size_t)b] = (double)cbn[(size_t)b] / (double)qc;
+  }
+  // Rows_cnt one row at a time: tile max / sum of squared deviations, uniq rows
+  std::vector<int64_t> h((size_t)B, 0);
+  for (int64_t r = 0; r < n; ++r) {
+    const int64_t tr = rbk(r);
+    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) ++h[(size_t)cbk(ci[k])];
+    for (int64_t tc = 0; tc < B; ++tc) {
+      const size_t t = (size_t)(tr * B + tc);
+      if (h[(size_t)tc]) ++urows[t];
+      tmax[t] = std::max(tmax[t], h[(size_t)tc]);
+      const double d = (double)h[(size_t)tc] - tave[t];
+      tstd[t] += d * d;
+      h[(size_t)tc] = 0;
+    }
+  }
+  for (size_t i = 0; i < T; ++i) {
+    if ((int64_t)i < mr * B) tstd[i] = tstd[i] / (double)(qr + 1);
+    else if (qr) tstd[i] = tstd[i] / (double)qr;
+    tstd[i] = std::sqrt(tstd[i]);
+  }
+  for (int64_t b = 0; b < B; ++b) {
+    const int64_t r0 = rstart(b), r1 = b < mr ? r0 + qr + 1 : r0 + qr;
+    for (int64_t r = r0; r < r1 && r < n; ++r) {
+      const int64_t len = rp[r + 1] - rp[r];
+      rbmax[(size_t)b] = std::max(rbmax[(size_t)b], len);
+      const double d = (double)len - rbave[(size_t)b];
+      rbstd[(size_t)b] += d * d;
+    }
+    const int64_t c0 = cstart(b), c1 = b < mc ? c0 + qc + 1 : c0 + qc;
+    for (int64_t c = c0; c < c1 && c < nc; ++c) {
+      cbmax[(size_t)b] = std::max(cbmax[(size_t)b], ccnt[(size_t)c]);
+      const double d = (double)ccnt[(size_t)c] - cbave[(size_t)b];
+      cbstd[(size_t)b] += d * d;
+    }
+  }
+  for (int64_t b = 0; b < B; ++b) {
+    if (b < mr) rbstd[(size_t)b] /= (double)(qr + 1);
+    else if (qr) rbstd[(size_t)b] /= (double)qr;
+    rbstd[(size_t)b] = std::sqrt(rbstd[(size_t)b]);
+    if (b < mc) cbstd[(size_t)b] /= (double)(qc + 1);
+    else if (qc) cbstd[(size_t)b] /= (double)qc;
+    cbstd[(size_t)b] = std::sqrt(cbstd[(size_t)b]);
+  }
+  // CalculateTilesFeatures: counts statistics with the -1 starts
+  auto stats = [&](const std::vector<int64_t>& cnt, double ave, double* nzr, int64_t* mn, int64_t* mx, double* var,
+                   double* sd, double* p, double* gini) {
+    double z = -1.0, v = -1.0;
+    int64_t lo = 100000000, hi = 0;
+    for (int64_t c : cnt) {
+      if (c) ++z;
+      const double d = (double)c - ave;
+      v += d * d;
+      lo = std::min(lo, c);
+      hi = std::max(hi, c);
+    }
+    *nzr = z / (double)cnt.size();
+    *var = v / (double)cnt.size();
+    *sd = std::sqrt(std::max(*var, 0.0));
+    *mn = lo;
+    *mx = hi;
+    double nz2, ave2, var2, sd2;
+    int64_t mn2, mx2;
+    count_stats(cnt, nnz, &nz2, &mn2, &mx2, &ave2, &var2, &sd2, p, gini);
+  };
+  double f[23];
+  int64_t ii[6];
+  const double ave_t = (double)nnz / ((double)B * (double)B), ave_b = (double)nnz / (double)B;
+  f[1] = ave_t;
+  stats(tnnz, ave_t, &f[0], &ii[0], &ii[1], &f[2], &f[3], &f[4], &f[5]);
+  f[7] = ave_b;
+  stats(rbn, ave_b, &f[6], &ii[2], &ii[3], &f[8], &f[9], &f[10], &f[11]);
+  f[13] = ave_b;
+  stats(cbn, ave_b, &f[12], &ii[4], &ii[5], &f[14], &f[15], &f[16], &f[17]);
+  int64_t su = 0, sc2 = 0;
+  for (size_t i = 0; i < T; ++i) {
+    su += urows[i];
+    sc2 += ucols[i];
+  }
+  f[18] = (double)su / (double)nnz;
+  f[19] = (double)sc2 / (double)nnz;
+  f[20] = (double)su / (double)n;
+  f[21] = (double)sc2 / (double)nc;
+  double dist = 0.0;
+  for (int64_t r = 0; r < n; ++r) {
+    const int64_t len = rp[r + 1] - rp[r];
+    int64_t dis = 0;
+    for (int64_t k = rp[r]; k + 1 < rp[r + 1]; ++k) dis += ci[k + 1] - ci[k];
+    if (len) dist += (double)dis / (double)len;
+  }
+  f[22] = dist / (double)n;
+  const double head[11] = {(double)B, (double)qr, (double)mr, (double)qc, (double)mc, (double)ii[0],
+                           (double)ii[1], (double)ii[2], (double)ii[3], (double)ii[4], (double)ii[5]};
+  std::memcpy(sc, head, sizeof(head));
+  std::memcpy(sc + 11, f, sizeof(f));
+  for (size_t i = 0; i < T; ++i) {
+    tile_i[i] = tnnz[i];
+    tile_i[T + i] = urows[i];
+    tile_i[2 * T + i] = ucols[i];
+    tile_i[3 * T + i] = tmax[i];
+    tile_d[i] = tave[i];
+    tile_d[T + i] = tstd[i];
+  }
+  for (int64_t b = 0; b < B; ++b) {
+    blk_i[b] = rbn[(size_t)b];
+    blk_i[B + b] = rbmax[(size_t)b];
+    blk_i[2 * B + b] = cbn[(size_t)b];
+    blk_i[3 * B + b] = cbmax[(size_t)b];
+    blk_d[b] = rbave[(size_t)b];
+    blk_d[B + b] = rbstd[(size_t)b];
+    blk_d[2 * B + b] = cbave[(size_t)b];
+    blk_d[3 * B + b] = cbstd[(size_t)b];
+  }
 }
 
 void orc_features(int64_t n, int64_t nc, const int64_t* rp, const int64_t* ci, const double* v, double* out) {

@@ -91,6 +91,8 @@ int64_t orc_coo_to_csr_f32(int64_t n, int64_t nnz, const int64_t* ri, const int6
 /* Structure features (src/sparse_features.cpp:643-775 with MtxLoad's counts,
  * :336-478) of a general CSR matrix, in spops_features_t order (32 values). */
 void orc_features(int64_t n, int64_t nc, const int64_t* rp, const int64_t* ci, const double* v, double* out);
+void orc_tile_features(int64_t n, int64_t nc, const int64_t* rp, const int64_t* ci, int64_t B, double* sc,
+                       int64_t* tile_i, double* tile_d, int64_t* blk_i, double* blk_d);
 
 /* y = A^T g by scatter (the value the reference's csr_transpose + SpOps_csr
  * gives, include/sparse_conversion.h:2066-2108), FP64. */

@@ -68,6 +68,34 @@ class Features(C.Structure):
         return {n: getattr(self, n) for n in FEATURE_NAMES}
 
 
+TILE_FEATURE_NAMES = ("num_blocks", "rows_per_block", "rows_mod", "cols_per_block", "cols_mod", "min_nnz_tile",
+                      "max_nnz_tile", "min_nnz_rb", "max_nnz_rb", "min_nnz_cb", "max_nnz_cb", "nz_ratio_tiles",
+                      "ave_nnz_tile", "var_nnz_tile", "std_nnz_tile", "p_ratio_tiles", "gini_tiles", "nz_ratio_rb",
+                      "ave_nnz_rb", "var_nnz_rb", "std_nnz_rb", "p_ratio_rb", "gini_rb", "nz_ratio_cb",
+                      "ave_nnz_cb", "var_nnz_cb", "std_nnz_cb", "p_ratio_cb", "gini_cb", "uniq_r", "uniq_c",
+                      "pot_reuse_r", "pot_reuse_c", "distance_per_row")
+
+
+class TileFeatures(C.Structure):
+    _fields_ = [(n, i64) for n in TILE_FEATURE_NAMES[:11]] + [(n, C.c_double) for n in TILE_FEATURE_NAMES[11:]]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n in TILE_FEATURE_NAMES}
+
+
+# spops_tile_maps_t: (name, per tile?, integer?)
+TILE_MAP_FIELDS = (("tile_nnz", True, True), ("tile_rows", True, True), ("tile_cols", True, True),
+                   ("tile_max_row_nnz", True, True), ("tile_ave_row_nnz", True, False),
+                   ("tile_std_row_nnz", True, False), ("rb_nnz", False, True), ("rb_max_row_nnz", False, True),
+                   ("rb_ave_row_nnz", False, False), ("rb_std_row_nnz", False, False), ("cb_nnz", False, True),
+                   ("cb_max_col_nnz", False, True), ("cb_ave_col_nnz", False, False),
+                   ("cb_std_col_nnz", False, False))
+
+
+class TileMaps(C.Structure):
+    _fields_ = [(n, vp) for n, _, _ in TILE_MAP_FIELDS]
+
+
 # name -> argtypes (restype is spops_status_t unless listed in _RESTYPE)
 _SIGS = {
     "spops_create": [vp, C.c_int, vp],
@@ -79,6 +107,7 @@ _SIGS = {
     "spops_csr_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
     "spops_coo_to_csr": [vp, vp, C.c_int32, C.POINTER(vp)],
     "spops_matrix_features": [vp, vp, vp],
+    "spops_matrix_tile_features": [vp, vp, i64, vp, vp],
     "spops_select_format": [vp, vp, i32, C.POINTER(C.c_int), vp, C.POINTER(C.c_double)],
     "spops_matrix_destroy": [vp],
     "spops_matrix_info": [vp, vp],

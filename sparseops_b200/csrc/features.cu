@@ -191,7 +191,7 @@ __global__ void symm_keys_kernel(const I* __restrict__ rp, const I* __restrict__
 // count statistics of one of the two count vectors (rows or columns)
 struct CountStats {
   int64_t nz = 0, mn = 0, mx = 0;
-  double ave = 0, var = 0, p = 0, gini = 0;
+  double ave = 0, sq = 0, var = 0, p = 0, gini = 0;
 };
 
 spops_status_t count_stats(Context* ctx, const int64_t* cnt, int64_t len, int64_t nnz, CountStats* out) {
@@ -244,6 +244,7 @@ spops_status_t count_stats(Context* ctx, const int64_t* cnt, int64_t len, int64_
   s.mn = h_min;
   s.mx = h_max;
   s.ave = (double)nnz / (double)len;
+  s.sq = h_var;
   s.var = h_var / (double)len;
   s.p = h_best == ~0ULL ? 1.0 : (double)(int64_t)h_best / (double)len;
   const double area_b = (double)(first + 0) / 2.0 + h_trap;
@@ -360,6 +361,19 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
 }
 
 }  // namespace
+
+spops_status_t count_summary(Context* ctx, const int64_t* cnt, int64_t len, int64_t nnz, CountSummary* out) {
+  CountStats s;
+  SPOPS_TRY(count_stats(ctx, cnt, len, nnz, &s));
+  out->nz = s.nz;
+  out->mn = s.mn;
+  out->mx = s.mx;
+  out->ave = s.ave;
+  out->sq = s.sq;
+  out->p = s.p;
+  out->gini = s.gini;
+  return SPOPS_OK;
+}
 
 spops_status_t csr_features(Context* ctx, Matrix* A, spops_features_t* f) {
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "features: needs a CSR matrix");

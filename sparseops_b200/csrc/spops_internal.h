@@ -364,6 +364,14 @@ spops_status_t rowwise_spgemm(Context* ctx, Matrix* A, Matrix* B, bool sort_outp
 spops_status_t topk_spgemm(Context* ctx, Matrix* A, int64_t top_k, Matrix** C);
 // adjoint.cu: A^T as a CSR handle owned by A (built once, values refreshed)
 spops_status_t csr_transpose_view(Context* ctx, Matrix* A, Matrix** view);
+// features.cu: statistics of a device count vector of length len whose
+// entries sum to nnz -- non-zero count, min, max, mean, the sum of squared
+// deviations from the mean, the P-ratio and the Gini coefficient
+struct CountSummary {
+  int64_t nz = 0, mn = 0, mx = 0;
+  double ave = 0, sq = 0, p = 0, gini = 0;
+};
+spops_status_t count_summary(Context* ctx, const int64_t* cnt, int64_t len, int64_t nnz, CountSummary* out);
 // batched.cu
 spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k, double beta,
                         void* Y, int64_t ldy);

@@ -390,6 +390,29 @@ def matrix_features(csr: CSR_Matrix) -> dict:
     return f.as_dict()
 
 
+def matrix_tile_features(csr: CSR_Matrix, num_blocks: int = 256, maps: bool = False):
+    """Tile features of the matrix, on the device: the tile part of the
+    reference's MTX::MtxLoad / CalculateTilesFeatures and the row distance of
+    CalculateTilesExtraFeatures (src/sparse_features.cpp:181-265, 484-625,
+    783-846, 943-965) on a num_blocks x num_blocks grid (MAT_TILE_SIZE = 256).
+    Returns a dict (names of spops_tile_features_t); with maps=True also the
+    per-tile arrays (num_blocks x num_blocks) and per-block arrays as a second
+    dict (names of spops_tile_maps_t)."""
+    h = csr.device()
+    f = _lib.TileFeatures()
+    B = 256 if num_blocks <= 0 else int(num_blocks)
+    arrays, m = {}, None
+    if maps:
+        m = _lib.TileMaps()
+        for name, per_tile, integer in _lib.TILE_MAP_FIELDS:
+            a = np.zeros((B, B) if per_tile else B, np.int64 if integer else np.float64)
+            arrays[name] = a
+            setattr(m, name, a.ctypes.data)
+    call("spops_matrix_tile_features", h.ctx.follow_torch().handle, h.handle, i64(B), C.byref(f),
+         C.byref(m) if m is not None else None)
+    return (f.as_dict(), arrays) if maps else f.as_dict()
+
+
 _FORMAT_NAMES = {v: k for k, v in _lib.FORMATS.items()}
 
 

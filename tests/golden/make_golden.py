@@ -233,6 +233,26 @@ def main():
         g[f"feat{k}_nc"] = np.int64(fnc)
         g[f"feat{k}_out"] = R.features(frp, fci, fv, fnc)
 
+    # ---- tile features (MtxLoad's tile counts, CalculateTilesFeatures and
+    # CalculateTilesExtraFeatures on the 256 x 256 grid): the three matrices
+    # above and a 3000 x 2500 one with uneven blocks, unsorted rows and
+    # repeated entries
+    rng = np.random.default_rng(92)
+    rp, ci = [0], []
+    for r in range(3000):
+        k = int(rng.integers(0, 30)) if rng.random() < 0.9 else int(rng.integers(100, 400))
+        cols = list(rng.integers(0, 2500, k))
+        if k and rng.random() < 0.2:
+            cols.append(cols[0])
+        ci += cols
+        rp.append(len(ci))
+    tcases = cases + [(np.array(rp), np.array(ci), np.ones(len(ci)), 2500)]
+    g["tile3_rp"], g["tile3_ci"] = np.array(rp, np.int64), np.array(ci, np.int64)
+    g["tile3_nc"] = np.int64(2500)
+    for k, (frp, fci, fv, fnc) in enumerate(tcases):
+        sc, ti, td, bi, bd = R.tile_features(frp, fci, fv, fnc)
+        g[f"tile{k}_sc"], g[f"tile{k}_ti"], g[f"tile{k}_td"], g[f"tile{k}_bi"], g[f"tile{k}_bd"] = sc, ti, td, bi, bd
+
     # ---- Matrix Market files through the reference's read_csr_matrix
     for k, text in enumerate(mtx_cases()):
         with tempfile.NamedTemporaryFile("wb", suffix=".mtx", delete=False) as f:

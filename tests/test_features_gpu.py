@@ -88,3 +88,96 @@ def test_spops_auto(cuda, orc, timed):
         ref = orc.spmv_csr(rp, ci, v, x, 0.8, 0.7, y0)
         den = 0.8 * orc.absdot(rp, ci, v, x) + np.abs(0.7 * y0)
         assert (np.abs(yd.cpu().numpy() - ref) / den).max() <= 1e-12
+
+
+# ---------------------------------------------------------------- tile features
+def _tile_parts(f, arrays):
+    """The device result in the layout of the oracle / golden tuples."""
+    from sparseops_b200._lib import TILE_FEATURE_NAMES
+    sc = np.array([float(f[n]) for n in TILE_FEATURE_NAMES])
+    ti = np.stack([arrays[n].ravel() for n in ("tile_nnz", "tile_rows", "tile_cols", "tile_max_row_nnz")])
+    td = np.stack([arrays[n].ravel() for n in ("tile_ave_row_nnz", "tile_std_row_nnz")])
+    bi = np.stack([arrays[n] for n in ("rb_nnz", "rb_max_row_nnz", "cb_nnz", "cb_max_col_nnz")])
+    bd = np.stack([arrays[n] for n in ("rb_ave_row_nnz", "rb_std_row_nnz", "cb_ave_col_nnz", "cb_std_col_nnz")])
+    return sc, ti, td, bi, bd
+
+
+def _tile_close(got, ref):
+    """Integers exact, floating-point values to 1e-12 relative, except the
+    variances (and deviations) of the tile, RB and CB counts: the reference
+    adds the len squared deviations one after another, so its own result is
+    only known to the bound of recursive summation, (len - 1) * 2^-53 times
+    the sum, which for 65,536 or 1,048,576 tiles is above 1e-12; the device
+    sums in a tree.  Those three pairs are held to that bound."""
+    sc_g, sc_r = np.asarray(got[0], np.float64), np.asarray(ref[0], np.float64)
+    B = int(sc_r[0])
+    spread = {}
+    for var_i, std_i, L in ((13, 14, B * B), (19, 20, B), (25, 26, B)):
+        total = sc_r[var_i] * L + 1.0  # the sum of squared deviations
+        tol = max(1e-12 * abs(sc_r[var_i]), (L - 1) * 2.0 ** -53 * total / L + 1e-300)
+        assert abs(sc_g[var_i] - sc_r[var_i]) <= tol, (var_i, sc_g[var_i], sc_r[var_i], tol)
+        assert abs(sc_g[std_i] ** 2 - sc_r[std_i] ** 2) <= tol + 1e-12 * sc_r[std_i] ** 2, (std_i, sc_g[std_i],
+                                                                                         sc_r[std_i])
+        spread.update({var_i: True, std_i: True})
+    keep = np.array([i not in spread for i in range(len(sc_r))])
+    for g, r, name in zip((sc_g[keep],) + tuple(got[1:]), (sc_r[keep],) + tuple(ref[1:]),
+                          ("sc", "ti", "td", "bi", "bd")):
+        g, r = np.asarray(g).reshape(r.shape), np.asarray(r)
+        if name == "sc":
+            assert np.array_equal(g[:11], r[:11]), (g[:11], r[:11])
+        if r.dtype == np.int64:
+            assert np.array_equal(g, r), name
+            continue
+        rel = np.abs(g - r) / np.maximum(np.abs(r), 1e-300)
+        ok = (rel <= 1e-12) | (g == r) | (np.isnan(g) & np.isnan(r))
+        assert ok.all(), (name, np.argwhere(~ok)[:5].ravel(), g[~ok][:5], r[~ok][:5])
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3])
+def test_tile_features_golden(cuda, golden, k):
+    """Against the reference's own MtxLoad + CalculateFeatures +
+    CalculateTilesExtraFeatures on its 256 x 256 grid: integers exact,
+    floating-point values to 1e-12 (the device sums in another order)."""
+    from sparseops_b200 import matrix_tile_features
+    from test_oracle_golden import tile_case
+    rp, ci, nc = tile_case(golden, k)
+    f, arrays = matrix_tile_features(_csr(rp, ci, np.ones(len(ci)), nc), maps=True)
+    ref = tuple(golden[f"tile{k}_{s}"] for s in ("sc", "ti", "td", "bi", "bd"))
+    _tile_close(_tile_parts(f, arrays), ref)
+
+
+@pytest.mark.parametrize("case,B", [("powerlaw", 256), ("laplacian", 256), ("graph", 256), ("narrow", 256),
+                                    ("i64", 256), ("powerlaw", 64), ("graph", 1024), ("powerlaw", 2048)])
+def test_tile_features_vs_oracle(cuda, orc, case, B):
+    """Against the oracle on larger matrices, other grid sizes (64 .. 2048
+    tiles per side), int64 indices and a matrix with fewer rows than tiles."""
+    from sparseops_b200 import matrix_tile_features
+    if case == "powerlaw":
+        rp, ci, v = synth.powerlaw(60000, hi=4000, seed=22)
+        nc = len(rp) - 1
+    elif case == "laplacian":
+        rp, ci, v = synth.laplacian_2d(300)
+        nc = len(rp) - 1
+    elif case == "graph":
+        rp, ci, v = synth.symmetric_graph(40000, 12.0, seed=7)
+        nc = len(rp) - 1
+    elif case == "narrow":  # 100 rows: every row block but the first 100 is empty
+        rng = np.random.default_rng(4)
+        lens = rng.integers(0, 300, 100)
+        rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+        ci = rng.integers(0, 70000, int(rp[-1])).astype(np.int32)
+        v, nc = np.ones(len(ci)), 70000
+    else:
+        rp, ci, v = synth.powerlaw(30000, hi=2000, seed=13)
+        rp, ci = rp.astype(np.int64), ci.astype(np.int64)
+        nc = len(rp) - 1
+    f, arrays = matrix_tile_features(_csr(rp, ci, v, nc), num_blocks=B, maps=True)
+    _tile_close(_tile_parts(f, arrays), orc.tile_features(rp.astype(np.int64), ci.astype(np.int64), nc, B))
+
+
+def test_tile_features_refusals(cuda):
+    from sparseops_b200 import SpOpsError, matrix_tile_features
+    rp, ci, v = synth.laplacian_2d(20)
+    with pytest.raises(SpOpsError) as e:
+        matrix_tile_features(_csr(rp, ci, v, len(rp) - 1), num_blocks=4096)
+    assert e.value.status == 5

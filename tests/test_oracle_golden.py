@@ -135,6 +135,37 @@ def test_features_golden(golden, orc, k):
     assert np.all(both_nan | (rel <= 1e-12) | (got == ref))
 
 
+def tile_case(golden, k):
+    """(rp, ci, ncols) of tile-feature case k."""
+    if k < 3:
+        return golden[f"feat{k}_rp"], golden[f"feat{k}_ci"], int(golden[f"feat{k}_nc"])
+    return golden[f"tile{k}_rp"], golden[f"tile{k}_ci"], int(golden[f"tile{k}_nc"])
+
+
+def assert_tile_close(got, golden, k):
+    """Tile features (scalars, tile maps, block maps) against the reference's
+    own: integers exact, floating-point values to 1e-12 relative."""
+    for part, name in zip(got, ("sc", "ti", "td", "bi", "bd")):
+        ref = golden[f"tile{k}_{name}"]
+        part = np.asarray(part).reshape(ref.shape)
+        if name == "sc":
+            assert np.array_equal(part[:11], ref[:11]), (part[:11], ref[:11])
+        if ref.dtype == np.int64:
+            assert np.array_equal(part, ref), name
+            continue
+        rel = np.abs(part - ref) / np.maximum(np.abs(ref), 1e-300)
+        ok = (rel <= 1e-12) | (part == ref) | (np.isnan(part) & np.isnan(ref))
+        assert ok.all(), (name, np.argwhere(~ok)[:5].ravel(), part[~ok][:5], ref[~ok][:5])
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3])
+def test_tile_features_golden(golden, orc, k):
+    """The restated tile features against the reference's MtxLoad +
+    CalculateFeatures + CalculateTilesExtraFeatures (256 x 256 tiles)."""
+    rp, ci, nc = tile_case(golden, k)
+    assert_tile_close(orc.tile_features(rp, ci, nc), golden, k)
+
+
 @pytest.mark.parametrize("kf", [1, 2, 3])
 def test_spgemm_rowwise_golden(golden, orc, kf):
     """Row-wise LeSpGEMM (src/spgemm.cpp:683): the restatement keeps every
