@@ -16,8 +16,11 @@ the measured HBM copy bandwidth (MEASURED_PEAKS.json).  The matrix (about
 
   value     device-resident: matrix, x and y already in HBM; K back-to-back
             SpMVs timed with CUDA events on the launching stream.
-  e2e       the C ABI host path (spops_spmv_host): pinned host x uploaded, the
-            SpMV, y downloaded, every step.
+  e2e       the C ABI host path: pinned host x uploaded, the SpMV, y
+            downloaded, every step.  The value queues the steps as
+            independent requests (spops_spmv_host_async, so one step's upload
+            overlaps the previous step's SpMV and download); e2e.blocking is
+            the one-call-at-a-time spops_spmv_host.
   cpu_baseline  the reference's own OpenMP CSR kernel (oracle/_ref, compiled
             from the reference sources; kernel_flag 2) on this host's cores,
             on a bounded sample of the same workload (rank 0, N = 1 only).
@@ -58,6 +61,28 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return PEAK_FALLBACK, "fallback"
+
+
+class quiet_stdout:
+    """Sends what native code writes to file descriptor 1 (the reference's own
+    progress lines) to stderr while it is active, so that stdout holds only
+    the one JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        self.libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
 
 
 def workload(rows=N_ROWS):
@@ -572,30 +597,31 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference library (oracle/_ref) not built"}))
         return 0
     threads = os.cpu_count()
-    R = Reference(threads=threads)
     n = len(rp) - 1
     full = spmv_bytes(n, n, len(ci))
-    y = np.zeros(n)
-    t0 = time.perf_counter()
-    R.spmv_csr(rp, ci, v, x, 1.0, 0.0, y, flag=2)
-    t_full = time.perf_counter() - t0
-    # each step is a bounded sample: the whole matrix if K steps fit ~2 minutes
-    budget = 120.0 / max(1, args.steps + args.warmup)
-    if t_full <= budget:
-        m, sample = n, "whole matrix per step"
-    else:
-        m = max(1, int(n * budget / t_full))
-        sample = f"rows [0,{m}) of {n} per step"
-    rps, cis, vs = rp[:m + 1], ci[:rp[m]], v[:rp[m]]
-    touched = int(np.count_nonzero(np.bincount(cis, minlength=n))) if m < n else n
-    nbytes = 4 * (m + 1) + 12 * int(rps[-1]) + 8 * touched + 8 * m if m < n else full
-    ys = np.zeros(m)
-    for _ in range(args.warmup):
-        R.spmv_csr(rps, cis, vs, x, 1.0, 0.0, None, flag=2, out=ys)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        R.spmv_csr(rps, cis, vs, x, 1.0, 0.0, None, flag=2, out=ys)
-    dt = (time.perf_counter() - t0) / args.steps
+    with quiet_stdout():
+        R = Reference(threads=threads)
+        y = np.zeros(n)
+        t0 = time.perf_counter()
+        R.spmv_csr(rp, ci, v, x, 1.0, 0.0, y, flag=2)
+        t_full = time.perf_counter() - t0
+        # each step is a bounded sample: the whole matrix if K steps fit ~2 minutes
+        budget = 120.0 / max(1, args.steps + args.warmup)
+        if t_full <= budget:
+            m, sample = n, "whole matrix per step"
+        else:
+            m = max(1, int(n * budget / t_full))
+            sample = f"rows [0,{m}) of {n} per step"
+        rps, cis, vs = rp[:m + 1], ci[:rp[m]], v[:rp[m]]
+        touched = int(np.count_nonzero(np.bincount(cis, minlength=n))) if m < n else n
+        nbytes = 4 * (m + 1) + 12 * int(rps[-1]) + 8 * touched + 8 * m if m < n else full
+        ys = np.zeros(m)
+        for _ in range(args.warmup):
+            R.spmv_csr(rps, cis, vs, x, 1.0, 0.0, None, flag=2, out=ys)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            R.spmv_csr(rps, cis, vs, x, 1.0, 0.0, None, flag=2, out=ys)
+        dt = (time.perf_counter() - t0) / args.steps
     gbs = nbytes / dt / 1e9
     peak, _ = peaks()
     out = {
@@ -657,22 +683,23 @@ def run_section(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
     ctx = default_context(0)
-    if args.section == "batched":
-        res = bench_batched(ctx, dev)
-    elif args.section == "fwd_bwd":
-        res = bench_fwd_bwd(ctx, dev)
-    elif args.section == "mtx":
-        res = bench_mtx(not args.no_cpu_baseline)
-    elif args.section == "spgemm":
-        res = bench_spgemm(dev, not args.no_cpu_baseline)
-    elif args.section == "features":
-        from sparseops_b200 import CSR_Matrix
-        rp, ci, v, _ = workload(args.rows)
-        A = CSR_Matrix(len(rp) - 1, len(rp) - 1, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
-                       torch.from_numpy(v).to(dev))
-        res = bench_features(A, not args.no_cpu_baseline, rp, ci)
-    else:
-        raise SystemExit(f"unknown section {args.section}")
+    with quiet_stdout():
+        if args.section == "batched":
+            res = bench_batched(ctx, dev)
+        elif args.section == "fwd_bwd":
+            res = bench_fwd_bwd(ctx, dev)
+        elif args.section == "mtx":
+            res = bench_mtx(not args.no_cpu_baseline)
+        elif args.section == "spgemm":
+            res = bench_spgemm(dev, not args.no_cpu_baseline)
+        elif args.section == "features":
+            from sparseops_b200 import CSR_Matrix
+            rp, ci, v, _ = workload(args.rows)
+            A = CSR_Matrix(len(rp) - 1, len(rp) - 1, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
+                           torch.from_numpy(v).to(dev))
+            res = bench_features(A, not args.no_cpu_baseline, rp, ci)
+        else:
+            raise SystemExit(f"unknown section {args.section}")
     print(json.dumps({"section": args.section, args.section: res}))
     return 0
 
@@ -741,29 +768,50 @@ def run_ours(args):
         dist.barrier()
     value = whole_job_gbs(world, nbytes, ms)
 
-    # ---- e2e: the host path through the C ABI (pinned x in, y out, per step)
-    xh = torch.from_numpy(x).pin_memory()
-    yh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    # ---- e2e: the host path through the C ABI, pinned x in and y out every
+    # step.  Headline: spops_spmv_host_async with the steps queued back to
+    # back as independent requests (two pinned x / y pairs used in turn), so a
+    # step's upload overlaps the previous step's SpMV and download; beside it
+    # the blocking spops_spmv_host, one step after the other.
+    xh = [torch.from_numpy(x).pin_memory() for _ in range(2)]
+    yh = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(2)]
     e2e_steps = max(3, min(args.steps, 200))
 
-    def step_host():
-        call("spops_spmv_host", ctx.handle, dbl(1.0), h.handle, vp(xh.data_ptr()), dbl(0.0), vp(yh.data_ptr()))
+    def step_blocking(i):
+        call("spops_spmv_host", ctx.handle, dbl(1.0), h.handle, vp(xh[0].data_ptr()), dbl(0.0),
+             vp(yh[0].data_ptr()))
 
-    for _ in range(max(3, args.warmup // 10)):
-        step_host()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        step_host()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ems = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, dev)
+    def step_queued(i):
+        call("spops_spmv_host_async", ctx.handle, dbl(1.0), h.handle, vp(xh[i & 1].data_ptr()), dbl(0.0),
+             vp(yh[i & 1].data_ptr()))
+
+    def host_wait():
+        call("spops_spmv_host_wait", ctx.handle)
+
+    def time_host(step):
+        for i in range(max(3, args.warmup // 10)):
+            step(i)
+        host_wait()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(e2e_steps):
+            step(i)
+        host_wait()  # every queued upload, SpMV and download has finished
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, dev)
+
+    bms = time_host(step_blocking)
+    e2e_blocking = whole_job_gbs(world, nbytes, bms)
+    yh[0].zero_()
+    yh[1].zero_()
+    ems = time_host(step_queued)
     e2e = whole_job_gbs(world, nbytes, ems)
-    # correctness spot check of the e2e result against the device result (the
-    # window variants may differ at rounding level between runs)
-    e2e_diff = float(((yh.to(dev) - yd).norm() / yd.norm().clamp_min(1e-300)).item())
+    # correctness spot check of both queued results against the device result
+    # (the window variants may differ at rounding level between runs)
+    e2e_diff = max(float(((y.to(dev) - yd).norm() / yd.norm().clamp_min(1e-300)).item()) for y in yh)
     ok = e2e_diff <= 1e-12
 
     peak, peak_kind = peaks()
@@ -771,7 +819,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            gbs, info = cpu_reference_sample(rp, ci, v, x, budget_s=args.cpu_budget)
+            with quiet_stdout():
+                gbs, info = cpu_reference_sample(rp, ci, v, x, budget_s=args.cpu_budget)
             cpu = dict(value=round(gbs, 3), unit="GB/s", **info)
         except Exception as e:  # keep the line even if the baseline cannot run
             cpu = {"value": None, "unit": "GB/s", "error": str(e)[:200]}
@@ -785,7 +834,8 @@ def run_ours(args):
                         ("features", lambda: bench_features(A, not args.no_cpu_baseline, rp, ci))):
             t0 = time.time()
             try:
-                extra[key] = fn()
+                with quiet_stdout():
+                    extra[key] = fn()
             except Exception as e:
                 extra[key] = {"error": str(e)[:200]}
             log(f"{key}: {time.time() - t0:.1f}s")
@@ -811,7 +861,11 @@ def run_ours(args):
                      "traffic": traffic},
         "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                 "steps": e2e_steps, "matches_device_result": ok, "normwise_diff_vs_device": e2e_diff,
-                "path": "spops_spmv_host (matrix resident after first upload)"},
+                "ms_per_step": round(ems, 4),
+                "path": "spops_spmv_host_async, steps queued back to back as independent requests; matrix "
+                        "resident after first upload",
+                "blocking": {"value": round(e2e_blocking, 2), "ms_per_step": round(bms, 4),
+                             "path": "spops_spmv_host, each step waits for its y"}},
         # tile kernel + its calibrator per SpMV; one launch for the segment and window kernels
         "gpu_launches": args.steps * (1 if args.csr_variant in (2, 3, 4, 7, 8, 9) else 2),
         "clocks": ck,

@@ -258,6 +258,18 @@ spops_status_t spops_spmv(spops_context_t ctx, double alpha, spops_matrix_t A, c
  * The drop-in path of the header shim (host pointers in, host pointers out). */
 spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x_host,
                                double beta, void* y_host);
+/* The same, queued: for a stream of independent requests (a server's SpMV
+ * calls) whose host x and y are page-locked.  Returns once the upload, the
+ * SpMV and the download are enqueued; the context alternates two device
+ * slots, so request k + 1's upload runs while request k computes and its y
+ * comes back.  x must stay unchanged and y unread until
+ * spops_spmv_host_wait(ctx) returns (or a spops_spmv_host call, which waits
+ * first).  With pageable x or y the call runs to completion as
+ * spops_spmv_host does.  No reference counterpart: SpOps_<fmt> returns when
+ * y is written. */
+spops_status_t spops_spmv_host_async(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x_host,
+                                     double beta, void* y_host);
+spops_status_t spops_spmv_host_wait(spops_context_t ctx);
 /* Multi-RHS: Y = alpha*A*X + beta*Y with X [cols x k], Y [rows x k],
  * row-major with leading dimensions ldx, ldy (>= k).  No reference
  * counterpart (the reference has no SpMM); equals k SpOps_csr calls. */

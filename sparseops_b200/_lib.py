@@ -153,6 +153,8 @@ _SIGS = {
     "spops_csr_spmv_noalloc": [i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, dbl, vp, dbl, vp, vp],
     "spops_spmv": [vp, dbl, vp, vp, dbl, vp],
     "spops_spmv_host": [vp, dbl, vp, vp, dbl, vp],
+    "spops_spmv_host_async": [vp, dbl, vp, vp, dbl, vp],
+    "spops_spmv_host_wait": [vp],
 }
 _RESTYPE = {"spops_last_error": C.c_char_p, "spops_status_string": C.c_char_p, "spops_abi_version": C.c_int}
 

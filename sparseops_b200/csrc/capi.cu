@@ -452,9 +452,24 @@ spops_status_t spops_spmv(spops_context_t ctx, double alpha, spops_matrix_t A, c
   }
 }
 
+spops_status_t spops_spmv_host_wait(spops_context_t ctx) {
+  if (!ctx) return fail(SPOPS_ERR_INVALID, "spops_spmv_host_wait: null context");
+  if (!ctx->a_pending) return SPOPS_OK;
+  DeviceGuard g(ctx->device);
+  cudaError_t e1 = ctx->in_stream ? cudaStreamSynchronize(ctx->in_stream) : cudaSuccess;
+  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  cudaError_t e3 = ctx->copy_stream ? cudaStreamSynchronize(ctx->copy_stream) : cudaSuccess;
+  ctx->a_pending = false;
+  SPOPS_CUDA(e1);
+  SPOPS_CUDA(e2);
+  SPOPS_CUDA(e3);
+  return SPOPS_OK;
+}
+
 spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x_host,
                                double beta, void* y_host) {
   if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_spmv_host: null context/matrix");
+  SPOPS_TRY(spops_spmv_host_wait(ctx));
   DeviceGuard g(ctx->device);
   const size_t xb = (size_t)A->cols * A->vsize(), yb = (size_t)A->rows * A->vsize();
   if (ctx->xbuf.bytes < xb) SPOPS_TRY(ctx->xbuf.alloc(xb));
@@ -504,6 +519,76 @@ spops_status_t spops_spmv_host(spops_context_t ctx, double alpha, spops_matrix_t
   if (yb) SPOPS_CUDA(cudaMemcpyAsync(y_host, ctx->ybuf.p, yb, cudaMemcpyDeviceToHost, st));
   SPOPS_CUDA(cudaStreamSynchronize(st));
   (void)reserve_pinned;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_spmv_host_async(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x_host,
+                                     double beta, void* y_host) {
+  if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_spmv_host_async: null context/matrix");
+  const size_t vs = A->vsize(), xb = (size_t)A->cols * vs, yb = (size_t)A->rows * vs;
+  if ((xb && !x_host) || (yb && !y_host)) return fail(SPOPS_ERR_INVALID, "spops_spmv_host_async: null vector");
+  DeviceGuard g(ctx->device);
+  auto pinned = [](const void* p) {
+    cudaPointerAttributes a{};
+    const bool ok = p && cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return ok;
+  };
+  if ((xb && !pinned(x_host)) || (yb && !pinned(y_host)))  // copies from pageable memory block the host anyway
+    return spops_spmv_host(ctx, alpha, A, x_host, beta, y_host);
+  constexpr int kHostParts = 8;
+  if (!ctx->in_stream) SPOPS_CUDA(cudaStreamCreateWithFlags(&ctx->in_stream, cudaStreamNonBlocking));
+  if (!ctx->copy_stream) SPOPS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; ++i)
+    for (cudaEvent_t* e : {&ctx->a_in[i], &ctx->a_read[i], &ctx->a_out[i]})
+      if (!*e) SPOPS_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  while ((int)ctx->part_events.size() < kHostParts) {
+    cudaEvent_t e;
+    SPOPS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->part_events.push_back(e);
+  }
+  const int s = ctx->a_next;
+  ctx->a_next ^= 1;
+  cudaStream_t st = ctx->stream, in = ctx->in_stream, out = ctx->copy_stream;
+  if (ctx->axbuf[s].bytes < xb || ctx->aybuf[s].bytes < yb) {  // the slot grows: its last call must be done
+    SPOPS_CUDA(cudaEventSynchronize(ctx->a_read[s]));
+    SPOPS_CUDA(cudaEventSynchronize(ctx->a_out[s]));
+    if (ctx->axbuf[s].bytes < xb) SPOPS_TRY(ctx->axbuf[s].alloc(xb));
+    if (ctx->aybuf[s].bytes < yb) SPOPS_TRY(ctx->aybuf[s].alloc(yb));
+  }
+  void* xd = ctx->axbuf[s].p;
+  char* yd = ctx->aybuf[s].as<char>();
+  ctx->a_pending = true;
+  // upload once the slot's previous SpMV has read x (and its download has read y)
+  SPOPS_CUDA(cudaStreamWaitEvent(in, ctx->a_read[s], 0));
+  if (beta != 0.0) SPOPS_CUDA(cudaStreamWaitEvent(in, ctx->a_out[s], 0));
+  if (xb) SPOPS_CUDA(cudaMemcpyAsync(xd, x_host, xb, cudaMemcpyHostToDevice, in));
+  if (beta != 0.0 && yb) SPOPS_CUDA(cudaMemcpyAsync(yd, y_host, yb, cudaMemcpyHostToDevice, in));
+  SPOPS_CUDA(cudaEventRecord(ctx->a_in[s], in));
+  // the SpMV after the upload and after the slot's previous download of y
+  SPOPS_CUDA(cudaStreamWaitEvent(st, ctx->a_in[s], 0));
+  SPOPS_CUDA(cudaStreamWaitEvent(st, ctx->a_out[s], 0));
+  int used = 0;
+  auto send = [&](int64_t r0, int64_t r1) -> spops_status_t {  // rows [r0, r1) of y back to the host
+    cudaEvent_t e = ctx->part_events[(size_t)(used++ % kHostParts)];
+    SPOPS_CUDA(cudaEventRecord(e, st));
+    SPOPS_CUDA(cudaStreamWaitEvent(out, e, 0));
+    if (r1 > r0)
+      SPOPS_CUDA(cudaMemcpyAsync(static_cast<char*>(y_host) + r0 * vs, yd + r0 * vs, (size_t)(r1 - r0) * vs,
+                                 cudaMemcpyDeviceToHost, out));
+    return SPOPS_OK;
+  };
+  if (A->format == SPOPS_FMT_CSR && !A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+  const bool piped = A->format == SPOPS_FMT_CSR && A->rows >= (int64_t)1 << 20 && A->nnz > 0 &&
+                     ctx->csr_variant == 0 && csr_tile_usable(A, 0);
+  if (piped) {
+    SPOPS_TRY(csr_tile_spmv_parts(ctx, A, kHostParts, alpha, xd, beta, yd, send));
+  } else {
+    SPOPS_TRY(spops_spmv(ctx, alpha, A, xd, beta, yd));
+    SPOPS_TRY(send(0, A->rows));
+  }
+  SPOPS_CUDA(cudaEventRecord(ctx->a_read[s], st));
+  SPOPS_CUDA(cudaEventRecord(ctx->a_out[s], out));
   return SPOPS_OK;
 }
 

@@ -132,6 +132,8 @@ spops_status_t spops_destroy(spops_context_t c) {
   if (!c) return SPOPS_OK;
   DeviceGuard g(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->in_stream) cudaStreamSynchronize(c->in_stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   c->scratch.release();
   c->errword.release();
   c->xbuf.release();
@@ -141,6 +143,13 @@ spops_status_t spops_destroy(spops_context_t c) {
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->copy_stream = nullptr;
   if (c->pinned) cudaFreeHost(c->pinned);
+  for (int i = 0; i < 2; ++i) {
+    c->axbuf[i].release();
+    c->aybuf[i].release();
+    for (cudaEvent_t e : {c->a_in[i], c->a_read[i], c->a_out[i]})
+      if (e) cudaEventDestroy(e);
+  }
+  if (c->in_stream) cudaStreamDestroy(c->in_stream);
   for (cudaEvent_t e : c->file_events) cudaEventDestroy(e);
   for (void* b : c->file_stage) cudaFreeHost(b);
   if (c->pool) {

@@ -65,6 +65,14 @@ struct Context {
   // second stream and per-range events of the pipelined spops_spmv_host
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> part_events;
+  // spops_spmv_host_async: two slots of device x / y used in turn, the
+  // upload stream, and per slot the events that order its upload (in), the
+  // SpMV's last read of x / y (read) and the download of y (out)
+  DevBuf axbuf[2], aybuf[2];
+  cudaStream_t in_stream = nullptr;
+  cudaEvent_t a_in[2] = {nullptr, nullptr}, a_read[2] = {nullptr, nullptr}, a_out[2] = {nullptr, nullptr};
+  int a_next = 0;
+  bool a_pending = false;
   // pinned staging of the Matrix Market reader (file chunks on their way to
   // the device) and the event that frees each buffer for its next chunk
   std::vector<void*> file_stage;

@@ -32,7 +32,7 @@ def _is_cuda_tensor(a) -> bool:
 def _ptr(a):
     if a is None:
         return None
-    if _is_cuda_tensor(a):
+    if _is_cuda_tensor(a) or (torch is not None and isinstance(a, torch.Tensor) and a.is_contiguous()):
         return vp(a.data_ptr())
     if isinstance(a, np.ndarray):
         return a.ctypes.data_as(vp)
@@ -198,6 +198,24 @@ def _spmv(alpha, A: Matrix_Features, x, beta, y):
         call("spops_spmv_host", ctx.handle, dbl(alpha), h.handle, _ptr(np.ascontiguousarray(x)), dbl(beta),
              _ptr(y))
     return y
+
+
+def spmv_host_async(alpha, A: Matrix_Features, x, beta, y):
+    """y = alpha*A*x + beta*y with host x and y, queued (spops_spmv_host_async):
+    returns before y is written.  For a stream of independent requests with
+    page-locked x and y (torch CPU tensors from pin_memory()), consecutive
+    calls overlap one request's upload with the previous one's SpMV and
+    download.  Keep x unchanged and y unread until spmv_host_wait()."""
+    h = A.device()
+    call("spops_spmv_host_async", h.ctx.handle, dbl(alpha), h.handle, _ptr(x), dbl(beta), _ptr(y))
+    return y
+
+
+def spmv_host_wait(A: Matrix_Features = None, ctx=None):
+    """Completes every spmv_host_async call queued on the matrix's (or the
+    given, or the default) context."""
+    ctx = A.device().ctx if A is not None else (ctx or default_context())
+    call("spops_spmv_host_wait", ctx.handle)
 
 
 class DeviceCSR(CSR_Matrix):

@@ -321,3 +321,46 @@ def test_host_path_pipelined(cuda, orc, pinned):
         assert torch.equal(yh, yd.cpu())
         yref = orc.spmv_csr(rp.astype(np.int64), ci.astype(np.int64), v, x, alpha, beta, y0)
         assert _err(orc, rp.astype(np.int64), ci.astype(np.int64), v, x, yh.numpy(), yref, beta, y0, alpha) <= TOL64
+
+
+@pytest.mark.parametrize("rows,pinned", [(1_300_000, True), (50_000, True), (50_000, False)])
+def test_host_path_queued(cuda, rows, pinned):
+    """spops_spmv_host_async: six independent requests (different x, alpha,
+    beta and y0, separate host buffers) queued back to back through the two
+    device slots, then one wait; every y equals the device-resident SpMV of
+    its own request bit for bit.  Covers the ranged path (rows >= 2^20), the
+    single-range path and pageable buffers (which run each call to the end)."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, default_context, spmv_host_async, spmv_host_wait
+    from sparseops_b200._lib import call, dbl, vp
+    rp, ci, v = synth.powerlaw(rows, mu=1.5, sigma=1.0, hi=3000, seed=10)
+    n = len(rp) - 1
+    ctx = default_context()
+    A = CSR_Matrix(n, n, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda())
+    h = A.device(ctx)
+    reqs = [(1.0, 0.0), (0.5, 0.25), (2.0, 0.0), (-1.0, 1.0), (1.0, 0.0), (0.75, -0.5)]
+    xs, y0s, yhs = [], [], []
+    for i, (alpha, beta) in enumerate(reqs):
+        x, y0 = synth.uniform(n, 20 + i), synth.uniform(n, 40 + i)
+        xh, yh = torch.from_numpy(x.copy()), torch.from_numpy(y0.copy())
+        if pinned:
+            xh, yh = xh.pin_memory(), yh.pin_memory()
+        xs.append(x)
+        y0s.append(y0)
+        yhs.append((xh, yh))
+    for (alpha, beta), (xh, yh) in zip(reqs, yhs):
+        spmv_host_async(alpha, A, xh, beta, yh)
+    spmv_host_wait(A)
+    for (alpha, beta), x, y0, (_, yh) in zip(reqs, xs, y0s, yhs):
+        xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+        call("spops_spmv", ctx.handle, dbl(alpha), h.handle, vp(xd.data_ptr()), dbl(beta), vp(yd.data_ptr()))
+        torch.cuda.synchronize()
+        assert torch.equal(yh, yd.cpu()), (alpha, beta)
+    # a blocking call after queued ones waits for them first
+    xh, yh = yhs[0][0], torch.zeros(n, dtype=torch.float64)
+    spmv_host_async(1.0, A, yhs[1][0], 0.0, yhs[1][1])
+    call("spops_spmv_host", ctx.handle, dbl(1.0), h.handle, vp(xh.data_ptr()), dbl(0.0), vp(yh.data_ptr()))
+    xd, yd = torch.from_numpy(xs[0]).cuda(), torch.empty(n, dtype=torch.float64, device="cuda")
+    call("spops_spmv", ctx.handle, dbl(1.0), h.handle, vp(xd.data_ptr()), dbl(0.0), vp(yd.data_ptr()))
+    torch.cuda.synchronize()
+    assert torch.equal(yh, yd.cpu())
