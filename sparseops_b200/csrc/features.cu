@@ -45,70 +45,149 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double 
   atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
 
-template <typename I, typename V>
-__global__ void row_pass_kernel(const I* __restrict__ rp, const I* __restrict__ ci, const V* __restrict__ val,
-                                int64_t n, int64_t ncols, int64_t close_thr, int64_t* __restrict__ row_cnt,
-                                unsigned long long* __restrict__ col_cnt, unsigned long long* __restrict__ col_max_bits,
-                                unsigned long long* __restrict__ col_negmin_bits, unsigned char* __restrict__ diag_seen,
-                                Totals* __restrict__ tot) {
-  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  const int64_t s = rp[r], e = rp[r + 1];
-  unsigned long long lo = 0, up = 0, dg = 0, close = 0;
-  double dom = 0.0, maxd = -1.0, maxo = -1.0, rmax = 0.0, rmin = 0.0;
-  for (int64_t k = s; k < e; ++k) {
-    const int64_t c = (int64_t)ci[k];
-    const double a = fabs((double)val[k]);
-    const int64_t d = c - r;
-    diag_seen[d + n - 1] = 1;
-    if ((d < 0 ? -d : d) <= close_thr) ++close;
-    if (d == 0) {
-      ++dg;
-      dom += a;
-      maxd = a > maxd ? a : maxd;
-    } else {
-      if (d < 0) ++lo; else ++up;
-      dom -= a;
-      maxo = a > maxo ? a : maxo;
+// sums and maxima of one block's rows, then one global atomic per block
+// and field (the totals are few addresses that every row would hit)
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_max(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) {
+    const unsigned long long u = __shfl_xor_sync(0xffffffffu, v, o);
+    v = u > v ? u : v;
+  }
+  return v;
+}
+enum { kLower, kUpper, kDiagonal, kDominant, kClose, kHasDiag, kHasOff, kMaxDiag, kMaxOff, kRowVar, kHasRowVar,
+       kColVar, kHasColVar, kFields };
+__device__ __forceinline__ unsigned long long* total_field(Totals* t, int f) {
+  switch (f) {
+    case kLower: return &t->lower;
+    case kUpper: return &t->upper;
+    case kDiagonal: return &t->diagonal;
+    case kDominant: return &t->dominant;
+    case kClose: return &t->close;
+    case kHasDiag: return &t->has_diag;
+    case kHasOff: return &t->has_off;
+    case kMaxDiag: return &t->max_diag_bits;
+    case kMaxOff: return &t->max_off_bits;
+    case kRowVar: return &t->row_var_bits;
+    case kHasRowVar: return &t->has_row_var;
+    case kColVar: return &t->col_var_bits;
+    default: return &t->has_col_var;
+  }
+}
+// fields kMaxDiag .. kColVar combine by max (non-negative doubles as bits),
+// the flags by max too, the counts by sum
+__device__ __forceinline__ bool is_max_field(int f) { return f >= kHasDiag; }
+
+// per-thread values into the block's shared totals, then to the device
+__device__ void flush_totals(const unsigned long long (&v)[kFields], unsigned long long* sh, Totals* tot) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int f = 0; f < kFields; ++f) {
+    const unsigned long long w = is_max_field(f) ? warp_max(v[f]) : warp_sum(v[f]);
+    if (lane == 0 && w) {
+      if (is_max_field(f)) atomicMax(&sh[f], w); else atomicAdd(&sh[f], w);
     }
-    const double l = log10(a);
-    if (rmax < l) rmax = l;
-    if (a > 0.0 && rmin > l) rmin = l;
-    atomicAdd(col_cnt + c, 1ULL);
-    if (l > 0.0) atomic_max_nonneg(col_max_bits + c, l);
-    if (a > 0.0 && l < 0.0) atomic_max_nonneg(col_negmin_bits + c, -l);
   }
-  row_cnt[r] = e - s;
-  if (lo) atomicAdd(&tot->lower, lo);
-  if (up) atomicAdd(&tot->upper, up);
-  if (dg) {
-    atomicAdd(&tot->diagonal, dg);
-    atomicOr(&tot->has_diag, 1ULL);
-    atomic_max_nonneg(&tot->max_diag_bits, maxd);
+  __syncthreads();
+  if (threadIdx.x < kFields && sh[threadIdx.x]) {
+    const int f = threadIdx.x;
+    if (is_max_field(f)) atomicMax(total_field(tot, f), sh[f]); else atomicAdd(total_field(tot, f), sh[f]);
   }
-  if (e - s > dg) {
-    atomicOr(&tot->has_off, 1ULL);
-    atomic_max_nonneg(&tot->max_off_bits, maxo);
+}
+
+// A warp per row (rows w, w + W, ... for warp w of W): lanes take the
+// row's entries for the counts, maxima, log10 ranges, diagonal offsets and
+// column statistics, which do not depend on the order; the diagonal-dominance
+// sum is added by lane 0 in entry order, as the reference adds it.
+template <typename I, typename V>
+__global__ void __launch_bounds__(256) row_pass_kernel(const I* __restrict__ rp, const I* __restrict__ ci,
+                                                       const V* __restrict__ val, int64_t n, int64_t ncols,
+                                                       int64_t close_thr, int64_t* __restrict__ row_cnt,
+                                                       unsigned long long* __restrict__ col_cnt,
+                                                       unsigned long long* __restrict__ col_max_bits,
+                                                       unsigned long long* __restrict__ col_negmin_bits,
+                                                       unsigned char* __restrict__ diag_seen,
+                                                       Totals* __restrict__ tot) {
+  __shared__ unsigned long long sh[kFields];
+  if (threadIdx.x < kFields) sh[threadIdx.x] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t W = (int64_t)gridDim.x * (blockDim.x >> 5);
+  unsigned long long v[kFields] = {};
+  double maxd = -1.0, maxo = -1.0;  // this lane's largest |a| on / off the diagonal
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += W) {
+    const int64_t s = rp[r], e = rp[r + 1];
+    unsigned long long dg = 0;
+    double rmax = 0.0, rmin = 0.0;
+    for (int64_t k = s + lane; k < e; k += 32) {
+      const int64_t c = (int64_t)ci[k];
+      const double a = fabs((double)val[k]);
+      const int64_t d = c - r;
+      diag_seen[d + n - 1] = 1;
+      if ((d < 0 ? -d : d) <= close_thr) ++v[kClose];
+      if (d == 0) {
+        ++dg;
+        maxd = a > maxd ? a : maxd;
+      } else {
+        if (d < 0) ++v[kLower]; else ++v[kUpper];
+        maxo = a > maxo ? a : maxo;
+      }
+      const double l = log10(a);
+      if (rmax < l) rmax = l;
+      if (a > 0.0 && rmin > l) rmin = l;
+      atomicAdd(col_cnt + c, 1ULL);
+      if (l > 0.0) atomic_max_nonneg(col_max_bits + c, l);
+      if (a > 0.0 && l < 0.0) atomic_max_nonneg(col_negmin_bits + c, -l);
+    }
+    v[kDiagonal] += dg;
+    // the row's diagonal count and log10 range over the warp
+    const unsigned long long row_dg = warp_sum(dg);
+    for (int o = 16; o; o >>= 1) {
+      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+      rmin = fmin(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+    }
+    if (lane == 0) {
+      double dom = 0.0;
+      for (int64_t k = s; k < e; ++k) {
+        const double a = fabs((double)val[k]);
+        if ((int64_t)ci[k] == r) dom += a; else dom -= a;
+      }
+      row_cnt[r] = e - s;
+      if (dom > 0.0) ++v[kDominant];
+      if (row_dg) v[kHasDiag] = 1;
+      if ((unsigned long long)(e - s) > row_dg) v[kHasOff] = 1;
+      if (rmin != 0.0) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(rmax - rmin);
+        v[kRowVar] = b > v[kRowVar] ? b : v[kRowVar];
+        v[kHasRowVar] = 1;
+      }
+    }
   }
-  if (close) atomicAdd(&tot->close, close);
-  if (dom > 0.0) atomicAdd(&tot->dominant, 1ULL);
-  if (rmin != 0.0) {
-    atomic_max_nonneg(&tot->row_var_bits, rmax - rmin);
-    atomicOr(&tot->has_row_var, 1ULL);
-  }
+  if (maxd >= 0.0) v[kMaxDiag] = (unsigned long long)__double_as_longlong(maxd);
+  if (maxo >= 0.0) v[kMaxOff] = (unsigned long long)__double_as_longlong(maxo);
+  flush_totals(v, sh, tot);
 }
 
 __global__ void col_var_kernel(const unsigned long long* __restrict__ col_max_bits,
                                const unsigned long long* __restrict__ col_negmin_bits, int64_t ncols,
                                Totals* __restrict__ tot) {
+  __shared__ unsigned long long sh[kFields];
+  if (threadIdx.x < kFields) sh[threadIdx.x] = 0;
+  __syncthreads();
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= ncols) return;
-  const double mn = -__longlong_as_double((long long)col_negmin_bits[c]);
-  if (mn != 0.0) {
-    const double mx = __longlong_as_double((long long)col_max_bits[c]);
-    atomic_max_nonneg(&tot->col_var_bits, mx - mn);
-    atomicOr(&tot->has_col_var, 1ULL);
+  unsigned long long v[kFields] = {};
+  if (c < ncols) {
+    const double mn = -__longlong_as_double((long long)col_negmin_bits[c]);
+    if (mn != 0.0) {
+      const double mx = __longlong_as_double((long long)col_max_bits[c]);
+      v[kColVar] = (unsigned long long)__double_as_longlong(mx - mn);
+      v[kHasColVar] = 1;
+    }
   }
+  flush_totals(v, sh, tot);
 }
 
 __global__ void count_flags_kernel(const unsigned char* __restrict__ f, int64_t m, unsigned long long* __restrict__ out) {
@@ -137,15 +216,24 @@ struct NonZero {
 
 // smallest prefix (from the largest counts) whose row share plus entry share
 // reaches 1, with the reference's expressions: p = count / length,
-// q = taken entries / nnz, stop when p + q >= 1.
+// q = taken entries / nnz, stop when p + q >= 1.  Both shares and their
+// rounded sum grow with the prefix, so the first prefix that stops is found
+// by bisection; *best stays ~0 when none does.
 __global__ void p_ratio_kernel(const int64_t* __restrict__ cum, int64_t len, int64_t nnz,
                                unsigned long long* __restrict__ best) {
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x + 1;  // rows taken, 1..len
-  if (q > len) return;
-  const int64_t taken = cum[len - 1] - (len - q - 1 >= 0 ? cum[len - q - 1] : 0);
-  const double p_tmp = (double)q / (double)len;
-  const double one_minus_p = (double)taken / (double)nnz;
-  if (!(p_tmp + one_minus_p < 1.0)) atomicMin(best, (unsigned long long)q);
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  auto stops = [&](int64_t q) {
+    const int64_t taken = cum[len - 1] - (len - q - 1 >= 0 ? cum[len - q - 1] : 0);
+    const double p_tmp = (double)q / (double)len;
+    const double one_minus_p = (double)taken / (double)nnz;
+    return !(p_tmp + one_minus_p < 1.0);
+  };
+  int64_t lo = 1, hi = len + 1;  // the answer is in [lo, hi); hi = len + 1: none
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (stops(mid)) hi = mid; else lo = mid + 1;
+  }
+  *best = lo <= len ? (unsigned long long)lo : ~0ULL;
 }
 
 struct Trap {
@@ -154,26 +242,52 @@ struct Trap {
 };
 
 // symmetric pairs: entry (r, c), r != c, whose mirror (c, r) exists, and with
-// the same value printed with six decimals (sign kept, as the text is)
-template <typename V>
-__global__ void symm_kernel(const uint64_t* __restrict__ keys, const V* __restrict__ vals, int64_t m,
-                            unsigned long long* __restrict__ pat, unsigned long long* __restrict__ same) {
+// the same value printed with six decimals (sign kept, as the text is).
+// The keys are the CSR's (row, col) pairs sorted, which only reorders each
+// row's columns: the mirror (c, r) can only sit in row c's segment
+// [rp[c], rp[c+1]), searched by bisection.  Matches are counted per warp.
+template <typename I, typename V>
+__global__ void symm_kernel(const I* __restrict__ rp, const uint64_t* __restrict__ keys, const V* __restrict__ vals,
+                            int64_t m, unsigned long long* __restrict__ pat, unsigned long long* __restrict__ same) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= m) return;
-  const uint64_t k = keys[t];
-  const uint64_t r = k >> 32, c = k & 0xffffffffu;
-  if (r == c) return;
-  const uint64_t want = (c << 32) | r;
-  int64_t lo = 0, hi = m;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (keys[mid] < want) lo = mid + 1; else hi = mid;
+  bool hit = false, eq = false;
+  if (t < m) {
+    const uint64_t k = keys[t];
+    const uint64_t r = k >> 32, c = k & 0xffffffffu;
+    if (r != c) {
+      const uint64_t want = (c << 32) | r;
+      int64_t lo = (int64_t)rp[c], hi = (int64_t)rp[c + 1];
+      const int64_t end = hi;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < want) lo = mid + 1; else hi = mid;
+      }
+      if (lo < end && keys[lo] == want) {
+        hit = true;
+        const double a = (double)vals[t], b = (double)vals[lo];
+        eq = signbit(a) == signbit(b) && rint(fabs(a) * 1e6) == rint(fabs(b) * 1e6);
+      }
+    }
   }
-  if (lo < m && keys[lo] == want) {
-    atomicAdd(pat, 1ULL);
-    const double a = (double)vals[t], b = (double)vals[lo];
-    if (signbit(a) == signbit(b) && rint(fabs(a) * 1e6) == rint(fabs(b) * 1e6)) atomicAdd(same, 1ULL);
+  const unsigned bh = __ballot_sync(0xffffffffu, hit), be = __ballot_sync(0xffffffffu, eq);
+  if ((threadIdx.x & 31) == 0) {
+    if (bh) atomicAdd(pat, (unsigned long long)__popc(bh));
+    if (be) atomicAdd(same, (unsigned long long)__popc(be));
   }
+}
+
+// flags[0] = 1 when some row's columns are not strictly ascending
+template <typename I>
+__global__ void rows_unsorted_kernel(const I* __restrict__ rp, const I* __restrict__ ci, int64_t n,
+                                     unsigned int* __restrict__ flag) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t s = (int64_t)rp[r], e = (int64_t)rp[r + 1];
+  for (int64_t k = s + 1; k < e; ++k)
+    if (ci[k] <= ci[k - 1]) {
+      *flag = 1;
+      return;
+    }
 }
 
 template <typename I, typename V>
@@ -201,7 +315,7 @@ spops_status_t count_stats(Context* ctx, const int64_t* cnt, int64_t len, int64_
     *out = s;
     return SPOPS_OK;
   }
-  DevBuf sorted, cum, red, best, tmp;
+  PoolBuf sorted(ctx), cum(ctx), red(ctx), best(ctx), tmp(ctx);
   SPOPS_TRY(sorted.alloc((size_t)len * 8));
   SPOPS_TRY(cum.alloc((size_t)len * 8));
   SPOPS_TRY(red.alloc(64));
@@ -226,7 +340,7 @@ spops_status_t count_stats(Context* ctx, const int64_t* cnt, int64_t len, int64_
   SPOPS_CUDA(cudaMemsetAsync(rdd + 1, 0, 8, st));
   if (len > 1) SPOPS_CUDA(cub::DeviceReduce::Sum(tmp.p, b5, trap, rdd + 1, len - 1, st));
   SPOPS_CUDA(cudaMemsetAsync(best.p, 0xff, 8, st));
-  p_ratio_kernel<<<grid_of(len), 256, 0, st>>>(cum.as<int64_t>(), len, nnz, best.as<unsigned long long>());
+  p_ratio_kernel<<<1, 32, 0, st>>>(cum.as<int64_t>(), len, nnz, best.as<unsigned long long>());
   SPOPS_LAUNCH_CHECK();
   int64_t h_nz = 0, h_min = 0, h_max = 0;
   double h_var = 0, h_trap = 0;
@@ -264,7 +378,7 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
   f->nnz = nnz;
   if (n <= 0 || nc <= 0) return SPOPS_OK;
   const int64_t ndl = n + nc - 1;
-  DevBuf rcnt, ccnt, cmax, cmin, seen, tot, ccnt64, cnt_flags;
+  PoolBuf rcnt(ctx), ccnt(ctx), cmax(ctx), cmin(ctx), seen(ctx), tot(ctx), ccnt64(ctx);
   SPOPS_TRY(rcnt.alloc((size_t)n * 8));
   SPOPS_TRY(ccnt.alloc((size_t)nc * 8));
   SPOPS_TRY(cmax.alloc((size_t)nc * 8));
@@ -279,7 +393,7 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
   SPOPS_CUDA(cudaMemsetAsync(tot.p, 0, sizeof(Totals) + 64, st));
   Totals* T = tot.as<Totals>();
   unsigned long long* ndiag_d = reinterpret_cast<unsigned long long*>(tot.as<char>() + sizeof(Totals));
-  row_pass_kernel<I, V><<<grid_of(n, 128), 128, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n, nc,
+  row_pass_kernel<I, V><<<(unsigned)std::min<int64_t>((n + 7) / 8, (int64_t)ctx->num_sms * 8), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n, nc,
                                                     ndl / 20, rcnt.as<int64_t>(), ccnt.as<unsigned long long>(),
                                                     cmax.as<unsigned long long>(), cmin.as<unsigned long long>(),
                                                     seen.as<unsigned char>(), T);
@@ -331,24 +445,37 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
   // symmetry (square matrices)
   if (n == nc && nnz > 0) {
     if (n > (int64_t)0xffffffffLL) return fail(SPOPS_ERR_UNSUPPORTED, "features: more than 2^32 rows");
-    DevBuf k0, k1, v0, v1, cntb, tmp;
+    PoolBuf k0(ctx), k1(ctx), v0(ctx), v1(ctx), cntb(ctx), tmp(ctx);
     SPOPS_TRY(k0.alloc((size_t)nnz * 8));
     SPOPS_TRY(k1.alloc((size_t)nnz * 8));
     SPOPS_TRY(v0.alloc((size_t)nnz * sizeof(V)));
     SPOPS_TRY(v1.alloc((size_t)nnz * sizeof(V)));
-    SPOPS_TRY(cntb.alloc(16));
-    SPOPS_CUDA(cudaMemsetAsync(cntb.p, 0, 16, st));
-    symm_keys_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n,
-                                                            k0.as<uint64_t>(), v0.as<V>());
+    SPOPS_TRY(cntb.alloc(32));
+    SPOPS_CUDA(cudaMemsetAsync(cntb.p, 0, 32, st));
+    // rows whose columns already ascend need no sort: the keys are in order
+    unsigned int* unsorted = reinterpret_cast<unsigned int*>(cntb.as<unsigned long long>() + 1) + 2;
+    SPOPS_CUDA(cudaMemsetAsync(unsorted, 0, 4, st));
+    rows_unsorted_kernel<I><<<grid_of(n), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), n, unsorted);
     SPOPS_LAUNCH_CHECK();
-    size_t b = 0;
-    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
-                                               v1.as<V>(), nnz, 0, 64, st));
-    SPOPS_TRY(tmp.alloc(b + 256));
-    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
-                                               v1.as<V>(), nnz, 0, 64, st));
+    unsigned int h_unsorted = 0;
+    SPOPS_CUDA(cudaMemcpyAsync(&h_unsorted, unsorted, 4, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    symm_keys_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n,
+                                                            (h_unsorted ? k0 : k1).as<uint64_t>(),
+                                                            (h_unsorted ? v0 : v1).as<V>());
+    SPOPS_LAUNCH_CHECK();
+    if (h_unsorted) {
+      int end_bit = 32;  // the row half of the key holds n - 1 at most
+      while (end_bit < 64 && ((uint64_t)(n - 1) >> (end_bit - 32)) != 0) ++end_bit;
+      size_t b = 0;
+      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
+                                                 v1.as<V>(), nnz, 0, end_bit, st));
+      SPOPS_TRY(tmp.alloc(b + 256));
+      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
+                                                 v1.as<V>(), nnz, 0, end_bit, st));
+    }
     unsigned long long* c2 = cntb.as<unsigned long long>();
-    symm_kernel<V><<<grid_of(nnz), 256, 0, st>>>(k1.as<uint64_t>(), v1.as<V>(), nnz, c2, c2 + 1);
+    symm_kernel<I, V><<<grid_of(nnz), 256, 0, st>>>(A->row.as<I>(), k1.as<uint64_t>(), v1.as<V>(), nnz, c2, c2 + 1);
     SPOPS_LAUNCH_CHECK();
     unsigned long long hc[2] = {0, 0};
     SPOPS_CUDA(cudaMemcpyAsync(hc, c2, 16, cudaMemcpyDeviceToHost, st));
