@@ -14,6 +14,7 @@
  *   hierarchical_clustering_v0_fast                                   LeSpGEMM preprocessing
  *   read_coo_matrix, read_csr_matrix                                  Matrix Market files
  *   LeSpGEMM<sortOutput>(A, B, C, kernel_flag), HashSpGEMMTopK(A, C, top_k)
+ *   MTX<I,V>: MtxLoad, CalculateFeatures, FeaturesPrint, FeaturesWrite ...  features
  *                                                                     row-wise SpGEMM (include/spgemm.h)
  *
  * What differs, and why:
@@ -37,10 +38,12 @@
 #ifndef SPOPS_B200_CXX_SPOPS_H
 #define SPOPS_B200_CXX_SPOPS_H
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <mutex>
 #include <new>
 #include <stdexcept>
@@ -1083,5 +1086,240 @@ void HashSpGEMMTopK(const CSR_Matrix<IndexType, ValueType>& A, CSR_Matrix<IndexT
   d::take_csr<IndexType, ValueType>(c, C);
   C.kernel_flag = 0;
 }
+
+/* ------------------------------------------------------------ features */
+/* The reference's feature class (include/sparse_features.h:15-328,
+ * src/sparse_features.cpp) with its public calls:
+ *   MtxLoad(path)                 the Matrix Market file read on the device
+ *                                 (read_csr_matrix, symmetric files expanded)
+ *   CalculateFeatures()           structure and tile features on the device
+ *                                 (spops_matrix_features, spops_matrix_tile_features)
+ *   CalculateTilesFeatures(), CalculateTilesExtraFeatures(path)
+ *                                 already computed by CalculateFeatures; true
+ *   FeaturesPrint(), ExtraFeaturesPrint()   the reference's text
+ *   FeaturesWrite(dir)            the .features file and the tile / RB / CB
+ *                                 maps under dir/<name>/ (the reference writes
+ *                                 under a fixed root); returns what the
+ *                                 reference returns: false (EXIT_SUCCESS)
+ *                                 when written, true when not
+ *   ConvertToCSR(csr), getRowNum(), getColNum(), getTileSize(), getMatName()
+ * Differences: a symmetric file's features are those of its expanded
+ * matrix (the reference counts each off-diagonal entry twice too, and sets
+ * the symmetry ratios to 1, which the expanded matrix gives); the GrX
+ * features of CalculateTilesExtraFeatures, compiled out in the reference,
+ * are not computed (printed as the reference's initial -1). */
+template <typename IndexType, typename ValueType>
+class MTX {
+ public:
+  explicit MTX(IndexType matID = 0) : matrixID_(matID) {
+    std::printf("== MTX Features Extraction ==\n\n");
+  }
+  ~MTX() {
+    if (h_) spops_matrix_destroy(h_);
+  }
+  MTX(const MTX&) = delete;
+  MTX& operator=(const MTX&) = delete;
+  IndexType getRowNum() { return (IndexType)f_.rows; }
+  IndexType getColNum() { return (IndexType)f_.cols; }
+  IndexType getTileSize() { return (IndexType)256; }
+  std::string getMatName() { return matrixName_; }
+
+  bool MtxLoad(const char* mat_path) {
+    namespace d = spops_b200::detail;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (h_) spops_matrix_destroy(h_);
+    h_ = nullptr;
+    d::check(spops_mtx_read_csr(d::ctx(), mat_path, d::itype<IndexType>(), d::vtype<ValueType>(), 0, &h_),
+             "spops_mtx_read_csr");
+    std::string name(mat_path);
+    const size_t slash = name.find_last_of('/');
+    if (slash != std::string::npos) name = name.substr(slash + 1);
+    const size_t dot = name.find_last_of('.');
+    matrixName_ = dot == std::string::npos ? name : name.substr(0, dot);
+    const spops_matrix_info_t i = d::info(h_);
+    f_.rows = i.rows;
+    f_.cols = i.cols;
+    f_.nnz = i.nnz;
+    MtxLoad_time_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+  }
+
+  bool CalculateFeatures() {
+    namespace d = spops_b200::detail;
+    if (!h_) throw std::runtime_error("spops_b200: MTX::CalculateFeatures before MtxLoad");
+    const auto t0 = std::chrono::steady_clock::now();
+    d::check(spops_matrix_features(d::ctx(), h_, &f_), "spops_matrix_features");
+    const size_t B = 256, T = B * B;
+    tile_i_.assign(4 * T, 0);
+    tile_d_.assign(2 * T, 0.0);
+    blk_i_.assign(4 * B, 0);
+    blk_d_.assign(4 * B, 0.0);
+    spops_tile_maps_t m{};
+    m.tile_nnz = tile_i_.data();
+    m.tile_rows = tile_i_.data() + T;
+    m.tile_cols = tile_i_.data() + 2 * T;
+    m.tile_max_row_nnz = tile_i_.data() + 3 * T;
+    m.tile_ave_row_nnz = tile_d_.data();
+    m.tile_std_row_nnz = tile_d_.data() + T;
+    m.rb_nnz = blk_i_.data();
+    m.rb_max_row_nnz = blk_i_.data() + B;
+    m.cb_nnz = blk_i_.data() + 2 * B;
+    m.cb_max_col_nnz = blk_i_.data() + 3 * B;
+    m.rb_ave_row_nnz = blk_d_.data();
+    m.rb_std_row_nnz = blk_d_.data() + B;
+    m.cb_ave_col_nnz = blk_d_.data() + 2 * B;
+    m.cb_std_col_nnz = blk_d_.data() + 3 * B;
+    d::check(spops_matrix_tile_features(d::ctx(), h_, (int64_t)B, &t_, &m), "spops_matrix_tile_features");
+    is_symmetric_ = f_.pattern_symm == 1.0 && f_.value_symm == 1.0;
+    computed_ = true;
+    CalculateFeatures_time_ =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+  }
+  bool CalculateTilesFeatures() { return computed_ || CalculateFeatures(); }
+  bool CalculateTilesExtraFeatures(const char*) { return computed_ || CalculateFeatures(); }
+
+  bool ConvertToCSR(CSR_Matrix<IndexType, ValueType>& csr) {
+    namespace d = spops_b200::detail;
+    if (!h_) return false;
+    const auto t0 = std::chrono::steady_clock::now();
+    const spops_matrix_info_t i = d::info(h_);
+    d::set_features<IndexType, ValueType>(csr, i.rows, i.cols, i.nnz);
+    csr.row_offset = d::fetch<IndexType>(h_, SPOPS_ARR_ROW, nullptr);
+    csr.col_index = d::fetch<IndexType>(h_, SPOPS_ARR_COL, nullptr);
+    csr.values = d::fetch<ValueType>(h_, SPOPS_ARR_VAL, nullptr);
+    ConvertToCSR_time_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+  }
+
+  void FeaturesPrint() {
+    std::printf("[%lld]  %scounting by %d-bit Index, %d-bit Value\n", (long long)matrixID_, matrixName_.c_str(),
+                (int)(8 * sizeof(IndexType)), (int)(8 * sizeof(ValueType)));
+    std::printf("is_symmetric %d\npattern_symm %g%%\nvalue_symm   %g%%\n\n", is_symmetric_ ? 1 : 0,
+                f_.pattern_symm * 100, f_.value_symm * 100);
+    std::printf("num_rows   = %lld\nnum_cols   = %lld\nnnz_mtx    = %lld\nreal_nnz   = %lld\n", (long long)f_.rows,
+                (long long)f_.cols, (long long)f_.nnz, (long long)f_.nnz);
+    std::printf("nnz_ratio  = %g%%\nnum_of_diags  = %lld\nnnz_closed2diag_ratio = %g%%\n\n", f_.nnz_ratio * 100,
+                (long long)f_.ndiags, f_.diag_close_ratio * 100);
+    std::printf("nnz_lower    : %lld\nnnz_upper    : %lld\nnnz_diagonal : %lld\n\n", (long long)f_.nnz_lower,
+                (long long)f_.nnz_upper, (long long)f_.nnz_diagonal);
+    std::printf("NoneZero_Row_Ratio      : %g%%\nmin_nnz_each_row        : %lld\nmax_nnz_each_row        : %lld\n",
+                f_.nz_row_ratio * 100, (long long)f_.min_nnz_row, (long long)f_.max_nnz_row);
+    std::printf("ave_nnz_each_row        : %g\nvar_nnz_each_row        : %g\nstandard_dev_row        : %g\n",
+                f_.ave_nnz_row, f_.var_nnz_row, f_.std_nnz_row);
+    std::printf("P-ratio_row             : %g\nGini_coeff_row          : %g\n\n", f_.p_ratio_row, f_.gini_row);
+    std::printf("NoneZero_Col_Ratio      : %g%%\nmin_nnz_each_col        : %lld\nmax_nnz_each_col        : %lld\n",
+                f_.nz_col_ratio * 100, (long long)f_.min_nnz_col, (long long)f_.max_nnz_col);
+    std::printf("ave_nnz_each_col        : %g\nvar_nnz_each_col        : %g\nstandard_dev_col        : %g\n",
+                f_.ave_nnz_col, f_.var_nnz_col, f_.std_nnz_col);
+    std::printf("P-ratio_col             : %g\nGini_coeff_col          : %g\n\n", f_.p_ratio_col, f_.gini_col);
+    std::printf("diagonal_dominant_ratio : %g%%\n\n", f_.diagonal_dominant_ratio * 100);
+    std::printf("max_value_offdiag  = %g\nmax_value_diagonal = %g\nrow_variability    = %g\n"
+                "col_variability    = %g\n\n",
+                f_.max_value_offdiag, f_.max_value_diagonal, f_.row_variability, f_.col_variability);
+    std::printf("==========   Tile Features   ==========\nNumber of Tiles  : %lld\nTile inner size  : %lld * %lld\n",
+                (long long)t_.num_blocks, (long long)t_.rows_per_block, (long long)t_.cols_per_block);
+    std::printf("t_ave_nnz_tiles     : %g\nt_ave_nnz_RB        : %g\nt_ave_nnz_CB        : %g\n\n", t_.ave_nnz_tile,
+                t_.ave_nnz_rb, t_.ave_nnz_cb);
+    std::printf("t_var_nnz_tiles     : %g\nt_var_nnz_RB        : %g\nt_var_nnz_CB        : %g\n\n", t_.var_nnz_tile,
+                t_.var_nnz_rb, t_.var_nnz_cb);
+    std::printf("t_stand_dev_tiles     : %g\nt_stand_dev_RB        : %g\nt_stand_dev_CB        : %g\n\n",
+                t_.std_nnz_tile, t_.std_nnz_rb, t_.std_nnz_cb);
+    std::printf("min_nnz_each_tiles       : %lld\nmax_nnz_each_tiles       : %lld\n", (long long)t_.min_nnz_tile,
+                (long long)t_.max_nnz_tile);
+    std::printf("min_nnz_each_RB          : %lld\nmax_nnz_each_RB          : %lld\n", (long long)t_.min_nnz_rb,
+                (long long)t_.max_nnz_rb);
+    std::printf("min_nnz_each_CB          : %lld\nmax_nnz_each_CB          : %lld\n\n", (long long)t_.min_nnz_cb,
+                (long long)t_.max_nnz_cb);
+    std::printf("Gini_nnz_tiles     : %g\nGini_nnz_RB        : %g\nGini_nnz_CB        : %g\n\n", t_.gini_tiles,
+                t_.gini_rb, t_.gini_cb);
+    std::printf("P-ratio_tiles      : %g\nP-ratio_RB         : %g\nP-ratio_CB         : %g\n\n", t_.p_ratio_tiles,
+                t_.p_ratio_rb, t_.p_ratio_cb);
+    std::printf("NE_ratio_tiles_     : %g\nNE_ratio_RB         : %g\nNE_ratio_CB         : %g\n\n",
+                t_.nz_ratio_tiles, t_.nz_ratio_rb, t_.nz_ratio_cb);
+  }
+
+  void ExtraFeaturesPrint() {
+    std::printf("==========   Tile Extra Features   ==========\n");
+    std::printf("uniq_R         = %g\nuniq_C         = %g\n\n", t_.uniq_r, t_.uniq_c);
+    std::printf("GrX_uniqR      = %g\nGrX_uniqC      = %g\n\n", -1.0, -1.0);
+    std::printf("potReuseR      = %g\npotReuseC      = %g\n\n", t_.pot_reuse_r, t_.pot_reuse_c);
+    std::printf("GrX_potReuseR  = %g\nGrX_potReuseC  = %g\n\n", -1.0, -1.0);
+    std::printf("ave_distance_= %g\n\n", t_.distance_per_row);
+  }
+
+  bool FeaturesWrite(const char* file_path) {
+    if (!computed_) return true;
+    const std::string dir = std::string(file_path ? file_path : ".") + "/" + matrixName_;
+    std::error_code ec;
+    std::filesystem::create_directories(dir, ec);
+    if (ec) return true;
+    const size_t B = 256, T = B * B;
+    auto put_i = [&](const char* suffix, const int64_t* a, size_t n) {
+      FILE* f = std::fopen((dir + "/" + matrixName_ + suffix).c_str(), "w");
+      if (!f) return false;
+      for (size_t i = 0; i < n; ++i) std::fprintf(f, "%lld\n", (long long)a[i]);
+      std::fclose(f);
+      return true;
+    };
+    auto put_d = [&](const char* suffix, const double* a, size_t n) {
+      FILE* f = std::fopen((dir + "/" + matrixName_ + suffix).c_str(), "w");
+      if (!f) return false;
+      for (size_t i = 0; i < n; ++i) std::fprintf(f, "%g\n", a[i]);
+      std::fclose(f);
+      return true;
+    };
+    bool ok = put_d(".ave", tile_d_.data(), T) && put_i(".max", tile_i_.data() + 3 * T, T) &&
+              put_i(".nnz", tile_i_.data(), T) && put_d(".std", tile_d_.data() + T, T) &&
+              put_i(".RBmax", blk_i_.data() + B, B) && put_i(".RBnnz", blk_i_.data(), B) &&
+              put_d(".RBave", blk_d_.data(), B) && put_d(".RBstd", blk_d_.data() + B, B) &&
+              put_i(".CBmax", blk_i_.data() + 3 * B, B) && put_i(".CBnnz", blk_i_.data() + 2 * B, B) &&
+              put_d(".CBave", blk_d_.data() + 2 * B, B) && put_d(".CBstd", blk_d_.data() + 3 * B, B);
+    FILE* f = ok ? std::fopen((dir + "/" + matrixName_ + ".features").c_str(), "w") : nullptr;
+    if (!f) return true;
+    std::fprintf(f, "[%lld]: %s\n", (long long)matrixID_, matrixName_.c_str());
+    std::fprintf(f, "num_rows %lld\nnum_cols %lld\nnum_nnz %lld\n", (long long)f_.rows, (long long)f_.cols,
+                 (long long)f_.nnz);
+    std::fprintf(f, "nnz_ratio %g\nnnz_on_maindiag_ratio %g\nnnz_row_distance_ratio %g\n", f_.nnz_ratio,
+                 f_.diag_close_ratio, t_.distance_per_row / (double)f_.cols);
+    std::fprintf(f, "nz_row_ratio %g\nmax_nnz_each_row %lld\nave_nnz_each_row %g\nstandard_dev_row %g\n",
+                 f_.nz_row_ratio, (long long)f_.max_nnz_row, f_.ave_nnz_row, f_.std_nnz_row);
+    std::fprintf(f, "P-ratio_row %g\nGini_coeff_row %g\n", f_.p_ratio_row, f_.gini_row);
+    std::fprintf(f, "nz_col_ratio %g\nmax_nnz_each_col %lld\nave_nnz_each_col %g\nstandard_dev_col %g\n",
+                 f_.nz_col_ratio, (long long)f_.max_nnz_col, f_.ave_nnz_col, f_.std_nnz_col);
+    std::fprintf(f, "P-ratio_col %g\nGini_coeff_col %g\n", f_.p_ratio_col, f_.gini_col);
+    std::fprintf(f, "nz_tiles_ratio %g\nmax_nnz_each_tiles %lld\nave_nnz_each_tiles %g\nstandard_dev_tiles %g\n",
+                 t_.nz_ratio_tiles, (long long)t_.max_nnz_tile, t_.ave_nnz_tile, t_.std_nnz_tile);
+    std::fprintf(f, "P-ratio_tiles %g\nGini_coeff_tiles %g\n", t_.p_ratio_tiles, t_.gini_tiles);
+    std::fprintf(f, "nz_ratio_RB %g\nmax_nnz_each_RB %lld\nave_nnz_each_RB %g\nstandard_dev_RB %g\n",
+                 t_.nz_ratio_rb, (long long)t_.max_nnz_rb, t_.ave_nnz_rb, t_.std_nnz_rb);
+    std::fprintf(f, "P-ratio_RB %g\nGini_coeff_RB %g\n", t_.p_ratio_rb, t_.gini_rb);
+    std::fprintf(f, "nz_ratio_CB %g\nmax_nnz_each_CB %lld\nave_nnz_each_CB %g\nstandard_dev_CB %g\n",
+                 t_.nz_ratio_cb, (long long)t_.max_nnz_cb, t_.ave_nnz_cb, t_.std_nnz_cb);
+    std::fprintf(f, "P-ratio_CB %g\nGini_coeff_CB %g\n", t_.p_ratio_cb, t_.gini_cb);
+    std::fprintf(f, "uniq_R %g\nuniq_C %g\npotReuseR %g\npotReuseC %g\n", t_.uniq_r, t_.uniq_c, t_.pot_reuse_r,
+                 t_.pot_reuse_c);
+    std::fclose(f);
+    return false;
+  }
+
+  // the computed values, by the C ABI's names
+  const spops_features_t& features() const { return f_; }
+  const spops_tile_features_t& tile_features() const { return t_; }
+
+  double MtxLoad_time_ = 0.0;
+  double CalculateFeatures_time_ = 0.0;
+  double ConvertToCSR_time_ = 0.0;
+
+ private:
+  IndexType matrixID_ = 0;
+  std::string matrixName_;
+  spops_matrix_t h_ = nullptr;
+  spops_features_t f_{};
+  spops_tile_features_t t_{};
+  std::vector<int64_t> tile_i_, blk_i_;
+  std::vector<double> tile_d_, blk_d_;
+  bool is_symmetric_ = false, computed_ = false;
+};
 
 #endif /* SPOPS_B200_CXX_SPOPS_H */

@@ -325,6 +325,53 @@ void mtx_checks() {
   std::remove(path);
 }
 
+// the feature class on a 300 x 200 general file: 300 rows make 256 row
+// blocks (44 of two rows), 200 columns one column per block
+void feature_checks() {
+  const char* path = "shim_test_features.mtx";
+  FILE* f = std::fopen(path, "w");
+  EXPECT(f != nullptr, "temporary file");
+  if (!f) return;
+  std::vector<int> rr, cc;
+  for (int r = 0; r < 300; ++r)
+    for (int k = 0; k < 1 + r % 5; ++k) {
+      rr.push_back(r);
+      cc.push_back((r * 7 + k * 31) % 200);
+    }
+  std::fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n300 200 %d\n", (int)rr.size());
+  for (size_t i = 0; i < rr.size(); ++i) std::fprintf(f, "%d %d %d.5\n", rr[i] + 1, cc[i] + 1, (int)(i % 9) - 4);
+  std::fclose(f);
+  // the row distance the reference's CalculateTilesExtraFeatures computes
+  double dist = 0.0;
+  for (size_t i = 0; i < rr.size();) {
+    size_t j = i;
+    while (j < rr.size() && rr[j] == rr[i]) ++j;
+    dist += (double)(cc[j - 1] - cc[i]) / (double)(j - i);
+    i = j;
+  }
+  dist /= 300.0;
+  MTX<int, double> m(7);
+  EXPECT(m.MtxLoad(path) && m.CalculateFeatures() && m.CalculateTilesExtraFeatures(path), "MTX calls");
+  m.FeaturesPrint();
+  m.ExtraFeaturesPrint();
+  const spops_features_t& s = m.features();
+  const spops_tile_features_t& t = m.tile_features();
+  const double nnz = (double)rr.size();
+  EXPECT(m.getRowNum() == 300 && m.getColNum() == 200 && s.nnz == (int64_t)rr.size() && m.getMatName() ==
+                                                                                             "shim_test_features",
+         "MTX shape and name");
+  EXPECT(t.num_blocks == 256 && t.rows_per_block == 1 && t.rows_mod == 44 && t.cols_per_block == 0 &&
+             t.cols_mod == 200,
+         "MTX tile grid");
+  EXPECT(t.uniq_r == 1.0 && t.pot_reuse_r == nnz / 300.0 && std::fabs(t.distance_per_row - dist) <= 1e-12 * 300,
+         "MTX tile extra features");
+  EXPECT(!m.FeaturesWrite("shim_test_features_out"), "MTX FeaturesWrite (false when written, as the reference)");
+  FILE* g = std::fopen("shim_test_features_out/shim_test_features/shim_test_features.features", "r");
+  EXPECT(g != nullptr, "MTX .features file");
+  if (g) std::fclose(g);
+  std::remove(path);
+}
+
 int main() {
   std::setvbuf(stdout, nullptr, _IONBF, 0);
   try {
@@ -334,6 +381,7 @@ int main() {
     lsh_checks();
     spgemm_checks();
     mtx_checks();
+    feature_checks();
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
     return 2;
