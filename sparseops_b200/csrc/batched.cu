@@ -228,6 +228,11 @@ spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, in
                         void* Y, int64_t ldy) {
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "SpMM needs a CSR matrix");
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
+  if (k == 8 && ctx->csr_variant == 0) {  // register tiles on the SpMV's plan
+    bool used = false;
+    SPOPS_TRY(csr_tile_spmm8(ctx, A, alpha, X, ldx, beta, Y, ldy, &used));
+    if (used) return SPOPS_OK;
+  }
   const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
   if (i32 && f64) return spmm_t<int32_t, double>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
   if (i32) return spmm_t<int32_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);

@@ -294,6 +294,200 @@ __global__ void csr_tile_calibrate_kernel(int64_t t_begin, int64_t tiles, const 
   }
 }
 
+// ---- multi-RHS with k = 8 on the same tile plan (csr_tile_spmm8)
+// Lane l of the warp that owns tile t takes the SpMV's 8 entries, gathers
+// each entry's X row (8 values, 32-byte vector loads, four rows at a time)
+// and keeps 8 running sums that are cut at every row start; the heads
+// combine across lanes with the SpMV's segmented scan, and the row open at a
+// tile's end goes to the 8-wide calibrator.  Every column is summed in an
+// order fixed by the matrix.
+template <typename V>
+__device__ __forceinline__ void ld_xrow8(const V* __restrict__ p, V (&r)[8]) {
+#pragma unroll
+  for (int q = 0; q < (int)sizeof(V); q += 4) {
+    uint32_t w[8];
+    asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+                 : "l"(reinterpret_cast<const char*>(p) + 8 * q));
+    memcpy(reinterpret_cast<char*>(r) + 8 * q, w, 32);
+  }
+}
+
+template <typename V>
+__device__ __forceinline__ void axpby_store8(V* __restrict__ y, const V (&v)[8], V alpha, V beta, bool bz) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) axpby_store(y + j, v[j], alpha, beta, bz);
+}
+
+template <typename I, typename V>
+__global__ void __launch_bounds__(kTileBlock, 2) csr_tile_spmm8_kernel(
+    const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
+    const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t tiles,
+    const V* __restrict__ X, int64_t ldx, V* __restrict__ Y, int64_t ldy, V alpha, V beta, bool bz,
+    V* __restrict__ carry_in, V* __restrict__ open_sum, int64_t* __restrict__ open_row) {
+  constexpr int K = 8;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
+  for (int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5); t < tiles; t += nw) {
+    I c[K];
+    V a[K];
+    tile_load<I, V, K>(ci, val, nnz, t, lane, c, a);
+    const uint32_t flags = flags_all[t * 32 + lane];
+    const int64_t tr = tile_row[t];
+    const int64_t el = t * (32 * K) + (int64_t)lane * K;
+    int64_t row;
+    if (tr >= 0) {
+      const int cnt = __popc(flags);
+      int excl = 0;
+#pragma unroll
+      for (int bit = 0; bit < 4; ++bit) excl += __popc(__ballot_sync(0xffffffffu, (cnt >> bit) & 1) & lt) << bit;
+      const int first0 = (int)(__ballot_sync(0xffffffffu, flags & 1u) & 1u);
+      row = tr + excl + (int)(flags & 1u) - first0;
+    } else {
+      row = row_holding(rp, n, el < nnz ? el : nnz - 1);
+    }
+    V acc[8], head[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] = head[j] = V(0);
+    bool in_head = (flags & 1u) == 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      V xr[4][8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ld_xrow8(X + (int64_t)c[4 * h + q] * ldx, xr[q]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int b = 4 * h + q;
+        if (b > 0 && ((flags >> b) & 1u)) {
+          if (in_head) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) head[j] = acc[j];
+            in_head = false;
+          } else {
+            axpby_store8(Y + row * ldy, acc, alpha, beta, bz);
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[j] = V(0);
+          ++row;
+          if (tr < 0)
+            while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const V prod = a[b] * xr[q][j];
+          acc[j] += prod;
+        }
+      }
+    }
+    V tail[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (in_head) head[j] = acc[j];
+      tail[j] = in_head ? V(0) : acc[j];
+    }
+    // segmented inclusive scan of the heads (a segment starts right after
+    // every flagged lane)
+    const bool has_flag = flags != 0;
+    const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
+    const unsigned starts = (fmask << 1) | 1u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned span = (lane >= o) ? ((2u << lane) - 1u) & ~((2u << (lane - o)) - 1u) : 0u;
+      const bool add = lane >= o && !(starts & span);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const V su = __shfl_up_sync(0xffffffffu, head[j], o);
+        if (add) head[j] += su;
+      }
+    }
+    const unsigned later = fmask & ~((2u << lane) - 1u);
+    const int m = later ? __ffs(later) - 1 : 31;
+    const int m0 = fmask ? __ffs(fmask) - 1 : 31;
+    V Sm[8], cin[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      Sm[j] = __shfl_sync(0xffffffffu, head[j], m);
+      cin[j] = __shfl_sync(0xffffffffu, head[j], m0);
+    }
+    if (has_flag) {
+      if (later) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) tail[j] += Sm[j];
+        axpby_store8(Y + row * ldy, tail, alpha, beta, bz);
+      } else {  // the tile's last row: may continue into the next tile
+#pragma unroll
+        for (int j = 0; j < 8; ++j) open_sum[t * 8 + j] = tail[j] + (lane < 31 ? Sm[j] : V(0));
+        open_row[t] = row;
+      }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) carry_in[t * 8 + j] = cin[j];
+      if (!fmask) open_row[t] = -1;
+    }
+  }
+}
+
+template <typename V>
+__global__ void csr_tile_calibrate8_kernel(int64_t tiles, const V* __restrict__ carry_in,
+                                           const V* __restrict__ open_sum, const int64_t* __restrict__ open_row,
+                                           const int64_t* __restrict__ empty, int64_t nempty, V* __restrict__ Y,
+                                           int64_t ldy, V alpha, V beta, bool bz) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  V tot[8];
+  if (t < tiles) {
+    const int64_t r = open_row[t];
+    if (r < 0) return;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) tot[j] = open_sum[t * 8 + j];
+    for (int64_t u = t + 1; u < tiles; ++u) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) tot[j] += carry_in[u * 8 + j];
+      if (open_row[u] >= 0) break;
+    }
+    axpby_store8(Y + r * ldy, tot, alpha, beta, bz);
+  } else if (t - tiles < nempty) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) tot[j] = V(0);
+    axpby_store8(Y + empty[t - tiles] * ldy, tot, alpha, beta, bz);
+  }
+}
+
+template <typename I, typename V>
+spops_status_t spmm8_t(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, double beta, void* Y,
+                       int64_t ldy) {
+  const CsrTiles& D = A->plan.tiles;
+  const bool bz = beta == 0.0;
+  PoolBuf cin(ctx), osum(ctx);
+  const size_t nt1 = (size_t)(D.tiles > 0 ? D.tiles : 1);
+  SPOPS_TRY(cin.alloc(nt1 * 8 * sizeof(V)));
+  SPOPS_TRY(osum.alloc(nt1 * 8 * sizeof(V)));
+  if (D.tiles > 0) {
+    static int blocks_per_sm = -1;  // per instantiation
+    if (blocks_per_sm < 0) {
+      int bps = 0;
+      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_spmm8_kernel<I, V>, kTileBlock, 0));
+      blocks_per_sm = bps > 0 ? bps : 1;
+    }
+    int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
+    const int64_t need = (D.tiles + kTileBlock / 32 - 1) / (kTileBlock / 32);
+    if (grid > need) grid = need;
+    csr_tile_spmm8_kernel<I, V><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
+        A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), A->val.as<V>(), D.tile_row.as<int64_t>(),
+        D.flags.as<uint8_t>(), D.tiles, static_cast<const V*>(X), ldx, static_cast<V*>(Y), ldy, (V)alpha, (V)beta,
+        bz, cin.as<V>(), osum.as<V>(), D.open_row.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  if (D.tiles + D.nempty > 0) {
+    csr_tile_calibrate8_kernel<V><<<grid_of(D.tiles + D.nempty), 256, 0, ctx->stream>>>(
+        D.tiles, cin.as<V>(), osum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), D.nempty,
+        static_cast<V*>(Y), ldy, (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
+}
+
 // Boundaries of `parts` tile ranges for the pipelined host SpMV: range p
 // starts at the first tile at or after p * tiles / parts whose first entry
 // starts a row (so every row lies in one range), and rb[p] is that row.
@@ -471,6 +665,23 @@ spops_status_t csr_tile_spmv_parts(Context* ctx, Matrix* A, int parts, double al
   if (i32) return spmv_parts_t<int32_t, float>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
   if (f64) return spmv_parts_t<int64_t, double>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
   return spmv_parts_t<int64_t, float>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
+}
+
+spops_status_t csr_tile_spmm8(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, double beta,
+                              void* Y, int64_t ldy, bool* used) {
+  *used = false;
+  const size_t vs = A->vsize();
+  // 32-byte vector gathers of X rows; the tile plan's vector loads of A
+  if (A->rows <= 0 || A->nnz <= 0 || !csr_tile_usable(A, 0) || ((uintptr_t)X % 32) != 0 ||
+      ((size_t)ldx * vs) % 32 != 0 || ldx < 8 || ldy < 8)
+    return SPOPS_OK;
+  if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(ctx, A, 8));
+  *used = true;
+  const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return spmm8_t<int32_t, double>(ctx, A, alpha, X, ldx, beta, Y, ldy);
+  if (i32) return spmm8_t<int32_t, float>(ctx, A, alpha, X, ldx, beta, Y, ldy);
+  if (f64) return spmm8_t<int64_t, double>(ctx, A, alpha, X, ldx, beta, Y, ldy);
+  return spmm8_t<int64_t, float>(ctx, A, alpha, X, ldx, beta, Y, ldy);
 }
 
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta,

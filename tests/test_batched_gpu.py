@@ -105,3 +105,57 @@ def test_single_spmm(cuda, orc, k):
     torch.cuda.synchronize()
     ref = orc.spmm_csr(rp, ci, v, X, 0.8, 0.7, Y0)
     assert _err(orc, rp, ci, v, X, Yd.cpu().numpy(), ref, 0.8, 0.7, Y0) <= 1e-12
+
+
+@pytest.mark.parametrize("case", ["empty_rows", "int64", "f32", "wide_ld", "misaligned", "beta0_nan"])
+def test_spmm8_tiles(cuda, orc, case):
+    """k = 8 runs on the SpMV's tile plan (register sums per lane, 32-byte X-row
+    gathers): empty rows (tiles that span them), a long row over many tiles,
+    int64 indices, FP32, a row stride wider than 8, beta = 0 over NaN, and a
+    misaligned X (the segment kernel then runs); every case against the
+    oracle, and two runs bit-identical."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, SpMM_csr
+    rng = np.random.default_rng(41)
+    n, k = 40000, 8
+    lens = rng.poisson(12, n)
+    lens[rng.random(n) < 0.1] = 0
+    lens[7] = 5000
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = rng.integers(0, n, int(rp[-1])).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    dt, tol = (np.float32, 1e-5) if case == "f32" else (np.float64, 1e-12)
+    if case == "int64":
+        rp, ci = rp.astype(np.int64), ci.astype(np.int64)
+    ld = 12 if case == "wide_ld" else k
+    Xfull = rng.standard_normal((n + 1, ld)).astype(dt)
+    Y0 = rng.standard_normal((n, ld)).astype(dt)
+    dev = torch.device("cuda")
+    A = CSR_Matrix(n, n, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
+                   torch.from_numpy(v.astype(dt)).to(dev))
+    Xd_full = torch.from_numpy(Xfull).to(dev)
+    if case == "misaligned":  # X starts one element after a 32-byte boundary
+        flat = torch.from_numpy(np.concatenate([[0.0], Xfull[:n].ravel()]).astype(dt)).to(dev)
+        Xd = flat[1:].view(n, ld)
+    else:
+        Xd = Xd_full[:n, :k] if ld != k else Xd_full[:n]
+    X = Xd.cpu().numpy()
+    beta = 0.0 if case == "beta0_nan" else 0.7
+    outs = []
+    for _ in range(2):
+        Yfull = torch.from_numpy(Y0.copy()).to(dev)
+        if case == "beta0_nan":
+            Yfull[:, :k] = float("nan")
+        Yd = Yfull[:, :k]
+        SpMM_csr(0.8, A, Xd, beta, Yd)
+        torch.cuda.synchronize()
+        outs.append(Yfull.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    Y = outs[0][:, :k].astype(np.float64)
+    if ld != k:
+        assert np.array_equal(outs[0][:, k:], Y0[:, k:])  # columns past k untouched
+    rp32, ci32 = rp.astype(np.int32), ci.astype(np.int32)  # the oracle's SpMM takes int32 indices
+    Y0k = Y0[:, :k].astype(np.float64)
+    ref = orc.spmm_csr(rp32, ci32, v.astype(dt).astype(np.float64), X.astype(np.float64), 0.8, beta, Y0k)
+    assert _err(orc, rp32, ci32, v.astype(dt).astype(np.float64), X.astype(np.float64), Y, ref, 0.8, beta,
+                Y0k) <= tol
