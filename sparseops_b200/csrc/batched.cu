@@ -228,7 +228,10 @@ spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, in
                         void* Y, int64_t ldy) {
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "SpMM needs a CSR matrix");
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
-  if (k == 8 && ctx->csr_variant == 0) {  // register tiles on the SpMV's plan
+  // k = 8 with narrow X rows: register tiles on the SpMV's plan.  (Passes of
+  // 8 columns over wider rows measured slower than the segment kernel: at
+  // k = 32 four passes took 20.5 ms against 6.5 ms on the power-law matrix.)
+  if (k == 8 && (size_t)ldx * A->vsize() <= 128 && ctx->csr_variant == 0) {
     bool used = false;
     SPOPS_TRY(csr_tile_spmm8(ctx, A, alpha, X, ldx, beta, Y, ldy, &used));
     if (used) return SPOPS_OK;
