@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "device_util.cuh"
+#include "csr_tile.cuh"
 #include "spops_internal.h"
 #include "warp_work.cuh"
 
@@ -60,6 +61,15 @@ struct BatchMat {
   const void* x;
   void* y;
   int64_t ldx, ldy;
+  // k = 8 register tiles on the matrix's SpMV tile plan (csr_tile.cuh)
+  const int64_t* tile_row;
+  const uint8_t* tflags;
+  int64_t tiles, nnz;
+  void* tcin;      // V [tiles * 8]: heads before each tile's first row start
+  void* tosum;     // V [tiles * 8]: the row open at each tile's end
+  int64_t* topen;  // [tiles]: that row, or -1
+  const int64_t* tempty;
+  int64_t tnempty;
 };
 
 namespace {
@@ -135,6 +145,58 @@ __global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(con
     grab = __shfl_sync(0xffffffffu, ahead, 0);
     if (lane == 0 && (int64_t)grab < nitems) ahead = atomicAdd(next_item, (unsigned long long)kGrab);
   }
+}
+
+// k = 8 tile items: item idx covers tiles [idx, idx + kTilesPerItem) of its
+// matrix, taken from the queue as in batch_kernel.
+constexpr int64_t kTilesPerItem = 4;
+
+template <typename I, typename V>
+__global__ void __launch_bounds__(kBatchBlock, 2) batch_tile8_kernel(const BatchItem* __restrict__ items,
+                                                                    int64_t nitems, const BatchMat* __restrict__ mats,
+                                                                    V alpha, V beta, bool bz,
+                                                                    unsigned long long* __restrict__ next_item) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long grab = 0, ahead = 0;
+  if (lane == 0) {
+    grab = atomicAdd(next_item, (unsigned long long)kGrab);
+    ahead = atomicAdd(next_item, (unsigned long long)kGrab);
+  }
+  grab = __shfl_sync(0xffffffffu, grab, 0);
+  for (;;) {
+    if ((int64_t)grab >= nitems) break;
+    const int64_t jend = (int64_t)grab + kGrab < nitems ? (int64_t)grab + kGrab : nitems;
+    for (int64_t j = (int64_t)grab; j < jend; ++j) {
+      const BatchItem it = items[j];
+      const BatchMat& M = mats[it.mat];
+      const int64_t t1 = it.idx + kTilesPerItem < M.tiles ? it.idx + kTilesPerItem : M.tiles;
+      for (int64_t t = it.idx; t < t1; ++t)
+        spmm8_tile<I, V>(static_cast<const I*>(M.rp), M.rows, M.nnz, static_cast<const I*>(M.ci),
+                         static_cast<const V*>(M.val), M.tile_row, M.tflags, t, static_cast<const V*>(M.x), M.ldx,
+                         static_cast<V*>(M.y), M.ldy, alpha, beta, bz, static_cast<V*>(M.tcin),
+                         static_cast<V*>(M.tosum), M.topen, lane);
+    }
+    grab = __shfl_sync(0xffffffffu, ahead, 0);
+    if (lane == 0 && (int64_t)grab < nitems) ahead = atomicAdd(next_item, (unsigned long long)kGrab);
+  }
+}
+
+// Calibration of every tile matrix: thread g takes entry g - cal_off[i] of
+// tile matrix i (its tiles, then its empty rows).
+template <typename V>
+__global__ void batch_calibrate8_kernel(const int64_t* __restrict__ cal_off, const int32_t* __restrict__ cal_mat,
+                                        int ncal, int64_t total, const BatchMat* __restrict__ mats, V alpha, V beta,
+                                        bool bz) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  int lo = 0, hi = ncal;  // last i with cal_off[i] <= g
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (cal_off[mid] <= g) lo = mid; else hi = mid;
+  }
+  const BatchMat& M = mats[cal_mat[lo]];
+  spmm8_calibrate<V>(g - cal_off[lo], M.tiles, static_cast<const V*>(M.tcin), static_cast<const V*>(M.tosum),
+                     M.topen, M.tempty, M.tnempty, static_cast<V*>(M.y), M.ldy, alpha, beta, bz);
 }
 
 // Single-matrix SpMM over the CSR plan (the per-matrix path of spops_spmm).
@@ -254,6 +316,13 @@ struct Batch {
   std::vector<int> choice;    // 0 CSR, 1.. padded candidate index
   std::vector<BatchMat> host;
   std::vector<DevBuf> spmm_partial;
+  // k = 8: matrices on register tiles, their carry buffers, items and the
+  // calibration index (offsets into all tile matrices' tiles + empty rows)
+  std::vector<char> tile_ok;
+  std::vector<DevBuf> t_cin, t_osum;
+  DevBuf titems, tqueue, cal_off, cal_mat;
+  int64_t ntitems = 0, ncal_total = 0;
+  int ncal = 0;
   DevBuf items, table;
   DevBuf queue;  // next item of the running launch
   int64_t nitems = 0;
@@ -271,6 +340,12 @@ struct Batch {
         delete static_cast<spops_matrix_s*>(m);
       }
     for (auto& b : spmm_partial) b.release();
+    for (auto& b : t_cin) b.release();
+    for (auto& b : t_osum) b.release();
+    titems.release();
+    tqueue.release();
+    cal_off.release();
+    cal_mat.release();
     items.release();
     table.release();
     queue.release();
@@ -289,11 +364,20 @@ const int64_t kCandSigma[4] = {256, 4096, 256, 4096};
 const spops_layout_t kCandLayout[4] = {SPOPS_ROW_MAJOR, SPOPS_ROW_MAJOR, SPOPS_COL_MAJOR, SPOPS_COL_MAJOR};
 
 spops_status_t build_items(Batch* B) {
-  std::vector<BatchItem> it;
+  std::vector<BatchItem> it, tit;
+  std::vector<int64_t> off;
+  std::vector<int32_t> mat;
+  int64_t total = 0;
   for (int64_t m = 0; m < B->count; ++m) {
     Matrix* A = B->src[m];
     Matrix* F = B->form[m];
-    if (!F || B->k > 1) {
+    if (B->tile_ok[m]) {
+      const CsrTiles& D = A->plan.tiles;
+      for (int64_t t = 0; t < D.tiles; t += kTilesPerItem) tit.push_back(BatchItem{(int32_t)m, 3, t});
+      off.push_back(total);
+      mat.push_back((int32_t)m);
+      total += D.tiles + D.nempty;
+    } else if (!F || B->k > 1) {
       for (int64_t s = 0; s < A->plan.nblocks; ++s) it.push_back(BatchItem{(int32_t)m, 0, s});
     } else {
       const int64_t groups = (F->rows + 31) / 32;
@@ -306,6 +390,18 @@ spops_status_t build_items(Batch* B) {
   SPOPS_TRY(B->items.alloc(std::max<size_t>(it.size(), 1) * sizeof(BatchItem)));
   if (!it.empty())
     SPOPS_CUDA(cudaMemcpy(B->items.p, it.data(), it.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
+  B->ntitems = (int64_t)tit.size();
+  B->ncal = (int)off.size();
+  B->ncal_total = total;
+  if (!tit.empty()) {
+    if (!B->tqueue.p) SPOPS_TRY(B->tqueue.alloc(8));
+    SPOPS_TRY(B->titems.alloc(tit.size() * sizeof(BatchItem)));
+    SPOPS_TRY(B->cal_off.alloc(off.size() * 8));
+    SPOPS_TRY(B->cal_mat.alloc(mat.size() * 4));
+    SPOPS_CUDA(cudaMemcpy(B->titems.p, tit.data(), tit.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
+    SPOPS_CUDA(cudaMemcpy(B->cal_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice));
+    SPOPS_CUDA(cudaMemcpy(B->cal_mat.p, mat.data(), mat.size() * 4, cudaMemcpyHostToDevice));
+  }
   return SPOPS_OK;
 }
 
@@ -321,6 +417,18 @@ spops_status_t build_table(Batch* B) {
     t.partial = B->k > 1 ? B->spmm_partial[m].p : A->plan.partial.p;
     t.counter = A->plan.counter.as<int>();
     t.rows = A->rows;
+    if (B->tile_ok[m]) {
+      const CsrTiles& D = A->plan.tiles;
+      t.tile_row = D.tile_row.as<int64_t>();
+      t.tflags = D.flags.as<uint8_t>();
+      t.tiles = D.tiles;
+      t.nnz = A->nnz;
+      t.tcin = B->t_cin[m].p;
+      t.tosum = B->t_osum[m].p;
+      t.topen = D.open_row.as<int64_t>();
+      t.tempty = D.empty.as<int64_t>();
+      t.tnempty = D.nempty;
+    }
     if (F) {
       t.pcol = F->col.p;
       t.pval = F->val.p;
@@ -341,9 +449,33 @@ spops_status_t build_table(Batch* B) {
 }
 
 template <typename I, typename V>
+int tile8_blocks_per_sm() {
+  static int cache[kMaxDevices];
+  return blocks_per_sm(batch_tile8_kernel<I, V>, kBatchBlock, 0, cache);
+}
+
+template <typename I, typename V>
 spops_status_t launch_batch(Batch* B, double alpha, double beta, cudaStream_t st) {
-  if (B->nitems == 0) return SPOPS_OK;
   const bool bz = beta == 0.0;
+  if (B->ntitems > 0) {  // k = 8 tile items, then their calibration
+    const int bps = tile8_blocks_per_sm<I, V>();
+    if (bps < 1) return fail(SPOPS_ERR_CUDA, "batch: kernel attributes could not be set");
+    int64_t grid = (int64_t)B->ctx->num_sms * bps;
+    const int64_t need = (B->ntitems + 7) / 8;
+    if (grid > need) grid = need;
+    SPOPS_CUDA(cudaMemsetAsync(B->tqueue.p, 0, 8, st));
+    batch_tile8_kernel<I, V><<<(unsigned)grid, kBatchBlock, 0, st>>>(B->titems.as<BatchItem>(), B->ntitems,
+                                                                   B->table.as<BatchMat>(), (V)alpha, (V)beta, bz,
+                                                                   B->tqueue.as<unsigned long long>());
+    SPOPS_LAUNCH_CHECK();
+    if (B->ncal_total > 0) {
+      batch_calibrate8_kernel<V><<<(unsigned)((B->ncal_total + 255) / 256), 256, 0, st>>>(
+          B->cal_off.as<int64_t>(), B->cal_mat.as<int32_t>(), B->ncal, B->ncal_total, B->table.as<BatchMat>(),
+          (V)alpha, (V)beta, bz);
+      SPOPS_LAUNCH_CHECK();
+    }
+  }
+  if (B->nitems == 0) return SPOPS_OK;
   auto go = [&](auto kern, size_t smem, int bps) -> spops_status_t {
     if (bps < 1) return fail(SPOPS_ERR_CUDA, "batch: kernel attributes could not be set");
     int64_t grid = (int64_t)B->ctx->num_sms * bps;
@@ -371,9 +503,23 @@ spops_status_t launch_any(Batch* B, double alpha, double beta, cudaStream_t st) 
 
 spops_status_t prepare(Batch* B) {
   if (!B->dirty) return SPOPS_OK;
+  B->tile_ok.assign((size_t)B->count, 0);
+  B->t_cin.resize((size_t)B->count);
+  B->t_osum.resize((size_t)B->count);
   for (int64_t m = 0; m < B->count; ++m) {
     Matrix* A = B->src[m];
     if (!A->plan.ready) SPOPS_TRY(csr_analyse(B->ctx, A));
+    // k = 8 over X rows of at most 128 bytes, vector loads aligned: register tiles
+    const BatchMat& h = B->host[m];
+    const size_t vs = A->vsize();
+    if (B->k == 8 && A->rows > 0 && A->nnz > 0 && csr_tile_usable(A, 0) && ((uintptr_t)h.x % 32) == 0 &&
+        ((size_t)h.ldx * vs) % 32 == 0 && (size_t)h.ldx * vs <= 128) {
+      if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(B->ctx, A, 8));
+      const size_t bytes = (size_t)A->plan.tiles.tiles * 8 * vs;
+      if (B->t_cin[m].bytes < bytes) SPOPS_TRY(B->t_cin[m].alloc(bytes));
+      if (B->t_osum[m].bytes < bytes) SPOPS_TRY(B->t_osum[m].alloc(bytes));
+      B->tile_ok[m] = 1;
+    }
     if (B->k > 1 && A->plan.nlong > 0) {
       const size_t bytes = (size_t)A->plan.nblocks * B->k * A->vsize();
       if (B->spmm_partial[m].bytes < bytes) SPOPS_TRY(B->spmm_partial[m].alloc(bytes));
@@ -622,7 +768,7 @@ spops_status_t spops_batch_capture(spops_context_t ctx, spops_batch_t B, double 
 
 spops_status_t spops_batch_info(spops_batch_t B, int64_t* items, int32_t* choice, int32_t* rhs_tile) {
   if (!B) return fail(SPOPS_ERR_INVALID, "spops_batch_info: null batch");
-  if (items) *items = B->nitems;
+  if (items) *items = B->nitems + B->ntitems;
   if (choice)
     for (int64_t m = 0; m < B->count; ++m) choice[m] = B->choice[m];
   if (rhs_tile) *rhs_tile = B->k > 1 ? B->kt : 1;

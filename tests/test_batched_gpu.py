@@ -159,3 +159,56 @@ def test_spmm8_tiles(cuda, orc, case):
     ref = orc.spmm_csr(rp32, ci32, v.astype(dt).astype(np.float64), X.astype(np.float64), 0.8, beta, Y0k)
     assert _err(orc, rp32, ci32, v.astype(dt).astype(np.float64), X.astype(np.float64), Y, ref, 0.8, beta,
                 Y0k) <= tol
+
+
+def test_batch_k8_tiles_mixed_and_replayed(cuda, orc):
+    """k = 8: matrices whose X rows allow 32-byte gathers run as register-tile
+    items (with one calibration launch for all of them); every other matrix
+    has a misaligned X and stays on segment items in the same run.  Direct
+    run, tuned run and graph replay all against the oracle; replays
+    bit-identical."""
+    import torch
+    from sparseops_b200 import Batch, CSR_Matrix
+    k = 8
+    mats = _mats(8, seed=5, long_row=True)
+    dev = torch.device("cuda")
+    A = [CSR_Matrix(len(rp) - 1, len(rp) - 1, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
+                    torch.from_numpy(v).to(dev)) for rp, ci, v in mats]
+    Xs, Ys, Y0s, keep = [], [], [], []
+    for m, (rp, ci, v) in enumerate(mats):
+        n = len(rp) - 1
+        X = synth.uniform(n * k, 300 + m).reshape(n, k)
+        if m % 2:  # misaligned: one element past a 32-byte boundary
+            buf = torch.zeros(n * k + 1, dtype=torch.float64, device=dev)
+            buf[1:] = torch.from_numpy(X.ravel()).to(dev)
+            Xd = buf[1:].view(n, k)
+            keep.append(buf)
+        else:
+            Xd = torch.from_numpy(X).to(dev)
+        Xs.append(Xd)
+        Y0 = synth.uniform(n * k, 400 + m).reshape(n, k)
+        Y0s.append(Y0)
+        Ys.append(torch.from_numpy(Y0.copy()).to(dev))
+    B = Batch(A, k=k)
+    B.set_vectors(Xs, Ys)
+    B.run(0.8, 0.7)
+    torch.cuda.synchronize()
+    for (rp, ci, v), Xd, Yd, Y0 in zip(mats, Xs, Ys, Y0s):
+        X = Xd.cpu().numpy()
+        ref = orc.spmm_csr(rp, ci, v, X, 0.8, 0.7, Y0)
+        assert _err(orc, rp, ci, v, X, Yd.cpu().numpy(), ref, 0.8, 0.7, Y0) <= 1e-12
+    B.tune()
+    B.capture(1.0, 0.0)
+    outs = []
+    for _ in range(2):
+        for Yd in Ys:
+            Yd.fill_(float("nan"))  # beta = 0: never read
+        B.run(1.0, 0.0)  # replays the captured graph
+        torch.cuda.synchronize()
+        outs.append([Yd.cpu().numpy().copy() for Yd in Ys])
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    for (rp, ci, v), Xd, Y in zip(mats, Xs, outs[0]):
+        X = Xd.cpu().numpy()
+        ref = orc.spmm_csr(rp, ci, v, X)
+        assert _err(orc, rp, ci, v, X, Y, ref, 1.0, 0.0, np.zeros_like(Y)) <= 1e-12
