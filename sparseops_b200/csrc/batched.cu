@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_tile8_kernel(const Batch
       const BatchMat& M = mats[it.mat];
       const int64_t t1 = it.idx + kTilesPerItem < M.tiles ? it.idx + kTilesPerItem : M.tiles;
       for (int64_t t = it.idx; t < t1; ++t)
-        spmm8_tile<I, V>(static_cast<const I*>(M.rp), M.rows, M.nnz, static_cast<const I*>(M.ci),
+        spmm8_tile_pairs<I, V>(static_cast<const I*>(M.rp), M.rows, M.nnz, static_cast<const I*>(M.ci),
                          static_cast<const V*>(M.val), M.tile_row, M.tflags, t, static_cast<const V*>(M.x), M.ldx,
                          static_cast<V*>(M.y), M.ldy, alpha, beta, bz, static_cast<V*>(M.tcin),
                          static_cast<V*>(M.tosum), M.topen, lane);

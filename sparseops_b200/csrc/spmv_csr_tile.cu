@@ -227,7 +227,7 @@ __global__ void csr_tile_calibrate_kernel(int64_t t_begin, int64_t tiles, const 
 }
 
 // ---- multi-RHS with k = 8 on the same tile plan (csr_tile_spmm8); the
-// per-tile work is spmm8_tile (csr_tile.cuh)
+// per-tile work is spmm8_tile_pairs (csr_tile.cuh)
 template <typename I, typename V>
 __global__ void __launch_bounds__(kTileBlock, 2) csr_tile_spmm8_kernel(
     const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kTileBlock, 2) csr_tile_spmm8_kernel(
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
   for (int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5); t < tiles; t += nw)
-    spmm8_tile<I, V>(rp, n, nnz, ci, val, tile_row, flags_all, t, X, ldx, Y, ldy, alpha, beta, bz, carry_in,
+    spmm8_tile_pairs<I, V>(rp, n, nnz, ci, val, tile_row, flags_all, t, X, ldx, Y, ldy, alpha, beta, bz, carry_in,
                      open_sum, open_row, lane);
 }
 
