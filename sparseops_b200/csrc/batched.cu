@@ -147,15 +147,15 @@ __global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(con
   }
 }
 
-// k = 8 tile items: item idx covers tiles [idx, idx + kTilesPerItem) of its
+// Tile items (k = 8, 16, 32): item idx covers tiles [idx, idx + kTilesPerItem) of its
 // matrix, taken from the queue as in batch_kernel.
 constexpr int64_t kTilesPerItem = 4;
 
-template <typename I, typename V>
-__global__ void __launch_bounds__(kBatchBlock, 2) batch_tile8_kernel(const BatchItem* __restrict__ items,
-                                                                    int64_t nitems, const BatchMat* __restrict__ mats,
-                                                                    V alpha, V beta, bool bz,
-                                                                    unsigned long long* __restrict__ next_item) {
+template <typename I, typename V, int G>
+__global__ void __launch_bounds__(kBatchBlock, 2) batch_tile_kernel(const BatchItem* __restrict__ items,
+                                                                   int64_t nitems, const BatchMat* __restrict__ mats,
+                                                                   V alpha, V beta, bool bz,
+                                                                   unsigned long long* __restrict__ next_item) {
   const int lane = threadIdx.x & 31;
   unsigned long long grab = 0, ahead = 0;
   if (lane == 0) {
@@ -171,10 +171,10 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_tile8_kernel(const Batch
       const BatchMat& M = mats[it.mat];
       const int64_t t1 = it.idx + kTilesPerItem < M.tiles ? it.idx + kTilesPerItem : M.tiles;
       for (int64_t t = it.idx; t < t1; ++t)
-        spmm8_tile_pairs<I, V>(static_cast<const I*>(M.rp), M.rows, M.nnz, static_cast<const I*>(M.ci),
-                         static_cast<const V*>(M.val), M.tile_row, M.tflags, t, static_cast<const V*>(M.x), M.ldx,
-                         static_cast<V*>(M.y), M.ldy, alpha, beta, bz, static_cast<V*>(M.tcin),
-                         static_cast<V*>(M.tosum), M.topen, lane);
+        spmm_tile_groups<I, V, G>(static_cast<const I*>(M.rp), M.rows, M.nnz, static_cast<const I*>(M.ci),
+                                  static_cast<const V*>(M.val), M.tile_row, M.tflags, t, static_cast<const V*>(M.x),
+                                  M.ldx, static_cast<V*>(M.y), M.ldy, alpha, beta, bz, static_cast<V*>(M.tcin),
+                                  static_cast<V*>(M.tosum), M.topen, lane);
     }
     grab = __shfl_sync(0xffffffffu, ahead, 0);
     if (lane == 0 && (int64_t)grab < nitems) ahead = atomicAdd(next_item, (unsigned long long)kGrab);
@@ -183,10 +183,10 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_tile8_kernel(const Batch
 
 // Calibration of every tile matrix: thread g takes entry g - cal_off[i] of
 // tile matrix i (its tiles, then its empty rows).
-template <typename V>
-__global__ void batch_calibrate8_kernel(const int64_t* __restrict__ cal_off, const int32_t* __restrict__ cal_mat,
-                                        int ncal, int64_t total, const BatchMat* __restrict__ mats, V alpha, V beta,
-                                        bool bz) {
+template <typename V, int KC>
+__global__ void batch_calibrate_kernel(const int64_t* __restrict__ cal_off, const int32_t* __restrict__ cal_mat,
+                                       int ncal, int64_t total, const BatchMat* __restrict__ mats, V alpha, V beta,
+                                       bool bz) {
   const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (g >= total) return;
   int lo = 0, hi = ncal;  // last i with cal_off[i] <= g
@@ -195,8 +195,8 @@ __global__ void batch_calibrate8_kernel(const int64_t* __restrict__ cal_off, con
     if (cal_off[mid] <= g) lo = mid; else hi = mid;
   }
   const BatchMat& M = mats[cal_mat[lo]];
-  spmm8_calibrate<V>(g - cal_off[lo], M.tiles, static_cast<const V*>(M.tcin), static_cast<const V*>(M.tosum),
-                     M.topen, M.tempty, M.tnempty, static_cast<V*>(M.y), M.ldy, alpha, beta, bz);
+  spmm_calibrate<V, KC>(g - cal_off[lo], M.tiles, static_cast<const V*>(M.tcin), static_cast<const V*>(M.tosum),
+                        M.topen, M.tempty, M.tnempty, static_cast<V*>(M.y), M.ldy, alpha, beta, bz);
 }
 
 // Single-matrix SpMM over the CSR plan (the per-matrix path of spops_spmm).
@@ -290,12 +290,13 @@ spops_status_t csr_spmm(Context* ctx, Matrix* A, double alpha, const void* X, in
                         void* Y, int64_t ldy) {
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "SpMM needs a CSR matrix");
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
-  // k = 8 with narrow X rows: register tiles on the SpMV's plan.  (Passes of
-  // 8 columns over wider rows measured slower than the segment kernel: at
-  // k = 32 four passes took 20.5 ms against 6.5 ms on the power-law matrix.)
-  if (k == 8 && (size_t)ldx * A->vsize() <= 128 && ctx->csr_variant == 0) {
+  // k = 8, 16, 32 with X rows at most 2k wide: register tiles on the SpMV's
+  // plan.  (Passes of 8 columns over wider rows measured slower than the
+  // segment kernel: four passes at k = 32 took 20.5 ms against 6.5 ms on the
+  // power-law matrix.)
+  if (ctx->csr_variant == 0) {
     bool used = false;
-    SPOPS_TRY(csr_tile_spmm8(ctx, A, alpha, X, ldx, beta, Y, ldy, &used));
+    SPOPS_TRY(csr_tile_spmm(ctx, A, alpha, X, ldx, k, beta, Y, ldy, &used));
     if (used) return SPOPS_OK;
   }
   const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
@@ -448,32 +449,41 @@ spops_status_t build_table(Batch* B) {
   return SPOPS_OK;
 }
 
-template <typename I, typename V>
-int tile8_blocks_per_sm() {
+template <typename I, typename V, int G>
+int tile_blocks_per_sm() {
   static int cache[kMaxDevices];
-  return blocks_per_sm(batch_tile8_kernel<I, V>, kBatchBlock, 0, cache);
+  return blocks_per_sm(batch_tile_kernel<I, V, G>, kBatchBlock, 0, cache);
+}
+
+template <typename I, typename V, int G>
+spops_status_t launch_tiles(Batch* B, double alpha, double beta, cudaStream_t st) {
+  const bool bz = beta == 0.0;
+  const int bps = tile_blocks_per_sm<I, V, G>();
+  if (bps < 1) return fail(SPOPS_ERR_CUDA, "batch: kernel attributes could not be set");
+  int64_t grid = (int64_t)B->ctx->num_sms * bps;
+  const int64_t need = (B->ntitems + 7) / 8;
+  if (grid > need) grid = need;
+  SPOPS_CUDA(cudaMemsetAsync(B->tqueue.p, 0, 8, st));
+  batch_tile_kernel<I, V, G><<<(unsigned)grid, kBatchBlock, 0, st>>>(B->titems.as<BatchItem>(), B->ntitems,
+                                                                    B->table.as<BatchMat>(), (V)alpha, (V)beta, bz,
+                                                                    B->tqueue.as<unsigned long long>());
+  SPOPS_LAUNCH_CHECK();
+  if (B->ncal_total > 0) {
+    batch_calibrate_kernel<V, 4 * G><<<(unsigned)((B->ncal_total + 255) / 256), 256, 0, st>>>(
+        B->cal_off.as<int64_t>(), B->cal_mat.as<int32_t>(), B->ncal, B->ncal_total, B->table.as<BatchMat>(),
+        (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
 }
 
 template <typename I, typename V>
 spops_status_t launch_batch(Batch* B, double alpha, double beta, cudaStream_t st) {
   const bool bz = beta == 0.0;
-  if (B->ntitems > 0) {  // k = 8 tile items, then their calibration
-    const int bps = tile8_blocks_per_sm<I, V>();
-    if (bps < 1) return fail(SPOPS_ERR_CUDA, "batch: kernel attributes could not be set");
-    int64_t grid = (int64_t)B->ctx->num_sms * bps;
-    const int64_t need = (B->ntitems + 7) / 8;
-    if (grid > need) grid = need;
-    SPOPS_CUDA(cudaMemsetAsync(B->tqueue.p, 0, 8, st));
-    batch_tile8_kernel<I, V><<<(unsigned)grid, kBatchBlock, 0, st>>>(B->titems.as<BatchItem>(), B->ntitems,
-                                                                   B->table.as<BatchMat>(), (V)alpha, (V)beta, bz,
-                                                                   B->tqueue.as<unsigned long long>());
-    SPOPS_LAUNCH_CHECK();
-    if (B->ncal_total > 0) {
-      batch_calibrate8_kernel<V><<<(unsigned)((B->ncal_total + 255) / 256), 256, 0, st>>>(
-          B->cal_off.as<int64_t>(), B->cal_mat.as<int32_t>(), B->ncal, B->ncal_total, B->table.as<BatchMat>(),
-          (V)alpha, (V)beta, bz);
-      SPOPS_LAUNCH_CHECK();
-    }
+  if (B->ntitems > 0) {  // tile items, then their calibration
+    if (B->k == 8) SPOPS_TRY((launch_tiles<I, V, 2>(B, alpha, beta, st)));
+    else if (B->k == 16) SPOPS_TRY((launch_tiles<I, V, 4>(B, alpha, beta, st)));
+    else SPOPS_TRY((launch_tiles<I, V, 8>(B, alpha, beta, st)));
   }
   if (B->nitems == 0) return SPOPS_OK;
   auto go = [&](auto kern, size_t smem, int bps) -> spops_status_t {
@@ -509,13 +519,12 @@ spops_status_t prepare(Batch* B) {
   for (int64_t m = 0; m < B->count; ++m) {
     Matrix* A = B->src[m];
     if (!A->plan.ready) SPOPS_TRY(csr_analyse(B->ctx, A));
-    // k = 8 over X rows of at most 128 bytes, vector loads aligned: register tiles
+    // k = 8, 16, 32 over X rows at most 2k wide, vector loads aligned: register tiles
     const BatchMat& h = B->host[m];
     const size_t vs = A->vsize();
-    if (B->k == 8 && A->rows > 0 && A->nnz > 0 && csr_tile_usable(A, 0) && ((uintptr_t)h.x % 32) == 0 &&
-        ((size_t)h.ldx * vs) % 32 == 0 && (size_t)h.ldx * vs <= 128) {
+    if (csr_tile_spmm_usable(A, h.x, h.ldx, B->k) && h.ldy >= B->k) {
       if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(B->ctx, A, 8));
-      const size_t bytes = (size_t)A->plan.tiles.tiles * 8 * vs;
+      const size_t bytes = (size_t)A->plan.tiles.tiles * (size_t)B->k * vs;
       if (B->t_cin[m].bytes < bytes) SPOPS_TRY(B->t_cin[m].alloc(bytes));
       if (B->t_osum[m].bytes < bytes) SPOPS_TRY(B->t_osum[m].alloc(bytes));
       B->tile_ok[m] = 1;

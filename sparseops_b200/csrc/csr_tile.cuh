@@ -81,8 +81,8 @@ __device__ __forceinline__ void tile_load(const I* __restrict__ ci, const V* __r
   }
 }
 
-// ---- multi-RHS with k = 8 on the SpMV's tile plan (csr_tile_spmm8 and the
-// batch's tile items)
+// ---- multi-RHS with k = 8, 16, 32 on the SpMV's tile plan (csr_tile_spmm
+// and the batch's tile items)
 template <typename V>
 __device__ __forceinline__ void axpby_store8(V* __restrict__ y, const V (&v)[8], V alpha, V beta, bool bz) {
 #pragma unroll
@@ -106,55 +106,59 @@ __device__ __forceinline__ void ld_xhalf(const V* __restrict__ p, V (&r)[4]) {
   }
 }
 
-// One tile t of a k = 8 product with lane pairs: lanes 2p and 2p + 1 take the
-// 16 consecutive entries of the plan's lanes 2p and 2p + 1, lane 2p + h
-// holding columns 4h .. 4h + 3.  Both lanes of a pair gather the same X row
-// in one instruction (32 bytes each), so each row costs one request.  The
-// pair's row starts are the two lanes' flags; the heads combine over the 16
-// pairs with the segmented scan, and the row open at the tile's end goes to
-// the 8-wide calibrator.  Every column is summed in an order fixed by the
+// One tile t of a multi-RHS product with k = 4G columns, G lanes per entry:
+// group q (lanes qG .. qG + G - 1) takes the 8G consecutive entries of the
+// plan's lanes qG .. qG + G - 1, lane qG + h holding columns 4h .. 4h + 3.
+// The group's lanes gather an entry's whole X row in one instruction (32
+// bytes each for FP64), so a row costs one L2 request per 128 bytes.  The
+// group's row starts are its G lanes' flags; the heads combine over the 32/G
+// groups with the segmented scan, and the row open at the tile's end goes to
+// the k-wide calibrator.  Every column is summed in an order fixed by the
 // matrix.
-template <typename I, typename V>
-__device__ __forceinline__ void spmm8_tile_pairs(const I* __restrict__ rp, int64_t n, int64_t nnz,
+template <typename I, typename V, int G>
+__device__ __forceinline__ void spmm_tile_groups(const I* __restrict__ rp, int64_t n, int64_t nnz,
                                                  const I* __restrict__ ci, const V* __restrict__ val,
                                                  const int64_t* __restrict__ tile_row,
                                                  const uint8_t* __restrict__ flags_all, int64_t t,
                                                  const V* __restrict__ X, int64_t ldx, V* __restrict__ Y, int64_t ldy,
                                                  V alpha, V beta, bool bz, V* __restrict__ carry_in,
                                                  V* __restrict__ open_sum, int64_t* __restrict__ open_row, int lane) {
-  constexpr int K = 8;
-  const int pr = lane >> 1, h = lane & 1;
-  const uint32_t f16 = (uint32_t)flags_all[t * 32 + 2 * pr] | ((uint32_t)flags_all[t * 32 + 2 * pr + 1] << 8);
-  const int64_t tr = tile_row[t];
-  const int64_t e0 = t * (32 * K) + (int64_t)pr * 2 * K;
-  // pair flags as a 16-bit mask (bit p: pair p holds a row start)
-  const unsigned lane_f = __ballot_sync(0xffffffffu, f16 != 0 && h == 0);
-  unsigned pf = 0;
+  constexpr int K = 8, NG = 32 / G, KC = 4 * G;
+  static_assert(G == 2 || G == 4 || G == 8, "2, 4 or 8 lanes per entry");
+  const int gq = lane / G, h = lane % G;
+  uint64_t fl = 0;  // bit b: entry b of the group's 8G starts a row
 #pragma unroll
-  for (int q = 0; q < 16; ++q) pf |= ((lane_f >> (2 * q)) & 1u) << q;
+  for (int r = 0; r < G; ++r) fl |= (uint64_t)flags_all[t * 32 + gq * G + r] << (8 * r);
+  const int64_t tr = tile_row[t];
+  const int64_t e0 = t * (32 * K) + (int64_t)gq * G * K;
+  // group flags as an NG-bit mask (bit q: group q holds a row start)
+  const unsigned lane_f = __ballot_sync(0xffffffffu, fl != 0 && h == 0);
+  unsigned gf = 0;
+#pragma unroll
+  for (int q = 0; q < NG; ++q) gf |= ((lane_f >> (G * q)) & 1u) << q;
   int64_t row;
   if (tr >= 0) {
-    const int cnt = __popc(f16);
-    const unsigned below = (1u << (2 * pr)) - 1u;  // lanes of the pairs before this one
+    const int cnt = __popcll(fl);
+    const unsigned below = (gq * G >= 32) ? 0xffffffffu : ((1u << (gq * G)) - 1u);  // lanes of earlier groups
     int excl = 0;
 #pragma unroll
-    for (int bit = 0; bit < 5; ++bit)
+    for (int bit = 0; bit < 7; ++bit)
       excl += __popc(__ballot_sync(0xffffffffu, ((cnt >> bit) & 1) && h == 0) & below) << bit;
-    const int first0 = (int)(__ballot_sync(0xffffffffu, f16 & 1u) & 1u);
-    row = tr + excl + (int)(f16 & 1u) - first0;
+    const int first0 = (int)(__ballot_sync(0xffffffffu, fl & 1u) & 1u);
+    row = tr + excl + (int)(fl & 1u) - first0;
   } else {
     row = row_holding(rp, n, e0 < nnz ? e0 : nnz - 1);
   }
   V acc[4], head[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) acc[j] = head[j] = V(0);
-  bool in_head = (f16 & 1u) == 0;
+  bool in_head = (fl & 1u) == 0;
   V* Yh = Y + 4 * h;
-#pragma unroll
-  for (int run = 0; run < 2; ++run) {  // plan lane 2p, then 2p + 1
+#pragma unroll 1
+  for (int run = 0; run < G; ++run) {  // plan lanes qG, qG + 1, ...
     I c[K];
     V a[K];
-    tile_load<I, V, K>(ci, val, nnz, t, 2 * pr + run, c, a);
+    tile_load<I, V, K>(ci, val, nnz, t, gq * G + run, c, a);
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
       V xr[4][4];
@@ -163,7 +167,7 @@ __device__ __forceinline__ void spmm8_tile_pairs(const I* __restrict__ rp, int64
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int b = run * K + 4 * half + q;
-        if (b > 0 && ((f16 >> b) & 1u)) {
+        if (b > 0 && ((fl >> b) & 1u)) {
           if (in_head) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) head[j] = acc[j];
@@ -192,26 +196,26 @@ __device__ __forceinline__ void spmm8_tile_pairs(const I* __restrict__ rp, int64
     if (in_head) head[j] = acc[j];
     tail[j] = in_head ? V(0) : acc[j];
   }
-  const bool has_flag = f16 != 0;
-  const unsigned starts = (pf << 1) | 1u;  // pair p starts a segment if pair p - 1 is flagged (or p == 0)
+  const bool has_flag = fl != 0;
+  const unsigned starts = (gf << 1) | 1u;  // group q starts a segment if group q - 1 is flagged (or q == 0)
 #pragma unroll
-  for (int o = 1; o < 16; o <<= 1) {
-    const unsigned span = (pr >= o) ? ((2u << pr) - 1u) & ~((2u << (pr - o)) - 1u) : 0u;
-    const bool add = pr >= o && !(starts & span);
+  for (int o = 1; o < NG; o <<= 1) {
+    const unsigned span = (gq >= o) ? ((2u << gq) - 1u) & ~((2u << (gq - o)) - 1u) : 0u;
+    const bool add = gq >= o && !(starts & span);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const V su = __shfl_up_sync(0xffffffffu, head[j], 2 * o);
+      const V su = __shfl_up_sync(0xffffffffu, head[j], G * o);
       if (add) head[j] += su;
     }
   }
-  const unsigned later = pf & ~((2u << pr) - 1u);
-  const int m = later ? __ffs(later) - 1 : 15;
-  const int m0 = pf ? __ffs(pf) - 1 : 15;
+  const unsigned later = gf & ~((2u << gq) - 1u);
+  const int m = later ? __ffs(later) - 1 : NG - 1;
+  const int m0 = gf ? __ffs(gf) - 1 : NG - 1;
   V Sm[4], cin[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    Sm[j] = __shfl_sync(0xffffffffu, head[j], 2 * m + h);
-    cin[j] = __shfl_sync(0xffffffffu, head[j], 2 * m0 + h);
+    Sm[j] = __shfl_sync(0xffffffffu, head[j], G * m + h);
+    cin[j] = __shfl_sync(0xffffffffu, head[j], G * m0 + h);
   }
   if (has_flag) {
     if (later) {
@@ -219,40 +223,42 @@ __device__ __forceinline__ void spmm8_tile_pairs(const I* __restrict__ rp, int64
       for (int j = 0; j < 4; ++j) axpby_store(Yh + row * ldy + j, tail[j] + Sm[j], alpha, beta, bz);
     } else {  // the tile's last row: may continue into the next tile
 #pragma unroll
-      for (int j = 0; j < 4; ++j) open_sum[t * 8 + 4 * h + j] = tail[j] + (pr < 15 ? Sm[j] : V(0));
+      for (int j = 0; j < 4; ++j) open_sum[t * KC + 4 * h + j] = tail[j] + (gq < NG - 1 ? Sm[j] : V(0));
       if (h == 0) open_row[t] = row;
     }
   }
-  if (pr == 0) {
+  if (gq == 0) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) carry_in[t * 8 + 4 * h + j] = cin[j];
-    if (h == 0 && !pf) open_row[t] = -1;
+    for (int j = 0; j < 4; ++j) carry_in[t * KC + 4 * h + j] = cin[j];
+    if (h == 0 && !gf) open_row[t] = -1;
   }
 }
 
 // Calibration of one tile t (t < tiles) or empty row (t - tiles < nempty)
-// of a k = 8 product.
-template <typename V>
-__device__ __forceinline__ void spmm8_calibrate(int64_t t, int64_t tiles, const V* __restrict__ carry_in,
-                                                const V* __restrict__ open_sum, const int64_t* __restrict__ open_row,
-                                                const int64_t* __restrict__ empty, int64_t nempty, V* __restrict__ Y,
-                                                int64_t ldy, V alpha, V beta, bool bz) {
+// of a product with KC columns (8 at a time).
+template <typename V, int KC>
+__device__ __forceinline__ void spmm_calibrate(int64_t t, int64_t tiles, const V* __restrict__ carry_in,
+                                               const V* __restrict__ open_sum, const int64_t* __restrict__ open_row,
+                                               const int64_t* __restrict__ empty, int64_t nempty, V* __restrict__ Y,
+                                               int64_t ldy, V alpha, V beta, bool bz) {
   V tot[8];
   if (t < tiles) {
     const int64_t r = open_row[t];
     if (r < 0) return;
+    for (int c0 = 0; c0 < KC; c0 += 8) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) tot[j] = open_sum[t * 8 + j];
-    for (int64_t u = t + 1; u < tiles; ++u) {
+      for (int j = 0; j < 8; ++j) tot[j] = open_sum[t * KC + c0 + j];
+      for (int64_t u = t + 1; u < tiles; ++u) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) tot[j] += carry_in[u * 8 + j];
-      if (open_row[u] >= 0) break;
+        for (int j = 0; j < 8; ++j) tot[j] += carry_in[u * KC + c0 + j];
+        if (open_row[u] >= 0) break;
+      }
+      axpby_store8(Y + r * ldy + c0, tot, alpha, beta, bz);
     }
-    axpby_store8(Y + r * ldy, tot, alpha, beta, bz);
   } else if (t - tiles < nempty) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) tot[j] = V(0);
-    axpby_store8(Y + empty[t - tiles] * ldy, tot, alpha, beta, bz);
+    for (int c0 = 0; c0 < KC; c0 += 8) axpby_store8(Y + empty[t - tiles] * ldy + c0, tot, alpha, beta, bz);
   }
 }
 

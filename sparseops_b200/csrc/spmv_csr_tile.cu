@@ -226,10 +226,10 @@ __global__ void csr_tile_calibrate_kernel(int64_t t_begin, int64_t tiles, const 
   }
 }
 
-// ---- multi-RHS with k = 8 on the same tile plan (csr_tile_spmm8); the
-// per-tile work is spmm8_tile_pairs (csr_tile.cuh)
-template <typename I, typename V>
-__global__ void __launch_bounds__(kTileBlock, 2) csr_tile_spmm8_kernel(
+// ---- multi-RHS with k = 4G on the same tile plan (csr_tile_spmm); the
+// per-tile work is spmm_tile_groups (csr_tile.cuh)
+template <typename I, typename V, int G>
+__global__ void __launch_bounds__(kTileBlock, 2) csr_tile_spmm_kernel(
     const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
     const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t tiles,
     const V* __restrict__ X, int64_t ldx, V* __restrict__ Y, int64_t ldy, V alpha, V beta, bool bz,
@@ -237,51 +237,60 @@ __global__ void __launch_bounds__(kTileBlock, 2) csr_tile_spmm8_kernel(
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
   for (int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5); t < tiles; t += nw)
-    spmm8_tile_pairs<I, V>(rp, n, nnz, ci, val, tile_row, flags_all, t, X, ldx, Y, ldy, alpha, beta, bz, carry_in,
-                     open_sum, open_row, lane);
+    spmm_tile_groups<I, V, G>(rp, n, nnz, ci, val, tile_row, flags_all, t, X, ldx, Y, ldy, alpha, beta, bz,
+                              carry_in, open_sum, open_row, lane);
 }
 
-template <typename V>
-__global__ void csr_tile_calibrate8_kernel(int64_t tiles, const V* __restrict__ carry_in,
-                                           const V* __restrict__ open_sum, const int64_t* __restrict__ open_row,
-                                           const int64_t* __restrict__ empty, int64_t nempty, V* __restrict__ Y,
-                                           int64_t ldy, V alpha, V beta, bool bz) {
-  spmm8_calibrate<V>(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, tiles, carry_in, open_sum, open_row, empty,
-                     nempty, Y, ldy, alpha, beta, bz);
+template <typename V, int KC>
+__global__ void csr_tile_calibrate_k_kernel(int64_t tiles, const V* __restrict__ carry_in,
+                                            const V* __restrict__ open_sum, const int64_t* __restrict__ open_row,
+                                            const int64_t* __restrict__ empty, int64_t nempty, V* __restrict__ Y,
+                                            int64_t ldy, V alpha, V beta, bool bz) {
+  spmm_calibrate<V, KC>(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, tiles, carry_in, open_sum, open_row, empty,
+                        nempty, Y, ldy, alpha, beta, bz);
 }
 
-template <typename I, typename V>
-spops_status_t spmm8_t(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, double beta, void* Y,
-                       int64_t ldy) {
+template <typename I, typename V, int G>
+spops_status_t spmm_tiles_t(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, double beta, void* Y,
+                            int64_t ldy) {
+  constexpr int KC = 4 * G;
   const CsrTiles& D = A->plan.tiles;
   const bool bz = beta == 0.0;
   PoolBuf cin(ctx), osum(ctx);
   const size_t nt1 = (size_t)(D.tiles > 0 ? D.tiles : 1);
-  SPOPS_TRY(cin.alloc(nt1 * 8 * sizeof(V)));
-  SPOPS_TRY(osum.alloc(nt1 * 8 * sizeof(V)));
+  SPOPS_TRY(cin.alloc(nt1 * KC * sizeof(V)));
+  SPOPS_TRY(osum.alloc(nt1 * KC * sizeof(V)));
   if (D.tiles > 0) {
     static int blocks_per_sm = -1;  // per instantiation
     if (blocks_per_sm < 0) {
       int bps = 0;
-      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_spmm8_kernel<I, V>, kTileBlock, 0));
+      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_spmm_kernel<I, V, G>, kTileBlock, 0));
       blocks_per_sm = bps > 0 ? bps : 1;
     }
     int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
     const int64_t need = (D.tiles + kTileBlock / 32 - 1) / (kTileBlock / 32);
     if (grid > need) grid = need;
-    csr_tile_spmm8_kernel<I, V><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
+    csr_tile_spmm_kernel<I, V, G><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
         A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), A->val.as<V>(), D.tile_row.as<int64_t>(),
         D.flags.as<uint8_t>(), D.tiles, static_cast<const V*>(X), ldx, static_cast<V*>(Y), ldy, (V)alpha, (V)beta,
         bz, cin.as<V>(), osum.as<V>(), D.open_row.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
   }
   if (D.tiles + D.nempty > 0) {
-    csr_tile_calibrate8_kernel<V><<<grid_of(D.tiles + D.nempty), 256, 0, ctx->stream>>>(
+    csr_tile_calibrate_k_kernel<V, KC><<<grid_of(D.tiles + D.nempty), 256, 0, ctx->stream>>>(
         D.tiles, cin.as<V>(), osum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), D.nempty,
         static_cast<V*>(Y), ldy, (V)alpha, (V)beta, bz);
     SPOPS_LAUNCH_CHECK();
   }
   return SPOPS_OK;
+}
+
+template <typename I, typename V>
+spops_status_t spmm_tiles_k(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k,
+                            double beta, void* Y, int64_t ldy) {
+  if (k == 8) return spmm_tiles_t<I, V, 2>(ctx, A, alpha, X, ldx, beta, Y, ldy);
+  if (k == 16) return spmm_tiles_t<I, V, 4>(ctx, A, alpha, X, ldx, beta, Y, ldy);
+  return spmm_tiles_t<I, V, 8>(ctx, A, alpha, X, ldx, beta, Y, ldy);
 }
 
 // Boundaries of `parts` tile ranges for the pipelined host SpMV: range p
@@ -463,21 +472,23 @@ spops_status_t csr_tile_spmv_parts(Context* ctx, Matrix* A, int parts, double al
   return spmv_parts_t<int64_t, float>(ctx, A, alpha, x, beta, y, D.part_tb, D.part_rb, done);
 }
 
-spops_status_t csr_tile_spmm8(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, double beta,
-                              void* Y, int64_t ldy, bool* used) {
-  *used = false;
+bool csr_tile_spmm_usable(const Matrix* A, const void* X, int64_t ldx, int64_t k) {
   const size_t vs = A->vsize();
-  // 32-byte vector gathers of X rows; the tile plan's vector loads of A
-  if (A->rows <= 0 || A->nnz <= 0 || !csr_tile_usable(A, 0) || ((uintptr_t)X % 32) != 0 ||
-      ((size_t)ldx * vs) % 32 != 0 || ldx < 8 || ldy < 8)
-    return SPOPS_OK;
+  return (k == 8 || k == 16 || k == 32) && A->rows > 0 && A->nnz > 0 && csr_tile_usable(A, 0) &&
+         ((uintptr_t)X % 32) == 0 && ((size_t)ldx * vs) % 32 == 0 && ldx >= k && ldx <= 2 * k;
+}
+
+spops_status_t csr_tile_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k,
+                             double beta, void* Y, int64_t ldy, bool* used) {
+  *used = false;
+  if (!csr_tile_spmm_usable(A, X, ldx, k) || ldy < k) return SPOPS_OK;
   if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(ctx, A, 8));
   *used = true;
   const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
-  if (i32 && f64) return spmm8_t<int32_t, double>(ctx, A, alpha, X, ldx, beta, Y, ldy);
-  if (i32) return spmm8_t<int32_t, float>(ctx, A, alpha, X, ldx, beta, Y, ldy);
-  if (f64) return spmm8_t<int64_t, double>(ctx, A, alpha, X, ldx, beta, Y, ldy);
-  return spmm8_t<int64_t, float>(ctx, A, alpha, X, ldx, beta, Y, ldy);
+  if (i32 && f64) return spmm_tiles_k<int32_t, double>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+  if (i32) return spmm_tiles_k<int32_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+  if (f64) return spmm_tiles_k<int64_t, double>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+  return spmm_tiles_k<int64_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
 }
 
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta,

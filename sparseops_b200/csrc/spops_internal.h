@@ -332,11 +332,12 @@ spops_status_t csr_spmv(Context* ctx, Matrix* A, double alpha, const void* x, do
 // tile kernel (spmv_csr_tile.cu); usable when the column and value arrays are
 // aligned for the lane's vector loads
 bool csr_tile_usable(const Matrix* A, int variant);
-// Y = alpha*A*X + beta*Y with exactly 8 right-hand sides on the SpMV's tile
-// plan; *used = false (nothing done) when the matrix or X is not aligned for
-// its vector loads.
-spops_status_t csr_tile_spmm8(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, double beta,
-                              void* Y, int64_t ldy, bool* used);
+// Y = alpha*A*X + beta*Y with k = 8, 16 or 32 right-hand sides on the SpMV's
+// tile plan (k / 4 lanes per entry); *used = false (nothing done) unless the
+// matrix and X allow its vector loads and X's row stride is at most 2k.
+bool csr_tile_spmm_usable(const Matrix* A, const void* X, int64_t ldx, int64_t k);
+spops_status_t csr_tile_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k,
+                             double beta, void* Y, int64_t ldy, bool* used);
 spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k);
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y);
 // The default tile SpMV in `parts` row ranges; done(r0, r1) is called after

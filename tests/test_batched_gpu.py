@@ -35,7 +35,7 @@ def _err(orc, rp, ci, v, X, Y, Yref, alpha, beta, Y0):
     return (np.abs(Y - Yref) / np.maximum(den, 1e-300)).max()
 
 
-@pytest.mark.parametrize("k", [1, 8, 32])
+@pytest.mark.parametrize("k", [1, 8, 16, 32])
 @pytest.mark.parametrize("tune", [False, True])
 def test_batch_matches_oracle(cuda, orc, k, tune):
     import torch
@@ -90,7 +90,7 @@ def test_graph_capture_replay(cuda, orc):
         assert (np.abs(y.cpu().numpy() - ref) / orc.absdot(rp, ci, v, x)).max() <= 1e-12
 
 
-@pytest.mark.parametrize("k", [3, 8, 32, 40])
+@pytest.mark.parametrize("k", [3, 8, 16, 32, 40])
 def test_single_spmm(cuda, orc, k):
     import torch
     from sparseops_b200 import CSR_Matrix, SpMM_csr
