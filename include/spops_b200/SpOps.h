@@ -15,6 +15,9 @@
  *   read_coo_matrix, read_csr_matrix                                  Matrix Market files
  *   LeSpGEMM<sortOutput>(A, B, C, kernel_flag), HashSpGEMMTopK(A, C, top_k)
  *   MTX<I,V>: MtxLoad, CalculateFeatures, FeaturesPrint, FeaturesWrite ...  features
+ *   read_<fmt>_matrix, coo_to_ell, sum_csr_duplicates, csr_transpose,
+ *   csr_to_binary_pattern, minhash_estimated_jaccard, delete_<fmt>_matrix,
+ *   Le_*_thread_* (kept settings only)
  *                                                                     row-wise SpGEMM (include/spgemm.h)
  *
  * What differs, and why:
@@ -48,6 +51,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <unordered_map>
 #include <vector>
@@ -70,6 +74,9 @@
 #endif
 #ifndef SIMD_WIDTH
 #define SIMD_WIDTH 256
+#endif
+#ifndef KERNEL_FLAG
+#define KERNEL_FLAG 1
 #endif
 
 typedef enum { RowMajor = 0, ColMajor = 1 } LeadingDimension;
@@ -1085,6 +1092,205 @@ void HashSpGEMMTopK(const CSR_Matrix<IndexType, ValueType>& A, CSR_Matrix<IndexT
   d::check(s, "spops_spgemm_topk");
   d::take_csr<IndexType, ValueType>(c, C);
   C.kernel_flag = 0;
+}
+
+/* ----------------------------------------- more of the reference's API */
+/* Per-format deletes (include/sparse_format.h:300-420): delete_host_matrix. */
+template <class I, class V> void delete_coo_matrix(COO_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_csr_matrix(CSR_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_bsr_matrix(BSR_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_dia_matrix(DIA_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_ell_matrix(ELL_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_s_ell_matrix(S_ELL_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_s_ell_c_sigma_matrix(SELL_C_Sigma_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class V> void delete_s_ell_c_R_matrix(SELL_C_R_Matrix<I, V>& m) { delete_host_matrix(m); }
+template <class I, class U, class V> void delete_csr5_matrix(CSR5_Matrix<I, U, V>& m) { delete_host_matrix(m); }
+
+/* The reference's OpenMP thread controls (include/thread.h).  The work runs on
+ * the GPU, so they only keep the caller's setting for its own queries. */
+namespace spops_b200 {
+namespace detail {
+inline int& thread_setting() {
+  static int n = 0;
+  return n;
+}
+}  // namespace detail
+}  // namespace spops_b200
+inline int Le_get_core_num() {
+  const unsigned c = std::thread::hardware_concurrency();
+  return c ? (int)c : 1;
+}
+inline void Le_set_thread_num(const int thread_num) { spops_b200::detail::thread_setting() = thread_num; }
+inline int Le_get_thread_num() {
+  const int n = spops_b200::detail::thread_setting();
+  return n > 0 ? n : Le_get_core_num();
+}
+inline int Le_get_thread_id() { return 0; }
+inline void set_omp_schedule(int, int) {}
+
+/* coo_to_ell (include/sparse_conversion.h:102): the rows keep the COO's
+ * entry order, as through coo_to_csr. */
+template <class IndexType, class ValueType>
+ELL_Matrix<IndexType, ValueType> coo_to_ell(const COO_Matrix<IndexType, ValueType>& coo,
+                                            const LeadingDimension ld = RowMajor) {
+  CSR_Matrix<IndexType, ValueType> csr = coo_to_csr(coo, false);
+  ELL_Matrix<IndexType, ValueType> ell = csr_to_ell(csr, ld);
+  delete_host_matrix(csr);
+  return ell;
+}
+
+/* Matrix Market files straight into a format (utils/sparse_io.cpp:225-390):
+ * read_csr_matrix (or read_coo_matrix for ELL) and the conversion, on the
+ * device; the reference's feature file argument is not written. */
+template <class IndexType, class ValueType>
+ELL_Matrix<IndexType, ValueType> read_ell_matrix(const char* mm_filename, LeadingDimension ld = RowMajor) {
+  COO_Matrix<IndexType, ValueType> coo = read_coo_matrix<IndexType, ValueType>(mm_filename);
+  ELL_Matrix<IndexType, ValueType> ell;
+  if (coo.num_rows == 0) {
+    std::memset(static_cast<void*>(&ell), 0, sizeof(ell));
+    delete_host_matrix(coo);
+    return ell;
+  }
+  ell = coo_to_ell(coo, ld);
+  delete_host_matrix(coo);
+  ell.kernel_flag = KERNEL_FLAG;
+  return ell;
+}
+template <class IndexType, class ValueType>
+DIA_Matrix<IndexType, ValueType> read_dia_matrix(const char* mm_filename,
+                                                 const spops_b200::detail::same_t<IndexType> max_diags,
+                                                 const spops_b200::detail::same_t<IndexType> alignment =
+                                                     (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  CSR_Matrix<IndexType, ValueType> csr = read_csr_matrix<IndexType, ValueType>(mm_filename);
+  DIA_Matrix<IndexType, ValueType> m = csr_to_dia(csr, max_diags, nullptr, alignment);
+  delete_host_matrix(csr);
+  return m;
+}
+template <class IndexType, class ValueType>
+S_ELL_Matrix<IndexType, ValueType> read_sell_matrix(const char* mm_filename, const int chunkwidth,
+                                                    const spops_b200::detail::same_t<IndexType> alignment) {
+  CSR_Matrix<IndexType, ValueType> csr = read_csr_matrix<IndexType, ValueType>(mm_filename);
+  S_ELL_Matrix<IndexType, ValueType> m = csr_to_sell(csr, nullptr, chunkwidth, alignment);
+  delete_host_matrix(csr);
+  return m;
+}
+template <class IndexType, class ValueType>
+SELL_C_Sigma_Matrix<IndexType, ValueType> read_sell_c_sigma_matrix(
+    const char* mm_filename, const int slicewidth, const int chunkwidth,
+    const spops_b200::detail::same_t<IndexType> alignment) {
+  CSR_Matrix<IndexType, ValueType> csr = read_csr_matrix<IndexType, ValueType>(mm_filename);
+  SELL_C_Sigma_Matrix<IndexType, ValueType> m = csr_to_sell_c_sigma(csr, nullptr, slicewidth, chunkwidth, alignment);
+  delete_host_matrix(csr);
+  return m;
+}
+template <class IndexType, class ValueType>
+SELL_C_R_Matrix<IndexType, ValueType> read_sell_c_R_matrix(const char* mm_filename, const int chunkwidth,
+                                                           const spops_b200::detail::same_t<IndexType> alignment) {
+  CSR_Matrix<IndexType, ValueType> csr = read_csr_matrix<IndexType, ValueType>(mm_filename);
+  SELL_C_R_Matrix<IndexType, ValueType> m = csr_to_sell_c_R(csr, nullptr, chunkwidth, alignment);
+  delete_host_matrix(csr);
+  return m;
+}
+template <class IndexType, class ValueType>
+BSR_Matrix<IndexType, ValueType> read_bsr_matrix(const char* mm_filename,
+                                                 const spops_b200::detail::same_t<IndexType> blockDimRow =
+                                                     BSR_BlockDimRow,
+                                                 const spops_b200::detail::same_t<IndexType> blockDimCol =
+                                                     (SIMD_WIDTH / 8 / sizeof(ValueType))) {
+  CSR_Matrix<IndexType, ValueType> csr = read_csr_matrix<IndexType, ValueType>(mm_filename);
+  BSR_Matrix<IndexType, ValueType> m = csr_to_bsr(csr, blockDimRow, blockDimCol);
+  delete_host_matrix(csr);
+  return m;
+}
+template <class IndexType, class UIndexType, class ValueType>
+CSR5_Matrix<IndexType, UIndexType, ValueType> read_csr5_matrix(const char* mm_filename) {
+  CSR_Matrix<IndexType, ValueType> csr = read_csr_matrix<IndexType, ValueType>(mm_filename);
+  CSR5_Matrix<IndexType, UIndexType, ValueType> m = csr_to_csr5<IndexType, UIndexType, ValueType>(csr, nullptr);
+  delete_host_matrix(csr);
+  return m;
+}
+
+/* sum_csr_duplicates (include/sparse_operation.h:21): duplicates of a row
+ * summed, the row's columns in reverse order of first appearance, exact
+ * zeros dropped, in place (row_ptr[num_rows] becomes the new count) -- the
+ * device coo_to_csr's compact mode. */
+template <class IndexType, class ValueType>
+void sum_csr_duplicates(const IndexType num_rows, const IndexType num_cols, IndexType* row_ptr, IndexType* col_index,
+                        ValueType* values) {
+  const IndexType nnz = num_rows > 0 ? row_ptr[num_rows] : 0;
+  COO_Matrix<IndexType, ValueType> coo;
+  std::memset(static_cast<void*>(&coo), 0, sizeof(coo));
+  coo.num_rows = num_rows;
+  coo.num_cols = num_cols;
+  coo.num_nnzs = nnz;
+  std::vector<IndexType> rows((size_t)nnz);
+  for (IndexType r = 0; r < num_rows; ++r)
+    for (IndexType k = row_ptr[r]; k < row_ptr[r + 1]; ++k) rows[(size_t)k] = r;
+  coo.row_index = rows.data();
+  coo.col_index = col_index;
+  coo.values = values;
+  const bool was = spops_b200::detail::caching();
+  spops_b200::set_cache(false);  // the result is copied out, nothing to keep
+  CSR_Matrix<IndexType, ValueType> c = coo_to_csr(coo, true);
+  spops_b200::set_cache(was);
+  std::memcpy(row_ptr, c.row_offset, sizeof(IndexType) * ((size_t)num_rows + 1));
+  std::memcpy(col_index, c.col_index, sizeof(IndexType) * (size_t)c.num_nnzs);
+  std::memcpy(values, c.values, sizeof(ValueType) * (size_t)c.num_nnzs);
+  delete_host_matrix(c);
+}
+
+/* csr_transpose (include/sparse_conversion.h:2067): the transpose with
+ * duplicates summed and exact zeros dropped (csr_to_coo, index swap,
+ * coo_to_csr compact), on the device. */
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> csr_transpose(const CSR_Matrix<IndexType, ValueType>& csr) {
+  if (csr.num_nnzs == 0) {
+    CSR_Matrix<IndexType, ValueType> t;
+    std::memset(static_cast<void*>(&t), 0, sizeof(t));
+    t.num_rows = csr.num_cols;
+    t.num_cols = csr.num_rows;
+    t.row_offset = spops_b200::detail::host_alloc<IndexType>((int64_t)csr.num_cols + 1);
+    std::fill_n(t.row_offset, (size_t)csr.num_cols + 1, (IndexType)0);
+    return t;
+  }
+  COO_Matrix<IndexType, ValueType> coo = csr_to_coo(csr);
+  std::swap(coo.row_index, coo.col_index);
+  std::swap(coo.num_rows, coo.num_cols);
+  spops_b200::invalidate(coo.col_index);  // the cached COO handle no longer matches the struct
+  spops_b200::invalidate(coo.row_index);
+  CSR_Matrix<IndexType, ValueType> t = coo_to_csr(coo, true);
+  delete_host_matrix(coo);
+  return t;
+}
+
+/* csr_to_binary_pattern (include/sparse_conversion.h:2121): the pattern with
+ * every value 1. */
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> csr_to_binary_pattern(const CSR_Matrix<IndexType, ValueType>& csr) {
+  namespace d = spops_b200::detail;
+  CSR_Matrix<IndexType, ValueType> b;
+  d::set_features<IndexType, ValueType>(b, csr.num_rows, csr.num_cols, csr.num_nnzs);
+  b.kernel_flag = csr.kernel_flag;
+  b.row_offset = d::host_alloc<IndexType>((int64_t)csr.num_rows + 1);
+  std::memcpy(b.row_offset, csr.row_offset, sizeof(IndexType) * ((size_t)csr.num_rows + 1));
+  b.col_index = d::host_alloc<IndexType>(csr.num_nnzs);
+  b.values = d::host_alloc<ValueType>(csr.num_nnzs);
+  if (csr.num_nnzs > 0) std::memcpy(b.col_index, csr.col_index, sizeof(IndexType) * (size_t)csr.num_nnzs);
+  std::fill_n(b.values, (size_t)csr.num_nnzs, (ValueType)1);
+  return b;
+}
+
+/* minhash_estimated_jaccard (include/spgemm_MinHashLSH.h:183-224): the share
+ * of equal signature entries. */
+inline double minhash_estimated_jaccard(const uint64_t* sig_a, const uint64_t* sig_b, int k) {
+  if (k <= 0) return 0.0;
+  int match = 0;
+  for (int d = 0; d < k; ++d) match += sig_a[d] == sig_b[d];
+  return (double)match / (double)k;
+}
+inline double minhash_estimated_jaccard(const std::vector<uint64_t>& sig_a, const std::vector<uint64_t>& sig_b) {
+  if (sig_a.size() != sig_b.size() || sig_a.empty()) return 0.0;
+  return minhash_estimated_jaccard(sig_a.data(), sig_b.data(), (int)sig_a.size());
 }
 
 /* ------------------------------------------------------------ features */

@@ -372,6 +372,85 @@ void feature_checks() {
   std::remove(path);
 }
 
+// the rest of the reference's API on a small file: read_<fmt>_matrix gives
+// the same y as the CSR read; sum_csr_duplicates, csr_transpose,
+// csr_to_binary_pattern, minhash_estimated_jaccard, the thread controls
+void api_checks() {
+  const char* path = "shim_test_api.mtx";
+  FILE* f = std::fopen(path, "w");
+  EXPECT(f != nullptr, "temporary file");
+  if (!f) return;
+  const int n = 600;
+  std::fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n%d %d %d\n", n, n, 3 * n - 2);
+  for (int r = 0; r < n; ++r)
+    for (int c = r - 1; c <= r + 1; ++c)
+      if (c >= 0 && c < n) std::fprintf(f, "%d %d %g\n", r + 1, c + 1, c == r ? 4.0 : -1.0 - 0.001 * r);
+  std::fclose(f);
+  std::vector<double> x(n), y0(n, 0.5), yc(n), y(n);
+  for (int i = 0; i < n; ++i) x[i] = 0.01 * (i % 97) - 0.3;
+  CSR_Matrix<int, double> csr = read_csr_matrix<int, double>(path);
+  yc = y0;
+  SpOps_csr(1.0, csr, x.data(), 0.5, yc.data());
+  auto same_y = [&](const char* what, auto&& op) {
+    y = y0;
+    op(y.data());
+    double worst = 0;
+    for (int i = 0; i < n; ++i) worst = std::max(worst, std::fabs(y[i] - yc[i]));
+    EXPECT(worst <= 1e-12, what);
+  };
+  ELL_Matrix<int, double> ell = read_ell_matrix<int, double>(path);
+  EXPECT(ell.num_rows == n && ell.max_row_width == 3 && ell.kernel_flag == KERNEL_FLAG, "read_ell_matrix shape");
+  same_y("read_ell_matrix y", [&](double* yy) { SpOps_ell(1.0, ell, x.data(), 0.5, yy); });
+  S_ELL_Matrix<int, double> sell = read_sell_matrix<int, double>(path, 4, 1);
+  same_y("read_sell_matrix y", [&](double* yy) { SpOps_sell(1.0, sell, x.data(), 0.5, yy); });
+  SELL_C_Sigma_Matrix<int, double> scs = read_sell_c_sigma_matrix<int, double>(path, 64, 8, 1);
+  same_y("read_sell_c_sigma_matrix y", [&](double* yy) { SpOps_sell_c_sigma(1.0, scs, x.data(), 0.5, yy); });
+  SELL_C_R_Matrix<int, double> scr = read_sell_c_R_matrix<int, double>(path, 8, 1);
+  same_y("read_sell_c_R_matrix y", [&](double* yy) { SpOps_sell_c_R(1.0, scr, x.data(), 0.5, yy); });
+  DIA_Matrix<int, double> dia = read_dia_matrix<int, double>(path, 16, 1);
+  EXPECT(dia.complete_ndiags == 3, "read_dia_matrix diagonals");
+  same_y("read_dia_matrix y", [&](double* yy) { SpOps_dia(1.0, dia, x.data(), 0.5, yy); });
+  BSR_Matrix<int, double> bsr = read_bsr_matrix<int, double>(path, 4, 4);
+  same_y("read_bsr_matrix y", [&](double* yy) { SpOps_bsr(1.0, bsr, x.data(), 0.5, yy); });
+  delete_ell_matrix(ell);
+  delete_s_ell_matrix(sell);
+  delete_s_ell_c_sigma_matrix(scs);
+  delete_s_ell_c_R_matrix(scr);
+  delete_dia_matrix(dia);
+  delete_bsr_matrix(bsr);
+  // csr_transpose of the tridiagonal matrix: entry (c, r) of the result is
+  // entry (r, c) of the input
+  CSR_Matrix<int, double> t = csr_transpose(csr);
+  bool tr_ok = t.num_rows == n && t.num_nnzs == csr.num_nnzs;
+  for (int r = 0; tr_ok && r < n; ++r)
+    for (int k = csr.row_offset[r]; k < csr.row_offset[r + 1]; ++k) {
+      const int c = csr.col_index[k];
+      bool found = false;
+      for (int q = t.row_offset[c]; q < t.row_offset[c + 1]; ++q)
+        found = found || (t.col_index[q] == r && t.values[q] == csr.values[k]);
+      tr_ok = tr_ok && found;
+    }
+  EXPECT(tr_ok, "csr_transpose entries");
+  CSR_Matrix<int, double> bp = csr_to_binary_pattern(csr);
+  EXPECT(bp.num_nnzs == csr.num_nnzs && bp.values[0] == 1.0 && bp.col_index[5] == csr.col_index[5],
+         "csr_to_binary_pattern");
+  delete_csr_matrix(t);
+  delete_csr_matrix(bp);
+  delete_csr_matrix(csr);
+  // sum_csr_duplicates: row 1 in file order 5, 3, 5, 7, 7 (7 cancels) -> 3, 5
+  int rp[3] = {0, 1, 6}, ci[6] = {2, 5, 3, 5, 7, 7};
+  double vv[6] = {1.0, 1.0, 2.0, 4.0, 1.5, -1.5};
+  sum_csr_duplicates(2, 8, rp, ci, vv);
+  EXPECT(rp[1] == 1 && rp[2] == 3 && ci[0] == 2 && ci[1] == 3 && ci[2] == 5 && vv[1] == 2.0 && vv[2] == 5.0,
+         "sum_csr_duplicates");
+  const uint64_t sa[4] = {1, 2, 3, 4}, sb[4] = {1, 9, 3, 8};
+  EXPECT(minhash_estimated_jaccard(sa, sb, 4) == 0.5 && minhash_estimated_jaccard(sa, sb, 0) == 0.0,
+         "minhash_estimated_jaccard");
+  Le_set_thread_num(3);
+  EXPECT(Le_get_thread_num() == 3 && Le_get_thread_id() == 0 && Le_get_core_num() >= 1, "thread controls");
+  std::remove(path);
+}
+
 int main() {
   std::setvbuf(stdout, nullptr, _IONBF, 0);
   try {
@@ -382,6 +461,7 @@ int main() {
     spgemm_checks();
     mtx_checks();
     feature_checks();
+    api_checks();
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
     return 2;
