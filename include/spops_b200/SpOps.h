@@ -14,11 +14,11 @@
  *   hierarchical_clustering_v0_fast                                   LeSpGEMM preprocessing
  *   read_coo_matrix, read_csr_matrix                                  Matrix Market files
  *   LeSpGEMM<sortOutput>(A, B, C, kernel_flag), HashSpGEMMTopK(A, C, top_k)
+ *                                                                     row-wise SpGEMM (include/spgemm.h)
  *   MTX<I,V>: MtxLoad, CalculateFeatures, FeaturesPrint, FeaturesWrite ...  features
  *   read_<fmt>_matrix, coo_to_ell, sum_csr_duplicates, csr_transpose,
  *   csr_to_binary_pattern, minhash_estimated_jaccard, delete_<fmt>_matrix,
  *   Le_*_thread_* (kept settings only)
- *                                                                     row-wise SpGEMM (include/spgemm.h)
  *
  * What differs, and why:
  *   - Work runs on the GPU.  The first SpOps call on a matrix uploads it and
