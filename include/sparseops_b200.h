@@ -5,8 +5,8 @@
  * i.e. a cudaStream_t).  Every entry point names the reference interface it
  * replaces (lsl036/SparseOps, file:line).  The reference is a C++ template
  * library with no FFI of its own; these are the functions a cgo / ctypes /
- * JNI binding of its hot path binds (INTEGRATION.md shows the stubs), and the
- * header-compatible C++ shim in include/spops_b200/SpOps.h is built on them.
+ * JNI binding of its hot path binds, and the header-compatible C++ shim in
+ * include/spops_b200/SpOps.h is built on them.
  *
  * Conventions
  *  - Every function returns spops_status_t; SPOPS_OK is 0.  On failure the
@@ -165,6 +165,11 @@ spops_status_t spops_mtx_parse_csr(spops_context_t ctx, const char* text, int64_
  * order, distinct columns listed in reverse order of first appearance,
  * exact-zero sums dropped -- bit-identical to the reference. */
 spops_status_t spops_coo_to_csr(spops_context_t ctx, spops_matrix_t coo, int32_t compact, spops_matrix_t* csr);
+/* Rows of a CSR matrix in a new order: row i of *out is row perm[i] of csr
+ * (csr_reorder_rows, include/sparse_conversion.h:1879-1998).  perm: host
+ * array of csr's index type, a permutation of 0 .. rows-1; anything else is
+ * refused with SPOPS_ERR_INVALID (the reference does not check). */
+spops_status_t spops_csr_reorder_rows(spops_context_t ctx, spops_matrix_t csr, const void* perm, spops_matrix_t* out);
 spops_status_t spops_matrix_destroy(spops_matrix_t A);
 spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info);
 /* Values changed in place (same pattern): drop value-derived caches. */

@@ -16,7 +16,7 @@
  *   LeSpGEMM<sortOutput>(A, B, C, kernel_flag), HashSpGEMMTopK(A, C, top_k)
  *                                                                     row-wise SpGEMM (include/spgemm.h)
  *   MTX<I,V>: MtxLoad, CalculateFeatures, FeaturesPrint, FeaturesWrite ...  features
- *   read_<fmt>_matrix, coo_to_ell, sum_csr_duplicates, csr_transpose,
+ *   read_<fmt>_matrix, coo_to_ell, sum_csr_duplicates, csr_transpose, csr_reorder_rows,
  *   csr_to_binary_pattern, minhash_estimated_jaccard, delete_<fmt>_matrix,
  *   Le_*_thread_* (kept settings only)
  *
@@ -1261,6 +1261,38 @@ CSR_Matrix<IndexType, ValueType> csr_transpose(const CSR_Matrix<IndexType, Value
   CSR_Matrix<IndexType, ValueType> t = coo_to_csr(coo, true);
   delete_host_matrix(coo);
   return t;
+}
+
+/* csr_reorder_rows (include/sparse_conversion.h:1879-1998): row i of the
+ * result is row row_permutation[i] of csr, gathered on the device. */
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> csr_reorder_rows(const CSR_Matrix<IndexType, ValueType>& csr,
+                                                  const IndexType* row_permutation) {
+  namespace d = spops_b200::detail;
+  if (csr.num_nnzs == 0) {
+    CSR_Matrix<IndexType, ValueType> r;
+    std::memset(static_cast<void*>(&r), 0, sizeof(r));
+    r.num_rows = csr.num_rows;
+    r.num_cols = csr.num_cols;
+    r.row_offset = d::host_alloc<IndexType>((int64_t)csr.num_rows + 1);
+    std::fill_n(r.row_offset, (size_t)csr.num_rows + 1, (IndexType)0);
+    return r;
+  }
+  spops_matrix_t a = d::upload_csr(csr), c = nullptr;
+  spops_status_t s = spops_csr_reorder_rows(d::ctx(), a, row_permutation, &c);
+  spops_matrix_destroy(a);
+  d::check(s, "spops_csr_reorder_rows");
+  CSR_Matrix<IndexType, ValueType> r;
+  d::take_csr<IndexType, ValueType>(c, r);
+  r.kernel_flag = 0;
+  return r;
+}
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> csr_reorder_rows(const CSR_Matrix<IndexType, ValueType>& csr,
+                                                  const std::vector<IndexType>& row_permutation) {
+  if (row_permutation.size() < (size_t)csr.num_rows)
+    throw std::invalid_argument("row_permutation size must be >= matrix rows");
+  return csr_reorder_rows(csr, row_permutation.data());
 }
 
 /* csr_to_binary_pattern (include/sparse_conversion.h:2121): the pattern with

@@ -216,6 +216,98 @@ spops_status_t coo_to_csr_t(Context* ctx, Matrix* coo, bool compact, Matrix** ou
   return SPOPS_OK;
 }
 
+// ---- csr_reorder_rows (include/sparse_conversion.h:1879-1998): row i of the
+// result is row perm[i] of the input.
+template <typename I>
+__global__ void reorder_len_kernel(const I* __restrict__ rp, const I* __restrict__ perm, int64_t n,
+                                   unsigned long long* __restrict__ len, unsigned int* __restrict__ seen,
+                                   int* __restrict__ bad) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t p = (int64_t)perm[i];
+  if (p < 0 || p >= n) {
+    atomicExch(bad, 1);
+    len[i] = 0;
+    return;
+  }
+  atomicAdd(seen + p, 1u);
+  len[i] = (unsigned long long)((int64_t)rp[p + 1] - (int64_t)rp[p]);
+}
+
+__global__ void perm_check_kernel(const unsigned int* __restrict__ seen, int64_t n, int* __restrict__ bad) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n && seen[i] != 1u) atomicExch(bad, 1);
+}
+
+// one warp per result row
+template <typename I, typename V>
+__global__ void reorder_copy_kernel(const I* __restrict__ rp, const I* __restrict__ ci, const V* __restrict__ val,
+                                    const I* __restrict__ perm, const unsigned long long* __restrict__ off, int64_t n,
+                                    I* __restrict__ nci, V* __restrict__ nval) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t p = (int64_t)perm[r];
+  const int64_t s = (int64_t)rp[p], m = (int64_t)rp[p + 1] - s, o = (int64_t)off[r];
+  for (int64_t k = lane; k < m; k += 32) {
+    nci[o + k] = ci[s + k];
+    nval[o + k] = val[s + k];
+  }
+}
+
+template <typename I, typename V>
+spops_status_t reorder_t(Context* ctx, Matrix* A, const void* perm_host, Matrix** out) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = A->rows, nz = A->nnz;
+  PoolBuf perm(ctx), len(ctx), seen(ctx), flag(ctx), scan(ctx), tmp(ctx);
+  SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(I)));
+  SPOPS_TRY(len.alloc((size_t)(n + 1) * 8));
+  SPOPS_TRY(scan.alloc((size_t)(n + 1) * 8));
+  SPOPS_TRY(seen.alloc((size_t)std::max<int64_t>(n, 1) * 4));
+  SPOPS_TRY(flag.alloc(16));
+  if (n > 0) SPOPS_CUDA(cudaMemcpyAsync(perm.p, perm_host, (size_t)n * sizeof(I), cudaMemcpyHostToDevice, st));
+  SPOPS_CUDA(cudaMemsetAsync(seen.p, 0, (size_t)std::max<int64_t>(n, 1) * 4, st));
+  SPOPS_CUDA(cudaMemsetAsync(flag.p, 0, 16, st));
+  SPOPS_CUDA(cudaMemsetAsync(len.as<unsigned long long>() + n, 0, 8, st));
+  if (n > 0) {
+    reorder_len_kernel<I><<<grid_of(n), 256, 0, st>>>(A->row.as<I>(), perm.as<I>(), n, len.as<unsigned long long>(),
+                                                      seen.as<unsigned int>(), flag.as<int>());
+    perm_check_kernel<<<grid_of(n), 256, 0, st>>>(seen.as<unsigned int>(), n, flag.as<int>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  int bad = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&bad, flag.p, 4, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  if (bad) return fail(SPOPS_ERR_INVALID, "csr_reorder_rows: the row permutation is not a permutation of 0..%lld",
+                       (long long)(n - 1));
+  size_t tb = 0;
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, len.as<unsigned long long>(), scan.as<unsigned long long>(),
+                                           n + 1, st));
+  SPOPS_TRY(tmp.alloc(tb + 256));
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb, len.as<unsigned long long>(), scan.as<unsigned long long>(),
+                                           n + 1, st));
+  Matrix* C = new_csr(ctx, A, nz);
+  spops_status_t s = C->row.alloc((size_t)(n + 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->col.alloc((size_t)std::max<int64_t>(nz, 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->val.alloc((size_t)std::max<int64_t>(nz, 1) * sizeof(V));
+  if (s == SPOPS_OK) {
+    offsets_kernel<I><<<grid_of(n + 1), 256, 0, st>>>(scan.as<unsigned long long>(), n + 1, C->row.as<I>());
+    if (n > 0)
+      reorder_copy_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(),
+                                                                 perm.as<I>(), scan.as<unsigned long long>(), n,
+                                                                 C->col.as<I>(), C->val.as<V>());
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+      s = fail(SPOPS_ERR_CUDA, "csr_reorder_rows: launch failed");
+  }
+  if (s != SPOPS_OK) {
+    C->release_all();
+    delete C;
+    return s;
+  }
+  *out = C;
+  return SPOPS_OK;
+}
+
 }  // namespace
 }  // namespace spops
 
@@ -237,5 +329,25 @@ extern "C" spops_status_t spops_coo_to_csr(spops_context_t ctx, spops_matrix_t c
                                       : coo_to_csr_t<int64_t, float>(ctx, coo, c, &out);
   if (s != SPOPS_OK) return s;
   *csr = static_cast<spops_matrix_s*>(out);
+  return SPOPS_OK;
+}
+
+extern "C" spops_status_t spops_csr_reorder_rows(spops_context_t ctx, spops_matrix_t csr, const void* perm,
+                                                 spops_matrix_t* out) {
+  if (!ctx || !csr || !out || (!perm && csr->rows > 0))
+    return fail(SPOPS_ERR_INVALID, "spops_csr_reorder_rows: null argument");
+  if (csr->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "spops_csr_reorder_rows: needs a CSR matrix");
+  DeviceGuard g(ctx->device);
+  if (!csr->plan.ready) SPOPS_TRY(csr_analyse(ctx, csr));  // validates the pattern
+  Matrix* C = nullptr;
+  spops_status_t s;
+  if (csr->itype == SPOPS_INDEX_I32)
+    s = csr->vtype == SPOPS_VALUE_F64 ? reorder_t<int32_t, double>(ctx, csr, perm, &C)
+                                      : reorder_t<int32_t, float>(ctx, csr, perm, &C);
+  else
+    s = csr->vtype == SPOPS_VALUE_F64 ? reorder_t<int64_t, double>(ctx, csr, perm, &C)
+                                      : reorder_t<int64_t, float>(ctx, csr, perm, &C);
+  if (s != SPOPS_OK) return s;
+  *out = static_cast<spops_matrix_s*>(C);
   return SPOPS_OK;
 }

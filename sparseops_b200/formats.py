@@ -470,6 +470,22 @@ def coo_to_csr(coo: COO_Matrix, compact: bool = False):
     return DeviceCSR(_Handle(ctx, out), coo.num_rows, coo.num_cols)
 
 
+def csr_reorder_rows(csr: CSR_Matrix, row_permutation):
+    """include/sparse_conversion.h:1879 on the device: row i of the result is
+    row row_permutation[i] of csr; a DeviceCSR.  The permutation must hold
+    every row once (SpOpsError otherwise)."""
+    from .spops import DeviceCSR
+    h = csr.device()
+    ctx = h.ctx.follow_torch()
+    it = np.int32 if int(h.info().index_type) == 0 else np.int64
+    perm = np.ascontiguousarray(np.asarray(row_permutation), dtype=it)
+    if len(perm) < csr.num_rows:
+        raise ValueError("row_permutation size must be >= matrix rows")
+    out = vp()
+    call("spops_csr_reorder_rows", ctx.handle, h.handle, perm.ctypes.data_as(vp), C.byref(out))
+    return DeviceCSR(_Handle(ctx, out), csr.num_rows, csr.num_cols)
+
+
 def _mtx_types(index_dtype, value_dtype):
     it = 0 if np.dtype(index_dtype) == np.int32 else 1
     vt = 0 if np.dtype(value_dtype) == np.float32 else 1

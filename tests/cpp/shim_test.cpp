@@ -431,6 +431,19 @@ void api_checks() {
       tr_ok = tr_ok && found;
     }
   EXPECT(tr_ok, "csr_transpose entries");
+  std::vector<int> perm(n);
+  for (int i = 0; i < n; ++i) perm[i] = (i * 7 + 3) % n;  // 7 is prime to 600
+  CSR_Matrix<int, double> ro = csr_reorder_rows(csr, perm);
+  bool ro_ok = ro.num_rows == n && ro.num_nnzs == csr.num_nnzs;
+  for (int i = 0; ro_ok && i < n; ++i) {
+    const int p = perm[i], len = csr.row_offset[p + 1] - csr.row_offset[p];
+    ro_ok = ro.row_offset[i + 1] - ro.row_offset[i] == len;
+    for (int k = 0; ro_ok && k < len; ++k)
+      ro_ok = ro.col_index[ro.row_offset[i] + k] == csr.col_index[csr.row_offset[p] + k] &&
+              ro.values[ro.row_offset[i] + k] == csr.values[csr.row_offset[p] + k];
+  }
+  EXPECT(ro_ok, "csr_reorder_rows");
+  delete_csr_matrix(ro);
   CSR_Matrix<int, double> bp = csr_to_binary_pattern(csr);
   EXPECT(bp.num_nnzs == csr.num_nnzs && bp.values[0] == 1.0 && bp.col_index[5] == csr.col_index[5],
          "csr_to_binary_pattern");

@@ -347,3 +347,37 @@ def test_coo_to_csr_vs_oracle(cuda, orc, itype, vtype, compact):
                        compact)
     rp, oc, ov = empty.host()
     assert np.array_equal(rp, np.zeros(8)) and len(oc) == 0
+
+
+@pytest.mark.parametrize("itype", [np.int32, np.int64])
+@pytest.mark.parametrize("vtype", [np.float64, np.float32])
+def test_csr_reorder_rows(cuda, itype, vtype):
+    """csr_reorder_rows (include/sparse_conversion.h:1879): row i of the
+    result is row perm[i] of the input, entries copied in order; empty rows
+    kept; a non-permutation is refused."""
+    from sparseops_b200 import SpOpsError, csr_reorder_rows
+    rp, ci, v = synth.powerlaw(20000, hi=500, seed=44)
+    lens = np.diff(rp)
+    lens[::7] = 0  # empty rows
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(itype)
+    ci = ci[:int(rp[-1])].astype(itype)
+    v = v[:int(rp[-1])].astype(vtype)
+    n = len(rp) - 1
+    A = _csr(rp, ci, v, n)
+    perm = np.random.default_rng(3).permutation(n)
+    R = csr_reorder_rows(A, perm)
+    rrp, rci, rv = R.host()
+    exp_lens = lens[perm]
+    assert np.array_equal(np.diff(rrp.astype(np.int64)), exp_lens)
+    starts = rp[perm].astype(np.int64)
+    idx = np.concatenate([np.arange(s, s + L) for s, L in zip(starts, exp_lens)]) if exp_lens.sum() else np.zeros(0, int)
+    assert np.array_equal(rci.astype(np.int64), ci[idx].astype(np.int64))
+    assert np.array_equal(rv, v[idx])
+    bad = perm.copy()
+    bad[5] = bad[6]  # a repeated row
+    with pytest.raises(SpOpsError):
+        csr_reorder_rows(A, bad)
+    bad = perm.copy()
+    bad[0] = n  # out of range
+    with pytest.raises(SpOpsError):
+        csr_reorder_rows(A, bad)
