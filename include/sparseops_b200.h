@@ -56,7 +56,8 @@ typedef enum {
   SPOPS_FMT_SELL_C_R = 5,     /* SELL-C-sigma with one global sort */
   SPOPS_FMT_DIA = 6,
   SPOPS_FMT_BSR = 7,
-  SPOPS_FMT_CSR5 = 8
+  SPOPS_FMT_CSR5 = 8,
+  SPOPS_FMT_VLCLUSTER = 9     /* CSR_VlengthCluster: clustered rows (LeSpGEMM_VLength operands) */
 } spops_format_t;
 
 /* Element layout inside an ELL matrix or a SELL chunk.  ROW_MAJOR is the
@@ -87,7 +88,8 @@ typedef struct {
  *   ELL:  [max_row_width, min_row_width]
  *   DIA:  [complete_ndiags, stride]
  *   BSR:  [mb, nb, nnzb, blockDim_r, blockDim_c]
- *   CSR5: [tiles, omega, sigma] */
+ *   CSR5: [tiles, omega, sigma]
+ *   VLCLUSTER: [clusters, nnzv, max_cluster_sz] (rows = CSR rows, nnz = nnzc) */
 typedef struct {
   int64_t rows, cols, nnz;
   int32_t format, index_type, value_type, layout;
@@ -240,7 +242,9 @@ typedef enum {
   SPOPS_ARR_BLOCK_ROW_PTR = 8, /* BSR row_ptr */
   SPOPS_ARR_BLOCK_COL = 9,     /* BSR block_colindex */
   SPOPS_ARR_TILE_PTR = 10,     /* CSR5 tile_ptr (uint32, bit 31: tile spans an empty row) */
-  SPOPS_ARR_TILE_DESC = 11     /* CSR5 per-lane row-start flags (uint32, tiles x 32) */
+  SPOPS_ARR_TILE_DESC = 11,    /* CSR5 per-lane row-start flags (uint32, tiles x 32) */
+  SPOPS_ARR_CLUSTER_SZ = 12,   /* VLCLUSTER cluster_sz (rows per cluster) */
+  SPOPS_ARR_ROWPTR_VAL = 13    /* VLCLUSTER rowptr_val (clusters + 1) */
 } spops_array_t;
 /* Device pointer, element count and element size of one array (no copy). */
 spops_status_t spops_matrix_array(spops_matrix_t A, spops_array_t which, const void** dev_ptr, int64_t* count,
@@ -490,6 +494,39 @@ spops_status_t spops_matrix_tile_features(spops_context_t ctx, spops_matrix_t cs
  * NULL) the measured time per SpMV of the choice (mode 1; 0 in mode 0). */
 spops_status_t spops_select_format(spops_context_t ctx, spops_matrix_t csr, int32_t mode, spops_format_t* format,
                                    spops_format_params_t* params, double* ms);
+
+/* ------------------------------------------------ clustered (VLength) form */
+/* CSR_VlengthCluster (spgemm_cluster.h:108-143) as a handle of format
+ * SPOPS_FMT_VLCLUSTER: clusters of consecutive rows; cluster i holds the
+ * union of its rows' columns, colids[rowptr[i] .. rowptr[i+1]), and for the
+ * cluster's column p and its row k the value
+ * values[rowptr_val[i] + p * cluster_sz[i] + k] (0 where the row lacks the
+ * column).  Arrays: ROW = rowptr, COL = colids, VAL = values, CLUSTER_SZ,
+ * ROWPTR_VAL; info: rows = CSR rows, nnz = nnzc, extra = [clusters, nnzv,
+ * max_cluster_sz (at least 256, as the reference starts it)].  Replaces the
+ * host struct consumed and produced by LeSpGEMM_VLength. */
+spops_status_t spops_vlcluster_create(spops_context_t ctx, spops_matrix_t* M, int64_t csr_rows, int64_t clusters,
+                                      int64_t cols, int64_t nnzc, int64_t nnzv, const void* cluster_sz,
+                                      const void* rowptr, const void* colids, const void* rowptr_val,
+                                      const void* values, spops_index_t itype, spops_value_t vtype, spops_mem_t mem);
+/* csr_to_vlength_cluster (sparse_conversion.h:1640-1765): cluster i is rows
+ * offsets[i] .. offsets[i+1] (host int64, from 0 to rows).  Each cluster's
+ * columns are ascending (the reference lists them in hash-map order). */
+spops_status_t spops_csr_to_vlength_cluster(spops_context_t ctx, spops_matrix_t csr, const int64_t* offsets,
+                                            int64_t clusters, spops_matrix_t* cluster);
+/* vlength_cluster2csr (sparse_conversion.h:1777-1862): rows in cluster
+ * order, each row's entries in its cluster's column order, exact zeros
+ * dropped. */
+spops_status_t spops_vlength_cluster_to_csr(spops_context_t ctx, spops_matrix_t cluster, spops_matrix_t* csr);
+/* LeSpGEMM_VLength (spgemm.h:175-180; kernel 3 rules, spgemm_Vlength_mixed.cpp)
+ * C = A * B with A clustered: C in A's clusters, the cluster's columns
+ * ascending, columns whose values all fall below 1e-12 dropped on the dense
+ * and sorted paths, as the reference does.  l2_budget_bytes: the dense rule's
+ * budget (the reference's CPU_L2CACHE_SIZE * mixed_l2_fraction).  A's exact
+ * zeros take no part in C's structure. */
+spops_status_t spops_spgemm_vlength(spops_context_t ctx, spops_matrix_t A_cluster, spops_matrix_t B,
+                                    int32_t sort_output, double l2_budget_bytes, spops_matrix_t* C_cluster,
+                                    spops_spgemm_stats_t* stats);
 
 /* ------------------------------------------------------ no allocation */
 /* y = alpha*A*x + beta*y for a CSR matrix given by device pointers, without

@@ -19,6 +19,7 @@
  *   read_<fmt>_matrix, coo_to_ell, sum_csr_duplicates, csr_transpose, csr_reorder_rows,
  *   csr_to_binary_pattern, minhash_estimated_jaccard, delete_<fmt>_matrix,
  *   Le_*_thread_* (kept settings only)
+ *   CSR_VlengthCluster, csr_to_vlength_cluster, LeSpGEMM_VLength, vlength_cluster2csr
  *
  * What differs, and why:
  *   - Work runs on the GPU.  The first SpOps call on a matrix uploads it and
@@ -1323,6 +1324,145 @@ inline double minhash_estimated_jaccard(const uint64_t* sig_a, const uint64_t* s
 inline double minhash_estimated_jaccard(const std::vector<uint64_t>& sig_a, const std::vector<uint64_t>& sig_b) {
   if (sig_a.size() != sig_b.size() || sig_a.empty()) return 0.0;
   return minhash_estimated_jaccard(sig_a.data(), sig_b.data(), (int)sig_a.size());
+}
+
+/* ----------------------------------------------- clustered (VLength) form */
+#ifndef CPU_L2CACHE_SIZE
+#define CPU_L2CACHE_SIZE 67108864
+#endif
+#ifndef MIXED_L2_FRACTION
+#define MIXED_L2_FRACTION 0.75
+#endif
+
+/* The reference's cluster struct (spgemm_cluster.h:108-143), same fields. */
+template <typename IndexType, typename ValueType>
+struct CSR_VlengthCluster : public Matrix_Features<IndexType> {
+  typedef IndexType index_type;
+  typedef ValueType value_type;
+  IndexType csr_rows;
+  IndexType rows;
+  IndexType cols;
+  IndexType nnzc;
+  IndexType nnzv;
+  IndexType max_cluster_sz;
+  IndexType* cluster_sz;
+  IndexType* rowptr;
+  IndexType* colids;
+  IndexType* rowptr_val;
+  ValueType* values;
+  int dense_cluster_count;
+  char* acc_flag = NULL;
+  IndexType* min_ccol = NULL;
+  IndexType* max_ccol = NULL;
+  double mixed_acc_setup_ms = 0.0;
+  double mixed_acc_malloc_ms = 0.0;
+  double mixed_acc_symbolic_ms = 0.0;
+  double mixed_acc_dispatcher_ms = 0.0;
+  double mixed_acc_numeric_ms = 0.0;
+};
+
+template <typename IndexType, typename ValueType>
+void delete_vlength_cluster_matrix(CSR_VlengthCluster<IndexType, ValueType>& c) {
+  std::free(c.cluster_sz);
+  std::free(c.rowptr);
+  std::free(c.colids);
+  std::free(c.rowptr_val);
+  std::free(c.values);
+  c.cluster_sz = c.rowptr = c.colids = c.rowptr_val = nullptr;
+  c.values = nullptr;
+  c.csr_rows = c.rows = c.cols = c.nnzc = c.nnzv = 0;
+}
+template <typename IndexType, typename ValueType>
+void delete_host_matrix(CSR_VlengthCluster<IndexType, ValueType>& c) { delete_vlength_cluster_matrix(c); }
+
+namespace spops_b200 {
+namespace detail {
+// a clustered-form device handle into the caller's struct (arrays from
+// posix_memalign, freed by delete_vlength_cluster_matrix)
+template <typename I, typename V>
+inline void take_vlcluster(spops_matrix_t h, CSR_VlengthCluster<I, V>& c) {
+  const spops_matrix_info_t i = info(h);
+  c.csr_rows = (I)i.rows;
+  c.cols = (I)i.cols;
+  c.nnzc = (I)i.nnz;
+  c.rows = (I)i.extra[0];
+  c.nnzv = (I)i.extra[1];
+  c.max_cluster_sz = (I)i.extra[2];
+  c.cluster_sz = fetch<I>(h, SPOPS_ARR_CLUSTER_SZ, nullptr);
+  c.rowptr = fetch<I>(h, SPOPS_ARR_ROW, nullptr);
+  c.colids = fetch<I>(h, SPOPS_ARR_COL, nullptr);
+  c.rowptr_val = fetch<I>(h, SPOPS_ARR_ROWPTR_VAL, nullptr);
+  c.values = fetch<V>(h, SPOPS_ARR_VAL, nullptr);
+  c.dense_cluster_count = 0;
+  c.num_rows = c.csr_rows;
+  c.num_cols = c.cols;
+  c.num_nnzs = c.nnzv;
+  spops_matrix_destroy(h);
+}
+template <typename I, typename V>
+inline spops_matrix_t upload_vlcluster(const CSR_VlengthCluster<I, V>& c) {
+  spops_matrix_t h = nullptr;
+  check(spops_vlcluster_create(ctx(), &h, c.csr_rows, c.rows, c.cols, c.nnzc, c.nnzv, c.cluster_sz, c.rowptr,
+                               c.colids, c.rowptr_val, c.values, itype<I>(), vtype<V>(), SPOPS_MEM_HOST),
+        "spops_vlcluster_create");
+  return h;
+}
+}  // namespace detail
+}  // namespace spops_b200
+
+/* csr_to_vlength_cluster (sparse_conversion.h:1640-1765): cluster i is rows
+ * offsets[i] .. offsets[i+1]; its columns ascending (the reference: hash-map
+ * order). */
+template <class IndexType, class ValueType>
+CSR_VlengthCluster<IndexType, ValueType> csr_to_vlength_cluster(const CSR_Matrix<IndexType, ValueType>& csr,
+                                                                const std::vector<IndexType>& offsets) {
+  namespace d = spops_b200::detail;
+  if (offsets.size() < 2) throw std::invalid_argument("offsets size must be >= 2");
+  std::vector<int64_t> off(offsets.begin(), offsets.end());
+  spops_matrix_t a = d::upload_csr(csr), h = nullptr;
+  spops_status_t s = spops_csr_to_vlength_cluster(d::ctx(), a, off.data(), (int64_t)off.size() - 1, &h);
+  spops_matrix_destroy(a);
+  d::check(s, "spops_csr_to_vlength_cluster");
+  CSR_VlengthCluster<IndexType, ValueType> c;
+  std::memset(static_cast<void*>(&c), 0, sizeof(c));
+  d::take_vlcluster<IndexType, ValueType>(h, c);
+  return c;
+}
+
+/* vlength_cluster2csr (sparse_conversion.h:1777-1862): rows in cluster order,
+ * exact zeros dropped. */
+template <class IndexType, class ValueType>
+CSR_Matrix<IndexType, ValueType> vlength_cluster2csr(const CSR_VlengthCluster<IndexType, ValueType>& cluster) {
+  namespace d = spops_b200::detail;
+  spops_matrix_t a = d::upload_vlcluster(cluster), h = nullptr;
+  spops_status_t s = spops_vlength_cluster_to_csr(d::ctx(), a, &h);
+  spops_matrix_destroy(a);
+  d::check(s, "spops_vlength_cluster_to_csr");
+  CSR_Matrix<IndexType, ValueType> csr;
+  d::take_csr<IndexType, ValueType>(h, csr);
+  csr.kernel_flag = 0;
+  return csr;
+}
+
+/* LeSpGEMM_VLength (spgemm.h:175-180): C = A * B with A clustered, kernel-3
+ * rules on the device for every kernel_flag; C in A's clusters (allocated
+ * here, columns ascending).  The caller's acc_flag / min_ccol / max_ccol, if
+ * any, are left untouched. */
+template <bool sortOutput = true, typename IndexType, typename ValueType>
+void LeSpGEMM_VLength(const CSR_VlengthCluster<IndexType, ValueType>& A_cluster,
+                      const CSR_Matrix<IndexType, ValueType>& B, CSR_VlengthCluster<IndexType, ValueType>& C_cluster,
+                      int kernel_flag = 1, double mixed_l2_fraction = -1.0) {
+  namespace d = spops_b200::detail;
+  (void)kernel_flag;
+  const double frac = mixed_l2_fraction < 0 ? MIXED_L2_FRACTION : mixed_l2_fraction;
+  spops_matrix_t a = d::upload_vlcluster(A_cluster), b = d::upload_csr(B), c = nullptr;
+  spops_status_t s = spops_spgemm_vlength(d::ctx(), a, b, sortOutput ? 1 : 0, (double)CPU_L2CACHE_SIZE * frac, &c,
+                                          nullptr);
+  spops_matrix_destroy(a);
+  spops_matrix_destroy(b);
+  d::check(s, "spops_spgemm_vlength");
+  d::take_vlcluster<IndexType, ValueType>(c, C_cluster);
+  C_cluster.max_cluster_sz = A_cluster.max_cluster_sz;
 }
 
 /* ------------------------------------------------------------ features */

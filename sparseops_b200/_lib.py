@@ -107,6 +107,11 @@ _SIGS = {
     "spops_csr_create": [vp, vp, i64, i64, i64, vp, vp, vp, C.c_int, C.c_int, C.c_int],
     "spops_coo_to_csr": [vp, vp, C.c_int32, C.POINTER(vp)],
     "spops_csr_reorder_rows": [vp, vp, vp, C.POINTER(vp)],
+    "spops_vlcluster_create": [vp, C.POINTER(vp), i64, i64, i64, i64, i64, vp, vp, vp, vp, vp, C.c_int, C.c_int,
+                               C.c_int],
+    "spops_csr_to_vlength_cluster": [vp, vp, vp, i64, C.POINTER(vp)],
+    "spops_vlength_cluster_to_csr": [vp, vp, C.POINTER(vp)],
+    "spops_spgemm_vlength": [vp, vp, vp, C.c_int32, C.c_double, C.POINTER(vp), vp],
     "spops_matrix_features": [vp, vp, vp],
     "spops_matrix_tile_features": [vp, vp, i64, vp, vp],
     "spops_select_format": [vp, vp, i32, C.POINTER(C.c_int), vp, C.POINTER(C.c_double)],

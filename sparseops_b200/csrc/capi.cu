@@ -267,15 +267,18 @@ spops_status_t spops_matrix_array(spops_matrix_t A, spops_array_t which, const v
   switch (which) {
     case SPOPS_ARR_ROW:
       p = A->row.p; eb = is;
-      n = A->format == SPOPS_FMT_CSR ? A->rows + 1 : A->format == SPOPS_FMT_COO ? A->nnz : 0;
+      n = A->format == SPOPS_FMT_CSR ? A->rows + 1 : A->format == SPOPS_FMT_COO ? A->nnz
+          : A->format == SPOPS_FMT_VLCLUSTER ? A->clusters + 1 : 0;
       break;
     case SPOPS_ARR_COL:
       p = A->col.p; eb = is;
-      n = (A->format == SPOPS_FMT_CSR || A->format == SPOPS_FMT_COO) ? A->nnz : A->pad.stored;
+      n = (A->format == SPOPS_FMT_CSR || A->format == SPOPS_FMT_COO || A->format == SPOPS_FMT_VLCLUSTER) ? A->nnz
+                                                                                                     : A->pad.stored;
       break;
     case SPOPS_ARR_VAL:
       eb = vs;
       if (A->format == SPOPS_FMT_DIA) { p = A->dia.data.p; n = A->dia.ndiag * A->dia.stride; }
+      else if (A->format == SPOPS_FMT_VLCLUSTER) { p = A->val.p; n = A->cl_nnzv; }
       else if (A->format == SPOPS_FMT_BSR) { p = A->bsr.data.p; n = A->bsr.nnzb * A->bsr.br * A->bsr.bc; }
       else { p = A->val.p; n = (A->format == SPOPS_FMT_CSR || A->format == SPOPS_FMT_COO) ? A->nnz : A->pad.stored; }
       break;
@@ -288,6 +291,10 @@ spops_status_t spops_matrix_array(spops_matrix_t A, spops_array_t which, const v
     case SPOPS_ARR_BLOCK_COL: p = A->bsr.bcol.p; eb = is; n = A->bsr.nnzb; break;
     case SPOPS_ARR_TILE_PTR: p = A->csr5.tile_ptr.p; eb = 4; n = A->csr5.tile_ptr.p ? A->csr5.tiles + 1 : 0; break;
     case SPOPS_ARR_TILE_DESC: p = A->csr5.desc.p; eb = 4; n = A->csr5.tiles * 32; break;
+    case SPOPS_ARR_CLUSTER_SZ: p = A->cl_sz.p; eb = is; n = A->format == SPOPS_FMT_VLCLUSTER ? A->clusters : 0; break;
+    case SPOPS_ARR_ROWPTR_VAL:
+      p = A->cl_rpv.p; eb = is; n = A->format == SPOPS_FMT_VLCLUSTER ? A->clusters + 1 : 0;
+      break;
     default: return fail(SPOPS_ERR_INVALID, "spops_matrix_array: unknown array %d", (int)which);
   }
   if (n > 0 && !p) return fail(SPOPS_ERR_INVALID, "spops_matrix_array: array %d not present", (int)which);
@@ -356,6 +363,9 @@ spops_status_t spops_matrix_info(spops_matrix_t A, spops_matrix_info_t* info) {
       break;
     case SPOPS_FMT_CSR5:
       info->extra[0] = A->csr5.tiles; info->extra[1] = 32; info->extra[2] = 16; info->extra[3] = A->csr5.nempty;
+      break;
+    case SPOPS_FMT_VLCLUSTER:
+      info->extra[0] = A->clusters; info->extra[1] = A->cl_nnzv; info->extra[2] = A->cl_max_sz;
       break;
     default: break;
   }

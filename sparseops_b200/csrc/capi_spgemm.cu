@@ -272,4 +272,131 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   return SPOPS_OK;
 }
 
+// ------------------------------------------------ clustered (VLength) form
+spops_status_t spops_vlcluster_create(spops_context_t ctx, spops_matrix_t* M, int64_t csr_rows, int64_t clusters,
+                                      int64_t cols, int64_t nnzc, int64_t nnzv, const void* cluster_sz,
+                                      const void* rowptr, const void* colids, const void* rowptr_val,
+                                      const void* values, spops_index_t itype, spops_value_t vtype, spops_mem_t mem) {
+  if (!ctx || !M || clusters < 0 || csr_rows < 0 || cols < 0 || nnzc < 0 || nnzv < 0 ||
+      (clusters > 0 && (!cluster_sz || !rowptr || !rowptr_val)) || (nnzc > 0 && !colids) || (nnzv > 0 && !values))
+    return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: null or negative argument");
+  if ((itype != SPOPS_INDEX_I32 && itype != SPOPS_INDEX_I64) || (vtype != SPOPS_VALUE_F32 && vtype != SPOPS_VALUE_F64))
+    return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: bad index or value type");
+  DeviceGuard g(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const size_t is = itype == SPOPS_INDEX_I32 ? 4 : 8, vs = vtype == SPOPS_VALUE_F32 ? 4 : 8;
+  const cudaMemcpyKind kind = mem == SPOPS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind back = mem == SPOPS_MEM_HOST ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost;
+  // the small per-cluster arrays on the host for the checks
+  std::vector<int64_t> sz((size_t)clusters), rp((size_t)clusters + 1), rpv((size_t)clusters + 1);
+  {
+    std::vector<char> a((size_t)clusters * is), b(((size_t)clusters + 1) * is), c(((size_t)clusters + 1) * is);
+    if (clusters > 0) {
+      SPOPS_CUDA(cudaMemcpy(a.data(), cluster_sz, a.size(), back));
+      SPOPS_CUDA(cudaMemcpy(b.data(), rowptr, b.size(), back));
+      SPOPS_CUDA(cudaMemcpy(c.data(), rowptr_val, c.size(), back));
+    }
+    auto get = [&](const std::vector<char>& v, size_t i) -> int64_t {
+      return is == 4 ? (int64_t)reinterpret_cast<const int32_t*>(v.data())[i] : reinterpret_cast<const int64_t*>(v.data())[i];
+    };
+    for (int64_t i = 0; i < clusters; ++i) sz[(size_t)i] = get(a, (size_t)i);
+    for (int64_t i = 0; clusters > 0 && i <= clusters; ++i) {
+      rp[(size_t)i] = get(b, (size_t)i);
+      rpv[(size_t)i] = get(c, (size_t)i);
+    }
+  }
+  std::vector<int64_t> off((size_t)clusters + 1, 0);
+  for (int64_t i = 0; i < clusters; ++i) {
+    if (sz[(size_t)i] < 0) return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: negative cluster size");
+    off[(size_t)i + 1] = off[(size_t)i] + sz[(size_t)i];
+  }
+  if (off[(size_t)clusters] != csr_rows)
+    return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: cluster sizes add up to %lld, not %lld rows",
+                (long long)off[(size_t)clusters], (long long)csr_rows);
+  if (clusters > 0) {
+    if (rp[0] != 0 || rpv[0] != 0 || rp[(size_t)clusters] != nnzc || rpv[(size_t)clusters] != nnzv)
+      return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: rowptr / rowptr_val do not span nnzc / nnzv");
+    for (int64_t i = 0; i < clusters; ++i)
+      if (rp[(size_t)i + 1] < rp[(size_t)i] ||
+          rpv[(size_t)i + 1] - rpv[(size_t)i] != (rp[(size_t)i + 1] - rp[(size_t)i]) * sz[(size_t)i])
+        return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: cluster %lld: rowptr_val does not match", (long long)i);
+  } else if (nnzc || nnzv || csr_rows) {
+    return fail(SPOPS_ERR_INVALID, "spops_vlcluster_create: entries without clusters");
+  }
+  Matrix* A = new spops_matrix_s();
+  A->ctx = ctx;
+  A->format = SPOPS_FMT_VLCLUSTER;
+  A->itype = itype;
+  A->vtype = vtype;
+  A->rows = csr_rows;
+  A->cols = cols;
+  A->nnz = nnzc;
+  A->clusters = clusters;
+  A->cl_nnzv = nnzv;
+  spops_status_t s = A->row.alloc(((size_t)clusters + 1) * is);
+  if (s == SPOPS_OK) s = A->cl_rpv.alloc(((size_t)clusters + 1) * is);
+  if (s == SPOPS_OK) s = A->col.alloc((size_t)std::max<int64_t>(nnzc, 1) * is);
+  if (s == SPOPS_OK) s = A->val.alloc((size_t)std::max<int64_t>(nnzv, 1) * vs);
+  if (s == SPOPS_OK && clusters > 0) {
+    if (cudaMemcpyAsync(A->row.p, rowptr, ((size_t)clusters + 1) * is, kind, st) != cudaSuccess ||
+        cudaMemcpyAsync(A->cl_rpv.p, rowptr_val, ((size_t)clusters + 1) * is, kind, st) != cudaSuccess ||
+        (nnzc > 0 && cudaMemcpyAsync(A->col.p, colids, (size_t)nnzc * is, kind, st) != cudaSuccess) ||
+        (nnzv > 0 && cudaMemcpyAsync(A->val.p, values, (size_t)nnzv * vs, kind, st) != cudaSuccess))
+      s = fail(SPOPS_ERR_CUDA, "spops_vlcluster_create: copy failed");
+  }
+  if (s == SPOPS_OK && nnzc > 0) s = validate_columns(ctx, A->col.p, nnzc, itype, cols, false);
+  if (s == SPOPS_OK) s = vlcluster_finish(ctx, A, off.data());
+  if (s != SPOPS_OK) {
+    A->release_all();
+    delete static_cast<spops_matrix_s*>(A);
+    return s;
+  }
+  *M = static_cast<spops_matrix_s*>(A);
+  return SPOPS_OK;
+}
+
+spops_status_t spops_csr_to_vlength_cluster(spops_context_t ctx, spops_matrix_t csr, const int64_t* offsets,
+                                            int64_t clusters, spops_matrix_t* cluster) {
+  if (!ctx || !csr || !offsets || !cluster) return fail(SPOPS_ERR_INVALID, "spops_csr_to_vlength_cluster: null argument");
+  DeviceGuard g(ctx->device);
+  Matrix* out = nullptr;
+  SPOPS_TRY(vlcluster_from_csr(ctx, csr, offsets, clusters, &out));
+  *cluster = static_cast<spops_matrix_s*>(out);
+  return SPOPS_OK;
+}
+
+spops_status_t spops_vlength_cluster_to_csr(spops_context_t ctx, spops_matrix_t cluster, spops_matrix_t* csr) {
+  if (!ctx || !cluster || !csr) return fail(SPOPS_ERR_INVALID, "spops_vlength_cluster_to_csr: null argument");
+  DeviceGuard g(ctx->device);
+  Matrix* out = nullptr;
+  SPOPS_TRY(vlcluster_to_csr(ctx, cluster, &out));
+  *csr = static_cast<spops_matrix_s*>(out);
+  return SPOPS_OK;
+}
+
+spops_status_t spops_spgemm_vlength(spops_context_t ctx, spops_matrix_t A_cluster, spops_matrix_t B,
+                                    int32_t sort_output, double l2_budget_bytes, spops_matrix_t* C_cluster,
+                                    spops_spgemm_stats_t* stats) {
+  if (!ctx || !A_cluster || !B || !C_cluster) return fail(SPOPS_ERR_INVALID, "spops_spgemm_vlength: null argument");
+  if (A_cluster->format != SPOPS_FMT_VLCLUSTER)
+    return fail(SPOPS_ERR_INVALID, "spops_spgemm_vlength: A must be a clustered matrix");
+  DeviceGuard g(ctx->device);
+  const int64_t ncl = A_cluster->clusters, n = A_cluster->rows;
+  std::vector<int64_t> off((size_t)ncl + 1), perm((size_t)std::max<int64_t>(n, 1));
+  SPOPS_CUDA(cudaMemcpy(off.data(), A_cluster->cl_off.p, ((size_t)ncl + 1) * 8, cudaMemcpyDeviceToHost));
+  for (int64_t r = 0; r < n; ++r) perm[(size_t)r] = r;
+  Matrix* A = nullptr;
+  SPOPS_TRY(vlcluster_to_csr(ctx, A_cluster, &A));
+  SpgemmStats s;
+  Matrix* out = nullptr;
+  spops_status_t rc =
+      cluster_spgemm(ctx, A, B, perm.data(), off.data(), ncl, sort_output != 0, l2_budget_bytes, &out, &s, false, true);
+  A->release_all();
+  delete static_cast<spops_matrix_s*>(A);
+  SPOPS_TRY(rc);
+  *C_cluster = static_cast<spops_matrix_s*>(out);
+  put_stats(s, stats);
+  return SPOPS_OK;
+}
+
 }  // extern "C"

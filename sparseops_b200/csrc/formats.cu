@@ -993,6 +993,9 @@ void Matrix::release_all() {
   tr.release();
   csr5.release();
   spmm_partial.release();
+  cl_sz.release();
+  cl_rpv.release();
+  cl_off.release();
   if (csr_view) {
     csr_view->release_all();
     delete csr_view;

@@ -955,9 +955,158 @@ struct Timer {
 
 // rowwise: the row-wise kernels' output rules (every structural entry kept,
 // exact zeros included; no small-value drop) instead of kernel 3's.
+// ---- clustered (VLength) form
+template <typename T, typename U>
+__global__ void cast_kernel(const T* __restrict__ a, int64_t m, U* __restrict__ b) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = (U)a[i];
+}
+
+__global__ void iota_kernel(int64_t* __restrict__ a, int64_t m) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) a[i] = i;
+}
+
+// Columns of C's clusters that stay in the clustered form: every column,
+// except in clusters under the drop rule (dense and sorted paths), where a
+// column whose values all came out as exactly 0 was dropped.  One warp per
+// cluster; kcnt[c] = kept columns.
+template <typename V>
+__global__ void cl_keep_count_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
+                                     const int64_t* __restrict__ offs, int64_t ncl, const V* __restrict__ cval,
+                                     const unsigned char* __restrict__ drop, int64_t* __restrict__ kcnt,
+                                     int64_t* __restrict__ kval) {
+  const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= ncl) return;
+  const int64_t csz = offs[c + 1] - offs[c], p0 = ccptr[c], np = ccptr[c + 1] - p0, v0 = ccptr_val[c];
+  const bool dr = drop[c] != 0;
+  int64_t kept = 0;
+  for (int64_t p = lane; p < np; p += 32) {
+    bool keep = !dr;
+    for (int64_t l = 0; l < csz && !keep; ++l) keep = cval[v0 + p * csz + l] != V(0);
+    kept += keep;
+  }
+  for (int o = 16; o; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if (lane == 0) {
+    kcnt[c] = kept;
+    kval[c] = kept * csz;
+  }
+}
+
+template <typename I, typename V>
+__global__ void cl_compact_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
+                                  const int64_t* __restrict__ offs, int64_t ncl, const int32_t* __restrict__ ccol,
+                                  const V* __restrict__ cval, const unsigned char* __restrict__ drop,
+                                  const int64_t* __restrict__ nrp, const int64_t* __restrict__ nrpv,
+                                  I* __restrict__ colids, V* __restrict__ vals) {
+  const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= ncl) return;
+  const int64_t csz = offs[c + 1] - offs[c], p0 = ccptr[c], np = ccptr[c + 1] - p0, v0 = ccptr_val[c];
+  const bool dr = drop[c] != 0;
+  int64_t out = 0;  // kept columns before this batch
+  for (int64_t b = 0; b < np; b += 32) {
+    const int64_t p = b + lane;
+    bool keep = false;
+    if (p < np) {
+      keep = !dr;
+      for (int64_t l = 0; l < csz && !keep; ++l) keep = cval[v0 + p * csz + l] != V(0);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int64_t q = out + __popc(m & ((1u << lane) - 1u));
+      colids[nrp[c] + q] = (I)ccol[p0 + p];
+      for (int64_t l = 0; l < csz; ++l) vals[nrpv[c] + q * csz + l] = cval[v0 + p * csz + l];
+    }
+    out += __popc(m);
+  }
+}
+
+// Clustered form back to CSR rows in cluster order (vlength_cluster2csr):
+// row off[c] + l holds, in the cluster's column order, the columns whose
+// value for row l is not exactly 0.  One thread per (cluster, row).
+template <typename I, typename V>
+__global__ void vlc_row_count_kernel(const I* __restrict__ rp, const I* __restrict__ rpv,
+                                     const int64_t* __restrict__ off, int64_t ncl, const int64_t* __restrict__ rowcl,
+                                     int64_t n, const V* __restrict__ val, int64_t* __restrict__ cnt) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t c = rowcl[r], l = r - off[c], csz = off[c + 1] - off[c];
+  const int64_t p0 = (int64_t)rp[c], np = (int64_t)rp[c + 1] - p0, v0 = (int64_t)rpv[c];
+  int64_t k = 0;
+  for (int64_t p = 0; p < np; ++p) k += val[v0 + p * csz + l] != V(0);
+  cnt[r] = k;
+}
+
+template <typename I, typename V>
+__global__ void vlc_row_write_kernel(const I* __restrict__ rp, const I* __restrict__ rpv, const I* __restrict__ colids,
+                                     const int64_t* __restrict__ off, const int64_t* __restrict__ rowcl, int64_t n,
+                                     const V* __restrict__ val, const int64_t* __restrict__ crp, I* __restrict__ ci,
+                                     V* __restrict__ cv) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t c = rowcl[r], l = r - off[c], csz = off[c + 1] - off[c];
+  const int64_t p0 = (int64_t)rp[c], np = (int64_t)rp[c + 1] - p0, v0 = (int64_t)rpv[c];
+  int64_t o = crp[r];
+  for (int64_t p = 0; p < np; ++p) {
+    const V v = val[v0 + p * csz + l];
+    if (v != V(0)) {
+      ci[o] = colids[p0 + p];
+      cv[o] = v;
+      ++o;
+    }
+  }
+}
+
+// A clustered-form handle's arrays from int64 / int32 device arrays.
+template <typename I, typename V>
+spops_status_t make_vlcluster(Context* ctx, int64_t rows, int64_t cols, int64_t ncl, const int64_t* offs_d,
+                              const int64_t* rptr, const int32_t* colids, int64_t nnzc, const int64_t* rptr_val,
+                              const V* vals, int64_t nnzv, spops_index_t itype, Matrix** out) {
+  cudaStream_t st = ctx->stream;
+  Matrix* M = new spops_matrix_s();
+  M->ctx = ctx;
+  M->format = SPOPS_FMT_VLCLUSTER;
+  M->itype = itype;
+  M->vtype = sizeof(V) == 8 ? SPOPS_VALUE_F64 : SPOPS_VALUE_F32;
+  M->rows = rows;
+  M->cols = cols;
+  M->nnz = nnzc;
+  M->clusters = ncl;
+  M->cl_nnzv = nnzv;
+  spops_status_t s = M->row.alloc((size_t)(ncl + 1) * sizeof(I));
+  if (s == SPOPS_OK) s = M->cl_rpv.alloc((size_t)(ncl + 1) * sizeof(I));
+  if (s == SPOPS_OK) s = M->col.alloc((size_t)std::max<int64_t>(nnzc, 1) * sizeof(I));
+  if (s == SPOPS_OK) s = M->val.alloc((size_t)std::max<int64_t>(nnzv, 1) * sizeof(V));
+  if (s == SPOPS_OK) {
+    cast_kernel<int64_t, I><<<grid_for(ncl + 1), 256, 0, st>>>(rptr, ncl + 1, M->row.as<I>());
+    cast_kernel<int64_t, I><<<grid_for(ncl + 1), 256, 0, st>>>(rptr_val, ncl + 1, M->cl_rpv.as<I>());
+    if (nnzc > 0) cast_kernel<int32_t, I><<<grid_for(nnzc), 256, 0, st>>>(colids, nnzc, M->col.as<I>());
+    if (nnzv > 0)
+      if (cudaMemcpyAsync(M->val.p, vals, (size_t)nnzv * sizeof(V), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        s = fail(SPOPS_ERR_CUDA, "clustered form: copy failed");
+    if (cudaGetLastError() != cudaSuccess) s = fail(SPOPS_ERR_CUDA, "clustered form: launch failed");
+  }
+  std::vector<int64_t> off_h((size_t)ncl + 1);
+  if (s == SPOPS_OK &&
+      cudaMemcpyAsync(off_h.data(), offs_d, (size_t)(ncl + 1) * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    s = fail(SPOPS_ERR_CUDA, "clustered form: copy failed");
+  if (s == SPOPS_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(SPOPS_ERR_CUDA, "clustered form: stream");
+  if (s == SPOPS_OK) s = vlcluster_finish(ctx, M, off_h.data());
+  if (s != SPOPS_OK) {
+    M->release_all();
+    delete static_cast<spops_matrix_s*>(M);
+    return s;
+  }
+  *out = M;
+  return SPOPS_OK;
+}
+
 template <typename I, typename V>
 spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_h, const int64_t* offs_h, int64_t ncl,
-                        bool sort_output, double l2_budget, bool rowwise, Matrix** out, SpgemmStats* stats) {
+                        bool sort_output, double l2_budget, bool rowwise, Matrix** out, SpgemmStats* stats,
+                        bool cluster_out) {
   cudaStream_t st = ctx->stream;
   const int64_t n = A->rows, nnz = A->nnz;
   Timer tm;
@@ -1303,6 +1452,53 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   if (stats) stats->numeric_ms = tm.lap(st);
   tr.mark(st, "numeric block kernels");
 
+  if (cluster_out) {  // --- C in the clustered form of A's clusters
+    PoolBuf kcnt(ctx), kval(ctx), nrp(ctx), nrpv(ctx), kcol(ctx), kv(ctx);
+    SPOPS_TRY(kcnt.alloc((size_t)(ncl + 1) * 8));
+    SPOPS_TRY(kval.alloc((size_t)(ncl + 1) * 8));
+    SPOPS_TRY(nrp.alloc((size_t)(ncl + 1) * 8));
+    SPOPS_TRY(nrpv.alloc((size_t)(ncl + 1) * 8));
+    SPOPS_CUDA(cudaMemsetAsync(kcnt.p, 0, (size_t)(ncl + 1) * 8, st));
+    SPOPS_CUDA(cudaMemsetAsync(kval.p, 0, (size_t)(ncl + 1) * 8, st));
+    if (ncl > 0) {
+      cl_keep_count_kernel<V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+                                                                 offs.as<int64_t>(), ncl, cval.as<V>(),
+                                                                 drop.as<unsigned char>(), kcnt.as<int64_t>(),
+                                                                 kval.as<int64_t>());
+      SPOPS_LAUNCH_CHECK();
+    }
+    size_t c1 = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c1, kcnt.as<int64_t>(), nrp.as<int64_t>(), ncl + 1, st));
+    SPOPS_TRY(tmp.alloc(c1 + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, kcnt.as<int64_t>(), nrp.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, kval.as<int64_t>(), nrpv.as<int64_t>(), ncl + 1, st));
+    int64_t h2[2] = {0, 0};
+    SPOPS_CUDA(cudaMemcpyAsync(h2, nrp.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(h2 + 1, nrpv.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    if (sizeof(I) == 4 && h2[1] > INT32_MAX)
+      return fail(SPOPS_ERR_TOO_LARGE, "SpGEMM: %lld clustered values exceed int32 indices", (long long)h2[1]);
+    SPOPS_TRY(kcol.alloc((size_t)std::max<int64_t>(h2[0], 1) * 4));
+    SPOPS_TRY(kv.alloc((size_t)std::max<int64_t>(h2[1], 1) * sizeof(V)));
+    if (ncl > 0) {
+      cl_compact_kernel<int32_t, V><<<grid_for(ncl * 32), 256, 0, st>>>(
+          ccptr.as<int64_t>(), ccptr_val.as<int64_t>(), offs.as<int64_t>(), ncl, ccol.as<int32_t>(), cval.as<V>(),
+          drop.as<unsigned char>(), nrp.as<int64_t>(), nrpv.as<int64_t>(), kcol.as<int32_t>(), kv.as<V>());
+      SPOPS_LAUNCH_CHECK();
+    }
+    SPOPS_TRY((make_vlcluster<I, V>(ctx, n, B->cols, ncl, offs.as<int64_t>(), nrp.as<int64_t>(), kcol.as<int32_t>(),
+                                    h2[0], nrpv.as<int64_t>(), kv.as<V>(), h2[1], A->itype, out)));
+    if (stats) {
+      stats->to_csr_ms = tm.lap(st);
+      stats->flops = 2 * total_products;
+      stats->clusters = ncl;
+      stats->dense_clusters = hdense;
+      stats->cluster_columns = nnzc;
+      stats->c_cluster_columns = h2[0];
+    }
+    return SPOPS_OK;
+  }
+
   // --- back to CSR, original row order
   PoolBuf rowcnt(ctx), crp(ctx);
   SPOPS_TRY(rowcnt.alloc((nn + 1) * 8));
@@ -1372,7 +1568,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
 
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
                               int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st,
-                              bool rowwise) {
+                              bool rowwise, bool cluster_out) {
   if (A->format != SPOPS_FMT_CSR || B->format != SPOPS_FMT_CSR)
     return fail(SPOPS_ERR_INVALID, "SpGEMM needs CSR matrices");
   if (A->cols != B->rows) return fail(SPOPS_ERR_INVALID, "SpGEMM: A.cols (%lld) != B.rows (%lld)",
@@ -1394,10 +1590,214 @@ spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t*
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));  // validates patterns
   if (!B->plan.ready) SPOPS_TRY(csr_analyse(ctx, B));
   const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
-  if (i32 && f64) return spgemm_t<int32_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
-  if (i32) return spgemm_t<int32_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
-  if (f64) return spgemm_t<int64_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
-  return spgemm_t<int64_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st);
+  if (i32 && f64) return spgemm_t<int32_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st,
+                                            cluster_out);
+  if (i32) return spgemm_t<int32_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st,
+                                            cluster_out);
+  if (f64) return spgemm_t<int64_t, double>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st,
+                                            cluster_out);
+  return spgemm_t<int64_t, float>(ctx, A, B, perm, offsets, nclusters, sort_output, l2_budget, rowwise, C, st,
+                                            cluster_out);
+}
+
+namespace {
+
+template <typename I, typename V>
+spops_status_t vl_from_csr_t(Context* ctx, Matrix* A, const int64_t* offs_h, int64_t ncl, Matrix** out) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = A->rows, nnz = A->nnz;
+  const size_t nn = (size_t)std::max<int64_t>(n, 1), nz1 = (size_t)std::max<int64_t>(nnz, 1);
+  PoolBuf perm(ctx), offs(ctx), rowcl(ctx), rlen(ctx), rpr(ctx), keys(ctx), skeys(ctx), src(ctx), ssrc(ctx),
+      flag(ctx), uidx(ctx), colids(ctx), ncols_u(ctx), cptr(ctx), cptr_val(ctx), cw(ctx), avals(ctx), roe(ctx),
+      tmp(ctx);
+  SPOPS_TRY(perm.alloc(nn * 8));
+  SPOPS_TRY(offs.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(rowcl.alloc(nn * 8));
+  SPOPS_TRY(rlen.alloc(nn * 8));
+  SPOPS_TRY(rpr.alloc((nn + 1) * 8));
+  SPOPS_CUDA(cudaMemcpyAsync(offs.p, offs_h, (size_t)(ncl + 1) * 8, cudaMemcpyHostToDevice, st));
+  if (n > 0) iota_kernel<<<grid_for(n), 256, 0, st>>>(perm.as<int64_t>(), n);
+  if (ncl > 0) row_cluster_kernel<<<grid_for(ncl), 256, 0, st>>>(offs.as<int64_t>(), ncl, rowcl.as<int64_t>());
+  if (n > 0) reordered_len_kernel<I><<<grid_for(n), 256, 0, st>>>(A->row.as<I>(), perm.as<int64_t>(), n, rlen.as<int64_t>());
+  SPOPS_LAUNCH_CHECK();
+  size_t cb = 0;
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cb, rlen.as<int64_t>(), rpr.as<int64_t>(), (int64_t)nn, st));
+  SPOPS_TRY(tmp.alloc(cb + 256));
+  if (n > 0) SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cb, rlen.as<int64_t>(), rpr.as<int64_t>(), n, st));
+  SPOPS_TRY(keys.alloc(nz1 * 8));
+  SPOPS_TRY(skeys.alloc(nz1 * 8));
+  SPOPS_TRY(src.alloc(nz1 * 8));
+  SPOPS_TRY(ssrc.alloc(nz1 * 8));
+  SPOPS_TRY(flag.alloc(nz1 * 8));
+  SPOPS_TRY(uidx.alloc(nz1 * 8));
+  SPOPS_TRY(roe.alloc(nz1 * 8));
+  if (n > 0) {
+    cluster_keys_kernel<I, V><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), perm.as<int64_t>(),
+                                                                rowcl.as<int64_t>(), n, rpr.as<int64_t>(),
+                                                                keys.as<uint64_t>(), src.as<int64_t>());
+    entry_row_kernel<I><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), perm.as<int64_t>(), n, roe.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  int64_t nnzc = 0;
+  SPOPS_TRY(ncols_u.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_CUDA(cudaMemsetAsync(ncols_u.p, 0, (size_t)(ncl + 1) * 8, st));
+  if (nnz > 0) {
+    size_t c1 = 0, c2 = 0;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, c1, keys.as<uint64_t>(), skeys.as<uint64_t>(), src.as<int64_t>(),
+                                               ssrc.as<int64_t>(), nnz, 0, 64, st));
+    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, c2, flag.as<int64_t>(), uidx.as<int64_t>(), nnz, st));
+    SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, c1, keys.as<uint64_t>(), skeys.as<uint64_t>(), src.as<int64_t>(),
+                                               ssrc.as<int64_t>(), nnz, 0, 64, st));
+    key_flag_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), nnz, flag.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, c2, flag.as<int64_t>(), uidx.as<int64_t>(), nnz, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&nnzc, uidx.as<int64_t>() + nnz - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+  }
+  SPOPS_TRY(colids.alloc((size_t)std::max<int64_t>(nnzc, 1) * 4));
+  if (nnz > 0) {
+    cluster_cols_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), flag.as<int64_t>(), uidx.as<int64_t>(),
+                                                       nnz, colids.as<int32_t>(),
+                                                       reinterpret_cast<unsigned long long*>(ncols_u.p));
+    SPOPS_LAUNCH_CHECK();
+  }
+  SPOPS_TRY(cptr.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(cptr_val.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(cw.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_CUDA(cudaMemsetAsync(cw.p, 0, (size_t)(ncl + 1) * 8, st));
+  const int64_t* cnt_d = reinterpret_cast<const int64_t*>(ncols_u.p);
+  if (ncl > 0) {
+    weight_kernel<<<grid_for(ncl), 256, 0, st>>>(cnt_d, offs.as<int64_t>(), ncl, cw.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  {
+    size_t c1 = 0, c2 = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c1, cnt_d, cptr.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c2, cw.as<int64_t>(), cptr_val.as<int64_t>(), ncl + 1, st));
+    SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, cnt_d, cptr.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c2, cw.as<int64_t>(), cptr_val.as<int64_t>(), ncl + 1, st));
+  }
+  int64_t nnzv = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&nnzv, cptr_val.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  if (sizeof(I) == 4 && nnzv > INT32_MAX)
+    return fail(SPOPS_ERR_TOO_LARGE, "csr_to_vlength_cluster: %lld values exceed int32 indices", (long long)nnzv);
+  SPOPS_TRY(avals.alloc((size_t)std::max<int64_t>(nnzv, 1) * sizeof(V)));
+  SPOPS_CUDA(cudaMemsetAsync(avals.p, 0, avals.bytes, st));
+  if (nnz > 0) {
+    cluster_vals_kernel<I, V><<<grid_for(nnz), 256, 0, st>>>(
+        skeys.as<uint64_t>(), ssrc.as<int64_t>(), uidx.as<int64_t>(), nnz, A->val.as<V>(), A->row.as<I>(),
+        perm.as<int64_t>(), offs.as<int64_t>(), cptr.as<int64_t>(), cptr_val.as<int64_t>(), roe.as<int64_t>(),
+        avals.as<V>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  return make_vlcluster<I, V>(ctx, n, A->cols, ncl, offs.as<int64_t>(), cptr.as<int64_t>(), colids.as<int32_t>(),
+                              nnzc, cptr_val.as<int64_t>(), avals.as<V>(), nnzv, A->itype, out);
+}
+
+template <typename I, typename V>
+spops_status_t vl_to_csr_t(Context* ctx, Matrix* M, Matrix** out) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = M->rows, ncl = M->clusters;
+  const size_t nn = (size_t)std::max<int64_t>(n, 1);
+  PoolBuf rowcl(ctx), cnt(ctx), crp(ctx), tmp(ctx);
+  SPOPS_TRY(rowcl.alloc(nn * 8));
+  SPOPS_TRY(cnt.alloc((nn + 1) * 8));
+  SPOPS_TRY(crp.alloc((nn + 1) * 8));
+  SPOPS_CUDA(cudaMemsetAsync(cnt.p, 0, (nn + 1) * 8, st));
+  if (ncl > 0) row_cluster_kernel<<<grid_for(ncl), 256, 0, st>>>(M->cl_off.as<int64_t>(), ncl, rowcl.as<int64_t>());
+  if (n > 0)
+    vlc_row_count_kernel<I, V><<<grid_for(n), 256, 0, st>>>(M->row.as<I>(), M->cl_rpv.as<I>(), M->cl_off.as<int64_t>(),
+                                                            ncl, rowcl.as<int64_t>(), n, M->val.as<V>(),
+                                                            cnt.as<int64_t>());
+  SPOPS_LAUNCH_CHECK();
+  size_t cb = 0;
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cb, cnt.as<int64_t>(), crp.as<int64_t>(), n + 1, st));
+  SPOPS_TRY(tmp.alloc(cb + 256));
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cb, cnt.as<int64_t>(), crp.as<int64_t>(), n + 1, st));
+  int64_t cnnz = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&cnnz, crp.as<int64_t>() + n, 8, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  Matrix* C = new spops_matrix_s();
+  C->ctx = ctx;
+  C->format = SPOPS_FMT_CSR;
+  C->itype = M->itype;
+  C->vtype = M->vtype;
+  C->rows = n;
+  C->cols = M->cols;
+  C->nnz = cnnz;
+  spops_status_t s = C->row.alloc((nn + 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->col.alloc((size_t)std::max<int64_t>(cnnz, 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->val.alloc((size_t)std::max<int64_t>(cnnz, 1) * sizeof(V));
+  if (s == SPOPS_OK) {
+    cast_kernel<int64_t, I><<<grid_for(n + 1), 256, 0, st>>>(crp.as<int64_t>(), n + 1, C->row.as<I>());
+    if (n > 0 && cnnz > 0)
+      vlc_row_write_kernel<I, V><<<grid_for(n), 256, 0, st>>>(M->row.as<I>(), M->cl_rpv.as<I>(), M->col.as<I>(),
+                                                              M->cl_off.as<int64_t>(), rowcl.as<int64_t>(), n,
+                                                              M->val.as<V>(), crp.as<int64_t>(), C->col.as<I>(),
+                                                              C->val.as<V>());
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+      s = fail(SPOPS_ERR_CUDA, "vlength_cluster2csr: launch failed");
+  }
+  if (s != SPOPS_OK) {
+    C->release_all();
+    delete static_cast<spops_matrix_s*>(C);
+    return s;
+  }
+  *out = C;
+  return SPOPS_OK;
+}
+
+}  // namespace
+
+spops_status_t vlcluster_finish(Context* ctx, Matrix* M, const int64_t* off_h) {
+  cudaStream_t st = ctx->stream;
+  const int64_t ncl = M->clusters;
+  int64_t mx = 256;  // as csr_to_vlength_cluster: starts at 256, raised by larger clusters
+  std::vector<int64_t> sz((size_t)std::max<int64_t>(ncl, 1), 0);
+  for (int64_t c = 0; c < ncl; ++c) {
+    sz[(size_t)c] = off_h[c + 1] - off_h[c];
+    mx = std::max(mx, sz[(size_t)c]);
+  }
+  M->cl_max_sz = mx;
+  SPOPS_TRY(M->cl_off.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(M->cl_sz.alloc((size_t)std::max<int64_t>(ncl, 1) * M->isize()));
+  SPOPS_CUDA(cudaMemcpyAsync(M->cl_off.p, off_h, (size_t)(ncl + 1) * 8, cudaMemcpyHostToDevice, st));
+  if (M->itype == SPOPS_INDEX_I64) {
+    SPOPS_CUDA(cudaMemcpyAsync(M->cl_sz.p, sz.data(), (size_t)ncl * 8, cudaMemcpyHostToDevice, st));
+  } else {
+    std::vector<int32_t> s32(sz.begin(), sz.end());
+    SPOPS_CUDA(cudaMemcpyAsync(M->cl_sz.p, s32.data(), (size_t)ncl * 4, cudaMemcpyHostToDevice, st));
+  }
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  return SPOPS_OK;
+}
+
+spops_status_t vlcluster_from_csr(Context* ctx, Matrix* A, const int64_t* offsets, int64_t nclusters, Matrix** out) {
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "csr_to_vlength_cluster: needs a CSR matrix");
+  if (nclusters < 0 || offsets[0] != 0 || offsets[nclusters] != A->rows)
+    return fail(SPOPS_ERR_INVALID, "csr_to_vlength_cluster: offsets must run from 0 to rows");
+  for (int64_t c = 0; c < nclusters; ++c)
+    if (offsets[c + 1] < offsets[c]) return fail(SPOPS_ERR_INVALID, "csr_to_vlength_cluster: offsets not monotone");
+  if (A->cols > INT32_MAX || nclusters > INT32_MAX)
+    return fail(SPOPS_ERR_UNSUPPORTED, "csr_to_vlength_cluster: more than 2^31 columns or clusters");
+  if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));  // validates the pattern
+  const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return vl_from_csr_t<int32_t, double>(ctx, A, offsets, nclusters, out);
+  if (i32) return vl_from_csr_t<int32_t, float>(ctx, A, offsets, nclusters, out);
+  if (f64) return vl_from_csr_t<int64_t, double>(ctx, A, offsets, nclusters, out);
+  return vl_from_csr_t<int64_t, float>(ctx, A, offsets, nclusters, out);
+}
+
+spops_status_t vlcluster_to_csr(Context* ctx, Matrix* M, Matrix** out) {
+  if (M->format != SPOPS_FMT_VLCLUSTER) return fail(SPOPS_ERR_INVALID, "vlength_cluster2csr: needs a clustered matrix");
+  const bool i32 = M->itype == SPOPS_INDEX_I32, f64 = M->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return vl_to_csr_t<int32_t, double>(ctx, M, out);
+  if (i32) return vl_to_csr_t<int32_t, float>(ctx, M, out);
+  if (f64) return vl_to_csr_t<int64_t, double>(ctx, M, out);
+  return vl_to_csr_t<int64_t, float>(ctx, M, out);
 }
 
 }  // namespace spops

@@ -305,6 +305,11 @@ struct Matrix {
   TransposeData tr;
   Csr5Data csr5;
   DevBuf spmm_partial;  // SpMM long-row chunk sums (k per chunk)
+  // SPOPS_FMT_VLCLUSTER (row = rowptr [clusters + 1], col = colids [nnz],
+  // val = values [cl_nnzv]; rows = CSR rows): rows per cluster, value
+  // offsets per cluster, and the first row of every cluster (int64)
+  DevBuf cl_sz, cl_rpv, cl_off;
+  int64_t clusters = 0, cl_nnzv = 0, cl_max_sz = 0;
   // COO: the same entries as a CSR matrix sorted by row (owned)
   Matrix* csr_view = nullptr;
   // host copy of the pattern (int64), made once for the host clustering
@@ -370,9 +375,15 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
 spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int64_t n, const int64_t* pi,
                                        const int64_t* pj, const double* ps, int64_t np, int64_t cluster_size,
                                        std::vector<int64_t>& perm, std::vector<int64_t>& offsets);
+// cluster_out: C in the clustered form of A's clusters (SPOPS_FMT_VLCLUSTER,
+// rows in cluster order) instead of CSR in A's row order
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
                               int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st,
-                              bool rowwise = false);
+                              bool rowwise = false, bool cluster_out = false);
+// clustered (VLength) form of a CSR matrix and back (spgemm.cu)
+spops_status_t vlcluster_from_csr(Context* ctx, Matrix* A, const int64_t* offsets, int64_t nclusters, Matrix** out);
+spops_status_t vlcluster_to_csr(Context* ctx, Matrix* M, Matrix** out);
+spops_status_t vlcluster_finish(Context* ctx, Matrix* M, const int64_t* off_h);  // cluster_sz, cl_off, max size
 // spgemm_topk.cu
 spops_status_t rowwise_spgemm(Context* ctx, Matrix* A, Matrix* B, bool sort_output, Matrix** C, SpgemmStats* st);
 spops_status_t topk_spgemm(Context* ctx, Matrix* A, int64_t top_k, Matrix** C);

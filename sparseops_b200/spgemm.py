@@ -121,6 +121,69 @@ def LeSpGEMM_clustered(A: CSR_Matrix, B: CSR_Matrix, permutation, offsets, sort_
     return SpGEMMResult(_Handle(ctx, out), A.num_rows, B.num_cols, it, vt, st.as_dict())
 
 
+class VLengthCluster:
+    """CSR_VlengthCluster (spgemm_cluster.h:108-143) held by a device handle:
+    clusters of consecutive rows, each with the union of its rows' columns and
+    values[rowptr_val[i] + p * cluster_sz[i] + k] for column p and row k."""
+
+    def __init__(self, handle: _Handle, index_dtype, value_dtype, stats=None):
+        info = handle.info()
+        self._h = handle
+        self.csr_rows, self.cols, self.nnzc = int(info.rows), int(info.cols), int(info.nnz)
+        self.rows, self.nnzv, self.max_cluster_sz = int(info.extra[0]), int(info.extra[1]), int(info.extra[2])
+        self._it = np.int32 if int(index_dtype) == 0 else np.int64  # spops_index_t / spops_value_t codes
+        self._vt = np.float32 if int(value_dtype) == 0 else np.float64
+        self._codes = (int(index_dtype), int(value_dtype))
+        self.stats = stats or {}
+
+    def host(self) -> dict:
+        """cluster_sz, rowptr, colids, rowptr_val, values as numpy arrays."""
+        h = self._h
+        out = {}
+        for name, which, n, dt in (("cluster_sz", 12, self.rows, self._it), ("rowptr", 0, self.rows + 1, self._it),
+                                   ("colids", 1, self.nnzc, self._it), ("rowptr_val", 13, self.rows + 1, self._it),
+                                   ("values", 2, self.nnzv, self._vt)):
+            a = np.empty(n, dt)
+            if n:
+                call("spops_matrix_download", h.ctx.handle, h.handle, which, vp(a.ctypes.data), i64(n))
+            out[name] = a
+        return out
+
+
+def csr_to_vlength_cluster(csr: CSR_Matrix, offsets) -> VLengthCluster:
+    """include/sparse_conversion.h:1641 on the device: cluster i is rows
+    offsets[i] .. offsets[i+1]; each cluster's columns ascending."""
+    h = csr.device()
+    ctx = h.ctx.follow_torch()
+    offs = np.ascontiguousarray(np.asarray(offsets, np.int64))
+    out = vp()
+    call("spops_csr_to_vlength_cluster", ctx.handle, h.handle, _p(offs), i64(len(offs) - 1), C.byref(out))
+    it, vt = _types(csr)
+    return VLengthCluster(_Handle(ctx, out), it, vt)
+
+
+def vlength_cluster2csr(cluster: VLengthCluster) -> DeviceCSR:
+    """include/sparse_conversion.h:1778 on the device: rows in cluster order,
+    exact zeros dropped."""
+    h = cluster._h
+    out = vp()
+    call("spops_vlength_cluster_to_csr", h.ctx.handle, h.handle, C.byref(out))
+    return DeviceCSR(_Handle(h.ctx, out), cluster.csr_rows, cluster.cols)
+
+
+def LeSpGEMM_VLength(A_cluster: VLengthCluster, B: CSR_Matrix, sort_output: bool = True, kernel_flag: int = 3,
+                     l2_budget: float = L2_BUDGET_DEFAULT) -> VLengthCluster:
+    """include/spgemm.h:176: C = A*B with A clustered, C in A's clusters
+    (kernel-3 rules; kernel_flag is accepted for the signature's sake)."""
+    ha, hb = A_cluster._h, B.device()
+    ctx = ha.ctx.follow_torch()
+    out = vp()
+    st = SpgemmStats()
+    call("spops_spgemm_vlength", ctx.handle, ha.handle, hb.handle, i32(1 if sort_output else 0), dbl(l2_budget),
+         C.byref(out), C.byref(st))
+    return VLengthCluster(_Handle(ctx, out), *A_cluster._codes, st.as_dict())
+
+
 def LeSpGEMM_lsh(A: CSR_Matrix, B: CSR_Matrix, k: int = 64, num_bands: int = 16, seed: int = 7,
                  cluster_size: int = 8, sort_output: bool = False,
                  l2_budget: float = L2_BUDGET_DEFAULT) -> SpGEMMResult:

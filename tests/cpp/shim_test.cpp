@@ -447,6 +447,30 @@ void api_checks() {
   CSR_Matrix<int, double> bp = csr_to_binary_pattern(csr);
   EXPECT(bp.num_nnzs == csr.num_nnzs && bp.values[0] == 1.0 && bp.col_index[5] == csr.col_index[5],
          "csr_to_binary_pattern");
+  // the clustered LeSpGEMM flow (test/test_spgemm_hc_lsh.cpp) against the
+  // row-wise LeSpGEMM: clusters of 8 rows, C = A * A^T
+  {
+    std::vector<int> offs;
+    for (int r = 0; r < n; r += 8) offs.push_back(r);
+    offs.push_back(n);
+    CSR_VlengthCluster<int, double> acl = csr_to_vlength_cluster(csr, offs);
+    EXPECT(acl.rows == (int)offs.size() - 1 && acl.cluster_sz[0] == 8 && acl.max_cluster_sz == 256,
+           "csr_to_vlength_cluster shape");
+    CSR_VlengthCluster<int, double> ccl;
+    std::memset(static_cast<void*>(&ccl), 0, sizeof(ccl));
+    LeSpGEMM_VLength<true>(acl, t, ccl, 3);
+    CSR_Matrix<int, double> c1 = vlength_cluster2csr(ccl), c2;
+    LeSpGEMM<true>(csr, t, c2, 1);
+    bool same = c1.num_rows == c2.num_rows && c1.num_nnzs == c2.num_nnzs;
+    for (int r = 0; same && r <= n; ++r) same = c1.row_offset[r] == c2.row_offset[r];
+    for (int k = 0; same && k < c1.num_nnzs; ++k)
+      same = c1.col_index[k] == c2.col_index[k] && std::fabs(c1.values[k] - c2.values[k]) <= 1e-12 * (1 + std::fabs(c2.values[k]));
+    EXPECT(same, "LeSpGEMM_VLength = row-wise LeSpGEMM");
+    delete_vlength_cluster_matrix(acl);
+    delete_host_matrix(ccl);
+    delete_csr_matrix(c1);
+    delete_csr_matrix(c2);
+  }
   delete_csr_matrix(t);
   delete_csr_matrix(bp);
   delete_csr_matrix(csr);

@@ -199,3 +199,68 @@ def test_topk_vs_oracle(cuda, orc, k):
     assert np.array_equal(rp.astype(np.int64), ref["rp"])
     assert np.array_equal(ci.astype(np.int64), ref["ci"])
     assert np.array_equal(v, ref["v"])
+
+
+@pytest.mark.parametrize("so", [0, 1])
+def test_vlength_pipeline_golden(cuda, golden, orc, so):
+    """The reference driver's flow (test/test_spgemm_hc_lsh.cpp:230-300):
+    csr_reorder_rows by the clustering, csr_to_vlength_cluster,
+    LeSpGEMM_VLength, vlength_cluster2csr and the inverse reorder give the
+    reference's C (structure bit-exact, values to 1e-12)."""
+    from sparseops_b200 import csr_reorder_rows
+    from sparseops_b200.spgemm import LeSpGEMM_VLength, csr_to_vlength_cluster, vlength_cluster2csr
+    g = golden
+    arp, aci, av = g["sp_arp"], g["sp_aci"], g["sp_av"]
+    brp, bci, bv = synth.transpose(arp, aci, av, 1024)
+    perm, offs = g["sp_perm"], g["sp_offsets"]
+    Acl = csr_to_vlength_cluster(csr_reorder_rows(_csr(arp, aci, av), perm), offs)
+    h = Acl.host()
+    assert h["cluster_sz"].sum() == len(perm) and h["rowptr"][-1] == Acl.nnzc and h["rowptr_val"][-1] == Acl.nnzv
+    assert Acl.max_cluster_sz == 256  # the reference starts it at 256
+    Ccl = LeSpGEMM_VLength(Acl, _csr(brp, bci, bv), sort_output=bool(so))
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    C = csr_reorder_rows(vlength_cluster2csr(Ccl), inv)
+    assert np.array_equal(C.host()[0].astype(np.int64), g[f"sp_c{so}_rp"])
+    assert np.array_equal(C.host()[1].astype(np.int64), g[f"sp_c{so}_ci"])
+    _check_c(C, orc.spgemm((arp, aci, av), (brp, bci, bv), perm, offs, sort_output=bool(so)))
+
+
+@pytest.mark.parametrize("itype,vtype", [(np.int32, np.float64), (np.int64, np.float32)])
+def test_vlength_cluster_layout(cuda, itype, vtype):
+    """csr_to_vlength_cluster against a plain construction: each cluster's
+    columns ascending, values[rowptr_val[c] + p * sz + k]; vlength_cluster2csr
+    gives the CSR back (rows sorted, no explicit zeros)."""
+    from sparseops_b200.spgemm import csr_to_vlength_cluster, vlength_cluster2csr
+    rng = np.random.default_rng(17)
+    n, nc = 3000, 900
+    rows = [np.sort(rng.choice(nc, int(rng.integers(0, 12)), replace=False)) for _ in range(n)]
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(itype)
+    ci = np.concatenate(rows).astype(itype)
+    v = (rng.standard_normal(len(ci)) + 3.0).astype(vtype)  # no zeros
+    sizes = rng.integers(1, 14, 600)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    offs = offs[offs < n]
+    offs = np.concatenate([offs, [n]]).astype(np.int64)
+    cl = csr_to_vlength_cluster(_csr(rp, ci, v, nc), offs)
+    h = cl.host()
+    assert cl.rows == len(offs) - 1 and np.array_equal(h["cluster_sz"], np.diff(offs))
+    p0 = 0
+    for c in range(cl.rows):
+        r0, r1 = offs[c], offs[c + 1]
+        cols = np.unique(ci[rp[r0]:rp[r1]].astype(np.int64))
+        got = h["colids"][h["rowptr"][c]:h["rowptr"][c + 1]].astype(np.int64)
+        assert np.array_equal(got, cols), c
+        sz = r1 - r0
+        block = h["values"][h["rowptr_val"][c]:h["rowptr_val"][c + 1]].reshape(len(cols), sz)
+        for k in range(sz):
+            r = r0 + k
+            rc, rv = ci[rp[r]:rp[r + 1]].astype(np.int64), v[rp[r]:rp[r + 1]]
+            want = np.zeros(len(cols), vtype)
+            want[np.searchsorted(cols, rc)] = rv
+            assert np.array_equal(block[:, k], want), (c, k)
+        p0 += len(cols)
+    assert p0 == cl.nnzc
+    back = vlength_cluster2csr(cl).host()
+    assert np.array_equal(back[0].astype(np.int64), rp.astype(np.int64))
+    assert np.array_equal(back[1].astype(np.int64), ci.astype(np.int64)) and np.array_equal(back[2], v)
