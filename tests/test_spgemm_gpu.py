@@ -264,3 +264,69 @@ def test_vlength_cluster_layout(cuda, itype, vtype):
     back = vlength_cluster2csr(cl).host()
     assert np.array_equal(back[0].astype(np.int64), rp.astype(np.int64))
     assert np.array_equal(back[1].astype(np.int64), ci.astype(np.int64)) and np.array_equal(back[2], v)
+
+
+def _vl_edge_case(rng):
+    """1200 x 500 A (every 7th row empty; rows 1000.. only in columns 400..,
+    which are B's empty rows) and 500 x 400 B, with positive values so that
+    no product cancels; clusters: one of 300 rows, two of none, then tens."""
+    n, k, m = 1200, 500, 400
+    lens = rng.integers(0, 5, n)
+    lens[::7] = 0
+    rows = [np.sort(rng.choice(400, int(ln), replace=False)) if r < 1000 else
+            np.sort(rng.choice(np.arange(400, k), int(ln), replace=False)) for r, ln in enumerate(lens)]
+    arp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    aci = np.concatenate(rows).astype(np.int64)
+    av = rng.uniform(0.5, 2.0, len(aci))
+    blens = rng.integers(0, 6, k)
+    blens[400:] = 0
+    brp = np.concatenate([[0], np.cumsum(blens)]).astype(np.int64)
+    bci = np.concatenate([np.sort(rng.choice(m, int(ln), replace=False)) for ln in blens]).astype(np.int64)
+    bv = rng.uniform(0.5, 2.0, len(bci))
+    offs = np.array([0, 300, 300, 300] + list(range(310, n, 10)) + [n], np.int64)
+    return (arp, aci, av, k), (brp, bci, bv, m), offs
+
+
+@pytest.mark.parametrize("so", [0, 1])
+def test_vlength_edges(cuda, so):
+    """Empty clusters, a cluster of 300 rows (max_cluster_sz follows it; its
+    accumulator exceeds shared memory), empty rows, and clusters whose
+    product is empty: vlength_cluster2csr(LeSpGEMM_VLength) equals A*B."""
+    import scipy.sparse as sp
+    from sparseops_b200.spgemm import LeSpGEMM_VLength, csr_to_vlength_cluster, vlength_cluster2csr
+    (arp, aci, av, k), (brp, bci, bv, m), offs = _vl_edge_case(np.random.default_rng(23))
+    n = len(arp) - 1
+    Acl = csr_to_vlength_cluster(_csr(arp, aci, av, k), offs)
+    assert Acl.rows == len(offs) - 1 and Acl.max_cluster_sz == 300
+    Ccl = LeSpGEMM_VLength(Acl, _csr(brp, bci, bv, m), sort_output=bool(so))
+    assert Ccl.rows == Acl.rows and Ccl.max_cluster_sz == 300 and Ccl.csr_rows == n and Ccl.cols == m
+    h = Ccl.host()
+    assert np.array_equal(h["cluster_sz"].astype(np.int64), np.diff(offs))
+    late = np.searchsorted(offs, 1000)  # clusters of rows 1000.. have no products
+    assert np.all(np.diff(h["rowptr"].astype(np.int64))[late:] == 0)
+    want = (sp.csr_matrix((av, aci, arp), shape=(n, k)) @ sp.csr_matrix((bv, bci, brp), shape=(k, m))).tocsr()
+    want.sort_indices()
+    rp, ci, v = vlength_cluster2csr(Ccl).host()
+    got = sp.csr_matrix((v, ci.astype(np.int64), rp.astype(np.int64)), shape=(n, m))
+    got.sort_indices()
+    assert np.array_equal(got.indptr, want.indptr) and np.array_equal(got.indices, want.indices)
+    assert np.abs(got.data - want.data).max() <= 1e-12 * np.abs(want.data).max()
+
+
+def test_vlength_refusals(cuda):
+    """Offsets that do not run from 0 to rows or go backwards, a plain CSR
+    where a clustered A is expected, and mismatched inner sizes are errors."""
+    from sparseops_b200._lib import SpOpsError
+    from sparseops_b200.spgemm import LeSpGEMM_VLength, VLengthCluster, csr_to_vlength_cluster
+    (arp, aci, av, k), (brp, bci, bv, m), offs = _vl_edge_case(np.random.default_rng(29))
+    A = _csr(arp, aci, av, k)
+    for bad in ([0, 600, 1100], [1, 600, 1200], [0, 700, 600, 1200]):
+        with pytest.raises(SpOpsError):
+            csr_to_vlength_cluster(A, np.array(bad, np.int64))
+    Acl = csr_to_vlength_cluster(A, offs)
+    with pytest.raises(SpOpsError):
+        LeSpGEMM_VLength(Acl, _csr(arp, aci, av, k))  # 500 columns of A against 1200 rows
+    fake = VLengthCluster.__new__(VLengthCluster)
+    fake._h, fake._codes = A.device(), Acl._codes
+    with pytest.raises(SpOpsError):
+        LeSpGEMM_VLength(fake, _csr(brp, bci, bv, m))
