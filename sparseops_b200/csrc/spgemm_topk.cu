@@ -19,10 +19,11 @@
 //      gives |A_i n A_j| for every structural pair (i, j);
 //   2. per entry j != i: u = |A_i| + |A_j| - inter (row lengths of A),
 //      jacc = u == 0 ? 0 : (V)1 * inter / (V)u in the value type;
-//   3. per row, entries sorted by (jacc descending, column ascending) -- one
-//      stable segmented radix sort of a descending key with the columns in
-//      ascending order as payload -- and the first top_k kept, the diagonal
-//      excluded.  Rows of the result are in that order, as the reference's.
+//   3. per row, entries ranked by (jacc descending, column ascending) and
+//      the first top_k kept, the diagonal excluded: for top_k <= 32 a warp
+//      per row selects them in registers, else one stable segmented radix
+//      sort of a descending key with the columns in ascending order as
+//      payload.  Rows of the result are in that order, as the reference's.
 #include <cub/cub.cuh>
 
 #include <numeric>
@@ -115,6 +116,106 @@ __global__ void topk_write_kernel(const I* __restrict__ crp, const uint64_t* __r
   }
 }
 
+// (key, column) order of the ranking: key ascending (similarity descending),
+// then column ascending -- the order the stable segmented sort gives.
+__device__ __forceinline__ bool rank_less(uint64_t ka, int64_t ca, uint64_t kb, int64_t cb) {
+  return ka < kb || (ka == kb && ca < cb);
+}
+
+// One compare-exchange step of a warp-wide bitonic network over one
+// (key, column) per lane; `up` says whether this lane's block ascends.
+__device__ __forceinline__ void warp_cx(uint64_t& k, int64_t& c, int j, bool up) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t pk = __shfl_xor_sync(0xffffffffu, k, j);
+  const int64_t pc = __shfl_xor_sync(0xffffffffu, c, j);
+  const bool keep_min = ((lane & j) == 0) == up;
+  const bool take = keep_min ? rank_less(pk, pc, k, c) : rank_less(k, c, pk, pc);
+  if (take) {
+    k = pk;
+    c = pc;
+  }
+}
+
+__device__ __forceinline__ void warp_sort32(uint64_t& k, int64_t& c) {
+  const int lane = threadIdx.x & 31;
+  for (int b = 2; b <= 32; b <<= 1)
+    for (int j = b >> 1; j > 0; j >>= 1) warp_cx(k, c, j, (lane & b) == 0);
+}
+
+// Top-k (k <= 32) without the full sort: one warp per row of the
+// intersection counts keeps its best 32 entries, sorted across the lanes, and
+// merges every further 32 entries into them (lane l keeps the better of
+// best[l] and new[31 - l], which leaves the best 32 of both as a bitonic
+// sequence; five steps sort it).  A chunk with nothing better than the
+// current k-th entry is skipped.  The first k of the row go to tkey / tcol at
+// row * k, and kept[row] = min(k, entries - diagonal).
+template <typename I, typename V>
+__global__ void topk_select_kernel(const I* __restrict__ crp, const I* __restrict__ cci, const V* __restrict__ cval,
+                                   const I* __restrict__ arp, int64_t n, int k, uint64_t* __restrict__ tkey,
+                                   I* __restrict__ tcol, int64_t* __restrict__ kept) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const int64_t e0 = crp[i], e1 = crp[i + 1];
+  const int64_t li = (int64_t)arp[i + 1] - (int64_t)arp[i];
+  uint64_t bk = kDiagKey;  // padding sorts after every entry, the diagonal included
+  int64_t bc = INT64_MAX;
+  int diag = 0;
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int64_t e = base + lane;
+    uint64_t key = kDiagKey;
+    int64_t col = INT64_MAX;
+    if (e < e1) {
+      col = (int64_t)cci[e];
+      if (col == i) {
+        diag = 1;
+      } else {
+        const V inter = cval[e];
+        const int64_t u = li + ((int64_t)arp[col + 1] - (int64_t)arp[col]) - (int64_t)inter;
+        key = desc_key(u == 0 ? V(0) : V(1) * inter / (V)u);
+      }
+    }
+    if (k > 0) {
+      const uint64_t tk = __shfl_sync(0xffffffffu, bk, k - 1);
+      const int64_t tc = __shfl_sync(0xffffffffu, bc, k - 1);
+      if (!__any_sync(0xffffffffu, rank_less(key, col, tk, tc))) continue;
+    }
+    warp_sort32(key, col);
+    const uint64_t rk = __shfl_sync(0xffffffffu, key, 31 - lane);
+    const int64_t rc = __shfl_sync(0xffffffffu, col, 31 - lane);
+    if (rank_less(rk, rc, bk, bc)) {
+      bk = rk;
+      bc = rc;
+    }
+    for (int j = 16; j > 0; j >>= 1) warp_cx(bk, bc, j, true);
+  }
+  diag = __any_sync(0xffffffffu, diag);
+  if (lane < k) {
+    tkey[i * k + lane] = bk;
+    tcol[i * k + lane] = (I)(bc == INT64_MAX ? 0 : bc);
+  }
+  if (lane == 0) {
+    const int64_t avail = e1 - e0 - diag;
+    kept[i] = avail < k ? avail : k;
+  }
+}
+
+template <typename I, typename V>
+__global__ void topk_write_strided_kernel(const uint64_t* __restrict__ tkey, const I* __restrict__ tcol, int k,
+                                          const int64_t* __restrict__ orp, int64_t n, I* __restrict__ out_rp,
+                                          I* __restrict__ oci, V* __restrict__ ov) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i > n) return;
+  if (lane == 0) out_rp[i] = (I)orp[i];
+  if (i == n) return;
+  const int64_t o = orp[i], m = orp[i + 1] - orp[i];
+  if (lane < m) {
+    oci[o + lane] = tcol[i * k + lane];
+    ov[o + lane] = from_key(tkey[i * k + lane], V(0));
+  }
+}
+
 Matrix* new_csr(Context* ctx, const Matrix* like, int64_t rows, int64_t cols, int64_t nnz) {
   Matrix* C = new spops_matrix_s();
   C->ctx = ctx;
@@ -154,8 +255,48 @@ spops_status_t topk_t(Context* ctx, Matrix* A, int64_t top_k, Matrix** out) {
   SPOPS_TRY(rowwise_spgemm(ctx, Ab, At, true, &Cn, nullptr));
   Guard gc{Cn};
   const int64_t cnnz = Cn->nnz;
-  // 3. keys, per-row stable sort, top k
+  // 3. keys and the best k per row: a warp selection for k <= 32, else a
+  //    per-row stable sort
   PoolBuf key(ctx), skey(ctx), col(ctx), scol(ctx), diag(ctx), kept(ctx), orp(ctx), tmp(ctx);
+  if (top_k <= 32) {
+    const int k = (int)std::max<int64_t>(top_k, 0);
+    const size_t nk = (size_t)std::max<int64_t>(n * k, 1);
+    SPOPS_TRY(skey.alloc(nk * 8));
+    SPOPS_TRY(scol.alloc(nk * sizeof(I)));
+    SPOPS_TRY(kept.alloc((size_t)(n + 1) * 8));
+    SPOPS_TRY(orp.alloc((size_t)(n + 1) * 8));
+    SPOPS_CUDA(cudaMemsetAsync(kept.p, 0, (size_t)(n + 1) * 8, st));
+    if (n > 0) {
+      topk_select_kernel<I, V><<<grid_for(n * 32), 256, 0, st>>>(Cn->row.as<I>(), Cn->col.as<I>(), Cn->val.as<V>(),
+                                                                 A->row.as<I>(), n, k, skey.as<uint64_t>(),
+                                                                 scol.as<I>(), kept.as<int64_t>());
+      SPOPS_LAUNCH_CHECK();
+    }
+    size_t sb = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, sb, kept.as<int64_t>(), orp.as<int64_t>(), n + 1, st));
+    SPOPS_TRY(tmp.alloc(sb + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, sb, kept.as<int64_t>(), orp.as<int64_t>(), n + 1, st));
+    int64_t onnz = 0;
+    SPOPS_CUDA(cudaMemcpyAsync(&onnz, orp.as<int64_t>() + n, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    Matrix* C = new_csr(ctx, A, n, n, onnz);
+    spops_status_t s = C->row.alloc((size_t)(n + 1) * sizeof(I));
+    if (s == SPOPS_OK) s = C->col.alloc((size_t)std::max<int64_t>(onnz, 1) * sizeof(I));
+    if (s == SPOPS_OK) s = C->val.alloc((size_t)std::max<int64_t>(onnz, 1) * sizeof(V));
+    if (s == SPOPS_OK) {
+      topk_write_strided_kernel<I, V><<<grid_for((n + 1) * 32), 256, 0, st>>>(
+          skey.as<uint64_t>(), scol.as<I>(), k, orp.as<int64_t>(), n, C->row.as<I>(), C->col.as<I>(), C->val.as<V>());
+      if (cudaGetLastError() != cudaSuccess) s = fail(SPOPS_ERR_CUDA, "top-k write launch failed");
+    }
+    if (s == SPOPS_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(SPOPS_ERR_CUDA, "top-k: stream error");
+    if (s != SPOPS_OK) {
+      C->release_all();
+      delete static_cast<spops_matrix_s*>(C);
+      return s;
+    }
+    *out = C;
+    return SPOPS_OK;
+  }
   const size_t c1 = (size_t)std::max<int64_t>(cnnz, 1);
   SPOPS_TRY(key.alloc(c1 * 8));
   SPOPS_TRY(skey.alloc(c1 * 8));

@@ -189,9 +189,10 @@ def test_topk_golden(cuda, golden, f32, itype):
     assert np.array_equal(v.astype(np.float64), g[f"topk{f32}_v"])
 
 
-@pytest.mark.parametrize("k", [0, 1, 40])
+@pytest.mark.parametrize("k", [0, 1, 16, 32, 33, 40])
 def test_topk_vs_oracle(cuda, orc, k):
-    """A larger planted matrix; k = 0 keeps nothing, k = 40 exceeds many rows."""
+    """A larger planted matrix; k = 0 keeps nothing, k <= 32 takes the warp
+    selection and 33, 40 the sort, 40 exceeds many rows."""
     from sparseops_b200.spgemm import HashSpGEMMTopK
     arp, aci, av = synth.planted_communities(20000, ncomm=128, mean=14.0, seed=29)
     ref = orc.spgemm_topk(arp, aci, 20000, k)
