@@ -184,6 +184,13 @@ spops_status_t spops_matrix_device_bytes(spops_matrix_t A, int64_t* bytes);
 /* Point a CSR handle at new values (same pattern, same length, device
  * pointer, borrowed).  Keeps the analysis; marks derived values stale. */
 spops_status_t spops_csr_set_values(spops_matrix_t A, const void* values);
+/* Copy new values from host memory into a CSR handle that owns its values
+ * (created from SPOPS_MEM_HOST arrays): same pattern, nnz values of the
+ * handle's value type, queued on the context's stream.  Keeps the analysis;
+ * marks derived values stale.  This is what the reference's per-call read of
+ * A.values amounts to when the pattern is kept on the device (SpOps_csr,
+ * src/spmv_csr.cpp:165, reads the host arrays on every call). */
+spops_status_t spops_csr_upload_values(spops_context_t ctx, spops_matrix_t A, const void* host_values);
 
 /* ------------------------------------------------------ format handles */
 /* Device conversion of a CSR handle into another format (all work on the
@@ -537,10 +544,13 @@ spops_status_t spops_spgemm_vlength(spops_context_t ctx, spops_matrix_t A_cluste
  * synchronisation).  Scratch lives in one fixed 4 MiB device array of the
  * library (held by every GPU that loads it until exit), which limits nnz to
  * 134,217,728 (larger: SPOPS_ERR_TOO_LARGE, nothing launched).  The first call
- * on a device looks that array up (make it before any stream capture).  Calls
- * whose work overlaps on the GPU race on the array.  Out-of-range column
- * indices are skipped and reported (SPOPS_ERR_INVALID).  Synchronises
- * `stream` (a cudaStream_t, may be NULL) before returning. */
+ * on a device (per CUDA context) looks that array up: make it before any
+ * stream capture begins.  Calls whose work overlaps on the GPU race on the
+ * array.  The row pointer is checked on the device first (row_offset[0] == 0,
+ * non-decreasing, row_offset[rows] == nnz); a bad one is reported as
+ * SPOPS_ERR_INVALID with y untouched.  Out-of-range column indices are
+ * skipped and reported (SPOPS_ERR_INVALID).  Synchronises `stream` (a
+ * cudaStream_t, may be NULL) before returning. */
 spops_status_t spops_csr_spmv_noalloc(int64_t rows, int64_t cols, int64_t nnz, const void* row_offset,
                                       const void* col_index, const void* values, spops_index_t itype,
                                       spops_value_t vtype, double alpha, const void* x, double beta, void* y,

@@ -22,13 +22,18 @@
  *   CSR_VlengthCluster, csr_to_vlength_cluster, LeSpGEMM_VLength, vlength_cluster2csr
  *
  * What differs, and why:
- *   - Work runs on the GPU.  The first SpOps call on a matrix uploads it and
- *     keeps the device copy (with its analysis) keyed by the struct's first
- *     array pointer; later calls only move x and y.  Host arrays are therefore
- *     read once: after changing them in place, call spops_b200::invalidate(ptr)
- *     (delete_host_matrix does it for you), or switch the cache off with
- *     spops_b200::set_cache(false) to upload on every call as the reference
- *     reads on every call.
+ *   - Work runs on the GPU.  By default (CacheMode::Pattern) the first
+ *     SpOps_csr call on a CSR struct uploads it and keeps the device copy of
+ *     its pattern (row_offset, col_index and the analysis) keyed by the
+ *     struct's first array pointer; every call then re-reads A.values from
+ *     the host, as the reference reads its arrays on every call, so values
+ *     changed in place are always seen.  Other formats are uploaded on every
+ *     call.  CacheMode::All (set_cache(true)) keeps whole device copies of
+ *     every format and moves only x and y: after changing a struct's arrays
+ *     in place, call spops_b200::invalidate(ptr) (delete_host_matrix does it
+ *     for you).  CacheMode::Off (set_cache(false)) uploads everything on
+ *     every call.  A CSR pattern changed in place (same pointers and sizes)
+ *     still needs invalidate(ptr) under the default mode.
  *   - Conversions run on the device; the returned host structs hold the
  *     reference's layouts (row-major chunks, reorder, chunk_len, ...) and the
  *     device copy used by SpOps_<fmt> keeps the device-native layout.
@@ -225,10 +230,12 @@ struct Entry {
   int64_t rows = 0, cols = 0, nnz = 0;
 };
 
+enum class CacheModeImpl { Off, Pattern, All };
+
 struct State {
   std::mutex mu;
   int device = 0;
-  bool cache = true;
+  CacheModeImpl cache = CacheModeImpl::Pattern;
   spops_context_t ctx = nullptr;
   std::unordered_map<const void*, Entry> handles;
 };
@@ -312,16 +319,20 @@ inline void put(const void* key, spops_matrix_t h, int64_t rows, int64_t cols, i
   s.handles[key] = Entry{h, rows, cols, nnz};
 }
 
-inline bool caching() { return state().cache; }
+// whole device copies of any format are kept between calls
+inline bool caching() { return state().cache == CacheModeImpl::All; }
+// CSR device copies are kept (their values re-read from the host per call
+// unless caching() holds)
+inline bool caching_csr() { return state().cache != CacheModeImpl::Off; }
 
 // run y = alpha*A*x + beta*y with host vectors on handle h.  A handle this
-// call created (fresh) is cached under `key`, or destroyed when the cache is
-// off; a handle found in the cache stays there.
+// call created (fresh) is cached under `key` when `keep`, or destroyed; a
+// handle found in the cache stays there.
 inline void spmv_host(spops_matrix_t h, bool fresh, const void* key, double alpha, const void* x, double beta,
-                      void* y, const char* what, int64_t rows, int64_t cols, int64_t nnz) {
+                      void* y, const char* what, int64_t rows, int64_t cols, int64_t nnz, bool keep) {
   spops_status_t s = spops_spmv_host(ctx(), alpha, h, x, beta, y);
   if (fresh) {
-    if (caching()) put(key, h, rows, cols, nnz); else spops_matrix_destroy(h);
+    if (keep) put(key, h, rows, cols, nnz); else spops_matrix_destroy(h);
   }
   check(s, what);
 }
@@ -409,8 +420,26 @@ inline std::vector<T> join_chunks(T* const* parts, const I* len, int64_t nchunks
 
 /* Device used by the calls below (before the first call). */
 inline void set_device(int device) { detail::state().device = device; }
-/* Keep device copies of matrices between calls (default) or upload on every call. */
-inline void set_cache(bool on) { detail::state().cache = on; }
+/* What the SpOps_<fmt> calls keep on the device between calls:
+ *   Off      nothing: every call uploads the struct (the reference's per-call read);
+ *   Pattern  (default) CSR patterns and their analysis; A.values re-read from
+ *            the host on every call; other formats uploaded on every call;
+ *   All      whole device copies of every format; only x and y move.  Host
+ *            arrays changed in place need invalidate(ptr). */
+enum class CacheMode { Off, Pattern, All };
+inline void set_cache_mode(CacheMode m) {
+  detail::state().cache = m == CacheMode::Off ? detail::CacheModeImpl::Off
+                          : m == CacheMode::All ? detail::CacheModeImpl::All
+                                                : detail::CacheModeImpl::Pattern;
+}
+inline CacheMode cache_mode() {
+  const detail::CacheModeImpl m = detail::state().cache;
+  return m == detail::CacheModeImpl::Off ? CacheMode::Off
+         : m == detail::CacheModeImpl::All ? CacheMode::All
+                                           : CacheMode::Pattern;
+}
+/* set_cache(true): CacheMode::All; set_cache(false): CacheMode::Off. */
+inline void set_cache(bool on) { set_cache_mode(on ? CacheMode::All : CacheMode::Off); }
 /* Drop the device copy of the matrix whose first array is `key` (e.g.
  * A.row_offset, coo.row_index, sell.reorder) after changing it in place. */
 inline void invalidate(const void* key) { detail::release(key); }
@@ -422,30 +451,33 @@ template <typename IndexType, typename ValueType>
 void SpOps_csr(const ValueType alpha, const CSR_Matrix<IndexType, ValueType>& A, const ValueType* x,
                const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.row_offset, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = d::caching_csr() ? d::find(A.row_offset, A.num_rows, A.num_cols, A.num_nnzs) : nullptr;
   const bool fresh = h == nullptr;
   if (!h) h = d::upload_csr(A);
-  d::spmv_host(h, fresh, A.row_offset, alpha, x, beta, y, "SpOps_csr", A.num_rows, A.num_cols, A.num_nnzs);
+  else if (!d::caching()) d::check(spops_csr_upload_values(d::ctx(), h, A.values), "spops_csr_upload_values");
+  d::spmv_host(h, fresh, A.row_offset, alpha, x, beta, y, "SpOps_csr", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching_csr());
 }
 
 template <typename IndexType, typename ValueType>
 void SpOps_coo(const ValueType alpha, const COO_Matrix<IndexType, ValueType>& A, const ValueType* x,
                const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.row_index, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.row_index, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h)
     d::check(spops_coo_create(d::ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.row_index, A.col_index, A.values,
                               d::itype<IndexType>(), d::vtype<ValueType>(), SPOPS_MEM_HOST),
              "spops_coo_create");
-  d::spmv_host(h, fresh, A.row_index, alpha, x, beta, y, "SpOps_coo", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.row_index, alpha, x, beta, y, "SpOps_coo", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename ValueType>
 void SpOps_ell(const ValueType alpha, const ELL_Matrix<IndexType, ValueType>& A, const ValueType* x,
                const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.col_index, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.col_index, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h) {
     const IndexType w = A.max_row_width;
@@ -456,14 +488,15 @@ void SpOps_ell(const ValueType alpha, const ELL_Matrix<IndexType, ValueType>& A,
                                  SPOPS_MEM_HOST),
              "spops_padded_create");
   }
-  d::spmv_host(h, fresh, A.col_index, alpha, x, beta, y, "SpOps_ell", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.col_index, alpha, x, beta, y, "SpOps_ell", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename ValueType>
 void SpOps_sell(const ValueType alpha, const S_ELL_Matrix<IndexType, ValueType>& A, const ValueType* x,
                 const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.row_width, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.row_width, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h) {
     const std::vector<IndexType> col = d::join_chunks(A.col_index, A.row_width, A.chunk_num, A.sliceWidth);
@@ -474,14 +507,15 @@ void SpOps_sell(const ValueType alpha, const S_ELL_Matrix<IndexType, ValueType>&
                                  SPOPS_MEM_HOST),
              "spops_padded_create");
   }
-  d::spmv_host(h, fresh, A.row_width, alpha, x, beta, y, "SpOps_sell", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.row_width, alpha, x, beta, y, "SpOps_sell", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename ValueType>
 void SpOps_sell_c_sigma(const ValueType alpha, const SELL_C_Sigma_Matrix<IndexType, ValueType>& A, const ValueType* x,
                         const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.reorder, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.reorder, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h) {
     const std::vector<IndexType> col = d::join_chunks(A.col_index, A.chunk_len, A.validchunkNum, A.chunkWidth_C);
@@ -492,14 +526,15 @@ void SpOps_sell_c_sigma(const ValueType alpha, const SELL_C_Sigma_Matrix<IndexTy
                                  d::itype<IndexType>(), d::vtype<ValueType>(), SPOPS_MEM_HOST),
              "spops_padded_create");
   }
-  d::spmv_host(h, fresh, A.reorder, alpha, x, beta, y, "SpOps_sell_c_sigma", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.reorder, alpha, x, beta, y, "SpOps_sell_c_sigma", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename ValueType>
 void SpOps_sell_c_R(const ValueType alpha, const SELL_C_R_Matrix<IndexType, ValueType>& A, const ValueType* x,
                     const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.reorder, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.reorder, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h) {
     const std::vector<IndexType> col = d::join_chunks(A.col_index, A.chunk_len, A.validchunkNum, A.chunkWidth_C);
@@ -510,7 +545,8 @@ void SpOps_sell_c_R(const ValueType alpha, const SELL_C_R_Matrix<IndexType, Valu
                                  d::vtype<ValueType>(), SPOPS_MEM_HOST),
              "spops_padded_create");
   }
-  d::spmv_host(h, fresh, A.reorder, alpha, x, beta, y, "SpOps_sell_c_R", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.reorder, alpha, x, beta, y, "SpOps_sell_c_R", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename ValueType>
@@ -518,35 +554,37 @@ void SpOps_dia(const ValueType alpha, const DIA_Matrix<IndexType, ValueType>& A,
                const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
   static_assert(sizeof(long int) == 8, "diag_offsets must be 64-bit");
-  spops_matrix_t h = d::find(A.diag_offsets, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.diag_offsets, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h)
     d::check(spops_dia_create(d::ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.complete_ndiags, A.stride,
                               reinterpret_cast<const int64_t*>(A.diag_offsets), A.diag_data, d::vtype<ValueType>(),
                               SPOPS_MEM_HOST),
              "spops_dia_create");
-  d::spmv_host(h, fresh, A.diag_offsets, alpha, x, beta, y, "SpOps_dia", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.diag_offsets, alpha, x, beta, y, "SpOps_dia", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename ValueType>
 void SpOps_bsr(const ValueType alpha, const BSR_Matrix<IndexType, ValueType>& A, const ValueType* x,
                const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.row_ptr, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.row_ptr, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h)
     d::check(spops_bsr_create(d::ctx(), &h, A.num_rows, A.num_cols, A.num_nnzs, A.blockDim_r, A.blockDim_c, A.nnzb,
                               A.row_ptr, A.block_colindex, A.block_data, d::itype<IndexType>(), d::vtype<ValueType>(),
                               SPOPS_MEM_HOST),
              "spops_bsr_create");
-  d::spmv_host(h, fresh, A.row_ptr, alpha, x, beta, y, "SpOps_bsr", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.row_ptr, alpha, x, beta, y, "SpOps_bsr", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 template <typename IndexType, typename UIndexType, typename ValueType>
 void SpOps_csr5(const ValueType alpha, const CSR5_Matrix<IndexType, UIndexType, ValueType>& A, const ValueType* x,
                 const ValueType beta, ValueType* y) {
   namespace d = spops_b200::detail;
-  spops_matrix_t h = d::find(A.tile_ptr, A.num_rows, A.num_cols, A.num_nnzs);
+  spops_matrix_t h = !d::caching() ? nullptr : d::find(A.tile_ptr, A.num_rows, A.num_cols, A.num_nnzs);
   const bool fresh = h == nullptr;
   if (!h) {  // rebuild the device tiles from the CSR arrays the struct carries
     spops_matrix_t c = d::upload_csr(static_cast<const CSR_Matrix<IndexType, ValueType>&>(A));
@@ -556,7 +594,8 @@ void SpOps_csr5(const ValueType alpha, const CSR5_Matrix<IndexType, UIndexType, 
     spops_matrix_destroy(c);
     d::check(s, "spops_convert");
   }
-  d::spmv_host(h, fresh, A.tile_ptr, alpha, x, beta, y, "SpOps_csr5", A.num_rows, A.num_cols, A.num_nnzs);
+  d::spmv_host(h, fresh, A.tile_ptr, alpha, x, beta, y, "SpOps_csr5", A.num_rows, A.num_cols, A.num_nnzs,
+               d::caching());
 }
 
 /* ---------------------------------------------------------- conversions */
@@ -576,7 +615,7 @@ CSR_Matrix<IndexType, ValueType> coo_to_csr(const COO_Matrix<IndexType, ValueTyp
   csr.row_offset = d::fetch<IndexType>(h, SPOPS_ARR_ROW, nullptr);
   csr.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
   csr.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
-  if (d::caching()) d::put(csr.row_offset, h, i.rows, i.cols, i.nnz); else spops_matrix_destroy(h);
+  if (d::caching_csr()) d::put(csr.row_offset, h, i.rows, i.cols, i.nnz); else spops_matrix_destroy(h);
   return csr;
 }
 
@@ -1046,7 +1085,7 @@ CSR_Matrix<IndexType, ValueType> read_csr_matrix(const char* mm_filename, bool c
   csr.row_offset = d::fetch<IndexType>(h, SPOPS_ARR_ROW, nullptr);
   csr.col_index = d::fetch<IndexType>(h, SPOPS_ARR_COL, nullptr);
   csr.values = d::fetch<ValueType>(h, SPOPS_ARR_VAL, nullptr);
-  if (d::caching()) d::put(csr.row_offset, h, i.rows, i.cols, i.nnz); else spops_matrix_destroy(h);
+  if (d::caching_csr()) d::put(csr.row_offset, h, i.rows, i.cols, i.nnz); else spops_matrix_destroy(h);
   return csr;
 }
 
@@ -1230,10 +1269,10 @@ void sum_csr_duplicates(const IndexType num_rows, const IndexType num_cols, Inde
   coo.row_index = rows.data();
   coo.col_index = col_index;
   coo.values = values;
-  const bool was = spops_b200::detail::caching();
-  spops_b200::set_cache(false);  // the result is copied out, nothing to keep
+  const spops_b200::CacheMode was = spops_b200::cache_mode();
+  spops_b200::set_cache_mode(spops_b200::CacheMode::Off);  // the result is copied out, nothing to keep
   CSR_Matrix<IndexType, ValueType> c = coo_to_csr(coo, true);
-  spops_b200::set_cache(was);
+  spops_b200::set_cache_mode(was);
   std::memcpy(row_ptr, c.row_offset, sizeof(IndexType) * ((size_t)num_rows + 1));
   std::memcpy(col_index, c.col_index, sizeof(IndexType) * (size_t)c.num_nnzs);
   std::memcpy(values, c.values, sizeof(ValueType) * (size_t)c.num_nnzs);
@@ -1444,20 +1483,29 @@ CSR_Matrix<IndexType, ValueType> vlength_cluster2csr(const CSR_VlengthCluster<In
   return csr;
 }
 
-/* LeSpGEMM_VLength (spgemm.h:175-180): C = A * B with A clustered, kernel-3
- * rules on the device for every kernel_flag; C in A's clusters (allocated
- * here, columns ascending).  The caller's acc_flag / min_ccol / max_ccol, if
- * any, are left untouched. */
+/* LeSpGEMM_VLength (spgemm.h:175-180; src/spgemm.cpp:661-680): C = A * B
+ * with A clustered; C in A's clusters (allocated here, columns ascending).
+ * kernel_flag picks the reference kernel whose output rules C follows:
+ *   3  mixed accumulator (spgemm_Vlength_mixed.cpp): dense clusters by the
+ *      L2 rule; all-below-1e-12 columns dropped on the dense and sorted paths;
+ *   2  array accumulator (spgemm_Vlength_array.cpp): every structural column
+ *      kept, whatever sortOutput says;
+ *   1 and any other value  hash accumulator (spgemm_Vlength_hash.cpp): no
+ *      dense clusters; all-below-1e-12 columns dropped when sortOutput.
+ * The device computes all three with the same hash/dense kernels; only the
+ * dense budget and the drop rule differ.  The caller's acc_flag / min_ccol /
+ * max_ccol, if any, are left untouched. */
 template <bool sortOutput = true, typename IndexType, typename ValueType>
 void LeSpGEMM_VLength(const CSR_VlengthCluster<IndexType, ValueType>& A_cluster,
                       const CSR_Matrix<IndexType, ValueType>& B, CSR_VlengthCluster<IndexType, ValueType>& C_cluster,
                       int kernel_flag = 1, double mixed_l2_fraction = -1.0) {
   namespace d = spops_b200::detail;
-  (void)kernel_flag;
   const double frac = mixed_l2_fraction < 0 ? MIXED_L2_FRACTION : mixed_l2_fraction;
+  // a negative budget makes no cluster dense (the hash and array kernels)
+  const double budget = kernel_flag == 3 ? (double)CPU_L2CACHE_SIZE * frac : -1.0;
+  const int32_t drop_sorted = (kernel_flag == 2) ? 0 : (sortOutput ? 1 : 0);
   spops_matrix_t a = d::upload_vlcluster(A_cluster), b = d::upload_csr(B), c = nullptr;
-  spops_status_t s = spops_spgemm_vlength(d::ctx(), a, b, sortOutput ? 1 : 0, (double)CPU_L2CACHE_SIZE * frac, &c,
-                                          nullptr);
+  spops_status_t s = spops_spgemm_vlength(d::ctx(), a, b, drop_sorted, budget, &c, nullptr);
   spops_matrix_destroy(a);
   spops_matrix_destroy(b);
   d::check(s, "spops_spgemm_vlength");

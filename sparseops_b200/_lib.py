@@ -129,6 +129,7 @@ _SIGS = {
     "spops_matrix_array": [vp, C.c_int, vp, vp, vp],
     "spops_matrix_download": [vp, vp, C.c_int, vp, i64],
     "spops_csr_set_values": [vp, vp],
+    "spops_csr_upload_values": [vp, vp, vp],
     "spops_spmv_t": [vp, dbl, vp, vp, dbl, vp],
     "spops_sddmm": [vp, dbl, vp, vp, vp, vp],
     "spops_spmm": [vp, dbl, vp, vp, i64, i64, dbl, vp, i64],

@@ -389,6 +389,20 @@ spops_status_t spops_csr_set_values(spops_matrix_t A, const void* values) {
   return SPOPS_OK;
 }
 
+spops_status_t spops_csr_upload_values(spops_context_t ctx, spops_matrix_t A, const void* host_values) {
+  if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_csr_upload_values: null context/matrix");
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "spops_csr_upload_values: not a CSR matrix");
+  if (!A->val.own) return fail(SPOPS_ERR_INVALID, "spops_csr_upload_values: the handle borrows its values");
+  if (A->nnz == 0) return SPOPS_OK;
+  if (!host_values) return fail(SPOPS_ERR_INVALID, "spops_csr_upload_values: null values");
+  DeviceGuard g(ctx->device);
+  SPOPS_CUDA(cudaMemcpyAsync(A->val.p, host_values, (size_t)A->nnz * A->vsize(), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  A->tr.values_fresh = false;
+  A->plan.win.values_fresh = false;
+  return SPOPS_OK;
+}
+
 spops_status_t spops_spmv_t(spops_context_t ctx, double alpha, spops_matrix_t A, const void* x, double beta,
                             void* y) {
   if (!ctx || !A) return fail(SPOPS_ERR_INVALID, "spops_spmv_t: null context/matrix");

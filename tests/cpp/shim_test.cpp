@@ -92,6 +92,21 @@ void run_all() {
   };
   run("SpOps_csr", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
   run("SpOps_csr again (cached)", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+  // values changed in place between calls: the default cache mode keeps the
+  // pattern on the device but re-reads A.values, as the reference does
+  {
+    std::vector<V> saved(A.values, A.values + A.num_nnzs);
+    for (I k = 0; k < A.num_nnzs; ++k) A.values[k] = (V)(-2.5 * (double)A.values[k] + 0.125 * (double)(k % 7));
+    run("SpOps_csr after an in-place value edit", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+    spops_b200::set_cache(true);  // whole device copies: an edit needs invalidate()
+    spops_b200::invalidate(A.row_offset);
+    run("SpOps_csr, full cache", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+    std::copy(saved.begin(), saved.end(), A.values);
+    spops_b200::invalidate(A.row_offset);
+    run("SpOps_csr, full cache after invalidate", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
+    spops_b200::set_cache_mode(spops_b200::CacheMode::Pattern);
+    EXPECT(spops_b200::cache_mode() == spops_b200::CacheMode::Pattern, "cache mode back to the default");
+  }
 
   // COO both ways
   COO_Matrix<I, V> coo = csr_to_coo(A);
@@ -466,6 +481,22 @@ void api_checks() {
     for (int k = 0; same && k < c1.num_nnzs; ++k)
       same = c1.col_index[k] == c2.col_index[k] && std::fabs(c1.values[k] - c2.values[k]) <= 1e-12 * (1 + std::fabs(c2.values[k]));
     EXPECT(same, "LeSpGEMM_VLength = row-wise LeSpGEMM");
+    // kernel 2 (array accumulator) keeps every structural column: the same C
+    // as the row-wise product; kernel 1 (hash, sorted) the same again here
+    for (int kf : {1, 2}) {
+      CSR_VlengthCluster<int, double> ck;
+      std::memset(static_cast<void*>(&ck), 0, sizeof(ck));
+      LeSpGEMM_VLength<true>(acl, t, ck, kf);
+      CSR_Matrix<int, double> c3 = vlength_cluster2csr(ck);
+      bool same_k = c3.num_rows == c2.num_rows && c3.num_nnzs == c2.num_nnzs;
+      for (int r = 0; same_k && r <= n; ++r) same_k = c3.row_offset[r] == c2.row_offset[r];
+      for (int k = 0; same_k && k < c3.num_nnzs; ++k)
+        same_k = c3.col_index[k] == c2.col_index[k] &&
+                 std::fabs(c3.values[k] - c2.values[k]) <= 1e-12 * (1 + std::fabs(c2.values[k]));
+      EXPECT(same_k, kf == 1 ? "LeSpGEMM_VLength kernel 1 = row-wise" : "LeSpGEMM_VLength kernel 2 = row-wise");
+      delete_host_matrix(ck);
+      delete_csr_matrix(c3);
+    }
     delete_vlength_cluster_matrix(acl);
     delete_host_matrix(ccl);
     delete_csr_matrix(c1);
