@@ -92,6 +92,11 @@ def workload(rows=N_ROWS):
     return rp, ci, v, x
 
 
+def workload_name(n):
+    """The same string in both arms' config."""
+    return f"powerlaw CSR SpMV FP64 n={n} (lognormal ln12,1.2 clip [1,20000]; seed 1)"
+
+
 def spmv_bytes(n_rows, n_cols, nnz, isz=4, vsz=8):
     return isz * (n_rows + 1) + (isz + vsz) * nnz + vsz * n_cols + vsz * n_rows
 
@@ -628,8 +633,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(gbs, 2), "unit": "GB/s", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"powerlaw CSR SpMV FP64 n={n} (lognormal ln12,1.2; seed 1)",
-                   "nnz": int(len(ci)), "kernel_flag": 2},
+        "config": {"workload": workload_name(n), "nnz": int(len(ci)), "kernel_flag": 2},
         "pct_of_peak": round(100 * gbs / peak, 2),
         "cpu_baseline": {"value": round(gbs, 2), "unit": "GB/s", "cores": threads, "kind": "reference",
                          "sample": sample},
@@ -849,7 +853,7 @@ def run_ours(args):
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"powerlaw CSR SpMV FP64 n={n} (lognormal ln12,1.2 clip [1,20000]; seed 1)",
+        "config": {"workload": workload_name(n),
                    "nnz": int(nnz), "algorithmic_bytes_per_step": int(nbytes),
                    "l2": "inputs larger than L2 (matrix ~1.3 GB vs 126 MB), no flush",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
