@@ -44,6 +44,7 @@
 #include <vector>
 
 #include "spops_internal.h"
+#include "spgemm_sort.cuh"
 
 namespace spops {
 namespace {
@@ -434,8 +435,8 @@ __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nl
                                     const int64_t* __restrict__ cptr_val, const int32_t* __restrict__ colids,
                                     const V* __restrict__ avals, const int64_t* __restrict__ offsets,
                                     const I* __restrict__ brp, const I* __restrict__ bci, const V* __restrict__ bv,
-                                    const int64_t* __restrict__ nz, const int64_t* __restrict__ ccptr,
-                                    const int64_t* __restrict__ ccptr_val, const unsigned char* __restrict__ drop_small,
+                                    const int64_t* __restrict__ nz, const int64_t* __restrict__ soff,
+                                    const int64_t* __restrict__ soff_val, const unsigned char* __restrict__ drop_small,
                                     int32_t* __restrict__ ccol, V* __restrict__ cval) {
   extern __shared__ __align__(16) unsigned char sm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -467,7 +468,7 @@ __global__ void numeric_warp_kernel(const int64_t* __restrict__ list, int64_t nl
   // 2. compact (slot order), pad to lsize, 3. bitonic sort; positions and
   //    the output column list in ascending order
   warp_sort_keys(tab, S.tsize, keys, S.lsize, lane);
-  const int64_t co = ccptr[c], cvo = ccptr_val[c];
+  const int64_t co = soff[c], cvo = soff_val[c];
   for (int64_t p = lane; p < nzc; p += 32) {
     pos[hash_find(tab, mask, keys[p])] = (int32_t)p;
     ccol[co + p] = keys[p];
@@ -532,8 +533,8 @@ __global__ void numeric_warp_wide_kernel(const int64_t* __restrict__ list, int64
                                          const int32_t* __restrict__ colids, const V* __restrict__ avals,
                                          const int64_t* __restrict__ offsets, const I* __restrict__ brp,
                                          const I* __restrict__ bci, const V* __restrict__ bv,
-                                         const int64_t* __restrict__ nz, const int64_t* __restrict__ ccptr,
-                                         const int64_t* __restrict__ ccptr_val,
+                                         const int64_t* __restrict__ nz, const int64_t* __restrict__ soff,
+                                         const int64_t* __restrict__ soff_val,
                                          const unsigned char* __restrict__ drop_small, int32_t* __restrict__ ccol,
                                          V* __restrict__ cval) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -605,7 +606,7 @@ __global__ void numeric_warp_wide_kernel(const int64_t* __restrict__ list, int64
   // 2. compact (slot order), pad to lsize, bitonic sort ascending
   warp_sort_keys(tab, S.tsize, keys, S.lsize, lane);
   // 3. position of every column; the output column list
-  const int64_t co = ccptr[c], cvo = ccptr_val[c];
+  const int64_t co = soff[c], cvo = soff_val[c];
   for (int64_t p = lane; p < nzc; p += 32) {
     pos[hash_find(tab, mask, keys[p])] = (int32_t)p;
     ccol[co + p] = keys[p];
@@ -653,7 +654,7 @@ __global__ void numeric_kernel(const int64_t* __restrict__ list, int64_t nlist, 
                                const int32_t* __restrict__ colids, const V* __restrict__ avals,
                                const int64_t* __restrict__ offsets, const I* __restrict__ brp,
                                const I* __restrict__ bci, const V* __restrict__ bv, const int64_t* __restrict__ nz,
-                               const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
+                               const int64_t* __restrict__ soff, const int64_t* __restrict__ soff_val,
                                const unsigned char* __restrict__ drop_small, unsigned char* __restrict__ garena,
                                const int64_t* __restrict__ goff, int32_t* __restrict__ ccol, V* __restrict__ cval) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -721,7 +722,7 @@ __global__ void numeric_kernel(const int64_t* __restrict__ list, int64_t nlist, 
   }
   // 5. drop rule and output
   const bool drop = drop_small[c] != 0;
-  const int64_t co = ccptr[c], cvo = ccptr_val[c];
+  const int64_t co = soff[c], cvo = soff_val[c];
   for (int64_t p = threadIdx.x; p < nzc; p += blockDim.x) {
     ccol[co + p] = keys[p];
     bool small = drop;
@@ -735,10 +736,11 @@ __global__ void numeric_kernel(const int64_t* __restrict__ list, int64_t nlist, 
 __global__ void classify_kernel(const int64_t* __restrict__ cptr, const int64_t* __restrict__ offsets,
                                 const int64_t* __restrict__ nz, const int64_t* __restrict__ cmin,
                                 const int64_t* __restrict__ cmax, int64_t ncl, double b_rowdense, double budget,
-                                bool sort_output, size_t vbytes, size_t ibytes, unsigned char* __restrict__ drop,
+                                bool sort_output, size_t vbytes, size_t ibytes,
+                                const unsigned char* __restrict__ settled, unsigned char* __restrict__ drop,
                                 unsigned long long* __restrict__ ndense) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= ncl) return;
+  if (c >= ncl || settled[c]) return;  // the sort path classified it
   bool dense = false;
   if (nz[c] > 0) {
     const int64_t range = cmax[c] - cmin[c] + 1;
@@ -753,7 +755,7 @@ __global__ void classify_kernel(const int64_t* __restrict__ cptr, const int64_t*
 
 // ------------------------------------------------------------ to CSR
 template <typename V>
-__global__ void row_count_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
+__global__ void row_count_kernel(const int64_t* __restrict__ soff_val, const int64_t* __restrict__ nz,
                                  const int64_t* __restrict__ offsets, const int64_t* __restrict__ perm, int64_t ncl,
                                  const V* __restrict__ cval, bool keep_zeros, int64_t* __restrict__ rowcnt) {
   // warp per cluster, lanes over its rows (csz <= 32 common) and columns
@@ -761,35 +763,36 @@ __global__ void row_count_kernel(const int64_t* __restrict__ ccptr, const int64_
   const int lane = threadIdx.x & 31;
   if (c >= ncl) return;
   const int64_t csz = offsets[c + 1] - offsets[c];
-  const int64_t ncol = ccptr[c + 1] - ccptr[c];
+  const int64_t ncol = nz[c];
   for (int64_t l = 0; l < csz; ++l) {
     int64_t cnt = 0;
-    for (int64_t p = lane; p < ncol; p += 32) cnt += (keep_zeros || cval[ccptr_val[c] + p * csz + l] != V(0)) ? 1 : 0;
+    for (int64_t p = lane; p < ncol; p += 32) cnt += (keep_zeros || cval[soff_val[c] + p * csz + l] != V(0)) ? 1 : 0;
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
     if (lane == 0) rowcnt[perm[offsets[c] + l]] = cnt;
   }
 }
 
 template <typename I, typename V>
-__global__ void row_write_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
-                                 const int64_t* __restrict__ offsets, const int64_t* __restrict__ perm, int64_t ncl,
-                                 const int32_t* __restrict__ ccol, const V* __restrict__ cval, bool keep_zeros,
-                                 const int64_t* __restrict__ crp, I* __restrict__ oci, V* __restrict__ ov) {
+__global__ void row_write_kernel(const int64_t* __restrict__ soff, const int64_t* __restrict__ soff_val,
+                                 const int64_t* __restrict__ nz, const int64_t* __restrict__ offsets,
+                                 const int64_t* __restrict__ perm, int64_t ncl, const int32_t* __restrict__ ccol,
+                                 const V* __restrict__ cval, bool keep_zeros, const int64_t* __restrict__ crp,
+                                 I* __restrict__ oci, V* __restrict__ ov) {
   const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (c >= ncl) return;
   const int64_t csz = offsets[c + 1] - offsets[c];
-  const int64_t ncol = ccptr[c + 1] - ccptr[c];
+  const int64_t ncol = nz[c];
   for (int64_t l = 0; l < csz; ++l) {
     int64_t o = crp[perm[offsets[c] + l]];
     for (int64_t p0 = 0; p0 < ncol; p0 += 32) {
       const int64_t p = p0 + lane;
-      const V v = p < ncol ? cval[ccptr_val[c] + p * csz + l] : V(0);
+      const V v = p < ncol ? cval[soff_val[c] + p * csz + l] : V(0);
       const bool keep = p < ncol && (keep_zeros || v != V(0));
       const unsigned m = __ballot_sync(0xffffffffu, keep);
       if (keep) {
         const int64_t at = o + __popc(m & ((1u << lane) - 1));
-        oci[at] = (I)ccol[ccptr[c] + p];
+        oci[at] = (I)ccol[soff[c] + p];
         ov[at] = v;
       }
       o += __popc(m);
@@ -819,9 +822,16 @@ __global__ void weight_kernel(const int64_t* __restrict__ cnt, const int64_t* __
 // shared memory (smem0 / smem1 bytes), 3 block in global memory
 __global__ void sym_bin_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ cnt, int64_t ncl,
                                int64_t bcols, int64_t warp_tab, int64_t smem0, int64_t smem1,
-                               uint32_t* __restrict__ key, int64_t* __restrict__ ids, int64_t* __restrict__ tsz) {
+                               const unsigned char* __restrict__ settled, uint32_t* __restrict__ key,
+                               int64_t* __restrict__ ids, int64_t* __restrict__ tsz) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= ncl) return;
+  if (settled[c]) {  // the sort path counts its own columns
+    key[c] = kNoBin;
+    ids[c] = c;
+    tsz[c] = 0;
+    return;
+  }
   const int64_t f = flops[c] < bcols ? flops[c] : bcols;
   const int64_t ts = pow2_ceil(2 * f > 2 ? 2 * f : 2);
   uint32_t b;
@@ -844,12 +854,13 @@ struct NumBinLimits {
 
 __global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __restrict__ cnt,
                                const int64_t* __restrict__ offsets, int64_t ncl, int64_t vsize, NumBinLimits lim,
-                               uint32_t* __restrict__ key, int64_t* __restrict__ ids) {
+                               const unsigned char* __restrict__ settled, uint32_t* __restrict__ key,
+                               int64_t* __restrict__ ids) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= ncl) return;
   ids[c] = c;
   const int64_t z = nz[c];
-  if (z == 0) {
+  if (z == 0 || settled[c]) {
     key[c] = kNoBin;
     return;
   }
@@ -866,6 +877,50 @@ __global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __
     if (wide <= lim.wbytes[b]) { key[c] = b; return; }
   const int64_t bytes = ((accb + 15) & ~15LL) + 4 * (2 * tsize + lsize);
   key[c] = bytes <= lim.wbytes[5] ? 5 : (bytes <= lim.wbytes[6] ? 6 : 7);
+}
+
+// sort path (spgemm_sort.cuh): bin q (R = 2^q lanes' worth of keys, q = 0..5)
+// for a cluster with at most 32 * 2^q products and kSortCols columns whose
+// output columns fit the key beside the product index; settled[c] = 1 then.
+constexpr int kSortBins = 6;
+
+__global__ void sort_bin_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ cptr, int64_t ncl,
+                                int64_t bcols, unsigned char* __restrict__ settled, uint32_t* __restrict__ key,
+                                int64_t* __restrict__ ids) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= ncl) return;
+  ids[c] = c;
+  const int64_t P = flops[c], nj = cptr[c + 1] - cptr[c];
+  uint32_t b = kNoBin;
+  if (nj <= kSortCols) {
+    for (int q = 0; q < kSortBins; ++q) {
+      if (P <= (32LL << q)) {
+        const int tbits = 5 + q;
+        if (bcols <= (1LL << (32 - tbits)) - 1) b = (uint32_t)q;
+        break;
+      }
+    }
+  }
+  key[c] = b;
+  settled[c] = b != kNoBin ? 1 : 0;
+}
+
+// room in each cluster's output slab: its product count on the sort path (at
+// most 32 * 2^5, and never below its distinct columns whatever B holds), the
+// symbolic count otherwise; values: that times the cluster size
+__global__ void slab_cap_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ nz,
+                                const unsigned char* __restrict__ settled, const int64_t* __restrict__ offsets,
+                                int64_t ncl, int64_t* __restrict__ cap, int64_t* __restrict__ capv) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c > ncl) return;
+  if (c == ncl) {  // the scans' last slot
+    cap[c] = 0;
+    capv[c] = 0;
+    return;
+  }
+  const int64_t m = settled[c] ? flops[c] : nz[c];
+  cap[c] = m;
+  capv[c] = m * (offsets[c + 1] - offsets[c]);
 }
 
 __global__ void bin_bounds_kernel(const uint32_t* __restrict__ skey, int64_t ncl, int nb, int64_t* __restrict__ start) {
@@ -924,24 +979,6 @@ spops_status_t h2d(cudaStream_t st, PoolBuf& d, const std::vector<T>& h) {
   return SPOPS_OK;
 }
 
-// SPOPS_TRACE=1 in the environment: wall time of each step of the SpGEMM
-// driver on stderr (the stream is synchronised at every mark).
-struct Trace {
-  bool on = false;
-  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
-  Trace() {
-    const char* e = std::getenv("SPOPS_TRACE");
-    on = e && e[0] == '1';
-  }
-  void mark(cudaStream_t st, const char* what) {
-    if (!on) return;
-    cudaStreamSynchronize(st);
-    const auto n = std::chrono::steady_clock::now();
-    std::fprintf(stderr, "[spgemm] %-28s %9.3f ms\n", what, std::chrono::duration<double, std::milli>(n - t).count());
-    t = n;
-  }
-};
-
 struct Timer {
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
   double lap(cudaStream_t st) {
@@ -972,14 +1009,14 @@ __global__ void iota_kernel(int64_t* __restrict__ a, int64_t m) {
 // column whose values all came out as exactly 0 was dropped.  One warp per
 // cluster; kcnt[c] = kept columns.
 template <typename V>
-__global__ void cl_keep_count_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
+__global__ void cl_keep_count_kernel(const int64_t* __restrict__ soff_val, const int64_t* __restrict__ nz,
                                      const int64_t* __restrict__ offs, int64_t ncl, const V* __restrict__ cval,
                                      const unsigned char* __restrict__ drop, int64_t* __restrict__ kcnt,
                                      int64_t* __restrict__ kval) {
   const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (c >= ncl) return;
-  const int64_t csz = offs[c + 1] - offs[c], p0 = ccptr[c], np = ccptr[c + 1] - p0, v0 = ccptr_val[c];
+  const int64_t csz = offs[c + 1] - offs[c], np = nz[c], v0 = soff_val[c];
   const bool dr = drop[c] != 0;
   int64_t kept = 0;
   for (int64_t p = lane; p < np; p += 32) {
@@ -995,15 +1032,16 @@ __global__ void cl_keep_count_kernel(const int64_t* __restrict__ ccptr, const in
 }
 
 template <typename I, typename V>
-__global__ void cl_compact_kernel(const int64_t* __restrict__ ccptr, const int64_t* __restrict__ ccptr_val,
-                                  const int64_t* __restrict__ offs, int64_t ncl, const int32_t* __restrict__ ccol,
+__global__ void cl_compact_kernel(const int64_t* __restrict__ soff, const int64_t* __restrict__ soff_val,
+                                  const int64_t* __restrict__ nz, const int64_t* __restrict__ offs, int64_t ncl,
+                                  const int32_t* __restrict__ ccol,
                                   const V* __restrict__ cval, const unsigned char* __restrict__ drop,
                                   const int64_t* __restrict__ nrp, const int64_t* __restrict__ nrpv,
                                   I* __restrict__ colids, V* __restrict__ vals) {
   const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (c >= ncl) return;
-  const int64_t csz = offs[c + 1] - offs[c], p0 = ccptr[c], np = ccptr[c + 1] - p0, v0 = ccptr_val[c];
+  const int64_t csz = offs[c + 1] - offs[c], p0 = soff[c], np = nz[c], v0 = soff_val[c];
   const bool dr = drop[c] != 0;
   int64_t out = 0;  // kept columns before this batch
   for (int64_t b = 0; b < np; b += 32) {
@@ -1110,13 +1148,14 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   cudaStream_t st = ctx->stream;
   const int64_t n = A->rows, nnz = A->nnz;
   Timer tm;
-  Trace tr;
+  Trace tr("spgemm");
   // --- permutation, offsets, per-row cluster
   PoolBuf perm(ctx), offs(ctx), rowcl(ctx), rlen(ctx), rpr(ctx), keys(ctx), skeys(ctx), src(ctx), ssrc(ctx), flag(ctx), uidx(ctx), colids(ctx), ncols_u(ctx), cptr(ctx), cptr_val(ctx), avals(ctx), row_of_entry(ctx), tmp(ctx);
   SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(n, 1) * 8));
   SPOPS_TRY(offs.alloc((size_t)(ncl + 1) * 8));
-  SPOPS_CUDA(cudaMemcpyAsync(perm.p, perm_h, (size_t)n * 8, cudaMemcpyHostToDevice, st));
-  SPOPS_CUDA(cudaMemcpyAsync(offs.p, offs_h, (size_t)(ncl + 1) * 8, cudaMemcpyHostToDevice, st));
+  // host or device arrays (the device clustering hands over device ones)
+  SPOPS_CUDA(cudaMemcpyAsync(perm.p, perm_h, (size_t)n * 8, cudaMemcpyDefault, st));
+  SPOPS_CUDA(cudaMemcpyAsync(offs.p, offs_h, (size_t)(ncl + 1) * 8, cudaMemcpyDefault, st));
   const size_t nn = (size_t)std::max<int64_t>(n, 1), nz1 = (size_t)std::max<int64_t>(nnz, 1);
   SPOPS_TRY(rowcl.alloc(nn * 8));
   SPOPS_TRY(rlen.alloc(nn * 8));
@@ -1278,9 +1317,29 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   };
   tr.mark(st, "flops per cluster");
 
-  // --- symbolic: 0 warp per cluster (<= 32 A columns, table <= kSymWarpTab),
-  // 1 / 2 block with the table in 16 KB / 128 KB of shared memory, 3 global
+  // --- sort path: which clusters the one-warp sort-accumulate kernels take
+  // (their list kept apart: the bin buffers are reused below)
   const int64_t bcols = B->cols;
+  PoolBuf settled(ctx), slist(ctx);
+  SPOPS_TRY(settled.alloc(ncl1));
+  SPOPS_CUDA(cudaMemsetAsync(settled.p, 0, ncl1, st));
+  std::vector<int64_t> tstart((size_t)kSortBins + 1, 0);
+  if (ncl > 0) {
+    sort_bin_kernel<<<grid_for(ncl), 256, 0, st>>>(flops.as<int64_t>(), cptr.as<int64_t>(), ncl, bcols,
+                                                  settled.as<unsigned char>(), bkey.as<uint32_t>(),
+                                                  bid.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_TRY(sort_bins(kSortBins, tstart));
+  }
+  const int64_t nsorted = tstart[kSortBins];
+  SPOPS_TRY(slist.alloc((size_t)std::max<int64_t>(nsorted, 1) * 8));
+  if (nsorted > 0)
+    SPOPS_CUDA(cudaMemcpyAsync(slist.p, bid_s.p, (size_t)nsorted * 8, cudaMemcpyDeviceToDevice, st));
+  tr.mark(st, "sort-path bins");
+
+  // --- symbolic for the other clusters: 0 warp per cluster (<= 32 A
+  // columns, table <= kSymWarpTab), 1 / 2 block with the table in 16 KB /
+  // 128 KB of shared memory, 3 global
   constexpr int kSymWarps = 8;
   constexpr int64_t kSymWarpTab = 2048;
   const int sym_threads[4] = {32 * kSymWarps, 32, 256, 256};
@@ -1289,15 +1348,14 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(tszc.alloc(ncl1 * 8));
   SPOPS_TRY(ltsz.alloc(ncl1 * 8));
   SPOPS_TRY(sgoff.alloc(ncl1 * 8));
-  std::vector<int64_t> sstart;
-  if (ncl > 0) {
+  std::vector<int64_t> sstart(5, 0);
+  if (ncl > nsorted) {
     sym_bin_kernel<<<grid_for(ncl), 256, 0, st>>>(flops.as<int64_t>(), cnt_d, ncl, bcols, kSymWarpTab,
-                                                 (int64_t)sym_smem[1], (int64_t)sym_smem[2], bkey.as<uint32_t>(),
-                                                 bid.as<int64_t>(), tszc.as<int64_t>());
+                                                 (int64_t)sym_smem[1], (int64_t)sym_smem[2],
+                                                 settled.as<unsigned char>(), bkey.as<uint32_t>(), bid.as<int64_t>(),
+                                                 tszc.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
-  }
-  SPOPS_TRY(sort_bins(4, sstart));
-  if (ncl > 0) {
+    SPOPS_TRY(sort_bins(4, sstart));
     sym_list_kernel<<<grid_for(ncl), 256, 0, st>>>(bid_s.as<int64_t>(), tszc.as<int64_t>(), ncl, ltsz.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
   }
@@ -1328,57 +1386,87 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     }
     SPOPS_LAUNCH_CHECK();
   }
-  // output cluster pointers: exclusive scans of nz, plain and weighted
-  PoolBuf ccptr(ctx), ccptr_val(ctx), ccol(ctx), cval(ctx);
-  SPOPS_TRY(ccptr.alloc((size_t)(ncl + 1) * 8));
-  SPOPS_TRY(ccptr_val.alloc((size_t)(ncl + 1) * 8));
-  SPOPS_CUDA(cudaMemsetAsync(cw.p, 0, (size_t)(ncl + 1) * 8, st));
-  if (ncl > 0) {
-    weight_kernel<<<grid_for(ncl), 256, 0, st>>>(nzd.as<int64_t>(), offs.as<int64_t>(), ncl, cw.as<int64_t>());
-    SPOPS_LAUNCH_CHECK();
-  }
-  int64_t c_cols = 0, c_vals = 0;
+  gtab.release();
+  // output slabs: per cluster room for its columns (exact for the hash
+  // path, its product count for the sort path) and values
+  PoolBuf soff(ctx), soff_val(ctx), ccol(ctx), cval(ctx);
+  SPOPS_TRY(soff.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(soff_val.alloc((size_t)(ncl + 1) * 8));
+  PoolBuf capc(ctx), capv(ctx);
+  SPOPS_TRY(capc.alloc((size_t)(ncl + 1) * 8));
+  SPOPS_TRY(capv.alloc((size_t)(ncl + 1) * 8));
+  slab_cap_kernel<<<grid_for(ncl + 1), 256, 0, st>>>(flops.as<int64_t>(), nzd.as<int64_t>(),
+                                                     settled.as<unsigned char>(), offs.as<int64_t>(), ncl,
+                                                     capc.as<int64_t>(), capv.as<int64_t>());
+  SPOPS_LAUNCH_CHECK();
+  int64_t slab_cols = 0, slab_vals = 0;
   {
     size_t c1 = 0, c2 = 0;
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c1, nzd.as<int64_t>(), ccptr.as<int64_t>(), ncl + 1, st));
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c2, cw.as<int64_t>(), ccptr_val.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c1, capc.as<int64_t>(), soff.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c2, capv.as<int64_t>(), soff_val.as<int64_t>(), ncl + 1, st));
     SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, nzd.as<int64_t>(), ccptr.as<int64_t>(), ncl + 1, st));
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c2, cw.as<int64_t>(), ccptr_val.as<int64_t>(), ncl + 1, st));
-    SPOPS_CUDA(cudaMemcpyAsync(&c_cols, ccptr.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
-    SPOPS_CUDA(cudaMemcpyAsync(&c_vals, ccptr_val.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c1, capc.as<int64_t>(), soff.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, c2, capv.as<int64_t>(), soff_val.as<int64_t>(), ncl + 1, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&slab_cols, soff.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&slab_vals, soff_val.as<int64_t>() + ncl, 8, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
   }
-  gtab.release();
+  capc.release();
+  capv.release();
+  SPOPS_TRY(ccol.alloc((size_t)std::max<int64_t>(slab_cols, 1) * 4));
+  SPOPS_TRY(cval.alloc((size_t)std::max<int64_t>(slab_vals, 1) * sizeof(V)));
   if (stats) stats->symbolic_ms = tm.lap(st);
-  tr.mark(st, "symbolic kernels + nz scans");
+  tr.mark(st, "symbolic kernels + slab offsets");
 
-  // --- classify (drop rule)
+  // --- sort path: columns, classification and values in one pass
   PoolBuf drop(ctx), ndense(ctx);
   SPOPS_TRY(drop.alloc(ncl1));
   SPOPS_TRY(ndense.alloc(8));
   SPOPS_CUDA(cudaMemsetAsync(ndense.p, 0, 8, st));
+  if (rowwise) SPOPS_CUDA(cudaMemsetAsync(drop.p, 0, ncl1, st));
   const double b_rowdense = (double)B->nnz / (double)std::max<int64_t>(B->rows, 1);
-  if (rowwise) {
-    SPOPS_CUDA(cudaMemsetAsync(drop.p, 0, ncl1, st));
-  } else if (ncl > 0) {
+  for (int q = 0; q < kSortBins; ++q) {
+    const int64_t m = tstart[q + 1] - tstart[q];
+    if (m <= 0) continue;
+    const unsigned grid = (unsigned)((m + kSortWarps - 1) / kSortWarps);
+    const int64_t* dl = slist.as<int64_t>() + tstart[q];
+    const int tbits = 5 + q;
+#define SPOPS_SORT_LAUNCH(RR)                                                                                    \
+  sort_accum_kernel<I, V, RR><<<grid, 32 * kSortWarps, 0, st>>>(                                                \
+      dl, m, cptr.as<int64_t>(), cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), \
+      B->row.as<I>(), B->col.as<I>(), B->val.as<V>(), tbits, b_rowdense, l2_budget, sort_output, rowwise,        \
+      soff.as<int64_t>(), soff_val.as<int64_t>(), nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>(),      \
+      drop.as<unsigned char>(), reinterpret_cast<unsigned long long*>(ndense.p), ccol.as<int32_t>(), cval.as<V>())
+    switch (q) {
+      case 0: SPOPS_SORT_LAUNCH(1); break;
+      case 1: SPOPS_SORT_LAUNCH(2); break;
+      case 2: SPOPS_SORT_LAUNCH(4); break;
+      case 3: SPOPS_SORT_LAUNCH(8); break;
+      case 4: SPOPS_SORT_LAUNCH(16); break;
+      default: SPOPS_SORT_LAUNCH(32); break;
+    }
+#undef SPOPS_SORT_LAUNCH
+    SPOPS_LAUNCH_CHECK();
+  }
+  tr.mark(st, "sort-path kernels");
+
+  // --- classify the other clusters (drop rule)
+  if (!rowwise && ncl > nsorted) {
     classify_kernel<<<grid_for(ncl), 256, 0, st>>>(cptr.as<int64_t>(), offs.as<int64_t>(), nzd.as<int64_t>(),
                                                    cmin.as<int64_t>(), cmax.as<int64_t>(), ncl, b_rowdense, l2_budget,
-                                                   sort_output, sizeof(V), sizeof(int64_t), drop.as<unsigned char>(),
+                                                   sort_output, sizeof(V), sizeof(int64_t),
+                                                   settled.as<unsigned char>(), drop.as<unsigned char>(),
                                                    reinterpret_cast<unsigned long long*>(ndense.p));
     SPOPS_LAUNCH_CHECK();
   }
-  int64_t hdense = 0;
-  SPOPS_CUDA(cudaMemcpyAsync(&hdense, ndense.p, 8, cudaMemcpyDeviceToHost, st));
-  SPOPS_TRY(ccol.alloc((size_t)std::max<int64_t>(c_cols, 1) * 4));
-  SPOPS_TRY(cval.alloc((size_t)std::max<int64_t>(c_vals, 1) * sizeof(V)));
-  tr.mark(st, "classify + cluster output alloc");
+  tr.mark(st, "classify");
 
   // --- numeric bins: 0 / 1 warp per cluster (8 KB arena, 8 warps / 16 KB, 4
   // warps), 2 / 3 / 4 wide warp per cluster (16 KB, 2 warps / 32 KB, 1 warp /
   // 56 KB, 1 warp: small blocks so that the SM's shared memory fills), 5 / 6
   // block with the arena in 96 / 200 KB of shared memory, 7 block with the
-  // arena in global memory; clusters with nz == 0 are skipped
+  // arena in global memory; clusters with nz == 0 and those the sort path
+  // settled are skipped
   constexpr int kWarpBins = 5;
   const int64_t warp_bytes[kWarpBins] = {8 << 10, 16 << 10, 16 << 10, 32 << 10, 56 << 10};
   const int warp_count[kWarpBins] = {8, 4, 2, 1, 1};
@@ -1390,13 +1478,14 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(nslots.alloc(ncl1 * sizeof(NumSlot)));
   SPOPS_TRY(ngb.alloc(ncl1 * 8));
   SPOPS_TRY(ngoff.alloc(ncl1 * 8));
-  std::vector<int64_t> nstart;
-  if (ncl > 0) {
+  std::vector<int64_t> nstart(9, 0);
+  if (ncl > nsorted) {
     num_bin_kernel<<<grid_for(ncl), 256, 0, st>>>(nzd.as<int64_t>(), cnt_d, offs.as<int64_t>(), ncl, (int64_t)sizeof(V),
-                                                 lim, bkey.as<uint32_t>(), bid.as<int64_t>());
+                                                 lim, settled.as<unsigned char>(), bkey.as<uint32_t>(),
+                                                 bid.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
+    SPOPS_TRY(sort_bins(8, nstart));
   }
-  SPOPS_TRY(sort_bins(8, nstart));
   const int64_t nlisted = nstart[8];
   if (nlisted > 0) {
     num_list_kernel<<<grid_for(nlisted), 256, 0, st>>>(bid_s.as<int64_t>(), nzd.as<int64_t>(), offs.as<int64_t>(),
@@ -1418,7 +1507,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
       numeric_warp_kernel<I, V><<<grid, 32 * warp_count[w], smem, st>>>(
           bid_s.as<int64_t>() + nstart[w], m, nslots.as<NumSlot>() + nstart[w], warp_bytes[w], cptr.as<int64_t>(),
           cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
-          B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+          B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), soff.as<int64_t>(), soff_val.as<int64_t>(),
           drop.as<unsigned char>(), ccol.as<int32_t>(), cval.as<V>());
     } else {
       SPOPS_CUDA(cudaFuncSetAttribute(numeric_warp_wide_kernel<I, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1426,7 +1515,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
       numeric_warp_wide_kernel<I, V><<<grid, 32 * warp_count[w], smem, st>>>(
           bid_s.as<int64_t>() + nstart[w], m, nslots.as<NumSlot>() + nstart[w], warp_bytes[w], cptr.as<int64_t>(),
           cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
-          B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+          B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), soff.as<int64_t>(), soff_val.as<int64_t>(),
           drop.as<unsigned char>(), ccol.as<int32_t>(), cval.as<V>());
     }
     SPOPS_LAUNCH_CHECK();
@@ -1442,10 +1531,19 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     numeric_kernel<I, V><<<(unsigned)m, num_threads[w], num_smem[w], st>>>(
         bid_s.as<int64_t>() + nstart[w + kWarpBins], m, nslots.as<NumSlot>() + nstart[w + kWarpBins], cptr.as<int64_t>(),
         cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), B->row.as<I>(),
-        B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+        B->col.as<I>(), B->val.as<V>(), nzd.as<int64_t>(), soff.as<int64_t>(), soff_val.as<int64_t>(),
         drop.as<unsigned char>(), global ? arena.as<unsigned char>() : nullptr,
         global ? ngoff.as<int64_t>() + nstart[7] : nullptr, ccol.as<int32_t>(), cval.as<V>());
     SPOPS_LAUNCH_CHECK();
+  }
+  int64_t hdense = 0, c_cols = 0;
+  SPOPS_CUDA(cudaMemcpyAsync(&hdense, ndense.p, 8, cudaMemcpyDeviceToHost, st));
+  if (ncl > 0) {  // distinct output columns over all clusters (statistics)
+    size_t c1 = 0;
+    SPOPS_CUDA(cub::DeviceReduce::Sum(nullptr, c1, nzd.as<int64_t>(), tot.as<int64_t>(), ncl, st));
+    SPOPS_TRY(tmp.alloc(c1 + 256));
+    SPOPS_CUDA(cub::DeviceReduce::Sum(tmp.p, c1, nzd.as<int64_t>(), tot.as<int64_t>(), ncl, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&c_cols, tot.p, 8, cudaMemcpyDeviceToHost, st));
   }
   SPOPS_CUDA(cudaStreamSynchronize(st));
   arena.release();
@@ -1461,7 +1559,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_CUDA(cudaMemsetAsync(kcnt.p, 0, (size_t)(ncl + 1) * 8, st));
     SPOPS_CUDA(cudaMemsetAsync(kval.p, 0, (size_t)(ncl + 1) * 8, st));
     if (ncl > 0) {
-      cl_keep_count_kernel<V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+      cl_keep_count_kernel<V><<<grid_for(ncl * 32), 256, 0, st>>>(soff_val.as<int64_t>(), nzd.as<int64_t>(),
                                                                  offs.as<int64_t>(), ncl, cval.as<V>(),
                                                                  drop.as<unsigned char>(), kcnt.as<int64_t>(),
                                                                  kval.as<int64_t>());
@@ -1482,7 +1580,8 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_TRY(kv.alloc((size_t)std::max<int64_t>(h2[1], 1) * sizeof(V)));
     if (ncl > 0) {
       cl_compact_kernel<int32_t, V><<<grid_for(ncl * 32), 256, 0, st>>>(
-          ccptr.as<int64_t>(), ccptr_val.as<int64_t>(), offs.as<int64_t>(), ncl, ccol.as<int32_t>(), cval.as<V>(),
+          soff.as<int64_t>(), soff_val.as<int64_t>(), nzd.as<int64_t>(), offs.as<int64_t>(), ncl, ccol.as<int32_t>(),
+          cval.as<V>(),
           drop.as<unsigned char>(), nrp.as<int64_t>(), nrpv.as<int64_t>(), kcol.as<int32_t>(), kv.as<V>());
       SPOPS_LAUNCH_CHECK();
     }
@@ -1505,7 +1604,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(crp.alloc((nn + 1) * 8));
   SPOPS_CUDA(cudaMemsetAsync(rowcnt.p, 0, (nn + 1) * 8, st));
   if (ncl > 0) {
-    row_count_kernel<V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
+    row_count_kernel<V><<<grid_for(ncl * 32), 256, 0, st>>>(soff_val.as<int64_t>(), nzd.as<int64_t>(),
                                                             offs.as<int64_t>(), perm.as<int64_t>(), ncl, cval.as<V>(),
                                                             rowwise, rowcnt.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
@@ -1544,8 +1643,9 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     SPOPS_LAUNCH_CHECK();
   }
   if (ncl > 0 && cnnz > 0) {
-    row_write_kernel<I, V><<<grid_for(ncl * 32), 256, 0, st>>>(ccptr.as<int64_t>(), ccptr_val.as<int64_t>(),
-                                                               offs.as<int64_t>(), perm.as<int64_t>(), ncl,
+    row_write_kernel<I, V><<<grid_for(ncl * 32), 256, 0, st>>>(soff.as<int64_t>(), soff_val.as<int64_t>(),
+                                                               nzd.as<int64_t>(), offs.as<int64_t>(),
+                                                               perm.as<int64_t>(), ncl,
                                                                ccol.as<int32_t>(), cval.as<V>(), rowwise,
                                                                crp.as<int64_t>(), C->col.as<I>(), C->val.as<V>());
     SPOPS_LAUNCH_CHECK();

@@ -1,0 +1,258 @@
+// Sort-accumulate numeric phase of the cluster-wise SpGEMM: one warp per
+// cluster, no hash table, no separate symbolic pass.
+//
+// For a cluster whose products (pairs of a cluster column j and an entry k of
+// B's row j) number P <= 32*R, every product t (flat (j, k) order: the
+// cluster's columns in order, each B row in storage order) becomes one 32-bit
+// key (output column << tbits | t), held R to a lane in registers.  One
+// bitonic network over the 32*R keys (blocked: lane L holds sorted positions
+// L*R .. L*R+R-1) sorts them by column and, within a column, by t.  A column's
+// products are then adjacent, in flat order: their values are summed along
+// the sorted sequence (in each lane in order, then across lanes by a
+// segmented suffix scan), so the summation order depends only on the
+// matrices.  The number of distinct columns, their min and max come from the
+// same sorted keys, which settles the reference's dense/hash classification
+// (src/spgemm_Vlength_mixed.cpp:267-319) and its drop rule for the cluster
+// without a symbolic pass.
+//
+// Output goes to the cluster's slab: ccol[soff[c] ..], cval[soff_val[c] ..]
+// (room for P columns), columns ascending, values [column x csz] with the
+// rows of the cluster interleaved -- the same layout the hash kernels write.
+//
+// Limits (the caller bins clusters accordingly): P <= 32*R, the cluster has
+// at most kSortCols columns, and B's column count fits the key
+// (cols <= 2^(32 - tbits) - 1, tbits = log2(32*R)).
+#pragma once
+
+#include <cstdint>
+
+namespace spops {
+namespace {
+
+constexpr int kSortCols = 256;  // cluster columns staged per warp
+constexpr int kSortWarps = 4;   // warps per block
+
+// Ascending bitonic sort of 32*R keys, blocked: element e = lane*R + s.
+template <int R>
+__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&k)[R], int lane) {
+  constexpr int N = 32 * R;
+#pragma unroll
+  for (int kk = 2; kk <= N; kk <<= 1) {
+#pragma unroll
+    for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+      if (jj >= R) {  // partner: lane ^ (jj / R), same slot
+        const int lm = jj / R;
+        const bool lower = (lane & lm) == 0;
+        const bool asc = (kk >= N) ? true : ((lane & (kk / R)) == 0);
+        const bool keep_min = lower == asc;
+#pragma unroll
+        for (int s = 0; s < R; ++s) {
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, k[s], lm);
+          k[s] = keep_min ? min(k[s], o) : max(k[s], o);
+        }
+      } else {  // partner: slot s ^ jj of the same lane
+#pragma unroll
+        for (int s = 0; s < R; ++s) {
+          const int p = s ^ jj;
+          if (p > s) {
+            bool asc;
+            if (kk < R) asc = (s & kk) == 0;
+            else if (kk >= N) asc = true;
+            else asc = (lane & (kk / R)) == 0;
+            const uint32_t a = k[s], b = k[p];
+            const uint32_t lo = min(a, b), hi = max(a, b);
+            k[s] = asc ? lo : hi;
+            k[p] = asc ? hi : lo;
+          }
+        }
+      }
+    }
+  }
+}
+
+// largest j in [0, nj) with off[j] <= t (off ascending, off[0] = 0)
+__device__ __forceinline__ int sort_find_col(const int32_t* off, int nj, int32_t t) {
+  int lo = 0, hi = nj;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <typename I, typename V, int R>
+__global__ void __launch_bounds__(32 * kSortWarps)
+    sort_accum_kernel(const int64_t* __restrict__ list, int64_t nlist, const int64_t* __restrict__ cptr,
+                      const int64_t* __restrict__ cptr_val, const int32_t* __restrict__ colids,
+                      const V* __restrict__ avals, const int64_t* __restrict__ offsets, const I* __restrict__ brp,
+                      const I* __restrict__ bci, const V* __restrict__ bv, int tbits, double b_rowdense,
+                      double budget, bool sort_output, bool rowwise, const int64_t* __restrict__ soff,
+                      const int64_t* __restrict__ soff_val, int64_t* __restrict__ nz, int64_t* __restrict__ cmin,
+                      int64_t* __restrict__ cmax, unsigned char* __restrict__ drop_out,
+                      unsigned long long* __restrict__ ndense, int32_t* __restrict__ ccol, V* __restrict__ cval) {
+  __shared__ int32_t s_off[kSortWarps][kSortCols + 1];
+  __shared__ int64_t s_start[kSortWarps][kSortCols];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t b = blockIdx.x * (int64_t)kSortWarps + w;
+  if (b >= nlist) return;
+  const int64_t c = list[b];
+  const int64_t csz = offsets[c + 1] - offsets[c];
+  const int64_t j0 = cptr[c];
+  const int nj = (int)(cptr[c + 1] - j0);
+  int32_t* off = s_off[w];
+  int64_t* start = s_start[w];
+  // B row starts of the cluster's columns and the products before each
+  int32_t carry = 0;
+  for (int t0 = 0; t0 < nj; t0 += 32) {
+    const int t = t0 + lane;
+    int32_t len = 0;
+    if (t < nj) {
+      const int64_t r = colids[j0 + t];
+      const int64_t st = brp[r];
+      start[t] = st;
+      len = (int32_t)((int64_t)brp[r + 1] - st);
+    }
+    int32_t inc = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
+    }
+    if (t < nj) off[t + 1] = carry + inc;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  if (lane == 0) off[0] = 0;
+  __syncwarp();
+  const int32_t P = off[nj];
+  // keys: slot s of this lane holds product t = s*32 + lane before sorting
+  constexpr uint32_t kNone = 0xffffffffu;
+  uint32_t key[R];
+  {
+    int j = 0;
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      const int32_t t = s * 32 + lane;
+      key[s] = kNone;
+      if (t < P) {
+        while (off[j + 1] <= t) ++j;
+        const int64_t k = start[j] + (t - off[j]);
+        key[s] = ((uint32_t)bci[k] << tbits) | (uint32_t)t;
+      }
+    }
+  }
+  warp_bitonic_sort<R>(key, lane);
+  const uint32_t tmask = (1u << tbits) - 1u;
+  // column starts in this lane's sorted run; the distinct-column count
+  const uint32_t prev_last = __shfl_up_sync(0xffffffffu, key[R - 1], 1);
+  unsigned first = 0;  // bit s: sorted position lane*R + s starts a column
+  int cnt = 0;
+#pragma unroll
+  for (int s = 0; s < R; ++s) {
+    const uint32_t prev = s == 0 ? (lane == 0 ? kNone : prev_last) : key[s - 1];
+    const bool f = key[s] != kNone && (s == 0 && lane == 0 ? true : (prev >> tbits) != (key[s] >> tbits));
+    first |= (f ? 1u : 0u) << s;
+    cnt += f ? 1 : 0;
+  }
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
+  }
+  const int base = incl - cnt;  // rank of this lane's first column start
+  const int64_t nzc = __shfl_sync(0xffffffffu, incl, 31);
+  int64_t mx = -1;
+#pragma unroll
+  for (int s = 0; s < R; ++s)
+    if (key[s] != kNone) mx = (int64_t)(key[s] >> tbits);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  const int64_t mn = (int64_t)(__shfl_sync(0xffffffffu, key[0], 0) >> tbits);
+  // the reference's classification (the same arithmetic as classify_kernel)
+  bool dense = false;
+  if (nzc > 0) {
+    const int64_t range = mx - mn + 1;
+    const double density = (double)nzc / (double)range;
+    const size_t b_access = (size_t)((double)nj * b_rowdense * (double)(sizeof(int64_t) + sizeof(V)));
+    const size_t dense_bytes = (size_t)range * (size_t)csz * sizeof(V);
+    dense = (double)(b_access + dense_bytes) <= budget && density >= 0.15;
+  }
+  const bool drop = !rowwise && (dense || sort_output);
+  if (lane == 0) {
+    nz[c] = nzc;
+    cmin[c] = nzc ? mn : 0;
+    cmax[c] = nzc ? mx : 0;
+    drop_out[c] = drop ? 1 : 0;
+    if (dense && !rowwise) atomicAdd(ndense, 1ULL);
+  }
+  const int64_t co = soff[c], cvo = soff_val[c], vbase = cptr_val[c];
+  // output columns
+  {
+    int r = base;
+#pragma unroll
+    for (int s = 0; s < R; ++s)
+      if (first >> s & 1u) ccol[co + r++] = (int32_t)(key[s] >> tbits);
+  }
+  // values, one row of the cluster at a time
+  for (int64_t l = 0; l < csz; ++l) {
+    V head = V(0), run = V(0);
+    bool seen = false;
+    int r = base - 1;
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      if (key[s] != kNone) {
+        const int32_t t = (int32_t)(key[s] & tmask);
+        const int j = sort_find_col(off, nj, t);
+        const V v = avals[vbase + (int64_t)j * csz + l] * bv[start[j] + (t - off[j])];
+        if (first >> s & 1u) {
+          if (seen) {
+            const V o = (csz == 1 && drop && fabs((double)run) < 1e-12) ? V(0) : run;
+            cval[cvo + (int64_t)r * csz + l] = o;
+          }
+          seen = true;
+          run = v;
+          ++r;
+        } else if (seen) {
+          run += v;
+        } else {
+          head += v;
+        }
+      }
+    }
+    // the sums of the lanes after this one that continue its last column:
+    // S[L] = head[L] + (lane L starts a column ? 0 : S[L+1])
+    V S = head;
+    bool stop = seen;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const V ov = __shfl_down_sync(0xffffffffu, S, o);
+      const bool os = __shfl_down_sync(0xffffffffu, stop ? 1 : 0, o) != 0;
+      if (lane + o < 32 && !stop) {
+        S += ov;
+        stop = os;
+      }
+    }
+    V next = __shfl_down_sync(0xffffffffu, S, 1);
+    if (lane == 31) next = V(0);
+    if (seen) {
+      const V tot = run + next;
+      const V o = (csz == 1 && drop && fabs((double)tot) < 1e-12) ? V(0) : tot;
+      cval[cvo + (int64_t)r * csz + l] = o;
+    }
+  }
+  if (csz > 1 && drop) {  // a column is zeroed when all its rows fall below 1e-12
+    for (int r = base; r < base + cnt; ++r) {
+      bool small = true;
+      for (int64_t l = 0; l < csz; ++l)
+        if (fabs((double)cval[cvo + (int64_t)r * csz + l]) >= 1e-12) {
+          small = false;
+          break;
+        }
+      if (small)
+        for (int64_t l = 0; l < csz; ++l) cval[cvo + (int64_t)r * csz + l] = V(0);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace spops

@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <cstdlib>
+
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -87,6 +90,27 @@ struct Context {
 // Temporary device buffer of one API call, from the context's pool and
 // ordered on its stream (alloc and free both enqueue on ctx->stream, so the
 // memory is reused only by work queued after this call's last use of it).
+// SPOPS_TRACE=1 in the environment: wall time of each step of a host-side
+// driver on stderr, prefixed by its name (the stream is synchronised at every
+// mark, so tracing changes the timing it reports only by those waits).
+struct Trace {
+  bool on = false;
+  const char* name;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  explicit Trace(const char* who) : name(who) {
+    const char* e = std::getenv("SPOPS_TRACE");
+    on = e && e[0] == '1';
+  }
+  void mark(cudaStream_t st, const char* what) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    const auto n = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[%s] %-30s %9.3f ms\n", name, what,
+                 std::chrono::duration<double, std::milli>(n - t).count());
+    t = n;
+  }
+};
+
 struct PoolBuf {
   Context* ctx;
   void* p = nullptr;
@@ -251,6 +275,10 @@ struct DiaData {
   int64_t ndiag = 0, stride = 0;
   DevBuf offsets;  // int64 [ndiag]
   DevBuf data;     // V [ndiag * stride]
+  // smallest / largest offset, read back once by the first SpMV: a block of
+  // rows stages the x window its diagonals reach in shared memory when it fits
+  bool span_known = false;
+  int64_t lo = 0, hi = 0;
   void release() { offsets.release(); data.release(); }
 };
 
