@@ -323,6 +323,44 @@ __global__ void __launch_bounds__(256) dia_kernel(const int64_t* __restrict__ of
   if (i < n) axpby_store(y + i, s0 + s1, alpha, beta, bz);
 }
 
+// DIA with x staged in shared memory: the block's 256 rows reach x only in
+// [i0 + lo, i0 + 255 + hi], so that window (win = 256 + hi - lo entries) is
+// read once, coalesced, and every diagonal's gathers come from shared memory.
+// Used when the window fits (dia_spmv_t); the products are summed in the same
+// order as dia_kernel, so both give the same bits.
+constexpr int kDiaStageMaxDiags = 1024;
+constexpr int64_t kDiaStageMaxWin = 4096;
+
+template <typename V>
+__global__ void __launch_bounds__(256) dia_staged_kernel(const int64_t* __restrict__ offsets,
+                                                         const V* __restrict__ data, int64_t ndiag, int64_t stride,
+                                                         int64_t n, int64_t ncols, const V* __restrict__ x,
+                                                         V* __restrict__ y, V alpha, V beta, bool bz, int64_t lo,
+                                                         int64_t win) {
+  extern __shared__ __align__(16) unsigned char dia_sm[];
+  V* xs = reinterpret_cast<V*>(dia_sm);
+  __shared__ int64_t soff[kDiaStageMaxDiags];
+  const int64_t i0 = blockIdx.x * 256LL;
+  const int64_t w0 = i0 + lo;  // x index held by xs[0]
+  for (int t = threadIdx.x; t < ndiag; t += blockDim.x) soff[t] = offsets[t];
+  for (int64_t t = threadIdx.x; t < win; t += blockDim.x) {
+    const int64_t j = w0 + t;
+    xs[t] = (j >= 0 && j < ncols) ? ld_gather(x + j) : V(0);
+  }
+  __syncthreads();
+  const int64_t i = i0 + threadIdx.x;
+  if (i >= n) return;
+  V s0 = V(0), s1 = V(0);
+  for (int d = 0; d < (int)ndiag; ++d) {
+    const int64_t j = i + soff[d];
+    if (j >= 0 && j < ncols) {
+      const V p = ld_stream(data + d * stride + i) * xs[j - w0];
+      if (d & 1) s1 += p; else s0 += p;
+    }
+  }
+  axpby_store(y + i, s0 + s1, alpha, beta, bz);
+}
+
 // ------------------------------------------------------------------ BSR
 template <typename I>
 __global__ void bsr_keys_kernel(const I* __restrict__ rp, const I* __restrict__ ci, int64_t n, int64_t br,
@@ -939,6 +977,22 @@ spops_status_t coo_analyse_t(Context* ctx, Matrix* A) {
 template <typename I, typename V>
 spops_status_t dia_spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
   if (A->rows == 0) return SPOPS_OK;
+  DiaData& D = A->dia;
+  if (!D.span_known) {
+    std::vector<int64_t> off((size_t)D.ndiag);
+    if (D.ndiag > 0) SPOPS_TRY(download(ctx, off.data(), D.offsets.as<int64_t>(), D.ndiag));
+    D.lo = D.ndiag > 0 ? *std::min_element(off.begin(), off.end()) : 0;
+    D.hi = D.ndiag > 0 ? *std::max_element(off.begin(), off.end()) : 0;
+    D.span_known = true;
+  }
+  const int64_t win = 256 + D.hi - D.lo;
+  if (D.ndiag > 0 && D.ndiag <= kDiaStageMaxDiags && win <= kDiaStageMaxWin) {
+    dia_staged_kernel<V><<<grid_for(A->rows), 256, (size_t)win * sizeof(V), ctx->stream>>>(
+        D.offsets.as<int64_t>(), D.data.as<V>(), D.ndiag, D.stride, A->rows, A->cols, static_cast<const V*>(x),
+        static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, D.lo, win);
+    SPOPS_LAUNCH_CHECK();
+    return SPOPS_OK;
+  }
   dia_kernel<V><<<grid_for(A->rows), 256, 0, ctx->stream>>>(
       A->dia.offsets.as<int64_t>(), A->dia.data.as<V>(), A->dia.ndiag, A->dia.stride, A->rows, A->cols,
       static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0);
