@@ -262,6 +262,7 @@ spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H
   cudaStream_t st = ctx->stream;
   const int per = H.pattern ? 2 : 3;
   const int64_t nnz = H.nnz;
+  Trace tr("mtx");
   PoolBuf starts(ctx), nsel(ctx), tmp(ctx), tab(ctx), r(ctx), c(ctx), v(ctx), cnt(ctx), pos(ctx), misc(ctx),
       olist(ctx), ocand(ctx);
   // token starts
@@ -285,6 +286,7 @@ spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H
       return fail(SPOPS_ERR_INVALID, "Matrix Market: %lld entries announced, %lld numbers found", (long long)nnz,
                   (long long)ntok);
     SPOPS_CUDA(cudaMemcpyAsync(starts.p, all.p, (size_t)(nnz * per) * 8, cudaMemcpyDeviceToDevice, st));
+    tr.mark(st, "token select");
   } else if (nnz > 0) {
     return fail(SPOPS_ERR_INVALID, "Matrix Market: %lld entries announced, none found", (long long)nnz);
   }
@@ -314,6 +316,7 @@ spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H
   unsigned long long hm[3] = {0, 0, 0};
   SPOPS_CUDA(cudaMemcpyAsync(hm, misc.p, 24, cudaMemcpyDeviceToHost, st));
   SPOPS_CUDA(cudaStreamSynchronize(st));
+  tr.mark(st, "parse entries");
   const int64_t nopen = (int64_t)hm[0];
   if (nopen > 0) {
     exact_values_kernel<<<grid_for(nopen, 32), 32, 0, st>>>(dtext.as<char>(), len, starts.as<int64_t>(), per,
@@ -364,8 +367,10 @@ spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H
                                                       A->col.as<I>(), A->val.as<V>());
     if (cudaGetLastError() != cudaSuccess) s = fail(SPOPS_ERR_CUDA, "Matrix Market: place launch failed");
   }
+  tr.mark(st, "copies + COO arrays");
   if (s == SPOPS_OK) s = coo_analyse(ctx, A);
   if (s == SPOPS_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(SPOPS_ERR_CUDA, "Matrix Market: stream error");
+  tr.mark(st, "COO analysis");
   if (s != SPOPS_OK) {
     A->release_all();
     delete static_cast<spops_matrix_s*>(A);
@@ -398,9 +403,11 @@ spops_status_t parse_coo(Context* ctx, const char* text, size_t n, spops_index_t
   SPOPS_TRY(read_header(text, n, &H));
   SPOPS_TRY(check_header(H, itype));
   const int64_t len = (int64_t)(n - H.data);
+  Trace tr("mtx");
   PoolBuf dtext(ctx);
   SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
   if (len > 0) SPOPS_CUDA(cudaMemcpyAsync(dtext.p, text + H.data, (size_t)len, cudaMemcpyHostToDevice, ctx->stream));
+  tr.mark(ctx->stream, "upload from host memory");
   return read_typed(ctx, dtext, len, H, itype, vtype, out);
 }
 
@@ -454,6 +461,7 @@ struct FileCloser {
 };
 
 spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, spops_value_t vtype, Matrix** out) {
+  Trace tr("mtx");
   const int fd = ::open(path, O_RDONLY | O_CLOEXEC);
   if (fd < 0) return fail(SPOPS_ERR_INVALID, "Matrix Market: unable to open file: %s", path);
   FileCloser closer{fd};
@@ -484,8 +492,10 @@ spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, sp
   const int64_t len = size - (int64_t)H.data;
   PoolBuf dtext(ctx);
   SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
+  tr.mark(ctx->stream, "open + header + text buffer");
   if (len > 0) {
     SPOPS_TRY(ensure_file_stage(ctx));
+    tr.mark(ctx->stream, "pinned staging");
     const int64_t nchunks = (len + (int64_t)kChunk - 1) / (int64_t)kChunk;
     const int nt = (int)std::min<int64_t>(kReaders, nchunks);
     std::atomic<int> bad{0};  // 1: read error, 2: CUDA error
@@ -523,6 +533,7 @@ spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, sp
       for (int w = 0; w < nt; ++w) th.emplace_back(reader, w);
       for (auto& t : th) t.join();
     }
+    tr.mark(ctx->stream, "file read + upload");
     if (bad == 1) return fail(SPOPS_ERR_INVALID, "Matrix Market: read error: %s", path);
     if (bad == 2) {
       cudaStreamSynchronize(ctx->stream);
@@ -558,10 +569,14 @@ spops_status_t coo_to_csr_out(Context* ctx, Matrix* coo, int32_t compact, spops_
       *csr = static_cast<spops_matrix_s*>(C);
     }
   } else {
+    Trace tr("mtx");
     s = spops_coo_to_csr(static_cast<spops_context_s*>(ctx), static_cast<spops_matrix_s*>(coo), compact, csr);
+    tr.mark(ctx->stream, "coo_to_csr");
   }
+  Trace tr("mtx");
   coo->release_all();
   delete static_cast<spops_matrix_s*>(coo);
+  tr.mark(ctx->stream, "release COO");
   return s;
 }
 

@@ -280,4 +280,50 @@ void synth_planted_fill_i64(int64_t n, int64_t ncols, int64_t ncomm, double mu, 
   });
 }
 
+// ---------------------------------------------- grouped rows
+// Rows come in contiguous groups of `group` rows; group g draws from the
+// column block [(g mod (ncols / width)) * width, ... + width) with
+// probability p_in, else uniformly over all columns; row length
+// round(lognormal(mu, sigma)) clipped to [1, width]; duplicates removed.
+// Rows of a group share most of their columns, so MinHash-LSH pairs them,
+// and C = A A^T has dense group x group blocks.  Values N(0, 1).
+static void grouped_cols(int64_t r, int64_t ncols, int64_t group, int64_t width, double mu, double sigma,
+                         double p_in, uint64_t seed, std::vector<int64_t>& c) {
+  Rng g(seed, 12, (uint64_t)r);
+  const int64_t nblocks = std::max<int64_t>(1, ncols / width);
+  const int64_t blk = (r / group) % nblocks;
+  double Ld = std::floor(std::exp(mu + sigma * g.normal()) + 0.5);
+  int64_t L = (int64_t)std::min<double>(std::max<double>(Ld, 1.0), (double)width);
+  c.clear();
+  c.reserve(L);
+  for (int64_t k = 0; k < L; ++k) {
+    if (g.uniform() < p_in)
+      c.push_back(blk * width + (int64_t)g.below((uint64_t)width));
+    else
+      c.push_back((int64_t)g.below((uint64_t)ncols));
+  }
+  std::sort(c.begin(), c.end());
+  c.erase(std::unique(c.begin(), c.end()), c.end());
+}
+
+void synth_grouped_rowlen(int64_t n, int64_t ncols, int64_t group, int64_t width, double mu, double sigma,
+                          double p_in, uint64_t seed, int64_t* len) {
+  parallel_rows(n, [&](int64_t r) {
+    std::vector<int64_t> c;
+    grouped_cols(r, ncols, group, width, mu, sigma, p_in, seed, c);
+    len[r] = (int64_t)c.size();
+  });
+}
+
+void synth_grouped_fill_i64(int64_t n, int64_t ncols, int64_t group, int64_t width, double mu, double sigma,
+                            double p_in, uint64_t seed, const int64_t* rp, int64_t* ci, double* v) {
+  parallel_rows(n, [&](int64_t r) {
+    std::vector<int64_t> c;
+    grouped_cols(r, ncols, group, width, mu, sigma, p_in, seed, c);
+    for (size_t k = 0; k < c.size(); ++k) ci[rp[r] + (int64_t)k] = c[k];
+    Rng gv(seed, 13, (uint64_t)r);
+    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) v[k] = gv.normal();
+  });
+}
+
 }  // extern "C"

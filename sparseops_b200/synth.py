@@ -142,6 +142,28 @@ def planted_communities(n: int, ncols: int | None = None, ncomm: int = 2048, mea
     return rp, ci, v
 
 
+def grouped_rows(n: int, group: int = 32, width: int = 12, mean: float = 10.0, sigma: float = 0.5,
+                 p_in: float = 0.995, seed: int = 8, ncols: int | None = None):
+    """Rows in contiguous groups of `group`; a group draws from one block of
+    `width` columns (with probability p_in, else uniformly), so rows of a
+    group are near-duplicates: MinHash-LSH pairs them into multi-row
+    clusters and C = A A^T has dense group x group blocks.  Row length
+    lognormal with the given mean, clipped to [1, width]; duplicates removed;
+    values N(0, 1).  Default ncols = n / group * width.  Index type int64.
+    Returns (rp, ci, v, ncols)."""
+    ncols = n // group * width if ncols is None else ncols
+    mu = math.log(mean) - 0.5 * sigma * sigma
+    lens = np.empty(n, np.int64)
+    _lib().synth_grouped_rowlen(_i64(n), _i64(ncols), _i64(group), _i64(width), _dbl(mu), _dbl(sigma), _dbl(p_in),
+                                _u64(seed), _p(lens))
+    rp = _rowptr(lens)
+    ci = np.empty(int(rp[-1]), np.int64)
+    v = np.empty(int(rp[-1]), np.float64)
+    _lib().synth_grouped_fill_i64(_i64(n), _i64(ncols), _i64(group), _i64(width), _dbl(mu), _dbl(sigma), _dbl(p_in),
+                                  _u64(seed), _p(rp), _p(ci), _p(v))
+    return rp, ci, v, ncols
+
+
 def transpose(rp, ci, v, ncols: int):
     """Plain CSR transpose (stable by row), same index dtype as the input."""
     n = len(rp) - 1
