@@ -97,6 +97,13 @@ def workload_name(n):
     return f"powerlaw CSR SpMV FP64 n={n} (lognormal ln12,1.2 clip [1,20000]; seed 1)"
 
 
+def ref_bytes_per_spmv(n_rows, nnz, isz=4, vsz=8):
+    """The reference's own byte count for a CSR SpMV (bytes_per_spmv,
+    include/spmv_benchmark.h:43-51): row pointer twice per row, a column index,
+    A[i,j] and x[j] per entry, y read and written per row."""
+    return 2 * isz * n_rows + isz * nnz + 2 * vsz * nnz + 2 * vsz * n_rows
+
+
 def spmv_bytes(n_rows, n_cols, nnz, isz=4, vsz=8):
     return isz * (n_rows + 1) + (isz + vsz) * nnz + vsz * n_cols + vsz * n_rows
 
@@ -279,6 +286,104 @@ def _graph_ms(fn, reps, ctx):
         return None
 
 
+def bench_laplacian(ctx, dev, peak, cpu_ref: bool, iters=2000):
+    """The 512 x 512 five-point Laplacian (n = 262,144, diagonal 4, off-diagonals
+    -1; x uniform[-1,1], seed 0), FP64: CSR and DIA SpMV.  The whole working
+    set (about 21 MB) is resident in the 126 MB L2, so the GB/s here are
+    effective rates on the algorithmic bytes, not HBM traffic; iters
+    back-to-back launches, and the same launches replayed from a CUDA graph
+    (no host issue gaps).  e2e: pinned host x in, y out per step through
+    spops_spmv_host_async.  CPU: the reference's SpOps_csr (kernel_flag 2) on
+    all host cores, median of 20 runs."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, SpOps_dia, csr_to_dia, synth
+    from sparseops_b200._lib import call, dbl, vp
+    rp, ci, v = synth.laplacian_2d(512)
+    n, nnz = len(rp) - 1, len(ci)
+    x = synth.uniform(n, 0)
+    A = CSR_Matrix(n, n, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev), torch.from_numpy(v).to(dev))
+    h = A.device(ctx)
+    xd = torch.from_numpy(x).to(dev)
+    yd = torch.zeros(n, dtype=torch.float64, device=dev)
+    nbytes = spmv_bytes(n, n, nnz)
+    out = {"rows": n, "nnz": nnz, "algorithmic_bytes": nbytes, "reference_bytes_per_spmv": ref_bytes_per_spmv(n, nnz),
+           "residency": "L2 (working set ~21 MB < 126 MB L2): effective GB/s, not HBM traffic"}
+
+    def csr():
+        call("spops_spmv", ctx.handle, dbl(1.0), h.handle, vp(xd.data_ptr()), dbl(0.0), vp(yd.data_ptr()))
+
+    ctx.follow_torch()
+    ms = _ev_ms(csr, iters, warm=20)
+    gms = _graph_ms(lambda: [csr() for _ in range(100)], 20, ctx)
+    gms = None if gms is None else gms / 100
+    from oracle import Oracle
+    O = Oracle()
+    yref = O.spmv_csr(rp, ci, v, x)
+    den = np.maximum(O.absdot(rp, ci, v, x), 1e-300)
+    csr()
+    torch.cuda.synchronize()
+    err = float((np.abs(yd.cpu().numpy() - yref) / den).max())
+    best = ms if gms is None else min(ms, gms)
+    out["csr"] = {"ms": round(ms, 5), "graph_ms": None if gms is None else round(gms, 5),
+                  "GB/s": round(nbytes / best / 1e6, 1),
+                  "roofline": {"bound": "hbm", "achieved": round(nbytes / best / 1e6, 1), "peak": peak,
+                               "unit": "GB/s", "frac": round(nbytes / best / 1e6 / peak, 4),
+                               "note": "L2-resident working set; the fraction is of the HBM copy peak"},
+                  "GFLOP/s": round(2 * nnz / best / 1e6, 1), "rel_err": err}
+    D = csr_to_dia(A, 10240, None, 4)
+    yd2 = torch.zeros(n, dtype=torch.float64, device=dev)
+    SpOps_dia(1.0, D, xd, 0.0, yd2)
+    torch.cuda.synchronize()
+    dms = _ev_ms(lambda: SpOps_dia(1.0, D, xd, 0.0, yd2), iters, warm=20)
+    derr = float((np.abs(yd2.cpu().numpy() - yref) / den).max())
+    dbytes = 8 * D.complete_ndiags * D.stride + 16 * n
+    out["dia"] = {"ms": round(dms, 5), "diagonals": int(D.complete_ndiags), "bytes": dbytes,
+                  "GB/s": round(dbytes / dms / 1e6, 1), "csr_equivalent_GB/s": round(nbytes / dms / 1e6, 1),
+                  "GFLOP/s": round(2 * nnz / dms / 1e6, 1), "rel_err": derr,
+                  "kernel": "dia_staged_kernel (x window of each 256-row block in shared memory)"}
+    # e2e through the C ABI host path
+    xh = [torch.from_numpy(x).pin_memory() for _ in range(2)]
+    yh = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(2)]
+    steps = 200
+    for i in range(4):
+        call("spops_spmv_host_async", ctx.handle, dbl(1.0), h.handle, vp(xh[i & 1].data_ptr()), dbl(0.0),
+             vp(yh[i & 1].data_ptr()))
+    call("spops_spmv_host_wait", ctx.handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        call("spops_spmv_host_async", ctx.handle, dbl(1.0), h.handle, vp(xh[i & 1].data_ptr()), dbl(0.0),
+             vp(yh[i & 1].data_ptr()))
+    call("spops_spmv_host_wait", ctx.handle)
+    e1.record()
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / steps
+    out["e2e"] = {"ms_per_step": round(ems, 5), "GB/s": round(nbytes / ems / 1e6, 1),
+                  "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                  "path": "spops_spmv_host_async, pinned x in and y out per step"}
+    if cpu_ref:
+        try:
+            from oracle import Reference, reference_available
+            if reference_available():
+                with quiet_stdout():
+                    R = Reference(threads=os.cpu_count())
+                    ys = np.zeros(n)
+                    for _ in range(5):
+                        R.spmv_csr(rp, ci, v, x, 1.0, 0.0, None, flag=2, out=ys)
+                    ts = []
+                    for _ in range(20):
+                        t0 = time.perf_counter()
+                        R.spmv_csr(rp, ci, v, x, 1.0, 0.0, None, flag=2, out=ys)
+                        ts.append(time.perf_counter() - t0)
+                cms = float(np.median(ts)) * 1e3
+                out["cpu_baseline"] = {"ms": round(cms, 4), "GB/s": round(nbytes / cms / 1e6, 2),
+                                       "cores": os.cpu_count(), "kind": "reference",
+                                       "sample": "whole matrix, median of 20 SpOps_csr (kernel_flag 2)"}
+        except Exception as e:
+            out["cpu_baseline"] = {"error": str(e)[:160]}
+    return out
+
+
 def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
     """SpMV of the power-law matrix in each format (GB/s on the CSR algorithmic
     bytes; error componentwise against the CSR result over |A||x|)."""
@@ -324,9 +429,14 @@ def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
     return out
 
 
-def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024):
+def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024, peak=None, cpu_ref=False):
     """256 banded-plus-random matrices, n log-uniform in [1e3, 2e5], Poisson(16)
-    per row; one persistent graph-captured launch against per-matrix launches."""
+    per row; one persistent graph-captured launch against per-matrix launches.
+    Roofline: the algorithmic bytes sum_m [4(n_m+1) + 12 nnz_m + 16 k n_m]
+    against the measured HBM peak.  CPU: the reference's path for it, a loop
+    of SpOps_csr (kernel_flag 2, all host cores) per matrix and right-hand
+    side; for k > 1 one column per matrix is timed and multiplied by k (every
+    column is the same work)."""
     import torch
     from sparseops_b200 import Batch, CSR_Matrix, synth
     from sparseops_b200._lib import call, dbl, i64, vp
@@ -343,6 +453,30 @@ def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024):
         tot_rows += int(n)
         tot_nnz += len(ci)
     res = {"matrices": count, "rows": tot_rows, "nnz": tot_nnz}
+    cpu_col_ms = None
+    if cpu_ref:
+        try:
+            from oracle import Reference, reference_available
+            if reference_available():
+                with quiet_stdout():
+                    R = Reference(threads=os.cpu_count())
+                    host = [(M.row_offset.cpu().numpy(), M.col_index.cpu().numpy(), M.values.cpu().numpy())
+                            for M in mats]
+                    xs = [synth.uniform(len(rp) - 1, 7000 + i) for i, (rp, _, _) in enumerate(host)]
+                    ys = [np.zeros(len(rp) - 1) for rp, _, _ in host]
+
+                    def cpu_loop():
+                        for (rp, ci, v), xx, yy in zip(host, xs, ys):
+                            R.spmv_csr(rp, ci, v, xx, 1.0, 0.0, None, flag=2, out=yy)
+                    cpu_loop()
+                    ts = []
+                    for _ in range(5):
+                        t0 = time.perf_counter()
+                        cpu_loop()
+                        ts.append(time.perf_counter() - t0)
+                cpu_col_ms = float(np.median(ts)) * 1e3
+        except Exception as e:
+            res["cpu_reference_error"] = str(e)[:160]
     for k in ks:
         X = [torch.rand(int(n), k, dtype=torch.float64, device=dev) * 2 - 1 for n in ns]
         Yb = [torch.zeros(int(n), k, dtype=torch.float64, device=dev) for n in ns]
@@ -385,6 +519,14 @@ def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024):
         # the plain path: one spops_spmv launch per matrix and RHS column, as a
         # caller of the per-matrix API issues them; also replayed from a CUDA
         # graph (launch gaps removed), the stricter comparison
+        if peak:
+            r["roofline"] = {"bound": "hbm", "achieved": round(nbytes / bms / 1e6, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(nbytes / bms / 1e6 / peak, 4), "algorithmic_bytes": int(nbytes)}
+        if cpu_col_ms is not None:
+            r["cpu_reference"] = {"ms": round(cpu_col_ms * k, 2), "GB/s": round(nbytes / (cpu_col_ms * k) / 1e6, 2),
+                                  "cores": os.cpu_count(), "kind": "reference",
+                                  "sample": "SpOps_csr per matrix, median of 5 passes" +
+                                            ("" if k == 1 else f" over one column, times {k}")}
         r.update({"batched_ms": round(bms, 3), "batched_GB/s": round(nbytes / bms / 1e6, 1),
                   "speedup_vs_plain_launches": round(eager_cols / bms, 2),
                   "speedup_vs_plain_launches_graph": None if graph_cols is None else round(graph_cols / bms, 2),
@@ -400,21 +542,36 @@ def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024):
     return res
 
 
-def bench_fwd_bwd(ctx, dev, n=1 << 20):
-    """y = A(v) x, then grad_x = A^T g and grad_v = g_i x_j: the adjoint kernels
-    (cached device transpose, fused SDDMM) against a plain path that builds the
-    transpose as a new CSR matrix every step (the reference's csr_transpose
-    route) and forms grad_v elementwise."""
+def bench_fwd_bwd(ctx, dev, n=1 << 20, peak=None, cpu_ref=False):
+    """y = A(v) x, then grad_x = A^T g and grad_v = g_i x_j, on a random graph
+    (n = 1,048,576, mean degree 32, symmetric pattern, values U[0.1, 1]).
+
+    ours: the adjoint kernels -- the device transpose kept on the matrix with
+      its values refreshed through a permutation after a value change (an
+      optimizer step), the transpose SpMV, and the SDDMM.
+    plain: the reference's route for the same step built from this library's
+      own calls: the forward SpMV, then csr_transpose as the reference does it
+      (include/sparse_conversion.h:2066-2108: CSR -> COO with rows and columns
+      swapped -> coo_to_csr; here a COO handle on the swapped device arrays,
+      whose analysis is the device coo_to_csr), the SpMV on it, and grad_v
+      elementwise.  Every step builds the transpose anew, as a caller of the
+      reference's API must after the values change.
+    roofline: algorithmic bytes of the three products -- forward
+      4(n+1) + 12 nnz + 16 n, transpose SpMV over the CSC copy the same, SDDMM
+      4(n+1) + 4 nnz + 16 n + 8 nnz written (FP64) -- against the HBM peak; the
+      per-step value refresh (20 nnz bytes) is given beside it.
+    cpu: the reference's csr_transpose + SpOps_csr (kernel_flag 2, all host
+      cores) for grad_x, its SpOps_csr for y, and g_i x_j by numpy, FP64."""
     import torch
-    from sparseops_b200 import CSR_Matrix, synth
+    from sparseops_b200 import COO_Matrix, synth
     from sparseops_b200._lib import call, dbl, vp
     from sparseops_b200.autograd import SparsePattern, spmv
     rp, ci, v = synth.symmetric_graph(n, 32.0, seed=4)
     nnz = len(ci)
     rpt, cit = torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev)
-    rows = torch.repeat_interleave(torch.arange(n, device=dev, dtype=torch.int32), torch.diff(rpt.long()))
     out = {"rows": n, "nnz": nnz}
     for dt, name in ((torch.float64, "f64"), (torch.float32, "f32")):
+        vs = 8 if dt == torch.float64 else 4
         vt = torch.from_numpy(v).to(dev).to(dt)
         x = (torch.rand(n, device=dev, dtype=torch.float64) * 2 - 1).to(dt)
         g = torch.randn(n, device=dev, dtype=torch.float64).to(dt)
@@ -435,14 +592,14 @@ def bench_fwd_bwd(ctx, dev, n=1 << 20):
 
         def plain():
             call("spops_spmv", ctx.handle, dbl(1.0), h.handle, vp(x.data_ptr()), dbl(0.0), vp(py.data_ptr()))
-            key, perm = torch.sort(cit, stable=True)
-            trp = torch.zeros(n + 1, dtype=torch.int32, device=dev)
-            trp[1:] = torch.cumsum(torch.bincount(key, minlength=n), 0)
-            AT = CSR_Matrix(n, n, trp, rows[perm].contiguous(), vt[perm].contiguous())
-            call("spops_spmv", ctx.handle, dbl(1.0), AT.device(ctx).handle, vp(g.data_ptr()), dbl(0.0),
-                 vp(pgx.data_ptr()))
+            # csr_transpose: CSR -> COO (row of every entry), rows and columns swapped, -> CSR
+            rows = torch.repeat_interleave(torch.arange(n, device=dev, dtype=torch.int32),
+                                           torch.diff(rpt.long()), output_size=nnz)
+            T = COO_Matrix(n, n, cit, rows, vt)  # row index = A's column: the transpose
+            th = T.device(ctx)
+            call("spops_spmv", ctx.handle, dbl(1.0), th.handle, vp(g.data_ptr()), dbl(0.0), vp(pgx.data_ptr()))
             keep["gv"] = g[rows.long()] * x[cit.long()]
-            keep["AT"] = AT
+            keep["T"] = T
 
         ctx.follow_torch()
         t_ours = _ev_ms(ours, 20)
@@ -465,15 +622,51 @@ def bench_fwd_bwd(ctx, dev, n=1 << 20):
 
         def rel(a, b):
             return float((a.double() - b.double()).abs().max() / b.double().abs().max().clamp_min(1e-300))
-        out[name] = {"ours_ms": round(t_ours, 4), "plain_ms": round(t_plain, 4),
-                     "speedup_vs_plain": round(t_plain / t_ours, 2), "autograd_ms": round(t_auto, 4),
-                     "normwise_rel_err": {"y": rel(y, py), "grad_x": rel(gx, pgx), "grad_v": rel(gv, keep["gv"])}}
+        fwd = 4 * (n + 1) + (4 + vs) * nnz + 2 * vs * n
+        sddmm = 4 * (n + 1) + 4 * nnz + 2 * vs * n + vs * nnz
+        alg = 2 * fwd + sddmm
+        res = {"ours_ms": round(t_ours, 4), "plain_ms": round(t_plain, 4),
+               "speedup_vs_plain": round(t_plain / t_ours, 2), "autograd_ms": round(t_auto, 4),
+               "normwise_rel_err": {"y": rel(y, py), "grad_x": rel(gx, pgx), "grad_v": rel(gv, keep["gv"])},
+               "algorithmic_bytes": alg, "value_refresh_bytes": (2 * vs + 4) * nnz}
+        if peak:
+            res["roofline"] = {"bound": "hbm", "achieved": round(alg / t_ours / 1e6, 1), "peak": peak, "unit": "GB/s",
+                               "frac": round(alg / t_ours / 1e6 / peak, 4),
+                               "frac_with_refresh": round((alg + (2 * vs + 4) * nnz) / t_ours / 1e6 / peak, 4)}
+        if cpu_ref and name == "f64":
+            try:
+                from oracle import Reference, reference_available
+                if reference_available():
+                    xh, gh, vh = x.cpu().numpy(), g.cpu().numpy(), vt.cpu().numpy()
+                    rows_h = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp.astype(np.int64)))
+                    with quiet_stdout():
+                        R = Reference(threads=os.cpu_count())
+                        yc, gc = np.zeros(n), np.zeros(n)
+
+                        def cpu_step():
+                            R.spmv_csr(rp, ci, vh, xh, 1.0, 0.0, None, flag=2, out=yc)
+                            trp, tci, tv = R.csr_transpose(rp, ci, vh, n)
+                            R.spmv_csr(trp, tci, tv, gh, 1.0, 0.0, None, flag=2, out=gc)
+                            return gh[rows_h] * xh[ci]
+                        cpu_step()
+                        ts = []
+                        for _ in range(3):
+                            t0 = time.perf_counter()
+                            cpu_step()
+                            ts.append(time.perf_counter() - t0)
+                    cms = float(np.median(ts)) * 1e3
+                    res["cpu_reference"] = {"ms": round(cms, 2), "cores": os.cpu_count(), "kind": "reference",
+                                            "sample": "whole step, median of 3: SpOps_csr, csr_transpose + "
+                                                      "SpOps_csr, numpy g_i x_j"}
+            except Exception as e:
+                res["cpu_reference"] = {"error": str(e)[:160]}
+        out[name] = res
         del pat, keep
         torch.cuda.empty_cache()
     return out
 
 
-def bench_spgemm(dev, cpu_ref: bool, n=524288):
+def bench_spgemm(dev, cpu_ref: bool, n=524288, peak=None):
     """LeSpGEMM C = A A^T on the planted-community matrix (2,048 communities,
     85 % in-community, row nnz lognormal mean 20): MinHash (64), LSH (16
     bands), clustering (8), cluster-wise kernel-3 SpGEMM."""
@@ -488,7 +681,12 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
     C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
     st = C.stats
     flops = st["flops"]
+    isz, vsz = arp.dtype.itemsize, 8
+    # compulsory bytes: read A and B (index + value per entry, row pointers),
+    # write C (index + value per entry, row pointers)
+    compulsory = (2 * ((isz + vsz) * len(aci) + isz * (n + 1)) + (isz + vsz) * int(C.num_nnzs) + isz * (n + 1))
     out = {"rows": n, "nnz_A": int(len(aci)), "nnz_C": int(C.num_nnzs), "flops": int(flops),
+           "compulsory_bytes": int(compulsory),
            "pipeline_ms": round(total, 3), "pipeline_GFLOP/s": round(flops / total / 1e6, 2),
            "stages_ms": {k: round(st[k], 3) for k in st if k.endswith("_ms")},
            "clusters": st.get("clusters"), "dense_clusters": st.get("dense_clusters")}
@@ -499,6 +697,11 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
     kms = _host_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 5, warm=2)
     out["spgemm_clustered_ms"] = round(kms, 3)
     out["spgemm_clustered_GFLOP/s"] = round(flops / kms / 1e6, 2)
+    if peak:
+        out["spgemm_clustered_roofline"] = {"bound": "hbm", "achieved": round(compulsory / kms / 1e6, 1), "peak": peak,
+                                            "unit": "GB/s", "frac": round(compulsory / kms / 1e6 / peak, 4),
+                                            "note": "compulsory bytes over the host-timed call (symbolic, numeric, "
+                                                    "to CSR)"}
     # row-wise LeSpGEMM (kernel 1 entries) and the top-16 Jaccard rows of A
     from sparseops_b200.spgemm import HashSpGEMMTopK, LeSpGEMM
     rms = _host_ms(lambda: LeSpGEMM(A, B, 1, False), 3, warm=1)
@@ -521,6 +724,57 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288):
                                                         "kind": "reference"}
                 ms = R.spgemm_rowwise_time(A64, B64, 1, 16, iters=1)
                 out["cpu_reference_topk16"] = {"ms": round(ms, 2), "cores": os.cpu_count(), "kind": "reference"}
+        except Exception as e:
+            out["cpu_reference_kernel3"] = {"error": str(e)[:160]}
+    del A, B, C
+    torch.cuda.empty_cache()
+    out["grouped"] = bench_spgemm_grouped(dev, cpu_ref, n, peak)
+    return out
+
+
+def bench_spgemm_grouped(dev, cpu_ref: bool, n=524288, peak=None):
+    """LeSpGEMM C = A A^T on rows in contiguous groups of 32 that share a
+    12-column block (A 524,288 x 196,608, row nnz lognormal mean 10, 0.5 % of
+    draws uniform): LSH pairs the rows of a group, so clusters hold up to 14
+    rows and most of them are dense under the reference's rule -- the
+    multi-row and dense parts of the hybrid accumulator at scale."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, synth
+    from sparseops_b200.spgemm import (LeSpGEMM_clustered, LeSpGEMM_lsh, hierarchical_clustering_v0_fast,
+                                       lsh_candidate_pairs_vector)
+    arp, aci, av, nc = synth.grouped_rows(n)
+    brp, bci, bv = synth.transpose(arp, aci, av, nc)
+    A = CSR_Matrix(n, nc, torch.from_numpy(arp).to(dev), torch.from_numpy(aci).to(dev), torch.from_numpy(av).to(dev))
+    B = CSR_Matrix(nc, n, torch.from_numpy(brp).to(dev), torch.from_numpy(bci).to(dev), torch.from_numpy(bv).to(dev))
+    total = _host_ms(lambda: LeSpGEMM_lsh(A, B, 64, 16, 7, 8), 3, warm=1)
+    C = LeSpGEMM_lsh(A, B, 64, 16, 7, 8)
+    st = C.stats
+    flops = st["flops"]
+    pairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
+    perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
+    kms = _host_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 5, warm=2)
+    compulsory = (2 * 16 * len(aci) + 8 * (n + 1) + 8 * (nc + 1) + 16 * int(C.num_nnzs) + 8 * (n + 1))
+    out = {"rows": n, "cols_A": nc, "nnz_A": int(len(aci)), "nnz_C": int(C.num_nnzs), "flops": int(flops),
+           "pairs": st.get("pairs"), "clusters": st.get("clusters"), "dense_clusters": st.get("dense_clusters"),
+           "largest_cluster": int(np.diff(offs).max()), "compulsory_bytes": int(compulsory),
+           "pipeline_ms": round(total, 3), "stages_ms": {k: round(st[k], 3) for k in st if k.endswith("_ms")},
+           "spgemm_clustered_ms": round(kms, 3), "spgemm_clustered_GFLOP/s": round(flops / kms / 1e6, 2)}
+    if peak:
+        out["spgemm_clustered_roofline"] = {"bound": "hbm", "achieved": round(compulsory / kms / 1e6, 1),
+                                            "peak": peak, "unit": "GB/s",
+                                            "frac": round(compulsory / kms / 1e6 / peak, 4)}
+    if cpu_ref:
+        try:
+            from oracle import Reference, reference_available
+            if reference_available():
+                R = Reference(threads=os.cpu_count())
+                ms = R.spgemm_kernel3_time((arp, aci, av), (brp, bci, bv, n), perm, offs, iters=2)
+                out["cpu_reference_kernel3"] = {"ms": round(ms, 2), "GFLOP/s": round(flops / ms / 1e6, 2),
+                                                "cores": os.cpu_count(), "kind": "reference"}
+                t0 = time.perf_counter()
+                pi, pj, ps = pairs.host()
+                R.hc(arp, aci, pi, pj, ps, 8)
+                out["cpu_reference_hc_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
         except Exception as e:
             out["cpu_reference_kernel3"] = {"error": str(e)[:160]}
     return out
@@ -688,14 +942,29 @@ def run_section(args):
     torch.cuda.set_device(0)
     ctx = default_context(0)
     with quiet_stdout():
+        peak, _ = peaks()
+        cpu = not args.no_cpu_baseline
         if args.section == "batched":
-            res = bench_batched(ctx, dev)
+            res = bench_batched(ctx, dev, peak=peak, cpu_ref=cpu)
         elif args.section == "fwd_bwd":
-            res = bench_fwd_bwd(ctx, dev)
+            res = bench_fwd_bwd(ctx, dev, peak=peak, cpu_ref=cpu)
         elif args.section == "mtx":
-            res = bench_mtx(not args.no_cpu_baseline)
+            res = bench_mtx(cpu)
         elif args.section == "spgemm":
-            res = bench_spgemm(dev, not args.no_cpu_baseline)
+            res = bench_spgemm(dev, cpu, peak=peak)
+        elif args.section == "laplacian":
+            res = bench_laplacian(ctx, dev, peak, cpu)
+        elif args.section == "formats":
+            from sparseops_b200 import CSR_Matrix, SpOps_csr
+            rp, ci, v, x = workload(args.rows)
+            n = len(rp) - 1
+            A = CSR_Matrix(n, n, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev),
+                           torch.from_numpy(v).to(dev))
+            xd = torch.from_numpy(x).to(dev)
+            yd = torch.zeros(n, dtype=torch.float64, device=dev)
+            SpOps_csr(1.0, A, xd, 0.0, yd)
+            torch.cuda.synchronize()
+            res = bench_formats(A, ctx, xd, yd, n, len(ci), spmv_bytes(n, n, len(ci)), peak, dev)
         elif args.section == "features":
             from sparseops_b200 import CSR_Matrix
             rp, ci, v, _ = workload(args.rows)
@@ -831,9 +1100,10 @@ def run_ours(args):
     extra = {}
     if rank == 0 and world == 1 and not args.no_extras:
         for key, fn in (("formats", lambda: bench_formats(A, ctx, xd, yd, n, nnz, nbytes, peak, dev)),
-                        ("batched", lambda: bench_batched(ctx, dev)),
-                        ("fwd_bwd", lambda: bench_fwd_bwd(ctx, dev)),
-                        ("spgemm", lambda: bench_spgemm(dev, not args.no_cpu_baseline)),
+                        ("laplacian", lambda: bench_laplacian(ctx, dev, peak, not args.no_cpu_baseline)),
+                        ("batched", lambda: bench_batched(ctx, dev, peak=peak, cpu_ref=not args.no_cpu_baseline)),
+                        ("fwd_bwd", lambda: bench_fwd_bwd(ctx, dev, peak=peak, cpu_ref=not args.no_cpu_baseline)),
+                        ("spgemm", lambda: bench_spgemm(dev, not args.no_cpu_baseline, peak=peak)),
                         ("mtx", lambda: bench_mtx(not args.no_cpu_baseline)),
                         ("features", lambda: bench_features(A, not args.no_cpu_baseline, rp, ci))):
             t0 = time.time()
@@ -855,9 +1125,12 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_name(n),
                    "nnz": int(nnz), "algorithmic_bytes_per_step": int(nbytes),
+                   "reference_bytes_per_spmv": ref_bytes_per_spmv(n, nnz),
                    "l2": "inputs larger than L2 (matrix ~1.3 GB vs 126 MB), no flush",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "pct_of_peak": round(100 * value / world / peak, 2),
+        # the same time on the reference's own byte count (x per entry, y read and written)
+        "reference_convention_GB/s": round(ref_bytes_per_spmv(n, nnz) / (ms * 1e-3) / 1e9, 2),
         "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
                      "peak_source": peak_kind,
@@ -888,7 +1161,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
-    ap.add_argument("--section", default="all", choices=["all", "batched", "fwd_bwd", "spgemm", "mtx", "features"],
+    ap.add_argument("--section", default="all", choices=["all", "laplacian", "formats", "batched", "fwd_bwd", "spgemm", "mtx", "features"],
                     help="run one extra section alone (profiling); the headline line needs 'all'")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-format, batched, fwd+bwd and SpGEMM sections")

@@ -4,7 +4,9 @@ or the oracle.
 
 * LeSpGEMM, C = A*A^T with A 524,288 x 524,288 (2,048 planted column
   communities, 85 % of a row's entries in its community, row nnz lognormal
-  mean 20, seed 5): the device MinHash signatures (64 hashes, seed 7), the LSH
+  mean 20, seed 5), and with A 524,288 x 196,608 in contiguous groups of 32
+  rows that share a 12-column block (multi-row clusters, most of them dense
+  under the reference's rule): the device MinHash signatures (64 hashes, seed 7), the LSH
   pair list (16 bands) and the clustering permutation / offsets (cluster size
   8) bit-equal to the reference's minhash_signatures_flat,
   lsh_candidate_pairs_vector and hierarchical_clustering_v0_fast on the same
@@ -36,12 +38,16 @@ pytestmark = pytest.mark.gpu
 N_SPGEMM = 524288
 
 
-@pytest.fixture(scope="module")
-def planted():
+def _spgemm_workload(name):
+    """(rows, A's columns, A, B = A^T) of a SpGEMM benchmark workload."""
     n = N_SPGEMM
-    arp, aci, av = synth.planted_communities(n, ncomm=2048, mean=20.0, seed=5)
-    brp, bci, bv = synth.transpose(arp, aci, av, n)
-    return n, (arp, aci, av), (brp, bci, bv)
+    if name == "planted":
+        arp, aci, av = synth.planted_communities(n, ncomm=2048, mean=20.0, seed=5)
+        nc = n
+    else:  # contiguous row groups sharing a 12-column block: multi-row and dense clusters
+        arp, aci, av, nc = synth.grouped_rows(n)
+    brp, bci, bv = synth.transpose(arp, aci, av, nc)
+    return n, nc, (arp, aci, av), (brp, bci, bv)
 
 
 @pytest.fixture(scope="module")
@@ -67,11 +73,12 @@ def _rows_sorted(rp, ci, v):
     return ci[order], v[order]
 
 
-def test_spgemm_full_config_vs_reference(cuda, planted, full_ref, orc):
+@pytest.mark.parametrize("workload", ["planted", "grouped"])
+def test_spgemm_full_config_vs_reference(cuda, full_ref, orc, workload):
     from sparseops_b200.spgemm import (LeSpGEMM_clustered, hierarchical_clustering_v0_fast,
                                        lsh_candidate_pairs_vector, minhash_signatures_flat)
-    n, (arp, aci, av), (brp, bci, bv) = planted
-    A, B = _dev_csr(arp, aci, av, n), _dev_csr(brp, bci, bv, n)
+    n, nc, (arp, aci, av), (brp, bci, bv) = _spgemm_workload(workload)
+    A, B = _dev_csr(arp, aci, av, nc), _dev_csr(brp, bci, bv, n)
     # MinHash signatures, 64 hashes, seed 7
     sig = minhash_signatures_flat(A, 64, 7)
     assert np.array_equal(sig, full_ref.minhash(arp, aci, 64, 7))
@@ -89,8 +96,11 @@ def test_spgemm_full_config_vs_reference(cuda, planted, full_ref, orc):
     for so in (0, 1):
         C = LeSpGEMM_clustered(A, B, perm, offs, sort_output=bool(so))
         crp, cci, cv = C.host()
+        C_dense = C.stats["dense_clusters"]
         del C
-        ref = full_ref.spgemm_kernel3((arp, aci, av), (brp, bci, bv), rperm, roffs, sort_output=bool(so))
+        ref = full_ref.spgemm_kernel3((arp, aci, av), (brp, bci, bv, n), rperm, roffs, sort_output=bool(so))
+        if workload == "grouped":
+            assert C_dense == ref["dense_clusters"] > 0
         assert np.array_equal(crp.astype(np.int64), ref["rp"])
         rci, rv = _rows_sorted(ref["rp"], ref["ci"], ref["v"])
         del ref
