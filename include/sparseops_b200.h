@@ -338,6 +338,12 @@ spops_status_t spops_lsh_pairs(spops_context_t ctx, spops_matrix_t A, int32_t k,
 /* Same from precomputed device signatures (lsh_candidate_pairs_from_flat_vector, :427). */
 spops_status_t spops_lsh_pairs_from_signatures(spops_context_t ctx, const void* sig, int64_t rows, int32_t k,
                                                int32_t bands, int32_t constrain, spops_pairs_t* pairs);
+/* A pair set from a caller's arrays i, j (int64) and score (double) of
+ * `count` elements, host (SPOPS_MEM_HOST) or device (SPOPS_MEM_DEVICE) memory;
+ * the arrays are copied.  The reference's clustering takes any such vector of
+ * pairs (hierarchical_clustering_v0_fast, include/spgemm_utility.h:742). */
+spops_status_t spops_pairs_create(spops_context_t ctx, const int64_t* i, const int64_t* j, const double* score,
+                                  int64_t count, spops_mem_t mem, spops_pairs_t* pairs);
 spops_status_t spops_pairs_count(spops_pairs_t pairs, int64_t* count);
 /* Device arrays of the pairs: i, j (int64) and score (double). */
 spops_status_t spops_pairs_arrays(spops_pairs_t pairs, const int64_t** i, const int64_t** j, const double** score);
@@ -352,6 +358,16 @@ spops_status_t spops_hierarchical_clustering(const int64_t* row_ptr, const int64
                                              const int64_t* pi, const int64_t* pj, const double* score,
                                              int64_t npairs, int64_t cluster_size, int64_t* permutation,
                                              int64_t* offsets, int64_t* nclusters);
+
+/* The same clustering on the device, from device pairs (spops_lsh_pairs) and
+ * A's device pattern: bit-identical permutation[rows] and offsets[nclusters +
+ * 1] (host arrays; offsets sized rows + 1).  Replaces
+ * hierarchical_clustering_v0_fast (include/spgemm_utility.h:742-915): the
+ * candidates run as prioritised tasks in rounds of root reservations, which
+ * reproduce the sequential merge order; pair lists that are not sorted
+ * i < j pairs take the host loop. */
+spops_status_t spops_pairs_cluster(spops_context_t ctx, spops_matrix_t A, spops_pairs_t pairs, int64_t cluster_size,
+                                   int64_t* permutation, int64_t* offsets, int64_t* nclusters);
 
 typedef struct {
   int64_t flops;             /* 2 x intermediate products (get_spgemm_flop, src/spgemm.cpp:24) */
@@ -389,7 +405,7 @@ spops_status_t spops_spgemm_rowwise(spops_context_t ctx, spops_matrix_t A, spops
  * similarity descending then column ascending.  Replaces HashSpGEMMTopK
  * (src/spgemm.cpp:708-842, src/spgemm_hash.cpp:168-318). */
 spops_status_t spops_spgemm_topk(spops_context_t ctx, spops_matrix_t A, int64_t top_k, spops_matrix_t* C);
-/* The whole LeSpGEMM pipeline: MinHash + LSH (device), clustering (host),
+/* The whole LeSpGEMM pipeline: MinHash + LSH (device), clustering (device),
  * cluster-wise SpGEMM (device). */
 spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_matrix_t B, int32_t k, int32_t bands,
                                 uint64_t seed, int64_t cluster_size, int32_t sort_output, double l2_budget_bytes,

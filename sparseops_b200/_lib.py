@@ -130,6 +130,8 @@ _SIGS = {
     "spops_matrix_download": [vp, vp, C.c_int, vp, i64],
     "spops_csr_set_values": [vp, vp],
     "spops_csr_upload_values": [vp, vp, vp],
+    "spops_pairs_cluster": [vp, vp, vp, i64, vp, vp, vp],
+    "spops_pairs_create": [vp, vp, vp, vp, i64, i32, vp],
     "spops_spmv_t": [vp, dbl, vp, vp, dbl, vp],
     "spops_sddmm": [vp, dbl, vp, vp, vp, vp],
     "spops_spmm": [vp, dbl, vp, vp, i64, i64, dbl, vp, i64],

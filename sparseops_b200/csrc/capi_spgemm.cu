@@ -123,6 +123,34 @@ spops_status_t spops_lsh_pairs(spops_context_t ctx, spops_matrix_t A, int32_t k,
   return s;
 }
 
+spops_status_t spops_pairs_create(spops_context_t ctx, const int64_t* i, const int64_t* j, const double* score,
+                                  int64_t count, spops_mem_t mem, spops_pairs_t* pairs) {
+  if (!ctx || !pairs || count < 0 || (count > 0 && (!i || !j || !score)))
+    return fail(SPOPS_ERR_INVALID, "spops_pairs_create: null or negative argument");
+  DeviceGuard g(ctx->device);
+  spops_pairs_s* P = new spops_pairs_s();
+  P->ctx = ctx;
+  P->count = count;
+  const size_t n = (size_t)std::max<int64_t>(count, 1);
+  spops_status_t s = P->pi.alloc(n * 8);
+  if (s == SPOPS_OK) s = P->pj.alloc(n * 8);
+  if (s == SPOPS_OK) s = P->score.alloc(n * 8);
+  const cudaMemcpyKind kind = mem == SPOPS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  if (s == SPOPS_OK && count > 0 &&
+      (cudaMemcpyAsync(P->pi.p, i, (size_t)count * 8, kind, ctx->stream) != cudaSuccess ||
+       cudaMemcpyAsync(P->pj.p, j, (size_t)count * 8, kind, ctx->stream) != cudaSuccess ||
+       cudaMemcpyAsync(P->score.p, score, (size_t)count * 8, kind, ctx->stream) != cudaSuccess ||
+       cudaStreamSynchronize(ctx->stream) != cudaSuccess))
+    s = fail(SPOPS_ERR_CUDA, "spops_pairs_create: copy failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (s != SPOPS_OK) {
+    P->release();
+    delete P;
+    return s;
+  }
+  *pairs = P;
+  return SPOPS_OK;
+}
+
 spops_status_t spops_pairs_count(spops_pairs_t P, int64_t* count) {
   if (!P || !count) return fail(SPOPS_ERR_INVALID, "spops_pairs_count: null argument");
   *count = P->count;
@@ -171,6 +199,28 @@ spops_status_t spops_hierarchical_clustering(const int64_t* row_ptr, const int64
   std::memcpy(permutation, perm.data(), perm.size() * 8);
   std::memcpy(offsets, offs.data(), offs.size() * 8);
   *nclusters = (int64_t)offs.size() - 1;
+  return SPOPS_OK;
+}
+
+spops_status_t spops_pairs_cluster(spops_context_t ctx, spops_matrix_t A, spops_pairs_t pairs, int64_t cluster_size,
+                                   int64_t* permutation, int64_t* offsets, int64_t* nclusters) {
+  if (!ctx || !A || !pairs || !nclusters || (A->rows > 0 && (!permutation || !offsets)))
+    return fail(SPOPS_ERR_INVALID, "spops_pairs_cluster: null argument");
+  if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "spops_pairs_cluster: A must be a CSR matrix");
+  DeviceGuard g(ctx->device);
+  const PairSet& P = *pairs;
+  PoolBuf perm(ctx), offs(ctx);
+  SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(A->rows, 1) * 8));
+  SPOPS_TRY(offs.alloc(((size_t)A->rows + 1) * 8));
+  int64_t ncl = 0;
+  SPOPS_TRY(hierarchical_clustering_device(ctx, A, P.pi.as<int64_t>(), P.pj.as<int64_t>(), P.score.as<double>(),
+                                           P.count, cluster_size, perm.as<int64_t>(), offs.as<int64_t>(), &ncl,
+                                           nullptr));
+  if (A->rows > 0)
+    SPOPS_CUDA(cudaMemcpyAsync(permutation, perm.p, (size_t)A->rows * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (offsets) SPOPS_CUDA(cudaMemcpyAsync(offsets, offs.p, ((size_t)ncl + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SPOPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  *nclusters = ncl;
   return SPOPS_OK;
 }
 
@@ -236,33 +286,20 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   s.lsh_ms = ms_since(t0);
   s.pairs = P.count;
   t0 = std::chrono::steady_clock::now();
-  const bool trace = std::getenv("SPOPS_TRACE") && std::getenv("SPOPS_TRACE")[0] == '1';
-  auto lap = [&](const char* what) {
-    if (trace) std::fprintf(stderr, "[spgemm_lsh] %-24s %9.3f ms\n", what, ms_since(t0));
-  };
-  std::vector<int64_t> pi((size_t)P.count), pj((size_t)P.count), perm, offs;
-  std::vector<double> ps((size_t)P.count);
-  const std::vector<int64_t>* rp = nullptr;
-  const std::vector<int64_t>* ci = nullptr;
-  st = host_pattern(ctx, A, &rp, &ci);
-  lap("pattern to host");
-  if (st == SPOPS_OK && P.count) {
-    cudaMemcpy(pi.data(), P.pi.p, pi.size() * 8, cudaMemcpyDeviceToHost);
-    cudaMemcpy(pj.data(), P.pj.p, pj.size() * 8, cudaMemcpyDeviceToHost);
-    cudaMemcpy(ps.data(), P.score.p, ps.size() * 8, cudaMemcpyDeviceToHost);
-  }
+  // clustering on the device; permutation and offsets stay there
+  PoolBuf perm(ctx), offs(ctx);
+  SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(A->rows, 1) * 8));
+  SPOPS_TRY(offs.alloc(((size_t)A->rows + 1) * 8));
+  int64_t ncl = 0;
+  st = hierarchical_clustering_device(ctx, A, P.pi.as<int64_t>(), P.pj.as<int64_t>(), P.score.as<double>(), P.count,
+                                      cluster_size, perm.as<int64_t>(), offs.as<int64_t>(), &ncl, nullptr);
   P.release();
-  lap("pairs to host");
-  if (st == SPOPS_OK)
-    st = hierarchical_clustering(rp->data(), ci->data(), A->rows, pi.data(), pj.data(), ps.data(), (int64_t)pi.size(),
-                                 cluster_size, perm, offs);
   if (st != SPOPS_OK) return st;
-  lap("clustering");
   s.hc_ms = ms_since(t0);
   Matrix* out = nullptr;
   SpgemmStats s2;
-  SPOPS_TRY(cluster_spgemm(ctx, A, B, perm.data(), offs.data(), (int64_t)offs.size() - 1, sort_output != 0,
-                           l2_budget_bytes, &out, &s2));
+  SPOPS_TRY(cluster_spgemm(ctx, A, B, perm.as<int64_t>(), offs.as<int64_t>(), ncl, sort_output != 0, l2_budget_bytes,
+                           &out, &s2));
   s2.minhash_ms = s.minhash_ms;
   s2.lsh_ms = s.lsh_ms;
   s2.hc_ms = s.hc_ms;

@@ -403,6 +403,12 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
 spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int64_t n, const int64_t* pi,
                                        const int64_t* pj, const double* ps, int64_t np, int64_t cluster_size,
                                        std::vector<int64_t>& perm, std::vector<int64_t>& offsets);
+// The same clustering on the device from device pairs (falls back to the
+// host loop for pair lists that are not sorted i < j pairs); permutation and
+// offsets written to device memory (offsets sized rows + 1).
+spops_status_t hierarchical_clustering_device(Context* ctx, Matrix* A, const int64_t* pi, const int64_t* pj,
+                                              const double* ps, int64_t np, int64_t cluster_size, int64_t* perm_d,
+                                              int64_t* offs_d, int64_t* ncl_out, int64_t* rounds_out);
 // cluster_out: C in the clustered form of A's clusters (SPOPS_FMT_VLCLUSTER,
 // rows in cluster order) instead of CSR in A's row order
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,

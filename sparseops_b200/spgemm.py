@@ -93,6 +93,34 @@ def hierarchical_clustering_v0_fast(rowptr, colids, num_rows: int, pairs, cluste
     return perm, offs[:nc.value + 1]
 
 
+def pairs_from_arrays(i, j, score, ctx=None) -> CandidatePairs:
+    """A device pair set from host arrays (i, j, score) of equal length: a
+    caller's own candidate pairs for the device clustering."""
+    ctx = (ctx or default_context()).follow_torch()
+    pi, pj = (np.ascontiguousarray(np.asarray(a, np.int64)) for a in (i, j))
+    ps = np.ascontiguousarray(np.asarray(score, np.float64))
+    if not (len(pi) == len(pj) == len(ps)):
+        raise ValueError("pairs_from_arrays: i, j and score differ in length")
+    out = vp()
+    call("spops_pairs_create", ctx.handle, _p(pi), _p(pj), _p(ps), i64(len(pi)), i32(1), C.byref(out))
+    return CandidatePairs(ctx, out)
+
+
+def hierarchical_clustering_device(csr: CSR_Matrix, pairs: CandidatePairs, cluster_size: int):
+    """hierarchical_clustering_v0_fast (include/spgemm_utility.h:742) on the
+    device: A's device pattern and device pairs in, the same (permutation,
+    offsets) as the host loop out (numpy arrays)."""
+    h = csr.device()
+    ctx = h.ctx.follow_torch()
+    n = int(csr.num_rows)
+    perm = np.empty(n, np.int64)
+    offs = np.empty(n + 1, np.int64)
+    nc = C.c_int64()
+    call("spops_pairs_cluster", ctx.handle, h.handle, pairs.handle, i64(cluster_size), _p(perm), _p(offs),
+         C.byref(nc))
+    return perm, offs[:nc.value + 1]
+
+
 class SpGEMMResult(DeviceCSR):
     """C = A*B as a device CSR handle; arrays downloaded on first access."""
 
