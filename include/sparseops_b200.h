@@ -512,11 +512,20 @@ spops_status_t spops_matrix_tile_features(spops_context_t ctx, spops_matrix_t cs
  *   mode 1: timed -- converts to each candidate (CSR, SELL-C-R and
  *     SELL-C-sigma with C = 32, CSR5, and DIA / BSR where the features allow
  *     them), runs a few SpMVs of each on the context stream, and returns the
- *     fastest.
+ *     fastest;
+ *   mode 2: learned -- a decision tree over derived features, fitted on
+ *     seeded matrices whose SpMV time this library measured on a B200 in
+ *     every mode-1 candidate (sparseops_b200/selector.py); the features'
+ *     cost, no conversion or timing.  The model the reference's feature
+ *     output (src/sparse_features.cpp:1225) is meant for.
  * *params receives the conversion parameters for spops_convert; ms (may be
  * NULL) the measured time per SpMV of the choice (mode 1; 0 in mode 0). */
 spops_status_t spops_select_format(spops_context_t ctx, spops_matrix_t csr, int32_t mode, spops_format_t* format,
                                    spops_format_params_t* params, double* ms);
+/* Mode 2's choice from features already computed (host only: no device
+ * work), e.g. from spops_matrix_features or a stored feature file. */
+spops_status_t spops_select_format_from_features(const spops_features_t* features, spops_format_t* format,
+                                                 spops_format_params_t* params);
 
 /* ------------------------------------------------ clustered (VLength) form */
 /* CSR_VlengthCluster (spgemm_cluster.h:108-143) as a handle of format

@@ -132,6 +132,7 @@ _SIGS = {
     "spops_csr_upload_values": [vp, vp, vp],
     "spops_pairs_cluster": [vp, vp, vp, i64, vp, vp, vp],
     "spops_pairs_create": [vp, vp, vp, vp, i64, i32, vp],
+    "spops_select_format_from_features": [vp, vp, vp],
     "spops_spmv_t": [vp, dbl, vp, vp, dbl, vp],
     "spops_sddmm": [vp, dbl, vp, vp, vp, vp],
     "spops_spmm": [vp, dbl, vp, vp, i64, i64, dbl, vp, i64],

@@ -535,6 +535,10 @@ spops_status_t spops_select_format(spops_context_t ctx, spops_matrix_t csr, int3
   if (ms) *ms = 0.0;
   const int64_t mn = std::min(f.rows, f.cols);
   const bool dia_dense = f.ndiags > 0 && (double)f.nnz >= 0.5 * (double)f.ndiags * (double)mn;
+  if (mode == 2) {  // learned: the fitted decision tree (csrc/selector.cpp)
+    tree_select(f, format, params);
+    return SPOPS_OK;
+  }
   if (mode == 0) {
     if (f.ndiags <= 64 && dia_dense) {
       *format = SPOPS_FMT_DIA;

@@ -400,6 +400,10 @@ spops_status_t csr_sddmm(Context* ctx, Matrix* A, double alpha, const void* g, c
 spops_status_t minhash_signatures(Context* ctx, Matrix* A, int k, uint64_t seed, uint64_t* sig);
 spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, int bands, bool constrain,
                          PairSet* out);
+// Learned format choice (csrc/selector.cpp): the fitted decision tree over
+// derived features; fills spops_convert parameters.
+void tree_select(const spops_features_t& f, spops_format_t* format, spops_format_params_t* params);
+
 spops_status_t hierarchical_clustering(const int64_t* rp, const int64_t* ci, int64_t n, const int64_t* pi,
                                        const int64_t* pj, const double* ps, int64_t np, int64_t cluster_size,
                                        std::vector<int64_t>& perm, std::vector<int64_t>& offsets);

@@ -416,16 +416,18 @@ def matrix_tile_features(csr: CSR_Matrix, num_blocks: int = 256, maps: bool = Fa
 _FORMAT_NAMES = {v: k for k, v in _lib.FORMATS.items()}
 
 
-def select_format(csr: CSR_Matrix, timed: bool = False) -> dict:
+def select_format(csr: CSR_Matrix, timed: bool = False, learned: bool = False) -> dict:
     """Storage format for SpMV with this matrix on this GPU: rules on the
-    features (timed=False) or the fastest of the candidate formats measured
-    on the device (timed=True).  Returns {"format", "params", "ms"}; the
-    params are the spops_convert parameters (see convert_to)."""
+    features (default), the fastest of the candidate formats measured on the
+    device (timed=True), or the fitted decision tree over the features
+    (learned=True).  Returns {"format", "params", "ms"}; the params are the
+    spops_convert parameters (see convert_to)."""
     h = csr.device()
     fmt = C.c_int()
     p = FormatParams()
     ms = C.c_double()
-    call("spops_select_format", h.ctx.follow_torch().handle, h.handle, C.c_int32(1 if timed else 0), C.byref(fmt),
+    mode = 1 if timed else (2 if learned else 0)
+    call("spops_select_format", h.ctx.follow_torch().handle, h.handle, C.c_int32(mode), C.byref(fmt),
          C.byref(p), C.byref(ms))
     params = {k: int(getattr(p, k)) for k, _ in FormatParams._fields_ if k != "reserved" and getattr(p, k)}
     return {"format": _FORMAT_NAMES[fmt.value], "params": params, "ms": ms.value}
