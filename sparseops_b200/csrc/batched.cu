@@ -55,8 +55,8 @@ struct BatchMat {
   int* pcounter;
   int64_t C;
   int32_t colmajor;
-  int32_t pad0;
-  int64_t rows;
+  int32_t band;  // x window half-width of the CSR segments (0: none)
+  int64_t rows, cols;
   // vectors
   const void* x;
   void* y;
@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(con
                                                                V beta, bool bz,
                                                                unsigned long long* __restrict__ next_item) {
   __shared__ V prod_all[KT == 1 ? kBatchBlock / 32 : 1][KT == 1 ? 2 * kCsrCap : 1];
+  __shared__ V xs_all[KT == 1 ? kBatchBlock / 32 : 1][KT == 1 ? kBandWin : 1];  // staged x windows
   extern __shared__ __align__(16) unsigned char batch_dyn_smem[];  // SpMM: one SpmmStage per warp
   const int lane = threadIdx.x & 31;
   V* prod = prod_all[KT == 1 ? threadIdx.x >> 5 : 0];
@@ -109,7 +110,8 @@ __global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(con
       if (it.kind == 0) {
         csr_segment_spmv<I, V, 8>(M.seg[it.idx], it.idx, static_cast<const I*>(M.ci), static_cast<const V*>(M.val),
                                   static_cast<const I*>(M.rp), static_cast<const V*>(M.x), static_cast<V*>(M.y),
-                                  alpha, beta, bz, prod, static_cast<V*>(M.partial), M.counter, lane);
+                                  alpha, beta, bz, prod, static_cast<V*>(M.partial), M.counter, lane, M.band,
+                                  M.cols, xs_all[KT == 1 ? threadIdx.x >> 5 : 0]);
       } else if (it.kind == 1) {
         if (M.colmajor)
           padded_rows32<I, V, true>(it.idx * 32, static_cast<const I*>(M.pcol), static_cast<const V*>(M.pval),
@@ -418,6 +420,8 @@ spops_status_t build_table(Batch* B) {
     t.partial = B->k > 1 ? B->spmm_partial[m].p : A->plan.partial.p;
     t.counter = A->plan.counter.as<int>();
     t.rows = A->rows;
+    t.cols = A->cols;
+    t.band = B->k == 1 && A->plan.band > 0 ? A->plan.band : 0;
     if (B->tile_ok[m]) {
       const CsrTiles& D = A->plan.tiles;
       t.tile_row = D.tile_row.as<int64_t>();
@@ -511,6 +515,58 @@ spops_status_t launch_any(Batch* B, double alpha, double beta, cudaStream_t st) 
   return launch_batch<int64_t, float>(B, alpha, beta, st);
 }
 
+// Entries within 16, 32 and 64 (kBandMax) of the diagonal (warp per row).
+template <typename I>
+__global__ void band_count_kernel(const I* __restrict__ rp, const I* __restrict__ ci, int64_t n,
+                                  unsigned long long* __restrict__ cnt) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  unsigned long long c[3] = {0, 0, 0};
+  if (r < n)
+    for (int64_t k = (int64_t)rp[r] + lane; k < (int64_t)rp[r + 1]; k += 32) {
+      const int64_t d = (int64_t)ci[k] - r;
+      const int64_t a = d < 0 ? -d : d;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) c[b] += a <= (16 << b) ? 1 : 0;
+    }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    for (int o = 16; o; o >>= 1) c[b] += __shfl_xor_sync(0xffffffffu, c[b], o);
+    if (lane == 0 && c[b]) atomicAdd(cnt + b, c[b]);
+  }
+}
+
+// Half-width of the x window the batch's CSR segments stage: the smallest of
+// 16 .. kBandMax that holds 90 % of the entries the widest one holds, when
+// that is at least a tenth of all entries; otherwise 0 (no staging).
+spops_status_t csr_band(Context* ctx, Matrix* A) {
+  if (A->plan.band >= 0) return SPOPS_OK;
+  A->plan.band = 0;
+  if (A->nnz == 0 || A->rows == 0) return SPOPS_OK;
+  cudaStream_t st = ctx->stream;
+  PoolBuf cnt(ctx);
+  SPOPS_TRY(cnt.alloc(32));
+  SPOPS_CUDA(cudaMemsetAsync(cnt.p, 0, 32, st));
+  const unsigned grid = (unsigned)((A->rows * 32 + 255) / 256);
+  if (A->itype == SPOPS_INDEX_I32)
+    band_count_kernel<int32_t><<<grid, 256, 0, st>>>(A->row.as<int32_t>(), A->col.as<int32_t>(), A->rows,
+                                                     cnt.as<unsigned long long>());
+  else
+    band_count_kernel<int64_t><<<grid, 256, 0, st>>>(A->row.as<int64_t>(), A->col.as<int64_t>(), A->rows,
+                                                     cnt.as<unsigned long long>());
+  SPOPS_LAUNCH_CHECK();
+  unsigned long long h[3];
+  SPOPS_CUDA(cudaMemcpyAsync(h, cnt.p, 24, cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  if ((double)h[2] < 0.1 * (double)A->nnz) return SPOPS_OK;
+  for (int b = 0; b < 3; ++b)
+    if ((double)h[b] >= 0.9 * (double)h[2]) {
+      A->plan.band = 16 << b;
+      break;
+    }
+  return SPOPS_OK;
+}
+
 spops_status_t prepare(Batch* B) {
   if (!B->dirty) return SPOPS_OK;
   B->tile_ok.assign((size_t)B->count, 0);
@@ -519,6 +575,7 @@ spops_status_t prepare(Batch* B) {
   for (int64_t m = 0; m < B->count; ++m) {
     Matrix* A = B->src[m];
     if (!A->plan.ready) SPOPS_TRY(csr_analyse(B->ctx, A));
+    if (B->k == 1) SPOPS_TRY(csr_band(B->ctx, A));
     // k = 8, 16, 32 over X rows at most 2k wide, vector loads aligned: register tiles
     const BatchMat& h = B->host[m];
     const size_t vs = A->vsize();

@@ -211,11 +211,13 @@ struct CsrPlan {
   DevBuf seg;              // CsrSeg [nblocks]
   CsrTiles tiles;          // built on first use by the tile kernel
   CsrWin win;              // built on first use by the window kernel
+  int band = -1;           // half-width of the x window a segment stages (0 none, -1 not measured)
   void release() {
     blk_row.release(); blk_chunk.release(); partial.release(); counter.release(); seg.release();
     tiles.release();
     win.release();
     ready = false;
+    band = -1;
   }
 };
 

@@ -11,6 +11,11 @@ namespace spops {
 // kCsrRowCap rows; a long row is cut into chunks of kCsrCap entries.
 constexpr int kCsrCap = 256;
 constexpr int kCsrRowCap = 32;
+// Largest half-width of the x window a segment stages in shared memory
+// (csr_segment_spmv with band > 0): rows [r0, r0 + nr) read x[r0 - band,
+// r0 + nr + band) from the window, every other column from global memory.
+constexpr int kBandMax = 64;
+constexpr int kBandWin = kCsrRowCap + 2 * kBandMax;
 
 // Padded rows (SELL / ELL): stored rows longer than kPadLong slots are summed
 // by pieces of kPadPiece slots, one warp per piece.
@@ -53,17 +58,34 @@ __device__ __forceinline__ void warp_chunk_finish(V sum, int64_t slot, int64_t f
 // of kItems entries per lane per round, every gather of the round issued
 // before use, products to shared memory, then t lanes reduce each row.  Long
 // chunk: register sum, warp reduction, chunk combine.
+//
+// band > 0 (x window staging): the warp first copies x[r0 - band, r0 + nr +
+// band) (coalesced, out-of-range slots zero) into xs, its kBandWin-entry
+// shared-memory slice; a column inside the window is read from there, any
+// other with a global gather.  The products and their order are unchanged.
 template <typename I, typename V, int kItems>
 __device__ __forceinline__ void csr_segment_spmv(const CsrSeg& d, int64_t j, const I* __restrict__ ci,
                                                  const V* __restrict__ val, const I* __restrict__ rp,
                                                  const V* __restrict__ x, V* __restrict__ y, V alpha, V beta,
                                                  bool bz, V* __restrict__ prod, V* __restrict__ partial,
-                                                 int* __restrict__ counter, int lane) {
+                                                 int* __restrict__ counter, int lane, int band = 0,
+                                                 int64_t ncols = 0, V* __restrict__ xs = nullptr) {
   const int m = (int)(d.p1 - d.p0);
   const bool is_long = d.chunk >= 0;
   const I* cseg = ci + d.p0;
   const V* vseg = val + d.p0;
   V lsum = V(0);
+  const int64_t w0 = (int64_t)d.r0 - band;
+  int W = 0;
+  if (band > 0) {
+    W = (is_long ? 1 : d.nr) + 2 * band;
+    __syncwarp();  // the previous item's reads of xs are done
+    for (int t = lane; t < W; t += 32) {
+      const int64_t c = w0 + t;
+      xs[t] = (c >= 0 && c < ncols) ? ld_gather(x + c) : V(0);
+    }
+    __syncwarp();
+  }
   for (int base = 0; base < m; base += 32 * kItems) {
     I c[kItems];
     V a[kItems];
@@ -79,7 +101,8 @@ __device__ __forceinline__ void csr_segment_spmv(const CsrSeg& d, int64_t j, con
     for (int it = 0; it < kItems; ++it) {
       const int k = base + lane + 32 * it;
       if (k < m) {
-        const V p = a[it] * ld_gather(x + c[it]);
+        const int64_t o = (int64_t)c[it] - w0;
+        const V p = a[it] * ((o >= 0 && o < W) ? xs[o] : ld_gather(x + c[it]));
         if (is_long) lsum += p; else prod[k] = p;
       }
     }

@@ -209,10 +209,10 @@ void run_all() {
     check_y("SpOps_dia from host arrays", B, xb, yb0, alpha, beta, yb);
   }
 
-  // upload on every call
+  // upload on every call, then back to the default mode
   spops_b200::set_cache(false);
   run("SpOps_csr without cache", [&](V a, const V* xx, V b, V* yy) { SpOps_csr(a, A, xx, b, yy); });
-  spops_b200::set_cache(true);
+  spops_b200::set_cache_mode(spops_b200::CacheMode::Pattern);
 
   delete_host_matrix(back);
   delete_host_matrix(coo);
