@@ -879,10 +879,10 @@ __global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __
   key[c] = bytes <= lim.wbytes[5] ? 5 : (bytes <= lim.wbytes[6] ? 6 : 7);
 }
 
-// sort path (spgemm_sort.cuh): bin q (R = 2^q lanes' worth of keys, q = 0..5)
+// sort path (spgemm_sort.cuh): bin q (R = 2^q keys per lane, q = 0..6)
 // for a cluster with at most 32 * 2^q products and kSortCols columns whose
 // output columns fit the key beside the product index; settled[c] = 1 then.
-constexpr int kSortBins = 6;
+constexpr int kSortBins = 7;
 
 __global__ void sort_bin_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ cptr, int64_t ncl,
                                 int64_t bcols, unsigned char* __restrict__ settled, uint32_t* __restrict__ key,
@@ -906,7 +906,7 @@ __global__ void sort_bin_kernel(const int64_t* __restrict__ flops, const int64_t
 }
 
 // room in each cluster's output slab: its product count on the sort path (at
-// most 32 * 2^5, and never below its distinct columns whatever B holds), the
+// most 32 * 2^6, and never below its distinct columns whatever B holds), the
 // symbolic count otherwise; values: that times the cluster size
 __global__ void slab_cap_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ nz,
                                 const unsigned char* __restrict__ settled, const int64_t* __restrict__ offsets,
@@ -1443,7 +1443,8 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
       case 2: SPOPS_SORT_LAUNCH(4); break;
       case 3: SPOPS_SORT_LAUNCH(8); break;
       case 4: SPOPS_SORT_LAUNCH(16); break;
-      default: SPOPS_SORT_LAUNCH(32); break;
+      case 5: SPOPS_SORT_LAUNCH(32); break;
+      default: SPOPS_SORT_LAUNCH(64); break;
     }
 #undef SPOPS_SORT_LAUNCH
     SPOPS_LAUNCH_CHECK();

@@ -19,7 +19,7 @@
 // (room for P columns), columns ascending, values [column x csz] with the
 // rows of the cluster interleaved -- the same layout the hash kernels write.
 //
-// Limits (the caller bins clusters accordingly): P <= 32*R, the cluster has
+// Limits (the caller bins clusters accordingly): P <= 32*R (R <= 64), the cluster has
 // at most kSortCols columns, and B's column count fits the key
 // (cols <= 2^(32 - tbits) - 1, tbits = log2(32*R)).
 #pragma once
@@ -144,13 +144,13 @@ __global__ void __launch_bounds__(32 * kSortWarps)
   const uint32_t tmask = (1u << tbits) - 1u;
   // column starts in this lane's sorted run; the distinct-column count
   const uint32_t prev_last = __shfl_up_sync(0xffffffffu, key[R - 1], 1);
-  unsigned first = 0;  // bit s: sorted position lane*R + s starts a column
+  unsigned long long first = 0;  // bit s: sorted position lane*R + s starts a column
   int cnt = 0;
 #pragma unroll
   for (int s = 0; s < R; ++s) {
     const uint32_t prev = s == 0 ? (lane == 0 ? kNone : prev_last) : key[s - 1];
     const bool f = key[s] != kNone && (s == 0 && lane == 0 ? true : (prev >> tbits) != (key[s] >> tbits));
-    first |= (f ? 1u : 0u) << s;
+    first |= (f ? 1ULL : 0ULL) << s;
     cnt += f ? 1 : 0;
   }
   int incl = cnt;
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(32 * kSortWarps)
     int r = base;
 #pragma unroll
     for (int s = 0; s < R; ++s)
-      if (first >> s & 1u) ccol[co + r++] = (int32_t)(key[s] >> tbits);
+      if (first >> s & 1ULL) ccol[co + r++] = (int32_t)(key[s] >> tbits);
   }
   // values, one row of the cluster at a time
   for (int64_t l = 0; l < csz; ++l) {
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(32 * kSortWarps)
         const int32_t t = (int32_t)(key[s] & tmask);
         const int j = sort_find_col(off, nj, t);
         const V v = avals[vbase + (int64_t)j * csz + l] * bv[start[j] + (t - off[j])];
-        if (first >> s & 1u) {
+        if (first >> s & 1ULL) {
           if (seen) {
             const V o = (csz == 1 && drop && fabs((double)run) < 1e-12) ? V(0) : run;
             cval[cvo + (int64_t)r * csz + l] = o;
