@@ -376,6 +376,7 @@ spops_status_t spops_matrix_touch(spops_matrix_t A) {
   if (!A) return fail(SPOPS_ERR_INVALID, "spops_matrix_touch: null matrix");
   A->tr.values_fresh = false;  // the row-ordered CSR plans depend on the pattern only
   A->plan.win.values_fresh = false;  // the window plan keeps a copy of the values
+  A->pad.tails_fresh = false;        // the padded tails keep a copy of the values
   return SPOPS_OK;
 }
 

@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(256) padded_win_kernel(
     const int* __restrict__ row_len, const I* __restrict__ reorder, int64_t n, const V* __restrict__ x,
     V* __restrict__ y, V alpha, V beta, bool bz, const PadWin* __restrict__ wins, int64_t nwin,
     V* __restrict__ wpartial, int* __restrict__ wcounter, int64_t npieces, const PadPiece* __restrict__ pieces,
-    V* __restrict__ partial, int* __restrict__ counter) {
+    V* __restrict__ partial, int* __restrict__ counter, const int* __restrict__ head, const I* __restrict__ tcol,
+    const V* __restrict__ tval) {
   const int lane = threadIdx.x & 31;
   const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   if (w >= nwin) {
@@ -199,6 +200,8 @@ __global__ void __launch_bounds__(256) padded_win_kernel(
   if (i < n) {
     len = row_len[i];
     if (len > kPadLong || len < 0) len = 0;  // long rows: pieces
+    const int h = head[W.chunk];
+    if (len > h) len = h;  // the slots beyond the head are tail entries
   }
   auto store = [&](int r, V s) {
     const int64_t row = i0 + r;
@@ -210,8 +213,28 @@ __global__ void __launch_bounds__(256) padded_win_kernel(
     return;
   }
   V* part = wpartial + (W.first + W.widx) * 32;
-  padded_window32<I, V>(chunk_off[W.chunk], len, W.widx * kPadWindow, col, val, x, lane,
-                        [&](int r, V s) { part[r] = s; });
+  if (W.tail >= 0) {  // one row's tail entries, read contiguously, 4 per lane per step
+    V s0 = V(0), s1 = V(0), s2 = V(0), s3 = V(0);
+    const I* tc = tcol + W.tail;
+    const V* tv = tval + W.tail;
+    int e = lane;
+    for (; e + 96 < W.tlen; e += 128) {
+      const I c0 = ld_stream(tc + e), c1 = ld_stream(tc + e + 32), c2 = ld_stream(tc + e + 64),
+              c3 = ld_stream(tc + e + 96);
+      const V v0 = ld_stream(tv + e), v1 = ld_stream(tv + e + 32), v2 = ld_stream(tv + e + 64),
+              v3 = ld_stream(tv + e + 96);
+      s0 += v0 * ld_gather(x + c0);
+      s1 += v1 * ld_gather(x + c1);
+      s2 += v2 * ld_gather(x + c2);
+      s3 += v3 * ld_gather(x + c3);
+    }
+    for (; e < W.tlen; e += 32) s0 += ld_stream(tv + e) * ld_gather(x + ld_stream(tc + e));
+    const V s = warp_sum((s0 + s1) + (s2 + s3));
+    part[lane] = lane == W.tlane ? s : V(0);
+  } else {
+    padded_window32<I, V>(chunk_off[W.chunk], len, W.widx * kPadWindow, col, val, x, lane,
+                          [&](int r, V s) { part[r] = s; });
+  }
   __syncwarp();
   int last = 0;
   if (lane == 0) {
@@ -229,9 +252,16 @@ __global__ void __launch_bounds__(256) padded_win_kernel(
   }
 }
 
-// windows per 32-row chunk: ceil(longest row that is not long / kPadWindow)
-__global__ void pad_win_count_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks,
-                                     int64_t* __restrict__ nw) {
+// Entries of one tail window (a longer tail is cut into several).
+constexpr int kTailWin = 1024;
+
+// Per 32-row chunk (a warp): the head width h (the fourth-longest row's
+// length, rows longer than kPadLong left to pieces), the tail rows (longer
+// than h, at most three), their entries, and the chunk's windows: head
+// windows of kPadWindow slots (at least one) and tail windows of kTailWin
+// entries.
+__global__ void pad_head_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks, int* __restrict__ head,
+                                int64_t* __restrict__ ntr, int64_t* __restrict__ nte, int64_t* __restrict__ nw) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t c = t >> 5;
   const int lane = threadIdx.x & 31;
@@ -239,15 +269,91 @@ __global__ void pad_win_count_kernel(const int* __restrict__ row_len, int64_t n,
   const int64_t i = c * 32 + lane;
   int len = i < n ? row_len[i] : 0;
   if (len > kPadLong || len < 0) len = 0;
-  const unsigned m = __reduce_max_sync(0xffffffffu, (unsigned)len);
-  if (lane == 0) nw[c] = m > (unsigned)kPadWindow ? ((int64_t)m + kPadWindow - 1) / kPadWindow : 1;
+  unsigned key = (unsigned)len;  // descending across the lanes
+#pragma unroll
+  for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+    for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+      const unsigned other = __shfl_xor_sync(0xffffffffu, key, jj);
+      const bool first_half = (lane & kk) == 0, lower = (lane & jj) == 0;
+      key = (lower == first_half) ? (key > other ? key : other) : (key < other ? key : other);
+    }
+  }
+  const int h = (int)__shfl_sync(0xffffffffu, key, 3);
+  const int tl = len > h ? len - h : 0;
+  const unsigned rows = __reduce_add_sync(0xffffffffu, tl > 0 ? 1u : 0u);
+  const unsigned ents = __reduce_add_sync(0xffffffffu, (unsigned)tl);
+  const unsigned twin = __reduce_add_sync(0xffffffffu, (unsigned)((tl + kTailWin - 1) / kTailWin));
+  if (lane == 0) {
+    head[c] = h;
+    ntr[c] = rows;
+    nte[c] = ents;
+    nw[c] = (h > kPadWindow ? ((int64_t)h + kPadWindow - 1) / kPadWindow : 1) + twin;
+  }
 }
 
-__global__ void pad_win_fill_kernel(const int64_t* __restrict__ nw, const int64_t* __restrict__ off, int64_t nchunks,
-                                    PadWin* __restrict__ wins) {
-  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// The chunk's window list and tail records (offsets from exclusive scans of
+// pad_head_kernel's counts).
+__global__ void pad_win_fill_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks,
+                                    const int* __restrict__ head, const int64_t* __restrict__ woff,
+                                    const int64_t* __restrict__ nw, const int64_t* __restrict__ troff,
+                                    const int64_t* __restrict__ teoff, PadWin* __restrict__ wins,
+                                    PadTail* __restrict__ tails) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t c = t >> 5;
+  const int lane = threadIdx.x & 31;
   if (c >= nchunks) return;
-  for (int64_t q = 0; q < nw[c]; ++q) wins[off[c] + q] = PadWin{c, off[c], (int32_t)q, (int32_t)nw[c]};
+  const int64_t i = c * 32 + lane;
+  int len = i < n ? row_len[i] : 0;
+  if (len > kPadLong || len < 0) len = 0;
+  const int h = head[c];
+  const int tl = len > h ? len - h : 0;
+  const int tw = (tl + kTailWin - 1) / kTailWin;
+  // exclusive prefixes over the lanes: tail rows, entries, tail windows
+  int pr = tl > 0 ? 1 : 0, pe = tl, pw = tw;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ur = __shfl_up_sync(0xffffffffu, pr, o), ue = __shfl_up_sync(0xffffffffu, pe, o),
+              uw = __shfl_up_sync(0xffffffffu, pw, o);
+    if (lane >= o) {
+      pr += ur;
+      pe += ue;
+      pw += uw;
+    }
+  }
+  pr -= tl > 0 ? 1 : 0;
+  pe -= tl;
+  pw -= tw;
+  const int nh = h > kPadWindow ? (h + kPadWindow - 1) / kPadWindow : 1;
+  const int64_t first = woff[c];
+  const int32_t total = (int32_t)nw[c];
+  for (int q = lane; q < nh; q += 32) wins[first + q] = PadWin{c, first, q, total, -1, 0, 0};
+  if (tl > 0) {
+    const int64_t start = teoff[c] + pe;
+    tails[troff[c] + pr] = PadTail{i, start, h, tl};
+    for (int m = 0; m < tw; ++m) {
+      const int32_t len_m = tl - m * kTailWin < kTailWin ? tl - m * kTailWin : kTailWin;
+      wins[first + nh + pw + m] = PadWin{c, first, nh + pw + m, total, start + (int64_t)m * kTailWin, len_m, lane};
+    }
+  }
+}
+
+// Copy every tail's slots from the column-major chunks (warp per tail).
+template <typename I, typename V>
+__global__ void pad_tail_copy_kernel(const PadTail* __restrict__ tails, int64_t ntails,
+                                     const int64_t* __restrict__ chunk_off, const I* __restrict__ col,
+                                     const V* __restrict__ val, I* __restrict__ tcol, V* __restrict__ tval) {
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= ntails) return;
+  const PadTail T = tails[t];
+  const int64_t c = T.row >> 5;
+  const int64_t base = chunk_off[c] + (T.row - c * 32);
+  for (int e = lane; e < T.len; e += 32) {
+    const int64_t src = base + 32 * (int64_t)(T.from + e);
+    tcol[T.start + e] = col[src];
+    tval[T.start + e] = val[src];
+  }
 }
 
 // ------------------------------------------------------------------ DIA
@@ -710,21 +816,52 @@ spops_status_t padded_finish_t(Context* ctx, Matrix* M) {
   }
   SPOPS_CUDA(cudaStreamSynchronize(st));
   if (P.C == 32 && M->layout == SPOPS_COL_MAJOR && n > 0) {
-    // step windows of the 32-row chunks (np / off reused: one entry per chunk)
+    // heads, tails and windows of the 32-row chunks
     const int64_t nch = (n + 31) / 32;
-    pad_win_count_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, np);
+    PoolBuf cnt(ctx), offs(ctx), tmp(ctx);
+    SPOPS_TRY(cnt.alloc((size_t)(nch + 1) * 3 * 8));
+    SPOPS_TRY(offs.alloc((size_t)(nch + 1) * 3 * 8));
+    int64_t* ntr = cnt.as<int64_t>();
+    int64_t* nte = ntr + (nch + 1);
+    int64_t* nwc = nte + (nch + 1);
+    int64_t* troff = offs.as<int64_t>();
+    int64_t* teoff = troff + (nch + 1);
+    int64_t* woff = teoff + (nch + 1);
+    SPOPS_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, st));
+    SPOPS_TRY(P.head.alloc((size_t)nch * 4));
+    pad_head_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, P.head.as<int>(), ntr, nte,
+                                                         nwc);
     SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, np, off, nch, st));
-    int64_t h[2];
-    SPOPS_TRY(download(ctx, &h[0], off + nch - 1, 1));
-    SPOPS_TRY(download(ctx, &h[1], np + nch - 1, 1));
-    P.nwin = h[0] + h[1];
+    size_t cs = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cs, ntr, troff, nch + 1, st));
+    SPOPS_TRY(tmp.alloc(cs + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, ntr, troff, nch + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, nte, teoff, nch + 1, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, nwc, woff, nch + 1, st));
+    int64_t h[3];
+    SPOPS_TRY(download(ctx, &h[0], troff + nch, 1));
+    SPOPS_TRY(download(ctx, &h[1], teoff + nch, 1));
+    SPOPS_TRY(download(ctx, &h[2], woff + nch, 1));
+    P.ntails = h[0];
+    P.ntail_entries = h[1];
+    P.nwin = h[2];
     SPOPS_TRY(P.win.alloc((size_t)P.nwin * sizeof(PadWin)));
     SPOPS_TRY(P.win_partial.alloc((size_t)P.nwin * 32 * sizeof(double)));
     SPOPS_TRY(P.win_counter.alloc((size_t)nch * sizeof(int)));
+    SPOPS_TRY(P.tails.alloc((size_t)std::max<int64_t>(P.ntails, 1) * sizeof(PadTail)));
+    SPOPS_TRY(P.tcol.alloc((size_t)std::max<int64_t>(P.ntail_entries, 1) * sizeof(I)));
+    SPOPS_TRY(P.tval.alloc((size_t)std::max<int64_t>(P.ntail_entries, 1) * sizeof(V)));
     SPOPS_CUDA(cudaMemsetAsync(P.win_counter.p, 0, P.win_counter.bytes, st));
-    pad_win_fill_kernel<<<grid_for(nch), 256, 0, st>>>(np, off, nch, P.win.as<PadWin>());
+    pad_win_fill_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, P.head.as<int>(), woff, nwc,
+                                                             troff, teoff, P.win.as<PadWin>(), P.tails.as<PadTail>());
     SPOPS_LAUNCH_CHECK();
+    if (P.ntails > 0) {
+      pad_tail_copy_kernel<I, V><<<grid_for(P.ntails * 32), 256, 0, st>>>(
+          P.tails.as<PadTail>(), P.ntails, P.chunk_off.as<int64_t>(), M->col.as<I>(), M->val.as<V>(),
+          P.tcol.as<I>(), P.tval.as<V>());
+      SPOPS_LAUNCH_CHECK();
+    }
+    P.tails_fresh = true;
     SPOPS_CUDA(cudaStreamSynchronize(st));
   }
   return SPOPS_OK;
@@ -742,11 +879,19 @@ spops_status_t padded_spmv_t(Context* ctx, Matrix* A, double alpha, const void* 
   if (P.nwin > 0) {
     const int64_t g = (P.nwin + P.npieces + 7) / 8;
     if (g > INT32_MAX) return fail(SPOPS_ERR_TOO_LARGE, "padded SpMV grid");
+    if (!P.tails_fresh && P.ntails > 0) {  // values changed: copy the tails again
+      PaddedData& Pw = A->pad;
+      pad_tail_copy_kernel<I, V><<<grid_for(P.ntails * 32), 256, 0, ctx->stream>>>(
+          P.tails.as<PadTail>(), P.ntails, P.chunk_off.as<int64_t>(), A->col.as<I>(), A->val.as<V>(),
+          Pw.tcol.as<I>(), Pw.tval.as<V>());
+      SPOPS_LAUNCH_CHECK();
+      Pw.tails_fresh = true;
+    }
     padded_win_kernel<I, V><<<(unsigned)g, 256, 0, ctx->stream>>>(
         A->col.as<I>(), A->val.as<V>(), P.chunk_off.as<int64_t>(), P.row_len.as<int>(), ro, n,
         static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, beta == 0.0, P.win.as<PadWin>(), P.nwin,
         P.win_partial.as<V>(), P.win_counter.as<int>(), P.npieces, P.piece.as<PadPiece>(), P.partial.as<V>(),
-        P.counter.as<int>());
+        P.counter.as<int>(), P.head.as<int>(), P.tcol.as<I>(), P.tval.as<V>());
     SPOPS_LAUNCH_CHECK();
     return SPOPS_OK;
   }

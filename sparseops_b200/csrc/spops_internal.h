@@ -238,12 +238,27 @@ struct PadPiece {
   int32_t npieces;  // pieces of this row
 };
 
-// Step window of a 32-row column-major chunk (see padded_window32).
+// Window of a 32-row column-major chunk: a head window sums slots
+// [widx * kPadWindow, +kPadWindow) of the chunk's head (see padded_window32);
+// a tail window sums one row's tail entries, which sit contiguously in the
+// tail arrays.  The chunk's windows combine their per-row sums in window order.
 struct PadWin {
   int64_t chunk;   // chunk index
   int64_t first;   // index of the chunk's first window
-  int32_t widx;    // this window: steps [widx * kPadWindow, +kPadWindow)
-  int32_t nw;      // windows of the chunk
+  int32_t widx;    // this window's index among the chunk's windows
+  int32_t nw;      // windows of the chunk (head windows first, then tail windows)
+  int64_t tail;    // tail window: first entry in the tail arrays; head window: -1
+  int32_t tlen;    // tail window: entries
+  int32_t tlane;   // tail window: the row's position in the chunk
+};
+
+// A stored row's tail: its slots [from, from + len) of a column-major chunk,
+// copied to tail entries [start, start + len) (contiguous, row order).
+struct PadTail {
+  int64_t row;
+  int64_t start;
+  int32_t from;
+  int32_t len;
 };
 
 struct PaddedData {
@@ -258,16 +273,26 @@ struct PaddedData {
   DevBuf piece;      // PadPiece [npieces]
   DevBuf partial;    // double [npieces]
   DevBuf counter;    // int32 [npieces]
-  // windows of 32-row column-major chunks (C == 32 only)
+  // windows of 32-row column-major chunks (C == 32 only).  A chunk's head
+  // holds its slots up to the fourth-longest row's length; the slots beyond,
+  // held by at most three rows, are copied row by row into the tail arrays so
+  // that a row running alone is read contiguously.
   int64_t nwin = 0;
   DevBuf win;        // PadWin [nwin]
   DevBuf win_partial;  // double [nwin * 32]
   DevBuf win_counter;  // int32 [nchunks]
+  DevBuf head;       // int32 [nchunks]: head width in slots
+  int64_t ntails = 0, ntail_entries = 0;
+  DevBuf tails;      // PadTail [ntails]
+  DevBuf tcol, tval; // I / V [ntail_entries]
+  bool tails_fresh = true;  // tail values copied from the current values
   void release() {
     reorder.release(); chunk_len.release(); chunk_off.release(); row_len.release();
     piece.release(); partial.release(); counter.release();
     win.release(); win_partial.release(); win_counter.release();
+    head.release(); tails.release(); tcol.release(); tval.release();
     nwin = 0;
+    ntails = ntail_entries = 0;
   }
 };
 
