@@ -299,7 +299,7 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   Matrix* out = nullptr;
   SpgemmStats s2;
   SPOPS_TRY(cluster_spgemm(ctx, A, B, perm.as<int64_t>(), offs.as<int64_t>(), ncl, sort_output != 0, l2_budget_bytes,
-                           &out, &s2));
+                           &out, &s2, false, false, true));
   s2.minhash_ms = s.minhash_ms;
   s2.lsh_ms = s.lsh_ms;
   s2.hc_ms = s.hc_ms;

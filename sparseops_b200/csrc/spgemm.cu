@@ -1669,7 +1669,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
 
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
                               int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st,
-                              bool rowwise, bool cluster_out) {
+                              bool rowwise, bool cluster_out, bool device_arrays) {
   if (A->format != SPOPS_FMT_CSR || B->format != SPOPS_FMT_CSR)
     return fail(SPOPS_ERR_INVALID, "SpGEMM needs CSR matrices");
   if (A->cols != B->rows) return fail(SPOPS_ERR_INVALID, "SpGEMM: A.cols (%lld) != B.rows (%lld)",
@@ -1677,11 +1677,15 @@ spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t*
   if (A->itype != B->itype || A->vtype != B->vtype) return fail(SPOPS_ERR_INVALID, "SpGEMM: mixed types");
   if (B->cols > INT32_MAX || A->cols > INT32_MAX || nclusters > INT32_MAX)
     return fail(SPOPS_ERR_UNSUPPORTED, "SpGEMM: more than 2^31 columns or clusters");
-  if (nclusters < 0 || offsets[0] != 0 || offsets[nclusters] != A->rows)
+  if (nclusters < 0) return fail(SPOPS_ERR_INVALID, "SpGEMM: negative cluster count");
+  // a caller's host arrays are checked here; the device clustering's own
+  // output (device_arrays) is a permutation with offsets from 0 to rows by
+  // construction
+  if (!device_arrays && (offsets[0] != 0 || offsets[nclusters] != A->rows))
     return fail(SPOPS_ERR_INVALID, "SpGEMM: offsets must run from 0 to rows");
-  for (int64_t c = 0; c < nclusters; ++c)
+  for (int64_t c = 0; !device_arrays && c < nclusters; ++c)
     if (offsets[c + 1] < offsets[c]) return fail(SPOPS_ERR_INVALID, "SpGEMM: offsets not monotone");
-  {
+  if (!device_arrays) {
     std::vector<unsigned char> seen((size_t)A->rows, 0);
     for (int64_t r = 0; r < A->rows; ++r) {
       if (perm[r] < 0 || perm[r] >= A->rows || seen[perm[r]]) return fail(SPOPS_ERR_INVALID, "SpGEMM: bad permutation");

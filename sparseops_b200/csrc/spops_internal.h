@@ -444,7 +444,7 @@ spops_status_t hierarchical_clustering_device(Context* ctx, Matrix* A, const int
 // rows in cluster order) instead of CSR in A's row order
 spops_status_t cluster_spgemm(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm, const int64_t* offsets,
                               int64_t nclusters, bool sort_output, double l2_budget, Matrix** C, SpgemmStats* st,
-                              bool rowwise = false, bool cluster_out = false);
+                              bool rowwise = false, bool cluster_out = false, bool device_arrays = false);
 // clustered (VLength) form of a CSR matrix and back (spgemm.cu)
 spops_status_t vlcluster_from_csr(Context* ctx, Matrix* A, const int64_t* offsets, int64_t nclusters, Matrix** out);
 spops_status_t vlcluster_to_csr(Context* ctx, Matrix* M, Matrix** out);
