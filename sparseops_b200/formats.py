@@ -433,6 +433,20 @@ def select_format(csr: CSR_Matrix, timed: bool = False, learned: bool = False) -
     return {"format": _FORMAT_NAMES[fmt.value], "params": params, "ms": ms.value}
 
 
+def select_format_from_features(features: dict) -> dict:
+    """The learned choice (select_format(learned=True)) from features already
+    computed -- a dict with the names of spops_features_t -- without device
+    work.  Returns {"format", "params"}."""
+    f = _lib.Features()
+    for k in _lib.FEATURE_NAMES:
+        setattr(f, k, features[k])
+    fmt = C.c_int()
+    p = FormatParams()
+    call("spops_select_format_from_features", C.byref(f), C.byref(fmt), C.byref(p))
+    params = {k: int(getattr(p, k)) for k, _ in FormatParams._fields_ if k != "reserved" and getattr(p, k)}
+    return {"format": _FORMAT_NAMES[fmt.value], "params": params}
+
+
 _CONVERTED = {"sell_c_sigma": SELL_C_Sigma_Matrix, "sell_c_R": SELL_C_R_Matrix, "sell": S_ELL_Matrix,
               "ell": ELL_Matrix, "dia": DIA_Matrix, "bsr": BSR_Matrix, "csr5": CSR5_Matrix}
 
@@ -447,13 +461,14 @@ def convert_to(csr: CSR_Matrix, fmt: str, **params):
     return _wrap(_CONVERTED[fmt], csr, _convert(csr, fmt, **params))
 
 
-def SpOps_auto(alpha, csr: CSR_Matrix, x, beta, y, timed: bool = False):
-    """y = alpha*A*x + beta*y in the format select_format picks for A; the
-    choice and the converted matrix are kept on the CSR object."""
-    key = "timed" if timed else "rules"
+def SpOps_auto(alpha, csr: CSR_Matrix, x, beta, y, timed: bool = False, learned: bool = False):
+    """y = alpha*A*x + beta*y in the format select_format picks for A (rules,
+    timed or learned); the choice and the converted matrix are kept on the
+    CSR object."""
+    key = "timed" if timed else ("learned" if learned else "rules")
     cache = getattr(csr, "_auto", None)
     if cache is None or cache[0] != key:
-        choice = select_format(csr, timed)
+        choice = select_format(csr, timed, learned)
         cache = (key, choice, convert_to(csr, choice["format"], **choice["params"]))
         csr._auto = cache
     return _spmv(alpha, cache[2], x, beta, y)
