@@ -16,8 +16,12 @@
 //     and then cast to the value type; tokens after the nnz-th entry are
 //     ignored;
 //   * a file with zero rows gives an empty matrix (0 x 0).
-// The CSR form is the device coo_to_csr (coo_csr.cu), with or without the
-// duplicate summation.
+// The CSR form without the duplicate summation (compact = 0) is built straight
+// from the placed entries: row counts, a scan for the row offsets, and a
+// stable sort by row (skipped when the entries already come row by row), so
+// entries keep their file order within a row as the reference's counting sort
+// does (include/sparse_conversion.h:37-99).  With the summation it is the
+// device coo_to_csr (coo_csr.cu).
 //
 // From a path, the banner and size line are read from a prefix and the
 // entries part goes to the device in 4 MiB chunks: reader threads pread into
@@ -145,6 +149,37 @@ __global__ void copies_kernel(const int64_t* __restrict__ r, const int64_t* __re
   if (e < nnz) cnt[e] = (symm && r[e] != c[e]) ? 2 : 1;
 }
 
+// CSR straight from the placed entries (read_csr_matrix without a COO
+// handle): per-row counts, and whether the entries already come row by row.
+template <typename I>
+__global__ void csr_count_kernel(const I* __restrict__ ro, int64_t total, unsigned long long* __restrict__ cnt,
+                                 int* __restrict__ unsorted) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  atomicAdd(cnt + (int64_t)ro[k], 1ULL);
+  if (k > 0 && ro[k] < ro[k - 1]) *unsorted = 1;
+}
+
+template <typename I>
+__global__ void csr_rowptr_kernel(const unsigned long long* __restrict__ scan, int64_t n1, I* __restrict__ rp) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n1) rp[r] = (I)scan[r];
+}
+
+__global__ void csr_iota_kernel(int64_t* __restrict__ a, int64_t m) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) a[i] = i;
+}
+
+template <typename I, typename V>
+__global__ void csr_gather_kernel(const int64_t* __restrict__ perm, const I* __restrict__ ci, const V* __restrict__ v,
+                                  int64_t m, I* __restrict__ co, V* __restrict__ vo) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  co[i] = ci[perm[i]];
+  vo[i] = v[perm[i]];
+}
+
 template <typename I, typename V>
 __global__ void place_kernel(const int64_t* __restrict__ r, const int64_t* __restrict__ c,
                              const double* __restrict__ v, const int64_t* __restrict__ pos, int64_t nnz, bool symm,
@@ -258,7 +293,7 @@ spops_status_t read_header(const char* s, size_t n, Header* h) {
 // The entries part of the file (len bytes) is in dtext on the device,
 // written by work already queued on ctx->stream.
 template <typename I, typename V>
-spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H, Matrix** out) {
+spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H, Matrix** out, bool direct_csr) {
   cudaStream_t st = ctx->stream;
   const int per = H.pattern ? 2 : 3;
   const int64_t nnz = H.nnz;
@@ -350,6 +385,79 @@ spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H
   int64_t total = 0;
   SPOPS_CUDA(cudaMemcpyAsync(&total, pos.as<int64_t>() + nnz, 8, cudaMemcpyDeviceToHost, st));
   SPOPS_CUDA(cudaStreamSynchronize(st));
+  if (direct_csr && H.rows > 0) {  // CSR in file order within rows, no COO handle
+    PoolBuf prow(ctx), tc(ctx), tv(ctx), cnt2(ctx), scan(ctx), perm_in(ctx), perm(ctx), skey(ctx), tmp2(ctx);
+    const size_t t1 = (size_t)std::max<int64_t>(total, 1), n1 = (size_t)H.rows + 1;
+    SPOPS_TRY(prow.alloc(t1 * sizeof(I)));
+    SPOPS_TRY(tc.alloc(t1 * sizeof(I)));
+    SPOPS_TRY(tv.alloc(t1 * sizeof(V)));
+    SPOPS_TRY(cnt2.alloc((n1 + 1) * 8));
+    SPOPS_TRY(scan.alloc((n1 + 1) * 8));
+    SPOPS_CUDA(cudaMemsetAsync(cnt2.p, 0, (n1 + 1) * 8, st));
+    int* unsorted = reinterpret_cast<int*>(cnt2.as<unsigned long long>() + n1);
+    if (nnz > 0) {
+      place_kernel<I, V><<<grid_for(nnz), 256, 0, st>>>(r.as<int64_t>(), c.as<int64_t>(), v.as<double>(),
+                                                        pos.as<int64_t>(), nnz, H.symmetric, prow.as<I>(), tc.as<I>(),
+                                                        tv.as<V>());
+      csr_count_kernel<I><<<grid_for(total), 256, 0, st>>>(prow.as<I>(), total, cnt2.as<unsigned long long>(),
+                                                           unsorted);
+      SPOPS_LAUNCH_CHECK();
+    }
+    size_t sb2 = 0;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, sb2, cnt2.as<unsigned long long>(),
+                                             scan.as<unsigned long long>(), (int64_t)n1, st));
+    int rbits = 1;  // row keys are below rows
+    while (rbits < 62 && (int64_t(1) << rbits) < H.rows) ++rbits;
+    size_t ss2 = 0;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, ss2, prow.as<I>(), prow.as<I>(), perm_in.as<int64_t>(),
+                                               perm.as<int64_t>(), (int64_t)t1, 0, rbits, st));
+    SPOPS_TRY(tmp2.alloc(std::max(sb2, ss2) + 256));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.p, sb2, cnt2.as<unsigned long long>(),
+                                             scan.as<unsigned long long>(), (int64_t)n1, st));
+    int hu = 0;
+    SPOPS_CUDA(cudaMemcpyAsync(&hu, unsorted, 4, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaStreamSynchronize(st));
+    tr.mark(st, "place + row counts");
+    Matrix* C = new spops_matrix_s();
+    C->ctx = ctx;
+    C->format = SPOPS_FMT_CSR;
+    C->itype = sizeof(I) == 4 ? SPOPS_INDEX_I32 : SPOPS_INDEX_I64;
+    C->vtype = sizeof(V) == 8 ? SPOPS_VALUE_F64 : SPOPS_VALUE_F32;
+    C->rows = H.rows;
+    C->cols = H.cols;
+    C->nnz = total;
+    spops_status_t s2 = C->row.alloc(n1 * sizeof(I));
+    if (s2 == SPOPS_OK) s2 = C->col.alloc(t1 * sizeof(I));
+    if (s2 == SPOPS_OK) s2 = C->val.alloc(t1 * sizeof(V));
+    if (s2 == SPOPS_OK) {
+      csr_rowptr_kernel<I><<<grid_for((int64_t)n1), 256, 0, st>>>(scan.as<unsigned long long>(), (int64_t)n1,
+                                                                 C->row.as<I>());
+      if (total > 0 && !hu) {  // already row by row: the placed order is the CSR order
+        SPOPS_CUDA(cudaMemcpyAsync(C->col.p, tc.p, (size_t)total * sizeof(I), cudaMemcpyDeviceToDevice, st));
+        SPOPS_CUDA(cudaMemcpyAsync(C->val.p, tv.p, (size_t)total * sizeof(V), cudaMemcpyDeviceToDevice, st));
+      } else if (total > 0) {  // stable sort by row keeps file order within a row
+        if (perm_in.alloc(t1 * 8) != SPOPS_OK || perm.alloc(t1 * 8) != SPOPS_OK || skey.alloc(t1 * sizeof(I)) != SPOPS_OK)
+          s2 = fail(SPOPS_ERR_ALLOC, "Matrix Market: sort buffers");
+        if (s2 == SPOPS_OK) {
+          csr_iota_kernel<<<grid_for(total), 256, 0, st>>>(perm_in.as<int64_t>(), total);
+          SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp2.p, ss2, prow.as<I>(), skey.as<I>(), perm_in.as<int64_t>(),
+                                                     perm.as<int64_t>(), total, 0, rbits, st));
+          csr_gather_kernel<I, V><<<grid_for(total), 256, 0, st>>>(perm.as<int64_t>(), tc.as<I>(), tv.as<V>(), total,
+                                                                   C->col.as<I>(), C->val.as<V>());
+        }
+      }
+      if (s2 == SPOPS_OK && cudaGetLastError() != cudaSuccess) s2 = fail(SPOPS_ERR_CUDA, "Matrix Market: CSR build");
+      if (s2 == SPOPS_OK && cudaStreamSynchronize(st) != cudaSuccess) s2 = fail(SPOPS_ERR_CUDA, "Matrix Market: stream");
+    }
+    if (s2 != SPOPS_OK) {
+      C->release_all();
+      delete static_cast<spops_matrix_s*>(C);
+      return s2;
+    }
+    tr.mark(st, "CSR arrays");
+    *out = C;
+    return SPOPS_OK;
+  }
   Matrix* A = new spops_matrix_s();
   A->ctx = ctx;
   A->format = SPOPS_FMT_COO;
@@ -388,17 +496,17 @@ spops_status_t check_header(const Header& H, spops_index_t itype) {
 }
 
 spops_status_t read_typed(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H, spops_index_t itype,
-                          spops_value_t vtype, Matrix** out) {
+                          spops_value_t vtype, Matrix** out, bool direct_csr) {
   const bool i32 = itype == SPOPS_INDEX_I32, f64 = vtype == SPOPS_VALUE_F64;
-  if (i32 && f64) return read_t<int32_t, double>(ctx, dtext, len, H, out);
-  if (i32) return read_t<int32_t, float>(ctx, dtext, len, H, out);
-  if (f64) return read_t<int64_t, double>(ctx, dtext, len, H, out);
-  return read_t<int64_t, float>(ctx, dtext, len, H, out);
+  if (i32 && f64) return read_t<int32_t, double>(ctx, dtext, len, H, out, direct_csr);
+  if (i32) return read_t<int32_t, float>(ctx, dtext, len, H, out, direct_csr);
+  if (f64) return read_t<int64_t, double>(ctx, dtext, len, H, out, direct_csr);
+  return read_t<int64_t, float>(ctx, dtext, len, H, out, direct_csr);
 }
 
 // the file's bytes in host memory
 spops_status_t parse_coo(Context* ctx, const char* text, size_t n, spops_index_t itype, spops_value_t vtype,
-                         Matrix** out) {
+                         Matrix** out, bool direct_csr = false) {
   Header H;
   SPOPS_TRY(read_header(text, n, &H));
   SPOPS_TRY(check_header(H, itype));
@@ -408,7 +516,7 @@ spops_status_t parse_coo(Context* ctx, const char* text, size_t n, spops_index_t
   SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
   if (len > 0) SPOPS_CUDA(cudaMemcpyAsync(dtext.p, text + H.data, (size_t)len, cudaMemcpyHostToDevice, ctx->stream));
   tr.mark(ctx->stream, "upload from host memory");
-  return read_typed(ctx, dtext, len, H, itype, vtype, out);
+  return read_typed(ctx, dtext, len, H, itype, vtype, out, direct_csr);
 }
 
 // File chunks go to the device through pinned buffers: kReaders threads each
@@ -460,7 +568,8 @@ struct FileCloser {
   }
 };
 
-spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, spops_value_t vtype, Matrix** out) {
+spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, spops_value_t vtype, Matrix** out,
+                         bool direct_csr = false) {
   Trace tr("mtx");
   const int fd = ::open(path, O_RDONLY | O_CLOEXEC);
   if (fd < 0) return fail(SPOPS_ERR_INVALID, "Matrix Market: unable to open file: %s", path);
@@ -540,7 +649,7 @@ spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, sp
       return fail(SPOPS_ERR_CUDA, "Matrix Market: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
   }
-  return read_typed(ctx, dtext, len, H, itype, vtype, out);
+  return read_typed(ctx, dtext, len, H, itype, vtype, out, direct_csr);
 }
 
 spops_status_t check_types(spops_index_t itype, spops_value_t vtype) {
@@ -550,6 +659,10 @@ spops_status_t check_types(spops_index_t itype, spops_value_t vtype) {
 }
 
 spops_status_t coo_to_csr_out(Context* ctx, Matrix* coo, int32_t compact, spops_matrix_t* csr) {
+  if (coo->format == SPOPS_FMT_CSR) {  // built directly (compact = 0)
+    *csr = static_cast<spops_matrix_s*>(coo);
+    return SPOPS_OK;
+  }
   spops_status_t s;
   if (coo->rows == 0) {  // read_csr_matrix: a matrix with no rows is 0 x 0
     Matrix* C = new spops_matrix_s();
@@ -615,7 +728,7 @@ spops_status_t spops_mtx_parse_csr(spops_context_t ctx, const char* text, int64_
   SPOPS_TRY(check_types(itype, vtype));
   DeviceGuard g(ctx->device);
   Matrix* A = nullptr;
-  SPOPS_TRY(parse_coo(ctx, text, (size_t)len, itype, vtype, &A));
+  SPOPS_TRY(parse_coo(ctx, text, (size_t)len, itype, vtype, &A, compact == 0));
   return coo_to_csr_out(ctx, A, compact, csr);
 }
 
@@ -625,7 +738,7 @@ spops_status_t spops_mtx_read_csr(spops_context_t ctx, const char* path, spops_i
   SPOPS_TRY(check_types(itype, vtype));
   DeviceGuard g(ctx->device);
   Matrix* A = nullptr;
-  SPOPS_TRY(read_path(ctx, path, itype, vtype, &A));
+  SPOPS_TRY(read_path(ctx, path, itype, vtype, &A, compact == 0));
   return coo_to_csr_out(ctx, A, compact, csr);
 }
 

@@ -112,6 +112,36 @@ def test_large_random_file(cuda, tmp_path):
         assert np.array_equal(m.values.view(np.uint64), ev.view(np.uint64))
 
 
+@pytest.mark.parametrize("order", ["random", "rows_sorted", "symmetric"])
+def test_large_csr_no_compact(cuda, tmp_path, order):
+    """CSR without the duplicate summation, built straight from the parsed
+    entries: row offsets from counts, entries in file order within a row (a
+    stable sort by row), for files in random row order, already sorted by row
+    (no sort needed) and symmetric (mirror copies placed after their entry)."""
+    from sparseops_b200 import read_csr_matrix
+    rng = np.random.default_rng(31)
+    n, nnz = 7000, 250000
+    r, c = rng.integers(1, n + 1, nnz), rng.integers(1, n + 1, nnz)
+    if order == "rows_sorted":
+        r = np.sort(r)
+    if order == "symmetric":
+        r, c = np.maximum(r, c), np.minimum(r, c)
+    x = rng.standard_normal(nnz)
+    symm = "symmetric" if order == "symmetric" else "general"
+    body = "\n".join("%d %d %.17g" % (a, b, y) for a, b, y in zip(r, c, x))
+    text = "%%%%MatrixMarket matrix coordinate real %s\n%d %d %d\n%s\n" % (symm, n + 3, n, nnz, body)
+    path = _write(tmp_path, text, order + ".mtx")
+    _, _, er, ec, ev = _py_coo(text)
+    perm = np.argsort(er, kind="stable")
+    want_rp = np.zeros(n + 4, np.int64)
+    np.cumsum(np.bincount(er, minlength=n + 3), out=want_rp[1:])
+    for it, vt in ((np.int32, np.float64), (np.int64, np.float32)):
+        rp, ci, v = read_csr_matrix(path, False, it, vt).host()
+        assert np.array_equal(rp.astype(np.int64), want_rp)
+        assert np.array_equal(ci.astype(np.int64), ec[perm])
+        assert np.array_equal(v, ev[perm].astype(vt))
+
+
 @pytest.mark.parametrize("text,status", [
     ("%%MatrixMarket matrix coordinate real\n2 2 1\n1 1 1\n", 1),           # banner of four words
     ("%MatrixMarket matrix coordinate real general\n2 2 1\n1 1 1\n", 1),   # no banner
