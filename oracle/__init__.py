@@ -237,6 +237,15 @@ class Oracle:
         return out
 
 
+def _ll(a):
+    """int64, C-contiguous: the reference harness takes long long arrays."""
+    return np.ascontiguousarray(a, np.int64)
+
+
+def _f8(a):
+    return np.ascontiguousarray(a, np.float64)
+
+
 class Reference:
     """ctypes view of the reference library compiled from its own sources.
 
@@ -306,12 +315,14 @@ class Reference:
         self.L.ref_fmt_free(_vp(h))
 
     def minhash(self, rp, ci, k, seed):
+        rp, ci = _ll(rp), _ll(ci)
         n = len(rp) - 1
         sig = np.zeros((n, k), np.uint64)
         self.L.ref_minhash_flat(_p(rp), _p(ci), _i64(n), C.c_int(k), C.c_uint64(seed), _p(sig))
         return sig
 
     def lsh_pairs(self, rp, ci, k, bands, seed, constrain=True):
+        rp, ci = _ll(rp), _ll(ci)
         h = self.L.ref_lsh_pairs(_p(rp), _p(ci), _i64(len(rp) - 1), C.c_int(k), C.c_int(bands),
                                  C.c_uint64(seed), C.c_int(1 if constrain else 0))
         m = self.L.ref_pairs_count(_vp(h))
@@ -321,6 +332,7 @@ class Reference:
         return i, j, s
 
     def hc(self, rp, ci, pi, pj, ps, cluster_size):
+        rp, ci, pi, pj, ps = _ll(rp), _ll(ci), _ll(pi), _ll(pj), _f8(ps)
         n = len(rp) - 1
         perm, offs = np.zeros(n, np.int64), np.zeros(n + 1, np.int64)
         nc = self.L.ref_hc(_p(rp), _p(ci), _i64(n), _p(pi), _p(pj), _p(ps), _i64(len(pi)), _i64(cluster_size),
@@ -328,8 +340,9 @@ class Reference:
         return perm, offs[:nc + 1]
 
     def spgemm_kernel3(self, A, B, perm, offsets, sort_output=False, l2_fraction=-1.0):
-        arp, aci, av = A
-        brp, bci, bv = B[:3]
+        arp, aci, av = _ll(A[0]), _ll(A[1]), _f8(A[2])
+        brp, bci, bv = _ll(B[0]), _ll(B[1]), _f8(B[2])
+        perm, offsets = _ll(perm), _ll(offsets)
         n = len(arp) - 1
         bcols = int(B[3]) if len(B) > 3 else n
         h = self.L.ref_spgemm_kernel3(_i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av),
@@ -355,8 +368,8 @@ class Reference:
 
     def spgemm_rowwise(self, A, B, kernel_flag=1, sort_output=False):
         """The reference's LeSpGEMM<sortOutput, int64_t, double>(A, B, C, kernel_flag)."""
-        arp, aci, av = A
-        brp, bci, bv = B[:3]
+        arp, aci, av = _ll(A[0]), _ll(A[1]), _f8(A[2])
+        brp, bci, bv = _ll(B[0]), _ll(B[1]), _f8(B[2])
         n = len(arp) - 1
         bcols = int(B[3]) if len(B) > 3 else n
         h = self.L.ref_spgemm_rowwise(_i64(n), _i64(len(brp) - 1), _i64(len(aci)), _p(arp), _p(aci), _p(av),
@@ -366,6 +379,7 @@ class Reference:
 
     def spgemm_topk(self, rp, ci, ncols, top_k, f32=False):
         """The reference's HashSpGEMMTopK<int64_t, V>(A, C, top_k)."""
+        rp, ci = _ll(rp), _ll(ci)
         n = len(rp) - 1
         h = self.L.ref_spgemm_topk(_i64(n), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _i64(top_k),
                                    C.c_int(1 if f32 else 0))
@@ -380,8 +394,8 @@ class Reference:
     def spgemm_rowwise_time(self, A, B, kernel_flag=1, top_k=-1, iters=1):
         """Mean ms of the reference's LeSpGEMM<false>(A, B, C, kernel_flag), or
         of HashSpGEMMTopK(A, C, top_k) when top_k >= 0."""
-        arp, aci, av = A
-        brp, bci, bv = B[:3]
+        arp, aci, av = _ll(A[0]), _ll(A[1]), _f8(A[2])
+        brp, bci, bv = _ll(B[0]), _ll(B[1]), _f8(B[2])
         n = len(arp) - 1
         bcols = int(B[3]) if len(B) > 3 else n
         self.L.ref_spgemm_rowwise_time.restype = C.c_double
@@ -393,8 +407,9 @@ class Reference:
     def spgemm_kernel3_time(self, A, B, perm, offsets, iters=3, l2_fraction=-1.0):
         """Mean ms of the reference's LeSpGEMM_VLength kernel 3 (numeric and
         symbolic phases on the clustered A) over `iters` runs."""
-        arp, aci, av = A
-        brp, bci, bv = B[:3]
+        arp, aci, av = _ll(A[0]), _ll(A[1]), _f8(A[2])
+        brp, bci, bv = _ll(B[0]), _ll(B[1]), _f8(B[2])
+        perm, offsets = _ll(perm), _ll(offsets)
         n = len(arp) - 1
         bcols = int(B[3]) if len(B) > 3 else n
         self.L.ref_spgemm_kernel3_time.restype = C.c_double
@@ -466,6 +481,10 @@ class Reference:
             os.remove(path)
 
     def csr_transpose(self, rp, ci, v, ncols):
+        """The reference's csr_transpose on int64 / FP64 copies of the arrays."""
+        rp = np.ascontiguousarray(rp, np.int64)
+        ci = np.ascontiguousarray(ci, np.int64)
+        v = np.ascontiguousarray(v, np.float64)
         h = self.L.ref_csr_transpose(_i64(len(rp) - 1), _i64(ncols), _i64(len(ci)), _p(rp), _p(ci), _p(v))
         info = np.zeros(6, np.int64)
         self.L.ref_csr_info(_vp(h), _p(info))

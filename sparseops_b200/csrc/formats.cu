@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(256) padded_win_kernel(
       s3 += v3 * ld_gather(x + c3);
     }
     for (; e < W.tlen; e += 32) s0 += ld_stream(tv + e) * ld_gather(x + ld_stream(tc + e));
-    const V s = warp_sum((s0 + s1) + (s2 + s3));
+    const V s = __shfl_sync(0xffffffffu, warp_sum((s0 + s1) + (s2 + s3)), 0);  // the sum is in lane 0
     part[lane] = lane == W.tlane ? s : V(0);
   } else {
     padded_window32<I, V>(chunk_off[W.chunk], len, W.widx * kPadWindow, col, val, x, lane,

@@ -238,6 +238,15 @@ __global__ void hc_commit_kernel(const int32_t* __restrict__ live, int64_t nlive
   next_live[atomicAdd(nnext, 1ULL)] = (int32_t)t;
 }
 
+// the found pairs (tasks np .. ntask - 1) into a new, larger set
+__global__ void hc_seen_rebuild_kernel(Tasks T, int64_t np, int64_t ntask, unsigned long long* __restrict__ tab,
+                                       uint64_t mask, int* __restrict__ err) {
+  const int64_t t = np + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ntask) return;
+  const unsigned long long key = ((unsigned long long)(uint32_t)T.i[t] << 32) | (uint32_t)T.j[t];
+  hc_seen_insert(tab, mask, key, err);
+}
+
 // 3. clear the round's reservations
 __global__ void hc_release_kernel(const int32_t* __restrict__ ri_in, const int32_t* __restrict__ rj_in, int64_t nlive,
                                   int32_t* __restrict__ res) {
@@ -298,23 +307,26 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
                                                     open.as<unsigned char>(), res.as<int32_t>());
     SPOPS_LAUNCH_CHECK();
   }
-  // tasks: the initial pairs, then the pairs found while merging (a task that
-  // outlives a merge of one of its clusters can find one more pair, and the
-  // initial pairs one each, so np + n bounds them)
-  const int64_t cap = np + n + 1;
+  // tasks: the initial pairs, then the pairs found while merging.  A round
+  // creates at most one task per live task and never raises the live count,
+  // so the live lists hold np entries and the task arrays grow (between
+  // rounds) to ntask + nlive when needed; the set of found pairs grows with them.
+  int64_t cap = np + n + 1;
+  const size_t nl = (size_t)std::max<int64_t>(np, 1);
   PoolBuf ts(ctx), ti(ctx), tj(ctx), liveA(ctx), liveB(ctx), ri(ctx), rj(ctx), seen(ctx);
   SPOPS_TRY(ts.alloc((size_t)cap * 8));
   SPOPS_TRY(ti.alloc((size_t)cap * 4));
   SPOPS_TRY(tj.alloc((size_t)cap * 4));
-  SPOPS_TRY(liveA.alloc((size_t)cap * 4));
-  SPOPS_TRY(liveB.alloc((size_t)cap * 4));
-  SPOPS_TRY(ri.alloc((size_t)cap * 4));
-  SPOPS_TRY(rj.alloc((size_t)cap * 4));
+  SPOPS_TRY(liveA.alloc(nl * 4));
+  SPOPS_TRY(liveB.alloc(nl * 4));
+  SPOPS_TRY(ri.alloc(nl * 4));
+  SPOPS_TRY(rj.alloc(nl * 4));
   uint64_t seen_slots = 1;
   while (seen_slots < (uint64_t)(2 * cap)) seen_slots <<= 1;
   SPOPS_TRY(seen.alloc((size_t)seen_slots * 8));
   SPOPS_CUDA(cudaMemsetAsync(seen.p, 0xff, (size_t)seen_slots * 8, st));
   Tasks T{ts.as<double>(), ti.as<int32_t>(), tj.as<int32_t>()};
+  int64_t ntask = np;
   if (np > 0) {
     hc_init_tasks_kernel<<<hc_grid(np), 256, 0, st>>>(pi, pj, ps, np, T, liveA.as<int32_t>());
     SPOPS_LAUNCH_CHECK();
@@ -326,9 +338,36 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
   int32_t* live = liveA.as<int32_t>();
   int32_t* next = liveB.as<int32_t>();
   int64_t nlive = np, rounds = 0;
-  const int64_t max_rounds = cap + 2;
   while (nlive > 0) {
-    if (++rounds > max_rounds) return fail(SPOPS_ERR_CUDA, "clustering: rounds did not end");
+    // every round retires at least one task, so rounds <= tasks ever made
+    if (++rounds > cap + 2) return fail(SPOPS_ERR_CUDA, "clustering: rounds did not end");
+    if (ntask + nlive > cap) {  // room for this round's new tasks
+      const int64_t ncap = std::max<int64_t>(2 * cap, ntask + nlive + 1);
+      if (ncap > (int64_t)INT32_MAX) return fail(SPOPS_ERR_UNSUPPORTED, "clustering: more than 2^31 tasks");
+      PoolBuf ts2(ctx), ti2(ctx), tj2(ctx), seen2(ctx);
+      SPOPS_TRY(ts2.alloc((size_t)ncap * 8));
+      SPOPS_TRY(ti2.alloc((size_t)ncap * 4));
+      SPOPS_TRY(tj2.alloc((size_t)ncap * 4));
+      SPOPS_CUDA(cudaMemcpyAsync(ts2.p, ts.p, (size_t)ntask * 8, cudaMemcpyDeviceToDevice, st));
+      SPOPS_CUDA(cudaMemcpyAsync(ti2.p, ti.p, (size_t)ntask * 4, cudaMemcpyDeviceToDevice, st));
+      SPOPS_CUDA(cudaMemcpyAsync(tj2.p, tj.p, (size_t)ntask * 4, cudaMemcpyDeviceToDevice, st));
+      uint64_t slots2 = seen_slots;
+      while (slots2 < (uint64_t)(2 * ncap)) slots2 <<= 1;
+      SPOPS_TRY(seen2.alloc((size_t)slots2 * 8));
+      SPOPS_CUDA(cudaMemsetAsync(seen2.p, 0xff, (size_t)slots2 * 8, st));
+      std::swap(ts.p, ts2.p), std::swap(ts.bytes, ts2.bytes);
+      std::swap(ti.p, ti2.p), std::swap(ti.bytes, ti2.bytes);
+      std::swap(tj.p, tj2.p), std::swap(tj.bytes, tj2.bytes);
+      std::swap(seen.p, seen2.p), std::swap(seen.bytes, seen2.bytes);
+      seen_slots = slots2;
+      cap = ncap;
+      T = Tasks{ts.as<double>(), ti.as<int32_t>(), tj.as<int32_t>()};
+      if (ntask > np) {
+        hc_seen_rebuild_kernel<<<hc_grid(ntask - np), 256, 0, st>>>(T, np, ntask, seen.as<unsigned long long>(),
+                                                                     seen_slots - 1, err);
+        SPOPS_LAUNCH_CHECK();
+      }
+    }
     SPOPS_CUDA(cudaMemsetAsync(nnext, 0, 8, st));
     const unsigned g = hc_grid(nlive);
     hc_reserve_kernel<<<g, 256, 0, st>>>(live, nlive, T, parent.as<int32_t>(), open.as<unsigned char>(),
@@ -341,12 +380,13 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
     hc_release_kernel<<<g, 256, 0, st>>>(ri.as<int32_t>(), rj.as<int32_t>(), nlive, res.as<int32_t>());
     SPOPS_LAUNCH_CHECK();
     int herr = 0;
-    unsigned long long hn = 0;
+    unsigned long long hn[2] = {0, 0};  // next live count, tasks made
     SPOPS_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
-    SPOPS_CUDA(cudaMemcpyAsync(&hn, nnext, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(hn, flags.as<char>() + 8, 16, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
     if (herr) return fail(SPOPS_ERR_CUDA, "clustering: device task error %d", herr);
-    nlive = (int64_t)hn;
+    ntask = (int64_t)hn[0];
+    nlive = (int64_t)hn[1];
     std::swap(live, next);
   }
   tr.mark(st, "merge rounds");
