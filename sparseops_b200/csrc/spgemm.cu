@@ -1178,7 +1178,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(row_of_entry.alloc(nz1 * 8));
   tr.mark(st, "alloc key arrays");
   if (tr.on && ctx->pool) {  // the pool's reserved and used bytes, for the trace
-    cuuint64_t rsv = 0, used = 0;
+    unsigned long long rsv = 0, used = 0;
     cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &rsv);
     cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used);
     std::fprintf(stderr, "[spgemm] pool reserved %.1f MB, used %.1f MB\n", rsv / 1e6, used / 1e6);
