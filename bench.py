@@ -408,6 +408,21 @@ def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
         ("sell_c_R C=32 col-major", lambda: F.csr_to_sell_c_R(A, None, 32, 1, F.ColMajor), F.SpOps_sell_c_R),
         ("ell", lambda: F.csr_to_ell(A, F.ColMajor), F.SpOps_ell),
     ]
+
+    def no_tails(conv):  # the same conversion with every chunk's slots read in place
+        def run():
+            from sparseops_b200 import default_context
+            c = default_context()
+            c.set_option("sell_tails", 0)
+            try:
+                return conv()
+            finally:
+                c.set_option("sell_tails", 1)
+        return run
+    cands.insert(2, ("sell_c_sigma C=32 sigma=512 col-major, no tails",
+                     no_tails(lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.ColMajor)), F.SpOps_sell_c_sigma))
+    cands.insert(5, ("sell_c_R C=32 col-major, no tails",
+                     no_tails(lambda: F.csr_to_sell_c_R(A, None, 32, 1, F.ColMajor)), F.SpOps_sell_c_R))
     for name, conv, op in cands:
         try:
             torch.cuda.synchronize()
@@ -536,6 +551,17 @@ def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024, peak=None, cpu_
         items, choice, kt = B.info()
         r["tuned"] = {"work_items": int(items), "rhs_tile": int(kt),
                       "formats": {str(c): int(np.sum(np.asarray(choice) == c)) for c in sorted(set(choice))}}
+        if k == 1:  # the same batch with each CSR segment's banded x window staged in shared memory
+            try:
+                ctx.set_option("batch_band", 1)
+                Bb = Batch(mats, k=k, ctx=ctx)
+                Bb.set_vectors(X, Yb)
+                Bb.tune()
+                Bb.capture(1.0, 0.0)
+                r["band_staging_ms"] = round(_ev_ms(Bb.run, 20), 3)
+                del Bb
+            finally:
+                ctx.set_option("batch_band", 0)
         res[f"k={k}"] = r
         del B, X, Yb, Xc, Yc, Ym
         torch.cuda.empty_cache()

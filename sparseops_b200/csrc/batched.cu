@@ -83,13 +83,14 @@ constexpr int kBatchBlock = 256;
 // stride per warp lets warps drift apart across many matrices.)
 constexpr int kGrab = 2;
 
-template <typename I, typename V, int KT>
+template <typename I, typename V, int KT, bool kBand = false>
 __global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(const BatchItem* __restrict__ items, int64_t nitems,
                                                                const BatchMat* __restrict__ mats, int64_t k, V alpha,
                                                                V beta, bool bz,
                                                                unsigned long long* __restrict__ next_item) {
   __shared__ V prod_all[KT == 1 ? kBatchBlock / 32 : 1][KT == 1 ? 2 * kCsrCap : 1];
-  __shared__ V xs_all[KT == 1 ? kBatchBlock / 32 : 1][KT == 1 ? kBandWin : 1];  // staged x windows
+  // staged x windows (kBand: the context option "batch_band")
+  __shared__ V xs_all[KT == 1 && kBand ? kBatchBlock / 32 : 1][KT == 1 && kBand ? kBandWin : 1];
   extern __shared__ __align__(16) unsigned char batch_dyn_smem[];  // SpMM: one SpmmStage per warp
   const int lane = threadIdx.x & 31;
   V* prod = prod_all[KT == 1 ? threadIdx.x >> 5 : 0];
@@ -110,8 +111,8 @@ __global__ void __launch_bounds__(kBatchBlock, KT == 1 ? 4 : 3) batch_kernel(con
       if (it.kind == 0) {
         csr_segment_spmv<I, V, 8>(M.seg[it.idx], it.idx, static_cast<const I*>(M.ci), static_cast<const V*>(M.val),
                                   static_cast<const I*>(M.rp), static_cast<const V*>(M.x), static_cast<V*>(M.y),
-                                  alpha, beta, bz, prod, static_cast<V*>(M.partial), M.counter, lane, M.band,
-                                  M.cols, xs_all[KT == 1 ? threadIdx.x >> 5 : 0]);
+                                  alpha, beta, bz, prod, static_cast<V*>(M.partial), M.counter, lane,
+                                  kBand ? M.band : 0, M.cols, xs_all[KT == 1 && kBand ? threadIdx.x >> 5 : 0]);
       } else if (it.kind == 1) {
         if (M.colmajor)
           padded_rows32<I, V, true>(it.idx * 32, static_cast<const I*>(M.pcol), static_cast<const V*>(M.pval),
@@ -253,10 +254,10 @@ int spmm_blocks_per_sm() {
   return blocks_per_sm(spmm_kernel<I, V, KT>, 256, spmm_smem<I, V>(256), cache);
 }
 
-template <typename I, typename V, int KT>
+template <typename I, typename V, int KT, bool kBand = false>
 int batch_blocks_per_sm() {
   static int cache[kMaxDevices];
-  return blocks_per_sm(batch_kernel<I, V, KT>, kBatchBlock, KT == 1 ? 0 : spmm_smem<I, V>(kBatchBlock), cache);
+  return blocks_per_sm(batch_kernel<I, V, KT, kBand>, kBatchBlock, KT == 1 ? 0 : spmm_smem<I, V>(kBatchBlock), cache);
 }
 
 }  // namespace
@@ -421,7 +422,7 @@ spops_status_t build_table(Batch* B) {
     t.counter = A->plan.counter.as<int>();
     t.rows = A->rows;
     t.cols = A->cols;
-    t.band = B->k == 1 && A->plan.band > 0 ? A->plan.band : 0;
+    t.band = B->k == 1 && B->ctx->batch_band && A->plan.band > 0 ? A->plan.band : 0;
     if (B->tile_ok[m]) {
       const CsrTiles& D = A->plan.tiles;
       t.tile_row = D.tile_row.as<int64_t>();
@@ -501,6 +502,8 @@ spops_status_t launch_batch(Batch* B, double alpha, double beta, cudaStream_t st
     SPOPS_LAUNCH_CHECK();
     return SPOPS_OK;
   };
+  if (B->k == 1 && B->ctx->batch_band)
+    return go(batch_kernel<I, V, 1, true>, 0, batch_blocks_per_sm<I, V, 1, true>());
   if (B->k == 1) return go(batch_kernel<I, V, 1>, 0, batch_blocks_per_sm<I, V, 1>());
   if (B->kt == 32)
     return go(batch_kernel<I, V, 32>, spmm_smem<I, V>(kBatchBlock), batch_blocks_per_sm<I, V, 32>());
@@ -575,7 +578,7 @@ spops_status_t prepare(Batch* B) {
   for (int64_t m = 0; m < B->count; ++m) {
     Matrix* A = B->src[m];
     if (!A->plan.ready) SPOPS_TRY(csr_analyse(B->ctx, A));
-    if (B->k == 1) SPOPS_TRY(csr_band(B->ctx, A));
+    if (B->k == 1 && B->ctx->batch_band) SPOPS_TRY(csr_band(B->ctx, A));
     // k = 8, 16, 32 over X rows at most 2k wide, vector loads aligned: register tiles
     const BatchMat& h = B->host[m];
     const size_t vs = A->vsize();

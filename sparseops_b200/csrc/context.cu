@@ -1,4 +1,7 @@
 // Context, error reporting and device buffers behind the C ABI.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -67,6 +70,22 @@ spops_status_t Context::pool_alloc(void** out, size_t bytes) {
     SPOPS_CUDA(cudaMemPoolCreate(&pool, &props));
     uint64_t keep = ~0ULL;  // never trim on synchronisation: the next call reuses the memory
     SPOPS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  static const int trace = [] {  // SPOPS_TRACE=2: time every pool allocation
+    const char* e = std::getenv("SPOPS_TRACE");
+    return e && e[0] == '2' ? 2 : 0;
+  }();
+  if (trace == 2) {
+    cudaStreamSynchronize(stream);
+    const auto t0 = std::chrono::steady_clock::now();
+    SPOPS_CUDA(cudaMallocFromPoolAsync(out, bytes, pool, stream));
+    const auto t1 = std::chrono::steady_clock::now();
+    cudaStreamSynchronize(stream);
+    const auto t2 = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[pool] %12zu bytes: call %.3f ms, stream %.3f ms\n", bytes,
+                 std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                 std::chrono::duration<double, std::milli>(t2 - t1).count());
+    return SPOPS_OK;
   }
   SPOPS_CUDA(cudaMallocFromPoolAsync(out, bytes, pool, stream));
   return SPOPS_OK;
@@ -185,6 +204,16 @@ spops_status_t spops_set_option(spops_context_t c, const char* key, int64_t valu
   if (!strcmp(key, "csr_variant")) {
     if (value < 0 || value > 9) return fail(SPOPS_ERR_INVALID, "csr_variant must be 0..9");
     c->csr_variant = (int)value;
+    return SPOPS_OK;
+  }
+  if (!strcmp(key, "sell_tails")) {
+    if (value < 0 || value > 1) return fail(SPOPS_ERR_INVALID, "sell_tails must be 0 or 1");
+    c->sell_tails = (int)value;
+    return SPOPS_OK;
+  }
+  if (!strcmp(key, "batch_band")) {
+    if (value < 0 || value > 1) return fail(SPOPS_ERR_INVALID, "batch_band must be 0 or 1");
+    c->batch_band = (int)value;
     return SPOPS_OK;
   }
   return fail(SPOPS_ERR_INVALID, "spops_set_option: unknown key '%s'", key);

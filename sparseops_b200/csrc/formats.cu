@@ -260,8 +260,9 @@ constexpr int kTailWin = 1024;
 // than h, at most three), their entries, and the chunk's windows: head
 // windows of kPadWindow slots (at least one) and tail windows of kTailWin
 // entries.
-__global__ void pad_head_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks, int* __restrict__ head,
-                                int64_t* __restrict__ ntr, int64_t* __restrict__ nte, int64_t* __restrict__ nw) {
+__global__ void pad_head_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks, bool tails,
+                                int* __restrict__ head, int64_t* __restrict__ ntr, int64_t* __restrict__ nte,
+                                int64_t* __restrict__ nw) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t c = t >> 5;
   const int lane = threadIdx.x & 31;
@@ -279,7 +280,7 @@ __global__ void pad_head_kernel(const int* __restrict__ row_len, int64_t n, int6
       key = (lower == first_half) ? (key > other ? key : other) : (key < other ? key : other);
     }
   }
-  const int h = (int)__shfl_sync(0xffffffffu, key, 3);
+  const int h = (int)__shfl_sync(0xffffffffu, key, tails ? 3 : 0);
   const int tl = len > h ? len - h : 0;
   const unsigned rows = __reduce_add_sync(0xffffffffu, tl > 0 ? 1u : 0u);
   const unsigned ents = __reduce_add_sync(0xffffffffu, (unsigned)tl);
@@ -829,8 +830,8 @@ spops_status_t padded_finish_t(Context* ctx, Matrix* M) {
     int64_t* woff = teoff + (nch + 1);
     SPOPS_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, st));
     SPOPS_TRY(P.head.alloc((size_t)nch * 4));
-    pad_head_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, P.head.as<int>(), ntr, nte,
-                                                         nwc);
+    pad_head_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, ctx->sell_tails != 0,
+                                                         P.head.as<int>(), ntr, nte, nwc);
     SPOPS_LAUNCH_CHECK();
     size_t cs = 0;
     SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cs, ntr, troff, nch + 1, st));

@@ -61,6 +61,13 @@ struct Context {
   spops_status_t ensure_errword();
   // CSR SpMV kernel variant (spmv_csr.cu)
   int csr_variant = 0;
+  // batched k = 1: stage each CSR segment's banded x window in shared memory
+  // (measured slower on the 256-matrix batch than plain gathers, so off unless set)
+  int batch_band = 0;
+  // SELL (C = 32, column-major): a chunk's slots beyond its fourth-longest
+  // row are read from row-contiguous tails (1) or in place (0); read when the
+  // matrix is converted or uploaded
+  int sell_tails = 1;
   // pinned staging for host x / y in spops_spmv_host
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -99,7 +106,7 @@ struct Trace {
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
   explicit Trace(const char* who) : name(who) {
     const char* e = std::getenv("SPOPS_TRACE");
-    on = e && e[0] == '1';
+    on = e && (e[0] == '1' || e[0] == '2');
   }
   void mark(cudaStream_t st, const char* what) {
     if (!on) return;
