@@ -392,7 +392,8 @@ def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
     from sparseops_b200 import formats as F
     from sparseops_b200._lib import call, dbl, vp
     out = {}
-    absA = CSR_Matrix(n, n, A.row_offset, A.col_index, np.abs(A.values))
+    vals = A.values
+    absA = CSR_Matrix(n, n, A.row_offset, A.col_index, vals.abs() if hasattr(vals, "abs") else np.abs(vals))
     den = torch.zeros(n, dtype=torch.float64, device=dev)
     xa = xd.abs()
     call("spops_spmv", ctx.handle, dbl(1.0), absA.device(ctx).handle, vp(xa.data_ptr()), dbl(0.0),

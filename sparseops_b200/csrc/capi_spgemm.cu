@@ -209,6 +209,7 @@ spops_status_t spops_pairs_cluster(spops_context_t ctx, spops_matrix_t A, spops_
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_INVALID, "spops_pairs_cluster: A must be a CSR matrix");
   DeviceGuard g(ctx->device);
   const PairSet& P = *pairs;
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf perm(ctx), offs(ctx);
   SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(A->rows, 1) * 8));
   SPOPS_TRY(offs.alloc(((size_t)A->rows + 1) * 8));
@@ -268,6 +269,7 @@ spops_status_t spops_spgemm_lsh(spops_context_t ctx, spops_matrix_t A, spops_mat
   DeviceGuard g(ctx->device);
   SpgemmStats s;
   auto t0 = std::chrono::steady_clock::now();
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf sig(ctx);
   SPOPS_TRY(sig.alloc((size_t)std::max<int64_t>(A->rows, 1) * (size_t)std::max(k, 1) * 8));
   spops_status_t st = minhash_signatures(ctx, A, k, seed, sig.as<uint64_t>());

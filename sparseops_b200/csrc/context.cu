@@ -95,6 +95,36 @@ void Context::pool_free(void* q) {
   if (q) cudaFreeAsync(q, stream);
 }
 
+ArenaScope::ArenaScope(Context* c) : ctx(c) {
+  if (ctx->arena_depth++ > 0) {
+    mark = ctx->arena_top;
+    return;
+  }
+  // the last scope's work on another stream may still read the arena
+  if (ctx->arena_done && ctx->arena_stream != ctx->stream) cudaStreamWaitEvent(ctx->stream, ctx->arena_done, 0);
+  if (ctx->arena_need > ctx->arena.bytes) {  // regrow to what the earlier scopes needed
+    const size_t want = ((ctx->arena_need + ctx->arena_need / 8) + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+    cudaDeviceSynchronize();  // queued work may still read the old arena
+    ctx->arena.release();
+    if (ctx->arena.alloc(want) != SPOPS_OK) {  // no room: temporaries keep coming from the pool
+      ctx->arena.release();
+      cudaGetLastError();
+    }
+    ctx->arena_need = 0;
+  }
+  ctx->arena_top = 0;
+  ctx->arena_over = 0;
+  mark = 0;
+}
+
+ArenaScope::~ArenaScope() {
+  ctx->arena_top = mark;
+  if (--ctx->arena_depth > 0) return;
+  if (!ctx->arena_done) cudaEventCreateWithFlags(&ctx->arena_done, cudaEventDisableTiming);
+  if (ctx->arena_done) cudaEventRecord(ctx->arena_done, ctx->stream);
+  ctx->arena_stream = ctx->stream;
+}
+
 spops_status_t Context::scratch_reserve(size_t n) {
   if (scratch.bytes >= n && scratch.p) return SPOPS_OK;
   // work queued on the stream may still read the old scratch
@@ -171,6 +201,11 @@ spops_status_t spops_destroy(spops_context_t c) {
   if (c->in_stream) cudaStreamDestroy(c->in_stream);
   for (cudaEvent_t e : c->file_events) cudaEventDestroy(e);
   for (void* b : c->file_stage) cudaFreeHost(b);
+  if (c->arena_done) {
+    cudaEventSynchronize(c->arena_done);
+    cudaEventDestroy(c->arena_done);
+  }
+  c->arena.release();
   if (c->pool) {
     cudaStreamSynchronize(c->stream);
     cudaMemPoolDestroy(c->pool);

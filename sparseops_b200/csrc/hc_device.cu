@@ -291,6 +291,7 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
   const int64_t n = A->rows;
   Trace tr("hc");
   // rows
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf parent(ctx), size(ctx), open(ctx), res(ctx), flags(ctx);
   const size_t nn = (size_t)std::max<int64_t>(n, 1);
   SPOPS_TRY(parent.alloc(nn * 4));
@@ -355,10 +356,10 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
       while (slots2 < (uint64_t)(2 * ncap)) slots2 <<= 1;
       SPOPS_TRY(seen2.alloc((size_t)slots2 * 8));
       SPOPS_CUDA(cudaMemsetAsync(seen2.p, 0xff, (size_t)slots2 * 8, st));
-      std::swap(ts.p, ts2.p), std::swap(ts.bytes, ts2.bytes);
-      std::swap(ti.p, ti2.p), std::swap(ti.bytes, ti2.bytes);
-      std::swap(tj.p, tj2.p), std::swap(tj.bytes, tj2.bytes);
-      std::swap(seen.p, seen2.p), std::swap(seen.bytes, seen2.bytes);
+      ts.swap(ts2);
+      ti.swap(ti2);
+      tj.swap(tj2);
+      seen.swap(seen2);
       seen_slots = slots2;
       cap = ncap;
       T = Tasks{ts.as<double>(), ti.as<int32_t>(), tj.as<int32_t>()};

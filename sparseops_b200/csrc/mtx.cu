@@ -512,6 +512,7 @@ spops_status_t parse_coo(Context* ctx, const char* text, size_t n, spops_index_t
   SPOPS_TRY(check_header(H, itype));
   const int64_t len = (int64_t)(n - H.data);
   Trace tr("mtx");
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf dtext(ctx);
   SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
   if (len > 0) SPOPS_CUDA(cudaMemcpyAsync(dtext.p, text + H.data, (size_t)len, cudaMemcpyHostToDevice, ctx->stream));
@@ -599,6 +600,7 @@ spops_status_t read_path(Context* ctx, const char* path, spops_index_t itype, sp
   }
   SPOPS_TRY(check_header(H, itype));
   const int64_t len = size - (int64_t)H.data;
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf dtext(ctx);
   SPOPS_TRY(dtext.alloc((size_t)std::max<int64_t>(len, 1)));
   tr.mark(ctx->stream, "open + header + text buffer");

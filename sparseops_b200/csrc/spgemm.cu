@@ -1150,6 +1150,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   Timer tm;
   Trace tr("spgemm");
   // --- permutation, offsets, per-row cluster
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf perm(ctx), offs(ctx), rowcl(ctx), rlen(ctx), rpr(ctx), keys(ctx), skeys(ctx), src(ctx), ssrc(ctx), flag(ctx), uidx(ctx), colids(ctx), ncols_u(ctx), cptr(ctx), cptr_val(ctx), avals(ctx), row_of_entry(ctx), tmp(ctx);
   SPOPS_TRY(perm.alloc((size_t)std::max<int64_t>(n, 1) * 8));
   SPOPS_TRY(offs.alloc((size_t)(ncl + 1) * 8));
@@ -1438,7 +1439,10 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     const int64_t* dl = slist.as<int64_t>() + tstart[q];
     const int tbits = 5 + q;
 #define SPOPS_SORT_LAUNCH(RR)                                                                                    \
-  sort_accum_kernel<I, V, RR><<<grid, 32 * kSortWarps, 0, st>>>(                                                \
+  if (sort_accum_smem<V, RR>() > 48 * 1024)                                                                      \
+    SPOPS_CUDA(cudaFuncSetAttribute(sort_accum_kernel<I, V, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                    (int)sort_accum_smem<V, RR>()));                                              \
+  sort_accum_kernel<I, V, RR><<<grid, 32 * kSortWarps, sort_accum_smem<V, RR>(), st>>>(                         \
       dl, m, cptr.as<int64_t>(), cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), \
       B->row.as<I>(), B->col.as<I>(), B->val.as<V>(), tbits, b_rowdense, l2_budget, sort_output, rowwise,        \
       soff.as<int64_t>(), soff_val.as<int64_t>(), nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>(),      \
@@ -1718,6 +1722,7 @@ spops_status_t vl_from_csr_t(Context* ctx, Matrix* A, const int64_t* offs_h, int
   cudaStream_t st = ctx->stream;
   const int64_t n = A->rows, nnz = A->nnz;
   const size_t nn = (size_t)std::max<int64_t>(n, 1), nz1 = (size_t)std::max<int64_t>(nnz, 1);
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf perm(ctx), offs(ctx), rowcl(ctx), rlen(ctx), rpr(ctx), keys(ctx), skeys(ctx), src(ctx), ssrc(ctx),
       flag(ctx), uidx(ctx), colids(ctx), ncols_u(ctx), cptr(ctx), cptr_val(ctx), cw(ctx), avals(ctx), roe(ctx),
       tmp(ctx);
@@ -1813,6 +1818,7 @@ spops_status_t vl_to_csr_t(Context* ctx, Matrix* M, Matrix** out) {
   cudaStream_t st = ctx->stream;
   const int64_t n = M->rows, ncl = M->clusters;
   const size_t nn = (size_t)std::max<int64_t>(n, 1);
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf rowcl(ctx), cnt(ctx), crp(ctx), tmp(ctx);
   SPOPS_TRY(rowcl.alloc(nn * 8));
   SPOPS_TRY(cnt.alloc((nn + 1) * 8));

@@ -15,6 +15,11 @@
 // (src/spgemm_Vlength_mixed.cpp:267-319) and its drop rule for the cluster
 // without a symbolic pass.
 //
+// Each product's B value (its A value too, for a one-row cluster: then the
+// product itself) and its cluster column are parked in the warp's slice of
+// dynamic shared memory at index t while the keys are built, so that after
+// the sort a key's low bits find its operands with one shared-memory read.
+//
 // Output goes to the cluster's slab: ccol[soff[c] ..], cval[soff_val[c] ..]
 // (room for P columns), columns ascending, values [column x csz] with the
 // rows of the cluster interleaved -- the same layout the hash kernels write.
@@ -32,52 +37,55 @@ namespace {
 constexpr int kSortCols = 256;  // cluster columns staged per warp
 constexpr int kSortWarps = 4;   // warps per block
 
+// dynamic shared memory of sort_accum_kernel<I, V, R>: per warp 32R values
+// and 32R one-byte cluster columns
+template <typename V, int R>
+constexpr size_t sort_accum_smem() {
+  return (size_t)kSortWarps * 32 * R * (sizeof(V) + 1);
+}
+
 // Ascending bitonic sort of 32*R keys, blocked: element e = lane*R + s.
-template <int R>
-__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&k)[R], int lane) {
+// Stages are instantiated by template recursion so that every partner slot
+// index is a compile-time constant and the keys stay in registers.
+template <int R, int KK, int JJ>
+__device__ __forceinline__ void bitonic_stage(uint32_t (&k)[R], int lane) {
   constexpr int N = 32 * R;
+  if constexpr (JJ >= R) {  // partner: lane ^ (JJ / R), same slot
+    constexpr int lm = JJ / R;
+    const bool lower = (lane & lm) == 0;
+    const bool asc = (KK >= N) ? true : ((lane & (KK / R)) == 0);
+    const bool keep_min = lower == asc;
 #pragma unroll
-  for (int kk = 2; kk <= N; kk <<= 1) {
+    for (int s = 0; s < R; ++s) {
+      const uint32_t o = __shfl_xor_sync(0xffffffffu, k[s], lm);
+      k[s] = keep_min ? min(k[s], o) : max(k[s], o);
+    }
+  } else {  // partner: slot s ^ JJ of the same lane
+    const bool lane_asc = (KK >= N) ? true : ((lane & (KK / R)) == 0);
 #pragma unroll
-    for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-      if (jj >= R) {  // partner: lane ^ (jj / R), same slot
-        const int lm = jj / R;
-        const bool lower = (lane & lm) == 0;
-        const bool asc = (kk >= N) ? true : ((lane & (kk / R)) == 0);
-        const bool keep_min = lower == asc;
-#pragma unroll
-        for (int s = 0; s < R; ++s) {
-          const uint32_t o = __shfl_xor_sync(0xffffffffu, k[s], lm);
-          k[s] = keep_min ? min(k[s], o) : max(k[s], o);
-        }
-      } else {  // partner: slot s ^ jj of the same lane
-#pragma unroll
-        for (int s = 0; s < R; ++s) {
-          const int p = s ^ jj;
-          if (p > s) {
-            bool asc;
-            if (kk < R) asc = (s & kk) == 0;
-            else if (kk >= N) asc = true;
-            else asc = (lane & (kk / R)) == 0;
-            const uint32_t a = k[s], b = k[p];
-            const uint32_t lo = min(a, b), hi = max(a, b);
-            k[s] = asc ? lo : hi;
-            k[p] = asc ? hi : lo;
-          }
-        }
+    for (int s = 0; s < R; ++s) {
+      const int p = s ^ JJ;
+      if (p > s) {
+        const bool asc = KK < R ? (s & KK) == 0 : lane_asc;
+        const uint32_t a = k[s], b = k[p];
+        const uint32_t lo = min(a, b), hi = max(a, b);
+        k[s] = asc ? lo : hi;
+        k[p] = asc ? hi : lo;
       }
     }
   }
+  if constexpr (JJ > 1) bitonic_stage<R, KK, JJ / 2>(k, lane);
 }
 
-// largest j in [0, nj) with off[j] <= t (off ascending, off[0] = 0)
-__device__ __forceinline__ int sort_find_col(const int32_t* off, int nj, int32_t t) {
-  int lo = 0, hi = nj;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= t) lo = mid; else hi = mid;
-  }
-  return lo;
+template <int R, int KK>
+__device__ __forceinline__ void bitonic_pass(uint32_t (&k)[R], int lane) {
+  bitonic_stage<R, KK, KK / 2>(k, lane);
+  if constexpr (KK < 32 * R) bitonic_pass<R, KK * 2>(k, lane);
+}
+
+template <int R>
+__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&k)[R], int lane) {
+  bitonic_pass<R, 2>(k, lane);
 }
 
 template <typename I, typename V, int R>
@@ -92,7 +100,10 @@ __global__ void __launch_bounds__(32 * kSortWarps)
                       unsigned long long* __restrict__ ndense, int32_t* __restrict__ ccol, V* __restrict__ cval) {
   __shared__ int32_t s_off[kSortWarps][kSortCols + 1];
   __shared__ int64_t s_start[kSortWarps][kSortCols];
+  extern __shared__ __align__(16) unsigned char sort_dyn_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  V* pv = reinterpret_cast<V*>(sort_dyn_smem) + (size_t)w * 32 * R;  // per product: value or B value
+  unsigned char* pj = sort_dyn_smem + (size_t)kSortWarps * 32 * R * sizeof(V) + (size_t)w * 32 * R;  // its column
   const int64_t b = blockIdx.x * (int64_t)kSortWarps + w;
   if (b >= nlist) return;
   const int64_t c = list[b];
@@ -126,6 +137,7 @@ __global__ void __launch_bounds__(32 * kSortWarps)
   const int32_t P = off[nj];
   // keys: slot s of this lane holds product t = s*32 + lane before sorting
   constexpr uint32_t kNone = 0xffffffffu;
+  const int64_t vbase = cptr_val[c];
   uint32_t key[R];
   {
     int j = 0;
@@ -137,9 +149,17 @@ __global__ void __launch_bounds__(32 * kSortWarps)
         while (off[j + 1] <= t) ++j;
         const int64_t k = start[j] + (t - off[j]);
         key[s] = ((uint32_t)bci[k] << tbits) | (uint32_t)t;
+        const V b = bv[k];
+        if (csz == 1) {
+          pv[t] = avals[vbase + j] * b;
+        } else {
+          pv[t] = b;
+          pj[t] = (unsigned char)j;
+        }
       }
     }
   }
+  __syncwarp();
   warp_bitonic_sort<R>(key, lane);
   const uint32_t tmask = (1u << tbits) - 1u;
   // column starts in this lane's sorted run; the distinct-column count
@@ -185,7 +205,7 @@ __global__ void __launch_bounds__(32 * kSortWarps)
     drop_out[c] = drop ? 1 : 0;
     if (dense && !rowwise) atomicAdd(ndense, 1ULL);
   }
-  const int64_t co = soff[c], cvo = soff_val[c], vbase = cptr_val[c];
+  const int64_t co = soff[c], cvo = soff_val[c];
   // output columns
   {
     int r = base;
@@ -202,8 +222,7 @@ __global__ void __launch_bounds__(32 * kSortWarps)
     for (int s = 0; s < R; ++s) {
       if (key[s] != kNone) {
         const int32_t t = (int32_t)(key[s] & tmask);
-        const int j = sort_find_col(off, nj, t);
-        const V v = avals[vbase + (int64_t)j * csz + l] * bv[start[j] + (t - off[j])];
+        const V v = csz == 1 ? pv[t] : avals[vbase + (int64_t)pj[t] * csz + l] * pv[t];
         if (first >> s & 1ULL) {
           if (seen) {
             const V o = (csz == 1 && drop && fabs((double)run) < 1e-12) ? V(0) : run;

@@ -257,6 +257,7 @@ spops_status_t topk_t(Context* ctx, Matrix* A, int64_t top_k, Matrix** out) {
   const int64_t cnnz = Cn->nnz;
   // 3. keys and the best k per row: a warp selection for k <= 32, else a
   //    per-row stable sort
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   PoolBuf key(ctx), skey(ctx), col(ctx), scol(ctx), diag(ctx), kept(ctx), orp(ctx), tmp(ctx);
   if (top_k <= 32) {
     const int k = (int)std::max<int64_t>(top_k, 0);

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <string>
 #include <functional>
+#include <utility>
 #include <vector>
 
 #include "../../include/sparseops_b200.h"
@@ -92,6 +93,20 @@ struct Context {
   cudaMemPool_t pool = nullptr;
   spops_status_t pool_alloc(void** p, size_t bytes);
   void pool_free(void* p);
+  // arena for the temporaries of one call inside an ArenaScope: one buffer
+  // kept by the context and handed out by a bump pointer, so a call whose
+  // temporaries are the same sizes as the last one's maps no memory.  (The
+  // stream-ordered pool remaps its free pages into a new range when no free
+  // range fits, at several microseconds per 2 MB page.)  An allocation that
+  // does not fit goes to the pool; the arena is then regrown, between calls,
+  // to the largest total the scopes asked for.
+  DevBuf arena;
+  size_t arena_top = 0;       // bytes handed out
+  size_t arena_over = 0;      // bytes of live pool allocations made in a scope
+  size_t arena_need = 0;      // largest arena_top + arena_over seen
+  int arena_depth = 0;        // open ArenaScopes
+  cudaEvent_t arena_done = nullptr;    // recorded when the outermost scope ends
+  cudaStream_t arena_stream = nullptr;  // the stream that event was recorded on
 };
 
 // Temporary device buffer of one API call, from the context's pool and
@@ -118,10 +133,16 @@ struct Trace {
   }
 };
 
+// Temporary device buffer of one API call.  Inside an ArenaScope it comes
+// from the context's arena (released with the scope; the newest buffer is
+// handed back at once when released first), otherwise, and when the arena is
+// full, from the stream-ordered pool.
 struct PoolBuf {
   Context* ctx;
   void* p = nullptr;
   size_t bytes = 0;
+  size_t span = 0;     // arena bytes taken (0: pool memory)
+  bool over = false;   // pool memory counted in ctx->arena_over
   explicit PoolBuf(Context* c) : ctx(c) {}
   PoolBuf(const PoolBuf&) = delete;
   PoolBuf& operator=(const PoolBuf&) = delete;
@@ -129,20 +150,68 @@ struct PoolBuf {
   spops_status_t alloc(size_t n) {
     release();
     if (n == 0) n = 16;
+    if (ctx->arena_depth > 0) {
+      const size_t a = (n + 255) & ~size_t(255);
+      if (ctx->arena_top + a <= ctx->arena.bytes) {
+        p = static_cast<char*>(ctx->arena.p) + ctx->arena_top;
+        ctx->arena_top += a;
+        span = a;
+        bytes = n;
+        note_need();
+        return SPOPS_OK;
+      }
+      over = true;
+      ctx->arena_over += a;
+      note_need();
+    }
     spops_status_t s = ctx->pool_alloc(&p, n);
     if (s != SPOPS_OK) {
       p = nullptr;
+      if (over) ctx->arena_over -= (n + 255) & ~size_t(255);
+      over = false;
       return s;
     }
     bytes = n;
     return SPOPS_OK;
   }
   void release() {
-    if (p) ctx->pool_free(p);
+    if (p && span) {
+      if (static_cast<char*>(p) + span == static_cast<char*>(ctx->arena.p) + ctx->arena_top) ctx->arena_top -= span;
+    } else if (p) {
+      ctx->pool_free(p);
+      if (over) ctx->arena_over -= (bytes + 255) & ~size_t(255);
+    }
     p = nullptr;
-    bytes = 0;
+    bytes = span = 0;
+    over = false;
+  }
+  void swap(PoolBuf& o) {
+    std::swap(p, o.p);
+    std::swap(bytes, o.bytes);
+    std::swap(span, o.span);
+    std::swap(over, o.over);
   }
   template <typename T> T* as() const { return static_cast<T*>(p); }
+
+ private:
+  void note_need() {
+    const size_t t = ctx->arena_top + ctx->arena_over;
+    if (t > ctx->arena_need) ctx->arena_need = t;
+  }
+};
+
+// The temporaries of the calls made while an ArenaScope is open come from
+// the context's arena (PoolBuf).  Declare it before the call's PoolBufs.
+// Opening the outermost scope regrows the arena to what earlier scopes
+// needed (after the stream's queued work, which may still read it) and
+// orders this stream after the last scope's work on another stream.
+struct ArenaScope {
+  Context* ctx;
+  size_t mark = 0;
+  explicit ArenaScope(Context* c);
+  ~ArenaScope();
+  ArenaScope(const ArenaScope&) = delete;
+  ArenaScope& operator=(const ArenaScope&) = delete;
 };
 
 // RAII guard: make ctx->device current for the duration of an API call.
