@@ -410,20 +410,20 @@ def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
         ("ell", lambda: F.csr_to_ell(A, F.ColMajor), F.SpOps_ell),
     ]
 
-    def no_tails(conv):  # the same conversion with every chunk's slots read in place
+    def tails(conv):  # the same conversion with row-contiguous tails past each chunk's fourth-longest row
         def run():
             from sparseops_b200 import default_context
             c = default_context()
-            c.set_option("sell_tails", 0)
+            c.set_option("sell_tails", 1)
             try:
                 return conv()
             finally:
-                c.set_option("sell_tails", 1)
+                c.set_option("sell_tails", 0)
         return run
-    cands.insert(2, ("sell_c_sigma C=32 sigma=512 col-major, no tails",
-                     no_tails(lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.ColMajor)), F.SpOps_sell_c_sigma))
-    cands.insert(5, ("sell_c_R C=32 col-major, no tails",
-                     no_tails(lambda: F.csr_to_sell_c_R(A, None, 32, 1, F.ColMajor)), F.SpOps_sell_c_R))
+    cands.insert(2, ("sell_c_sigma C=32 sigma=512 col-major, tails",
+                     tails(lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.ColMajor)), F.SpOps_sell_c_sigma))
+    cands.insert(5, ("sell_c_R C=32 col-major, tails",
+                     tails(lambda: F.csr_to_sell_c_R(A, None, 32, 1, F.ColMajor)), F.SpOps_sell_c_R))
     for name, conv, op in cands:
         try:
             torch.cuda.synchronize()
@@ -694,13 +694,14 @@ def bench_fwd_bwd(ctx, dev, n=1 << 20, peak=None, cpu_ref=False):
 
 
 def bench_spgemm(dev, cpu_ref: bool, n=524288, peak=None):
-    """LeSpGEMM C = A A^T on the planted-community matrix (2,048 communities,
-    85 % in-community, row nnz lognormal mean 20): MinHash (64), LSH (16
-    bands), clustering (8), cluster-wise kernel-3 SpGEMM."""
+    """LeSpGEMM C = A A^T on the planted-community matrix (communities of 256
+    rows: 2,048 at n = 524,288; 85 % in-community, row nnz lognormal mean
+    20): MinHash (64), LSH (16 bands), clustering (8), cluster-wise kernel-3
+    SpGEMM."""
     import torch
     from sparseops_b200 import CSR_Matrix, synth
     from sparseops_b200.spgemm import LeSpGEMM_clustered, LeSpGEMM_lsh
-    arp, aci, av = synth.planted_communities(n, ncomm=2048, mean=20.0, seed=5)
+    arp, aci, av = synth.planted_communities(n, ncomm=max(1, n // 256), mean=20.0, seed=5)
     brp, bci, bv = synth.transpose(arp, aci, av, n)
     A = CSR_Matrix(n, n, torch.from_numpy(arp).to(dev), torch.from_numpy(aci).to(dev), torch.from_numpy(av).to(dev))
     B = CSR_Matrix(n, n, torch.from_numpy(brp).to(dev), torch.from_numpy(bci).to(dev), torch.from_numpy(bv).to(dev))
@@ -978,7 +979,7 @@ def run_section(args):
         elif args.section == "mtx":
             res = bench_mtx(cpu)
         elif args.section == "spgemm":
-            res = bench_spgemm(dev, cpu, peak=peak)
+            res = bench_spgemm(dev, cpu, n=args.spgemm_rows, peak=peak)
         elif args.section == "laplacian":
             res = bench_laplacian(ctx, dev, peak, cpu)
         elif args.section == "formats":
@@ -1193,6 +1194,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-format, batched, fwd+bwd and SpGEMM sections")
     ap.add_argument("--csr-variant", type=int, default=0, help="CSR kernel shape (spops_set_option)")
+    ap.add_argument("--spgemm-rows", type=int, default=524288,
+                    help="rows of the SpGEMM section's matrices (a smaller case for profiling captures)")
     ap.add_argument("--rows", type=int, default=N_ROWS,
                     help="matrix rows (default: the benchmark size; smaller only for profiling captures)")
     args = ap.parse_args()

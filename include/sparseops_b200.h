@@ -124,10 +124,10 @@ spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
  *   segment's x window [r0 - H, r0 + rows + H) in shared memory, H in
  *   {16, 32, 64} from the matrix's band profile (0, the default: plain
  *   gathers).  Read when a batch is prepared and launched.
- *   "sell_tails" 1 / 0: SELL with C = 32, column-major: each 32-row chunk's
+ *   "sell_tails" 0 / 1: SELL with C = 32, column-major: each 32-row chunk's
  *   slots beyond its fourth-longest row (held by at most three rows) are
- *   also kept row-contiguous and read from there (1, the default), or read
- *   in place (0).  Read when the matrix is converted or uploaded. */
+ *   read in place (0, the default), or also kept row-contiguous and read from
+ *   there (1).  Read when the matrix is converted or uploaded. */
 spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);

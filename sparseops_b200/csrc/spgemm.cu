@@ -86,11 +86,19 @@ __device__ __forceinline__ uint32_t hash_find(const int32_t* tab, uint32_t mask,
 }
 
 // ----------------------------------------------------------- reorder + clusters
+// bits that hold every value below m (at least 1)
+inline int key_bits(int64_t m) {
+  int b = 1;
+  while (b < 62 && (int64_t(1) << b) < m) ++b;
+  return b;
+}
+
 template <typename I, typename V>
 __global__ void cluster_keys_kernel(const I* __restrict__ rp, const I* __restrict__ ci, const int64_t* __restrict__ perm,
                                     const int64_t* __restrict__ row_cluster, int64_t n, const int64_t* __restrict__ rpr,
-                                    uint64_t* __restrict__ keys, int64_t* __restrict__ src) {
-  // warp per reordered row: entries of original row perm[r] in order
+                                    int shift, uint64_t* __restrict__ keys, int64_t* __restrict__ src) {
+  // warp per reordered row: entries of original row perm[r] in order; key =
+  // cluster << shift | column (shift: the bits of A's column count)
   const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (r >= n) return;
@@ -98,7 +106,7 @@ __global__ void cluster_keys_kernel(const I* __restrict__ rp, const I* __restric
   const int64_t s = rp[orow], e = rp[orow + 1], o = rpr[r];
   const uint64_t c = (uint64_t)row_cluster[r];
   for (int64_t k = lane; k < e - s; k += 32) {
-    keys[o + k] = (c << 32) | (uint64_t)(uint32_t)ci[s + k];
+    keys[o + k] = (c << shift) | (uint64_t)(uint32_t)ci[s + k];
     src[o + k] = s + k;  // entry of A
   }
 }
@@ -123,25 +131,25 @@ __global__ void key_flag_kernel(const uint64_t* __restrict__ keys, int64_t m, in
 
 // per unique key: its cluster's column count, and the column itself
 __global__ void cluster_cols_kernel(const uint64_t* __restrict__ keys, const int64_t* __restrict__ flag,
-                                    const int64_t* __restrict__ uidx, int64_t m, int32_t* __restrict__ colids,
+                                    const int64_t* __restrict__ uidx, int64_t m, int shift, int32_t* __restrict__ colids,
                                     unsigned long long* __restrict__ ncols) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= m || !flag[i]) return;
   const int64_t u = uidx[i] - 1;
-  colids[u] = (int32_t)(keys[i] & 0xffffffffULL);
-  atomicAdd(ncols + (keys[i] >> 32), 1ULL);
+  colids[u] = (int32_t)(keys[i] & ((1ULL << shift) - 1ULL));
+  atomicAdd(ncols + (keys[i] >> shift), 1ULL);
 }
 
 template <typename I, typename V>
 __global__ void cluster_vals_kernel(const uint64_t* __restrict__ keys, const int64_t* __restrict__ src,
-                                    const int64_t* __restrict__ uidx, int64_t m, const V* __restrict__ av,
+                                    const int64_t* __restrict__ uidx, int64_t m, int shift, const V* __restrict__ av,
                                     const I* __restrict__ rp, const int64_t* __restrict__ perm,
                                     const int64_t* __restrict__ offsets, const int64_t* __restrict__ cptr,
                                     const int64_t* __restrict__ cptr_val, const int64_t* __restrict__ row_of_entry,
                                     V* __restrict__ cvals) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= m) return;
-  const int64_t c = (int64_t)(keys[i] >> 32);
+  const int64_t c = (int64_t)(keys[i] >> shift);
   const int64_t u = uidx[i] - 1;
   const int64_t l = row_of_entry[src[i]] - offsets[c];  // row within the cluster
   const int64_t csz = offsets[c + 1] - offsets[c];
@@ -1184,9 +1192,11 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used);
     std::fprintf(stderr, "[spgemm] pool reserved %.1f MB, used %.1f MB\n", rsv / 1e6, used / 1e6);
   }
+  // key = cluster << kshift | column: sort only the bits in use
+  const int kshift = key_bits(A->cols), kend = std::min(64, kshift + key_bits(ncl));
   if (n > 0) {
     cluster_keys_kernel<I, V><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), perm.as<int64_t>(),
-                                                                rowcl.as<int64_t>(), n, rpr.as<int64_t>(),
+                                                                rowcl.as<int64_t>(), n, rpr.as<int64_t>(), kshift,
                                                                 keys.as<uint64_t>(), src.as<int64_t>());
     entry_row_kernel<I><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), perm.as<int64_t>(), n,
                                                           row_of_entry.as<int64_t>());
@@ -1198,11 +1208,11 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   if (nnz > 0) {
     size_t c1 = 0, c2 = 0;
     SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, c1, keys.as<uint64_t>(), skeys.as<uint64_t>(), src.as<int64_t>(),
-                                               ssrc.as<int64_t>(), nnz, 0, 64, st));
+                                               ssrc.as<int64_t>(), nnz, 0, kend, st));
     SPOPS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, c2, flag.as<int64_t>(), uidx.as<int64_t>(), nnz, st));
     SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
     SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, c1, keys.as<uint64_t>(), skeys.as<uint64_t>(), src.as<int64_t>(),
-                                               ssrc.as<int64_t>(), nnz, 0, 64, st));
+                                               ssrc.as<int64_t>(), nnz, 0, kend, st));
     key_flag_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), nnz, flag.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
     SPOPS_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, c2, flag.as<int64_t>(), uidx.as<int64_t>(), nnz, st));
@@ -1213,7 +1223,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_TRY(colids.alloc((size_t)std::max<int64_t>(nnzc, 1) * 4));
   if (nnz > 0) {
     cluster_cols_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), flag.as<int64_t>(), uidx.as<int64_t>(),
-                                                       nnz, colids.as<int32_t>(),
+                                                       nnz, kshift, colids.as<int32_t>(),
                                                        reinterpret_cast<unsigned long long*>(ncols_u.p));
     SPOPS_LAUNCH_CHECK();
   }
@@ -1246,7 +1256,7 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   SPOPS_CUDA(cudaMemsetAsync(avals.p, 0, avals.bytes, st));
   if (nnz > 0) {
     cluster_vals_kernel<I, V><<<grid_for(nnz), 256, 0, st>>>(
-        skeys.as<uint64_t>(), ssrc.as<int64_t>(), uidx.as<int64_t>(), nnz, A->val.as<V>(), A->row.as<I>(),
+        skeys.as<uint64_t>(), ssrc.as<int64_t>(), uidx.as<int64_t>(), nnz, kshift, A->val.as<V>(), A->row.as<I>(),
         perm.as<int64_t>(), offs.as<int64_t>(), cptr.as<int64_t>(), cptr_val.as<int64_t>(),
         row_of_entry.as<int64_t>(), avals.as<V>());
     SPOPS_LAUNCH_CHECK();
@@ -1439,9 +1449,9 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
     const int64_t* dl = slist.as<int64_t>() + tstart[q];
     const int tbits = 5 + q;
 #define SPOPS_SORT_LAUNCH(RR)                                                                                    \
-  if (sort_accum_smem<V, RR>() > 48 * 1024)                                                                      \
-    SPOPS_CUDA(cudaFuncSetAttribute(sort_accum_kernel<I, V, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                                    (int)sort_accum_smem<V, RR>()));                                              \
+  /* static + dynamic shared memory can pass 48 KB: raise the limit */                                         \
+  SPOPS_CUDA(cudaFuncSetAttribute(sort_accum_kernel<I, V, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                  (int)sort_accum_smem<V, RR>()));                                                \
   sort_accum_kernel<I, V, RR><<<grid, 32 * kSortWarps, sort_accum_smem<V, RR>(), st>>>(                         \
       dl, m, cptr.as<int64_t>(), cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), \
       B->row.as<I>(), B->col.as<I>(), B->val.as<V>(), tbits, b_rowdense, l2_budget, sort_output, rowwise,        \
@@ -1747,9 +1757,11 @@ spops_status_t vl_from_csr_t(Context* ctx, Matrix* A, const int64_t* offs_h, int
   SPOPS_TRY(flag.alloc(nz1 * 8));
   SPOPS_TRY(uidx.alloc(nz1 * 8));
   SPOPS_TRY(roe.alloc(nz1 * 8));
+  // key = cluster << kshift | column: sort only the bits in use
+  const int kshift = key_bits(A->cols), kend = std::min(64, kshift + key_bits(ncl));
   if (n > 0) {
     cluster_keys_kernel<I, V><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), perm.as<int64_t>(),
-                                                                rowcl.as<int64_t>(), n, rpr.as<int64_t>(),
+                                                                rowcl.as<int64_t>(), n, rpr.as<int64_t>(), kshift,
                                                                 keys.as<uint64_t>(), src.as<int64_t>());
     entry_row_kernel<I><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), perm.as<int64_t>(), n, roe.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
@@ -1760,11 +1772,11 @@ spops_status_t vl_from_csr_t(Context* ctx, Matrix* A, const int64_t* offs_h, int
   if (nnz > 0) {
     size_t c1 = 0, c2 = 0;
     SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, c1, keys.as<uint64_t>(), skeys.as<uint64_t>(), src.as<int64_t>(),
-                                               ssrc.as<int64_t>(), nnz, 0, 64, st));
+                                               ssrc.as<int64_t>(), nnz, 0, kend, st));
     SPOPS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, c2, flag.as<int64_t>(), uidx.as<int64_t>(), nnz, st));
     SPOPS_TRY(tmp.alloc(std::max(c1, c2) + 256));
     SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, c1, keys.as<uint64_t>(), skeys.as<uint64_t>(), src.as<int64_t>(),
-                                               ssrc.as<int64_t>(), nnz, 0, 64, st));
+                                               ssrc.as<int64_t>(), nnz, 0, kend, st));
     key_flag_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), nnz, flag.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
     SPOPS_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, c2, flag.as<int64_t>(), uidx.as<int64_t>(), nnz, st));
@@ -1774,7 +1786,7 @@ spops_status_t vl_from_csr_t(Context* ctx, Matrix* A, const int64_t* offs_h, int
   SPOPS_TRY(colids.alloc((size_t)std::max<int64_t>(nnzc, 1) * 4));
   if (nnz > 0) {
     cluster_cols_kernel<<<grid_for(nnz), 256, 0, st>>>(skeys.as<uint64_t>(), flag.as<int64_t>(), uidx.as<int64_t>(),
-                                                       nnz, colids.as<int32_t>(),
+                                                       nnz, kshift, colids.as<int32_t>(),
                                                        reinterpret_cast<unsigned long long*>(ncols_u.p));
     SPOPS_LAUNCH_CHECK();
   }
@@ -1804,7 +1816,7 @@ spops_status_t vl_from_csr_t(Context* ctx, Matrix* A, const int64_t* offs_h, int
   SPOPS_CUDA(cudaMemsetAsync(avals.p, 0, avals.bytes, st));
   if (nnz > 0) {
     cluster_vals_kernel<I, V><<<grid_for(nnz), 256, 0, st>>>(
-        skeys.as<uint64_t>(), ssrc.as<int64_t>(), uidx.as<int64_t>(), nnz, A->val.as<V>(), A->row.as<I>(),
+        skeys.as<uint64_t>(), ssrc.as<int64_t>(), uidx.as<int64_t>(), nnz, kshift, A->val.as<V>(), A->row.as<I>(),
         perm.as<int64_t>(), offs.as<int64_t>(), cptr.as<int64_t>(), cptr_val.as<int64_t>(), roe.as<int64_t>(),
         avals.as<V>());
     SPOPS_LAUNCH_CHECK();

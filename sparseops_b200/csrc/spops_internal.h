@@ -66,9 +66,10 @@ struct Context {
   // (measured slower on the 256-matrix batch than plain gathers, so off unless set)
   int batch_band = 0;
   // SELL (C = 32, column-major): a chunk's slots beyond its fourth-longest
-  // row are read from row-contiguous tails (1) or in place (0); read when the
-  // matrix is converted or uploaded
-  int sell_tails = 1;
+  // row are read from row-contiguous tails (1) or in place (0, the default:
+  // measured faster on the power-law matrix); read when the matrix is
+  // converted or uploaded
+  int sell_tails = 0;
   // pinned staging for host x / y in spops_spmv_host
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

@@ -10,7 +10,7 @@ or the oracle.
   pair list (16 bands) and the clustering permutation / offsets (cluster size
   8) bit-equal to the reference's minhash_signatures_flat,
   lsh_candidate_pairs_vector and hierarchical_clustering_v0_fast on the same
-  input; C bit-equal in row_ptr and per-row col_idx to the reference's kernel
+  input (the clustering both by the host loop and on the device); C bit-equal in row_ptr and per-row col_idx to the reference's kernel
   3 run through its test driver's flow (csr_reorder_rows,
   csr_to_vlength_cluster, LeSpGEMM_VLength, vlength_cluster2csr, inverse
   reorder; test/test_spgemm_hc_lsh.cpp:230-300) for sortOutput false and
@@ -75,8 +75,9 @@ def _rows_sorted(rp, ci, v):
 
 @pytest.mark.parametrize("workload", ["planted", "grouped"])
 def test_spgemm_full_config_vs_reference(cuda, full_ref, orc, workload):
-    from sparseops_b200.spgemm import (LeSpGEMM_clustered, hierarchical_clustering_v0_fast,
-                                       lsh_candidate_pairs_vector, minhash_signatures_flat)
+    from sparseops_b200.spgemm import (LeSpGEMM_clustered, hierarchical_clustering_device,
+                                       hierarchical_clustering_v0_fast, lsh_candidate_pairs_vector,
+                                       minhash_signatures_flat)
     n, nc, (arp, aci, av), (brp, bci, bv) = _spgemm_workload(workload)
     A, B = _dev_csr(arp, aci, av, nc), _dev_csr(brp, bci, bv, n)
     # MinHash signatures, 64 hashes, seed 7
@@ -84,13 +85,17 @@ def test_spgemm_full_config_vs_reference(cuda, full_ref, orc, workload):
     assert np.array_equal(sig, full_ref.minhash(arp, aci, 64, 7))
     del sig
     # LSH pairs, 16 bands (pairs, their order and their scores)
-    pairs = lsh_candidate_pairs_vector(A, 64, 16, 7).host()
+    dpairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
+    pairs = dpairs.host()
     rpi, rpj, rps = full_ref.lsh_pairs(arp, aci, 64, 16, 7)
     assert np.array_equal(pairs[0], rpi) and np.array_equal(pairs[1], rpj) and np.array_equal(pairs[2], rps)
     # clustering, cluster size 8
     perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
     rperm, roffs = full_ref.hc(arp, aci, rpi, rpj, rps, 8)
     assert np.array_equal(perm, rperm) and np.array_equal(offs, roffs)
+    dperm, doffs = hierarchical_clustering_device(A, dpairs, 8)  # the pipeline's clustering, on the device
+    assert np.array_equal(dperm, rperm) and np.array_equal(doffs, roffs)
+    del dpairs, dperm, doffs
     # error scale sum_k |a_ik b_kj| per entry of C (rows ascending)
     scale = orc.spgemm((arp, aci, av), (brp, bci, bv), perm, offs, sort_output=True)
     for so in (0, 1):
