@@ -184,6 +184,76 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_tile_kernel(const BatchI
   }
 }
 
+// Tile items with one right-hand side: the SpMV tile body (csr_tile.cuh; the
+// default single-matrix CSR kernel) over tiles [idx, idx + kTilesPerItem) of
+// the item's matrix, the next tile's entries loaded before this one's
+// gathers are used.
+template <typename I, typename V>
+__global__ void __launch_bounds__(kBatchBlock, 2) batch_tile1_kernel(const BatchItem* __restrict__ items,
+                                                                    int64_t nitems, const BatchMat* __restrict__ mats,
+                                                                    V alpha, V beta, bool bz,
+                                                                    unsigned long long* __restrict__ next_item) {
+  constexpr int K = 8;
+  const int lane = threadIdx.x & 31;
+  unsigned long long grab = 0, ahead = 0;
+  if (lane == 0) {
+    grab = atomicAdd(next_item, (unsigned long long)kGrab);
+    ahead = atomicAdd(next_item, (unsigned long long)kGrab);
+  }
+  grab = __shfl_sync(0xffffffffu, grab, 0);
+  for (;;) {
+    if ((int64_t)grab >= nitems) break;
+    const int64_t jend = (int64_t)grab + kGrab < nitems ? (int64_t)grab + kGrab : nitems;
+    for (int64_t j = (int64_t)grab; j < jend; ++j) {
+      const BatchItem it = items[j];
+      const BatchMat& M = mats[it.mat];
+      const I* ci = static_cast<const I*>(M.ci);
+      const V* val = static_cast<const V*>(M.val);
+      const V* x = static_cast<const V*>(M.x);
+      const int64_t t1 = it.idx + kTilesPerItem < M.tiles ? it.idx + kTilesPerItem : M.tiles;
+      I c[K];
+      V a[K];
+      int64_t t = it.idx;
+      tile_load<I, V, K>(ci, val, M.nnz, t, lane, c, a);
+      uint32_t flags = M.tflags[t * 32 + lane];
+      int64_t tr = M.tile_row[t];
+      for (; t < t1; ++t) {
+        V pr[K];
+#pragma unroll
+        for (int b = 0; b < K; ++b) pr[b] = a[b] * ld_gather(x + c[b]);
+        const uint32_t f = flags;
+        const int64_t r0 = tr;
+        if (t + 1 < t1) {
+          tile_load<I, V, K>(ci, val, M.nnz, t + 1, lane, c, a);
+          flags = M.tflags[(t + 1) * 32 + lane];
+          tr = M.tile_row[t + 1];
+        }
+        tile_finish<I, V, K>(static_cast<const I*>(M.rp), M.rows, M.nnz, t, lane, f, r0, pr, static_cast<V*>(M.y),
+                             alpha, beta, bz, static_cast<V*>(M.tcin), static_cast<V*>(M.tosum), M.topen);
+      }
+    }
+    grab = __shfl_sync(0xffffffffu, ahead, 0);
+    if (lane == 0 && (int64_t)grab < nitems) ahead = atomicAdd(next_item, (unsigned long long)kGrab);
+  }
+}
+
+// Calibration of every tile matrix of a single-vector batch (as below).
+template <typename V>
+__global__ void batch_calibrate1_kernel(const int64_t* __restrict__ cal_off, const int32_t* __restrict__ cal_mat,
+                                        int ncal, int64_t total, const BatchMat* __restrict__ mats, V alpha, V beta,
+                                        bool bz) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  int lo = 0, hi = ncal;  // last i with cal_off[i] <= g
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (cal_off[mid] <= g) lo = mid; else hi = mid;
+  }
+  const BatchMat& M = mats[cal_mat[lo]];
+  spmv_calibrate1<V>(g - cal_off[lo], M.tiles, static_cast<const V*>(M.tcin), static_cast<const V*>(M.tosum),
+                     M.topen, M.tempty, M.tnempty, static_cast<V*>(M.y), alpha, beta, bz);
+}
+
 // Calibration of every tile matrix: thread g takes entry g - cal_off[i] of
 // tile matrix i (its tiles, then its empty rows).
 template <typename V, int KC>
@@ -454,6 +524,34 @@ spops_status_t build_table(Batch* B) {
   return SPOPS_OK;
 }
 
+template <typename I, typename V>
+int tile1_blocks_per_sm() {
+  static int cache[kMaxDevices];
+  return blocks_per_sm(batch_tile1_kernel<I, V>, kBatchBlock, 0, cache);
+}
+
+template <typename I, typename V>
+spops_status_t launch_tiles1(Batch* B, double alpha, double beta, cudaStream_t st) {
+  const bool bz = beta == 0.0;
+  const int bps = tile1_blocks_per_sm<I, V>();
+  if (bps < 1) return fail(SPOPS_ERR_CUDA, "batch: kernel attributes could not be set");
+  int64_t grid = (int64_t)B->ctx->num_sms * bps;
+  const int64_t need = (B->ntitems + 7) / 8;
+  if (grid > need) grid = need;
+  SPOPS_CUDA(cudaMemsetAsync(B->tqueue.p, 0, 8, st));
+  batch_tile1_kernel<I, V><<<(unsigned)grid, kBatchBlock, 0, st>>>(B->titems.as<BatchItem>(), B->ntitems,
+                                                                  B->table.as<BatchMat>(), (V)alpha, (V)beta, bz,
+                                                                  B->tqueue.as<unsigned long long>());
+  SPOPS_LAUNCH_CHECK();
+  if (B->ncal_total > 0) {
+    batch_calibrate1_kernel<V><<<(unsigned)((B->ncal_total + 255) / 256), 256, 0, st>>>(
+        B->cal_off.as<int64_t>(), B->cal_mat.as<int32_t>(), B->ncal, B->ncal_total, B->table.as<BatchMat>(),
+        (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
+}
+
 template <typename I, typename V, int G>
 int tile_blocks_per_sm() {
   static int cache[kMaxDevices];
@@ -486,7 +584,8 @@ template <typename I, typename V>
 spops_status_t launch_batch(Batch* B, double alpha, double beta, cudaStream_t st) {
   const bool bz = beta == 0.0;
   if (B->ntitems > 0) {  // tile items, then their calibration
-    if (B->k == 8) SPOPS_TRY((launch_tiles<I, V, 2>(B, alpha, beta, st)));
+    if (B->k == 1) SPOPS_TRY((launch_tiles1<I, V>(B, alpha, beta, st)));
+    else if (B->k == 8) SPOPS_TRY((launch_tiles<I, V, 2>(B, alpha, beta, st)));
     else if (B->k == 16) SPOPS_TRY((launch_tiles<I, V, 4>(B, alpha, beta, st)));
     else SPOPS_TRY((launch_tiles<I, V, 8>(B, alpha, beta, st)));
   }
@@ -582,7 +681,13 @@ spops_status_t prepare(Batch* B) {
     // k = 8, 16, 32 over X rows at most 2k wide, vector loads aligned: register tiles
     const BatchMat& h = B->host[m];
     const size_t vs = A->vsize();
-    if (csr_tile_spmm_usable(A, h.x, h.ldx, B->k) && h.ldy >= B->k) {
+    if (B->k == 1 && !B->form[m] && csr_tile_usable(A, 0)) {  // CSR with one vector: SpMV tile items
+      if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(B->ctx, A, 8));
+      const size_t bytes = (size_t)A->plan.tiles.tiles * vs;
+      if (B->t_cin[m].bytes < bytes) SPOPS_TRY(B->t_cin[m].alloc(bytes));
+      if (B->t_osum[m].bytes < bytes) SPOPS_TRY(B->t_osum[m].alloc(bytes));
+      B->tile_ok[m] = 1;
+    } else if (csr_tile_spmm_usable(A, h.x, h.ldx, B->k) && h.ldy >= B->k) {
       if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(B->ctx, A, 8));
       const size_t bytes = (size_t)A->plan.tiles.tiles * (size_t)B->k * vs;
       if (B->t_cin[m].bytes < bytes) SPOPS_TRY(B->t_cin[m].alloc(bytes));

@@ -86,81 +86,6 @@ __global__ void tile_empty_kernel(const I* __restrict__ rp, int64_t n, int64_t* 
   if (r < n && rp[r] == rp[r + 1]) list[atomicAdd(count, 1ULL)] = r;
 }
 
-// Given the products p of the lane's run: rows complete inside the lane go to
-// y, the heads combine across lanes, the tile's open row and carry go to the
-// calibrator arrays.
-template <typename I, typename V, int K>
-__device__ __forceinline__ void tile_finish(const I* __restrict__ rp, int64_t n, int64_t nnz, int64_t t, int lane,
-                                            uint32_t flags, int64_t tr, const V (&p)[K], V* __restrict__ y, V alpha,
-                                            V beta, bool bz, V* __restrict__ carry_in, V* __restrict__ open_sum,
-                                            int64_t* __restrict__ open_row) {
-  const unsigned lt = (1u << lane) - 1u;  // lanes below this one
-  const int64_t el = t * (32 * K) + (int64_t)lane * K;
-  // ---- row of the lane's first entry
-  int64_t row;
-  if (tr >= 0) {
-    const int cnt = __popc(flags);
-    int excl = 0;
-#pragma unroll
-    for (int bit = 0; bit < 4; ++bit) excl += __popc(__ballot_sync(0xffffffffu, (cnt >> bit) & 1) & lt) << bit;
-    const int first0 = (int)(__ballot_sync(0xffffffffu, flags & 1u) & 1u);
-    row = tr + excl + (int)(flags & 1u) - first0;
-  } else {
-    row = row_holding(rp, n, el < nnz ? el : nnz - 1);
-  }
-  // ---- in-lane segments
-  V head = V(0), acc = V(0);
-  bool in_head = (flags & 1u) == 0;
-#pragma unroll
-  for (int b = 0; b < K; ++b) {
-    if (b > 0 && ((flags >> b) & 1u)) {
-      if (in_head) {
-        head = acc;
-        in_head = false;
-      } else {
-        axpby_store(y + row, acc, alpha, beta, bz);
-      }
-      acc = V(0);
-      ++row;
-      if (tr < 0)
-        while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
-    }
-    acc += p[b];
-  }
-  V tail = V(0);
-  if (in_head) head = acc; else tail = acc;
-  // ---- cross-lane: segmented inclusive scan of the heads, a segment
-  // starting right after every flagged lane
-  const bool has_flag = flags != 0;
-  const unsigned fmask = __ballot_sync(0xffffffffu, has_flag);
-  const unsigned starts = (fmask << 1) | 1u;  // lane l starts a segment if lane l-1 is flagged (or l == 0)
-  V S = head;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const V su = __shfl_up_sync(0xffffffffu, S, o);
-    // add lane (l - o)'s sum unless a segment starts in lanes l-o+1 .. l
-    const unsigned span = (lane >= o) ? ((2u << lane) - 1u) & ~((2u << (lane - o)) - 1u) : 0u;
-    if (lane >= o && !(starts & span)) S += su;
-  }
-  const unsigned later = fmask & ~((2u << lane) - 1u);  // flagged lanes after this one
-  const int m = later ? __ffs(later) - 1 : 31;
-  const V Sm = __shfl_sync(0xffffffffu, S, m);
-  const int m0 = fmask ? __ffs(fmask) - 1 : 31;
-  const V cin = __shfl_sync(0xffffffffu, S, m0);
-  if (has_flag) {
-    if (later) {
-      axpby_store(y + row, tail + Sm, alpha, beta, bz);
-    } else {  // the tile's last row: may continue into the next tile
-      open_sum[t] = tail + (lane < 31 ? Sm : V(0));
-      open_row[t] = row;
-    }
-  }
-  if (lane == 0) {
-    carry_in[t] = cin;
-    if (!fmask) open_row[t] = -1;
-  }
-}
-
 // One warp per tile, grid-stride over tiles.  kPipe: the next tile's columns,
 // values and flags are loaded before this tile's gathers are used, so the
 // streaming loads of one tile overlap the gathers of the previous one.
