@@ -294,6 +294,47 @@ __device__ __forceinline__ void csr_segment_spmm(const CsrSeg& d, int64_t j, con
 }
 
 // Padded rows: stored rows [i0, i0+32) with one warp (see formats.cu).
+// Sum of one lane's row in a column-major chunk: slots [0, len) at base +
+// k * stride.  Eight slots at a time: their columns and values are loaded,
+// then their eight x gathers issued, before any is added, so each lane keeps
+// eight gathers in flight.  Even slots go to one sum and odd slots to the
+// other, in slot order (padding columns, -1, are skipped).
+template <typename I, typename V>
+__device__ __forceinline__ V colmajor_row_sum(const I* __restrict__ col, const V* __restrict__ val,
+                                              const V* __restrict__ x, int64_t base, int len, int64_t stride) {
+  V s0 = V(0), s1 = V(0);
+  int k = 0;
+  for (; k + 8 <= len; k += 8) {
+    I c[8];
+    V a[8], p[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t e = base + (int64_t)(k + u) * stride;
+      c[u] = ld_stream(col + e);
+      a[u] = ld_stream(val + e);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) p[u] = c[u] >= 0 ? a[u] * ld_gather(x + c[u]) : V(0);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (c[u] >= 0) {
+        if (u & 1) s1 += p[u]; else s0 += p[u];
+      }
+  }
+  for (; k + 1 < len; k += 2) {
+    const int64_t a = base + (int64_t)k * stride, b = a + stride;
+    const I ca = ld_stream(col + a), cb = ld_stream(col + b);
+    if (ca >= 0) s0 += ld_stream(val + a) * ld_gather(x + ca);
+    if (cb >= 0) s1 += ld_stream(val + b) * ld_gather(x + cb);
+  }
+  if (k < len) {
+    const int64_t a = base + (int64_t)k * stride;
+    const I ca = ld_stream(col + a);
+    if (ca >= 0) s0 += ld_stream(val + a) * ld_gather(x + ca);
+  }
+  return s0 + s1;
+}
+
 template <typename I, typename V, bool kColMajor>
 __device__ __forceinline__ void padded_rows32(int64_t i0, const I* __restrict__ col, const V* __restrict__ val,
                                               const I* __restrict__ chunk_len,
@@ -311,20 +352,8 @@ __device__ __forceinline__ void padded_rows32(int64_t i0, const I* __restrict__ 
     base = chunk_off[c] + (kColMajor ? (i - c * C) : (i - c * C) * (int64_t)chunk_len[c]);
   }
   if (kColMajor) {
-    V s0 = V(0), s1 = V(0);
-    int k = 0;
-    for (; k + 1 < len; k += 2) {
-      const int64_t a = base + (int64_t)k * C, b = a + C;
-      const I ca = ld_stream(col + a), cb = ld_stream(col + b);
-      if (ca >= 0) s0 += ld_stream(val + a) * ld_gather(x + ca);
-      if (cb >= 0) s1 += ld_stream(val + b) * ld_gather(x + cb);
-    }
-    if (k < len) {
-      const int64_t a = base + (int64_t)k * C;
-      const I ca = ld_stream(col + a);
-      if (ca >= 0) s0 += ld_stream(val + a) * ld_gather(x + ca);
-    }
-    if (i < n && len >= 0) axpby_store(y + (reorder ? (int64_t)reorder[i] : i), s0 + s1, alpha, beta, bz);
+    const V s = colmajor_row_sum<I, V>(col, val, x, base, len, C);
+    if (i < n && len >= 0) axpby_store(y + (reorder ? (int64_t)reorder[i] : i), s, alpha, beta, bz);
   } else {
     const unsigned ml = __reduce_max_sync(0xffffffffu, (unsigned)(len > 0 ? len : 0));
     int t = 1;
@@ -378,23 +407,7 @@ __device__ __forceinline__ void padded_window32(int64_t base, int len, int k0, c
   const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned)len);
   const unsigned longest = __reduce_max_sync(0xffffffffu, (unsigned)len);
   if (32u * longest <= total + total / 4 + 32u * 8u) {
-    V s0 = V(0), s1 = V(0);
-    const int64_t rb = base + lane;
-    int k = 0;
-    for (; k + 1 < len; k += 2) {
-      const int64_t a = rb + 32 * (int64_t)k, b = a + 32;
-      const I ca = ld_stream(col + a), cb = ld_stream(col + b);
-      const V va = ld_stream(val + a), vb = ld_stream(val + b);
-      if (ca >= 0) s0 += va * ld_gather(x + ca);
-      if (cb >= 0) s1 += vb * ld_gather(x + cb);
-    }
-    if (k < len) {
-      const int64_t a = rb + 32 * (int64_t)k;
-      const I ca = ld_stream(col + a);
-      const V va = ld_stream(val + a);
-      if (ca >= 0) s0 += va * ld_gather(x + ca);
-    }
-    emit(lane, s0 + s1);
+    emit(lane, colmajor_row_sum<I, V>(col, val, x, base + lane, len, 32));
     return;
   }
   // rank rows by length, descending (ties: lower row first)
