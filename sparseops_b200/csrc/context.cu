@@ -54,10 +54,82 @@ spops_status_t DevBuf::alloc(size_t n) {
 }
 
 void DevBuf::release() {
-  if (own && p) cudaFree(p);
+  if (own && p) {
+    if (home) home->cache_block(p, bytes);
+    else cudaFree(p);
+  }
   p = nullptr;
   bytes = 0;
   own = false;
+  home = nullptr;
+}
+
+constexpr size_t kCacheMin = size_t(8) << 20;   // blocks below this go back to the driver
+constexpr size_t kCacheMax = size_t(24) << 30;  // bytes the cache may hold
+
+spops_status_t DevBuf::alloc_cached(Context* ctx, size_t n) {
+  release();
+  if (n == 0) n = 16;
+  if (n >= kCacheMin) {
+    void* q = nullptr;
+    size_t b = 0;
+    if (ctx->take_block(n, &q, &b)) {
+      p = q;
+      bytes = b;
+      own = true;
+      home = ctx;
+      return SPOPS_OK;
+    }
+  }
+  SPOPS_TRY(alloc(n));
+  if (n >= kCacheMin) home = ctx;
+  return SPOPS_OK;
+}
+
+void Context::cache_block(void* q, size_t b) {
+  if (b < kCacheMin || block_cache_bytes + b > kCacheMax) {
+    cudaFree(q);
+    return;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(e, stream) != cudaSuccess) {  // cannot order a reuse: give it back
+    if (e) cudaEventDestroy(e);
+    cudaGetLastError();
+    cudaFree(q);
+    return;
+  }
+  block_cache.push_back(CachedBlock{q, b, e});
+  block_cache_bytes += b;
+}
+
+bool Context::take_block(size_t n, void** q, size_t* b) {
+  // the smallest block of at least n bytes and at most n + n / 8 + 2 MB
+  const size_t hi = n + n / 8 + (size_t(2) << 20);
+  int best = -1;
+  for (int i = 0; i < (int)block_cache.size(); ++i) {
+    const size_t s = block_cache[i].bytes;
+    if (s >= n && s <= hi && (best < 0 || s < block_cache[best].bytes)) best = i;
+  }
+  if (best < 0) return false;
+  const CachedBlock c = block_cache[best];
+  block_cache.erase(block_cache.begin() + best);
+  block_cache_bytes -= c.bytes;
+  cudaStreamWaitEvent(stream, c.done, 0);  // work queued before the release may still use it
+  cudaEventDestroy(c.done);
+  *q = c.p;
+  *b = c.bytes;
+  return true;
+}
+
+void Context::drop_block_cache() {
+  for (const CachedBlock& c : block_cache) {
+    cudaEventSynchronize(c.done);
+    cudaEventDestroy(c.done);
+    cudaFree(c.p);
+  }
+  block_cache.clear();
+  block_cache_bytes = 0;
 }
 
 spops_status_t Context::pool_alloc(void** out, size_t bytes) {
@@ -206,6 +278,7 @@ spops_status_t spops_destroy(spops_context_t c) {
     cudaEventDestroy(c->arena_done);
   }
   c->arena.release();
+  c->drop_block_cache();
   if (c->pool) {
     cudaStreamSynchronize(c->stream);
     cudaMemPoolDestroy(c->pool);

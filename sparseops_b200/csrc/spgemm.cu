@@ -1647,9 +1647,9 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
   C->rows = n;
   C->cols = B->cols;
   C->nnz = cnnz;
-  spops_status_t s = C->row.alloc((nn + 1) * sizeof(I));
-  if (s == SPOPS_OK) s = C->col.alloc((size_t)std::max<int64_t>(cnnz, 1) * sizeof(I));
-  if (s == SPOPS_OK) s = C->val.alloc((size_t)std::max<int64_t>(cnnz, 1) * sizeof(V));
+  spops_status_t s = C->row.alloc_cached(ctx, (nn + 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->col.alloc_cached(ctx, (size_t)std::max<int64_t>(cnnz, 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->val.alloc_cached(ctx, (size_t)std::max<int64_t>(cnnz, 1) * sizeof(V));
   if (s != SPOPS_OK) {
     C->release_all();
     delete static_cast<spops_matrix_s*>(C);
@@ -1857,9 +1857,9 @@ spops_status_t vl_to_csr_t(Context* ctx, Matrix* M, Matrix** out) {
   C->rows = n;
   C->cols = M->cols;
   C->nnz = cnnz;
-  spops_status_t s = C->row.alloc((nn + 1) * sizeof(I));
-  if (s == SPOPS_OK) s = C->col.alloc((size_t)std::max<int64_t>(cnnz, 1) * sizeof(I));
-  if (s == SPOPS_OK) s = C->val.alloc((size_t)std::max<int64_t>(cnnz, 1) * sizeof(V));
+  spops_status_t s = C->row.alloc_cached(ctx, (nn + 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->col.alloc_cached(ctx, (size_t)std::max<int64_t>(cnnz, 1) * sizeof(I));
+  if (s == SPOPS_OK) s = C->val.alloc_cached(ctx, (size_t)std::max<int64_t>(cnnz, 1) * sizeof(V));
   if (s == SPOPS_OK) {
     cast_kernel<int64_t, I><<<grid_for(n + 1), 256, 0, st>>>(crp.as<int64_t>(), n + 1, C->row.as<I>());
     if (n > 0 && cnnz > 0)

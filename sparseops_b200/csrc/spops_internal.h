@@ -39,11 +39,16 @@ spops_status_t cuda_fail(cudaError_t e, const char* what, const char* file, int 
 
 // ---------------------------------------------------------------- buffers
 // Device allocation owned by a handle (or borrowed when own == false).
+struct Context;
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   bool own = false;
+  Context* home = nullptr;  // set by alloc_cached: released into home's block cache
   spops_status_t alloc(size_t n);
+  // n bytes, reusing a block of about that size that an earlier result of
+  // this context released (large results only; see Context::block_cache)
+  spops_status_t alloc_cached(Context* ctx, size_t n);
   void release();
   void borrow(const void* q, size_t n) { release(); p = const_cast<void*>(q); bytes = n; own = false; }
   template <typename T> T* as() const { return static_cast<T*>(p); }
@@ -102,6 +107,21 @@ struct Context {
   // does not fit goes to the pool; the arena is then regrown, between calls,
   // to the largest total the scopes asked for.
   DevBuf arena;
+  // large blocks released by results allocated with DevBuf::alloc_cached (a
+  // SpGEMM's C, for instance), kept for the next result of about the same
+  // size: cudaMalloc / cudaFree of a GB-sized array cost milliseconds, and
+  // their time varies.  Each block carries an event recorded on the context
+  // stream when it was released; a reuse waits for it.
+  struct CachedBlock {
+    void* p;
+    size_t bytes;
+    cudaEvent_t done;
+  };
+  std::vector<CachedBlock> block_cache;
+  size_t block_cache_bytes = 0;
+  void cache_block(void* p, size_t bytes);
+  bool take_block(size_t n, void** p, size_t* bytes);
+  void drop_block_cache();
   size_t arena_top = 0;       // bytes handed out
   size_t arena_over = 0;      // bytes of live pool allocations made in a scope
   size_t arena_need = 0;      // largest arena_top + arena_over seen
