@@ -420,6 +420,18 @@ def bench_formats(A, ctx, xd, yref, n, nnz, nbytes, peak, dev):
             finally:
                 c.set_option("sell_tails", 0)
         return run
+    def chunk_order(conv):  # the same conversion with the windows listed in chunk order
+        def run():
+            from sparseops_b200 import default_context
+            c = default_context()
+            c.set_option("sell_order", 0)
+            try:
+                return conv()
+            finally:
+                c.set_option("sell_order", 1)
+        return run
+    cands.insert(2, ("sell_c_sigma C=32 sigma=512 col-major, windows in chunk order",
+                     chunk_order(lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.ColMajor)), F.SpOps_sell_c_sigma))
     cands.insert(2, ("sell_c_sigma C=32 sigma=512 col-major, tails",
                      tails(lambda: F.csr_to_sell_c_sigma(A, None, 512, 32, 1, F.ColMajor)), F.SpOps_sell_c_sigma))
     cands.insert(5, ("sell_c_R C=32 col-major, tails",
@@ -552,6 +564,12 @@ def bench_batched(ctx, dev, ks=(1, 8, 32), count=256, seed=2024, peak=None, cpu_
         items, choice, kt = B.info()
         r["tuned"] = {"work_items": int(items), "rhs_tile": int(kt),
                       "formats": {str(c): int(np.sum(np.asarray(choice) == c)) for c in sorted(set(choice))}}
+        if k == 1:  # every matrix in CSR (no tuning): all tile items
+            Bu = Batch(mats, k=k, ctx=ctx)
+            Bu.set_vectors(X, Yb)
+            Bu.capture(1.0, 0.0)
+            r["untuned_csr_ms"] = round(_ev_ms(Bu.run, 20), 3)
+            del Bu
         if k == 1:  # the same batch with each CSR segment's banded x window staged in shared memory
             try:
                 ctx.set_option("batch_band", 1)
@@ -973,7 +991,7 @@ def run_section(args):
         peak, _ = peaks()
         cpu = not args.no_cpu_baseline
         if args.section == "batched":
-            res = bench_batched(ctx, dev, peak=peak, cpu_ref=cpu)
+            res = bench_batched(ctx, dev, ks=tuple(int(k) for k in args.batched_ks.split(",")), peak=peak, cpu_ref=cpu)
         elif args.section == "fwd_bwd":
             res = bench_fwd_bwd(ctx, dev, peak=peak, cpu_ref=cpu)
         elif args.section == "mtx":
@@ -1194,6 +1212,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-format, batched, fwd+bwd and SpGEMM sections")
     ap.add_argument("--csr-variant", type=int, default=0, help="CSR kernel shape (spops_set_option)")
+    ap.add_argument("--batched-ks", default="1,8,32",
+                    help="right-hand-side counts of the batched section (a subset for profiling captures)")
     ap.add_argument("--spgemm-rows", type=int, default=524288,
                     help="rows of the SpGEMM section's matrices (a smaller case for profiling captures)")
     ap.add_argument("--rows", type=int, default=N_ROWS,

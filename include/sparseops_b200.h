@@ -127,7 +127,12 @@ spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
  *   "sell_tails" 0 / 1: SELL with C = 32, column-major: each 32-row chunk's
  *   slots beyond its fourth-longest row (held by at most three rows) are
  *   read in place (0, the default), or also kept row-contiguous and read from
- *   there (1).  Read when the matrix is converted or uploaded. */
+ *   there (1).  Read when the matrix is converted or uploaded.
+ *   "sell_order" 1 / 0: SELL with C = 32, column-major: the chunks' step
+ *   windows are listed longest chunk first, so that warps running at the
+ *   same time hold rows of like length (1, the default), or in chunk order
+ *   (0).  The per-row results do not depend on it.  Read when the matrix is
+ *   converted or uploaded. */
 spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);

@@ -314,6 +314,11 @@ spops_status_t spops_set_option(spops_context_t c, const char* key, int64_t valu
     c->csr_variant = (int)value;
     return SPOPS_OK;
   }
+  if (!strcmp(key, "sell_order")) {
+    if (value < 0 || value > 1) return fail(SPOPS_ERR_INVALID, "sell_order must be 0 or 1");
+    c->sell_order = (int)value;
+    return SPOPS_OK;
+  }
   if (!strcmp(key, "sell_tails")) {
     if (value < 0 || value > 1) return fail(SPOPS_ERR_INVALID, "sell_tails must be 0 or 1");
     c->sell_tails = (int)value;

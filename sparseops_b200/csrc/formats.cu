@@ -262,7 +262,7 @@ constexpr int kTailWin = 1024;
 // entries.
 __global__ void pad_head_kernel(const int* __restrict__ row_len, int64_t n, int64_t nchunks, bool tails,
                                 int* __restrict__ head, int64_t* __restrict__ ntr, int64_t* __restrict__ nte,
-                                int64_t* __restrict__ nw) {
+                                int64_t* __restrict__ nw, uint32_t* __restrict__ order_key) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t c = t >> 5;
   const int lane = threadIdx.x & 31;
@@ -287,10 +287,32 @@ __global__ void pad_head_kernel(const int* __restrict__ row_len, int64_t n, int6
   const unsigned twin = __reduce_add_sync(0xffffffffu, (unsigned)((tl + kTailWin - 1) / kTailWin));
   if (lane == 0) {
     head[c] = h;
+    order_key[c] = ~key;  // key is the longest row here: longest chunks first
     ntr[c] = rows;
     nte[c] = ents;
     nw[c] = (h > kPadWindow ? ((int64_t)h + kPadWindow - 1) / kPadWindow : 1) + twin;
   }
+}
+
+__global__ void iota_i32_kernel(int32_t* __restrict__ a, int64_t m) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) a[i] = (int32_t)i;
+}
+
+// Window offsets in the order the chunks are taken (order[i]: the i-th
+// chunk): the counts gathered into that order, scanned, and scattered back.
+__global__ void pad_gather_nw_kernel(const int32_t* __restrict__ order, const int64_t* __restrict__ nw, int64_t nch,
+                                     int64_t* __restrict__ nw_sorted) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < nch) nw_sorted[i] = nw[order[i]];
+  if (i == nch) nw_sorted[i] = 0;
+}
+
+__global__ void pad_scatter_woff_kernel(const int32_t* __restrict__ order, const int64_t* __restrict__ woff_sorted,
+                                        int64_t nch, int64_t* __restrict__ woff) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < nch) woff[order[i]] = woff_sorted[i];
+  if (i == nch) woff[nch] = woff_sorted[nch];
 }
 
 // The chunk's window list and tail records (offsets from exclusive scans of
@@ -830,15 +852,35 @@ spops_status_t padded_finish_t(Context* ctx, Matrix* M) {
     int64_t* woff = teoff + (nch + 1);
     SPOPS_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, st));
     SPOPS_TRY(P.head.alloc((size_t)nch * 4));
+    PoolBuf okey(ctx), okey_s(ctx), ord_in(ctx), ord(ctx), nws(ctx), woffs(ctx);
+    SPOPS_TRY(okey.alloc((size_t)nch * 4));
     pad_head_kernel<<<grid_for(nch * 32), 256, 0, st>>>(P.row_len.as<int>(), n, nch, ctx->sell_tails != 0,
-                                                         P.head.as<int>(), ntr, nte, nwc);
+                                                         P.head.as<int>(), ntr, nte, nwc, okey.as<uint32_t>());
     SPOPS_LAUNCH_CHECK();
-    size_t cs = 0;
+    size_t cs = 0, cso = 0;
     SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cs, ntr, troff, nch + 1, st));
-    SPOPS_TRY(tmp.alloc(cs + 256));
+    if (ctx->sell_order)
+      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cso, okey.as<uint32_t>(), okey.as<uint32_t>(),
+                                                 ord.as<int32_t>(), ord.as<int32_t>(), nch, 0, 32, st));
+    SPOPS_TRY(tmp.alloc(std::max(cs, cso) + 256));
     SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, ntr, troff, nch + 1, st));
     SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, nte, teoff, nch + 1, st));
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, nwc, woff, nch + 1, st));
+    if (ctx->sell_order) {  // windows of chunks of like length side by side in the list: longest first
+      SPOPS_TRY(okey_s.alloc((size_t)nch * 4));
+      SPOPS_TRY(ord_in.alloc((size_t)nch * 4));
+      SPOPS_TRY(ord.alloc((size_t)nch * 4));
+      SPOPS_TRY(nws.alloc((size_t)(nch + 1) * 8));
+      SPOPS_TRY(woffs.alloc((size_t)(nch + 1) * 8));
+      iota_i32_kernel<<<grid_for(nch), 256, 0, st>>>(ord_in.as<int32_t>(), nch);
+      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, cso, okey.as<uint32_t>(), okey_s.as<uint32_t>(),
+                                                 ord_in.as<int32_t>(), ord.as<int32_t>(), nch, 0, 32, st));
+      pad_gather_nw_kernel<<<grid_for(nch + 1), 256, 0, st>>>(ord.as<int32_t>(), nwc, nch, nws.as<int64_t>());
+      SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, nws.as<int64_t>(), woffs.as<int64_t>(), nch + 1, st));
+      pad_scatter_woff_kernel<<<grid_for(nch + 1), 256, 0, st>>>(ord.as<int32_t>(), woffs.as<int64_t>(), nch, woff);
+      SPOPS_LAUNCH_CHECK();
+    } else {
+      SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cs, nwc, woff, nch + 1, st));
+    }
     int64_t h[3];
     SPOPS_TRY(download(ctx, &h[0], troff + nch, 1));
     SPOPS_TRY(download(ctx, &h[1], teoff + nch, 1));

@@ -153,6 +153,8 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   const int r = k / bands;
   cudaStream_t st = ctx->stream;
   const size_t nn = (size_t)n;
+  Trace tr("lsh");
+  ArenaScope scope(ctx);  // this call's temporaries come from the arena
   size_t cub_sort = 0, cub_scan = 0, cub_rle = 0;
   {
     uint64_t* kk = nullptr;
@@ -186,8 +188,9 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   int64_t* nruns = reinterpret_cast<int64_t*>(take(8));
   void* cub_tmp = take(cub_max);
 
+  tr.mark(st, "setup");
   // pairs of every band, appended
-  DevBuf all;
+  PoolBuf all(ctx);
   int64_t total = 0, cap = 0;
   for (int band = 0; band < bands; ++band) {
     band_hash_kernel<<<grid_for(n), 256, 0, st>>>(sig, n, k, band, r, key_in, row_in);
@@ -209,55 +212,49 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
     const int64_t np = h[0] + h[1];
     if (np == 0) continue;
     if (total + np > cap) {  // grow the pair buffer
-      DevBuf bigger;
+      PoolBuf bigger(ctx);
       const int64_t ncap = std::max<int64_t>(2 * cap, total + np);
       SPOPS_TRY(bigger.alloc((size_t)ncap * 8));
       if (total) SPOPS_CUDA(cudaMemcpyAsync(bigger.p, all.p, (size_t)total * 8, cudaMemcpyDeviceToDevice, st));
-      SPOPS_CUDA(cudaStreamSynchronize(st));
-      all.release();
-      all = bigger;
-      bigger.p = nullptr;
-      bigger.own = false;
+      all.swap(bigger);
       cap = ncap;
     }
     pair_emit_kernel<<<grid_for(n), 256, 0, st>>>(row_out, n, cnt, off, all.as<uint64_t>() + total);
     SPOPS_LAUNCH_CHECK();
     total += np;
   }
-  if (total == 0) {
-    all.release();
-    return SPOPS_OK;
-  }
-  // sort + unique all pairs
+  tr.mark(st, "bands");
+  if (total == 0) return SPOPS_OK;
+  // sort + unique all pairs (key i << 32 | j: only the bits of i in use above 32)
+  int kend = 33;
+  while (kend < 64 && (int64_t(1) << (kend - 32)) < n) ++kend;
   size_t cub2 = 0, cub3 = 0;
   int64_t* nsel = nullptr;
   {
     uint64_t* kk = nullptr;
-    SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, cub2, kk, kk, total, 0, 64, st));
+    SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, cub2, kk, kk, total, 0, kend, st));
     SPOPS_CUDA(cub::DeviceSelect::Unique(nullptr, cub3, kk, kk, nsel, total, st));
   }
-  DevBuf sorted, uniq, tmp;
+  PoolBuf sorted(ctx), uniq(ctx), tmp(ctx);
   SPOPS_TRY(sorted.alloc((size_t)total * 8));
   SPOPS_TRY(uniq.alloc((size_t)total * 8));
   const size_t nsel_off = (std::max(cub2, cub3) + 255) & ~(size_t)255;  // 8-byte aligned count slot
   SPOPS_TRY(tmp.alloc(nsel_off + 256));
   nsel = reinterpret_cast<int64_t*>(tmp.as<char>() + nsel_off);
-  SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, cub2, all.as<uint64_t>(), sorted.as<uint64_t>(), total, 0, 64, st));
+  SPOPS_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, cub2, all.as<uint64_t>(), sorted.as<uint64_t>(), total, 0, kend, st));
   SPOPS_CUDA(cub::DeviceSelect::Unique(tmp.p, cub3, sorted.as<uint64_t>(), uniq.as<uint64_t>(), nsel, total, st));
   int64_t nu = 0;
   SPOPS_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, st));
   SPOPS_CUDA(cudaStreamSynchronize(st));
-  all.release();
-  sorted.release();
-  tmp.release();
-  SPOPS_TRY(out->pi.alloc((size_t)nu * 8));
-  SPOPS_TRY(out->pj.alloc((size_t)nu * 8));
-  SPOPS_TRY(out->score.alloc((size_t)nu * 8));
+  tr.mark(st, "sort + unique");
+  SPOPS_TRY(out->pi.alloc_cached(ctx, (size_t)nu * 8));
+  SPOPS_TRY(out->pj.alloc_cached(ctx, (size_t)nu * 8));
+  SPOPS_TRY(out->score.alloc_cached(ctx, (size_t)nu * 8));
   score_kernel<<<grid_for(nu * 32), 256, 0, st>>>(sig, k, uniq.as<uint64_t>(), nu, out->pi.as<int64_t>(),
                                                   out->pj.as<int64_t>(), out->score.as<double>());
   SPOPS_LAUNCH_CHECK();
   SPOPS_CUDA(cudaStreamSynchronize(st));
-  uniq.release();
+  tr.mark(st, "scores");
   out->count = nu;
   return SPOPS_OK;
 }

@@ -75,6 +75,10 @@ struct Context {
   // measured faster on the power-law matrix); read when the matrix is
   // converted or uploaded
   int sell_tails = 0;
+  // SELL (C = 32, column-major): the chunks' windows are listed longest chunk
+  // first, so that warps running together hold rows of like length (1), or
+  // in chunk order (0); read when the matrix is converted or uploaded
+  int sell_order = 1;
   // pinned staging for host x / y in spops_spmv_host
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

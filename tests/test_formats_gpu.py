@@ -196,21 +196,24 @@ def test_sell_long_rows_and_empty_rows(cuda, orc):
         _check(orc, rp, ci, v, x, _spmv(SpOps_sell_c_sigma, S, x))
 
 
-@pytest.mark.parametrize("tails", [0, 1])
+@pytest.mark.parametrize("tails,order", [(0, 1), (1, 1), (0, 0)])
 @pytest.mark.parametrize("sigma", [32, 512, 1 << 20])
-def test_sell_col_major_windows_and_packing(cuda, orc, sigma, tails):
+def test_sell_col_major_windows_and_packing(cuda, orc, sigma, tails, order):
     """C = 32 column-major: chunks cut into step windows (rows longer than 128
     slots, one with more than 2048), rows of very different lengths in one
     chunk (the lane re-dealing path), empty rows, rows past the last full
     chunk, unsorted (sigma = C) and sorted slices; FP64 and FP32 values; the
     slots past a chunk's fourth-longest row read from row-contiguous tails
-    (tails = 1, tail windows of up to 1024 entries) or in place (the default)."""
-    from sparseops_b200 import SpOps_sell_c_sigma, csr_to_sell_c_sigma, default_context
+    (tails = 1, tail windows of up to 1024 entries) or in place (the default);
+    the windows listed longest chunk first (the default) or in chunk order."""
+    from sparseops_b200 import default_context
     default_context().set_option("sell_tails", tails)
+    default_context().set_option("sell_order", order)
     try:
         _sell_windows_case(orc, sigma)
     finally:
         default_context().set_option("sell_tails", 0)
+        default_context().set_option("sell_order", 1)
 
 
 def _sell_windows_case(orc, sigma):
