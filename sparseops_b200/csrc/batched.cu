@@ -8,6 +8,8 @@
 //   kind 0  CSR segment of the matrix's CSR plan (csr_segment_spmv / _spmm)
 //   kind 1  32 stored rows of the matrix's padded (SELL) form (padded_rows32)
 //   kind 2  one piece of a long padded row (padded_piece)
+//   kind 3  four tiles of the matrix's CSR tile plan (separate tile-item
+//           launch and a batch-wide calibration; k = 1, 8, 16, 32)
 // A persistent grid (SMs x resident blocks) of warps walks the item list.
 // Per-matrix pointers live in a device table; the launch itself (on the
 // batch's own stream, ordered against the caller's stream with events) can
@@ -16,8 +18,12 @@
 // Autotuner (spops_batch_tune): per matrix, times the candidate forms with
 // CUDA events on the device -- CSR (segments of kCsrCap entries), and
 // SELL-C-sigma with C = 32 and sigma in {256, 4096}, row-major and
-// column-major chunks -- and keeps the fastest for the batched launch.  For
-// k > 1 the CSR form is used and the tuner picks the RHS tile (8 or 32 lanes).
+// column-major chunks -- and keeps the fastest for the batched launch, then
+// times the whole batch with those choices and with every matrix in CSR and
+// keeps the faster of the two.  With one right-hand side a CSR matrix runs
+// as SpMV tile items (the single-matrix tile kernel's body) when its arrays
+// allow the vector loads, otherwise as segments.  For k > 1 the CSR form is
+// used and the tuner picks the RHS tile (8 or 32 lanes).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -783,6 +789,36 @@ spops_status_t batch_tune(Batch* B, int flags) {
       B->choice[m] = 1 + c;
       best = ms;
     }
+  }
+  if (B->k == 1 && try_padded) {
+    // Each matrix timed alone says little about how the forms run together
+    // in one launch (a small matrix's time is mostly launch latency): keep
+    // the per-matrix choices only if the whole batch runs faster with them
+    // than with every matrix in CSR.
+    float t_mixed = 0, t_csr = 0;
+    B->dirty = true;
+    SPOPS_TRY(prepare(B));
+    SPOPS_TRY(time_ms(st, [&] { return launch_any(B, 1.0, 0.0, st); }, 3, &t_mixed));
+    std::vector<Matrix*> kept = B->form;
+    const std::vector<int> kept_choice = B->choice;
+    for (int64_t m = 0; m < B->count; ++m) {
+      B->form[m] = nullptr;
+      B->choice[m] = 0;
+    }
+    B->dirty = true;
+    spops_status_t s = prepare(B);
+    if (s == SPOPS_OK) s = time_ms(st, [&] { return launch_any(B, 1.0, 0.0, st); }, 3, &t_csr);
+    if (s != SPOPS_OK || t_csr > t_mixed) {  // the per-matrix forms win (or CSR could not be timed)
+      B->form = kept;
+      B->choice = kept_choice;
+    } else {
+      for (Matrix* F : kept)
+        if (F) {
+          F->release_all();
+          delete static_cast<spops_matrix_s*>(F);
+        }
+    }
+    SPOPS_TRY(s);
   }
   if (B->k > 1) {  // RHS tile: time both on the whole batch
     float t8 = 0, t32 = 0;

@@ -70,16 +70,24 @@ constexpr size_t kCacheMax = size_t(24) << 30;  // bytes the cache may hold
 spops_status_t DevBuf::alloc_cached(Context* ctx, size_t n) {
   release();
   if (n == 0) n = 16;
+  static const bool trace = [] {
+    const char* e = std::getenv("SPOPS_TRACE");
+    return e && (e[0] == '1' || e[0] == '2');
+  }();
   if (n >= kCacheMin) {
     void* q = nullptr;
     size_t b = 0;
     if (ctx->take_block(n, &q, &b)) {
+      if (trace) std::fprintf(stderr, "[cache] %zu bytes from a cached block of %zu\n", n, b);
       p = q;
       bytes = b;
       own = true;
       home = ctx;
       return SPOPS_OK;
     }
+    if (trace)
+      std::fprintf(stderr, "[cache] %zu bytes: no cached block (%zu blocks, %zu bytes held)\n", n,
+                   ctx->block_cache.size(), ctx->block_cache_bytes);
   }
   SPOPS_TRY(alloc(n));
   if (n >= kCacheMin) home = ctx;
