@@ -123,12 +123,13 @@ __global__ void hc_init_tasks_kernel(const int64_t* __restrict__ pi, const int64
 }
 
 // 1. roots and reservations; tasks that can have no effect retire here
-__global__ void hc_reserve_kernel(const int32_t* __restrict__ live, int64_t nlive, Tasks T,
+__global__ void hc_reserve_kernel(const int32_t* __restrict__ live, const unsigned long long* __restrict__ nlive_d,
+                                  Tasks T,
                                   const int32_t* __restrict__ parent, const unsigned char* __restrict__ open,
                                   int32_t* __restrict__ res, int32_t* __restrict__ ri_out, int32_t* __restrict__ rj_out,
                                   int* __restrict__ err) {
   const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nlive) return;
+  if (q >= (int64_t)*nlive_d) return;
   const int32_t c = live[q];
   const int32_t ri = hc_find(parent, T.i[c], err), rj = hc_find(parent, T.j[c], err);
   if (ri == rj || !open[ri] || !open[rj]) {  // no effect, now or later
@@ -197,7 +198,8 @@ __device__ __forceinline__ bool hc_seen_insert(unsigned long long* __restrict__ 
 
 // 2. tasks holding both roots apply the sequential step
 template <typename I>
-__global__ void hc_commit_kernel(const int32_t* __restrict__ live, int64_t nlive, Tasks T,
+__global__ void hc_commit_kernel(const int32_t* __restrict__ live, const unsigned long long* __restrict__ nlive_d,
+                                 Tasks T,
                                  const int32_t* __restrict__ ri_in, const int32_t* __restrict__ rj_in,
                                  const int32_t* __restrict__ res, int32_t* __restrict__ parent,
                                  int32_t* __restrict__ size, unsigned char* __restrict__ open, int64_t cluster_size,
@@ -207,7 +209,7 @@ __global__ void hc_commit_kernel(const int32_t* __restrict__ live, int64_t nlive
                                  int32_t* __restrict__ next_live, unsigned long long* __restrict__ nnext,
                                  int* __restrict__ err) {
   const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nlive) return;
+  if (q >= (int64_t)*nlive_d) return;
   const int32_t ri = ri_in[q], rj = rj_in[q];
   if (ri < 0) return;  // retired in the reserve pass
   const int32_t c = live[q];
@@ -248,10 +250,10 @@ __global__ void hc_seen_rebuild_kernel(Tasks T, int64_t np, int64_t ntask, unsig
 }
 
 // 3. clear the round's reservations
-__global__ void hc_release_kernel(const int32_t* __restrict__ ri_in, const int32_t* __restrict__ rj_in, int64_t nlive,
-                                  int32_t* __restrict__ res) {
+__global__ void hc_release_kernel(const int32_t* __restrict__ ri_in, const int32_t* __restrict__ rj_in,
+                                  const unsigned long long* __restrict__ nlive_d, int32_t* __restrict__ res) {
   const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nlive) return;
+  if (q >= (int64_t)*nlive_d) return;
   const int32_t ri = ri_in[q], rj = rj_in[q];
   if (ri >= 0) res[ri] = -1;
   if (rj >= 0) res[rj] = -1;
@@ -302,7 +304,8 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
   SPOPS_CUDA(cudaMemsetAsync(flags.p, 0, 64, st));
   int* err = flags.as<int>();
   unsigned long long* ntasks = reinterpret_cast<unsigned long long*>(flags.as<char>() + 8);
-  unsigned long long* nnext = reinterpret_cast<unsigned long long*>(flags.as<char>() + 16);
+  // live counts: cnt[cur] of the round about to run, cnt[cur ^ 1] of the next
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(flags.as<char>() + 16);
   if (n > 0) {
     hc_init_rows_kernel<<<hc_grid(n), 256, 0, st>>>(n, parent.as<int32_t>(), size.as<int32_t>(),
                                                     open.as<unsigned char>(), res.as<int32_t>());
@@ -332,18 +335,24 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
     hc_init_tasks_kernel<<<hc_grid(np), 256, 0, st>>>(pi, pj, ps, np, T, liveA.as<int32_t>());
     SPOPS_LAUNCH_CHECK();
   }
-  const unsigned long long np_u = (unsigned long long)np;
-  SPOPS_CUDA(cudaMemcpyAsync(ntasks, &np_u, 8, cudaMemcpyHostToDevice, st));
+  const unsigned long long np_u[2] = {(unsigned long long)np, (unsigned long long)np};
+  SPOPS_CUDA(cudaMemcpyAsync(ntasks, np_u, 16, cudaMemcpyHostToDevice, st));  // tasks made, cnt[0]
   tr.mark(st, "setup");
-  // rounds
+  // rounds, several per host synchronisation once few tasks are live: the
+  // kernels read the live count on the device (grids sized by the last count
+  // the host read, which no later round exceeds), and a round with no live
+  // task does nothing
   int32_t* live = liveA.as<int32_t>();
   int32_t* next = liveB.as<int32_t>();
   int64_t nlive = np, rounds = 0;
+  int cur = 0;
   while (nlive > 0) {
+    const int K = nlive > 65536 ? 1 : (int)std::min<int64_t>(16, std::max<int64_t>(1, 65536 / nlive));
     // every round retires at least one task, so rounds <= tasks ever made
-    if (++rounds > cap + 2) return fail(SPOPS_ERR_CUDA, "clustering: rounds did not end");
-    if (ntask + nlive > cap) {  // room for this round's new tasks
-      const int64_t ncap = std::max<int64_t>(2 * cap, ntask + nlive + 1);
+    rounds += K;
+    if (rounds > cap + 2 + 16) return fail(SPOPS_ERR_CUDA, "clustering: rounds did not end");
+    if (ntask + (int64_t)K * nlive > cap) {  // room for these rounds' new tasks (at most one per live task each)
+      const int64_t ncap = std::max<int64_t>(2 * cap, ntask + (int64_t)K * nlive + 1);
       if (ncap > (int64_t)INT32_MAX) return fail(SPOPS_ERR_UNSUPPORTED, "clustering: more than 2^31 tasks");
       PoolBuf ts2(ctx), ti2(ctx), tj2(ctx), seen2(ctx);
       SPOPS_TRY(ts2.alloc((size_t)ncap * 8));
@@ -369,26 +378,30 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
         SPOPS_LAUNCH_CHECK();
       }
     }
-    SPOPS_CUDA(cudaMemsetAsync(nnext, 0, 8, st));
     const unsigned g = hc_grid(nlive);
-    hc_reserve_kernel<<<g, 256, 0, st>>>(live, nlive, T, parent.as<int32_t>(), open.as<unsigned char>(),
-                                         res.as<int32_t>(), ri.as<int32_t>(), rj.as<int32_t>(), err);
-    hc_commit_kernel<I><<<g, 256, 0, st>>>(live, nlive, T, ri.as<int32_t>(), rj.as<int32_t>(), res.as<int32_t>(),
-                                           parent.as<int32_t>(), size.as<int32_t>(), open.as<unsigned char>(),
-                                           cluster_size, A->row.as<I>(), A->col.as<I>(), pi, pj, np,
-                                           seen.as<unsigned long long>(), seen_slots - 1, cap, ntasks, next, nnext,
-                                           err);
-    hc_release_kernel<<<g, 256, 0, st>>>(ri.as<int32_t>(), rj.as<int32_t>(), nlive, res.as<int32_t>());
-    SPOPS_LAUNCH_CHECK();
+    for (int r = 0; r < K; ++r) {
+      const unsigned long long* nl_d = cnt + cur;
+      SPOPS_CUDA(cudaMemsetAsync(cnt + (cur ^ 1), 0, 8, st));
+      hc_reserve_kernel<<<g, 256, 0, st>>>(live, nl_d, T, parent.as<int32_t>(), open.as<unsigned char>(),
+                                           res.as<int32_t>(), ri.as<int32_t>(), rj.as<int32_t>(), err);
+      hc_commit_kernel<I><<<g, 256, 0, st>>>(live, nl_d, T, ri.as<int32_t>(), rj.as<int32_t>(), res.as<int32_t>(),
+                                             parent.as<int32_t>(), size.as<int32_t>(), open.as<unsigned char>(),
+                                             cluster_size, A->row.as<I>(), A->col.as<I>(), pi, pj, np,
+                                             seen.as<unsigned long long>(), seen_slots - 1, cap, ntasks, next,
+                                             cnt + (cur ^ 1), err);
+      hc_release_kernel<<<g, 256, 0, st>>>(ri.as<int32_t>(), rj.as<int32_t>(), nl_d, res.as<int32_t>());
+      SPOPS_LAUNCH_CHECK();
+      std::swap(live, next);
+      cur ^= 1;
+    }
     int herr = 0;
-    unsigned long long hn[2] = {0, 0};  // next live count, tasks made
+    unsigned long long hn[3] = {0, 0, 0};  // tasks made, cnt[0], cnt[1]
     SPOPS_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
-    SPOPS_CUDA(cudaMemcpyAsync(hn, flags.as<char>() + 8, 16, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(hn, flags.as<char>() + 8, 24, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
     if (herr) return fail(SPOPS_ERR_CUDA, "clustering: device task error %d", herr);
     ntask = (int64_t)hn[0];
-    nlive = (int64_t)hn[1];
-    std::swap(live, next);
+    nlive = (int64_t)hn[1 + cur];
   }
   tr.mark(st, "merge rounds");
   // clusters by root row, rows ascending inside each
