@@ -32,8 +32,7 @@
 //     larger matrices are rejected with SPOPS_ERR_TOO_LARGE before any work;
 //   * every GPU that loads the library holds the array until the process
 //     exits; the first call on a device (with that device current) looks up
-//     its address once per CUDA context (set-up), so make that first call
-//     before any stream capture begins;
+//     its address once per CUDA context;
 //   * all calls on a device share the array: two calls whose work overlaps
 //     on the GPU (different streams, no ordering) race on it.  The error word
 //     is cleared at the start of every call; the window slots need no
