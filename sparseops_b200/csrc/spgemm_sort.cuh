@@ -83,9 +83,64 @@ __device__ __forceinline__ void bitonic_pass(uint32_t (&k)[R], int lane) {
   if constexpr (KK < 32 * R) bitonic_pass<R, KK * 2>(k, lane);
 }
 
+// The same network with the stage loop kept as a loop: one copy of the
+// compare-exchange code per in-lane partner distance (log2 R of them) and one
+// cross-lane copy, so that a large R does not outgrow the instruction cache.
+// Slot indices stay compile-time constants; only the stage sizes are read at
+// run time.
+template <int R, int JJ>
+__device__ __forceinline__ void bitonic_inlane(uint32_t (&k)[R], int lane, int kk) {
+  constexpr int N = 32 * R;
+  const bool lane_asc = (kk >= N) ? true : ((lane & (kk / R)) == 0);
+#pragma unroll
+  for (int s = 0; s < R; ++s) {
+    const int p = s ^ JJ;
+    if (p > s) {
+      const bool asc = kk < R ? (s & kk) == 0 : lane_asc;
+      const uint32_t a = k[s], b = k[p];
+      const uint32_t lo = min(a, b), hi = max(a, b);
+      k[s] = asc ? lo : hi;
+      k[p] = asc ? hi : lo;
+    }
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void bitonic_cross(uint32_t (&k)[R], int lane, int kk, int jj) {
+  constexpr int N = 32 * R;
+  const int lm = jj / R;
+  const bool lower = (lane & lm) == 0;
+  const bool asc = (kk >= N) ? true : ((lane & (kk / R)) == 0);
+  const bool keep_min = lower == asc;
+#pragma unroll
+  for (int s = 0; s < R; ++s) {
+    const uint32_t o = __shfl_xor_sync(0xffffffffu, k[s], lm);
+    k[s] = keep_min ? min(k[s], o) : max(k[s], o);
+  }
+}
+
+template <int R, int JJ>
+__device__ __forceinline__ void bitonic_inlane_at(uint32_t (&k)[R], int lane, int kk, int jj) {
+  if constexpr (JJ >= 1) {
+    if (jj == JJ) bitonic_inlane<R, JJ>(k, lane, kk);
+    else bitonic_inlane_at<R, JJ / 2>(k, lane, kk, jj);
+  }
+}
+
 template <int R>
 __device__ __forceinline__ void warp_bitonic_sort(uint32_t (&k)[R], int lane) {
-  bitonic_pass<R, 2>(k, lane);
+  if constexpr (R < 32) {
+    bitonic_pass<R, 2>(k, lane);
+  } else {
+    constexpr int N = 32 * R;
+#pragma unroll 1
+    for (int kk = 2; kk <= N; kk <<= 1)
+#pragma unroll 1
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        if (jj >= R) bitonic_cross<R>(k, lane, kk, jj);
+        else bitonic_inlane_at<R, R / 2>(k, lane, kk, jj);
+      }
+  }
 }
 
 template <typename I, typename V, int R>
