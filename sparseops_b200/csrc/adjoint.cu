@@ -15,6 +15,7 @@
 
 #include <algorithm>
 
+#include "csr_tile.cuh"
 #include "device_util.cuh"
 #include "spops_internal.h"
 
@@ -167,6 +168,61 @@ spops_status_t build_transpose_t(Context* ctx, Matrix* A) {
   return SPOPS_OK;
 }
 
+// The same SDDMM over the SpMV's tile plan (32 lanes x 8 consecutive
+// entries per tile): each lane loads its 8 columns with one vector load and
+// issues their 8 x gathers together, finds the row of its first entry from
+// the tile's row-start flags (as the tile SpMV does) and steps the row at
+// each flag.  Same products as sddmm_kernel, in the same arithmetic.
+template <typename I, typename V>
+__global__ void __launch_bounds__(256) sddmm_tile_kernel(const I* __restrict__ rp, int64_t n, int64_t nnz,
+                                                         const I* __restrict__ ci,
+                                                         const int64_t* __restrict__ tile_row,
+                                                         const uint8_t* __restrict__ flags_all, int64_t tiles,
+                                                         const V* __restrict__ g, const V* __restrict__ x,
+                                                         V* __restrict__ out, V alpha) {
+  constexpr int K = 8;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;  // lanes below this one
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; t < tiles; t += nw) {
+    const int64_t el = t * (32 * K) + (int64_t)lane * K;
+    I c[K];
+    if (el + K <= nnz) {
+      load_run<I, K>(ci + el, c);
+    } else {
+#pragma unroll
+      for (int b = 0; b < K; ++b) c[b] = el + b < nnz ? ci[el + b] : I(0);
+    }
+    V xv[K];
+#pragma unroll
+    for (int b = 0; b < K; ++b) xv[b] = ld_gather(x + c[b]);
+    const uint32_t flags = flags_all[t * 32 + lane];
+    const int64_t tr = tile_row[t];
+    int64_t row;
+    if (tr >= 0) {
+      const int cnt = __popc(flags);
+      int excl = 0;
+#pragma unroll
+      for (int bit = 0; bit < 4; ++bit) excl += __popc(__ballot_sync(0xffffffffu, (cnt >> bit) & 1) & lt) << bit;
+      const int first0 = (int)(__ballot_sync(0xffffffffu, flags & 1u) & 1u);
+      row = tr + excl + (int)(flags & 1u) - first0;
+    } else {
+      row = row_holding(rp, n, el < nnz ? el : nnz - 1);
+    }
+    V gi = (el < nnz && row < n) ? alpha * g[row] : V(0);
+#pragma unroll
+    for (int b = 0; b < K; ++b) {
+      if (b > 0 && ((flags >> b) & 1u)) {
+        ++row;
+        if (tr < 0)
+          while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
+        gi = row < n ? alpha * g[row] : V(0);
+      }
+      if (el + b < nnz) out[el + b] = gi * xv[b];
+    }
+  }
+}
+
 template <typename I, typename V>
 spops_status_t refresh_values_t(Context* ctx, Matrix* A) {
   TransposeData& T = A->tr;
@@ -183,6 +239,20 @@ template <typename I, typename V>
 spops_status_t sddmm_t(Context* ctx, Matrix* A, double alpha, const void* g, const void* x, void* out) {
   const CsrPlan& P = A->plan;
   if (P.nblocks == 0) return SPOPS_OK;
+  if (ctx->csr_variant == 0 && csr_tile_usable(A, 0)) {  // the tile plan the default SpMV uses
+    if (!P.tiles.ready || P.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(ctx, A, 8));
+    const CsrTiles& D = A->plan.tiles;
+    int64_t grid = (int64_t)ctx->num_sms * 8;
+    const int64_t need = (D.tiles + 7) / 8;
+    if (grid > need) grid = need;
+    if (grid > 0) {
+      sddmm_tile_kernel<I, V><<<(unsigned)grid, 256, 0, ctx->stream>>>(
+          A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), D.tile_row.as<int64_t>(), D.flags.as<uint8_t>(), D.tiles,
+          static_cast<const V*>(g), static_cast<const V*>(x), static_cast<V*>(out), (V)alpha);
+      SPOPS_LAUNCH_CHECK();
+    }
+    return SPOPS_OK;
+  }
   int64_t grid = (int64_t)ctx->num_sms * 8;
   const int64_t need = (P.nblocks + 7) / 8;
   if (grid > need) grid = need;
@@ -219,8 +289,17 @@ spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const v
   if (A->format != SPOPS_FMT_CSR) return fail(SPOPS_ERR_UNSUPPORTED, "transpose SpMV needs a CSR matrix");
   if (!A->plan.ready) SPOPS_TRY(csr_analyse(ctx, A));
   if (!A->tr.ready) SPOPS_TRY(SPOPS_DISPATCH2(A, build_transpose_t, ctx, A));
+  Matrix* V_ = A->tr.view;
+  if (!A->tr.values_fresh && ctx->csr_variant == 0 && csr_tile_usable(V_, 0) &&
+      ((uintptr_t)A->tr.perm.p % 64) == 0) {
+    // values changed since the last refresh (an optimizer step): read A's
+    // values through the permutation inside the SpMV; the reordered copy is
+    // refreshed only when something asks for it (csr_transpose_view)
+    if (!V_->plan.ready) SPOPS_TRY(csr_analyse(ctx, V_));
+    return csr_tile_spmv_indirect(ctx, V_, A->tr.perm.as<int64_t>(), A->val.p, alpha, x, beta, y);
+  }
   if (!A->tr.values_fresh) SPOPS_TRY(SPOPS_DISPATCH2(A, refresh_values_t, ctx, A));
-  return csr_spmv(ctx, A->tr.view, alpha, x, beta, y);
+  return csr_spmv(ctx, V_, alpha, x, beta, y);
 }
 
 spops_status_t csr_transpose_view(Context* ctx, Matrix* A, Matrix** view) {

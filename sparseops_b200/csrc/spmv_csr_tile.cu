@@ -128,6 +128,58 @@ __global__ void __launch_bounds__(kTileBlock, kMinBlocks) csr_tile_kernel(
   }
 }
 
+// The same SpMV with each value read through a permutation: value e is
+// vsrc[perm[e]].  For A^T g while A's values change every step: A^T's
+// values are A's, reordered, and reading them through the permutation inside
+// the SpMV skips writing and re-reading the reordered copy.  The products and
+// their order are those of the plain kernel on the reordered copy.
+template <typename I, typename V>
+__global__ void __launch_bounds__(kTileBlock, 3) csr_tile_indirect_kernel(
+    const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const int64_t* __restrict__ perm,
+    const V* __restrict__ vsrc, const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all,
+    int64_t tiles, const V* __restrict__ x, V* __restrict__ y, V alpha, V beta, bool bz, V* __restrict__ carry_in,
+    V* __restrict__ open_sum, int64_t* __restrict__ open_row) {
+  constexpr int K = 8;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (kTileBlock / 32);
+  int64_t t = blockIdx.x * (int64_t)(kTileBlock / 32) + (threadIdx.x >> 5);
+  if (t >= tiles) return;
+  I c[K];
+  int64_t pm[K];
+  uint32_t flags = 0;
+  int64_t tr = 0;
+  auto load = [&](int64_t tt) {
+    const int64_t el = tt * (32 * K) + (int64_t)lane * K;
+    if (el + K <= nnz) {
+      load_run<I, K>(ci + el, c);
+      load_run<int64_t, K>(perm + el, pm);
+    } else {
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const bool in = el + b < nnz;
+        c[b] = in ? ci[el + b] : I(0);
+        pm[b] = in ? perm[el + b] : 0;
+      }
+    }
+    flags = flags_all[tt * 32 + lane];
+    tr = tile_row[tt];
+  };
+  load(t);
+  for (; t < tiles; t += nw) {
+    const int64_t el = t * (32 * K) + (int64_t)lane * K;
+    V p[K];
+#pragma unroll
+    for (int b = 0; b < K; ++b) {
+      const V a = el + b < nnz ? ld_gather(vsrc + pm[b]) : V(0);
+      p[b] = a * ld_gather(x + c[b]);
+    }
+    const uint32_t f = flags;
+    const int64_t r0 = tr;
+    if (t + nw < tiles) load(t + nw);
+    tile_finish<I, V, K>(rp, n, nnz, t, lane, f, r0, p, y, alpha, beta, bz, carry_in, open_sum, open_row);
+  }
+}
+
 // Rows open at a tile's end receive the heads of the following tiles up to the
 // first one that starts a row; empty rows get y = beta*y.  Tiles [t_begin,
 // tiles) only: a range ends where a row starts, so no chain crosses it.
@@ -330,6 +382,37 @@ spops_status_t spmv_parts_t(Context* ctx, Matrix* A, double alpha, const void* x
   return SPOPS_OK;
 }
 
+template <typename I, typename V>
+spops_status_t spmv_indirect_t(Context* ctx, Matrix* A, const int64_t* perm, const void* vsrc, double alpha,
+                               const void* x, double beta, void* y) {
+  const CsrTiles& D = A->plan.tiles;
+  const bool bz = beta == 0.0;
+  const int64_t tiles = D.tiles;
+  if (tiles > 0) {
+    static int blocks_per_sm = -1;  // per instantiation
+    if (blocks_per_sm < 0) {
+      int bps = 0;
+      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_tile_indirect_kernel<I, V>, kTileBlock, 0));
+      blocks_per_sm = bps > 0 ? bps : 1;
+    }
+    int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
+    const int64_t need = (tiles + kTileBlock / 32 - 1) / (kTileBlock / 32);
+    if (grid > need) grid = need;
+    csr_tile_indirect_kernel<I, V><<<(unsigned)grid, kTileBlock, 0, ctx->stream>>>(
+        A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), perm, static_cast<const V*>(vsrc),
+        D.tile_row.as<int64_t>(), D.flags.as<uint8_t>(), tiles, static_cast<const V*>(x), static_cast<V*>(y),
+        (V)alpha, (V)beta, bz, D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  if (tiles + D.nempty > 0) {
+    csr_tile_calibrate_kernel<V><<<grid_of(tiles + D.nempty), 256, 0, ctx->stream>>>(
+        0, tiles, D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), D.nempty,
+        static_cast<V*>(y), (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
+}
+
 // Kernel shape by variant: (entries per lane, resident blocks, pipelined).
 template <typename I, typename V>
 spops_status_t dispatch(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y) {
@@ -414,6 +497,16 @@ spops_status_t csr_tile_spmm(Context* ctx, Matrix* A, double alpha, const void* 
   if (i32) return spmm_tiles_k<int32_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
   if (f64) return spmm_tiles_k<int64_t, double>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
   return spmm_tiles_k<int64_t, float>(ctx, A, alpha, X, ldx, k, beta, Y, ldy);
+}
+
+spops_status_t csr_tile_spmv_indirect(Context* ctx, Matrix* A, const int64_t* perm, const void* vsrc, double alpha,
+                                      const void* x, double beta, void* y) {
+  if (!A->plan.tiles.ready || A->plan.tiles.k != 8) SPOPS_TRY(csr_tile_analyse(ctx, A, 8));
+  const bool i32 = A->itype == SPOPS_INDEX_I32, f64 = A->vtype == SPOPS_VALUE_F64;
+  if (i32 && f64) return spmv_indirect_t<int32_t, double>(ctx, A, perm, vsrc, alpha, x, beta, y);
+  if (i32) return spmv_indirect_t<int32_t, float>(ctx, A, perm, vsrc, alpha, x, beta, y);
+  if (f64) return spmv_indirect_t<int64_t, double>(ctx, A, perm, vsrc, alpha, x, beta, y);
+  return spmv_indirect_t<int64_t, float>(ctx, A, perm, vsrc, alpha, x, beta, y);
 }
 
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta,

@@ -500,6 +500,10 @@ bool csr_tile_spmm_usable(const Matrix* A, const void* X, int64_t ldx, int64_t k
 spops_status_t csr_tile_spmm(Context* ctx, Matrix* A, double alpha, const void* X, int64_t ldx, int64_t k,
                              double beta, void* Y, int64_t ldy, bool* used);
 spops_status_t csr_tile_analyse(Context* ctx, Matrix* A, int k);
+// the tile SpMV with value e read as vsrc[perm[e]] (A's column and value
+// arrays as csr_tile_usable(A, 0) wants; perm 64-byte aligned)
+spops_status_t csr_tile_spmv_indirect(Context* ctx, Matrix* A, const int64_t* perm, const void* vsrc, double alpha,
+                                      const void* x, double beta, void* y);
 spops_status_t csr_tile_spmv(Context* ctx, Matrix* A, int variant, double alpha, const void* x, double beta, void* y);
 // The default tile SpMV in `parts` row ranges; done(r0, r1) is called after
 // each range is enqueued, when rows [r0, r1) of y are final on the stream.

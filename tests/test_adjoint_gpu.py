@@ -145,3 +145,92 @@ def test_values_update_refreshes_transpose(cuda, orc):
     gx_ref = orc.spmv_t(rp, ci, vals, g.cpu().numpy(), n)
     den = orc.spmv_t(rp, ci, np.abs(vals), np.abs(g.cpu().numpy()), n)
     assert (np.abs(x.grad.cpu().numpy() - gx_ref) / np.maximum(den, 1e-300)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("itype", ["int32", "int64"])
+def test_sddmm_tile_path_exact(cuda, itype):
+    """SDDMM on the tile plan (default CSR variant) and on the segment plan
+    (variant 2) give g_i * x_j * alpha exactly, on rows of very different
+    lengths: empty rows (also inside tiles), one row of 5,000 entries, and a
+    last tile cut short."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, default_context
+    from sparseops_b200._lib import call, dbl, vp
+    rng = np.random.default_rng(23)
+    n, ncols = 3001, 7000
+    lens = rng.integers(0, 40, n)
+    lens[rng.choice(n, 300, replace=False)] = 0
+    lens[17] = 5000
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(itype)
+    rp = rp.astype(itype)
+    v = rng.standard_normal(len(ci))
+    x, g = rng.uniform(-1, 1, ncols), rng.standard_normal(n)
+    dev = torch.device("cuda")
+    A = CSR_Matrix(n, ncols, torch.from_numpy(rp).to(dev), torch.from_numpy(ci).to(dev), torch.from_numpy(v).to(dev))
+    ctx = default_context()
+    h = A.device(ctx)
+    xd, gd = torch.from_numpy(x).to(dev), torch.from_numpy(g).to(dev)
+    rows = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+    want = (0.75 * g[rows]) * x[ci.astype(np.int64)]
+    outs = []
+    try:
+        for variant in (0, 2):
+            ctx.set_option("csr_variant", variant)
+            out = torch.full((len(ci),), np.nan, dtype=torch.float64, device=dev)
+            call("spops_sddmm", ctx.handle, dbl(0.75), h.handle, vp(gd.data_ptr()), vp(xd.data_ptr()),
+                 vp(out.data_ptr()))
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy())
+    finally:
+        ctx.set_option("csr_variant", 0)
+    for o in outs:
+        assert np.array_equal(o.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.parametrize("itype", ["int32", "int64"])
+def test_transpose_spmv_values_through_permutation(cuda, orc, itype):
+    """A^T g right after a value change reads A's values through the
+    transpose's permutation inside the SpMV (default CSR variant); the segment
+    variant refreshes the reordered copy first.  Both agree with the oracle's
+    transpose SpMV to 1e-12 on a rectangular matrix with empty rows and
+    columns and one long row, before and after the values change in place."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, default_context
+    from sparseops_b200._lib import call, dbl, vp
+    rng = np.random.default_rng(29)
+    n, ncols = 2500, 9000
+    lens = rng.integers(0, 30, n)
+    lens[rng.choice(n, 200, replace=False)] = 0
+    lens[5] = 4000
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    g = rng.standard_normal(n)
+    dev = torch.device("cuda")
+    vd = torch.from_numpy(v).to(dev)
+    A = CSR_Matrix(n, ncols, torch.from_numpy(rp.astype(itype)).to(dev), torch.from_numpy(ci.astype(itype)).to(dev), vd)
+    ctx = default_context()
+    h = A.device(ctx)
+    gd = torch.from_numpy(g).to(dev)
+    rp32 = rp.astype(np.int32)
+    try:
+        for step in range(2):
+            if step == 1:  # values changed in place: the handle is told
+                vd.mul_(-1.5).add_(0.25)
+                call("spops_matrix_touch", h.handle)
+            vals = vd.cpu().numpy()
+            want = orc.spmv_t(rp32, ci, vals, g, ncols)
+            den = orc.spmv_t(rp32, ci, np.abs(vals), np.abs(g), ncols)
+            for variant in (0, 2):
+                ctx.set_option("csr_variant", variant)
+                call("spops_matrix_touch", h.handle)
+                out = torch.full((ncols,), np.nan, dtype=torch.float64, device=dev)
+                call("spops_spmv_t", ctx.handle, dbl(1.0), h.handle, vp(gd.data_ptr()), dbl(0.0), vp(out.data_ptr()))
+                torch.cuda.synchronize()
+                err = np.abs(out.cpu().numpy() - want) / np.maximum(den, 1e-300)
+                assert err.max() <= 1e-12, (step, variant, err.max())
+    finally:
+        ctx.set_option("csr_variant", 0)
