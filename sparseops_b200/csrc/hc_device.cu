@@ -18,7 +18,8 @@
 //      are not both roots, queue the root pair with its exact Jaccard score if
 //      it is new and not an initial pair -- a new task, live from the next
 //      round;
-//   3. the reservations are cleared.
+//   3. (nothing to clear: a reservation carries its round's number, so the
+//      next round sees every old one as free).
 // A task that holds its roots is the highest-priority live task touching
 // them, so every cluster sees its steps in the sequential order; steps on
 // disjoint clusters commute.  A new task touches only its creator's roots,
@@ -38,6 +39,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <vector>
 
 #include "spops_internal.h"
@@ -79,13 +81,20 @@ __device__ __forceinline__ int32_t hc_find(const int32_t* __restrict__ parent, i
 
 constexpr int kCasLimit = 1 << 22;  // CAS attempts on one root before the round reports an error
 
-// keep the better of the current holder and task c in res[r]
-__device__ __forceinline__ void hc_reserve(int32_t* __restrict__ res, int32_t r, int32_t c, const Tasks& T,
-                                           int* __restrict__ err) {
-  int32_t cur = res[r];
+// A reservation is (round << 32 | task): one made in an earlier round is
+// stale, so nothing needs clearing between rounds.
+__device__ __forceinline__ unsigned long long hc_stamp(uint32_t round, int32_t c) {
+  return ((unsigned long long)round << 32) | (uint32_t)c;
+}
+
+// keep the better of the current holder (of this round) and task c in res[r]
+__device__ __forceinline__ void hc_reserve(unsigned long long* __restrict__ res, int32_t r, int32_t c, uint32_t round,
+                                           const Tasks& T, int* __restrict__ err) {
+  unsigned long long cur = res[r];
+  const unsigned long long mine = hc_stamp(round, c);
   for (int it = 0; it < kCasLimit; ++it) {
-    if (cur >= 0 && !hc_above(T, c, cur)) return;
-    const int32_t old = atomicCAS(res + r, cur, c);
+    if ((uint32_t)(cur >> 32) == round && !hc_above(T, c, (int32_t)(uint32_t)cur)) return;
+    const unsigned long long old = atomicCAS(res + r, cur, mine);
     if (old == cur) return;
     cur = old;
   }
@@ -103,13 +112,13 @@ __global__ void hc_check_pairs_kernel(const int64_t* __restrict__ pi, const int6
 }
 
 __global__ void hc_init_rows_kernel(int64_t n, int32_t* __restrict__ parent, int32_t* __restrict__ size,
-                                    unsigned char* __restrict__ open, int32_t* __restrict__ res) {
+                                    unsigned char* __restrict__ open, unsigned long long* __restrict__ res) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
   parent[r] = (int32_t)r;
   size[r] = 1;
   open[r] = 1;
-  res[r] = -1;
+  res[r] = 0;  // round 0: no round runs as 0
 }
 
 __global__ void hc_init_tasks_kernel(const int64_t* __restrict__ pi, const int64_t* __restrict__ pj,
@@ -122,13 +131,16 @@ __global__ void hc_init_tasks_kernel(const int64_t* __restrict__ pi, const int64
   live[t] = (int32_t)t;
 }
 
-// 1. roots and reservations; tasks that can have no effect retire here
+// 1. roots and reservations; tasks that can have no effect retire here.
+// Also zeroes the count of the next round's live tasks (the commit kernel
+// after it adds to that count).
 __global__ void hc_reserve_kernel(const int32_t* __restrict__ live, const unsigned long long* __restrict__ nlive_d,
-                                  Tasks T,
+                                  unsigned long long* __restrict__ nnext, uint32_t round, Tasks T,
                                   const int32_t* __restrict__ parent, const unsigned char* __restrict__ open,
-                                  int32_t* __restrict__ res, int32_t* __restrict__ ri_out, int32_t* __restrict__ rj_out,
-                                  int* __restrict__ err) {
+                                  unsigned long long* __restrict__ res, int32_t* __restrict__ ri_out,
+                                  int32_t* __restrict__ rj_out, int* __restrict__ err) {
   const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q == 0) *nnext = 0;
   if (q >= (int64_t)*nlive_d) return;
   const int32_t c = live[q];
   const int32_t ri = hc_find(parent, T.i[c], err), rj = hc_find(parent, T.j[c], err);
@@ -139,8 +151,8 @@ __global__ void hc_reserve_kernel(const int32_t* __restrict__ live, const unsign
   }
   ri_out[q] = ri;
   rj_out[q] = rj;
-  hc_reserve(res, ri, c, T, err);
-  hc_reserve(res, rj, c, T, err);
+  hc_reserve(res, ri, c, round, T, err);
+  hc_reserve(res, rj, c, round, T, err);
 }
 
 // |row a ∩ row b| / |row a ∪ row b| over entry counts, as the host loop
@@ -201,7 +213,8 @@ template <typename I>
 __global__ void hc_commit_kernel(const int32_t* __restrict__ live, const unsigned long long* __restrict__ nlive_d,
                                  Tasks T,
                                  const int32_t* __restrict__ ri_in, const int32_t* __restrict__ rj_in,
-                                 const int32_t* __restrict__ res, int32_t* __restrict__ parent,
+                                 const unsigned long long* __restrict__ res, uint32_t round,
+                                 int32_t* __restrict__ parent,
                                  int32_t* __restrict__ size, unsigned char* __restrict__ open, int64_t cluster_size,
                                  const I* __restrict__ rp, const I* __restrict__ ci, const int64_t* __restrict__ pi,
                                  const int64_t* __restrict__ pj, int64_t np, unsigned long long* __restrict__ seen,
@@ -213,7 +226,8 @@ __global__ void hc_commit_kernel(const int32_t* __restrict__ live, const unsigne
   const int32_t ri = ri_in[q], rj = rj_in[q];
   if (ri < 0) return;  // retired in the reserve pass
   const int32_t c = live[q];
-  if (res[ri] != c || res[rj] != c) {  // a better task holds a root: next round
+  const unsigned long long mine = hc_stamp(round, c);
+  if (res[ri] != mine || res[rj] != mine) {  // a better task holds a root: next round
     next_live[atomicAdd(nnext, 1ULL)] = c;
     return;
   }
@@ -247,16 +261,6 @@ __global__ void hc_seen_rebuild_kernel(Tasks T, int64_t np, int64_t ntask, unsig
   if (t >= ntask) return;
   const unsigned long long key = ((unsigned long long)(uint32_t)T.i[t] << 32) | (uint32_t)T.j[t];
   hc_seen_insert(tab, mask, key, err);
-}
-
-// 3. clear the round's reservations
-__global__ void hc_release_kernel(const int32_t* __restrict__ ri_in, const int32_t* __restrict__ rj_in,
-                                  const unsigned long long* __restrict__ nlive_d, int32_t* __restrict__ res) {
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= (int64_t)*nlive_d) return;
-  const int32_t ri = ri_in[q], rj = rj_in[q];
-  if (ri >= 0) res[ri] = -1;
-  if (rj >= 0) res[rj] = -1;
 }
 
 __global__ void hc_roots_kernel(const int32_t* __restrict__ parent, int64_t n, uint32_t* __restrict__ key,
@@ -299,7 +303,7 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
   SPOPS_TRY(parent.alloc(nn * 4));
   SPOPS_TRY(size.alloc(nn * 4));
   SPOPS_TRY(open.alloc(nn));
-  SPOPS_TRY(res.alloc(nn * 4));
+  SPOPS_TRY(res.alloc(nn * 8));
   SPOPS_TRY(flags.alloc(64));
   SPOPS_CUDA(cudaMemsetAsync(flags.p, 0, 64, st));
   int* err = flags.as<int>();
@@ -308,7 +312,7 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
   unsigned long long* cnt = reinterpret_cast<unsigned long long*>(flags.as<char>() + 16);
   if (n > 0) {
     hc_init_rows_kernel<<<hc_grid(n), 256, 0, st>>>(n, parent.as<int32_t>(), size.as<int32_t>(),
-                                                    open.as<unsigned char>(), res.as<int32_t>());
+                                                    open.as<unsigned char>(), res.as<unsigned long long>());
     SPOPS_LAUNCH_CHECK();
   }
   // tasks: the initial pairs, then the pairs found while merging.  A round
@@ -346,6 +350,7 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
   int32_t* next = liveB.as<int32_t>();
   int64_t nlive = np, rounds = 0;
   int cur = 0;
+  uint64_t round_stamp = 0;  // below 2^32: the round bound keeps it there
   while (nlive > 0) {
     const int K = nlive > 65536 ? 1 : (int)std::min<int64_t>(16, std::max<int64_t>(1, 65536 / nlive));
     // every round retires at least one task, so rounds <= tasks ever made
@@ -381,15 +386,16 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
     const unsigned g = hc_grid(nlive);
     for (int r = 0; r < K; ++r) {
       const unsigned long long* nl_d = cnt + cur;
-      SPOPS_CUDA(cudaMemsetAsync(cnt + (cur ^ 1), 0, 8, st));
-      hc_reserve_kernel<<<g, 256, 0, st>>>(live, nl_d, T, parent.as<int32_t>(), open.as<unsigned char>(),
-                                           res.as<int32_t>(), ri.as<int32_t>(), rj.as<int32_t>(), err);
-      hc_commit_kernel<I><<<g, 256, 0, st>>>(live, nl_d, T, ri.as<int32_t>(), rj.as<int32_t>(), res.as<int32_t>(),
-                                             parent.as<int32_t>(), size.as<int32_t>(), open.as<unsigned char>(),
-                                             cluster_size, A->row.as<I>(), A->col.as<I>(), pi, pj, np,
+      const uint32_t stamp = (uint32_t)(++round_stamp);  // reservations of earlier rounds are stale
+      hc_reserve_kernel<<<g, 256, 0, st>>>(live, nl_d, cnt + (cur ^ 1), stamp, T, parent.as<int32_t>(),
+                                           open.as<unsigned char>(), res.as<unsigned long long>(), ri.as<int32_t>(),
+                                           rj.as<int32_t>(), err);
+      hc_commit_kernel<I><<<g, 256, 0, st>>>(live, nl_d, T, ri.as<int32_t>(), rj.as<int32_t>(),
+                                             res.as<unsigned long long>(), stamp, parent.as<int32_t>(),
+                                             size.as<int32_t>(), open.as<unsigned char>(), cluster_size,
+                                             A->row.as<I>(), A->col.as<I>(), pi, pj, np,
                                              seen.as<unsigned long long>(), seen_slots - 1, cap, ntasks, next,
                                              cnt + (cur ^ 1), err);
-      hc_release_kernel<<<g, 256, 0, st>>>(ri.as<int32_t>(), rj.as<int32_t>(), nl_d, res.as<int32_t>());
       SPOPS_LAUNCH_CHECK();
       std::swap(live, next);
       cur ^= 1;
@@ -403,7 +409,11 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
     ntask = (int64_t)hn[0];
     nlive = (int64_t)hn[1 + cur];
   }
-  tr.mark(st, "merge rounds");
+  if (tr.on) {
+    char what[48];
+    std::snprintf(what, sizeof(what), "merge rounds (%lld)", (long long)rounds);
+    tr.mark(st, what);
+  }
   // clusters by root row, rows ascending inside each
   PoolBuf key(ctx), skey(ctx), row(ctx), flag(ctx), cid(ctx), tmp(ctx);
   SPOPS_TRY(key.alloc(nn * 4));
