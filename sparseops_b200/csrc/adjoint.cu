@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) sddmm_tile_kernel(const I* __restrict__ r
                                                          const int64_t* __restrict__ tile_row,
                                                          const uint8_t* __restrict__ flags_all, int64_t tiles,
                                                          const V* __restrict__ g, const V* __restrict__ x,
-                                                         V* __restrict__ out, V alpha) {
+                                                         V* __restrict__ out, V alpha, bool vec_out) {
   constexpr int K = 8;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;  // lanes below this one
@@ -210,6 +210,7 @@ __global__ void __launch_bounds__(256) sddmm_tile_kernel(const I* __restrict__ r
       row = row_holding(rp, n, el < nnz ? el : nnz - 1);
     }
     V gi = (el < nnz && row < n) ? alpha * g[row] : V(0);
+    V o[K];
 #pragma unroll
     for (int b = 0; b < K; ++b) {
       if (b > 0 && ((flags >> b) & 1u)) {
@@ -218,7 +219,14 @@ __global__ void __launch_bounds__(256) sddmm_tile_kernel(const I* __restrict__ r
           while (row + 1 < n && rp[row] == rp[row + 1]) ++row;  // skip empty rows
         gi = row < n ? alpha * g[row] : V(0);
       }
-      if (el + b < nnz) out[el + b] = gi * xv[b];
+      o[b] = gi * xv[b];
+    }
+    if (vec_out && el + K <= nnz) {  // whole 32-byte sectors: one store request per sector
+      store_run<V, K>(out + el, o);
+    } else {
+#pragma unroll
+      for (int b = 0; b < K; ++b)
+        if (el + b < nnz) out[el + b] = o[b];
     }
   }
 }
@@ -248,7 +256,8 @@ spops_status_t sddmm_t(Context* ctx, Matrix* A, double alpha, const void* g, con
     if (grid > 0) {
       sddmm_tile_kernel<I, V><<<(unsigned)grid, 256, 0, ctx->stream>>>(
           A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), D.tile_row.as<int64_t>(), D.flags.as<uint8_t>(), D.tiles,
-          static_cast<const V*>(g), static_cast<const V*>(x), static_cast<V*>(out), (V)alpha);
+          static_cast<const V*>(g), static_cast<const V*>(x), static_cast<V*>(out), (V)alpha,
+          ((uintptr_t)out % 32) == 0);
       SPOPS_LAUNCH_CHECK();
     }
     return SPOPS_OK;

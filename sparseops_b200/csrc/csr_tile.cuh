@@ -62,6 +62,21 @@ __device__ __forceinline__ void load_run(const T* __restrict__ p, T (&out)[K]) {
   }
 }
 
+// K elements of T to p (32-byte aligned) with 256-bit stores: a lane's run
+// is written as whole 32-byte sectors.
+template <typename T, int K>
+__device__ __forceinline__ void store_run(T* __restrict__ p, const T (&v)[K]) {
+  constexpr int BYTES = K * (int)sizeof(T);
+  static_assert(BYTES % 32 == 0, "run must be a multiple of 32 bytes");
+  unsigned long long w[BYTES / 8];
+  memcpy(w, v, BYTES);
+#pragma unroll
+  for (int q = 0; q < BYTES / 32; ++q)
+    asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(reinterpret_cast<char*>(p) + 32 * q),
+                 "l"(w[4 * q]), "l"(w[4 * q + 1]), "l"(w[4 * q + 2]), "l"(w[4 * q + 3])
+                 : "memory");
+}
+
 // Columns and values of lane `lane`'s run of tile t; entries past nnz read as
 // column 0 with value 0.
 template <typename I, typename V, int K>
