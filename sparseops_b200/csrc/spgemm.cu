@@ -890,7 +890,10 @@ __global__ void num_bin_kernel(const int64_t* __restrict__ nz, const int64_t* __
 // sort path (spgemm_sort.cuh): bin q (R = 2^q keys per lane, q = 0..6)
 // for a cluster with at most 32 * 2^q products and kSortCols columns whose
 // output columns fit the key beside the product index; settled[c] = 1 then.
-constexpr int kSortBins = 7;
+// bins 0-4: one warp, 2^q keys per lane (sort_accum_kernel); bins 5-8: 2^(q-4)
+// warps of 16 keys per lane (sort_accum_multi_kernel); bin q holds P <= 32 << q
+constexpr int kSortBins = 9;
+constexpr int kSortOneWarpBins = 5;
 
 __global__ void sort_bin_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ cptr, int64_t ncl,
                                 int64_t bcols, unsigned char* __restrict__ settled, uint32_t* __restrict__ key,
@@ -900,13 +903,12 @@ __global__ void sort_bin_kernel(const int64_t* __restrict__ flops, const int64_t
   ids[c] = c;
   const int64_t P = flops[c], nj = cptr[c + 1] - cptr[c];
   uint32_t b = kNoBin;
-  if (nj <= kSortCols) {
-    for (int q = 0; q < kSortBins; ++q) {
-      if (P <= (32LL << q)) {
-        const int tbits = 5 + q;
-        if (bcols <= (1LL << (32 - tbits)) - 1) b = (uint32_t)q;
-        break;
-      }
+  for (int q = 0; q < kSortBins; ++q) {
+    if (P <= (32LL << q)) {
+      const int tbits = 5 + q;
+      const int64_t max_cols = q < kSortOneWarpBins ? kSortCols : kMultiCols;
+      if (nj <= max_cols && bcols <= (1LL << (32 - tbits)) - 1) b = (uint32_t)q;
+      break;
     }
   }
   key[c] = b;
@@ -914,7 +916,7 @@ __global__ void sort_bin_kernel(const int64_t* __restrict__ flops, const int64_t
 }
 
 // room in each cluster's output slab: its product count on the sort path (at
-// most 32 * 2^6, and never below its distinct columns whatever B holds), the
+// most 32 * 2^8, and never below its distinct columns whatever B holds), the
 // symbolic count otherwise; values: that times the cluster size
 __global__ void slab_cap_kernel(const int64_t* __restrict__ flops, const int64_t* __restrict__ nz,
                                 const unsigned char* __restrict__ settled, const int64_t* __restrict__ offsets,
@@ -1457,16 +1459,27 @@ spops_status_t spgemm_t(Context* ctx, Matrix* A, Matrix* B, const int64_t* perm_
       B->row.as<I>(), B->col.as<I>(), B->val.as<V>(), tbits, b_rowdense, l2_budget, sort_output, rowwise,        \
       soff.as<int64_t>(), soff_val.as<int64_t>(), nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>(),      \
       drop.as<unsigned char>(), reinterpret_cast<unsigned long long*>(ndense.p), ccol.as<int32_t>(), cval.as<V>())
+#define SPOPS_MULTI_LAUNCH(WW)                                                                                    \
+  SPOPS_CUDA(cudaFuncSetAttribute(sort_accum_multi_kernel<I, V, WW>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)sort_multi_smem<V, WW>()));                                                \
+  sort_accum_multi_kernel<I, V, WW><<<(unsigned)m, 32 * WW, sort_multi_smem<V, WW>(), st>>>(                     \
+      dl, m, cptr.as<int64_t>(), cptr_val.as<int64_t>(), colids.as<int32_t>(), avals.as<V>(), offs.as<int64_t>(), \
+      B->row.as<I>(), B->col.as<I>(), B->val.as<V>(), tbits, b_rowdense, l2_budget, sort_output, rowwise,        \
+      soff.as<int64_t>(), soff_val.as<int64_t>(), nzd.as<int64_t>(), cmin.as<int64_t>(), cmax.as<int64_t>(),      \
+      drop.as<unsigned char>(), reinterpret_cast<unsigned long long*>(ndense.p), ccol.as<int32_t>(), cval.as<V>())
     switch (q) {
       case 0: SPOPS_SORT_LAUNCH(1); break;
       case 1: SPOPS_SORT_LAUNCH(2); break;
       case 2: SPOPS_SORT_LAUNCH(4); break;
       case 3: SPOPS_SORT_LAUNCH(8); break;
       case 4: SPOPS_SORT_LAUNCH(16); break;
-      case 5: SPOPS_SORT_LAUNCH(32); break;
-      default: SPOPS_SORT_LAUNCH(64); break;
+      case 5: SPOPS_MULTI_LAUNCH(2); break;
+      case 6: SPOPS_MULTI_LAUNCH(4); break;
+      case 7: SPOPS_MULTI_LAUNCH(8); break;
+      default: SPOPS_MULTI_LAUNCH(16); break;
     }
 #undef SPOPS_SORT_LAUNCH
+#undef SPOPS_MULTI_LAUNCH
     SPOPS_LAUNCH_CHECK();
   }
   tr.mark(st, "sort-path kernels");
