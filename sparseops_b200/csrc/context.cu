@@ -64,7 +64,7 @@ void DevBuf::release() {
   home = nullptr;
 }
 
-constexpr size_t kCacheMin = size_t(8) << 20;   // blocks below this go back to the driver
+constexpr size_t kCacheMin = size_t(1) << 20;   // blocks below this go back to the driver
 constexpr size_t kCacheMax = size_t(24) << 30;  // bytes the cache may hold
 
 spops_status_t DevBuf::alloc_cached(Context* ctx, size_t n) {

@@ -67,6 +67,34 @@ __global__ void band_hash_kernel(const uint64_t* __restrict__ sig, int64_t n, in
   rows[i] = (int32_t)i;
 }
 
+// Bucket value -> a small id: its slot in an open-addressing table of at
+// least 2n slots (equal values get equal slots, different values different
+// ones), so that the rows are grouped by a sort on log2(slots) + 1 bits
+// instead of 64.  The value ~0 (the table's empty mark) gets id mask + 1.
+__global__ void bucket_id_kernel(uint64_t* __restrict__ key, int64_t n, unsigned long long* __restrict__ tab,
+                                 uint64_t mask, int* __restrict__ err) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long h = key[i];
+  if (h == ~0ULL) {
+    key[i] = mask + 1;
+    return;
+  }
+  unsigned long long x = h ^ (h >> 29);
+  x *= 0xbf58476d1ce4e5b9ULL;
+  x ^= x >> 32;
+  uint64_t slot = x & mask;
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    const unsigned long long old = atomicCAS(tab + slot, ~0ULL, h);
+    if (old == ~0ULL || old == h) {
+      key[i] = slot;
+      return;
+    }
+    slot = (slot + 1) & mask;
+  }
+  atomicOr(err, 1);  // table full: cannot happen with 2n slots
+}
+
 __global__ void run_flag_kernel(const uint64_t* __restrict__ key, int64_t n, int64_t* __restrict__ flag) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) flag[i] = (i == 0 || key[i] != key[i - 1]) ? 1 : 0;
@@ -169,7 +197,11 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   }
   const size_t cub_max = std::max({cub_sort, cub_scan, cub_rle});
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t need = al(nn * 8) * 2 + al(nn * 4) * 2 + al(nn * 8) * 7 + cub_max + 512;
+  uint64_t slots = 1;
+  while (slots < 2 * nn) slots <<= 1;
+  int id_bits = 1;  // ids are below slots + 1
+  while (id_bits < 64 && (uint64_t(1) << id_bits) <= slots) ++id_bits;
+  const size_t need = al(nn * 8) * 2 + al(nn * 4) * 2 + al(nn * 8) * 7 + cub_max + 512 + al(slots * 8) + 256;
   SPOPS_TRY(ctx->scratch_reserve(need));
   char* base = ctx->scratch.as<char>();
   size_t o = 0;
@@ -187,6 +219,9 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   int64_t* off = reinterpret_cast<int64_t*>(take(nn * 8));
   int64_t* nruns = reinterpret_cast<int64_t*>(take(8));
   void* cub_tmp = take(cub_max);
+  unsigned long long* tab = reinterpret_cast<unsigned long long*>(take(slots * 8));
+  int* id_err = reinterpret_cast<int*>(take(8));
+  SPOPS_CUDA(cudaMemsetAsync(id_err, 0, 4, st));
 
   tr.mark(st, "setup");
   // pairs of every band, appended
@@ -194,8 +229,11 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   int64_t total = 0, cap = 0;
   for (int band = 0; band < bands; ++band) {
     band_hash_kernel<<<grid_for(n), 256, 0, st>>>(sig, n, k, band, r, key_in, row_in);
+    SPOPS_CUDA(cudaMemsetAsync(tab, 0xff, slots * 8, st));
+    bucket_id_kernel<<<grid_for(n), 256, 0, st>>>(key_in, n, tab, slots - 1, id_err);
     SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_sort, key_in, key_out, row_in, row_out, n, 0, 64, st));
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_sort, key_in, key_out, row_in, row_out, n, 0, id_bits,
+                                               st));
     run_flag_kernel<<<grid_for(n), 256, 0, st>>>(key_out, n, flag);
     SPOPS_LAUNCH_CHECK();
     size_t inc_bytes = cub_max;
@@ -206,9 +244,12 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
     SPOPS_LAUNCH_CHECK();
     SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, cnt, off, n, st));
     int64_t h[2];
+    int herr = 0;
     SPOPS_CUDA(cudaMemcpyAsync(&h[0], off + n - 1, 8, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaMemcpyAsync(&h[1], cnt + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&herr, id_err, 4, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
+    if (herr) return fail(SPOPS_ERR_CUDA, "LSH: bucket table full");
     const int64_t np = h[0] + h[1];
     if (np == 0) continue;
     if (total + np > cap) {  // grow the pair buffer
