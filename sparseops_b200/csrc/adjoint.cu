@@ -127,10 +127,11 @@ spops_status_t build_transpose_t(Context* ctx, Matrix* A) {
   void* cub_tmp = take(std::max(cub_sort, cub_scan));
 
   T.release();
-  SPOPS_TRY(T.rp.alloc(nc1 * sizeof(I)));
-  SPOPS_TRY(T.ri.alloc(nz * sizeof(I)));
-  SPOPS_TRY(T.perm.alloc(nz * 8));
-  SPOPS_TRY(T.val.alloc(nz * sizeof(V)));
+  // large arrays: reuse blocks earlier results of this context released
+  SPOPS_TRY(T.rp.alloc_cached(ctx, nc1 * sizeof(I)));
+  SPOPS_TRY(T.ri.alloc_cached(ctx, nz * sizeof(I)));
+  SPOPS_TRY(T.perm.alloc_cached(ctx, nz * 8));
+  SPOPS_TRY(T.val.alloc_cached(ctx, nz * sizeof(V)));
   SPOPS_CUDA(cudaMemsetAsync(cnt, 0, nc1 * 8, st));
   if (nnz > 0) {
     count_cols_kernel<I><<<std::min<unsigned>(grid_for(nnz), 8192u), 256, 0, st>>>(A->col.as<I>(), nnz, cnt);

@@ -243,7 +243,7 @@ spops_status_t topk_t(Context* ctx, Matrix* A, int64_t top_k, Matrix** out) {
   } gb{Ab};
   Ab->row.borrow(A->row.p, A->row.bytes);
   Ab->col.borrow(A->col.p, A->col.bytes);
-  SPOPS_TRY(Ab->val.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(V)));
+  SPOPS_TRY(Ab->val.alloc_cached(ctx, (size_t)std::max<int64_t>(nnz, 1) * sizeof(V)));
   if (nnz > 0) {
     fill_kernel<V><<<grid_for(nnz), 256, 0, st>>>(Ab->val.as<V>(), nnz, V(1));
     SPOPS_LAUNCH_CHECK();
