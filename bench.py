@@ -744,7 +744,8 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288, peak=None):
            "clusters": st.get("clusters"), "dense_clusters": st.get("dense_clusters")}
     # the SpGEMM proper (symbolic + numeric + to CSR) for a fixed clustering
     from sparseops_b200.spgemm import hierarchical_clustering_v0_fast, lsh_candidate_pairs_vector
-    pairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
+    with torch_nvtx_range("lsh_pairs_planted"):
+        pairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
     perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
     with torch.cuda.nvtx.range("clustered_spgemm_planted"):  # a range profilers can select
         kms = _host_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 5, warm=2)
@@ -760,7 +761,8 @@ def bench_spgemm(dev, cpu_ref: bool, n=524288, peak=None):
     rms = _host_ms(lambda: LeSpGEMM(A, B, 1, False), 3, warm=1)
     out["rowwise_ms"] = round(rms, 3)
     out["rowwise_GFLOP/s"] = round(flops / rms / 1e6, 2)
-    tms = _host_ms(lambda: HashSpGEMMTopK(A, 16), 3, warm=1)
+    with torch_nvtx_range("topk16_planted"):
+        tms = _host_ms(lambda: HashSpGEMMTopK(A, 16), 3, warm=1)
     out["topk16_ms"] = round(tms, 3)
     if cpu_ref:
         try:
@@ -793,8 +795,8 @@ def bench_spgemm_grouped(dev, cpu_ref: bool, n=524288, peak=None):
     multi-row and dense parts of the hybrid accumulator at scale."""
     import torch
     from sparseops_b200 import CSR_Matrix, synth
-    from sparseops_b200.spgemm import (LeSpGEMM_clustered, LeSpGEMM_lsh, hierarchical_clustering_v0_fast,
-                                       lsh_candidate_pairs_vector)
+    from sparseops_b200.spgemm import (LeSpGEMM_clustered, LeSpGEMM_lsh, hierarchical_clustering_device,
+                                       hierarchical_clustering_v0_fast, lsh_candidate_pairs_vector)
     arp, aci, av, nc = synth.grouped_rows(n)
     brp, bci, bv = synth.transpose(arp, aci, av, nc)
     A = CSR_Matrix(n, nc, torch.from_numpy(arp).to(dev), torch.from_numpy(aci).to(dev), torch.from_numpy(av).to(dev))
@@ -805,12 +807,15 @@ def bench_spgemm_grouped(dev, cpu_ref: bool, n=524288, peak=None):
     flops = st["flops"]
     pairs = lsh_candidate_pairs_vector(A, 64, 16, 7)
     perm, offs = hierarchical_clustering_v0_fast(arp, aci, n, pairs, 8)
+    with torch_nvtx_range("hc_device_grouped"):
+        hms = _host_ms(lambda: hierarchical_clustering_device(A, pairs, 8), 3, warm=1)
     kms = _host_ms(lambda: LeSpGEMM_clustered(A, B, perm, offs), 5, warm=2)
     compulsory = (2 * 16 * len(aci) + 8 * (n + 1) + 8 * (nc + 1) + 16 * int(C.num_nnzs) + 8 * (n + 1))
     out = {"rows": n, "cols_A": nc, "nnz_A": int(len(aci)), "nnz_C": int(C.num_nnzs), "flops": int(flops),
            "pairs": st.get("pairs"), "clusters": st.get("clusters"), "dense_clusters": st.get("dense_clusters"),
            "largest_cluster": int(np.diff(offs).max()), "compulsory_bytes": int(compulsory),
            "pipeline_ms": round(total, 3), "stages_ms": {k: round(st[k], 3) for k in st if k.endswith("_ms")},
+           "hc_device_ms": round(hms, 3),
            "spgemm_clustered_ms": round(kms, 3), "spgemm_clustered_GFLOP/s": round(flops / kms / 1e6, 2)}
     if peak:
         out["spgemm_clustered_roofline"] = {"bound": "hbm", "achieved": round(compulsory / kms / 1e6, 1),

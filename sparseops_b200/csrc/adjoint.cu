@@ -104,12 +104,15 @@ spops_status_t build_transpose_t(Context* ctx, Matrix* A) {
   cudaStream_t st = ctx->stream;
   const int64_t n = A->rows, nc = A->cols, nnz = A->nnz;
   size_t cub_sort = 0, cub_scan = 0;
+  // columns are in [0, nc): the stable sort needs only their low bits
+  int col_bits = 1;
+  while (col_bits < 8 * (int)sizeof(I) - 1 && ((nc - 1) >> col_bits) > 0) ++col_bits;
   {
     I* k = nullptr;
     int64_t* v = nullptr;
     unsigned long long* u = nullptr;
     SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort, k, k, v, v, (int64_t)(nnz > 0 ? nnz : 1), 0,
-                                               8 * (int)sizeof(I), st));
+                                               col_bits, st));
     SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, u, u, (int64_t)(nc + 1), st));
   }
   const size_t nz = (size_t)(nnz > 0 ? nnz : 1), nc1 = (size_t)nc + 1;
@@ -138,7 +141,7 @@ spops_status_t build_transpose_t(Context* ctx, Matrix* A) {
     iota64_kernel<<<grid_for(nnz), 256, 0, st>>>(idx, nnz);
     SPOPS_LAUNCH_CHECK();
     SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_sort, A->col.as<I>(), keys_out, idx, T.perm.as<int64_t>(),
-                                               nnz, 0, 8 * (int)sizeof(I), st));
+                                               nnz, 0, col_bits, st));
     expand_rows_kernel<I><<<grid_for(n * 32), 256, 0, st>>>(A->row.as<I>(), n, rows);
     gather_index_kernel<I><<<grid_for(nnz), 256, 0, st>>>(T.perm.as<int64_t>(), rows, nnz, T.ri.as<I>());
     SPOPS_LAUNCH_CHECK();

@@ -142,52 +142,104 @@ __device__ __forceinline__ void warp_sort32(uint64_t& k, int64_t& c) {
     for (int j = b >> 1; j > 0; j >>= 1) warp_cx(k, c, j, (lane & b) == 0);
 }
 
-// Top-k (k <= 32) without the full sort: one warp per row of the
-// intersection counts keeps its best 32 entries, sorted across the lanes, and
-// merges every further 32 entries into them (lane l keeps the better of
-// best[l] and new[31 - l], which leaves the best 32 of both as a bitonic
-// sequence; five steps sort it).  A chunk with nothing better than the
-// current k-th entry is skipped.  The first k of the row go to tkey / tcol at
-// row * k, and kept[row] = min(k, entries - diagonal).
+// Top-k (k <= 32) without sorting every entry: one warp per row of the
+// intersection counts keeps the row's best 32 entries so far sorted across
+// the lanes (lane l holds the l-th best).  Only entries that rank before the
+// current k-th best are kept as candidates, compacted into a per-warp buffer
+// in shared memory; each time 32 are there they are sorted and merged into
+// the best 32 (lane l keeps the better of best[l] and cand[31 - l], which
+// leaves the best 32 of both as a bitonic sequence; five steps sort it) and
+// the k-th best moves up.  An entry that does not beat the k-th best when it
+// is read ranks after k entries of the row, so the filter drops nothing of
+// the result; the candidates left at the end of the row are merged last.
+// A random order of m entries brings about k ln(m / k) candidates, so most
+// chunks of 32 entries cost a ballot instead of a 32-wide sort.  Two chunks
+// are read per step to keep more loads in flight.  The first k of the row go
+// to tkey / tcol at row * k, and kept[row] = min(k, entries - diagonal).
+constexpr int kSelectWarps = 8;
+
 template <typename I, typename V>
-__global__ void topk_select_kernel(const I* __restrict__ crp, const I* __restrict__ cci, const V* __restrict__ cval,
-                                   const I* __restrict__ arp, int64_t n, int k, uint64_t* __restrict__ tkey,
-                                   I* __restrict__ tcol, int64_t* __restrict__ kept) {
-  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+__global__ void __launch_bounds__(kSelectWarps * 32)
+    topk_select_kernel(const I* __restrict__ crp, const I* __restrict__ cci, const V* __restrict__ cval,
+                       const I* __restrict__ arp, int64_t n, int k, uint64_t* __restrict__ tkey,
+                       I* __restrict__ tcol, int64_t* __restrict__ kept) {
+  __shared__ uint64_t s_key[kSelectWarps][64];
+  __shared__ int64_t s_col[kSelectWarps][64];
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;  // one row per warp
   const int lane = threadIdx.x & 31;
-  if (i >= n) return;
+  if (i >= n || k <= 0) return;  // kept[] is zeroed by the caller
+  uint64_t* const buf_k = s_key[threadIdx.x >> 5];
+  int64_t* const buf_c = s_col[threadIdx.x >> 5];
+  const unsigned below = (1u << lane) - 1u;
   const int64_t e0 = crp[i], e1 = crp[i + 1];
   const int64_t li = (int64_t)arp[i + 1] - (int64_t)arp[i];
   uint64_t bk = kDiagKey;  // padding sorts after every entry, the diagonal included
   int64_t bc = INT64_MAX;
-  int diag = 0;
-  for (int64_t base = e0; base < e1; base += 32) {
-    const int64_t e = base + lane;
-    uint64_t key = kDiagKey;
-    int64_t col = INT64_MAX;
-    if (e < e1) {
-      col = (int64_t)cci[e];
-      if (col == i) {
-        diag = 1;
-      } else {
-        const V inter = cval[e];
-        const int64_t u = li + ((int64_t)arp[col + 1] - (int64_t)arp[col]) - (int64_t)inter;
-        key = desc_key(u == 0 ? V(0) : V(1) * inter / (V)u);
-      }
-    }
-    if (k > 0) {
-      const uint64_t tk = __shfl_sync(0xffffffffu, bk, k - 1);
-      const int64_t tc = __shfl_sync(0xffffffffu, bc, k - 1);
-      if (!__any_sync(0xffffffffu, rank_less(key, col, tk, tc))) continue;
-    }
-    warp_sort32(key, col);
-    const uint64_t rk = __shfl_sync(0xffffffffu, key, 31 - lane);
-    const int64_t rc = __shfl_sync(0xffffffffu, col, 31 - lane);
+  uint64_t tk = kDiagKey;  // the k-th best so far: a candidate must rank before it
+  int64_t tc = INT64_MAX;
+  int nbuf = 0, diag = 0;
+  auto merge = [&](uint64_t ck, int64_t cc) {
+    warp_sort32(ck, cc);
+    const uint64_t rk = __shfl_sync(0xffffffffu, ck, 31 - lane);
+    const int64_t rc = __shfl_sync(0xffffffffu, cc, 31 - lane);
     if (rank_less(rk, rc, bk, bc)) {
       bk = rk;
       bc = rc;
     }
     for (int j = 16; j > 0; j >>= 1) warp_cx(bk, bc, j, true);
+    tk = __shfl_sync(0xffffffffu, bk, k - 1);
+    tc = __shfl_sync(0xffffffffu, bc, k - 1);
+  };
+  auto offer = [&](uint64_t key, int64_t col, bool ok) {
+    const bool cand = ok && rank_less(key, col, tk, tc);
+    const unsigned m = __ballot_sync(0xffffffffu, cand);
+    if (cand) {
+      const int p = nbuf + __popc(m & below);  // nbuf <= 31 before, so p <= 62
+      buf_k[p] = key;
+      buf_c[p] = col;
+    }
+    nbuf += __popc(m);
+    if (nbuf >= 32) {
+      __syncwarp();
+      const uint64_t ck = buf_k[lane];
+      const int64_t cc = buf_c[lane];
+      const int rest = nbuf - 32;
+      uint64_t rk = 0;
+      int64_t rc = 0;
+      if (lane < rest) {
+        rk = buf_k[32 + lane];
+        rc = buf_c[32 + lane];
+      }
+      __syncwarp();
+      if (lane < rest) {
+        buf_k[lane] = rk;
+        buf_c[lane] = rc;
+      }
+      nbuf = rest;
+      merge(ck, cc);
+    }
+  };
+  auto entry_key = [&](int64_t col, V inter) {
+    const int64_t u = li + ((int64_t)arp[col + 1] - (int64_t)arp[col]) - (int64_t)inter;
+    return desc_key(u == 0 ? V(0) : V(1) * inter / (V)u);
+  };
+  for (int64_t base = e0; base < e1; base += 64) {
+    const int64_t ea = base + lane, eb = ea + 32;
+    const bool ha = ea < e1, hb = eb < e1;
+    const int64_t ca = ha ? (int64_t)cci[ea] : -1, cb = hb ? (int64_t)cci[eb] : -1;
+    const V va = ha ? cval[ea] : V(0), vb = hb ? cval[eb] : V(0);
+    const bool oa = ha && ca != i, ob = hb && cb != i;
+    diag |= (ha && ca == i) || (hb && cb == i);
+    const uint64_t ka = oa ? entry_key(ca, va) : kDiagKey;
+    const uint64_t kb = ob ? entry_key(cb, vb) : kDiagKey;
+    offer(ka, ca, oa);
+    offer(kb, cb, ob);
+  }
+  if (nbuf > 0) {
+    __syncwarp();
+    const uint64_t ck = lane < nbuf ? buf_k[lane] : kDiagKey;
+    const int64_t cc = lane < nbuf ? buf_c[lane] : INT64_MAX;
+    merge(ck, cc);
   }
   diag = __any_sync(0xffffffffu, diag);
   if (lane < k) {
@@ -268,7 +320,7 @@ spops_status_t topk_t(Context* ctx, Matrix* A, int64_t top_k, Matrix** out) {
     SPOPS_TRY(orp.alloc((size_t)(n + 1) * 8));
     SPOPS_CUDA(cudaMemsetAsync(kept.p, 0, (size_t)(n + 1) * 8, st));
     if (n > 0) {
-      topk_select_kernel<I, V><<<grid_for(n * 32), 256, 0, st>>>(Cn->row.as<I>(), Cn->col.as<I>(), Cn->val.as<V>(),
+      topk_select_kernel<I, V><<<grid_for(n * 32), kSelectWarps * 32, 0, st>>>(Cn->row.as<I>(), Cn->col.as<I>(), Cn->val.as<V>(),
                                                                  A->row.as<I>(), n, k, skey.as<uint64_t>(),
                                                                  scol.as<I>(), kept.as<int64_t>());
       SPOPS_LAUNCH_CHECK();

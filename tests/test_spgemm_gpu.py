@@ -202,6 +202,34 @@ def test_topk_vs_oracle(cuda, orc, k):
     assert np.array_equal(v, ref["v"])
 
 
+@pytest.mark.parametrize("k", [5, 16, 32])
+def test_topk_ties_and_long_rows(cuda, orc, k):
+    """Groups of identical rows (every pair in a group has similarity 1, so
+    the ranking falls back to the column) next to rows that share single
+    columns with thousands of others (long rows of the counts product, many
+    candidate merges per row)."""
+    from sparseops_b200.spgemm import HashSpGEMMTopK
+    rng = np.random.default_rng(31)
+    rows = []
+    for g in range(40):  # 40 groups of 75 identical rows, 8 columns each
+        pat = np.sort(rng.choice(4000, 8, replace=False))
+        rows += [pat] * 75
+    hub = np.sort(rng.choice(4000, 3, replace=False))
+    for _ in range(500):  # rows holding one of three hub columns and 4 random ones
+        rows.append(np.unique(np.concatenate([hub[rng.integers(0, 3, 1)], rng.choice(4000, 4, replace=False)])))
+    order = rng.permutation(len(rows))
+    rows = [rows[o] for o in order]
+    n = len(rows)
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int64)
+    ci = np.concatenate(rows).astype(np.int64)
+    av = np.ones(len(ci))
+    ref = orc.spgemm_topk(rp, ci, 4000, k)
+    got_rp, got_ci, got_v = HashSpGEMMTopK(_csr(rp, ci, av, 4000), k).host()
+    assert np.array_equal(got_rp.astype(np.int64), ref["rp"])
+    assert np.array_equal(got_ci.astype(np.int64), ref["ci"])
+    assert np.array_equal(got_v, ref["v"])
+
+
 @pytest.mark.parametrize("so", [0, 1])
 def test_vlength_pipeline_golden(cuda, golden, orc, so):
     """The reference driver's flow (test/test_spgemm_hc_lsh.cpp:230-300):
