@@ -1042,6 +1042,8 @@ def csr_kernel_name(variant):
         return f"csr_win_kernel<double,{1024 // per_sm},{per_sm}>"
     if variant in (2, 3, 4):
         return "csr_warp_kernel<int,double,%d,%d>" % {2: (8, 4), 3: (4, 6), 4: (16, 2)}[variant]
+    if variant == 10:
+        return "csr_stage_kernel<int,double,2,6> + csr_tile_calibrate_kernel<double>"
     return "csr_tile_kernel<int,double,8,3,1> + csr_tile_calibrate_kernel<double>"
 
 

@@ -108,7 +108,7 @@ spops_status_t spops_synchronize(spops_context_t ctx);
  * when any bit was set; *flags (may be NULL) receives the bits. */
 spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
 /* Tuning switches by name; unknown keys are rejected with SPOPS_ERR_INVALID.
- *   "csr_variant" 0..9: CSR SpMV kernel.  Tiles of 32*K entries summed in
+ *   "csr_variant" 0..10: CSR SpMV kernel.  Tiles of 32*K entries summed in
  *   registers (K entries per lane / resident blocks per SM / next tile's
  *   loads issued early): 0 = 8/3/yes (default), 1 = 8/4/no, 5 = 4/4/no,
  *   6 = 8/5/no; they need the column and value arrays aligned to
@@ -119,7 +119,11 @@ spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
  *   they keep a copy of the values (refreshed after spops_csr_set_values or
  *   spops_matrix_touch), need cols and nnz below 2^31 (otherwise variant 2
  *   runs), and add a row's products in an order that can change from run to
- *   run at rounding level; variants 0-6 are bit-reproducible.
+ *   run at rounding level; variants 0-6 are bit-reproducible.  10: the tiles
+ *   of variant 0 with each warp's columns, values and flags brought into
+ *   shared memory by bulk copies two tiles ahead (measured slower than 0 on
+ *   the power-law matrix: the x gathers need the L1 capacity the slots take);
+ *   bit-reproducible, equal to variant 0 up to rounding. 
  *   "batch_band" 0 / 1: batched SpMV with one right-hand side stages each CSR
  *   segment's x window [r0 - H, r0 + rows + H) in shared memory, H in
  *   {16, 32, 64} from the matrix's band profile (0, the default: plain

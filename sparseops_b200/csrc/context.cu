@@ -318,7 +318,7 @@ spops_status_t spops_check_device(spops_context_t c, int32_t* flags) {
 spops_status_t spops_set_option(spops_context_t c, const char* key, int64_t value) {
   if (!c || !key) return fail(SPOPS_ERR_INVALID, "spops_set_option: null argument");
   if (!strcmp(key, "csr_variant")) {
-    if (value < 0 || value > 9) return fail(SPOPS_ERR_INVALID, "csr_variant must be 0..9");
+    if (value < 0 || value > 10) return fail(SPOPS_ERR_INVALID, "csr_variant must be 0..10");
     c->csr_variant = (int)value;
     return SPOPS_OK;
   }

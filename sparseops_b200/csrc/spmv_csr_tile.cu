@@ -34,6 +34,7 @@
 #include <functional>
 #include <vector>
 
+#include "bulk_copy.cuh"
 #include "csr_tile.cuh"
 #include "device_util.cuh"
 #include "spops_internal.h"
@@ -125,6 +126,190 @@ __global__ void __launch_bounds__(kTileBlock, kMinBlocks) csr_tile_kernel(
       tr = tile_row[t + nw];
     }
     tile_finish<I, V, K>(rp, n, nnz, t, lane, f, r0, p, y, alpha, beta, bz, carry_in, open_sum, open_row);
+  }
+}
+
+// ---- staged form (csr_variant 10): the matrix stream by bulk copies
+// Each warp owns a ring of S slots in shared memory; lane 0 fills a slot with
+// one tile's columns, values and row-start flags by three bulk copies
+// (cp.async.bulk, completing on the slot's mbarrier) S tiles ahead.  The
+// lanes read their runs from the slot, so the only per-entry loads that go
+// through the SM's L1 request port are the x gathers.  The gathers of the
+// next tile are issued before this tile's products are summed (its columns
+// are already in shared memory), so a warp keeps gathers in flight through
+// the cross-lane row sums.  The summation order is that of csr_tile_kernel
+// (results agree to rounding: the compiler may fuse a product into its sum in
+// one kernel and not in the other).  The partial last tile, if any, is read
+// with plain loads.
+template <typename I, typename V>
+struct alignas(16) StageSlot {
+  I col[256];
+  V val[256];
+  uint8_t flags[32];
+};
+
+template <typename I, typename V, int S>
+struct alignas(128) StageRing {
+  StageSlot<I, V> slot[S];
+  unsigned long long bar[S];
+};
+
+// A lane's 32-byte run from a slot, its two 16-byte halves read in an order
+// that spreads the 32 lanes over all banks (8 lanes per 128 bytes).
+__device__ __forceinline__ void slot_run32(const void* base, int lane, uint4& q0, uint4& q1) {
+  const uint4* p = reinterpret_cast<const uint4*>(base);
+  const int h = (lane >> 2) & 1;
+  const uint4 a = p[h], b = p[h ^ 1];
+  q0 = h ? b : a;
+  q1 = h ? a : b;
+}
+
+// A lane's 64-byte run, its four 16-byte quarters read rotated by
+// (lane >> 1) & 3 for the same reason.
+__device__ __forceinline__ void slot_run64(const void* base, int lane, uint4 (&q)[4]) {
+  const uint4* p = reinterpret_cast<const uint4*>(base);
+  const int r = (lane >> 1) & 3;
+  uint4 w0 = p[r], w1 = p[(r + 1) & 3], w2 = p[(r + 2) & 3], w3 = p[(r + 3) & 3];
+  if (r & 1) {  // rotate right by one
+    const uint4 t = w3;
+    w3 = w2;
+    w2 = w1;
+    w1 = w0;
+    w0 = t;
+  }
+  if (r & 2) {  // and by two
+    uint4 t = w0;
+    w0 = w2;
+    w2 = t;
+    t = w1;
+    w1 = w3;
+    w3 = t;
+  }
+  q[0] = w0;
+  q[1] = w1;
+  q[2] = w2;
+  q[3] = w3;
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void slot_read(const T* base, int lane, T (&out)[K]) {
+  static_assert(K * sizeof(T) == 32 || K * sizeof(T) == 64, "runs of 32 or 64 bytes");
+  if constexpr (K * sizeof(T) == 32) {
+    uint4 q[2];
+    slot_run32(base + lane * K, lane, q[0], q[1]);
+    memcpy(out, q, 32);
+  } else {
+    uint4 q[4];
+    slot_run64(base + lane * K, lane, q);
+    memcpy(out, q, 64);
+  }
+}
+
+constexpr int kStageWarps = 4;
+
+template <typename I, typename V, int S, int kMinBlocks>
+__global__ void __launch_bounds__(kStageWarps * 32, kMinBlocks) csr_stage_kernel(
+    const I* __restrict__ rp, int64_t n, int64_t nnz, const I* __restrict__ ci, const V* __restrict__ val,
+    const int64_t* __restrict__ tile_row, const uint8_t* __restrict__ flags_all, int64_t tiles,
+    const V* __restrict__ x, V* __restrict__ y, V alpha, V beta, bool bz, V* __restrict__ carry_in,
+    V* __restrict__ open_sum, int64_t* __restrict__ open_row, int* __restrict__ err) {
+  constexpr int K = 8;
+  constexpr uint32_t kColB = 32 * K * sizeof(I), kValB = 32 * K * sizeof(V), kTx = kColB + kValB + 32;
+  using Ring = StageRing<I, V, S>;
+  extern __shared__ __align__(128) unsigned char stage_smem[];
+  const int lane = threadIdx.x & 31;
+  Ring& R = reinterpret_cast<Ring*>(stage_smem)[threadIdx.x >> 5];
+  const int64_t nw = (int64_t)gridDim.x * kStageWarps;
+  int64_t t = blockIdx.x * (int64_t)kStageWarps + (threadIdx.x >> 5);
+  if (t >= tiles) return;
+  const int64_t full = nnz / (32 * K);  // tiles [0, full) come by bulk copies
+  const uint32_t bar0 = smem_u32(&R.bar[0]);
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) mbar_init(bar0 + 8 * s, 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  uint32_t pend = 0, phase = 0;  // per slot: a copy in flight; the parity its completion has
+  auto issue = [&](int64_t tt, int s) {
+    if (tt < full) {
+      pend |= 1u << s;
+      if (lane == 0) {
+        const uint32_t b = bar0 + 8 * s;
+        mbar_arrive_expect(b, kTx);
+        bulk_g2s(smem_u32(R.slot[s].col), ci + tt * (32 * K), kColB, b);
+        bulk_g2s(smem_u32(R.slot[s].val), val + tt * (32 * K), kValB, b);
+        bulk_g2s(smem_u32(R.slot[s].flags), flags_all + tt * 32, 32, b);
+      }
+    }
+  };
+  auto wait = [&](int s) {
+    const bool ok = mbar_wait_bounded(bar0 + 8 * s, (phase >> s) & 1u);
+    phase ^= 1u << s;
+    pend &= ~(1u << s);
+    return __all_sync(0xffffffffu, ok);
+  };
+  auto give_up = [&]() {  // a copy did not complete in time: flag it, let the others land, leave
+    if (lane == 0) atomicOr(err, 1);
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      if ((pend >> s) & 1u) mbar_wait_bounded(bar0 + 8 * s, (phase >> s) & 1u);
+  };
+#pragma unroll
+  for (int q = 0; q < S; ++q)
+    if (t + q * nw < tiles) issue(t + q * nw, q);
+  I c[K];
+  V xv[K], xn[K];
+  auto columns = [&](int64_t tt, int s) {
+    if (tt < full) {
+      slot_read<I, K>(R.slot[s].col, lane, c);
+    } else {
+      const int64_t el = tt * (32 * K) + (int64_t)lane * K;
+#pragma unroll
+      for (int b = 0; b < K; ++b) c[b] = el + b < nnz ? ci[el + b] : I(0);
+    }
+  };
+  int s = 0;
+  if (t < full && !wait(0)) return give_up();
+  columns(t, 0);
+#pragma unroll
+  for (int b = 0; b < K; ++b) xv[b] = ld_gather(x + c[b]);
+  while (true) {
+    const int64_t tn = t + nw;
+    const int sn = s + 1 == S ? 0 : s + 1;
+    const int64_t tr = tile_row[t];
+    V a[K];
+    uint32_t f;
+    if (t < full) {
+      slot_read<V, K>(R.slot[s].val, lane, a);
+      f = R.slot[s].flags[lane];
+    } else {
+      const int64_t el = t * (32 * K) + (int64_t)lane * K;
+#pragma unroll
+      for (int b = 0; b < K; ++b) a[b] = el + b < nnz ? val[el + b] : V(0);
+      f = flags_all[t * 32 + lane];
+    }
+    const bool more = tn < tiles;
+    if (more) {
+      if (tn < full && !wait(sn)) return give_up();
+      columns(tn, sn);
+#pragma unroll
+      for (int b = 0; b < K; ++b) xn[b] = ld_gather(x + c[b]);
+    }
+    __syncwarp();  // every lane is done with slot s
+    if (t + S * nw < tiles) {
+      if (lane == 0) fence_proxy_async_smem();
+      issue(t + S * nw, s);
+    }
+    V p[K];
+#pragma unroll
+    for (int b = 0; b < K; ++b) p[b] = a[b] * xv[b];
+    tile_finish<I, V, K>(rp, n, nnz, t, lane, f, tr, p, y, alpha, beta, bz, carry_in, open_sum, open_row);
+    if (!more) break;
+    t = tn;
+    s = sn;
+#pragma unroll
+    for (int b = 0; b < K; ++b) xv[b] = xn[b];
   }
 }
 
@@ -362,6 +547,42 @@ spops_status_t spmv_range(Context* ctx, Matrix* A, double alpha, const void* x, 
   return SPOPS_OK;
 }
 
+// The staged kernel over all tiles, then the calibration.
+template <typename I, typename V, int S, int kMinBlocks>
+spops_status_t spmv_stage_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
+  const CsrTiles& D = A->plan.tiles;
+  const bool bz = beta == 0.0;
+  const int64_t tiles = D.tiles;
+  if (tiles > 0) {
+    SPOPS_TRY(ctx->ensure_errword());
+    constexpr size_t smem = kStageWarps * sizeof(StageRing<I, V, S>);
+    static int blocks_per_sm = -1;  // per instantiation
+    if (blocks_per_sm < 0) {
+      SPOPS_CUDA(cudaFuncSetAttribute(csr_stage_kernel<I, V, S, kMinBlocks>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int bps = 0;
+      SPOPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, csr_stage_kernel<I, V, S, kMinBlocks>,
+                                                               kStageWarps * 32, smem));
+      blocks_per_sm = bps > 0 ? bps : 1;
+    }
+    int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
+    const int64_t need = (tiles + kStageWarps - 1) / kStageWarps;
+    if (grid > need) grid = need;
+    csr_stage_kernel<I, V, S, kMinBlocks><<<(unsigned)grid, kStageWarps * 32, smem, ctx->stream>>>(
+        A->row.as<I>(), A->rows, A->nnz, A->col.as<I>(), A->val.as<V>(), D.tile_row.as<int64_t>(),
+        D.flags.as<uint8_t>(), tiles, static_cast<const V*>(x), static_cast<V*>(y), (V)alpha, (V)beta, bz,
+        D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>(), ctx->errword.as<int>());
+    SPOPS_LAUNCH_CHECK();
+  }
+  if (tiles + D.nempty > 0) {
+    csr_tile_calibrate_kernel<V><<<grid_of(tiles + D.nempty), 256, 0, ctx->stream>>>(
+        0, tiles, D.carry_in.as<V>(), D.open_sum.as<V>(), D.open_row.as<int64_t>(), D.empty.as<int64_t>(), D.nempty,
+        static_cast<V*>(y), (V)alpha, (V)beta, bz);
+    SPOPS_LAUNCH_CHECK();
+  }
+  return SPOPS_OK;
+}
+
 template <typename I, typename V, int K, int kMinBlocks, bool kPipe>
 spops_status_t spmv_t(Context* ctx, Matrix* A, double alpha, const void* x, double beta, void* y) {
   return spmv_range<I, V, K, kMinBlocks, kPipe>(ctx, A, alpha, x, beta, y, 0, A->plan.tiles.tiles, true);
@@ -420,6 +641,7 @@ spops_status_t dispatch(Context* ctx, Matrix* A, int variant, double alpha, cons
     case 1: return spmv_t<I, V, 8, 4, false>(ctx, A, alpha, x, beta, y);
     case 5: return spmv_t<I, V, 4, 4, false>(ctx, A, alpha, x, beta, y);
     case 6: return spmv_t<I, V, 8, 5, false>(ctx, A, alpha, x, beta, y);
+    case 10: return spmv_stage_t<I, V, 2, 6>(ctx, A, alpha, x, beta, y);
     default: return spmv_t<I, V, 8, 3, true>(ctx, A, alpha, x, beta, y);
   }
 }

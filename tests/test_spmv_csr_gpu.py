@@ -201,7 +201,7 @@ def test_kernel_variants_identical(cuda, orc, dtype, itype):
     ctx = default_context()
     ys = []
     try:
-        for var in range(10):
+        for var in range(11):
             ctx.set_option("csr_variant", var)
             y, _ = _run(rp, ci, v, x, 0.8, 0.7, y0)
             ys.append(y)
@@ -215,6 +215,32 @@ def test_kernel_variants_identical(cuda, orc, dtype, itype):
                     y.astype(np.float64), yref, 0.7, y0.astype(np.float64), 0.8) <= tol, var
         if var in (3, 4):
             assert np.array_equal(y, ys[2]), var
+
+
+@pytest.mark.parametrize("nnz", [0, 100, 256, 512, 777, 256 * 600, 256 * 600 + 3])
+def test_staged_tile_counts(cuda, orc, nnz):
+    """The staged tile kernel (bulk copies into shared memory) on tile counts
+    around its edges: no full tile, exactly one or two tiles, a partial last
+    tile, more tiles than resident warps, with and without a partial tail."""
+    rng = np.random.default_rng(nnz + 3)
+    n, ncols = max(1, nnz // 7), 5000
+    rows = np.sort(rng.integers(0, n, nnz))
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, rows + 1, 1)
+    rp = np.cumsum(rp)
+    ci = np.concatenate([np.sort(rng.choice(ncols, int(L), replace=False)) for L in np.diff(rp)]
+                        + [np.zeros(0, np.int64)]).astype(np.int32)
+    rp = rp.astype(np.int32)
+    v = rng.standard_normal(nnz)
+    x = rng.uniform(-1, 1, ncols)
+    y0 = rng.uniform(-1, 1, n)
+    yref = orc.spmv_csr(rp.astype(np.int64), ci.astype(np.int64), v, x, 1.5, -0.5, y0)
+    ys = {}
+    for var in (0, 10):
+        ys[var], _ = _with_variant(var, lambda: _run(rp, ci, v, x, 1.5, -0.5, y0))
+        assert _err(orc, rp.astype(np.int64), ci.astype(np.int64), v, x, ys[var], yref, -0.5, y0, 1.5) <= TOL64, var
+    from sparseops_b200 import default_context
+    assert default_context().check_device() == 0  # no bounded wait ran out
 
 
 def _with_variant(var, fn):
