@@ -230,6 +230,36 @@ def test_topk_ties_and_long_rows(cuda, orc, k):
     assert np.array_equal(got_v, ref["v"])
 
 
+@pytest.mark.parametrize("k", [1, 16, 32])
+def test_topk_every_table_size(cuda, orc, k):
+    """Rows of every product count the top-k path bins by: short random rows
+    (tables of 256 and 1024 slots), rows of three 3000-row hub blocks (about
+    3000 products: one block's table of 16384 slots) and four rows that hold
+    all three hubs (more than 8192 products: tables in global memory)."""
+    from sparseops_b200.spgemm import HashSpGEMMTopK
+    rng = np.random.default_rng(37)
+    n, ncols = 12000, 60000
+    rows = [set(rng.choice(ncols - 3, int(rng.integers(1, 9)), replace=False).tolist()) for _ in range(n)]
+    for h in range(3):
+        for r in range(3000 * h, 3000 * (h + 1)):
+            rows[r].add(ncols - 3 + h)
+    for r in (9000, 9001, 11998, 11999):
+        rows[r].update({ncols - 3, ncols - 2, ncols - 1})
+    rows = [np.array(sorted(r), np.int64) for r in rows]
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int64)
+    ci = np.concatenate(rows)
+    ref = orc.spgemm_topk(rp, ci, ncols, k)
+    for itype, vtype in [(np.int64, np.float64), (np.int32, np.float32)]:
+        got = HashSpGEMMTopK(_csr(rp.astype(itype), ci.astype(itype), np.ones(len(ci), vtype), ncols), k).host()
+        if vtype == np.float32:
+            ref = orc.spgemm_topk(rp, ci, ncols, k, f32=True)
+        assert np.array_equal(got[0].astype(np.int64), ref["rp"])
+        assert np.array_equal(got[1].astype(np.int64), ref["ci"])
+        assert np.array_equal(got[2].astype(np.float64), ref["v"])
+    from sparseops_b200 import default_context
+    assert default_context().check_device() == 0
+
+
 @pytest.mark.parametrize("so", [0, 1])
 def test_vlength_pipeline_golden(cuda, golden, orc, so):
     """The reference driver's flow (test/test_spgemm_hc_lsh.cpp:230-300):
