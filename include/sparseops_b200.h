@@ -98,7 +98,10 @@ typedef struct {
 } spops_matrix_info_t;
 
 /* ------------------------------------------------------------ context */
-/* One context per (device, stream).  stream may be NULL (legacy default). */
+/* One context per (device, stream).  stream may be NULL (legacy default).
+ * Matrices, batches and pair sets made with a context use its stream, and
+ * their large arrays go back to its block cache when they are destroyed:
+ * destroy them before the context. */
 spops_status_t spops_create(spops_context_t* ctx, int device, void* stream);
 spops_status_t spops_destroy(spops_context_t ctx);
 spops_status_t spops_set_stream(spops_context_t ctx, void* stream);

@@ -426,9 +426,10 @@ spops_status_t read_t(Context* ctx, PoolBuf& dtext, int64_t len, const Header& H
     C->rows = H.rows;
     C->cols = H.cols;
     C->nnz = total;
-    spops_status_t s2 = C->row.alloc(n1 * sizeof(I));
-    if (s2 == SPOPS_OK) s2 = C->col.alloc(t1 * sizeof(I));
-    if (s2 == SPOPS_OK) s2 = C->val.alloc(t1 * sizeof(V));
+    // the result's arrays reuse blocks earlier results of this context released
+    spops_status_t s2 = C->row.alloc_cached(ctx, n1 * sizeof(I));
+    if (s2 == SPOPS_OK) s2 = C->col.alloc_cached(ctx, t1 * sizeof(I));
+    if (s2 == SPOPS_OK) s2 = C->val.alloc_cached(ctx, t1 * sizeof(V));
     if (s2 == SPOPS_OK) {
       csr_rowptr_kernel<I><<<grid_for((int64_t)n1), 256, 0, st>>>(scan.as<unsigned long long>(), (int64_t)n1,
                                                                  C->row.as<I>());
