@@ -408,6 +408,11 @@ spops_status_t hc_device_t(Context* ctx, Matrix* A, const int64_t* pi, const int
     if (herr) return fail(SPOPS_ERR_CUDA, "clustering: device task error %d", herr);
     ntask = (int64_t)hn[0];
     nlive = (int64_t)hn[1 + cur];
+    if (tr.on) {
+      char what[64];
+      std::snprintf(what, sizeof(what), "rounds to %lld: %lld live", (long long)rounds, (long long)nlive);
+      tr.mark(st, what);
+    }
   }
   if (tr.on) {
     char what[48];
