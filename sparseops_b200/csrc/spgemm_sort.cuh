@@ -24,7 +24,7 @@
 // (room for P columns), columns ascending, values [column x csz] with the
 // rows of the cluster interleaved -- the same layout the hash kernels write.
 //
-// Limits (the caller bins clusters accordingly): P <= 32*R (R <= 64), the cluster has
+// Limits (the caller bins clusters accordingly): P <= 32*R (R <= 16), the cluster has
 // at most kSortCols columns, and B's column count fits the key
 // (cols <= 2^(32 - tbits) - 1, tbits = log2(32*R)).
 #pragma once
@@ -83,64 +83,12 @@ __device__ __forceinline__ void bitonic_pass(uint32_t (&k)[R], int lane) {
   if constexpr (KK < 32 * R) bitonic_pass<R, KK * 2>(k, lane);
 }
 
-// The same network with the stage loop kept as a loop: one copy of the
-// compare-exchange code per in-lane partner distance (log2 R of them) and one
-// cross-lane copy, so that a large R does not outgrow the instruction cache.
-// Slot indices stay compile-time constants; only the stage sizes are read at
-// run time.
-template <int R, int JJ>
-__device__ __forceinline__ void bitonic_inlane(uint32_t (&k)[R], int lane, int kk) {
-  constexpr int N = 32 * R;
-  const bool lane_asc = (kk >= N) ? true : ((lane & (kk / R)) == 0);
-#pragma unroll
-  for (int s = 0; s < R; ++s) {
-    const int p = s ^ JJ;
-    if (p > s) {
-      const bool asc = kk < R ? (s & kk) == 0 : lane_asc;
-      const uint32_t a = k[s], b = k[p];
-      const uint32_t lo = min(a, b), hi = max(a, b);
-      k[s] = asc ? lo : hi;
-      k[p] = asc ? hi : lo;
-    }
-  }
-}
-
-template <int R>
-__device__ __forceinline__ void bitonic_cross(uint32_t (&k)[R], int lane, int kk, int jj) {
-  constexpr int N = 32 * R;
-  const int lm = jj / R;
-  const bool lower = (lane & lm) == 0;
-  const bool asc = (kk >= N) ? true : ((lane & (kk / R)) == 0);
-  const bool keep_min = lower == asc;
-#pragma unroll
-  for (int s = 0; s < R; ++s) {
-    const uint32_t o = __shfl_xor_sync(0xffffffffu, k[s], lm);
-    k[s] = keep_min ? min(k[s], o) : max(k[s], o);
-  }
-}
-
-template <int R, int JJ>
-__device__ __forceinline__ void bitonic_inlane_at(uint32_t (&k)[R], int lane, int kk, int jj) {
-  if constexpr (JJ >= 1) {
-    if (jj == JJ) bitonic_inlane<R, JJ>(k, lane, kk);
-    else bitonic_inlane_at<R, JJ / 2>(k, lane, kk, jj);
-  }
-}
-
+// One warp's bitonic sort of its 32*R keys, R <= 16 (larger sorts run on
+// several warps, sort_accum_multi_kernel).
 template <int R>
 __device__ __forceinline__ void warp_bitonic_sort(uint32_t (&k)[R], int lane) {
-  if constexpr (R < 32) {
-    bitonic_pass<R, 2>(k, lane);
-  } else {
-    constexpr int N = 32 * R;
-#pragma unroll 1
-    for (int kk = 2; kk <= N; kk <<= 1)
-#pragma unroll 1
-      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-        if (jj >= R) bitonic_cross<R>(k, lane, kk, jj);
-        else bitonic_inlane_at<R, R / 2>(k, lane, kk, jj);
-      }
-  }
+  static_assert(R >= 1 && R <= 16 && (R & (R - 1)) == 0, "R: a power of two up to 16");
+  bitonic_pass<R, 2>(k, lane);
 }
 
 template <typename I, typename V, int R>
