@@ -8,9 +8,11 @@
 //               134-141); empty rows keep UINT64_MAX.  One warp per row, the
 //               row's columns broadcast, each lane owning k/32 hash functions.
 //   records     bucket = band hash of the band's r = k/bands values
-//               (h = h*0x9e3779b97f4a7c15 + v, 277-283), per band a stable
-//               radix sort of (bucket -> row) over rows given in ascending
-//               order, i.e. the reference's (band, bucket, row) order.
+//               (h = h*0x9e3779b97f4a7c15 + v, 277-283); the bands go in
+//               batches (as many as 2^24 records hold), each batch one stable
+//               radix sort of ((band, bucket) -> row) over records given in
+//               (band, row) order, i.e. the reference's (band, bucket, row)
+//               order, with one host synchronisation per batch.
 //   pairs       each run of equal buckets (size >= 2) pairs every row with
 //               every later row, or -- when constrained and the run is longer
 //               than 256 -- with its next 16 rows (481-516); pairs (i < j)
@@ -56,28 +58,35 @@ __global__ void minhash_kernel(const I* __restrict__ rp, const I* __restrict__ c
   }
 }
 
-__global__ void band_hash_kernel(const uint64_t* __restrict__ sig, int64_t n, int k, int band, int r,
+// Bands [band0, band0 + nb): record q = b * n + i holds row i's hash in band
+// band0 + b.
+__global__ void band_hash_kernel(const uint64_t* __restrict__ sig, int64_t n, int k, int band0, int nb, int r,
                                  uint64_t* __restrict__ bucket, int32_t* __restrict__ rows) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t* s = sig + i * k + band * r;
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n * nb) return;
+  const int64_t b = q / n, i = q - b * n;
+  const uint64_t* s = sig + i * k + (band0 + b) * r;
   uint64_t h = 0;
   for (int t = 0; t < r; ++t) h = h * 0x9e3779b97f4a7c15ULL + s[t];
-  bucket[i] = h;
-  rows[i] = (int32_t)i;
+  bucket[q] = h;
+  rows[q] = (int32_t)i;
 }
 
-// Bucket value -> a small id: its slot in an open-addressing table of at
-// least 2n slots (equal values get equal slots, different values different
-// ones), so that the rows are grouped by a sort on log2(slots) + 1 bits
-// instead of 64.  The value ~0 (the table's empty mark) gets id mask + 1.
-__global__ void bucket_id_kernel(uint64_t* __restrict__ key, int64_t n, unsigned long long* __restrict__ tab,
-                                 uint64_t mask, int* __restrict__ err) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const unsigned long long h = key[i];
+// Bucket value -> a small id: its slot in its band's open-addressing table of
+// at least 2n slots (equal values get equal slots, different values different
+// ones), so that the rows are grouped by a sort on the band's index and
+// log2(slots) + 1 bits instead of 64.  The value ~0 (the table's empty mark)
+// gets id mask + 1.  The key becomes band << id_bits | id.
+__global__ void bucket_id_kernel(uint64_t* __restrict__ key, int64_t n, int nb, unsigned long long* __restrict__ tabs,
+                                 uint64_t mask, int id_bits, int* __restrict__ err) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n * nb) return;
+  const int64_t b = q / n;
+  unsigned long long* tab = tabs + b * (int64_t)(mask + 1);
+  const uint64_t hi = (uint64_t)b << id_bits;
+  const unsigned long long h = key[q];
   if (h == ~0ULL) {
-    key[i] = mask + 1;
+    key[q] = hi | (mask + 1);
     return;
   }
   unsigned long long x = h ^ (h >> 29);
@@ -87,7 +96,7 @@ __global__ void bucket_id_kernel(uint64_t* __restrict__ key, int64_t n, unsigned
   for (uint64_t probe = 0; probe <= mask; ++probe) {
     const unsigned long long old = atomicCAS(tab + slot, ~0ULL, h);
     if (old == ~0ULL || old == h) {
-      key[i] = slot;
+      key[q] = hi | slot;
       return;
     }
     slot = (slot + 1) & mask;
@@ -180,73 +189,85 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
   if (n > INT32_MAX) return fail(SPOPS_ERR_UNSUPPORTED, "LSH: more than 2^31 rows");
   const int r = k / bands;
   cudaStream_t st = ctx->stream;
-  const size_t nn = (size_t)n;
   Trace tr("lsh");
   ArenaScope scope(ctx);  // this call's temporaries come from the arena
+  // bands per batch: the records (band, row) of a batch stay below 2^24
+  // (about 80 bytes each of temporaries) unless one band alone has more
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>(bands, ((int64_t)1 << 24) / n));
+  const int64_t m = (int64_t)nb * n;  // records of a full batch
+  const size_t mm = (size_t)m;
+  uint64_t slots = 1;  // per band
+  while (slots < 2 * (uint64_t)n) slots <<= 1;
+  int id_bits = 1;  // ids are below slots + 1
+  while (id_bits < 64 && (uint64_t(1) << id_bits) <= slots) ++id_bits;
+  int band_bits = 0;
+  while ((1 << band_bits) < nb) ++band_bits;
+  const int key_bits = id_bits + band_bits;
   size_t cub_sort = 0, cub_scan = 0, cub_rle = 0;
   {
     uint64_t* kk = nullptr;
     int32_t* vv = nullptr;
     int64_t* cc = nullptr;
-    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort, kk, kk, vv, vv, (int64_t)n, 0, 64, st));
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, cc, cc, (int64_t)n, st));
-    SPOPS_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, cub_rle, kk, kk, cc, cc, (int64_t)n, st));
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort, kk, kk, vv, vv, m, 0, key_bits, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, cc, cc, m, st));
+    SPOPS_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, cub_rle, kk, kk, cc, cc, m, st));
     size_t inc = 0;
-    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, inc, cc, cc, (int64_t)n, st));
+    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, inc, cc, cc, m, st));
     cub_scan = std::max(cub_scan, inc);
   }
   const size_t cub_max = std::max({cub_sort, cub_scan, cub_rle});
-  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  uint64_t slots = 1;
-  while (slots < 2 * nn) slots <<= 1;
-  int id_bits = 1;  // ids are below slots + 1
-  while (id_bits < 64 && (uint64_t(1) << id_bits) <= slots) ++id_bits;
-  const size_t need = al(nn * 8) * 2 + al(nn * 4) * 2 + al(nn * 8) * 7 + cub_max + 512 + al(slots * 8) + 256;
-  SPOPS_TRY(ctx->scratch_reserve(need));
-  char* base = ctx->scratch.as<char>();
-  size_t o = 0;
-  auto take = [&](size_t b) { char* p = base + o; o += al(b); return p; };
-  uint64_t* key_in = reinterpret_cast<uint64_t*>(take(nn * 8));
-  uint64_t* key_out = reinterpret_cast<uint64_t*>(take(nn * 8));
-  int32_t* row_in = reinterpret_cast<int32_t*>(take(nn * 4));
-  int32_t* row_out = reinterpret_cast<int32_t*>(take(nn * 4));
-  int64_t* flag = reinterpret_cast<int64_t*>(take(nn * 8));
-  int64_t* gid = reinterpret_cast<int64_t*>(take(nn * 8));
-  uint64_t* ukeys = reinterpret_cast<uint64_t*>(take(nn * 8));
-  int64_t* run_len = reinterpret_cast<int64_t*>(take(nn * 8));
-  int64_t* run_off = reinterpret_cast<int64_t*>(take(nn * 8));
-  int64_t* cnt = reinterpret_cast<int64_t*>(take(nn * 8));
-  int64_t* off = reinterpret_cast<int64_t*>(take(nn * 8));
-  int64_t* nruns = reinterpret_cast<int64_t*>(take(8));
-  void* cub_tmp = take(cub_max);
-  unsigned long long* tab = reinterpret_cast<unsigned long long*>(take(slots * 8));
-  int* id_err = reinterpret_cast<int*>(take(8));
+  PoolBuf key_in(ctx), key_out(ctx), row_in(ctx), row_out(ctx), flag(ctx), gid(ctx), ukeys(ctx), run_len(ctx),
+      run_off(ctx), cnt(ctx), off(ctx), small(ctx), cub_tmp(ctx), tab(ctx);
+  SPOPS_TRY(key_in.alloc(mm * 8));
+  SPOPS_TRY(key_out.alloc(mm * 8));
+  SPOPS_TRY(row_in.alloc(mm * 4));
+  SPOPS_TRY(row_out.alloc(mm * 4));
+  SPOPS_TRY(flag.alloc(mm * 8));
+  SPOPS_TRY(gid.alloc(mm * 8));
+  SPOPS_TRY(ukeys.alloc(mm * 8));
+  SPOPS_TRY(run_len.alloc(mm * 8));
+  SPOPS_TRY(run_off.alloc(mm * 8));
+  SPOPS_TRY(cnt.alloc(mm * 8));
+  SPOPS_TRY(off.alloc(mm * 8));
+  SPOPS_TRY(small.alloc(64));  // the run count, the table error flag
+  SPOPS_TRY(cub_tmp.alloc(cub_max + 256));
+  SPOPS_TRY(tab.alloc((size_t)nb * slots * 8));
+  int64_t* nruns = small.as<int64_t>();
+  int* id_err = reinterpret_cast<int*>(small.as<char>() + 8);
   SPOPS_CUDA(cudaMemsetAsync(id_err, 0, 4, st));
 
   tr.mark(st, "setup");
   // pairs of every band, appended
   PoolBuf all(ctx);
   int64_t total = 0, cap = 0;
-  for (int band = 0; band < bands; ++band) {
-    band_hash_kernel<<<grid_for(n), 256, 0, st>>>(sig, n, k, band, r, key_in, row_in);
-    SPOPS_CUDA(cudaMemsetAsync(tab, 0xff, slots * 8, st));
-    bucket_id_kernel<<<grid_for(n), 256, 0, st>>>(key_in, n, tab, slots - 1, id_err);
+  for (int band0 = 0; band0 < bands; band0 += nb) {
+    const int nbb = std::min(nb, bands - band0);
+    const int64_t mb = (int64_t)nbb * n;
+    band_hash_kernel<<<grid_for(mb), 256, 0, st>>>(sig, n, k, band0, nbb, r, key_in.as<uint64_t>(),
+                                                   row_in.as<int32_t>());
+    SPOPS_CUDA(cudaMemsetAsync(tab.p, 0xff, (size_t)nbb * slots * 8, st));
+    bucket_id_kernel<<<grid_for(mb), 256, 0, st>>>(key_in.as<uint64_t>(), n, nbb, tab.as<unsigned long long>(),
+                                                   slots - 1, id_bits, id_err);
     SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_sort, key_in, key_out, row_in, row_out, n, 0, id_bits,
-                                               st));
-    run_flag_kernel<<<grid_for(n), 256, 0, st>>>(key_out, n, flag);
+    size_t sort_bytes = cub_max;
+    SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.p, sort_bytes, key_in.as<uint64_t>(), key_out.as<uint64_t>(),
+                                               row_in.as<int32_t>(), row_out.as<int32_t>(), mb, 0, key_bits, st));
+    run_flag_kernel<<<grid_for(mb), 256, 0, st>>>(key_out.as<uint64_t>(), mb, flag.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
-    size_t inc_bytes = cub_max;
-    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, inc_bytes, flag, gid, n, st));
-    SPOPS_CUDA(cub::DeviceRunLengthEncode::Encode(cub_tmp, cub_rle, key_out, ukeys, run_len, nruns, n, st));
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, run_len, run_off, n, st));
-    pair_count_kernel<<<grid_for(n), 256, 0, st>>>(gid, run_off, run_len, n, constrain, cnt);
+    size_t b1 = cub_max, b2 = cub_max, b3 = cub_max;
+    SPOPS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp.p, b1, flag.as<int64_t>(), gid.as<int64_t>(), mb, st));
+    SPOPS_CUDA(cub::DeviceRunLengthEncode::Encode(cub_tmp.p, b2, key_out.as<uint64_t>(), ukeys.as<uint64_t>(),
+                                                  run_len.as<int64_t>(), nruns, mb, st));
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp.p, b3, run_len.as<int64_t>(), run_off.as<int64_t>(), mb, st));
+    pair_count_kernel<<<grid_for(mb), 256, 0, st>>>(gid.as<int64_t>(), run_off.as<int64_t>(), run_len.as<int64_t>(),
+                                                    mb, constrain, cnt.as<int64_t>());
     SPOPS_LAUNCH_CHECK();
-    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_scan, cnt, off, n, st));
+    size_t b4 = cub_max;
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp.p, b4, cnt.as<int64_t>(), off.as<int64_t>(), mb, st));
     int64_t h[2];
     int herr = 0;
-    SPOPS_CUDA(cudaMemcpyAsync(&h[0], off + n - 1, 8, cudaMemcpyDeviceToHost, st));
-    SPOPS_CUDA(cudaMemcpyAsync(&h[1], cnt + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&h[0], off.as<int64_t>() + mb - 1, 8, cudaMemcpyDeviceToHost, st));
+    SPOPS_CUDA(cudaMemcpyAsync(&h[1], cnt.as<int64_t>() + mb - 1, 8, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaMemcpyAsync(&herr, id_err, 4, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
     if (herr) return fail(SPOPS_ERR_CUDA, "LSH: bucket table full");
@@ -260,7 +281,8 @@ spops_status_t lsh_pairs(Context* ctx, const uint64_t* sig, int64_t n, int k, in
       all.swap(bigger);
       cap = ncap;
     }
-    pair_emit_kernel<<<grid_for(n), 256, 0, st>>>(row_out, n, cnt, off, all.as<uint64_t>() + total);
+    pair_emit_kernel<<<grid_for(mb), 256, 0, st>>>(row_out.as<int32_t>(), mb, cnt.as<int64_t>(), off.as<int64_t>(),
+                                                   all.as<uint64_t>() + total);
     SPOPS_LAUNCH_CHECK();
     total += np;
   }

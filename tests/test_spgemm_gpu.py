@@ -85,6 +85,21 @@ def test_pipeline_vs_oracle(cuda, orc, n, ncomm):
     assert C.stats["flops"] == orc.spgemm_flop((arp, aci), (brp,))
 
 
+def test_lsh_band_batches(cuda, orc):
+    """More records than one batch of bands holds (2^24): 600,000 rows with 32
+    bands of 4 hashes go in two batches; pairs, order and scores as the
+    oracle's."""
+    from sparseops_b200.spgemm import lsh_candidate_pairs_vector, minhash_signatures_flat
+    n = 600000
+    arp, aci, av = synth.planted_communities(n, ncomm=n // 256, mean=12.0, seed=23)
+    A = _csr(arp, aci, av)
+    sig = minhash_signatures_flat(A, 128, 11)
+    pairs = lsh_candidate_pairs_vector(A, 128, 32, 11).host()
+    opi, opj, ops = orc.lsh_pairs(sig, 32, True)
+    assert len(opi) > 0
+    assert np.array_equal(pairs[0], opi) and np.array_equal(pairs[1], opj) and np.array_equal(pairs[2], ops)
+
+
 def test_int32_and_float32(cuda, orc):
     from sparseops_b200.spgemm import LeSpGEMM_lsh
     arp, aci, av = synth.planted_communities(8192, ncomm=32, mean=12.0, seed=19)
