@@ -294,7 +294,8 @@ def _graph_ms(fn, reps, ctx):
 
 def bench_laplacian(ctx, dev, peak, cpu_ref: bool, iters=2000):
     """The 512 x 512 five-point Laplacian (n = 262,144, diagonal 4, off-diagonals
-    -1; x uniform[-1,1], seed 0), FP64: CSR and DIA SpMV.  The whole working
+    -1; x uniform[-1,1], seed 0), FP64: CSR and DIA SpMV, and COO, S-ELL and
+    BSR with the reference's default parameters.  The whole working
     set (about 21 MB) is resident in the 126 MB L2, so the GB/s here are
     effective rates on the algorithmic bytes, not HBM traffic; iters
     back-to-back launches, and the same launches replayed from a CUDA graph
@@ -347,6 +348,25 @@ def bench_laplacian(ctx, dev, peak, cpu_ref: bool, iters=2000):
                   "GB/s": round(dbytes / dms / 1e6, 1), "csr_equivalent_GB/s": round(nbytes / dms / 1e6, 1),
                   "GFLOP/s": round(2 * nnz / dms / 1e6, 1), "rel_err": derr,
                   "kernel": "dia_staged_kernel (x window of each 256-row block in shared memory)"}
+    # the other formats the reference runs on this matrix (csr_to_coo,
+    # csr_to_sell with its default chunk, csr_to_bsr with its default blocks):
+    # GB/s on the CSR algorithmic bytes; BSR also on the bytes its blocks hold
+    from sparseops_b200 import SpOps_bsr, SpOps_coo, SpOps_sell, csr_to_bsr, csr_to_coo, csr_to_sell
+    for name, conv, run in (("coo", csr_to_coo, SpOps_coo), ("s_ell", csr_to_sell, SpOps_sell),
+                            ("bsr", csr_to_bsr, SpOps_bsr)):
+        M = conv(A)
+        yd3 = torch.zeros(n, dtype=torch.float64, device=dev)
+        run(1.0, M, xd, 0.0, yd3)
+        torch.cuda.synchronize()
+        fms = _ev_ms(lambda: run(1.0, M, xd, 0.0, yd3), iters, warm=20)
+        ferr = float((np.abs(yd3.cpu().numpy() - yref) / den).max())
+        out[name] = {"ms": round(fms, 5), "csr_equivalent_GB/s": round(nbytes / fms / 1e6, 1),
+                     "GFLOP/s": round(2 * nnz / fms / 1e6, 1), "rel_err": ferr}
+        if name == "bsr":
+            bb = M.nnzb * (M.blockDim_r * M.blockDim_c * 8 + 4) + 16 * n
+            out[name].update({"blocks": M.nnzb, "block": [M.blockDim_r, M.blockDim_c], "bytes": bb,
+                              "GB/s": round(bb / fms / 1e6, 1)})
+        del M
     # e2e through the C ABI host path
     xh = [torch.from_numpy(x).pin_memory() for _ in range(2)]
     yh = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(2)]
@@ -959,12 +979,22 @@ def run_reference(args):
 def bench_features(A, cpu_ref: bool, rp=None, ci=None):
     """Structure features and tile features (256 x 256 grid) of the power-law
     matrix on the device: median of 3 calls after a first call (which builds
-    the transpose that the column side of the tile features reads).  The CPU
+    the transpose that the column side of the tile features and, from then
+    on, the symmetry count read), and the structure features' first call on
+    a fresh handle over the same arrays (no transpose on it).  The CPU
     leg runs the oracle's restatement of the reference's tile counting on the
     first 1/16 of the rows, and the device on the same sample."""
     import torch
     from sparseops_b200 import CSR_Matrix, matrix_features, matrix_tile_features
     out = {}
+    # structure features on a fresh handle over the same arrays (no transpose
+    # on it yet: the symmetry count searches the stored keys)
+    F = CSR_Matrix(A.num_rows, A.num_cols, A.row_offset, A.col_index, A.values)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    matrix_features(F)
+    out["structure_first_call_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    del F
     t0 = time.perf_counter()
     matrix_tile_features(A)
     out["tile_first_call_ms"] = round((time.perf_counter() - t0) * 1e3, 2)

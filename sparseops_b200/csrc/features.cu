@@ -13,7 +13,10 @@
 //   counts -> min / max / mean / variance (deterministic cub reductions);
 //   P-ratio and Gini from the sorted counts (the P search is exact: the same
 //   double expressions as the reference, evaluated for every prefix);
-//   symmetry from the sorted (row, col) keys by binary search of each mirror.
+//   symmetry: with ascending rows and a transpose pattern already on the
+//   handle, column by column over it (a warp bisects row c of A for every
+//   entry of column c); otherwise from the sorted (row, col) keys, a
+//   bisection per mirror (rows that ascend need no sort).
 // The selector (spops_select_format) applies rules to the features or times
 // the candidate formats.
 #include <cub/cub.cuh>
@@ -276,6 +279,52 @@ __global__ void symm_kernel(const I* __restrict__ rp, const uint64_t* __restrict
   }
 }
 
+// The same counts for rows whose columns strictly ascend, taken column by
+// column: the entries (r, c) of column c are row c of A^T (trp, tri; perm
+// gives each one's position in A), and the mirror (c, r) of each can only be
+// in row c of A.  A warp takes row c and every lane bisects that same row of
+// A for its own r, so the warp's probes share the row's few cache lines
+// instead of every entry fetching its own from DRAM.  The warps stride over
+// the rows and add their counts once at the end.
+template <typename I, typename V>
+__global__ void __launch_bounds__(256) symm_by_column_kernel(const I* __restrict__ rp, const I* __restrict__ ci,
+                                                             const V* __restrict__ vals, const I* __restrict__ trp,
+                                                             const I* __restrict__ tri,
+                                                             const int64_t* __restrict__ perm, int64_t n,
+                                                             unsigned long long* __restrict__ pat,
+                                                             unsigned long long* __restrict__ same) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  unsigned long long hits = 0, eqs = 0;
+  for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
+    const int64_t s = (int64_t)rp[c], e = (int64_t)rp[c + 1];
+    const int64_t t1 = (int64_t)trp[c + 1];
+    for (int64_t t = (int64_t)trp[c] + lane; t < t1; t += 32) {
+      const int64_t r = (int64_t)tri[t];
+      if (r == c) continue;
+      int64_t lo = s, hi = e;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)ci[mid] < r) lo = mid + 1; else hi = mid;
+      }
+      if (lo < e && (int64_t)ci[lo] == r) {
+        ++hits;
+        const double a = (double)vals[perm[t]], b = (double)vals[lo];
+        if (signbit(a) == signbit(b) && rint(fabs(a) * 1e6) == rint(fabs(b) * 1e6)) ++eqs;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    hits += __shfl_down_sync(0xffffffffu, hits, o);
+    eqs += __shfl_down_sync(0xffffffffu, eqs, o);
+  }
+  if (lane == 0) {
+    if (hits) atomicAdd(pat, hits);
+    if (eqs) atomicAdd(same, eqs);
+  }
+}
+
 // flags[0] = 1 when some row's columns are not strictly ascending
 template <typename I>
 __global__ void rows_unsorted_kernel(const I* __restrict__ rp, const I* __restrict__ ci, int64_t n,
@@ -446,10 +495,6 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
   if (n == nc && nnz > 0) {
     if (n > (int64_t)0xffffffffLL) return fail(SPOPS_ERR_UNSUPPORTED, "features: more than 2^32 rows");
     PoolBuf k0(ctx), k1(ctx), v0(ctx), v1(ctx), cntb(ctx), tmp(ctx);
-    SPOPS_TRY(k0.alloc((size_t)nnz * 8));
-    SPOPS_TRY(k1.alloc((size_t)nnz * 8));
-    SPOPS_TRY(v0.alloc((size_t)nnz * sizeof(V)));
-    SPOPS_TRY(v1.alloc((size_t)nnz * sizeof(V)));
     SPOPS_TRY(cntb.alloc(32));
     SPOPS_CUDA(cudaMemsetAsync(cntb.p, 0, 32, st));
     // rows whose columns already ascend need no sort: the keys are in order
@@ -460,23 +505,40 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
     unsigned int h_unsorted = 0;
     SPOPS_CUDA(cudaMemcpyAsync(&h_unsorted, unsorted, 4, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
-    symm_keys_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n,
-                                                            (h_unsorted ? k0 : k1).as<uint64_t>(),
-                                                            (h_unsorted ? v0 : v1).as<V>());
-    SPOPS_LAUNCH_CHECK();
-    if (h_unsorted) {
-      int end_bit = 32;  // the row half of the key holds n - 1 at most
-      while (end_bit < 64 && ((uint64_t)(n - 1) >> (end_bit - 32)) != 0) ++end_bit;
-      size_t b = 0;
-      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
-                                                 v1.as<V>(), nnz, 0, end_bit, st));
-      SPOPS_TRY(tmp.alloc(b + 256));
-      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
-                                                 v1.as<V>(), nnz, 0, end_bit, st));
-    }
     unsigned long long* c2 = cntb.as<unsigned long long>();
-    symm_kernel<I, V><<<grid_of(nnz), 256, 0, st>>>(A->row.as<I>(), k1.as<uint64_t>(), v1.as<V>(), nnz, c2, c2 + 1);
-    SPOPS_LAUNCH_CHECK();
+    if (!h_unsorted && A->tr.ready) {
+      // column by column over the transpose pattern the handle already keeps
+      // (built by the tile features, A^T x or the adjoint).  It is not built
+      // for this count alone: building it costs more than the search it saves.
+      const int64_t blocks = std::min<int64_t>((n + 7) / 8, (int64_t)ctx->num_sms * 8);
+      symm_by_column_kernel<I, V><<<(unsigned)blocks, 256, 0, st>>>(
+          A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), A->tr.rp.as<I>(), A->tr.ri.as<I>(),
+          A->tr.perm.as<int64_t>(), n, c2, c2 + 1);
+      SPOPS_LAUNCH_CHECK();
+    } else {  // the (row, col) keys, sorted unless every row ascends
+      SPOPS_TRY(k1.alloc((size_t)nnz * 8));
+      SPOPS_TRY(v1.alloc((size_t)nnz * sizeof(V)));
+      if (h_unsorted) {
+        SPOPS_TRY(k0.alloc((size_t)nnz * 8));
+        SPOPS_TRY(v0.alloc((size_t)nnz * sizeof(V)));
+      }
+      symm_keys_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n,
+                                                              (h_unsorted ? k0 : k1).as<uint64_t>(),
+                                                              (h_unsorted ? v0 : v1).as<V>());
+      SPOPS_LAUNCH_CHECK();
+      if (h_unsorted) {
+        int end_bit = 32;  // the row half of the key holds n - 1 at most
+        while (end_bit < 64 && ((uint64_t)(n - 1) >> (end_bit - 32)) != 0) ++end_bit;
+        size_t b = 0;
+        SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
+                                                   v1.as<V>(), nnz, 0, end_bit, st));
+        SPOPS_TRY(tmp.alloc(b + 256));
+        SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
+                                                   v1.as<V>(), nnz, 0, end_bit, st));
+      }
+      symm_kernel<I, V><<<grid_of(nnz), 256, 0, st>>>(A->row.as<I>(), k1.as<uint64_t>(), v1.as<V>(), nnz, c2, c2 + 1);
+      SPOPS_LAUNCH_CHECK();
+    }
     unsigned long long hc[2] = {0, 0};
     SPOPS_CUDA(cudaMemcpyAsync(hc, c2, 16, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));

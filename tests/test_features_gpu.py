@@ -60,6 +60,62 @@ def test_features_vs_oracle(cuda, orc, case):
     _close(got, ref)
 
 
+def _partly_symmetric(n, seed):
+    """Random pattern where about half the off-diagonal entries have a mirror;
+    mirror values equal, equal to six decimals, of the other sign, or
+    different; a diagonal entry in some rows.  Rows sorted by column."""
+    rng = np.random.default_rng(seed)
+    m = 8 * n
+    r = rng.integers(0, n, m)
+    c = rng.integers(0, n, m)
+    v = rng.standard_normal(m)
+    mir = rng.random(m) < 0.5
+    kind = rng.integers(0, 4, m)
+    mv = np.where(kind == 0, v, np.where(kind == 1, v + 1e-9, np.where(kind == 2, -v, v + 0.5)))
+    d = rng.integers(0, n, n // 3)
+    R = np.concatenate([r, c[mir], d])
+    Cc = np.concatenate([c, r[mir], d])
+    V = np.concatenate([v, mv[mir], rng.standard_normal(len(d))])
+    key = R.astype(np.int64) * n + Cc
+    key, first = np.unique(key, return_index=True)  # one entry per (row, col)
+    R, Cc, V = key // n, key % n, V[first]
+    rp = np.concatenate([[0], np.cumsum(np.bincount(R, minlength=n))]).astype(np.int32)
+    return rp, Cc.astype(np.int32), V
+
+
+def test_symmetry_both_paths(cuda, orc):
+    """pattern_symm and value_symm by each of the three counts: ascending rows
+    on a fresh handle (the keys as stored, no sort), the same rows shuffled
+    (the keys sorted first), and ascending rows once the tile features have
+    left a transpose pattern on the handle (column by column over it).  All
+    three give the oracle's values exactly."""
+    import torch
+    from sparseops_b200 import matrix_features, matrix_tile_features
+    from sparseops_b200._lib import FEATURE_NAMES
+    n = 6000
+    rp, ci, v = _partly_symmetric(n, seed=21)
+    rng = np.random.default_rng(22)
+    ci_u, v_u = ci.copy(), v.copy()
+    for r in range(n):  # shuffle every row's entries: the unsorted path
+        s, e = rp[r], rp[r + 1]
+        p = s + rng.permutation(e - s)
+        ci_u[s:e], v_u[s:e] = ci[p], v[p]
+    assert any(np.any(np.diff(ci_u[rp[r]:rp[r + 1]]) < 0) for r in range(n))
+    iP, iV = FEATURE_NAMES.index("pattern_symm"), FEATURE_NAMES.index("value_symm")
+    A = _csr(rp, ci, v, n)
+    got_s = _vec(matrix_features(A))
+    got_u = _vec(matrix_features(_csr(rp, ci_u, v_u, n)))
+    matrix_tile_features(A, 256)  # builds and keeps the transpose on the handle
+    torch.cuda.synchronize()
+    got_c = _vec(matrix_features(A))
+    ref = orc.features(rp.astype(np.int64), ci.astype(np.int64), v, n)
+    assert 0.2 < ref[iP] < 0.9 and 0.0 < ref[iV] < ref[iP]
+    for got in (got_s, got_u, got_c):
+        assert got[iP] == ref[iP] and got[iV] == ref[iV], (got[iP], got[iV], ref[iP], ref[iV])
+    _close(got_s, ref)
+    _close(got_c, ref)
+
+
 def test_select_rules(cuda):
     from sparseops_b200 import select_format
     rp, ci, v = synth.laplacian_2d(200)
