@@ -988,7 +988,7 @@ def bench_features(A, cpu_ref: bool, rp=None, ci=None):
     from sparseops_b200 import CSR_Matrix, matrix_features, matrix_tile_features
     out = {}
     # structure features on a fresh handle over the same arrays (no transpose
-    # on it yet: the symmetry count searches the stored keys)
+    # on it yet: the symmetry count bisects the CSR's own rows)
     F = CSR_Matrix(A.num_rows, A.num_cols, A.row_offset, A.col_index, A.values)
     torch.cuda.synchronize()
     t0 = time.perf_counter()

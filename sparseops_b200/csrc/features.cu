@@ -13,10 +13,10 @@
 //   counts -> min / max / mean / variance (deterministic cub reductions);
 //   P-ratio and Gini from the sorted counts (the P search is exact: the same
 //   double expressions as the reference, evaluated for every prefix);
-//   symmetry: with ascending rows and a transpose pattern already on the
-//   handle, column by column over it (a warp bisects row c of A for every
-//   entry of column c); otherwise from the sorted (row, col) keys, a
-//   bisection per mirror (rows that ascend need no sort).
+//   symmetry by a bisection per mirror: with ascending rows, column by
+//   column over a transpose pattern the handle already holds (a warp bisects
+//   row c of A for every entry of column c), else row by row on the CSR's
+//   own arrays; rows in any other order through sorted (row, col) keys.
 // The selector (spops_select_format) applies rules to the features or times
 // the candidate formats.
 #include <cub/cub.cuh>
@@ -325,6 +325,47 @@ __global__ void __launch_bounds__(256) symm_by_column_kernel(const I* __restrict
   }
 }
 
+// The same counts for rows whose columns strictly ascend, with no transpose
+// and no copy: a warp takes row r, each lane an entry (r, c), and bisects
+// row c of the CSR's own column array for r (4-byte probes, nothing to
+// allocate).  The warps stride over the rows and add their counts at the end.
+template <typename I, typename V>
+__global__ void __launch_bounds__(256) symm_by_row_kernel(const I* __restrict__ rp, const I* __restrict__ ci,
+                                                          const V* __restrict__ vals, int64_t n,
+                                                          unsigned long long* __restrict__ pat,
+                                                          unsigned long long* __restrict__ same) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  unsigned long long hits = 0, eqs = 0;
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+    const int64_t k1 = (int64_t)rp[r + 1];
+    for (int64_t k = (int64_t)rp[r] + lane; k < k1; k += 32) {
+      const int64_t c = (int64_t)ci[k];
+      if (c == r) continue;
+      const int64_t end = (int64_t)rp[c + 1];
+      int64_t lo = (int64_t)rp[c], hi = end;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)ci[mid] < r) lo = mid + 1; else hi = mid;
+      }
+      if (lo < end && (int64_t)ci[lo] == r) {
+        ++hits;
+        const double a = (double)vals[k], b = (double)vals[lo];
+        if (signbit(a) == signbit(b) && rint(fabs(a) * 1e6) == rint(fabs(b) * 1e6)) ++eqs;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    hits += __shfl_down_sync(0xffffffffu, hits, o);
+    eqs += __shfl_down_sync(0xffffffffu, eqs, o);
+  }
+  if (lane == 0) {
+    if (hits) atomicAdd(pat, hits);
+    if (eqs) atomicAdd(same, eqs);
+  }
+}
+
 // flags[0] = 1 when some row's columns are not strictly ascending
 template <typename I>
 __global__ void rows_unsorted_kernel(const I* __restrict__ rp, const I* __restrict__ ci, int64_t n,
@@ -506,36 +547,35 @@ spops_status_t features_t(Context* ctx, Matrix* A, spops_features_t* f) {
     SPOPS_CUDA(cudaMemcpyAsync(&h_unsorted, unsorted, 4, cudaMemcpyDeviceToHost, st));
     SPOPS_CUDA(cudaStreamSynchronize(st));
     unsigned long long* c2 = cntb.as<unsigned long long>();
+    const int64_t sblocks = std::min<int64_t>((n + 7) / 8, (int64_t)ctx->num_sms * 8);
     if (!h_unsorted && A->tr.ready) {
       // column by column over the transpose pattern the handle already keeps
       // (built by the tile features, A^T x or the adjoint).  It is not built
       // for this count alone: building it costs more than the search it saves.
-      const int64_t blocks = std::min<int64_t>((n + 7) / 8, (int64_t)ctx->num_sms * 8);
-      symm_by_column_kernel<I, V><<<(unsigned)blocks, 256, 0, st>>>(
+      symm_by_column_kernel<I, V><<<(unsigned)sblocks, 256, 0, st>>>(
           A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), A->tr.rp.as<I>(), A->tr.ri.as<I>(),
           A->tr.perm.as<int64_t>(), n, c2, c2 + 1);
       SPOPS_LAUNCH_CHECK();
-    } else {  // the (row, col) keys, sorted unless every row ascends
-      SPOPS_TRY(k1.alloc((size_t)nnz * 8));
-      SPOPS_TRY(v1.alloc((size_t)nnz * sizeof(V)));
-      if (h_unsorted) {
-        SPOPS_TRY(k0.alloc((size_t)nnz * 8));
-        SPOPS_TRY(v0.alloc((size_t)nnz * sizeof(V)));
-      }
-      symm_keys_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n,
-                                                              (h_unsorted ? k0 : k1).as<uint64_t>(),
-                                                              (h_unsorted ? v0 : v1).as<V>());
+    } else if (!h_unsorted) {  // row by row on the CSR arrays themselves
+      symm_by_row_kernel<I, V><<<(unsigned)sblocks, 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(),
+                                                                   n, c2, c2 + 1);
       SPOPS_LAUNCH_CHECK();
-      if (h_unsorted) {
-        int end_bit = 32;  // the row half of the key holds n - 1 at most
-        while (end_bit < 64 && ((uint64_t)(n - 1) >> (end_bit - 32)) != 0) ++end_bit;
-        size_t b = 0;
-        SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
-                                                   v1.as<V>(), nnz, 0, end_bit, st));
-        SPOPS_TRY(tmp.alloc(b + 256));
-        SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
-                                                   v1.as<V>(), nnz, 0, end_bit, st));
-      }
+    } else {  // the (row, col) keys sorted, then a bisection per mirror
+      SPOPS_TRY(k0.alloc((size_t)nnz * 8));
+      SPOPS_TRY(k1.alloc((size_t)nnz * 8));
+      SPOPS_TRY(v0.alloc((size_t)nnz * sizeof(V)));
+      SPOPS_TRY(v1.alloc((size_t)nnz * sizeof(V)));
+      symm_keys_kernel<I, V><<<grid_of(n * 32), 256, 0, st>>>(A->row.as<I>(), A->col.as<I>(), A->val.as<V>(), n,
+                                                              k0.as<uint64_t>(), v0.as<V>());
+      SPOPS_LAUNCH_CHECK();
+      int end_bit = 32;  // the row half of the key holds n - 1 at most
+      while (end_bit < 64 && ((uint64_t)(n - 1) >> (end_bit - 32)) != 0) ++end_bit;
+      size_t b = 0;
+      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
+                                                 v1.as<V>(), nnz, 0, end_bit, st));
+      SPOPS_TRY(tmp.alloc(b + 256));
+      SPOPS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, k0.as<uint64_t>(), k1.as<uint64_t>(), v0.as<V>(),
+                                                 v1.as<V>(), nnz, 0, end_bit, st));
       symm_kernel<I, V><<<grid_of(nnz), 256, 0, st>>>(A->row.as<I>(), k1.as<uint64_t>(), v1.as<V>(), nnz, c2, c2 + 1);
       SPOPS_LAUNCH_CHECK();
     }

@@ -85,10 +85,10 @@ def _partly_symmetric(n, seed):
 
 def test_symmetry_both_paths(cuda, orc):
     """pattern_symm and value_symm by each of the three counts: ascending rows
-    on a fresh handle (the keys as stored, no sort), the same rows shuffled
-    (the keys sorted first), and ascending rows once the tile features have
-    left a transpose pattern on the handle (column by column over it).  All
-    three give the oracle's values exactly."""
+    on a fresh handle (row by row on the CSR's own arrays), the same rows
+    shuffled (sorted (row, col) keys), and ascending rows once the tile
+    features have left a transpose pattern on the handle (column by column
+    over it).  All three give the oracle's values exactly."""
     import torch
     from sparseops_b200 import matrix_features, matrix_tile_features
     from sparseops_b200._lib import FEATURE_NAMES
