@@ -674,6 +674,9 @@ def bench_fwd_bwd(ctx, dev, n=1 << 20, peak=None, cpu_ref=False):
 
         ctx.follow_torch()
         t_ours = _ev_ms(ours, 20)
+        ctx.set_option("adjoint_bands", 1)  # A^T g in one pass over all source rows, for comparison
+        t_one = _ev_ms(ours, 20)
+        ctx.set_option("adjoint_bands", 0)
         t_plain = _ev_ms(plain, 5)
         torch.cuda.synchronize()
         # the user-facing torch.autograd.Function, forward + backward
@@ -696,7 +699,7 @@ def bench_fwd_bwd(ctx, dev, n=1 << 20, peak=None, cpu_ref=False):
         fwd = 4 * (n + 1) + (4 + vs) * nnz + 2 * vs * n
         sddmm = 4 * (n + 1) + 4 * nnz + 2 * vs * n + vs * nnz
         alg = 2 * fwd + sddmm
-        res = {"ours_ms": round(t_ours, 4), "plain_ms": round(t_plain, 4),
+        res = {"ours_ms": round(t_ours, 4), "ours_one_band_ms": round(t_one, 4), "plain_ms": round(t_plain, 4),
                "speedup_vs_plain": round(t_plain / t_ours, 2), "autograd_ms": round(t_auto, 4),
                "normwise_rel_err": {"y": rel(y, py), "grad_x": rel(gx, pgx), "grad_v": rel(gv, keep["gv"])},
                "algorithmic_bytes": alg, "value_refresh_bytes": (2 * vs + 4) * nnz}

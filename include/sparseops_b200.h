@@ -139,7 +139,17 @@ spops_status_t spops_check_device(spops_context_t ctx, int32_t* flags);
  *   windows are listed longest chunk first, so that warps running at the
  *   same time hold rows of like length (1, the default), or in chunk order
  *   (0).  The per-row results do not depend on it.  Read when the matrix is
- *   converted or uploaded. */
+ *   converted or uploaded.
+ *   "adjoint_bands" 0 .. 8: spops_spmv_t right after a value change reads A's
+ *   values through the transpose's permutation; it can do so in bands of
+ *   source rows of about equal entry counts, each band's slice of the values
+ *   small enough to stay in L2 while its gathers run, the bands adding into
+ *   y in band order.  0 (the default): as many bands as keep each slice
+ *   within 64 MB once the values pass 96 MB, else one pass; 1: one pass;
+ *   2 .. 8: that many bands.  The bands' row offsets, columns and positions
+ *   are built once per pattern and count (about 12 bytes per entry with
+ *   int32 indices) and kept with the matrix.  Summation order changes with
+ *   the count (rounding level); every count is bit-reproducible. */
 spops_status_t spops_set_option(spops_context_t ctx, const char* key, int64_t value);
 const char* spops_status_string(spops_status_t s);
 const char* spops_last_error(void);

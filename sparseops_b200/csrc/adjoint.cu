@@ -14,6 +14,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <vector>
 
 #include "csr_tile.cuh"
 #include "device_util.cuh"
@@ -172,6 +173,167 @@ spops_status_t build_transpose_t(Context* ctx, Matrix* A) {
   return SPOPS_OK;
 }
 
+// ---- source-row bands of the transpose.  A row of A^T lists its source rows
+// in ascending order (the transpose's sort is stable), so the entries of
+// each band of source rows are one subrange of it, found by bisection.
+struct BandStarts {
+  int64_t v[TransposeData::kMaxBands + 1];  // band b: source rows [v[b], v[b + 1])
+};
+struct BandPtrs {
+  const void* rp[TransposeData::kMaxBands];
+  void* ri[TransposeData::kMaxBands];
+  int64_t* perm[TransposeData::kMaxBands];
+};
+
+template <typename I>
+__device__ __forceinline__ int64_t first_source_at(const I* __restrict__ tri, int64_t s, int64_t e, int64_t r0) {
+  while (s < e) {
+    const int64_t m = (s + e) >> 1;
+    if ((int64_t)tri[m] < r0) s = m + 1; else e = m;
+  }
+  return s;
+}
+
+// cnt[b * (nc + 1) + c] = entries of row c of A^T in band b
+template <typename I>
+__global__ void band_count_kernel(const I* __restrict__ trp, const I* __restrict__ tri, int64_t nc, int nb,
+                                  BandStarts bs, unsigned long long* __restrict__ cnt) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int64_t e = (int64_t)trp[c + 1];
+  int64_t p = (int64_t)trp[c];
+  for (int b = 0; b < nb; ++b) {
+    const int64_t q = b + 1 < nb ? first_source_at(tri, p, e, bs.v[b + 1]) : e;
+    cnt[(int64_t)b * (nc + 1) + c] = (unsigned long long)(q - p);
+    p = q;
+  }
+}
+
+// A warp per row c of A^T copies each band's subrange of the row (source
+// rows and positions in A) to that band's arrays at the band's row offset.
+template <typename I>
+__global__ void band_fill_kernel(const I* __restrict__ trp, const I* __restrict__ tri,
+                                 const int64_t* __restrict__ perm, int64_t nc, int nb, BandStarts bs, BandPtrs P) {
+  const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= nc) return;
+  const int64_t e = (int64_t)trp[c + 1];
+  int64_t p = (int64_t)trp[c];
+  for (int b = 0; b < nb; ++b) {
+    const int64_t q = b + 1 < nb ? first_source_at(tri, p, e, bs.v[b + 1]) : e;
+    const int64_t d = (int64_t)static_cast<const I*>(P.rp[b])[c] - p;
+    I* ri = static_cast<I*>(P.ri[b]);
+    for (int64_t k = p + lane; k < q; k += 32) {
+      ri[d + k] = tri[k];
+      P.perm[b][d + k] = perm[k];
+    }
+    p = q;
+  }
+}
+
+void release_bands(TransposeData& T) {
+  for (int b = 0; b < T.nbands; ++b) {
+    if (T.bview[b]) {
+      T.bview[b]->release_all();
+      delete T.bview[b];
+      T.bview[b] = nullptr;
+    }
+    T.brp[b].release();
+    T.bri[b].release();
+    T.bperm[b].release();
+  }
+  T.nbands = 0;
+}
+
+// The bands of A's transpose (built after the transpose, once per pattern
+// and band count): row ranges of A with about nnz / nb entries each.
+template <typename I, typename V>
+spops_status_t build_bands_t(Context* ctx, Matrix* A, int nb) {
+  TransposeData& T = A->tr;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = A->rows, nc = A->cols, nnz = A->nnz;
+  release_bands(T);
+  std::vector<I> rp_h((size_t)n + 1);
+  SPOPS_CUDA(cudaMemcpyAsync(rp_h.data(), A->row.p, ((size_t)n + 1) * sizeof(I), cudaMemcpyDeviceToHost, st));
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  BandStarts bs{};
+  for (int b = 1; b < nb; ++b) {  // first row starting at or after entry b * nnz / nb
+    const I target = (I)(nnz / nb * b + (nnz % nb) * b / nb);
+    bs.v[b] = std::max<int64_t>(bs.v[b - 1], std::lower_bound(rp_h.begin(), rp_h.end(), target) - rp_h.begin());
+    if (bs.v[b] > n) bs.v[b] = n;
+  }
+  bs.v[nb] = n;
+  const size_t stride = (size_t)nc + 1;
+  PoolBuf cnt(ctx), scan(ctx), tmp(ctx);
+  SPOPS_TRY(cnt.alloc((size_t)nb * stride * 8));
+  SPOPS_TRY(scan.alloc(stride * 8));
+  size_t cub_b = 0;
+  SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_b, (unsigned long long*)nullptr,
+                                           (unsigned long long*)nullptr, (int64_t)stride, st));
+  SPOPS_TRY(tmp.alloc(cub_b + 256));
+  SPOPS_CUDA(cudaMemsetAsync(cnt.p, 0, (size_t)nb * stride * 8, st));
+  band_count_kernel<I><<<grid_for(nc), 256, 0, st>>>(T.rp.as<I>(), T.ri.as<I>(), nc, nb, bs,
+                                                      cnt.as<unsigned long long>());
+  SPOPS_LAUNCH_CHECK();
+  unsigned long long nnzb[TransposeData::kMaxBands] = {};
+  T.nbands = nb;  // from here on release_bands frees what was allocated
+  for (int b = 0; b < nb; ++b) {
+    SPOPS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, cub_b, cnt.as<unsigned long long>() + b * stride,
+                                             scan.as<unsigned long long>(), (int64_t)stride, st));
+    SPOPS_TRY(T.brp[b].alloc(stride * sizeof(I)));
+    cast_kernel<I><<<grid_for((int64_t)stride), 256, 0, st>>>(scan.as<unsigned long long>(), (int64_t)stride,
+                                                               T.brp[b].as<I>());
+    SPOPS_LAUNCH_CHECK();
+    SPOPS_CUDA(cudaMemcpyAsync(&nnzb[b], scan.as<unsigned long long>() + nc, 8, cudaMemcpyDeviceToHost, st));
+  }
+  SPOPS_CUDA(cudaStreamSynchronize(st));
+  BandPtrs P{};
+  for (int b = 0; b < nb; ++b) {
+    const size_t m = (size_t)(nnzb[b] > 0 ? nnzb[b] : 1);
+    SPOPS_TRY(T.bri[b].alloc(m * sizeof(I)));
+    SPOPS_TRY(T.bperm[b].alloc(m * 8));
+    P.rp[b] = T.brp[b].p;
+    P.ri[b] = T.bri[b].p;
+    P.perm[b] = T.bperm[b].as<int64_t>();
+  }
+  if (nc > 0) {
+    band_fill_kernel<I><<<grid_for(nc * 32), 256, 0, st>>>(T.rp.as<I>(), T.ri.as<I>(), T.perm.as<int64_t>(), nc, nb,
+                                                           bs, P);
+    SPOPS_LAUNCH_CHECK();
+  }
+  for (int b = 0; b < nb; ++b) {  // CSR handles of the bands (values read through perm, never from val)
+    if (nnzb[b] == 0) continue;    // an empty band: no handle, no launch
+    Matrix* V_ = new Matrix();
+    V_->ctx = ctx;
+    V_->format = SPOPS_FMT_CSR;
+    V_->itype = A->itype;
+    V_->vtype = A->vtype;
+    V_->rows = nc;
+    V_->cols = n;
+    V_->nnz = (int64_t)nnzb[b];
+    V_->row.borrow(T.brp[b].p, T.brp[b].bytes);
+    V_->col.borrow(T.bri[b].p, T.bri[b].bytes);
+    V_->val.borrow(T.val.p, (size_t)(nnzb[b] > 0 ? nnzb[b] : 1) * sizeof(V));
+    T.bview[b] = V_;
+    const spops_status_t s = csr_analyse(ctx, V_);
+    if (s != SPOPS_OK) {
+      release_bands(T);
+      return s;
+    }
+  }
+  return SPOPS_OK;
+}
+
+// bands for A^T x through perm: the context's setting, or as many as keep
+// each band's values within 64 MB once A's values pass 96 MB
+int adjoint_band_count(const Context* ctx, const Matrix* A) {
+  if (ctx->adjoint_bands > 0) return ctx->adjoint_bands;
+  const int64_t bytes = A->nnz * (int64_t)A->vsize();
+  if (bytes <= ((int64_t)96 << 20)) return 1;
+  const int64_t nb = (bytes + ((int64_t)64 << 20) - 1) / ((int64_t)64 << 20);
+  return (int)std::min<int64_t>(nb, TransposeData::kMaxBands);
+}
+
 // The same SDDMM over the SpMV's tile plan (32 lanes x 8 consecutive
 // entries per tile): each lane loads its 8 columns with one vector load and
 // issues their 8 x gathers together, finds the row of its first entry from
@@ -285,6 +447,7 @@ spops_status_t sddmm_t(Context* ctx, Matrix* A, double alpha, const void* g, con
 }  // namespace
 
 void TransposeData::release() {
+  release_bands(*this);
   rp.release();
   ri.release();
   perm.release();
@@ -309,6 +472,20 @@ spops_status_t csr_spmv_transpose(Context* ctx, Matrix* A, double alpha, const v
     // values through the permutation inside the SpMV; the reordered copy is
     // refreshed only when something asks for it (csr_transpose_view)
     if (!V_->plan.ready) SPOPS_TRY(csr_analyse(ctx, V_));
+    const int nb = adjoint_band_count(ctx, A);
+    if (nb > 1) {
+      // one band of source rows at a time: its slice of A's values stays in
+      // L2 while the band's gathers run; the bands add into y in band order
+      if (A->tr.nbands != nb) SPOPS_TRY(SPOPS_DISPATCH2(A, build_bands_t, ctx, A, nb));
+      bool first = true;  // the first band run applies beta, the others add
+      for (int b = 0; b < nb; ++b) {
+        if (!A->tr.bview[b]) continue;
+        SPOPS_TRY(csr_tile_spmv_indirect(ctx, A->tr.bview[b], A->tr.bperm[b].as<int64_t>(), A->val.p, alpha, x,
+                                         first ? beta : 1.0, y));
+        first = false;
+      }
+      if (!first) return SPOPS_OK;
+    }
     return csr_tile_spmv_indirect(ctx, V_, A->tr.perm.as<int64_t>(), A->val.p, alpha, x, beta, y);
   }
   if (!A->tr.values_fresh) SPOPS_TRY(SPOPS_DISPATCH2(A, refresh_values_t, ctx, A));

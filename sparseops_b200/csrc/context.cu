@@ -332,6 +332,12 @@ spops_status_t spops_set_option(spops_context_t c, const char* key, int64_t valu
     c->sell_tails = (int)value;
     return SPOPS_OK;
   }
+  if (!strcmp(key, "adjoint_bands")) {
+    if (value < 0 || value > TransposeData::kMaxBands)
+      return fail(SPOPS_ERR_INVALID, "adjoint_bands must be 0 (automatic) or 1 .. %d", TransposeData::kMaxBands);
+    c->adjoint_bands = (int)value;
+    return SPOPS_OK;
+  }
   if (!strcmp(key, "batch_band")) {
     if (value < 0 || value > 1) return fail(SPOPS_ERR_INVALID, "batch_band must be 0 or 1");
     c->batch_band = (int)value;

@@ -70,6 +70,10 @@ struct Context {
   // batched k = 1: stage each CSR segment's banded x window in shared memory
   // (measured slower on the 256-matrix batch than plain gathers, so off unless set)
   int batch_band = 0;
+  // A^T x through the transpose's permutation: source-row bands (0: as many
+  // as put each band's values within 64 MB, when A's values exceed 96 MB;
+  // 1: one pass; 2..8: that many bands)
+  int adjoint_bands = 0;
   // SELL (C = 32, column-major): a chunk's slots beyond its fourth-longest
   // row are read from row-contiguous tails (1) or in place (0, the default:
   // measured faster on the power-law matrix); read when the matrix is
@@ -441,6 +445,14 @@ struct TransposeData {
   DevBuf perm;  // int64 [nnz]: entry of A at each position of A^T
   DevBuf val;   // V [nnz]
   Matrix* view = nullptr;  // CSR handle of A^T over the arrays above
+  // Source-row bands for A^T x read through perm: band b holds, row by row,
+  // the entries of A^T whose source rows lie in the b-th of nbands row ranges
+  // of about equal entry counts, so that one band's slice of A's values stays
+  // in L2 while its gathers run (adjoint.cu).  nbands = 0: not built.
+  static constexpr int kMaxBands = 8;
+  int nbands = 0;
+  DevBuf brp[kMaxBands], bri[kMaxBands], bperm[kMaxBands];  // I [cols + 1], I, int64 [band entries]
+  Matrix* bview[kMaxBands] = {};                             // CSR handles over them
   void release();
 };
 

@@ -234,3 +234,56 @@ def test_transpose_spmv_values_through_permutation(cuda, orc, itype):
                 assert err.max() <= 1e-12, (step, variant, err.max())
     finally:
         ctx.set_option("csr_variant", 0)
+
+
+@pytest.mark.parametrize("long_row", [4000, 40000])
+def test_transpose_spmv_source_row_bands(cuda, orc, long_row):
+    """A^T g through the permutation in source-row bands (context option
+    "adjoint_bands"): 1, 3 and 8 bands give the oracle's alpha A^T g + beta y
+    to 1e-12, with beta = 0 over a NaN-filled y and beta != 0 over y0, on a
+    rectangular matrix with empty rows and columns.  With one row holding
+    most entries, several of the 8 bands are empty.  Each band count gives
+    the same bits on a second call (the bands are rebuilt when the count
+    changes)."""
+    import torch
+    from sparseops_b200 import CSR_Matrix, default_context
+    from sparseops_b200._lib import call, dbl, vp
+    rng = np.random.default_rng(31)
+    n, ncols = 2500, 9000
+    lens = rng.integers(0, 30, n)
+    lens[rng.choice(n, 200, replace=False)] = 0
+    lens[5] = long_row
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([np.sort(rng.choice(ncols, L, replace=L > ncols)) for L in lens]).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    g = rng.standard_normal(n)
+    y0 = rng.standard_normal(ncols)
+    dev = torch.device("cuda")
+    A = CSR_Matrix(n, ncols, torch.from_numpy(rp.astype(np.int32)).to(dev), torch.from_numpy(ci).to(dev),
+                   torch.from_numpy(v).to(dev))
+    ctx = default_context()
+    h = A.device(ctx)
+    gd = torch.from_numpy(g).to(dev)
+    rp32 = rp.astype(np.int32)
+    at_g = orc.spmv_t(rp32, ci, v, g, ncols)
+    den = orc.spmv_t(rp32, ci, np.abs(v), np.abs(g), ncols)
+    try:
+        for bands in (1, 3, 8, 3):
+            ctx.set_option("adjoint_bands", bands)
+            for alpha, beta in ((1.0, 0.0), (0.8, 0.7)):
+                outs = []
+                for _ in range(2):
+                    call("spops_matrix_touch", h.handle)  # values "changed": the permutation path
+                    init = np.full(ncols, np.nan) if beta == 0.0 else y0
+                    out = torch.from_numpy(init.copy()).to(dev)
+                    call("spops_spmv_t", ctx.handle, dbl(alpha), h.handle, vp(gd.data_ptr()), dbl(beta),
+                         vp(out.data_ptr()))
+                    torch.cuda.synchronize()
+                    outs.append(out.cpu().numpy())
+                assert np.array_equal(outs[0], outs[1])
+                want = alpha * at_g + beta * y0
+                err = np.abs(outs[0] - want) / np.maximum(alpha * den + abs(beta) * np.abs(y0), 1e-300)
+                assert err.max() <= 1e-12, (bands, alpha, beta, err.max())
+    finally:
+        ctx.set_option("adjoint_bands", 0)
